@@ -1,0 +1,946 @@
+/*
+ * CPU oracle (test infrastructure only): plain-C restatement of the reference
+ * DG residual and FD-Jacobian algorithms, 2D quadrilaterals, Burgers and
+ * compressible Navier-Stokes. Each routine cites the reference file:line it
+ * follows (paths relative to the reference project root):
+ *   CL  = src/FiniteElement/include/iceicle/disc/conservation_law.hpp
+ *   BU  = src/FiniteElement/include/iceicle/disc/burgers.hpp
+ *   NS  = src/FiniteElement/include/iceicle/disc/navier_stokes.hpp
+ *   FR  = src/solvers/include/iceicle/form_residual.hpp
+ *   FJ  = src/solvers/include/iceicle/form_petsc_jacobian.hpp
+ *   ME  = src/FiniteElement/include/iceicle/mesh/mesh.hpp
+ *   FE  = src/FiniteElement/include/iceicle/element/finite_element.hpp
+ *   HT  = src/FiniteElement/include/iceicle/transformations/HypercubeTransformations.hpp
+ *   L1  = src/FiniteElement/include/iceicle/basis/lagrange_1d.hpp
+ *   Q1  = src/FiniteElement/include/iceicle/quadrature/quadrules_1d.hpp
+ */
+#include "oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define MAXP 8            /* max 1D nodes (basis or geometry) */
+#define MAXQ 12           /* max 1D quadrature points */
+#define MAXNB (MAXP * MAXP)
+#define MAXEQ 4
+
+/* ------------------------------------------------------------------ */
+/* 1D Lagrange basis on equispaced nodes of [-1, 1] (L1:19-212)        */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  int pn;
+  double xi[MAXP];
+  double wj[MAXP];
+} lag1d;
+
+static void lag_init(lag1d* l, int pn) {
+  l->pn = pn;
+  if (pn == 0) { l->xi[0] = 0.0; l->wj[0] = 1.0; return; }
+  double dx = 2.0 / pn;
+  l->xi[0] = -1.0;
+  for (int j = 1; j <= pn; ++j) l->xi[j] = l->xi[j - 1] + dx; /* accumulated (L1:36-40) */
+  for (int j = 0; j <= pn; ++j) {
+    double w = 1.0;
+    for (int k = 0; k <= pn; ++k) if (k != j) w *= (l->xi[j] - l->xi[k]);
+    l->wj[j] = 1.0 / w;
+  }
+}
+
+/* values and first derivatives (L1:126-195) */
+static void lag_deriv(const lag1d* l, double x, double* N, double* dN) {
+  int pn = l->pn;
+  if (pn == 0) { N[0] = 1.0; dN[0] = 0.0; return; }
+  if (pn == 1) {
+    N[0] = 0.5 * (1 - x); N[1] = 1.0 - N[0];
+    dN[0] = -0.5; dN[1] = 0.5;
+    return;
+  }
+  double lskip = 1;
+  int k;
+  for (k = 0; k < pn; ++k) {
+    if (x >= (l->xi[k] + l->xi[k + 1]) / 2) lskip *= (x - l->xi[k]);
+    else break;
+  }
+  for (int i = k + 1; i < pn + 1; ++i) lskip *= (x - l->xi[i]);
+  double lprod = lskip * (x - l->xi[k]);
+  double s = 0.0;
+  int j;
+  for (j = 0; j < k; ++j) {
+    double inv = 1.0 / (x - l->xi[j]);
+    s += inv;
+    N[j] = lprod * inv * l->wj[j];
+  }
+  N[k] = lskip * l->wj[k];
+  for (++j; j < pn + 1; ++j) {
+    double inv = 1.0 / (x - l->xi[j]);
+    s += inv;
+    N[j] = lprod * inv * l->wj[j];
+  }
+  double lprime = lprod * s + lskip;
+  for (j = 0; j < k; ++j) dN[j] = (lprime * l->wj[j] - N[j]) / (x - l->xi[j]);
+  dN[k] = s * N[k];
+  for (++j; j < pn + 1; ++j) dN[j] = (lprime * l->wj[j] - N[j]) / (x - l->xi[j]);
+}
+
+/* second derivative of the j-th Lagrange polynomial through x_m = -1 + 2m/pn:
+ * d2/dx2 prod_{m!=j}(x - x_m) / prod_{m!=j}(x_j - x_m)
+ *   = 2 sum_{a<b, a,b!=j} prod_{m!=j,a,b}(x - x_m) / denom   (L1:209) */
+static double lag_d2(int pn, int j, double x) {
+  if (pn < 2) return 0.0;
+  double nodes[MAXP];
+  for (int m = 0; m <= pn; ++m) nodes[m] = -1.0 + 2.0 * m / pn;
+  double denom = 1.0;
+  for (int m = 0; m <= pn; ++m) if (m != j) denom *= (nodes[j] - nodes[m]);
+  double sum = 0.0;
+  for (int a = 0; a <= pn; ++a) {
+    if (a == j) continue;
+    for (int b = a + 1; b <= pn; ++b) {
+      if (b == j) continue;
+      double p = 1.0;
+      for (int m = 0; m <= pn; ++m) if (m != j && m != a && m != b) p *= (x - nodes[m]);
+      sum += p;
+    }
+  }
+  return 2.0 * sum / denom;
+}
+
+/* tensor-product basis of order pn at xi (dim 0 slowest: i = i0*(pn+1)+i1),
+ * values, reference gradients [i][2], reference Hessians [i][2][2] */
+static void tp_eval(const lag1d* l, const double xi[2], double* B, double* dB, double* H) {
+  int n = l->pn + 1;
+  double N0[MAXP], N1[MAXP], d0[MAXP], d1[MAXP], s0[MAXP], s1[MAXP];
+  lag_deriv(l, xi[0], N0, d0);
+  lag_deriv(l, xi[1], N1, d1);
+  for (int j = 0; j < n; ++j) { s0[j] = lag_d2(l->pn, j, xi[0]); s1[j] = lag_d2(l->pn, j, xi[1]); }
+  for (int i0 = 0; i0 < n; ++i0)
+    for (int i1 = 0; i1 < n; ++i1) {
+      int i = i0 * n + i1;
+      if (B) B[i] = N0[i0] * N1[i1];
+      if (dB) { dB[2 * i] = d0[i0] * N1[i1]; dB[2 * i + 1] = N0[i0] * d1[i1]; }
+      if (H) {
+        H[4 * i + 0] = s0[i0] * N1[i1];
+        H[4 * i + 1] = d0[i0] * d1[i1];
+        H[4 * i + 2] = d0[i0] * d1[i1];
+        H[4 * i + 3] = N0[i0] * s1[i1];
+      }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Gauss-Legendre, points ordered (+x1, -x1, +x2, -x2, ..., 0) (Q1:21-82) */
+/* ------------------------------------------------------------------ */
+static void leg_eval(int n, double x, double* P, double* dP) {
+  double pkm1 = 1.0, pk = x, dkm1 = 0.0, dk = 1.0;
+  if (n == 0) { *P = 1.0; *dP = 0.0; return; }
+  for (int k = 1; k < n; ++k) {
+    double pkp1 = ((2 * k + 1) * x * pk - k * pkm1) / (k + 1);
+    double dkp1 = dkm1 + (2 * k + 1) * pk;
+    pkm1 = pk; pk = pkp1; dkm1 = dk; dk = dkp1;
+  }
+  *P = pk; *dP = dk;
+}
+
+static void gauss_legendre(int n, double* x, double* w) {
+  int m = n / 2;
+  double wc = 2.0;
+  for (int i = 1; i <= m; ++i) {
+    double xi = cos(M_PI * (i - 0.25) / (n + 0.5));
+    double P, dP = 0.0;
+    for (int it = 0; it < 50; ++it) {
+      leg_eval(n, xi, &P, &dP);
+      double dxi = P / dP;
+      xi -= dxi;
+      if (fabs(dxi) < 1e-16) break;
+    }
+    leg_eval(n, xi, &P, &dP);
+    double wt = 2.0 / ((1 - xi * xi) * dP * dP);
+    wc -= 2 * wt;
+    x[2 * (i - 1)] = xi;     w[2 * (i - 1)] = wt;
+    x[2 * (i - 1) + 1] = -xi; w[2 * (i - 1) + 1] = wt;
+  }
+  if (n % 2) { x[n - 1] = 0.0; w[n - 1] = wc; }
+}
+
+/* ------------------------------------------------------------------ */
+/* mesh (ME:553-913)                                                   */
+/* ------------------------------------------------------------------ */
+int orc_n_nodes(const orc_problem* pb) {
+  return (pb->nx * pb->geo_order + 1) * (pb->ny * pb->geo_order + 1);
+}
+int orc_n_faces(const orc_problem* pb) {
+  return (pb->nx - 1) * pb->ny + pb->nx * (pb->ny - 1) + 2 * pb->nx + 2 * pb->ny;
+}
+int orc_neq(const orc_problem* pb) { return pb->pde == 0 ? 1 : 4; }
+
+void orc_mesh_coords(const orc_problem* pb, double* coord) {
+  int g = pb->geo_order;
+  int nnx = pb->nx * g + 1, nny = pb->ny * g + 1;
+  for (int iy = 0; iy < nny; ++iy)
+    for (int ix = 0; ix < nnx; ++ix) {
+      int k = ix + nnx * iy;
+      coord[2 * k] = pb->xmin[0] + (pb->xmax[0] - pb->xmin[0]) * ix / (pb->nx * g);
+      coord[2 * k + 1] = pb->xmin[1] + (pb->xmax[1] - pb->xmin[1]) * iy / (pb->ny * g);
+    }
+}
+
+/* global node of local geometry node k (dim 0 slowest) of element e */
+static int el_node(const orc_problem* pb, int e, int k) {
+  int g = pb->geo_order, nnx = pb->nx * g + 1;
+  int i = e % pb->nx, j = e / pb->nx;
+  int k0 = k / (g + 1), k1 = k % (g + 1);
+  return (i * g + k0) + nnx * (j * g + k1);
+}
+
+/* reference coordinates on local face `fnr` at trace coordinate s (HT:1215-1236) */
+static void face_to_ref(int fnr, double s, double xi[2]) {
+  switch (fnr) {
+    case 0: xi[0] = -1.0; xi[1] = -s; break;
+    case 1: xi[0] = s; xi[1] = -1.0; break;
+    case 2: xi[0] = 1.0; xi[1] = s; break;
+    default: xi[0] = -s; xi[1] = 1.0; break;
+  }
+}
+/* d xi / d s for each local face */
+static const double DXI_DS[4][2] = {{0.0, -1.0}, {1.0, 0.0}, {0.0, 1.0}, {-1.0, 0.0}};
+
+/* local node (dim 0 slowest) at reference vertex xi in {-1,1}^2 */
+static int vert_local(int g, const double xi[2]) {
+  int k0 = xi[0] < 0 ? 0 : g, k1 = xi[1] < 0 ? 0 : g;
+  return k0 * (g + 1) + k1;
+}
+
+int orc_mesh_topology(const orc_problem* pb, int* conn, int* faces, int* n_interior) {
+  int g = pb->geo_order, ng = (g + 1) * (g + 1);
+  int E = pb->nx * pb->ny;
+  for (int e = 0; e < E; ++e)
+    for (int k = 0; k < ng; ++k) conn[e * ng + k] = el_node(pb, e, k);
+  int f = 0;
+  /* interior faces per direction, L element index with dim 0 fastest (ME:674-756) */
+  for (int idir = 0; idir < 2; ++idir) {
+    int ni = pb->nx - (idir == 0 ? 1 : 0), nj = pb->ny - (idir == 1 ? 1 : 0);
+    if ((idir == 0 ? pb->nx : pb->ny) <= 1) continue;
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        int L = i + pb->nx * j;
+        int R = idir == 0 ? L + 1 : L + pb->nx;
+        int fnl = 2 + idir, fnr = idir;
+        /* orientation from vertex matching (HT:1060-1129): reversed when the
+         * right face's first vertex is the left face's last vertex */
+        double a[2], b[2];
+        face_to_ref(fnr, -1.0, a);
+        face_to_ref(fnl, 1.0, b);
+        int vR0 = el_node(pb, R, vert_local(g, a));
+        int vL1 = el_node(pb, L, vert_local(g, b));
+        int orient = (vR0 == vL1) ? 1 : 0;
+        int* F = faces + 7 * f++;
+        F[0] = L; F[1] = R; F[2] = fnl; F[3] = fnr; F[4] = orient; F[5] = ORC_BC_INTERIOR; F[6] = 0;
+      }
+  }
+  *n_interior = f;
+  /* boundary faces in (-, +) pairs per direction (ME:758-892) */
+  for (int idim = 0; idim < 2; ++idim) {
+    int nb = idim == 0 ? pb->ny : pb->nx;
+    for (int t = 0; t < nb; ++t) {
+      int LA = idim == 0 ? pb->nx * t : t;
+      int LB = idim == 0 ? pb->nx * t + pb->nx - 1 : t + pb->nx * (pb->ny - 1);
+      int* F = faces + 7 * f++;
+      F[0] = LA; F[1] = -1; F[2] = idim; F[3] = 0; F[4] = 0; F[5] = pb->bctype[idim]; F[6] = pb->bcflag[idim];
+      F = faces + 7 * f++;
+      F[0] = LB; F[1] = -1; F[2] = idim + 2; F[3] = 0; F[4] = 0; F[5] = pb->bctype[idim + 2];
+      F[6] = pb->bcflag[idim + 2];
+    }
+  }
+  return f;
+}
+
+/* ------------------------------------------------------------------ */
+/* element geometry (HT:60-161, FE:220-398)                            */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  double x[MAXP * MAXP][2];
+  int ng;
+} elgeo;
+
+static void el_geo(const orc_problem* pb, const double* coord, int e, elgeo* G) {
+  int g = pb->geo_order;
+  G->ng = (g + 1) * (g + 1);
+  for (int k = 0; k < G->ng; ++k) {
+    int n = el_node(pb, e, k);
+    G->x[k][0] = coord[2 * n];
+    G->x[k][1] = coord[2 * n + 1];
+  }
+}
+
+/* x(xi), J[i][j] = dx_i/dxi_j and H[k][i][j] = d2 x_k / dxi_i dxi_j */
+static void el_map(const lag1d* lg, const elgeo* G, const double xi[2], double x[2], double J[2][2],
+                   double H[2][2][2]) {
+  double B[MAXNB], dB[2 * MAXNB], HB[4 * MAXNB];
+  tp_eval(lg, xi, B, dB, HB);
+  if (x) {
+    x[0] = x[1] = 0.0;
+    for (int k = 0; k < G->ng; ++k)
+      for (int d = 0; d < 2; ++d) x[d] += B[k] * G->x[k][d];
+  }
+  if (J) {
+    J[0][0] = J[0][1] = J[1][0] = J[1][1] = 0.0;
+    for (int k = 0; k < G->ng; ++k)
+      for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) J[i][j] += dB[2 * k + j] * G->x[k][i];
+  }
+  if (H) {
+    memset(H, 0, sizeof(double) * 8);
+    for (int k = 0; k < G->ng; ++k)
+      for (int kd = 0; kd < 2; ++kd)
+        for (int i = 0; i < 2; ++i)
+          for (int j = i; j < 2; ++j) H[kd][i][j] += HB[4 * k + 2 * i + j] * G->x[k][kd];
+    for (int kd = 0; kd < 2; ++kd) H[kd][1][0] = H[kd][0][1];
+  }
+}
+
+/* physical gradients of nb basis functions: dB/dx_j = sum_k dB/dxi_k adj[k][j] / det (FE:220-258) */
+static void phys_grad(int nb, const double J[2][2], const double* dBref, double* dBx) {
+  double adj[2][2] = {{J[1][1], -J[0][1]}, {-J[1][0], J[0][0]}};
+  double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+  if (det == 0.0) det = 1.0;
+  for (int i = 0; i < nb; ++i)
+    for (int j = 0; j < 2; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 2; ++k) s += dBref[2 * i + k] * adj[k][j];
+      dBx[2 * i + j] = s;
+    }
+  for (int i = 0; i < 2 * nb; ++i) dBx[i] /= det;
+}
+
+/* physical Hessians (FE:328-398) */
+static void phys_hess(int nb, const double J[2][2], const double H[2][2][2], const double* dBx,
+                      const double* HBref, double* HBx) {
+  double adj[2][2] = {{J[1][1], -J[0][1]}, {-J[1][0], J[0][0]}};
+  double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+  if (det == 0.0) det = 1.0;
+  double det2 = det * det;
+  for (int i = 0; i < nb; ++i) {
+    double rhs[2][2];
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b) {
+        rhs[a][b] = HBref[4 * i + 2 * a + b];
+        for (int k = 0; k < 2; ++k) rhs[a][b] -= H[k][a][b] * dBx[2 * i + k];
+      }
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b) {
+        double s = 0.0;
+        for (int k = 0; k < 2; ++k)
+          for (int l = 0; l < 2; ++l) s += adj[k][b] * adj[l][a] * rhs[l][k];
+        HBx[4 * i + 2 * a + b] = s / det2;
+      }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* physics                                                             */
+/* ------------------------------------------------------------------ */
+/* Burgers (BU:41-250) */
+static void burgers_flux(const orc_problem* pb, const double* u, const double* g, double F[][2]) {
+  for (int d = 0; d < 2; ++d) {
+    double lam = pb->a[d] + 0.5 * pb->b[d] * u[0];
+    F[0][d] = lam * u[0] - pb->mu * g[d];
+  }
+}
+static void burgers_upwind(const orc_problem* pb, const double* uL, const double* uR, const double n[2],
+                           double* f) {
+  double uavg = 0.5 * (uL[0] + uR[0]);
+  double P = 0.0;
+  for (int d = 0; d < 2; ++d) P += n[d] * (pb->a[d] + 0.5 * pb->b[d] * uavg);
+  double uup = (P > 0) ? uL[0] : uR[0];
+  double fa = 0.0;
+  for (int d = 0; d < 2; ++d) fa += n[d] * (pb->a[d] + 0.5 * pb->b[d] * uup);
+  f[0] = fa * uup;
+}
+static void burgers_diff(const orc_problem* pb, const double* u, const double* g, const double n[2],
+                         double* f) {
+  (void)u;
+  double fv = 0.0;
+  for (int d = 0; d < 2; ++d) fv += pb->mu * g[d] * n[d];
+  f[0] = fv;
+}
+
+/* Navier-Stokes, conservative variables, unit reference parameters so that
+ * Re = Eu = e_coeff = 1, CaloricallyPerfectEoS with Rgas = 287.052874 and a
+ * constant viscosity (NS:133-216, 321-449, 554-587, 700-746) */
+typedef struct {
+  double rho, mom[2], rhoE, gamma, vel[2], T, vv, p, c, E;
+} ns_state;
+
+static const double NS_RGAS = 287.052874;
+
+static void ns_thermo(const orc_problem* pb, const double* u, ns_state* s) {
+  double gamma = pb->gamma;
+  s->gamma = gamma;
+  s->rho = fmax(1e-14, u[0]);
+  s->vv = 0.0;
+  for (int d = 0; d < 2; ++d) {
+    s->mom[d] = u[1 + d];
+    s->vel[d] = u[1 + d] / s->rho;
+    s->vv += s->vel[d] * s->vel[d];
+  }
+  s->rhoE = u[3];
+  double cp = gamma / (gamma - 1) * NS_RGAS;
+  double T_coeff = cp * 1.0 * 1.0 / 1.0;
+  s->E = s->rhoE / s->rho;
+  double e = s->E - 0.5 * 1.0 * s->vv;
+  s->p = fmax(1e-12, (gamma - 1) / (1.0 * 1.0) * s->rho * e);
+  s->T = s->p / s->rho * gamma / (gamma - 1) / T_coeff;
+  s->c = sqrt((gamma * 1.0 * s->p) / s->rho);
+}
+
+/* velocity gradient gv[i][j] and total energy gradient gE[j] (NS:554-587) */
+static void ns_grads(const ns_state* s, const double* g, double gv[2][2], double gE[2]) {
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j) gv[i][j] = g[2 * (1 + i) + j] / s->rho - s->vel[i] / s->rho * g[2 * 0 + j];
+  for (int j = 0; j < 2; ++j) gE[j] = (g[2 * 3 + j] - s->E * g[2 * 0 + j]) / s->rho;
+}
+
+static void ns_tau(const orc_problem* pb, const double gv[2][2], double tau[2][2]) {
+  double mu = pb->ns_mu;
+  double div = gv[0][0] + gv[1][1];
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j) tau[i][j] = mu * (gv[i][j] + gv[j][i]);
+  for (int i = 0; i < 2; ++i) tau[i][i] -= 2.0 / 3.0 * mu * div;
+}
+
+/* physical flux (NS:916-973) */
+static void ns_flux(const orc_problem* pb, const double* u, const double* g, double F[][2]) {
+  ns_state s;
+  ns_thermo(pb, u, &s);
+  for (int j = 0; j < 2; ++j) {
+    F[0][j] = s.mom[j];
+    for (int i = 0; i < 2; ++i) F[1 + i][j] = s.mom[i] * s.vel[j];
+    F[1 + j][j] += 1.0 * s.p;
+    F[3][j] = s.vel[j] * (s.rhoE + 1.0 * 1.0 * s.p);
+  }
+  double gv[2][2], gE[2], tau[2][2], q[2];
+  ns_grads(&s, g, gv, gE);
+  ns_tau(pb, gv, tau);
+  double mu = pb->ns_mu;
+  for (int j = 0; j < 2; ++j) { /* heat flux (NS:724-745) */
+    q[j] = gE[j] / 1.0;
+    for (int k = 0; k < 2; ++k) q[j] -= s.vel[k] * gv[k][j];
+    q[j] *= mu * s.gamma / pb->Pr;
+  }
+  for (int j = 0; j < 2; ++j) {
+    double ef = q[j];
+    for (int i = 0; i < 2; ++i) {
+      F[1 + i][j] -= tau[i][j] / 1.0;
+      ef += s.vel[i] * tau[i][j];
+    }
+    ef *= 1.0 / 1.0;
+    F[3][j] -= ef;
+  }
+}
+
+/* Van Leer flux vector splitting (NS:776-864) */
+static void ns_vanleer(const orc_problem* pb, const double* uL, const double* uR, const double n[2],
+                       double* f) {
+  (void)pb;
+  ns_state L, R;
+  ns_thermo(pb, uL, &L);
+  ns_thermo(pb, uR, &R);
+  double vnL = L.vel[0] * n[0] + L.vel[1] * n[1];
+  double vnR = R.vel[0] * n[0] + R.vel[1] * n[1];
+  double mL = vnL / L.c, mR = vnR / R.c;
+  if (mL > 1) {
+    f[0] = L.rho * vnL;
+    for (int d = 0; d < 2; ++d) f[1 + d] = L.mom[d] * vnL + 1.0 * L.p * n[d];
+    f[3] = vnL * (L.rhoE + 1.0 * 1.0 * L.p);
+  } else if (mL < -1) {
+    f[0] = f[1] = f[2] = f[3] = 0.0;
+  } else {
+    double fmL = L.rho * L.c * (mL + 1) * (mL + 1) / 4.0;
+    f[0] = fmL;
+    for (int d = 0; d < 2; ++d) f[1 + d] = fmL * (L.vel[d] + n[d] * (-vnL + 2 * L.c) / L.gamma);
+    double t = (L.gamma - 1) * vnL + 2 * L.c;
+    f[3] = fmL * ((L.vv - vnL * vnL) / 2 + t * t / (2 * (L.gamma * L.gamma - 1)));
+  }
+  if (mR < -1) {
+    f[0] += R.rho * vnR;
+    for (int d = 0; d < 2; ++d) f[1 + d] += R.mom[d] * vnR + 1.0 * R.p * n[d];
+    f[3] += vnR * (R.rhoE + 1.0 * 1.0 * R.p);
+  } else if (mR <= 1) {
+    double fmR = -R.rho * R.c * (mR - 1) * (mR - 1) / 4.0;
+    f[0] += fmR;
+    for (int d = 0; d < 2; ++d) f[1 + d] += fmR * (R.vel[d] + n[d] * (-vnR - 2 * R.c) / R.gamma);
+    double t = (R.gamma - 1) * vnR - 2 * R.c;
+    f[3] += fmR * ((R.vv - vnR * vnR) / 2 + t * t / (2 * (R.gamma * R.gamma - 1)));
+  }
+}
+
+/* viscous normal flux (NS:1241-1289): the energy term is mu*gamma/Pr*dE/dx.n */
+static void ns_diff(const orc_problem* pb, const double* u, const double* g, const double n[2], double* f) {
+  ns_state s;
+  ns_thermo(pb, u, &s);
+  double gv[2][2], gE[2], tau[2][2];
+  ns_grads(&s, g, gv, gE);
+  ns_tau(pb, gv, tau);
+  f[0] = f[1] = f[2] = f[3] = 0.0;
+  double mu = pb->ns_mu;
+  for (int j = 0; j < 2; ++j) {
+    double ef = mu * s.gamma / pb->Pr * gE[j] * n[j];
+    for (int i = 0; i < 2; ++i) {
+      f[1 + i] += tau[i][j] / 1.0 * n[j];
+      ef += s.vel[i] * tau[i][j] * n[j];
+    }
+    ef *= 1.0 / 1.0;
+    f[3] += ef;
+  }
+}
+
+static void phys_flux(const orc_problem* pb, const double* u, const double* g, double F[][2]) {
+  if (pb->pde == 0) burgers_flux(pb, u, g, F);
+  else ns_flux(pb, u, g, F);
+}
+static void conv_flux(const orc_problem* pb, const double* uL, const double* uR, const double n[2], double* f) {
+  if (pb->pde == 0) burgers_upwind(pb, uL, uR, n, f);
+  else ns_vanleer(pb, uL, uR, n, f);
+}
+static void diff_flux(const orc_problem* pb, const double* u, const double* g, const double n[2], double* f) {
+  if (pb->pde == 0) burgers_diff(pb, u, g, n, f);
+  else ns_diff(pb, u, g, n, f);
+}
+
+/* ------------------------------------------------------------------ */
+/* discretization context                                              */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  const orc_problem* pb;
+  const double* coord;
+  lag1d lb, lg;      /* solution and geometry 1D bases */
+  int nb, neq, nq1, nqv;
+  double qx[MAXQ], qw[MAXQ];
+  int nf, nint;
+  int* faces;
+} disc;
+
+static int disc_init(disc* D, const orc_problem* pb, const double* coord) {
+  D->pb = pb;
+  D->coord = coord;
+  if (pb->p < 1 || pb->p >= MAXP || pb->geo_order < 1 || pb->geo_order >= MAXP) return -1;
+  lag_init(&D->lb, pb->p);
+  lag_init(&D->lg, pb->geo_order);
+  D->nb = (pb->p + 1) * (pb->p + 1);
+  D->neq = orc_neq(pb);
+  D->nq1 = pb->geo_order + pb->p; /* RE:80, RE:240-245 */
+  if (D->nq1 > MAXQ) return -1;
+  D->nqv = D->nq1 * D->nq1;
+  gauss_legendre(D->nq1, D->qx, D->qw);
+  D->nf = orc_n_faces(pb);
+  D->faces = (int*)malloc(sizeof(int) * 7 * D->nf);
+  int* conn = (int*)malloc(sizeof(int) * pb->nx * pb->ny * (pb->geo_order + 1) * (pb->geo_order + 1));
+  orc_mesh_topology(pb, conn, D->faces, &D->nint);
+  free(conn);
+  return 0;
+}
+static void disc_free(disc* D) { free(D->faces); }
+
+/* volume integral of one element (CL:244-314) */
+static void domain_integral(const disc* D, int e, const double* ue, double* re) {
+  const orc_problem* pb = D->pb;
+  int nb = D->nb, neq = D->neq;
+  elgeo G;
+  el_geo(pb, D->coord, e, &G);
+  for (int q0 = 0; q0 < D->nq1; ++q0)
+    for (int q1 = 0; q1 < D->nq1; ++q1) {
+      double xi[2] = {D->qx[q0], D->qx[q1]};
+      double w = D->qw[q0] * D->qw[q1];
+      double J[2][2], B[MAXNB], dB[2 * MAXNB], dBx[2 * MAXNB];
+      el_map(&D->lg, &G, xi, NULL, J, NULL);
+      double detJ = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+      detJ = fmax(0.0, detJ);
+      tp_eval(&D->lb, xi, B, dB, NULL);
+      phys_grad(nb, J, dB, dBx);
+      double u[MAXEQ] = {0}, g[2 * MAXEQ] = {0};
+      for (int i = 0; i < nb; ++i)
+        for (int k = 0; k < neq; ++k) u[k] += ue[i * neq + k] * B[i];
+      for (int i = 0; i < nb; ++i)
+        for (int k = 0; k < neq; ++k)
+          for (int d = 0; d < 2; ++d) g[2 * k + d] += ue[i * neq + k] * dBx[2 * i + d];
+      double F[MAXEQ][2];
+      phys_flux(pb, u, g, F);
+      for (int i = 0; i < nb; ++i)
+        for (int k = 0; k < neq; ++k)
+          for (int d = 0; d < 2; ++d) re[i * neq + k] += F[k][d] * dBx[2 * i + d] * detJ * w;
+      if (pb->source) {
+        double x[2], s[MAXEQ];
+        el_map(&D->lg, &G, xi, x, NULL, NULL);
+        pb->source(x, s, pb->source_user);
+        for (int i = 0; i < nb; ++i)
+          for (int k = 0; k < neq; ++k) re[i * neq + k] -= s[k] * B[i] * detJ * w;
+      }
+    }
+}
+
+/* volume Jacobian by flux-level finite differences (CL:316-432) */
+static void domain_integral_jacobian(const disc* D, int e, const double* ue, double* jac) {
+  const orc_problem* pb = D->pb;
+  int nb = D->nb, neq = D->neq, n = nb * neq;
+  const double sqeps = sqrt(DBL_EPSILON);
+  elgeo G;
+  el_geo(pb, D->coord, e, &G);
+  for (int q0 = 0; q0 < D->nq1; ++q0)
+    for (int q1 = 0; q1 < D->nq1; ++q1) {
+      double xi[2] = {D->qx[q0], D->qx[q1]};
+      double w = D->qw[q0] * D->qw[q1];
+      double J[2][2], B[MAXNB], dB[2 * MAXNB], dBx[2 * MAXNB];
+      el_map(&D->lg, &G, xi, NULL, J, NULL);
+      double detJ = fmax(0.0, J[0][0] * J[1][1] - J[0][1] * J[1][0]);
+      tp_eval(&D->lb, xi, B, dB, NULL);
+      phys_grad(nb, J, dB, dBx);
+      double u[MAXEQ] = {0}, g[2 * MAXEQ] = {0};
+      for (int i = 0; i < nb; ++i)
+        for (int k = 0; k < neq; ++k) u[k] += ue[i * neq + k] * B[i];
+      for (int i = 0; i < nb; ++i)
+        for (int k = 0; k < neq; ++k)
+          for (int d = 0; d < 2; ++d) g[2 * k + d] += ue[i * neq + k] * dBx[2 * i + d];
+      double F[MAXEQ][2], Fp[MAXEQ][2];
+      phys_flux(pb, u, g, F);
+      double fro = 0.0;
+      for (int k = 0; k < neq; ++k)
+        for (int d = 0; d < 2; ++d) fro += F[k][d] * F[k][d];
+      double eps = fmax(sqeps, sqrt(fro) * sqeps);
+      double dFdu[MAXEQ][2][MAXEQ], dFdg[MAXEQ][2][MAXEQ][2];
+      for (int je = 0; je < neq; ++je) {
+        double old = u[je];
+        u[je] += eps;
+        phys_flux(pb, u, g, Fp);
+        for (int k = 0; k < neq; ++k)
+          for (int d = 0; d < 2; ++d) dFdu[k][d][je] = (Fp[k][d] - F[k][d]) / eps;
+        u[je] = old;
+        for (int jd = 0; jd < 2; ++jd) {
+          double og = g[2 * je + jd];
+          g[2 * je + jd] += eps;
+          phys_flux(pb, u, g, Fp);
+          for (int k = 0; k < neq; ++k)
+            for (int d = 0; d < 2; ++d) dFdg[k][d][je][jd] = (Fp[k][d] - F[k][d]) / eps;
+          g[2 * je + jd] = og;
+        }
+      }
+      for (int it = 0; it < nb; ++it)
+        for (int ie = 0; ie < neq; ++ie)
+          for (int id = 0; id < 2; ++id)
+            for (int jt = 0; jt < nb; ++jt)
+              for (int je = 0; je < neq; ++je) {
+                double* J_ = &jac[(it * neq + ie) * n + jt * neq + je];
+                *J_ += dFdu[ie][id][je] * B[jt] * dBx[2 * it + id] * detJ * w;
+                for (int jd = 0; jd < 2; ++jd)
+                  *J_ += dFdg[ie][id][je][jd] * dBx[2 * jt + jd] * dBx[2 * it + id] * detJ * w;
+              }
+    }
+}
+
+/* per face-quadrature-point geometry (HT:1268-1330, face.hpp:410-446) */
+typedef struct {
+  double x[2], n[2], sqrtg, w;
+  double xiL[2], xiR[2];
+} faceqp;
+
+static void face_qp(const disc* D, const elgeo* GL, int fnl, int fnr, int orient, int q, faceqp* fq) {
+  double s = D->qx[q];
+  fq->w = D->qw[q];
+  face_to_ref(fnl, s, fq->xiL);
+  face_to_ref(fnr, orient ? -s : s, fq->xiR);
+  double J[2][2];
+  el_map(&D->lg, GL, fq->xiL, fq->x, J, NULL);
+  double t[2];
+  for (int i = 0; i < 2; ++i) t[i] = J[i][0] * DXI_DS[fnl][0] + J[i][1] * DXI_DS[fnl][1];
+  fq->sqrtg = sqrt(t[0] * t[0] + t[1] * t[1]);
+  double nrm[2] = {t[1], -t[0]};
+  double nn = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1]);
+  fq->n[0] = nrm[0] / nn;
+  fq->n[1] = nrm[1] / nn;
+}
+
+/* state, gradient and (optionally) Hessian of one side at a reference point */
+static void side_eval(const disc* D, const elgeo* G, const double xi[2], const double* ue, int want_hess,
+                      double* B, double* dBx, double* u, double* g, double* h) {
+  int nb = D->nb, neq = D->neq;
+  double dB[2 * MAXNB], HB[4 * MAXNB], HBx[4 * MAXNB], J[2][2], H[2][2][2];
+  tp_eval(&D->lb, xi, B, dB, HB);
+  el_map(&D->lg, G, xi, NULL, J, H);
+  phys_grad(nb, J, dB, dBx);
+  for (int k = 0; k < neq; ++k) {
+    u[k] = 0.0;
+    for (int i = 0; i < nb; ++i) u[k] += ue[i * neq + k] * B[i];
+  }
+  for (int k = 0; k < 2 * neq; ++k) g[k] = 0.0;
+  for (int i = 0; i < nb; ++i)
+    for (int k = 0; k < neq; ++k)
+      for (int d = 0; d < 2; ++d) g[2 * k + d] += ue[i * neq + k] * dBx[2 * i + d];
+  if (want_hess) {
+    phys_hess(nb, J, H, dBx, HB, HBx);
+    for (int k = 0; k < 4 * neq; ++k) h[k] = 0.0;
+    for (int i = 0; i < nb; ++i)
+      for (int k = 0; k < neq; ++k)
+        for (int a = 0; a < 4; ++a) h[4 * k + a] += ue[i * neq + k] * HBx[4 * i + a];
+  }
+}
+
+/* interior trace integral (CL:434-612) */
+static void trace_integral(const disc* D, const int* F, const double* uL, const double* uR, double* resL,
+                           double* resR) {
+  const orc_problem* pb = D->pb;
+  int nb = D->nb, neq = D->neq;
+  elgeo GL, GR;
+  el_geo(pb, D->coord, F[0], &GL);
+  el_geo(pb, D->coord, F[1], &GR);
+  double zero[2] = {0.0, 0.0}, cL[2], cR[2];
+  el_map(&D->lg, &GL, zero, cL, NULL, NULL);
+  el_map(&D->lg, &GR, zero, cR, NULL, NULL);
+  int order = pb->p;
+  double beta0 = pow(order + 1, 2);
+  double beta1 = 1 / fmax((double)(2 * order * (order + 1)), 1.0);
+  if (pb->interior_penalty) beta1 = 0.0;
+  for (int q = 0; q < D->nq1; ++q) {
+    faceqp fq;
+    face_qp(D, &GL, F[2], F[3], F[4], q, &fq);
+    double BL[MAXNB], BR[MAXNB], dBL[2 * MAXNB], dBR[2 * MAXNB];
+    double ul[MAXEQ], ur[MAXEQ], gl[2 * MAXEQ], gr[2 * MAXEQ], hl[4 * MAXEQ], hr[4 * MAXEQ];
+    side_eval(D, &GL, fq.xiL, uL, 1, BL, dBL, ul, gl, hl);
+    side_eval(D, &GR, fq.xiR, uR, 1, BR, dBR, ur, gr, hr);
+    double fadv[MAXEQ], fvis[MAXEQ];
+    conv_flux(pb, ul, ur, fq.n, fadv);
+    double h = 0.0;
+    for (int d = 0; d < 2; ++d) h += fq.n[d] * ((fq.x[d] - cL[d]) + (cR[d] - fq.x[d]));
+    h = copysign(fmax(fabs(h), DBL_EPSILON), h);
+    double gddg[2 * MAXEQ], uavg[MAXEQ];
+    for (int k = 0; k < neq; ++k) {
+      double jump = ur[k] - ul[k];
+      for (int d = 0; d < 2; ++d) {
+        gddg[2 * k + d] = beta0 * jump / h * fq.n[d] + 0.5 * (gl[2 * k + d] + gr[2 * k + d]);
+        double ht = 0.0;
+        for (int j = 0; j < 2; ++j) ht += (hr[4 * k + 2 * j + d] - hl[4 * k + 2 * j + d]) * fq.n[j];
+        gddg[2 * k + d] += beta1 * h * ht;
+      }
+    }
+    for (int k = 0; k < neq; ++k) uavg[k] = 0.5 * (ul[k] + ur[k]);
+    diff_flux(pb, uavg, gddg, fq.n, fvis);
+    for (int k = 0; k < neq; ++k) {
+      fadv[k] *= fq.w * fq.sqrtg;
+      fvis[k] *= fq.w * fq.sqrtg;
+    }
+    for (int i = 0; i < nb; ++i)
+      for (int k = 0; k < neq; ++k) resL[i * neq + k] += (fvis[k] - fadv[k]) * BL[i];
+    for (int i = 0; i < nb; ++i)
+      for (int k = 0; k < neq; ++k) resR[i * neq + k] -= (fvis[k] - fadv[k]) * BR[i];
+    /* interface correction, Burgers only (homogeneity tensor, CL:580-610) */
+    if (pb->pde == 0 && pb->sigma_ic != 0.0) {
+      for (int i = 0; i < nb; ++i)
+        for (int kd = 0; kd < 2; ++kd) {
+          double jump = ur[0] - ul[0];
+          double icc = pb->sigma_ic * pb->mu * fq.n[kd] * jump * fq.w * fq.sqrtg;
+          resL[i] -= icc * 0.5 * dBL[2 * i + kd];
+          resR[i] -= icc * 0.5 * dBR[2 * i + kd];
+        }
+    }
+  }
+}
+
+/* boundary integral (CL:631-1176) */
+static int boundary_integral(const disc* D, const int* F, const double* uL, double* resL) {
+  const orc_problem* pb = D->pb;
+  int nb = D->nb, neq = D->neq;
+  int bct = F[5], flag = F[6];
+  elgeo GL;
+  el_geo(pb, D->coord, F[0], &GL);
+  double zero[2] = {0.0, 0.0}, cL[2];
+  el_map(&D->lg, &GL, zero, cL, NULL, NULL);
+  int order = pb->p;
+  double beta0 = pow(order + 1, 2);
+  for (int q = 0; q < D->nq1; ++q) {
+    faceqp fq;
+    face_qp(D, &GL, F[2], 0, 0, q, &fq);
+    double BL[MAXNB], dBL[2 * MAXNB], ul[MAXEQ], gl[2 * MAXEQ];
+    side_eval(D, &GL, fq.xiL, uL, 0, BL, dBL, ul, gl, NULL);
+    double fadv[MAXEQ] = {0}, fvis[MAXEQ] = {0};
+    if (bct == ORC_BC_DIRICHLET) {
+      if (flag < 0 || flag >= pb->n_dirichlet) return -2;
+      double ud[MAXEQ] = {0};
+      pb->dirichlet[flag](fq.x, ud, pb->dirichlet_user[flag]);
+      conv_flux(pb, ul, ud, fq.n, fadv);
+      double h = 0.0;
+      for (int d = 0; d < 2; ++d) h += fabs(fq.n[d] * (fq.x[d] - cL[d]));
+      h = copysign(fmax(fabs(h), DBL_EPSILON), h);
+      double gddg[2 * MAXEQ], uavg[MAXEQ];
+      for (int k = 0; k < neq; ++k)
+        for (int d = 0; d < 2; ++d) gddg[2 * k + d] = beta0 * (ud[k] - ul[k]) / h * fq.n[d] + gl[2 * k + d];
+      for (int k = 0; k < neq; ++k) uavg[k] = 0.5 * (ul[k] + ud[k]);
+      diff_flux(pb, uavg, gddg, fq.n, fvis);
+      for (int k = 0; k < neq; ++k) { fadv[k] *= fq.w * fq.sqrtg; fvis[k] *= fq.w * fq.sqrtg; }
+      for (int i = 0; i < nb; ++i)
+        for (int k = 0; k < neq; ++k) resL[i * neq + k] += (fvis[k] - fadv[k]) * BL[i];
+      if (pb->pde == 0 && pb->sigma_ic != 0.0) {
+        for (int i = 0; i < nb; ++i)
+          for (int kd = 0; kd < 2; ++kd)
+            resL[i] -= pb->sigma_ic * pb->mu * fq.n[kd] * dBL[2 * i + kd] * (ud[0] - ul[0]) * fq.w * fq.sqrtg;
+      }
+    } else if (bct == ORC_BC_NEUMANN) {
+      if (flag < 0 || flag >= pb->n_neumann) return -2;
+      double gn[MAXEQ] = {0};
+      pb->neumann[flag](fq.x, gn, pb->neumann_user[flag]);
+      if (pb->pde == 0) fvis[0] = pb->mu * gn[0];
+      for (int k = 0; k < neq; ++k) fvis[k] *= fq.w * fq.sqrtg;
+      for (int i = 0; i < nb; ++i)
+        for (int k = 0; k < neq; ++k) resL[i * neq + k] += fvis[k] * BL[i];
+    } else if (bct == ORC_BC_EXTRAPOLATION || bct == ORC_BC_SPACETIME_FUTURE) {
+      conv_flux(pb, ul, ul, fq.n, fadv);
+      diff_flux(pb, ul, gl, fq.n, fvis);
+      for (int k = 0; k < neq; ++k) { fadv[k] *= fq.w * fq.sqrtg; fvis[k] *= fq.w * fq.sqrtg; }
+      for (int i = 0; i < nb; ++i)
+        for (int k = 0; k < neq; ++k) resL[i * neq + k] += (fvis[k] - fadv[k]) * BL[i];
+    } else if (pb->pde == 0) {
+      /* Burgers implements no PDE-level boundary conditions: no contribution */
+    } else {
+      return -3; /* PDE-level Navier-Stokes boundary conditions are not restated */
+    }
+  }
+  return 0;
+}
+
+int orc_form_residual(const orc_problem* pb, const double* coord, const double* u, double* res) {
+  disc D;
+  if (disc_init(&D, pb, coord)) return -1;
+  int nb = D.nb, neq = D.neq, bs = nb * neq;
+  int E = pb->nx * pb->ny;
+  memset(res, 0, sizeof(double) * (size_t)E * bs);
+  double rl[MAXNB * MAXEQ], rr[MAXNB * MAXEQ];
+  int rc = 0;
+  /* boundary faces, then interior faces, then volumes (FR:136-262) */
+  for (int f = D.nint; f < D.nf && !rc; ++f) {
+    const int* F = D.faces + 7 * f;
+    memset(rl, 0, sizeof rl);
+    rc = boundary_integral(&D, F, u + (size_t)F[0] * bs, rl);
+    for (int i = 0; i < bs; ++i) res[(size_t)F[0] * bs + i] += rl[i];
+  }
+  for (int f = 0; f < D.nint && !rc; ++f) {
+    const int* F = D.faces + 7 * f;
+    memset(rl, 0, sizeof rl);
+    memset(rr, 0, sizeof rr);
+    trace_integral(&D, F, u + (size_t)F[0] * bs, u + (size_t)F[1] * bs, rl, rr);
+    for (int i = 0; i < bs; ++i) res[(size_t)F[0] * bs + i] += rl[i];
+    for (int i = 0; i < bs; ++i) res[(size_t)F[1] * bs + i] += rr[i];
+  }
+  for (int e = 0; e < E && !rc; ++e) {
+    memset(rl, 0, sizeof rl);
+    domain_integral(&D, e, u + (size_t)e * bs, rl);
+    for (int i = 0; i < bs; ++i) res[(size_t)e * bs + i] += rl[i];
+  }
+  disc_free(&D);
+  return rc;
+}
+
+/* block pattern: per element row, itself and its face neighbours, ascending */
+int orc_bsr_pattern(const orc_problem* pb, int* rowptr, int* colidx) {
+  int E = pb->nx * pb->ny, nnz = 0;
+  rowptr[0] = 0;
+  for (int e = 0; e < E; ++e) {
+    int i = e % pb->nx, j = e / pb->nx;
+    if (j > 0) colidx[nnz++] = e - pb->nx;
+    if (i > 0) colidx[nnz++] = e - 1;
+    colidx[nnz++] = e;
+    if (i < pb->nx - 1) colidx[nnz++] = e + 1;
+    if (j < pb->ny - 1) colidx[nnz++] = e + pb->nx;
+    rowptr[e + 1] = nnz;
+  }
+  return nnz;
+}
+
+static double* block_of(const int* rowptr, const int* colidx, double* vals, int bs, int r, int c) {
+  for (int k = rowptr[r]; k < rowptr[r + 1]; ++k)
+    if (colidx[k] == c) return vals + (size_t)k * bs * bs;
+  return NULL;
+}
+
+static double vnorm(const double* v, int n) {
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += v[i] * v[i];
+  return sqrt(s);
+}
+
+/* FD Jacobian with the reference perturbation scheme (FJ:55-317) */
+int orc_form_jacobian_fd(const orc_problem* pb, const double* coord, const double* u, double* res,
+                         const int* rowptr, const int* colidx, double* vals) {
+  disc D;
+  if (disc_init(&D, pb, coord)) return -1;
+  int nb = D.nb, neq = D.neq, bs = nb * neq;
+  int E = pb->nx * pb->ny;
+  const double eps = sqrt(DBL_EPSILON);
+  memset(res, 0, sizeof(double) * (size_t)E * bs);
+  memset(vals, 0, sizeof(double) * (size_t)rowptr[E] * bs * bs);
+  double ul[MAXNB * MAXEQ], ur[MAXNB * MAXEQ], rl[MAXNB * MAXEQ], rr[MAXNB * MAXEQ];
+  double rlp[MAXNB * MAXEQ], rrp[MAXNB * MAXEQ];
+  int rc = 0;
+  for (int f = D.nint; f < D.nf && !rc; ++f) {
+    const int* F = D.faces + 7 * f;
+    memcpy(ul, u + (size_t)F[0] * bs, sizeof(double) * bs);
+    memset(rl, 0, sizeof rl);
+    rc = boundary_integral(&D, F, ul, rl);
+    for (int i = 0; i < bs; ++i) res[(size_t)F[0] * bs + i] += rl[i];
+    double es = fmax(eps, vnorm(rl, bs) * eps);
+    double* JLL = block_of(rowptr, colidx, vals, bs, F[0], F[0]);
+    for (int c = 0; c < bs && !rc; ++c) {
+      double old = ul[c];
+      ul[c] += es;
+      memset(rlp, 0, sizeof rlp);
+      rc = boundary_integral(&D, F, ul, rlp);
+      for (int r = 0; r < bs; ++r) JLL[r * bs + c] += (rlp[r] - rl[r]) / es;
+      ul[c] = old;
+    }
+  }
+  for (int f = 0; f < D.nint && !rc; ++f) {
+    const int* F = D.faces + 7 * f;
+    memcpy(ul, u + (size_t)F[0] * bs, sizeof(double) * bs);
+    memcpy(ur, u + (size_t)F[1] * bs, sizeof(double) * bs);
+    memset(rl, 0, sizeof rl);
+    memset(rr, 0, sizeof rr);
+    trace_integral(&D, F, ul, ur, rl, rr);
+    for (int i = 0; i < bs; ++i) res[(size_t)F[0] * bs + i] += rl[i];
+    for (int i = 0; i < bs; ++i) res[(size_t)F[1] * bs + i] += rr[i];
+    double es = fmax(eps, fmax(vnorm(rl, bs), vnorm(rr, bs)) * eps);
+    double* JLL = block_of(rowptr, colidx, vals, bs, F[0], F[0]);
+    double* JRL = block_of(rowptr, colidx, vals, bs, F[1], F[0]);
+    double* JLR = block_of(rowptr, colidx, vals, bs, F[0], F[1]);
+    double* JRR = block_of(rowptr, colidx, vals, bs, F[1], F[1]);
+    for (int c = 0; c < bs; ++c) {
+      double old = ul[c];
+      ul[c] += es;
+      memset(rlp, 0, sizeof rlp);
+      memset(rrp, 0, sizeof rrp);
+      trace_integral(&D, F, ul, ur, rlp, rrp);
+      for (int r = 0; r < bs; ++r) JLL[r * bs + c] += (rlp[r] - rl[r]) / es;
+      for (int r = 0; r < bs; ++r) JRL[r * bs + c] += (rrp[r] - rr[r]) / es;
+      ul[c] = old;
+    }
+    for (int c = 0; c < bs; ++c) {
+      double old = ur[c];
+      ur[c] += es;
+      memset(rlp, 0, sizeof rlp);
+      memset(rrp, 0, sizeof rrp);
+      trace_integral(&D, F, ul, ur, rlp, rrp);
+      for (int r = 0; r < bs; ++r) JLR[r * bs + c] += (rlp[r] - rl[r]) / es;
+      for (int r = 0; r < bs; ++r) JRR[r * bs + c] += (rrp[r] - rr[r]) / es;
+      ur[c] = old;
+    }
+  }
+  double* jel = (double*)malloc(sizeof(double) * bs * bs);
+  for (int e = 0; e < E && !rc; ++e) {
+    memset(rl, 0, sizeof rl);
+    domain_integral(&D, e, u + (size_t)e * bs, rl);
+    for (int i = 0; i < bs; ++i) res[(size_t)e * bs + i] += rl[i];
+    memset(jel, 0, sizeof(double) * bs * bs);
+    domain_integral_jacobian(&D, e, u + (size_t)e * bs, jel);
+    double* Jd = block_of(rowptr, colidx, vals, bs, e, e);
+    for (int i = 0; i < bs * bs; ++i) Jd[i] += jel[i];
+  }
+  free(jel);
+  disc_free(&D);
+  return rc;
+}

@@ -1,0 +1,72 @@
+/*
+ * CPU oracle for the DG residual / FD-Jacobian path: a plain-C restatement of
+ * the reference algorithm (iceicle's ConservationLawDDG with the Burgers and
+ * compressible Navier-Stokes fluxes, form_residual and form_petsc_jacobian_fd)
+ * used ONLY as the checker in tests, in smoke() and as the CPU baseline in
+ * bench.py. Nothing in the product links, imports or calls it.
+ *
+ * Parity of this restatement is pinned against the reference's own headers
+ * compiled here (oracle/ref_harness, built into oracle/_ref).
+ */
+#ifndef ICEICLE_ORACLE_H
+#define ICEICLE_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* host callback for boundary data and sources: x[2] -> out[neq] */
+typedef void (*orc_point_fn)(const double* x, double* out, void* user);
+
+/* problem description; same layout as the reference harness' ref_problem */
+typedef struct orc_problem {
+  int pde;              /* 0: Burgers, 1: Navier-Stokes */
+  int nx, ny;           /* elements per direction */
+  int geo_order;        /* geometry (node) order of the quads */
+  int p;                /* Lagrange basis order */
+  double xmin[2], xmax[2];
+  int bctype[4];        /* BOUNDARY_CONDITIONS values: left, bottom, right, top */
+  int bcflag[4];
+  int interior_penalty;
+  double sigma_ic;
+  double mu;            /* Burgers viscosity */
+  double a[2], b[2];    /* Burgers linear / nonlinear advection */
+  double gamma, Pr;     /* Navier-Stokes */
+  double ns_mu;         /* constant viscosity */
+  int n_dirichlet;
+  orc_point_fn dirichlet[8];
+  void* dirichlet_user[8];
+  int n_neumann;
+  orc_point_fn neumann[8];
+  void* neumann_user[8];
+  orc_point_fn source;
+  void* source_user;
+} orc_problem;
+
+/* reference BOUNDARY_CONDITIONS enumerators used here */
+enum {
+  ORC_BC_PERIODIC = 0, ORC_BC_PARALLEL_COM = 1, ORC_BC_NEUMANN = 2, ORC_BC_DIRICHLET = 3,
+  ORC_BC_EXTRAPOLATION = 4, ORC_BC_SPACETIME_FUTURE = 12, ORC_BC_INTERIOR = 13
+};
+
+int orc_n_nodes(const orc_problem* pb);
+int orc_n_faces(const orc_problem* pb);
+int orc_neq(const orc_problem* pb);
+/* equispaced node lattice, x fastest */
+void orc_mesh_coords(const orc_problem* pb, double* coord);
+/* element node lists and faces (elemL, elemR, face_nr_l, face_nr_r, orient, bctype, bcflag) */
+int orc_mesh_topology(const orc_problem* pb, int* conn, int* faces, int* n_interior);
+/* res = R(u); returns 0 on success */
+int orc_form_residual(const orc_problem* pb, const double* coord, const double* u, double* res);
+/* FD Jacobian (reference perturbation scheme) into block-sparse rows: block
+ * row e holds the diagonal block and one block per face neighbour, columns in
+ * ascending element order; rowptr[E+1], colidx[nnzb], vals[nnzb*bs*bs]
+ * (each block row-major). Also writes res. */
+int orc_bsr_pattern(const orc_problem* pb, int* rowptr, int* colidx);
+int orc_form_jacobian_fd(const orc_problem* pb, const double* coord, const double* u, double* res,
+                         const int* rowptr, const int* colidx, double* vals);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

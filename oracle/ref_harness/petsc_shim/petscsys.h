@@ -1,0 +1,2 @@
+#pragma once
+#include "petsc_shim_impl.h"

@@ -1,0 +1,263 @@
+// CPU reference build of the DG residual path: the reference project's own,
+// unmodified headers (ConservationLawDDG, BurgersFlux/Upwind/DiffusionFlux,
+// navier_stokes::Flux/VanLeer/DiffusionFlux, AbstractMesh, FESpace,
+// form_residual, form_petsc_jacobian_fd) compiled against the project-written
+// Numtool/PETSc stand-ins in this directory, exported through a small C ABI so
+// that tests can call it with ctypes.
+//
+// Test infrastructure only: used to pin the oracle restatement and as the
+// timed CPU baseline. Never linked into the product.
+#include <chrono>
+#include <functional>
+#include <optional>
+#include "iceicle/disc/conservation_law.hpp"
+#include "iceicle/disc/burgers.hpp"
+#include "iceicle/disc/navier_stokes.hpp"
+#include "iceicle/fespace/fespace.hpp"
+#include "iceicle/fe_function/fespan.hpp"
+#include "iceicle/fe_function/layout_right.hpp"
+#include "iceicle/form_residual.hpp"
+#ifdef REF_WITH_JACOBIAN
+#include "iceicle/form_petsc_jacobian.hpp"
+#endif
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <vector>
+
+using namespace iceicle;
+using T = double;
+using IDX = int;
+static constexpr int ndim = 2;
+
+extern "C" {
+/// host callback for boundary data and sources: x[ndim] -> out[neq]
+typedef void (*ref_point_fn)(const double* x, double* out, void* user);
+
+/// problem description shared with the oracle restatement
+struct ref_problem {
+  int pde;              // 0: Burgers, 1: Navier-Stokes
+  int nx, ny;
+  int geo_order;
+  int p;
+  double xmin[2], xmax[2];
+  int bctype[4];        // reference BOUNDARY_CONDITIONS values, order: left, bottom, right, top
+  int bcflag[4];
+  int interior_penalty;
+  double sigma_ic;
+  double mu;            // Burgers viscosity
+  double a[2], b[2];    // Burgers linear / nonlinear advection
+  double gamma, Pr;     // Navier-Stokes
+  double ns_mu;         // constant viscosity
+  int n_dirichlet;
+  ref_point_fn dirichlet[8];
+  void* dirichlet_user[8];
+  int n_neumann;
+  ref_point_fn neumann[8];
+  void* neumann_user[8];
+  ref_point_fn source;
+  void* source_user;
+};
+}
+
+namespace {
+
+// Builds the uniform hypercube mesh with the reference's constructor and then
+// writes the caller's node coordinates into it. The reference's uniform
+// constructor sizes its 1D node lattice for geometry order 1 only
+// (generate_directional_nodes makes nelem+1 points, the constructor reads
+// nelem*order+1 of them); the lattice vectors are given enough capacity that
+// those reads stay inside their allocations, and every coordinate is
+// overwritten right after construction.
+std::unique_ptr<AbstractMesh<T, IDX, ndim>> build_mesh(const ref_problem& pb, const double* coord) {
+  std::array<std::vector<T>, ndim> nodes_1d;
+  int nel[2] = {pb.nx, pb.ny};
+  for (int d = 0; d < ndim; ++d) {
+    int nfull = nel[d] * pb.geo_order + 1;
+    std::vector<T> v;
+    v.reserve(nfull);
+    for (int i = 0; i < nfull; ++i)
+      v.push_back(pb.xmin[d] + (pb.xmax[d] - pb.xmin[d]) * i / (nel[d] * pb.geo_order));
+    v.resize(nel[d] + 1);  // capacity (and contents) of the full lattice kept
+    nodes_1d[d] = std::move(v);
+  }
+  std::array<BOUNDARY_CONDITIONS, 4> bct;
+  std::array<int, 4> bcf;
+  for (int i = 0; i < 4; ++i) { bct[i] = (BOUNDARY_CONDITIONS)pb.bctype[i]; bcf[i] = pb.bcflag[i]; }
+  auto mesh = std::make_unique<AbstractMesh<T, IDX, ndim>>(nodes_1d, pb.geo_order, bct, bcf);
+  if (coord) {
+    for (std::size_t i = 0; i < mesh->coord.size(); ++i) {
+      mesh->coord[i][0] = coord[2 * i];
+      mesh->coord[i][1] = coord[2 * i + 1];
+    }
+    mesh->update_coord_els();
+  }
+  return mesh;
+}
+
+template <class Disc>
+void add_callbacks(Disc& disc, const ref_problem& pb) {
+  for (int i = 0; i < pb.n_dirichlet; ++i) {
+    ref_point_fn f = pb.dirichlet[i];
+    void* u = pb.dirichlet_user[i];
+    disc.dirichlet_callbacks.push_back([f, u](const T* x, T* out) { f(x, out, u); });
+  }
+  for (int i = 0; i < pb.n_neumann; ++i) {
+    ref_point_fn f = pb.neumann[i];
+    void* u = pb.neumann_user[i];
+    disc.neumann_callbacks.push_back([f, u](const T* x, T* out) { f(x, out, u); });
+  }
+  if (pb.source) {
+    ref_point_fn f = pb.source;
+    void* u = pb.source_user;
+    disc.user_source = std::function<void(const T*, T*)>{[f, u](const T* x, T* out) { f(x, out, u); }};
+  }
+  disc.interior_penalty = pb.interior_penalty != 0;
+  disc.sigma_ic = pb.sigma_ic;
+}
+
+// runs `body(fespace, disc)` with the discretization of the problem
+template <int P, class Body>
+int with_disc(const ref_problem& pb, const double* coord, Body&& body) {
+  auto mesh = build_mesh(pb, coord);
+  FESpace<T, IDX, ndim> fespace{mesh.get(), FESPACE_ENUMS::LAGRANGE, FESPACE_ENUMS::GAUSS_LEGENDRE,
+                                std::integral_constant<int, P>{}};
+  if (pb.pde == 0) {
+    BurgersCoefficients<T, ndim> coeffs{};
+    coeffs.mu = pb.mu;
+    coeffs.a[0] = pb.a[0]; coeffs.a[1] = pb.a[1];
+    coeffs.b[0] = pb.b[0]; coeffs.b[1] = pb.b[1];
+    BurgersFlux pf{coeffs};
+    BurgersUpwind cf{coeffs};
+    BurgersDiffusionFlux df{coeffs};
+    ConservationLawDDG disc{std::move(pf), std::move(cf), std::move(df)};
+    add_callbacks(disc, pb);
+    return body(fespace, disc, std::integral_constant<std::size_t, 1>{});
+  } else {
+    navier_stokes::ReferenceParameters<T> ref{};
+    navier_stokes::CaloricallyPerfectEoS<T, ndim> eos{};
+    eos.gamma = pb.gamma;
+    navier_stokes::constant_viscosity<T> visc{pb.ns_mu};
+    navier_stokes::Physics<T, ndim, navier_stokes::CaloricallyPerfectEoS<T, ndim>> physics{ref, eos, visc, pb.Pr};
+    navier_stokes::Flux flux{physics, std::true_type{}};
+    navier_stokes::VanLeer numflux{physics};
+    navier_stokes::DiffusionFlux dflux{physics, std::true_type{}};
+    ConservationLawDDG disc{std::move(flux), std::move(numflux), std::move(dflux)};
+    add_callbacks(disc, pb);
+    return body(fespace, disc, std::integral_constant<std::size_t, 4>{});
+  }
+}
+
+template <class Body>
+int dispatch_p(const ref_problem& pb, const double* coord, Body&& body) {
+  switch (pb.p) {
+    case 1: return with_disc<1>(pb, coord, body);
+    case 2: return with_disc<2>(pb, coord, body);
+    case 3: return with_disc<3>(pb, coord, body);
+    case 4: return with_disc<4>(pb, coord, body);
+    default: return -1;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+/// number of mesh nodes of the uniform mesh of a problem
+int ref_n_nodes(const ref_problem* pb) {
+  return (pb->nx * pb->geo_order + 1) * (pb->ny * pb->geo_order + 1);
+}
+
+/// node coordinates of the unperturbed uniform mesh, x fastest
+int ref_mesh_coords(const ref_problem* pb, double* coord_out) {
+  auto mesh = build_mesh(*pb, nullptr);
+  for (std::size_t i = 0; i < mesh->coord.size(); ++i) {
+    coord_out[2 * i] = mesh->coord[i][0];
+    coord_out[2 * i + 1] = mesh->coord[i][1];
+  }
+  return (int)mesh->coord.size();
+}
+
+/// Mesh topology as built by the reference: element node lists (conn_el,
+/// nnode per element) and faces in reference order with
+/// (elemL, elemR, face_nr_l, face_nr_r, orientation_r, bctype, bcflag).
+/// Returns the number of faces; sizes: conn_out[nelem*nnode], face_out[nface*7].
+int ref_mesh_topology(const ref_problem* pb, int* conn_out, int* face_out, int* n_interior_out) {
+  auto mesh = build_mesh(*pb, nullptr);
+  IDX nel = mesh->nelem();
+  int k = 0;
+  for (IDX e = 0; e < nel; ++e)
+    for (std::size_t j = 0; j < mesh->conn_el.rowsize(e); ++j) conn_out[k++] = mesh->conn_el[e, j];
+  int nf = (int)mesh->faces.size();
+  for (int f = 0; f < nf; ++f) {
+    const auto& fc = *mesh->faces[f];
+    face_out[7 * f + 0] = fc.elemL;
+    face_out[7 * f + 1] = fc.elemR;
+    face_out[7 * f + 2] = (int)fc.face_nr_l();
+    face_out[7 * f + 3] = (int)fc.face_nr_r();
+    face_out[7 * f + 4] = (int)(fc.face_infoR % FACE_INFO_MOD);
+    face_out[7 * f + 5] = (int)fc.bctype;
+    face_out[7 * f + 6] = fc.bcflag;
+  }
+  *n_interior_out = (int)(mesh->interiorFaceEnd - mesh->interiorFaceStart);
+  return nf;
+}
+
+/// form_residual(fespace, disc, u, res) of the reference
+int ref_form_residual(const ref_problem* pb, const double* coord, const double* u, double* res) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    fe_layout_right layout{fespace.dg_map, neq_c};
+    std::vector<T> ubuf(u, u + layout.size());
+    std::vector<T> rbuf(layout.size());
+    fespan uspan{ubuf.data(), layout};
+    fespan rspan{rbuf.data(), layout};
+    solvers::form_residual(fespace, disc, uspan, rspan);
+    std::memcpy(res, rbuf.data(), sizeof(T) * rbuf.size());
+    return 0;
+  });
+}
+
+/// time `nrep` calls of form_residual (mesh, space and disc built once);
+/// returns seconds per call through *seconds
+int ref_time_form_residual(const ref_problem* pb, const double* coord, const double* u, int nrep,
+                           double* seconds) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    fe_layout_right layout{fespace.dg_map, neq_c};
+    std::vector<T> ubuf(u, u + layout.size());
+    std::vector<T> rbuf(layout.size());
+    fespan uspan{ubuf.data(), layout};
+    fespan rspan{rbuf.data(), layout};
+    solvers::form_residual(fespace, disc, uspan, rspan);  // warm-up
+    auto t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < nrep; ++i) solvers::form_residual(fespace, disc, uspan, rspan);
+    auto t1 = std::chrono::steady_clock::now();
+    *seconds = std::chrono::duration<double>(t1 - t0).count() / nrep;
+    return 0;
+  });
+}
+
+#ifdef REF_WITH_JACOBIAN
+/// form_petsc_jacobian_fd of the reference into a dense row-major N x N
+/// matrix (small meshes only), plus the residual
+int ref_form_jacobian_dense(const ref_problem* pb, const double* coord, const double* u, double* res,
+                            double* jac_dense) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    fe_layout_right layout{fespace.dg_map, neq_c};
+    std::size_t n = layout.size();
+    std::vector<T> ubuf(u, u + n);
+    std::vector<T> rbuf(n);
+    fespan uspan{ubuf.data(), layout};
+    fespan rspan{rbuf.data(), layout};
+    Mat jac;
+    MatCreate(PETSC_COMM_WORLD, &jac);
+    MatSetSizes(jac, (PetscInt)n, (PetscInt)n, PETSC_DETERMINE, PETSC_DETERMINE);
+    solvers::form_petsc_jacobian_fd(fespace, disc, uspan, rspan, jac);
+    std::memcpy(res, rbuf.data(), sizeof(T) * n);
+    petsc_shim_to_dense(jac, jac_dense);
+    MatDestroy(&jac);
+    return 0;
+  });
+}
+#endif
+
+}  // extern "C"
