@@ -1,0 +1,279 @@
+"""Benchmark of the DG residual hot path: DOF-residual evaluations per second
+on the 2D compressible Navier-Stokes manufactured-solution workload
+(128 x 128 quads, p = 3, geometry order 2 with seeded curved-node
+perturbation, 5x5 / 5-point Gauss-Legendre, Van Leer + interior penalty, FP64).
+
+One step = one full residual evaluation R(u) of the whole mesh
+(form_residual, src/solvers/include/iceicle/form_residual.hpp:56-268).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torch.distributed.run: every rank evaluates its own replica
+(weak scaling; the single-GPU path has no data-path collective), the timed
+region is bracketed by a barrier and synchronisations and the time is the
+maximum over ranks. --impl reference times the reference's own CPU
+implementation (its headers compiled as oracle/_ref) on the host cores.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(workload="ns_mms_residual", pde="navier_stokes", mesh="128x128 quads", p=3, geometry_order=2,
+                quadrature="5x5 volume / 5 face Gauss-Legendre", conv_flux="van_leer", diffusive="interior_penalty",
+                node_perturbation="smooth seeded, 0.05 h", n_dof=1048576,
+                l2="inputs < L2; L2 flushed (256 MiB write) between timed steps")
+METRIC = "DOF-residual evals/s"
+NX = NY = 128
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ------------------------------------------------------------ CPU baseline
+def _ref_worker(args):
+    """time the reference's form_residual on the full workload in one process"""
+    nrep, seed = args
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bindings as ob
+    from specs import NS, Spec
+    spec = Spec(pde=NS, nx=NX, ny=NY, p=3, g=2, ip=True, source=True, perturb=0.05, seed=4321)
+    pb = spec.oracle_problem()
+    c = spec.coords()
+    u = spec.state(np.random.default_rng(seed))
+    s = C.c_double()
+    rc = ob.ref().fn("time_form_residual")(C.byref(pb), c.ctypes.data_as(C.c_void_p),
+                                           u.ctypes.data_as(C.c_void_p), nrep, C.byref(s))
+    assert rc == 0
+    return spec.N, s.value
+
+
+def cpu_reference(nrep, procs):
+    """aggregate throughput of `procs` concurrent single-threaded reference
+    processes (the reference is serial per MPI rank), each evaluating the full
+    workload `nrep` times"""
+    import multiprocessing as mp
+    if procs == 1:
+        res = [_ref_worker((nrep, 0))]
+    else:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            res = pool.map(_ref_worker, [(nrep, i) for i in range(procs)])
+    value = sum(n / t for n, t in res)
+    return value, res
+
+
+def run_reference(a):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bindings as ob
+    if not ob.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref not present"}))
+        return
+    procs = os.cpu_count() or 1
+    t0 = time.time()
+    # each process: one untimed warm-up evaluation, then `steps` timed ones
+    value, res = cpu_reference(a.steps, procs)
+    wall = time.time() - t0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": 0,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * np.mean([t for _, t in res]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": WORKLOAD,
+        "cpu_baseline": {"value": value, "unit": "DOF/s", "cores": procs, "kind": "reference",
+                         "sample": f"{procs} concurrent processes x full 128x128 p3 residual (reference headers, -O3)"},
+        "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------- GPU arm
+class ClockSampler:
+    def __init__(self, index):
+        self.proc = None
+        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        try:
+            os.makedirs(os.path.dirname(self.out), exist_ok=True)
+            self.f = open(self.out, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}", "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        rows = []
+        for line in open(self.out):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        smax = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def residual_work(wl):
+    """algorithmic bytes and FP64 flops of the volume+lift kernel per launch"""
+    L = wl.ctx.layout
+    E, nb, neq, nqv, nqf, F = L.n_elem, L.nbasis, L.neq, L.nq_vol, L.nq_face, L.n_faces
+    N = L.n_dof
+    # u read, res write, per-point geometry (J^-1, w det) + source, face fluxes
+    bytes_vol = 8 * (2 * N + E * nqv * (5 + neq) + F * nqf * neq)
+    flux_flops = 160  # NS physical flux incl. viscous terms, counted once per point
+    ph1 = nqv * (6 * nb * neq + 8 * neq + flux_flops + 8 * neq + 2 * neq)
+    ph2 = nb * neq * (4 * nqv + 2 * nqv + 4 * 2 * nqf)
+    flops_vol = E * (ph1 + ph2)
+    return bytes_vol, flops_vol
+
+
+def run_ours(a):
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from iceicle_b200.workloads import ns_mms_config
+    wl = ns_mms_config(nx=NX, ny=NY, p=3, geo_order=2, device=local)
+    N = wl.ctx.layout.n_dof
+    dev = torch.device("cuda", local)
+    u = torch.from_numpy(wl.u0).to(dev)
+    res = torch.empty_like(u)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(a.warmup, 3)):
+        wl.ctx.form_residual(u, res, stream)
+    torch.cuda.synchronize(dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    sampler = ClockSampler(local)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    for k in range(a.steps):
+        flush.zero_()
+        starts[k].record(stream)
+        wl.ctx.form_residual(u, res, stream)
+        ends[k].record(stream)
+    torch.cuda.synchronize(dev)
+    if ws > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    # per-kernel split (events around each kernel on the same stream)
+    t_face, t_vol = [], []
+    for _ in range(max(3, min(a.steps, 10))):
+        flush.zero_()
+        f, v = wl.ctx.form_residual_timed(u, res, stream)
+        t_face.append(f)
+        t_vol.append(v)
+    # end to end through the public API with host buffers
+    h_u = torch.from_numpy(wl.u0).pin_memory()
+    h_r = torch.empty(N, dtype=torch.float64).pin_memory()
+    e2e_s = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    e2e_e = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    for k in range(a.steps):
+        flush.zero_()
+        e2e_s[k].record(stream)
+        u.copy_(h_u, non_blocking=True)
+        wl.ctx.form_residual(u, res, stream)
+        h_r.copy_(res, non_blocking=True)
+        e2e_e[k].record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = sum(s.elapsed_time(e) for s, e in zip(e2e_s, e2e_e))
+    if ws > 1:
+        t = torch.tensor([ms, ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = t.tolist()
+    if rank == 0:
+        value = ws * N * a.steps / (ms * 1e-3)
+        e2e = ws * N * a.steps / (ms_e2e * 1e-3)
+        bytes_vol, flops_vol = residual_work(wl)
+        tv = float(np.median(t_vol)) * 1e-3
+        tf = float(np.median(t_face)) * 1e-3
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        achieved = bytes_vol / tv / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded manufactured solution)",
+            "config": dict(WORKLOAD, parallelism=f"replicas x{ws}" if ws > 1 else "single GPU"),
+            "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N},
+            "gpu_launches": 2 * a.steps,
+            "roofline": {"bound": "hbm", "kernel": "vol_lift_kernel<NS,p3,g2>", "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                         else "fallback 6650 GB/s",
+                         "traffic": None, "algorithmic_bytes": bytes_vol,
+                         "kernel_ms": {"face_flux": tf * 1e3, "vol_lift": tv * 1e3},
+                         "fp64": {"flops_per_launch": flops_vol, "achieved_tflops": flops_vol / tv / 1e12,
+                                  "nominal_peak_tflops": 37.0}},
+            "clocks": clocks,
+        }
+        if not a.no_cpu_baseline and ws == 1:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            import oracle_bindings as ob
+            if ob.ref_available():
+                n, t = _ref_worker((3, 0))
+                line["cpu_baseline"] = {"value": n / t, "unit": "DOF/s", "cores": 1, "kind": "reference",
+                                        "sample": "3 full 128x128 p3 residuals, 1 thread (reference is serial)"}
+            else:
+                line["cpu_baseline"] = None
+        print(json.dumps(line))
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

