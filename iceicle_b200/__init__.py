@@ -96,6 +96,7 @@ def lib():
             "icx_newton_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport)]),
             "icx_basis_node_coords": (C.c_int, [vp, vp]),
             "icx_form_residual_timed": (C.c_int, [vp, vp, vp, vp, dp, dp]),
+            "icx_form_residual_noalloc": (C.c_int, [vp, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -230,6 +231,12 @@ class Context:
 
     def form_residual(self, u, res, stream=None):
         self._check(lib().icx_form_residual(self._h, _ptr(u), _ptr(res), _stream_ptr(stream)), "form_residual")
+
+    def form_residual_noalloc(self, u, res, stream=None):
+        """icx_form_residual_noalloc: same result, face scratch in a fixed
+        device array instead of context memory; allocates nothing"""
+        self._check(lib().icx_form_residual_noalloc(self._h, _ptr(u), _ptr(res), _stream_ptr(stream)),
+                    "form_residual_noalloc")
 
     def form_residual_timed(self, u, res, stream=None):
         """(ms face kernel, ms volume kernel) from CUDA events; synchronises"""

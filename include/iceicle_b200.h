@@ -106,6 +106,20 @@ icx_status icx_get_layout(const icx_ctx* ctx, icx_layout_info* info);
  * length n_dof in the reference layout u[(elem*nbasis + idof)*neq + ieq]. */
 icx_status icx_form_residual(icx_ctx* ctx, const double* d_u, double* d_res, void* stream);
 
+/* Allocation-free variant of icx_form_residual (no counterpart in the
+ * reference, which has no device code). For callers that cannot allocate
+ * device memory while they evaluate residuals: a host framework that owns all
+ * device memory through its own pool and forbids other allocations during a
+ * solve, or a time-critical loop that must not pay the device-wide
+ * synchronisation of cudaMalloc/cudaFree. It calls no allocating routine; the
+ * face-flux scratch lives in a fixed 8 MiB __device__ array per device, so it
+ * serves problems with n_faces * nq_face * neq <= 2^20 (the 128x128 p=3
+ * Navier-Stokes mesh needs 660,480) and returns ICX_ERR_SIZE beyond that.
+ * The first call on a device looks up the array's address (make it before
+ * any stream capture on that device). All calls on a device share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+icx_status icx_form_residual_noalloc(icx_ctx* ctx, const double* d_u, double* d_res, void* stream);
+
 /* diagnostics: the same computation as icx_form_residual, with CUDA events
  * around each kernel on `stream`; synchronises and returns the two kernel
  * durations in milliseconds (face fluxes, volume + face lifting). */
