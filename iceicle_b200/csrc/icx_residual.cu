@@ -20,20 +20,10 @@
 #include <cstdio>
 
 #include "icx_internal.h"
-#include "icx_physics.cuh"
+#include "icx_dg.cuh"
 
 namespace icx {
 
-template <int PDE, int P, int G>
-struct Cfg {
-  static constexpr int NEQ = Phys<PDE>::NEQ;
-  static constexpr int NB = (P + 1) * (P + 1);
-  static constexpr int BS = NB * NEQ;
-  static constexpr int NQ1 = G + P;
-  static constexpr int NQV = NQ1 * NQ1;
-  static constexpr int NQF = NQ1;
-  static constexpr int NG = (G + 1) * (G + 1);
-};
 
 __constant__ double c_dxi_ds[4][2] = {{0.0, -1.0}, {1.0, 0.0}, {0.0, 1.0}, {-1.0, 0.0}};
 
@@ -156,175 +146,6 @@ __global__ void geo_face_kernel(DeviceMesh dm) {
 }
 
 // ------------------------------------------------------------- face fluxes
-// value, physical gradient and (if WANT_H) physical Hessian of the solution
-// on one side of a face point. tab: [NB][6] = phi, dphi/dxi0, dphi/dxi1, h00, h01, h11.
-template <int NB, int NEQ, bool WANT_H>
-__device__ inline void side_state(const double* __restrict__ ue, const double* __restrict__ tab, const double* Ji,
-                                  const double* Hm, double* u, double* gx, double* hx) {
-  double gxi[NEQ][2], hxi[NEQ][3];
-#pragma unroll
-  for (int eq = 0; eq < NEQ; ++eq) {
-    u[eq] = 0.0;
-    gxi[eq][0] = gxi[eq][1] = 0.0;
-    hxi[eq][0] = hxi[eq][1] = hxi[eq][2] = 0.0;
-  }
-#pragma unroll 4
-  for (int i = 0; i < NB; ++i) {
-    const double* t = tab + i * 6;
-    double phi = t[0], d0 = t[1], d1 = t[2];
-#pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) {
-      double c = ue[i * NEQ + eq];
-      u[eq] += c * phi;
-      gxi[eq][0] += c * d0;
-      gxi[eq][1] += c * d1;
-      if (WANT_H) {
-        hxi[eq][0] += c * t[3];
-        hxi[eq][1] += c * t[4];
-        hxi[eq][2] += c * t[5];
-      }
-    }
-  }
-#pragma unroll
-  for (int eq = 0; eq < NEQ; ++eq) {
-#pragma unroll
-    for (int d = 0; d < 2; ++d) gx[eq * 2 + d] = gxi[eq][0] * Ji[0 * 2 + d] + gxi[eq][1] * Ji[1 * 2 + d];
-    if (WANT_H) {
-      // Hx = Ji^T (Hxi - sum_m H_m dx_m) Ji  (finite_element.hpp:328-398, contracted first)
-      double rhs[2][2];
-      double r00 = hxi[eq][0] - Hm[0] * gx[eq * 2 + 0] - Hm[3] * gx[eq * 2 + 1];
-      double r01 = hxi[eq][1] - Hm[1] * gx[eq * 2 + 0] - Hm[4] * gx[eq * 2 + 1];
-      double r11 = hxi[eq][2] - Hm[2] * gx[eq * 2 + 0] - Hm[5] * gx[eq * 2 + 1];
-      rhs[0][0] = r00; rhs[0][1] = r01; rhs[1][0] = r01; rhs[1][1] = r11;
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-          double s = 0.0;
-#pragma unroll
-          for (int l = 0; l < 2; ++l)
-#pragma unroll
-            for (int kk = 0; kk < 2; ++kk) s += Ji[l * 2 + a] * rhs[l][kk] * Ji[kk * 2 + b];
-          hx[eq * 4 + a * 2 + b] = s;
-        }
-    }
-  }
-}
-
-// numerical flux at one face point; writes out[NEQ] = (f_visc - f_adv) w sqrt(g)
-// and, when the interface correction is active, gq[2][NEQ][2] (left, right).
-template <int PDE, int P, int G, bool DDG>
-__device__ inline void face_point_flux(const DeviceMesh& dm, const PhysParams& pp, int f, int q,
-                                       const double* __restrict__ uL_coef, const double* __restrict__ uR_coef,
-                                       double* out, double* gq) {
-  using C = Cfg<PDE, P, G>;
-  constexpr int NEQ = C::NEQ, NB = C::NB, NQF = C::NQF;
-  const int* fi = dm.face_info + 8 * f;
-  int R = fi[1], fnl = fi[2], fnr = fi[3], orient = fi[4], bct = fi[5], bidx = fi[7];
-  int nfq = dm.F * NQF, k = f * NQF + q;
-  const double* g = dm.fgeo;
-  double n[2] = {g[FG_N0 * nfq + k], g[FG_N1 * nfq + k]};
-  double wsq = g[FG_WSQ * nfq + k], h = g[FG_H * nfq + k];
-  double JiL[4], HL[6];
-#pragma unroll
-  for (int a = 0; a < 4; ++a) JiL[a] = g[(FG_JIL + a) * nfq + k];
-#pragma unroll
-  for (int a = 0; a < 6; ++a) HL[a] = g[(FG_HL + a) * nfq + k];
-  double uL[NEQ], gL[2 * NEQ], hL[4 * NEQ];
-  side_state<NB, NEQ, DDG>(uL_coef, dm.tab_face + (size_t)((fnl * 2 + 0) * NQF + q) * NB * 6, JiL, HL, uL, gL, hL);
-  double fadv[NEQ], fvis[NEQ];
-  bool ic = Phys<PDE>::has_ic && pp.sigma_ic != 0.0;
-  if (R >= 0) {
-    double JiR[4], HR[6];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) JiR[a] = g[(FG_JIR + a) * nfq + k];
-#pragma unroll
-    for (int a = 0; a < 6; ++a) HR[a] = g[(FG_HR + a) * nfq + k];
-    double uR[NEQ], gR[2 * NEQ], hR[4 * NEQ];
-    side_state<NB, NEQ, DDG>(uR_coef, dm.tab_face + (size_t)((fnr * 2 + orient) * NQF + q) * NB * 6, JiR, HR, uR,
-                             gR, hR);
-    Phys<PDE>::conv(pp, uL, uR, n, fadv);
-    double gddg[2 * NEQ], uavg[NEQ];
-#pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) {
-      double jump = uR[eq] - uL[eq];
-#pragma unroll
-      for (int d = 0; d < 2; ++d) {
-        double v = pp.beta0 * jump / h * n[d] + 0.5 * (gL[eq * 2 + d] + gR[eq * 2 + d]);
-        if (DDG) {
-          double ht = (hR[eq * 4 + 0 * 2 + d] - hL[eq * 4 + 0 * 2 + d]) * n[0] +
-                      (hR[eq * 4 + 1 * 2 + d] - hL[eq * 4 + 1 * 2 + d]) * n[1];
-          v += pp.beta1 * h * ht;
-        }
-        gddg[eq * 2 + d] = v;
-      }
-      uavg[eq] = 0.5 * (uL[eq] + uR[eq]);
-    }
-    Phys<PDE>::diff(pp, uavg, gddg, n, fvis);
-#pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq - fadv[eq] * wsq;
-    if (ic) {
-      // resL, resR -= sum_s (sigma mu n_s [u] w sqrt(g) / 2) dphi/dx_s   (conservation_law.hpp:580-610)
-      double cs[2];
-#pragma unroll
-      for (int s = 0; s < 2; ++s) cs[s] = 0.5 * pp.sigma_ic * pp.mu * n[s] * (uR[0] - uL[0]) * wsq;
-#pragma unroll
-      for (int kk = 0; kk < 2; ++kk) {
-        gq[0 * 2 + kk] = cs[0] * JiL[kk * 2 + 0] + cs[1] * JiL[kk * 2 + 1];
-        gq[1 * 2 + kk] = cs[0] * JiR[kk * 2 + 0] + cs[1] * JiR[kk * 2 + 1];
-      }
-    }
-  } else {
-    if (bct == ICX_BC_DIRICHLET) {
-      const double* ud = dm.bvals + ((size_t)bidx * NQF + q) * NEQ;
-      double udv[NEQ];
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) udv[eq] = ud[eq];
-      Phys<PDE>::conv(pp, uL, udv, n, fadv);
-      double gddg[2 * NEQ], uavg[NEQ];
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) {
-#pragma unroll
-        for (int d = 0; d < 2; ++d) gddg[eq * 2 + d] = pp.beta0 * (udv[eq] - uL[eq]) / h * n[d] + gL[eq * 2 + d];
-        uavg[eq] = 0.5 * (uL[eq] + udv[eq]);
-      }
-      Phys<PDE>::diff(pp, uavg, gddg, n, fvis);
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq - fadv[eq] * wsq;
-      if (ic) {
-        double cs[2];
-#pragma unroll
-        for (int s = 0; s < 2; ++s) cs[s] = pp.sigma_ic * pp.mu * n[s] * (udv[0] - uL[0]) * wsq;
-#pragma unroll
-        for (int kk = 0; kk < 2; ++kk) {
-          gq[0 * 2 + kk] = cs[0] * JiL[kk * 2 + 0] + cs[1] * JiL[kk * 2 + 1];
-          gq[1 * 2 + kk] = 0.0;
-        }
-      }
-    } else if (bct == ICX_BC_NEUMANN) {
-      const double* gnv = dm.bvals + ((size_t)bidx * NQF + q) * NEQ;
-      double gn[NEQ];
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) gn[eq] = gnv[eq];
-      Phys<PDE>::neumann(pp, gn, fvis);
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq;
-      if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
-    } else if (bct == ICX_BC_EXTRAPOLATION || bct == ICX_BC_SPACETIME_FUTURE) {
-      Phys<PDE>::conv(pp, uL, uL, n, fadv);
-      Phys<PDE>::diff(pp, uL, gL, n, fvis);
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq - fadv[eq] * wsq;
-      if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
-    } else {
-      // boundary kinds the PDE does not implement contribute nothing
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) out[eq] = 0.0;
-      if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
-    }
-  }
-}
-
 template <int PDE, int P, int G, bool DDG>
 __global__ void face_flux_kernel(DeviceMesh dm, PhysParams pp, const double* __restrict__ u) {
   using C = Cfg<PDE, P, G>;
