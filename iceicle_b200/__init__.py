@@ -97,6 +97,7 @@ def lib():
             "icx_basis_node_coords": (C.c_int, [vp, vp]),
             "icx_form_residual_timed": (C.c_int, [vp, vp, vp, vp, dp, dp]),
             "icx_form_residual_noalloc": (C.c_int, [vp, vp, vp, vp]),
+            "icx_gmres_solve": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, ip, dp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -258,6 +259,15 @@ class Context:
 
     def bsr_spmv(self, vals, x, y, stream=None):
         self._check(lib().icx_bsr_spmv(self._h, _ptr(vals), _ptr(x), _ptr(y), _stream_ptr(stream)), "bsr_spmv")
+
+    def gmres_solve(self, vals, b, x, restart=30, maxit=2000, rtol=1e-5, preconditioner=2, stream=None):
+        """(iterations, relative residual, converged) of J x = b"""
+        it, rr = C.c_int(), C.c_double()
+        st = lib().icx_gmres_solve(self._h, _ptr(vals), _ptr(b), _ptr(x), restart, maxit, rtol, preconditioner,
+                                   C.byref(it), C.byref(rr), _stream_ptr(stream))
+        if st not in (0, 5):
+            self._check(st, "gmres_solve")
+        return it.value, rr.value, st == 0
 
     def newton_solve(self, u, options=None):
         opt = options or default_newton_options()

@@ -259,6 +259,7 @@ icx_status icx_create(icx_ctx** out, int device) {
 void icx_destroy(icx_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
+  icx::free_solver_work(c);
   free_dev(c->dm);
   for (void* p : c->scratch)
     if (p) cudaFree(p);

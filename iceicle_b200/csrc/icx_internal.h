@@ -85,6 +85,7 @@ struct icx_ctx {
   icx::DeviceMesh dm;
   // solver scratch (device), grown on demand
   std::vector<void*> scratch;
+  struct icx_solver_work* sw = nullptr;  // Newton / GMRES buffers (icx_solver.cu)
 };
 
 namespace icx {
@@ -98,4 +99,6 @@ cudaError_t launch_jacobian_fd(const DeviceMesh& dm, const PhysParams& pp, const
                                double* vals, double eps, cudaStream_t s);
 cudaError_t launch_bsr_spmv(const DeviceMesh& dm, const double* vals, const double* x, double* y,
                             cudaStream_t s);
+// releases the Newton / GMRES buffers of a context (icx_solver.cu)
+void free_solver_work(icx_ctx* c);
 }  // namespace icx

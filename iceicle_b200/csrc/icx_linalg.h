@@ -1,0 +1,30 @@
+// Device linear algebra used by the Newton solver (icx_linalg.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "icx_internal.h"
+
+namespace icx {
+
+struct LinalgWork {
+  double* partial = nullptr;  // [32 vectors][296 blocks] partial dot products
+};
+
+// d_out[j] = V_j . x for j < nvec, V_j = V + j * ld (deterministic two-stage reduction)
+cudaError_t la_mdot(LinalgWork& w, long long n, const double* V, long long ld, int nvec, const double* x,
+                    double* d_out, cudaStream_t s);
+// w += sign * sum_j d_h[j] V_j
+cudaError_t la_maxpy(long long n, const double* V, long long ld, int nvec, const double* d_h, double sign, double* w,
+                     cudaStream_t s);
+cudaError_t la_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);
+cudaError_t la_xpay(long long n, const double* x, double a, const double* y, double* z, cudaStream_t s);
+// dst[b] = inv(src[blk_index[b]]) for b < nblk (bs x bs blocks); *flag set on a singular block
+cudaError_t la_block_invert(int nblk, int bs, const double* src, const int* blk_index, double* dst, int* flag,
+                            cudaStream_t s);
+cudaError_t la_block_diag_apply(int E, int bs, const double* D, const double* x, double* y, cudaStream_t s);
+// block-ILU(0) on the structured element grid: LU holds a copy of the BSR values on entry
+cudaError_t la_ilu_factor(const DeviceMesh& dm, int nx, int ny, double* LU, double* Uinv, int* flag, cudaStream_t s);
+cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU, const double* Uinv, const double* x,
+                         double* y, cudaStream_t s);
+
+}  // namespace icx

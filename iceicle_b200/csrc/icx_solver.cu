@@ -1,15 +1,273 @@
-// C ABI of the FD Jacobian and BSR products; the Newton driver.
+// Newton solver around the GPU residual and FD Jacobian:
+//   PetscNewton::solve (src/solvers/include/iceicle/petsc_newton.hpp:205-329)
+//   with the reference's line searches (nonlinear_solver_utils.hpp:83-191)
+// and the linear solve J du = r by restarted, right-preconditioned GMRES(m)
+// (classical Gram-Schmidt with one re-orthogonalisation, FP64 Hessenberg and
+// Givens rotations on the host) with block-Jacobi or block-ILU(0)
+// preconditioning on the BSR Jacobian. Every vector operation runs on the
+// device; the host holds only the (m+1) x m Hessenberg matrix and the scalar
+// line-search logic.
 #include <cfloat>
 #include <cmath>
+#include <cstring>
+#include <functional>
+#include <vector>
 
 #include "icx_internal.h"
+#include "icx_linalg.h"
+
+struct icx_solver_work {
+  long long n = 0;
+  int nnzb = 0, bs = 0, m = 0;
+  double* vals = nullptr;   // Jacobian
+  double* pc = nullptr;     // preconditioner: block inverses (Jacobi) or ILU factors
+  double* uinv = nullptr;   // ILU: inverses of the U diagonal blocks
+  double* V = nullptr;      // Krylov basis, (m + 1) x n
+  double* w = nullptr;      // work vectors
+  double* z = nullptr;
+  double* r = nullptr;
+  double* du = nullptr;
+  double* ustep = nullptr;
+  double* rwork = nullptr;
+  double* dh = nullptr;     // device scalars (dot results)
+  int* flag = nullptr;
+  icx::LinalgWork lw;
+};
 
 namespace {
+
 icx_status set_err(icx_ctx* c, icx_status st, const std::string& m) {
   if (c) c->err = m;
   return st;
 }
+
+#define CK(expr)                                                                       \
+  do {                                                                                 \
+    cudaError_t _e = (expr);                                                           \
+    if (_e != cudaSuccess) return set_err(c, ICX_ERR_CUDA, std::string(#expr) + ": " + \
+                                                              cudaGetErrorString(_e)); \
+  } while (0)
+
+icx_status ensure_work(icx_ctx* c, int m) {
+  const icx::DeviceMesh& dm = c->dm;
+  long long n = (long long)dm.E * dm.nb * dm.neq;
+  int bs = dm.nb * dm.neq;
+  icx_solver_work*& w = c->sw;
+  if (w && w->n == n && w->nnzb == dm.nnzb && w->bs == bs && w->m >= m) return ICX_OK;
+  icx::free_solver_work(c);
+  w = new icx_solver_work();
+  w->n = n;
+  w->nnzb = dm.nnzb;
+  w->bs = bs;
+  w->m = m;
+  size_t vb = sizeof(double) * (size_t)dm.nnzb * bs * bs;
+  CK(cudaMalloc((void**)&w->vals, vb));
+  CK(cudaMalloc((void**)&w->pc, vb));
+  CK(cudaMalloc((void**)&w->uinv, sizeof(double) * (size_t)dm.E * bs * bs));
+  CK(cudaMalloc((void**)&w->V, sizeof(double) * (size_t)(m + 1) * n));
+  double** vecs[] = {&w->w, &w->z, &w->r, &w->du, &w->ustep, &w->rwork};
+  for (double** p : vecs) CK(cudaMalloc((void**)p, sizeof(double) * n));
+  CK(cudaMalloc((void**)&w->dh, sizeof(double) * 2 * (m + 2)));
+  CK(cudaMalloc((void**)&w->flag, sizeof(int)));
+  CK(cudaMalloc((void**)&w->lw.partial, sizeof(double) * 64 * 296));
+  return ICX_OK;
+}
+
+double dev_norm(icx_ctx* c, const double* x, cudaStream_t s) {
+  icx_solver_work* w = c->sw;
+  icx::la_mdot(w->lw, w->n, x, 0, 1, x, w->dh, s);
+  double h = 0.0;
+  cudaMemcpyAsync(&h, w->dh, sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  return std::sqrt(h);
+}
+
+// z = M^-1 x
+cudaError_t apply_pc(icx_ctx* c, int kind, const double* x, double* z, cudaStream_t s) {
+  icx_solver_work* w = c->sw;
+  const icx::DeviceMesh& dm = c->dm;
+  if (kind == 1) return icx::la_block_diag_apply(dm.E, w->bs, w->pc, x, z, s);
+  if (kind == 2) return icx::la_ilu_apply(dm, c->nx, c->ny, w->pc, w->uinv, x, z, s);
+  return cudaMemcpyAsync(z, x, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
+}
+
+// builds the preconditioner from w->vals
+cudaError_t build_pc(icx_ctx* c, int kind, cudaStream_t s) {
+  icx_solver_work* w = c->sw;
+  const icx::DeviceMesh& dm = c->dm;
+  cudaMemsetAsync(w->flag, 0, sizeof(int), s);
+  if (kind == 1) return icx::la_block_invert(dm.E, w->bs, w->vals, dm.bsr_diag, w->pc, w->flag, s);
+  if (kind == 2) {
+    cudaError_t e = cudaMemcpyAsync(w->pc, w->vals, sizeof(double) * (size_t)dm.nnzb * w->bs * w->bs,
+                                    cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return e;
+    return icx::la_ilu_factor(dm, c->nx, c->ny, w->pc, w->uinv, w->flag, s);
+  }
+  return cudaSuccess;
+}
+
+// x = J^-1 b by GMRES(m), right preconditioning; returns iterations, writes the
+// final relative residual estimate
+icx_status gmres(icx_ctx* c, int pc, int m, int maxit, double rtol, const double* b, double* x, int* iters,
+                 double* relres, cudaStream_t s) {
+  icx_solver_work* w = c->sw;
+  const icx::DeviceMesh& dm = c->dm;
+  long long n = w->n;
+  CK(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+  double bnorm = dev_norm(c, b, s);
+  *iters = 0;
+  *relres = 0.0;
+  if (bnorm == 0.0) return ICX_OK;
+  if (!std::isfinite(bnorm)) return set_err(c, ICX_ERR_NONFINITE, "non-finite right-hand side");
+  double tol = rtol * bnorm;
+  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hcol(m + 2);
+  CK(cudaMemcpyAsync(w->r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  double beta = bnorm;
+  int total = 0;
+  while (true) {
+    CK(icx::la_axpby(n, 1.0 / beta, w->r, 0.0, w->V, s));
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int j = 0;
+    double resid = beta;
+    for (; j < m && total < maxit; ++j) {
+      double* vj = w->V + (size_t)j * n;
+      double* vj1 = w->V + (size_t)(j + 1) * n;
+      CK(apply_pc(c, pc, vj, w->z, s));
+      CK(icx::launch_bsr_spmv(dm, w->vals, w->z, vj1, s));
+      // classical Gram-Schmidt, twice
+      std::fill(hcol.begin(), hcol.end(), 0.0);
+      for (int pass = 0; pass < 2; ++pass) {
+        CK(icx::la_mdot(w->lw, n, w->V, n, j + 1, vj1, w->dh, s));
+        CK(icx::la_maxpy(n, w->V, n, j + 1, w->dh, -1.0, vj1, s));
+        std::vector<double> hp(j + 1);
+        CK(cudaMemcpyAsync(hp.data(), w->dh, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (int i = 0; i <= j; ++i) hcol[i] += hp[i];
+      }
+      double hn = dev_norm(c, vj1, s);
+      hcol[j + 1] = hn;
+      if (!std::isfinite(hn)) return set_err(c, ICX_ERR_NONFINITE, "non-finite Krylov vector");
+      if (hn > 0.0) CK(icx::la_axpby(n, 1.0 / hn, vj1, 0.0, vj1, s));
+      // apply the previous rotations, then a new one
+      for (int i = 0; i < j; ++i) {
+        double t = cs[i] * hcol[i] + sn[i] * hcol[i + 1];
+        hcol[i + 1] = -sn[i] * hcol[i] + cs[i] * hcol[i + 1];
+        hcol[i] = t;
+      }
+      double den = std::hypot(hcol[j], hcol[j + 1]);
+      cs[j] = den == 0.0 ? 1.0 : hcol[j] / den;
+      sn[j] = den == 0.0 ? 0.0 : hcol[j + 1] / den;
+      hcol[j] = den;
+      hcol[j + 1] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hcol[i];
+      ++total;
+      resid = std::fabs(g[j + 1]);
+      if (resid <= tol || hn == 0.0) { ++j; break; }
+    }
+    // y = H^-1 g (upper triangular j x j), x += M^-1 (V y)
+    for (int i = j - 1; i >= 0; --i) {
+      double sacc = g[i];
+      for (int k = i + 1; k < j; ++k) sacc -= H[(size_t)i * m + k] * y[k];
+      y[i] = sacc / H[(size_t)i * m + i];
+    }
+    CK(cudaMemcpyAsync(w->dh, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(w->w, 0, sizeof(double) * n, s));
+    CK(icx::la_maxpy(n, w->V, n, j, w->dh, 1.0, w->w, s));
+    CK(apply_pc(c, pc, w->w, w->z, s));
+    CK(icx::la_axpby(n, 1.0, w->z, 1.0, x, s));
+    // true residual for the restart
+    CK(icx::launch_bsr_spmv(dm, w->vals, x, w->w, s));
+    CK(icx::la_xpay(n, b, -1.0, w->w, w->r, s));
+    beta = dev_norm(c, w->r, s);
+    *relres = beta / bnorm;
+    if (beta <= tol || total >= maxit || resid <= tol) break;
+  }
+  *iters = total;
+  return ICX_OK;
+}
+
+// wolfe_ls / zoom / corrigan_ls of the reference (nonlinear_solver_utils.hpp:83-191)
+double finite_difference(const std::function<double(double)>& f, double eps, double x) {
+  double a = f(x), b = f(x + eps);
+  return (b - a) / eps;
+}
+
+double zoom(const std::function<double(double)>& f, double lo, double hi, int kmax, double c1, double c2) {
+  const double EPS = std::sqrt(DBL_EPSILON);
+  for (int k = 0; k < kmax; ++k) {
+    double phi_lo = f(lo), dphi_lo = finite_difference(f, EPS, lo);
+    double phi_hi = f(hi), dphi_hi = finite_difference(f, EPS, hi);
+    double d1 = dphi_lo + dphi_hi - 3 * (phi_lo - phi_hi) / (lo - hi);
+    double d2 = std::sqrt(std::max(d1 * d1 - dphi_lo * dphi_hi, 1e-8));
+    d2 = std::copysign(d2, hi - lo);
+    double aj = hi - (hi - lo) * ((dphi_hi + d2 - d1) / (dphi_hi - dphi_lo + 2 * d2));
+    double phi_aj = f(aj);
+    double dphi_0 = finite_difference(f, EPS, 0.0);
+    if (phi_aj > (f(0) + c1 * aj * dphi_0) || phi_aj >= phi_lo) {
+      hi = aj;
+    } else {
+      double dphi_aj = finite_difference(f, EPS, aj);
+      if (std::fabs(dphi_aj) <= -c2 * dphi_0) return aj;
+      if (dphi_aj * (hi - lo) >= 0) hi = lo;
+      lo = aj;
+    }
+  }
+  return 0.5 * (lo + hi);
+}
+
+double wolfe_ls(const std::function<double(double)>& f, double alpha_max, double alpha1, int kmax, double c1,
+                double c2) {
+  const double EPS = std::sqrt(DBL_EPSILON);
+  double a_im1 = 0, a_i = alpha1;
+  double phi_0 = f(0);
+  double dphi_0 = finite_difference(f, EPS, 0.0);
+  for (int k = 0; k < kmax; ++k) {
+    double phi_i = f(a_i), phi_im1 = f(a_im1);
+    if (phi_i > phi_0 + c1 * a_i * dphi_0 || (phi_i >= phi_im1 && k > 0)) return zoom(f, a_im1, a_i, kmax, c1, c2);
+    double dphi_i = finite_difference(f, EPS, a_i);
+    if (std::fabs(dphi_i) <= -c2 * dphi_0) return a_i;
+    if (dphi_i >= 0) return zoom(f, a_i, a_im1, kmax, c1, c2);
+    double t = 0.5 * (a_i + alpha_max);
+    a_im1 = a_i;
+    a_i = t;
+  }
+  return a_i;
+}
+
+double corrigan_ls(const std::function<double(double)>& f, double alpha_max, double alpha1, int kmax,
+                   double alpha_min) {
+  double alpha_a = alpha_min, alpha_b = alpha_max, alpha = alpha1;
+  for (int k = 0; k < kmax; ++k) {
+    double phi_0 = f(0);
+    if (k > 0) alpha = (alpha_a + alpha_b) / 2;
+    double phi_star = f(alpha);
+    if (std::fabs(phi_star) < std::fabs(phi_0)) {
+      if (alpha == alpha1) break;
+      alpha_a = alpha;
+    } else {
+      alpha_b = alpha;
+    }
+  }
+  return alpha;
+}
+
 }  // namespace
+
+namespace icx {
+void free_solver_work(icx_ctx* c) {
+  if (!c || !c->sw) return;
+  icx_solver_work* w = c->sw;
+  void* ptrs[] = {w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->du, w->ustep, w->rwork, w->dh, w->flag,
+                  w->lw.partial};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete w;
+  c->sw = nullptr;
+}
+}  // namespace icx
 
 extern "C" {
 
@@ -31,8 +289,109 @@ icx_status icx_bsr_spmv(icx_ctx* c, const double* d_vals, const double* d_x, dou
   return ICX_OK;
 }
 
-icx_status icx_newton_default_options(icx_newton_options*) { return ICX_ERR_UNSUPPORTED; }
-icx_status icx_newton_solve(icx_ctx*, double*, const icx_newton_options*, icx_newton_report*) {
-  return ICX_ERR_UNSUPPORTED;
+icx_status icx_newton_default_options(icx_newton_options* o) {
+  if (!o) return ICX_ERR_INVALID;
+  std::memset(o, 0, sizeof(*o));
+  o->tau_abs = 1e-10;
+  o->tau_rel = 0.0;
+  o->kmax = 20;
+  o->linesearch = 1;         // wolfe_linesearch defaults (nonlinear_solver_utils.hpp:207-233)
+  o->ls_max_it = 20;
+  o->ls_alpha_initial = 1.0;
+  o->ls_alpha_max = 10.0;
+  o->ls_alpha_min = 0.0;
+  o->ls_c1 = 1e-4;
+  o->ls_c2 = 0.9;
+  o->gmres_restart = 30;     // PETSc KSPGMRES default restart
+  o->gmres_max_it = 2000;
+  o->gmres_rtol = 1e-5;      // PETSc KSP default relative tolerance
+  o->preconditioner = 2;     // block-ILU(0)
+  o->verbosity = 0;
+  return ICX_OK;
+}
+
+icx_status icx_gmres_solve(icx_ctx* c, const double* d_vals, const double* d_b, double* d_x, int restart, int maxit,
+                           double rtol, int preconditioner, int* iterations, double* relres, void* stream) {
+  if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
+  if (!d_vals || !d_b || !d_x) return set_err(c, ICX_ERR_INVALID, "null device pointer");
+  if (restart < 1 || restart > 60 || preconditioner < 0 || preconditioner > 2)
+    return set_err(c, ICX_ERR_INVALID, "restart must be in 1..60 and preconditioner in 0..2");
+  cudaStream_t s = (cudaStream_t)stream;
+  icx_status st = ensure_work(c, restart);
+  if (st != ICX_OK) return st;
+  icx_solver_work* w = c->sw;
+  CK(cudaMemcpyAsync(w->vals, d_vals, sizeof(double) * (size_t)c->dm.nnzb * w->bs * w->bs, cudaMemcpyDeviceToDevice,
+                     s));
+  CK(build_pc(c, preconditioner, s));
+  int it = 0;
+  double rr = 0.0;
+  st = gmres(c, preconditioner, restart, maxit, rtol, d_b, d_x, &it, &rr, s);
+  if (iterations) *iterations = it;
+  if (relres) *relres = rr;
+  if (st != ICX_OK) return st;
+  return rr <= rtol ? ICX_OK : ICX_ERR_NOT_CONVERGED;
+}
+
+icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* opt, icx_newton_report* rep) {
+  if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
+  if (!d_u || !opt) return set_err(c, ICX_ERR_INVALID, "null argument");
+  if (opt->gmres_restart < 1 || opt->gmres_restart > 60) return set_err(c, ICX_ERR_INVALID, "restart in 1..60");
+  cudaStream_t s = 0;
+  icx_status st = ensure_work(c, opt->gmres_restart);
+  if (st != ICX_OK) return st;
+  icx_solver_work* w = c->sw;
+  long long n = w->n;
+  icx_newton_report local{};
+  icx_newton_report* R = rep ? rep : &local;
+  std::memset(R, 0, sizeof(*R));
+  const double eps = std::sqrt(DBL_EPSILON);
+  // residual and Jacobian at the initial state (petsc_newton.hpp:211-221)
+  CK(icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->r, w->vals, eps, s));
+  double r0 = dev_norm(c, w->r, s);
+  R->r0 = r0;
+  R->residual_history[0] = r0;
+  if (!std::isfinite(r0)) return set_err(c, ICX_ERR_NONFINITE, "non-finite initial residual");
+  double tau = opt->tau_abs + opt->tau_rel * r0;
+  double rk = r0;
+  int k = 0;
+  bool converged = rk <= tau;
+  for (; k < opt->kmax && !converged; ++k) {
+    CK(build_pc(c, opt->preconditioner, s));
+    int it = 0;
+    double rr = 0.0;
+    st = gmres(c, opt->preconditioner, opt->gmres_restart, opt->gmres_max_it, opt->gmres_rtol, w->r, w->du, &it, &rr,
+               s);
+    if (st != ICX_OK) return st;
+    R->linear_iterations_total += it;
+    double alpha = 1.0;
+    if (opt->linesearch != 0) {
+      // phi(alpha) = |R(u - alpha du)|_2, non-finite -> 1e9 (petsc_newton.hpp:262-293)
+      std::function<double(double)> phi = [&](double a) -> double {
+        icx::la_xpay(n, d_u, -a, w->du, w->ustep, s);
+        icx::launch_residual(c->dm, c->phys, w->ustep, w->rwork, s);
+        double v = dev_norm(c, w->rwork, s);
+        return std::isfinite(v) ? v : 1e9;
+      };
+      if (opt->linesearch == 1)
+        alpha = wolfe_ls(phi, opt->ls_alpha_max, opt->ls_alpha_initial, opt->ls_max_it, opt->ls_c1, opt->ls_c2);
+      else
+        alpha = corrigan_ls(phi, opt->ls_alpha_max, opt->ls_alpha_initial, opt->ls_max_it, opt->ls_alpha_min);
+    }
+    CK(icx::la_axpby(n, -alpha, w->du, 1.0, d_u, s));
+    CK(icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->r, w->vals, eps, s));
+    rk = dev_norm(c, w->r, s);
+    if (k + 1 < 64) {
+      R->residual_history[k + 1] = rk;
+      R->alpha_history[k] = alpha;
+    }
+    if (opt->verbosity > 0) std::printf("newton %d: |r| = %.6e alpha = %.4f gmres its = %d\n", k, rk, alpha, it);
+    if (!std::isfinite(rk)) return set_err(c, ICX_ERR_NONFINITE, "non-finite residual");
+    converged = rk <= tau;
+  }
+  CK(cudaStreamSynchronize(s));
+  R->iterations = k;
+  R->converged = converged;
+  R->r_final = rk;
+  return converged ? ICX_OK : ICX_ERR_NOT_CONVERGED;
 }
 }

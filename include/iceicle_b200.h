@@ -162,6 +162,13 @@ typedef struct icx_newton_report {
   double alpha_history[64];
 } icx_newton_report;
 
+/* Linear solve J x = b with the BSR values d_vals (the KSPSolve of
+ * petsc_newton.hpp:243-244): restarted right-preconditioned GMRES(restart),
+ * preconditioner 0 none / 1 block-Jacobi / 2 block-ILU(0). Returns
+ * ICX_ERR_NOT_CONVERGED when the relative residual stays above rtol. */
+icx_status icx_gmres_solve(icx_ctx* ctx, const double* d_vals, const double* d_b, double* d_x, int restart,
+                           int maxit, double rtol, int preconditioner, int* iterations, double* relres, void* stream);
+
 icx_status icx_newton_default_options(icx_newton_options* opt);
 icx_status icx_newton_solve(icx_ctx* ctx, double* d_u, const icx_newton_options* opt, icx_newton_report* rep);
 

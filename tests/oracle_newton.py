@@ -1,0 +1,79 @@
+"""Oracle Newton (test infrastructure): PetscNewton::solve
+(src/solvers/include/iceicle/petsc_newton.hpp:205-329) restated over the oracle
+residual and FD Jacobian, with a sparse direct linear solve, and the
+reference's Wolfe / Corrigan line searches
+(src/solvers/include/iceicle/nonlinear_solver_utils.hpp:83-191)."""
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import oracle_bindings as ob
+
+SQEPS = np.sqrt(np.finfo(float).eps)
+
+
+def _fd(f, eps, x):
+    a = f(x)
+    b = f(x + eps)
+    return (b - a) / eps
+
+
+def zoom(f, lo, hi, kmax, c1, c2):
+    for _ in range(kmax):
+        phi_lo, dphi_lo = f(lo), _fd(f, SQEPS, lo)
+        phi_hi, dphi_hi = f(hi), _fd(f, SQEPS, hi)
+        d1 = dphi_lo + dphi_hi - 3 * (phi_lo - phi_hi) / (lo - hi)
+        d2 = np.sqrt(max(d1 * d1 - dphi_lo * dphi_hi, 1e-8))
+        d2 = np.copysign(d2, hi - lo)
+        aj = hi - (hi - lo) * ((dphi_hi + d2 - d1) / (dphi_hi - dphi_lo + 2 * d2))
+        phi_aj = f(aj)
+        dphi_0 = _fd(f, SQEPS, 0.0)
+        if phi_aj > f(0.0) + c1 * aj * dphi_0 or phi_aj >= phi_lo:
+            hi = aj
+        else:
+            dphi_aj = _fd(f, SQEPS, aj)
+            if abs(dphi_aj) <= -c2 * dphi_0:
+                return aj
+            if dphi_aj * (hi - lo) >= 0:
+                hi = lo
+            lo = aj
+    return 0.5 * (lo + hi)
+
+
+def wolfe_ls(f, alpha_max=10.0, alpha1=1.0, kmax=20, c1=1e-4, c2=0.9):
+    a_im1, a_i = 0.0, alpha1
+    phi_0 = f(0.0)
+    dphi_0 = _fd(f, SQEPS, 0.0)
+    for k in range(kmax):
+        phi_i, phi_im1 = f(a_i), f(a_im1)
+        if phi_i > phi_0 + c1 * a_i * dphi_0 or (phi_i >= phi_im1 and k > 0):
+            return zoom(f, a_im1, a_i, kmax, c1, c2)
+        dphi_i = _fd(f, SQEPS, a_i)
+        if abs(dphi_i) <= -c2 * dphi_0:
+            return a_i
+        if dphi_i >= 0:
+            return zoom(f, a_i, a_im1, kmax, c1, c2)
+        a_im1, a_i = a_i, 0.5 * (a_i + alpha_max)
+    return a_i
+
+
+def newton(pb, coord, u0, tau_abs=1e-10, kmax=20, linesearch=None):
+    """returns (u, residual norm history)"""
+    u = np.array(u0, dtype=np.float64)
+    r, rowptr, colidx, vals = ob.jacobian_bsr(pb, coord, u)
+    hist = [np.linalg.norm(r)]
+    for _ in range(kmax):
+        if hist[-1] <= tau_abs:
+            break
+        A = sp.bsr_matrix((vals, colidx, rowptr), shape=(u.size, u.size)).tocsc()
+        du = spla.spsolve(A, r)
+        alpha = 1.0
+        if linesearch == "wolfe":
+            def phi(a):
+                v = np.linalg.norm(ob.residual(ob.oracle(), pb, coord, u - a * du))
+                return v if np.isfinite(v) else 1e9
+            alpha = wolfe_ls(phi)
+        u = u - alpha * du
+        r, rowptr, colidx, vals = ob.jacobian_bsr(pb, coord, u)
+        hist.append(np.linalg.norm(r))
+    return u, hist

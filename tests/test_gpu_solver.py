@@ -1,0 +1,125 @@
+"""GMRES / block preconditioners and the Newton solver on the GPU (C ABI),
+against dense solves and the oracle Newton (PetscNewton::solve restated)."""
+import numpy as np
+import pytest
+import torch
+
+import iceicle_b200 as ib
+import oracle_bindings as ob
+import oracle_newton as on
+from specs import BURGERS, NS, Spec
+
+pytestmark = pytest.mark.gpu
+
+
+def _jac(ctx, u):
+    L = ctx.layout
+    bs = L.block_size
+    du = torch.from_numpy(u).cuda()
+    dr = torch.empty_like(du)
+    dv = torch.empty(L.nnz_blocks * bs * bs, dtype=torch.float64, device="cuda")
+    ctx.form_jacobian_fd(du, dr, dv)
+    return dr, dv
+
+
+@pytest.mark.parametrize("pc", [0, 1, 2], ids=["none", "block_jacobi", "block_ilu0"])
+def test_gmres_matches_dense_solve(pc):
+    spec = Spec(pde=NS, nx=4, ny=3, p=2, ip=True)
+    ctx = spec.context()
+    u = spec.state(np.random.default_rng(3))
+    dr, dv = _jac(ctx, u)
+    x = torch.zeros_like(dr)
+    it, rr, ok = ctx.gmres_solve(dv, dr, x, restart=30, maxit=3000, rtol=1e-11, preconditioner=pc)
+    assert ok, (it, rr)
+    rp, ci = ctx.jacobian_pattern()
+    bs = ctx.layout.block_size
+    Jd = ob.bsr_to_dense(rp, ci, dv.cpu().numpy().reshape(-1, bs, bs))
+    xr = np.linalg.solve(Jd, dr.cpu().numpy())
+    assert np.linalg.norm(x.cpu().numpy() - xr) <= 1e-8 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("shape", [(6, 1), (1, 5)])
+def test_block_ilu0_is_exact_on_block_tridiagonal(shape):
+    """one row (or column) of elements gives a block-tridiagonal Jacobian, on
+    which block ILU(0) is the exact block LU: GMRES converges in one step"""
+    spec = Spec(pde=NS, nx=shape[0], ny=shape[1], p=2, ip=True)
+    ctx = spec.context()
+    u = spec.state(np.random.default_rng(4))
+    dr, dv = _jac(ctx, u)
+    x = torch.zeros_like(dr)
+    it, rr, ok = ctx.gmres_solve(dv, dr, x, restart=30, maxit=50, rtol=1e-10, preconditioner=2)
+    assert ok and it == 1, (it, rr)
+
+
+def test_preconditioners_reduce_iterations():
+    spec = Spec(pde=BURGERS, nx=12, ny=12, p=2, mu=0.05)
+    ctx = spec.context()
+    u = spec.state(np.random.default_rng(6))
+    dr, dv = _jac(ctx, u)
+    its = []
+    for pc in (0, 1, 2):
+        x = torch.zeros_like(dr)
+        it, rr, ok = ctx.gmres_solve(dv, dr, x, restart=30, maxit=5000, rtol=1e-8, preconditioner=pc)
+        assert ok
+        its.append(it)
+    assert its[2] < its[1] <= its[0], its
+
+
+def _newton_opts(**kw):
+    o = ib.default_newton_options()
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def test_newton_burgers_matches_oracle_newton():
+    """no line search, tight linear solves: both sides take the same Newton
+    steps, so the residual histories agree while |r| >> roundoff and the
+    converged states agree to 1e-10 (L2, relative)"""
+    spec = Spec(pde=BURGERS, nx=6, ny=6, p=2, g=2, mu=1e-2, a=(0.0, 0.0), b=(1.0, 0.5),
+                dirichlet=[("constant", [1, 0.0])])
+    c = spec.coords()
+    rng = np.random.default_rng(8)
+    xy = None
+    ctx = spec.context(c)
+    xy = ctx.basis_node_coords().reshape(-1, 2)
+    u0 = 0.5 * np.sin(2 * np.pi * xy[:, 0]) * np.sin(2 * np.pi * xy[:, 1]) + 1e-3 * rng.standard_normal(len(xy))
+    u_or, hist_or = on.newton(spec.oracle_problem(), c, u0, tau_abs=1e-12, kmax=15)
+    du = torch.from_numpy(u0.copy()).cuda()
+    rep = ctx.newton_solve(du, _newton_opts(tau_abs=1e-12, kmax=15, linesearch=0, gmres_rtol=1e-13,
+                                            gmres_max_it=5000))
+    assert rep.converged, list(rep.residual_history[:rep.iterations + 1])
+    hist = list(rep.residual_history[:rep.iterations + 1])
+    for a, b in zip(hist, hist_or):
+        if b > 1e-6:
+            assert abs(a - b) <= 1e-6 * b, (hist, hist_or)
+    u = du.cpu().numpy()
+    assert np.linalg.norm(u - u_or) <= 1e-10 * max(np.linalg.norm(u_or), 1e-300) or \
+        np.linalg.norm(u - u_or) <= 1e-12
+
+
+def test_newton_ns_mms_with_linesearch_converges_to_oracle_state():
+    spec = Spec(pde=NS, nx=4, ny=4, p=2, g=2, ip=True, source=True, perturb=0.05)
+    c = spec.coords()
+    ctx = spec.context(c)
+    from iceicle_b200 import workload_fn
+    import ctypes as C
+    from iceicle_b200.workloads import ns_mms_params
+    prm = ns_mms_params()
+    f = workload_fn("ns_mms_state")
+    xy = ctx.basis_node_coords().reshape(-1, 2)
+    out = (C.c_double * 4)()
+    pt = (C.c_double * 2)()
+    u0 = np.zeros((len(xy), 4))
+    for k in range(len(xy)):
+        pt[0], pt[1] = xy[k]
+        f(pt, out, C.cast(prm, C.c_void_p))
+        u0[k] = out[:]
+    u0 = (u0 * (1 + 1e-2 * np.random.default_rng(2).standard_normal(u0.shape))).reshape(-1)
+    u_or, hist_or = on.newton(spec.oracle_problem(), c, u0, tau_abs=1e-11, kmax=20, linesearch="wolfe")
+    du = torch.from_numpy(u0.copy()).cuda()
+    rep = ctx.newton_solve(du, _newton_opts(tau_abs=1e-11, kmax=20, linesearch=1, gmres_rtol=1e-12,
+                                            gmres_max_it=5000))
+    assert rep.converged and rep.r_final <= 1e-11
+    u = du.cpu().numpy()
+    assert np.linalg.norm(u - u_or) <= 1e-10 * np.linalg.norm(u_or)
