@@ -25,7 +25,8 @@ struct icx_solver_work {
   double* V = nullptr;      // Krylov basis, (m + 1) x n
   double* w = nullptr;      // work vectors
   double* z = nullptr;
-  double* r = nullptr;
+  double* r = nullptr;      // GMRES restart residual (internal to gmres)
+  double* res = nullptr;    // Newton residual R(u), the right-hand side of the linear solves
   double* du = nullptr;
   double* ustep = nullptr;
   double* rwork = nullptr;
@@ -65,7 +66,7 @@ icx_status ensure_work(icx_ctx* c, int m) {
   CK(cudaMalloc((void**)&w->pc, vb));
   CK(cudaMalloc((void**)&w->uinv, sizeof(double) * (size_t)dm.E * bs * bs));
   CK(cudaMalloc((void**)&w->V, sizeof(double) * (size_t)(m + 1) * n));
-  double** vecs[] = {&w->w, &w->z, &w->r, &w->du, &w->ustep, &w->rwork};
+  double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork};
   for (double** p : vecs) CK(cudaMalloc((void**)p, sizeof(double) * n));
   CK(cudaMalloc((void**)&w->dh, sizeof(double) * 2 * (m + 2)));
   CK(cudaMalloc((void**)&w->flag, sizeof(int)));
@@ -113,6 +114,8 @@ icx_status gmres(icx_ctx* c, int pc, int m, int maxit, double rtol, const double
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
   long long n = w->n;
+  if (b == w->r || b == w->w || b == w->z || x == w->r || x == w->w || x == w->z)
+    return set_err(c, ICX_ERR_INVALID, "gmres vectors alias its work buffers");
   CK(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
   double bnorm = dev_norm(c, b, s);
   *iters = 0;
@@ -260,7 +263,7 @@ namespace icx {
 void free_solver_work(icx_ctx* c) {
   if (!c || !c->sw) return;
   icx_solver_work* w = c->sw;
-  void* ptrs[] = {w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->du, w->ustep, w->rwork, w->dh, w->flag,
+  void* ptrs[] = {w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du, w->ustep, w->rwork, w->dh, w->flag,
                   w->lw.partial};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -346,8 +349,8 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   std::memset(R, 0, sizeof(*R));
   const double eps = std::sqrt(DBL_EPSILON);
   // residual and Jacobian at the initial state (petsc_newton.hpp:211-221)
-  CK(icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->r, w->vals, eps, s));
-  double r0 = dev_norm(c, w->r, s);
+  CK(icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->res, w->vals, eps, s));
+  double r0 = dev_norm(c, w->res, s);
   R->r0 = r0;
   R->residual_history[0] = r0;
   if (!std::isfinite(r0)) return set_err(c, ICX_ERR_NONFINITE, "non-finite initial residual");
@@ -359,7 +362,7 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
     CK(build_pc(c, opt->preconditioner, s));
     int it = 0;
     double rr = 0.0;
-    st = gmres(c, opt->preconditioner, opt->gmres_restart, opt->gmres_max_it, opt->gmres_rtol, w->r, w->du, &it, &rr,
+    st = gmres(c, opt->preconditioner, opt->gmres_restart, opt->gmres_max_it, opt->gmres_rtol, w->res, w->du, &it, &rr,
                s);
     if (st != ICX_OK) return st;
     R->linear_iterations_total += it;
@@ -378,8 +381,8 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
         alpha = corrigan_ls(phi, opt->ls_alpha_max, opt->ls_alpha_initial, opt->ls_max_it, opt->ls_alpha_min);
     }
     CK(icx::la_axpby(n, -alpha, w->du, 1.0, d_u, s));
-    CK(icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->r, w->vals, eps, s));
-    rk = dev_norm(c, w->r, s);
+    CK(icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->res, w->vals, eps, s));
+    rk = dev_norm(c, w->res, s);
     if (k + 1 < 64) {
       R->residual_history[k + 1] = rk;
       R->alpha_history[k] = alpha;

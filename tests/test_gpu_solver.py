@@ -98,6 +98,27 @@ def test_newton_burgers_matches_oracle_newton():
         np.linalg.norm(u - u_or) <= 1e-12
 
 
+def test_newton_with_gmres_restarts_matches_oracle():
+    """short restarts force several GMRES cycles per Newton step: the Newton
+    right-hand side must survive them (regression: it once shared a buffer
+    with GMRES's restart residual)"""
+    # non-zero boundary data so that the converged state is not ~0
+    spec = Spec(pde=BURGERS, nx=6, ny=5, p=2, g=2, mu=1e-2, a=(0.2, 0.1), b=(1.0, 0.5),
+                dirichlet=[("constant", [1, 0.25])])
+    c = spec.coords()
+    ctx = spec.context(c)
+    u0 = 0.25 + 0.2 * np.random.default_rng(12).standard_normal(spec.N)
+    u_or, hist_or = on.newton(spec.oracle_problem(), c, u0, tau_abs=1e-12, kmax=20)
+    du = torch.from_numpy(u0.copy()).cuda()
+    rep = ctx.newton_solve(du, _newton_opts(tau_abs=1e-12, kmax=20, linesearch=0, gmres_restart=3,
+                                            gmres_rtol=1e-12, gmres_max_it=20000, preconditioner=1))
+    assert rep.converged
+    hist = list(rep.residual_history[:rep.iterations + 1])
+    for a, b in zip(hist[:4], hist_or[:4]):
+        assert abs(a - b) <= 1e-6 * b, (hist, hist_or)
+    assert np.linalg.norm(du.cpu().numpy() - u_or) <= 1e-10 * np.linalg.norm(u_or)
+
+
 def test_newton_ns_mms_with_linesearch_converges_to_oracle_state():
     spec = Spec(pde=NS, nx=4, ny=4, p=2, g=2, ip=True, source=True, perturb=0.05)
     c = spec.coords()
