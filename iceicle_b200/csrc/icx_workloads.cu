@@ -21,6 +21,11 @@ void icx_wl_sine_product(const double* x, double* out, void* user) {
   out[0] = amp * std::sin(2.0 * M_PI * x[0]) * std::sin(2.0 * M_PI * x[1]);
 }
 
+void icx_wl_oblique_step(const double* x, double* out, void* user) {
+  const double* p = (const double*)user;  // {x0, slope, u_left, u_right}
+  out[0] = (x[0] < p[0] + p[1] * x[1]) ? p[2] : p[3];
+}
+
 void icx_wl_ns_mms_state(const double* x, double* out, void* user) {
   const double* p = (const double*)user;
   icx_ns_mms_state(x[0], x[1], p[0], p[1], p[2], p[3], p[4], p[5], p[6], out);

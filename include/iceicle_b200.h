@@ -180,6 +180,8 @@ icx_status icx_newton_solve(icx_ctx* ctx, double* d_u, const icx_newton_options*
  *   (conservative variables) and the matching source term */
 void icx_wl_constant(const double* x, double* out, void* user);
 void icx_wl_sine_product(const double* x, double* out, void* user);
+/* user -> double[4] = {x0, slope, u_left, u_right}: out[0] = u_left if x < x0 + slope*y else u_right */
+void icx_wl_oblique_step(const double* x, double* out, void* user);
 void icx_wl_ns_mms_state(const double* x, double* out, void* user);
 void icx_wl_ns_mms_source(const double* x, double* out, void* user);
 

@@ -944,3 +944,358 @@ int orc_form_jacobian_fd(const orc_problem* pb, const double* coord, const doubl
   disc_free(&D);
   return rc;
 }
+
+/* ================================================================== */
+/* MDG-ICE                                                             */
+/* ================================================================== */
+/* geo_dof_map over a list of traces (fe_function/geo_layouts.hpp:359-498)
+ * with the hyper_rectangle boundary parametrisation (geo_layouts.hpp:510-540)
+ * of geometry-order-1 meshes: a node on x = xmin/xmax keeps x and slides in y
+ * (and vice versa); corners keep both; the free coordinates are clamped to
+ * the box (BoundedFixedCoordinateSubset, geo_layouts.hpp:162-210). */
+typedef struct {
+  int nsel, ngeo;
+  int* sel;        /* selected node ids, ascending */
+  int* inv;        /* node -> selected index or nsel */
+  int* fixmask;    /* per selected node: bit d set = coordinate d fixed */
+  int* cols;       /* nsel + 1 offsets into x */
+  double* fixval;  /* per selected node: value of each fixed coordinate */
+  double box[4];   /* xmin0, xmin1, xmax0, xmax1 */
+} mdgmap;
+
+static int face_node(const orc_problem* pb, const int* F, int i) {
+  int g = pb->geo_order;
+  double xi[2];
+  face_to_ref(F[2], -1.0 + 2.0 * i / g, xi);
+  int k0 = (int)lround((xi[0] + 1.0) * 0.5 * g), k1 = (int)lround((xi[1] + 1.0) * 0.5 * g);
+  return el_node(pb, F[0], k0 * (g + 1) + k1);
+}
+
+static void mdg_build(const orc_problem* pb, const int* faces, int ntr, const int* traces, int hyper, mdgmap* M) {
+  int nn = orc_n_nodes(pb), g = pb->geo_order;
+  char* pick = (char*)calloc(nn, 1);
+  for (int t = 0; t < ntr; ++t)
+    for (int i = 0; i <= g; ++i) pick[face_node(pb, faces + 7 * traces[t], i)] = 1;
+  M->sel = (int*)malloc(sizeof(int) * nn);
+  M->inv = (int*)malloc(sizeof(int) * nn);
+  M->nsel = 0;
+  for (int n = 0; n < nn; ++n)
+    if (pick[n]) M->sel[M->nsel++] = n;
+  for (int n = 0; n < nn; ++n) M->inv[n] = M->nsel;
+  for (int k = 0; k < M->nsel; ++k) M->inv[M->sel[k]] = k;
+  M->fixmask = (int*)calloc(M->nsel + 1, sizeof(int));
+  M->cols = (int*)malloc(sizeof(int) * (M->nsel + 1));
+  M->box[0] = pb->xmin[0]; M->box[1] = pb->xmin[1]; M->box[2] = pb->xmax[0]; M->box[3] = pb->xmax[1];
+  M->fixval = (double*)calloc(2 * (M->nsel + 1), sizeof(double));
+  M->cols[0] = 0;
+  for (int k = 0; k < M->nsel; ++k) {
+    int n = M->sel[k], m = 0;
+    /* hyper_rectangle walks the (nx+1) x (ny+1) index product (dim 0 fastest)
+     * with a running node counter, i.e. it addresses the geometry-order-1
+     * lattice: node n < (nx+1)(ny+1) gets the fixed coordinates of index
+     * (n % (nx+1), n / (nx+1)) (geo_layouts.hpp:520-537) */
+    if (hyper && n < (pb->nx + 1) * (pb->ny + 1)) {
+      int ix = n % (pb->nx + 1), iy = n / (pb->nx + 1);
+      if (ix == 0) { m |= 1; M->fixval[2 * k] = pb->xmin[0]; }
+      else if (ix == pb->nx) { m |= 1; M->fixval[2 * k] = pb->xmax[0]; }
+      if (iy == 0) { m |= 2; M->fixval[2 * k + 1] = pb->xmin[1]; }
+      else if (iy == pb->ny) { m |= 2; M->fixval[2 * k + 1] = pb->xmax[1]; }
+    }
+    M->fixmask[k] = m;
+    M->cols[k + 1] = M->cols[k] + 2 - ((m & 1) ? 1 : 0) - ((m & 2) ? 1 : 0);
+  }
+  M->ngeo = M->cols[M->nsel];
+  free(pick);
+}
+
+static void mdg_free(mdgmap* M) { free(M->sel); free(M->inv); free(M->fixmask); free(M->cols); free(M->fixval); }
+
+/* extract_geospan: coordinates -> parameters */
+static void mdg_x_from_coord(const mdgmap* M, const double* coord, double* x) {
+  for (int k = 0; k < M->nsel; ++k) {
+    int n = M->sel[k], c = M->cols[k];
+    for (int d = 0; d < 2; ++d)
+      if (!(M->fixmask[k] & (1 << d))) x[c++] = coord[2 * n + d];
+  }
+}
+
+/* s_to_x of one node: fixed coordinates take the box value they sit on, free
+ * ones the parameter clamped to the box */
+static void mdg_node_s_to_x(const mdgmap* M, int k, const double* s, double* xy, const double* cur) {
+  (void)cur;
+  int c = 0;
+  for (int d = 0; d < 2; ++d) {
+    if (M->fixmask[k] & (1 << d)) {
+      xy[d] = M->fixval[2 * k + d];
+    } else {
+      double v = s[c++];
+      if (M->fixmask[k]) v = fmin(M->box[2 + d], fmax(M->box[d], v));
+      xy[d] = v;
+    }
+  }
+}
+
+/* update_mesh: parameters -> coordinates (component_span.hpp:193-210) */
+static void mdg_coord_from_x(const mdgmap* M, const double* x, double* coord) {
+  for (int k = 0; k < M->nsel; ++k) {
+    int n = M->sel[k];
+    double xy[2];
+    mdg_node_s_to_x(M, k, x + M->cols[k], xy, coord + 2 * n);
+    coord[2 * n] = xy[0];
+    coord[2 * n + 1] = xy[1];
+  }
+}
+
+/* interface_conservation of one trace (conservation_law.hpp:1178-1288):
+ * res[i][eq] over the g+1 trace (geometry) basis functions */
+static void interface_conservation(const disc* D, const int* F, const double* uL, const double* uR, double* res) {
+  const orc_problem* pb = D->pb;
+  int neq = D->neq, g = pb->geo_order;
+  int interior = F[1] >= 0;
+  elgeo GL, GR;
+  el_geo(pb, D->coord, F[0], &GL);
+  el_geo(pb, D->coord, interior ? F[1] : F[0], &GR);
+  lag1d lt;
+  lag_init(&lt, g);
+  for (int i = 0; i < (g + 1) * neq; ++i) res[i] = 0.0;
+  for (int q = 0; q < D->nq1; ++q) {
+    faceqp fq;
+    /* boundary traces: the right side is element L again, at face 0 with orientation 0 */
+    face_qp(D, &GL, F[2], interior ? F[3] : 0, interior ? F[4] : 0, q, &fq);
+    double BL[MAXNB], BR[MAXNB], dBL[2 * MAXNB], dBR[2 * MAXNB];
+    double ul[MAXEQ], ur[MAXEQ], gl[2 * MAXEQ], gr[2 * MAXEQ];
+    side_eval(D, &GL, fq.xiL, uL, 0, BL, dBL, ul, gl, NULL);
+    side_eval(D, &GR, fq.xiR, uR, 0, BR, dBR, ur, gr, NULL);
+    if (!interior) {
+      if (F[5] == ORC_BC_DIRICHLET) {
+        pb->dirichlet[F[6]](fq.x, ur, pb->dirichlet_user[F[6]]);
+      } else {
+        for (int i = 0; i < (g + 1) * neq; ++i) res[i] = 0.0;
+        return;
+      }
+    }
+    if (pb->p == 1) { /* linear elements: gradients dropped (conservation_law.hpp:1262-1266) */
+      for (int k = 0; k < 2 * neq; ++k) gl[k] = gr[k] = 0.0;
+    }
+    double FL[MAXEQ][2], FR[MAXEQ][2];
+    phys_flux(pb, ul, gl, FL);
+    phys_flux(pb, ur, gr, FR);
+    double psi[MAXP], dpsi[MAXP];
+    lag_deriv(&lt, D->qx[q], psi, dpsi);
+    for (int k = 0; k < neq; ++k) {
+      double jump = (FR[k][0] * fq.n[0] + FR[k][1] * fq.n[1]) - (FL[k][0] * fq.n[0] + FL[k][1] * fq.n[1]);
+      for (int i = 0; i <= g; ++i) res[i * neq + k] -= jump * fq.sqrtg * fq.w * psi[i];
+    }
+  }
+}
+
+/* icres[sel][neq] += interface conservation of the selected traces (form_residual.hpp:327-381) */
+static void mdg_ic_residual(const disc* D, const mdgmap* M, int ntr, const int* traces, const double* u, double* ic) {
+  int bs = D->nb * D->neq, neq = D->neq, g = D->pb->geo_order;
+  double r[MAXP * MAXEQ];
+  memset(ic, 0, sizeof(double) * M->nsel * neq);
+  for (int t = 0; t < ntr; ++t) {
+    const int* F = D->faces + 7 * traces[t];
+    int R = F[1] >= 0 ? F[1] : F[0];
+    interface_conservation(D, F, u + (size_t)F[0] * bs, u + (size_t)R * bs, r);
+    for (int i = 0; i <= g; ++i) {
+      int k = M->inv[face_node(D->pb, F, i)];
+      if (k == M->nsel) continue;
+      for (int e = 0; e < neq; ++e) ic[k * neq + e] += r[i * neq + e];
+    }
+  }
+}
+
+int orc_mdg_select(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper, int* nsel,
+                   int* sel_nodes, double* x) {
+  int nf = orc_n_faces(pb), nint;
+  int* faces = (int*)malloc(sizeof(int) * 7 * nf);
+  int* conn = (int*)malloc(sizeof(int) * pb->nx * pb->ny * (pb->geo_order + 1) * (pb->geo_order + 1));
+  orc_mesh_topology(pb, conn, faces, &nint);
+  mdgmap M;
+  mdg_build(pb, faces, ntr, traces, hyper, &M);
+  *nsel = M.nsel;
+  memcpy(sel_nodes, M.sel, sizeof(int) * M.nsel);
+  mdg_x_from_coord(&M, coord, x);
+  int ngeo = M.ngeo;
+  mdg_free(&M);
+  free(faces);
+  free(conn);
+  return ngeo;
+}
+
+/* [res; ic] at [u; x] (form_residual.hpp:426-452) */
+int orc_mdg_residual(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                     const double* u_and_x, double* res_and_ic) {
+  int nn = orc_n_nodes(pb);
+  double* cw = (double*)malloc(sizeof(double) * 2 * nn);
+  memcpy(cw, coord, sizeof(double) * 2 * nn);
+  disc D;
+  if (disc_init(&D, pb, cw)) { free(cw); return -1; }
+  mdgmap M;
+  mdg_build(pb, D.faces, ntr, traces, hyper, &M);
+  size_t N = (size_t)pb->nx * pb->ny * D.nb * D.neq;
+  mdg_coord_from_x(&M, u_and_x + N, cw);
+  int rc = orc_form_residual(pb, cw, u_and_x, res_and_ic);
+  if (!rc) mdg_ic_residual(&D, &M, ntr, traces, u_and_x, res_and_ic + N);
+  mdg_free(&M);
+  disc_free(&D);
+  free(cw);
+  return rc;
+}
+
+/* Jacobian of [res; ic] w.r.t. [u; x] with the reference's perturbation scheme
+ * (form_petsc_jacobian_fd, then form_petsc_mdg_jacobian_fd, FJ:665-1049) into a
+ * dense row-major (N + nic) x (N + ngeo) array (small meshes only). dICE/dx
+ * visits only the selected traces of elements around the node: the others
+ * do not change when the node moves and contribute exact zeros. */
+int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                           const double* u, const double* x, double* res_and_ic, double* J) {
+  int nn = orc_n_nodes(pb);
+  double* cw = (double*)malloc(sizeof(double) * 2 * nn);
+  memcpy(cw, coord, sizeof(double) * 2 * nn);
+  disc D;
+  if (disc_init(&D, pb, cw)) { free(cw); return -1; }
+  mdgmap M;
+  mdg_build(pb, D.faces, ntr, traces, hyper, &M);
+  int E = pb->nx * pb->ny, neq = D.neq, bs = D.nb * neq, g = pb->geo_order;
+  size_t N = (size_t)E * bs, nrow = N + (size_t)M.nsel * neq, ncol = N + M.ngeo;
+  const double eps = sqrt(DBL_EPSILON);
+  mdg_coord_from_x(&M, x, cw);
+  memset(J, 0, sizeof(double) * nrow * ncol);
+  /* DG block */
+  int* rowptr = (int*)malloc(sizeof(int) * (E + 1));
+  int* colidx = (int*)malloc(sizeof(int) * 5 * E);
+  int nnzb = orc_bsr_pattern(pb, rowptr, colidx);
+  double* vals = (double*)malloc(sizeof(double) * (size_t)nnzb * bs * bs);
+  int rc = orc_form_jacobian_fd(pb, cw, u, res_and_ic, rowptr, colidx, vals);
+  for (int r = 0; r < E && !rc; ++r)
+    for (int k = rowptr[r]; k < rowptr[r + 1]; ++k)
+      for (int i = 0; i < bs; ++i)
+        for (int j = 0; j < bs; ++j)
+          J[((size_t)r * bs + i) * ncol + (size_t)colidx[k] * bs + j] += vals[((size_t)k * bs + i) * bs + j];
+  free(vals); free(rowptr); free(colidx);
+  double* ic = res_and_ic + N;
+  mdg_ic_residual(&D, &M, ntr, traces, u, ic);
+  double r0[MAXP * MAXEQ], r1[MAXP * MAXEQ], ul[MAXNB * MAXEQ], ur[MAXNB * MAXEQ];
+  /* dICE/du (FJ:712-806) */
+  for (int t = 0; t < ntr && !rc; ++t) {
+    const int* F = D.faces + 7 * traces[t];
+    int L = F[0], R = F[1] >= 0 ? F[1] : F[0];
+    memcpy(ul, u + (size_t)L * bs, sizeof(double) * bs);
+    memcpy(ur, u + (size_t)R * bs, sizeof(double) * bs);
+    interface_conservation(&D, F, ul, ur, r0);
+    double es = fmax(eps, vnorm(r0, (g + 1) * neq) * eps);
+    for (int side = 0; side < 2; ++side) {
+      double* us = side ? ur : ul;
+      int el = side ? R : L;
+      for (int c = 0; c < bs; ++c) {
+        double old = us[c];
+        us[c] += es;
+        interface_conservation(&D, F, ul, ur, r1);
+        us[c] = old;
+        for (int i = 0; i <= g; ++i) {
+          int k = M.inv[face_node(pb, F, i)];
+          if (k == M.nsel) continue;
+          for (int e = 0; e < neq; ++e)
+            J[(N + (size_t)k * neq + e) * ncol + (size_t)el * bs + c] += (r1[i * neq + e] - r0[i * neq + e]) / es;
+        }
+      }
+    }
+  }
+  /* dR/dx and dICE/dx per selected node (FJ:813-1046) */
+  double rl[MAXNB * MAXEQ], rr[MAXNB * MAXEQ], rlp[MAXNB * MAXEQ], rrp[MAXNB * MAXEQ];
+  for (int k = 0; k < M.nsel && !rc; ++k) {
+    int node = M.sel[k];
+    int ns = M.cols[k + 1] - M.cols[k];
+    /* elements around the node, ascending */
+    int els[4], nel = 0;
+    int ngl = (g + 1) * (g + 1);
+    for (int e = 0; e < E && nel < 4; ++e)
+      for (int kk = 0; kk < ngl; ++kk)
+        if (el_node(pb, e, kk) == node) { els[nel++] = e; break; }
+    int c0 = M.cols[k];
+    double sk[2];
+    {
+      int c = 0;
+      for (int d = 0; d < 2; ++d)
+        if (!(M.fixmask[k] & (1 << d))) sk[c++] = cw[2 * node + d];
+    }
+    /* volume integrals of the surrounding elements */
+    for (int a = 0; a < nel; ++a) {
+      int e = els[a];
+      memset(rl, 0, sizeof(double) * bs);
+      domain_integral(&D, e, u + (size_t)e * bs, rl);
+      double es = fmax(eps, vnorm(rl, bs) * eps);
+      for (int is = 0; is < ns; ++is) {
+        double sp[2] = {sk[0], sk[1]}, xy[2], save[2] = {cw[2 * node], cw[2 * node + 1]};
+        sp[is] += es;
+        mdg_node_s_to_x(&M, k, sp, xy, save);
+        cw[2 * node] = xy[0]; cw[2 * node + 1] = xy[1];
+        memset(rlp, 0, sizeof(double) * bs);
+        domain_integral(&D, e, u + (size_t)e * bs, rlp);
+        cw[2 * node] = save[0]; cw[2 * node + 1] = save[1];
+        for (int i = 0; i < bs; ++i) J[((size_t)e * bs + i) * ncol + N + c0 + is] += (rlp[i] - rl[i]) / es;
+      }
+    }
+    /* traces of the surrounding elements, each once */
+    int tv[16], ntv = 0;
+    for (int f = 0; f < D.nf; ++f) {
+      const int* F = D.faces + 7 * f;
+      int hit = 0;
+      for (int a = 0; a < nel; ++a) hit |= (F[0] == els[a]) || (F[1] == els[a]);
+      if (hit && ntv < 16) tv[ntv++] = f;
+    }
+    for (int a = 0; a < ntv && !rc; ++a) {
+      const int* F = D.faces + 7 * tv[a];
+      int L = F[0], R = F[1];
+      memset(rl, 0, sizeof(double) * bs);
+      memset(rr, 0, sizeof(double) * bs);
+      if (R >= 0) trace_integral(&D, F, u + (size_t)L * bs, u + (size_t)R * bs, rl, rr);
+      else rc = boundary_integral(&D, F, u + (size_t)L * bs, rl);
+      double es = fmax(eps, fmax(vnorm(rl, bs), vnorm(rr, bs)) * eps);
+      for (int is = 0; is < ns; ++is) {
+        double sp[2] = {sk[0], sk[1]}, xy[2], save[2] = {cw[2 * node], cw[2 * node + 1]};
+        sp[is] += es;
+        mdg_node_s_to_x(&M, k, sp, xy, save);
+        cw[2 * node] = xy[0]; cw[2 * node + 1] = xy[1];
+        memset(rlp, 0, sizeof(double) * bs);
+        memset(rrp, 0, sizeof(double) * bs);
+        if (R >= 0) trace_integral(&D, F, u + (size_t)L * bs, u + (size_t)R * bs, rlp, rrp);
+        else boundary_integral(&D, F, u + (size_t)L * bs, rlp);
+        cw[2 * node] = save[0]; cw[2 * node + 1] = save[1];
+        for (int i = 0; i < bs; ++i) J[((size_t)L * bs + i) * ncol + N + c0 + is] += (rlp[i] - rl[i]) / es;
+        if (R >= 0)
+          for (int i = 0; i < bs; ++i) J[((size_t)R * bs + i) * ncol + N + c0 + is] += (rrp[i] - rr[i]) / es;
+      }
+    }
+    /* interface conservation of the selected traces among them */
+    for (int t = 0; t < ntr; ++t) {
+      const int* F = D.faces + 7 * traces[t];
+      int hit = 0;
+      for (int a = 0; a < nel; ++a) hit |= (F[0] == els[a]) || (F[1] == els[a]);
+      if (!hit) continue;
+      int L = F[0], R = F[1] >= 0 ? F[1] : F[0];
+      interface_conservation(&D, F, u + (size_t)L * bs, u + (size_t)R * bs, r0);
+      double es = fmax(eps, vnorm(r0, (g + 1) * neq) * eps);
+      for (int is = 0; is < ns; ++is) {
+        double sp[2] = {sk[0], sk[1]}, xy[2], save[2] = {cw[2 * node], cw[2 * node + 1]};
+        sp[is] += es;
+        mdg_node_s_to_x(&M, k, sp, xy, save);
+        cw[2 * node] = xy[0]; cw[2 * node + 1] = xy[1];
+        interface_conservation(&D, F, u + (size_t)L * bs, u + (size_t)R * bs, r1);
+        cw[2 * node] = save[0]; cw[2 * node + 1] = save[1];
+        for (int i = 0; i <= g; ++i) {
+          int kk = M.inv[face_node(pb, F, i)];
+          if (kk == M.nsel) continue;
+          for (int e = 0; e < neq; ++e)
+            J[(N + (size_t)kk * neq + e) * ncol + N + c0 + is] += (r1[i * neq + e] - r0[i * neq + e]) / es;
+        }
+      }
+    }
+  }
+  mdg_free(&M);
+  disc_free(&D);
+  free(cw);
+  return rc;
+}

@@ -66,6 +66,18 @@ int orc_bsr_pattern(const orc_problem* pb, int* rowptr, int* colidx);
 int orc_form_jacobian_fd(const orc_problem* pb, const double* coord, const double* u, double* res,
                          const int* rowptr, const int* colidx, double* vals);
 
+/* MDG-ICE over the selected traces, optionally with the hyper_rectangle
+ * boundary parametrisation. orc_mdg_select returns the number of geometry
+ * parameters and writes the selected nodes and x (extract_geospan). */
+int orc_mdg_select(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper, int* nsel,
+                   int* sel_nodes, double* x);
+/* [res; ic] at [u; x] */
+int orc_mdg_residual(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                     const double* u_and_x, double* res_and_ic);
+/* dense (N + nsel*neq) x (N + ngeo) Jacobian of [res; ic] w.r.t. [u; x]; writes [res; ic] */
+int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                           const double* u, const double* x, double* res_and_ic, double* J);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,6 +5,7 @@
 #include <array>
 #include <cmath>
 #include <cstddef>
+#include <span>
 #include <type_traits>
 
 namespace MATH::GEOMETRY {
@@ -30,6 +31,8 @@ struct Point {
   constexpr const T* data() const { return x.data(); }
   constexpr operator T*() { return x.data(); }
   constexpr operator const T*() const { return x.data(); }
+  constexpr operator std::span<T, N>() { return std::span<T, N>(x.data(), N); }
+  constexpr operator std::span<const T, N>() const { return std::span<const T, N>(x.data(), N); }
   constexpr auto begin() { return x.begin(); }
   constexpr auto end() { return x.end(); }
   constexpr auto begin() const { return x.begin(); }

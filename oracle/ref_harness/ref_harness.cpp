@@ -17,6 +17,8 @@
 #include "iceicle/fe_function/fespan.hpp"
 #include "iceicle/fe_function/layout_right.hpp"
 #include "iceicle/form_residual.hpp"
+#include "iceicle/fe_function/geo_layouts.hpp"
+#include "iceicle/fe_function/component_span.hpp"
 #ifdef REF_WITH_JACOBIAN
 #include "iceicle/form_petsc_jacobian.hpp"
 #endif
@@ -236,7 +238,86 @@ int ref_time_form_residual(const ref_problem* pb, const double* coord, const dou
   });
 }
 
+/// MDG-ICE: geo_dof_map over the given traces (optionally with the
+/// hyper_rectangle boundary parametrisation). Writes the selected node list,
+/// the geometry parameters x (extract_geospan) and returns their count; the
+/// caller sizes arrays with ref_n_nodes.
+int ref_mdg_select(const ref_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                   int* n_selected, int* selected_nodes, double* x_out) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    std::vector<int> tr(traces, traces + ntr);
+    geo_dof_map geo_map{tr, fespace};
+    if (hyper)
+      mesh_parameterizations::hyper_rectangle(std::array<int, 2>{pb->nx, pb->ny},
+                                              std::array<double, 2>{pb->xmin[0], pb->xmin[1]},
+                                              std::array<double, 2>{pb->xmax[0], pb->xmax[1]}, geo_map);
+    *n_selected = (int)geo_map.selected_nodes.size();
+    for (std::size_t i = 0; i < geo_map.selected_nodes.size(); ++i) selected_nodes[i] = geo_map.selected_nodes[i];
+    geo_data_layout x_layout{geo_map};
+    std::vector<T> xdata(x_layout.size());
+    component_span x{xdata, x_layout};
+    extract_geospan(*fespace.meshptr, x);
+    std::memcpy(x_out, xdata.data(), sizeof(T) * xdata.size());
+    return (int)xdata.size();
+  });
+}
+
+/// form_residual(fespace, disc, geo_map, [u; x], [res; ic]) (form_residual.hpp:426-452)
+int ref_mdg_residual(const ref_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                     const double* u_and_x, int n_total, double* res_and_ic, int n_res) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    std::vector<int> tr(traces, traces + ntr);
+    geo_dof_map geo_map{tr, fespace};
+    if (hyper)
+      mesh_parameterizations::hyper_rectangle(std::array<int, 2>{pb->nx, pb->ny},
+                                              std::array<double, 2>{pb->xmin[0], pb->xmin[1]},
+                                              std::array<double, 2>{pb->xmax[0], pb->xmax[1]}, geo_map);
+    std::vector<T> ux(u_and_x, u_and_x + n_total);
+    std::vector<T> rr(n_res);
+    solvers::form_residual(fespace, disc, geo_map, std::span<T>{ux}, std::span<T>{rr});
+    std::memcpy(res_and_ic, rr.data(), sizeof(T) * n_res);
+    return 0;
+  });
+}
+
 #ifdef REF_WITH_JACOBIAN
+/// MDG Jacobian of [res; ic] w.r.t. [u; x] (form_petsc_jacobian_fd followed by
+/// form_petsc_mdg_jacobian_fd, the sparse path of CorriganLM::solve,
+/// corrigan_lm.hpp:385-396) into a dense row-major (N + nic) x (N + ngeo) array
+int ref_mdg_jacobian_dense(const ref_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                           const double* u, const double* x, int ngeo, double* res_and_ic, int nres,
+                           double* jac_dense) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    std::vector<int> tr(traces, traces + ntr);
+    geo_dof_map geo_map{tr, fespace};
+    if (hyper)
+      mesh_parameterizations::hyper_rectangle(std::array<int, 2>{pb->nx, pb->ny},
+                                              std::array<double, 2>{pb->xmin[0], pb->xmin[1]},
+                                              std::array<double, 2>{pb->xmax[0], pb->xmax[1]}, geo_map);
+    fe_layout_right layout{fespace.dg_map, neq_c};
+    std::size_t n = layout.size();
+    std::vector<T> ubuf(u, u + n);
+    std::vector<T> rbuf(nres);
+    fespan uspan{ubuf.data(), layout};
+    fespan rspan{rbuf.data(), layout};
+    geo_data_layout x_layout{geo_map};
+    std::vector<T> xdata(x, x + ngeo);
+    component_span xspan{xdata, x_layout};
+    ic_residual_layout<T, IDX, ndim, decltype(neq_c)::value> ic_layout{geo_map};
+    dofspan mdg_res{rbuf.data() + n, ic_layout};
+    Mat jac;
+    MatCreate(PETSC_COMM_WORLD, &jac);
+    MatSetSizes(jac, (PetscInt)nres, (PetscInt)(n + ngeo), PETSC_DETERMINE, PETSC_DETERMINE);
+    update_mesh(xspan, *fespace.meshptr);
+    solvers::form_petsc_jacobian_fd(fespace, disc, uspan, rspan, jac);
+    solvers::form_petsc_mdg_jacobian_fd(fespace, disc, uspan, xspan, mdg_res, jac);
+    std::memcpy(res_and_ic, rbuf.data(), sizeof(T) * nres);
+    petsc_shim_to_dense(jac, jac_dense);
+    MatDestroy(&jac);
+    return 0;
+  });
+}
+
 /// form_petsc_jacobian_fd of the reference into a dense row-major N x N
 /// matrix (small meshes only), plus the residual
 int ref_form_jacobian_dense(const ref_problem* pb, const double* coord, const double* u, double* res,

@@ -158,3 +158,49 @@ def bsr_to_dense(rowptr, colidx, vals):
             c = colidx[k]
             J[r * bs:(r + 1) * bs, c * bs:(c + 1) * bs] = vals[k]
     return J
+
+
+# ------------------------------------------------------------------ MDG-ICE
+def mdg_select(lib, pb, coord, traces, hyper=True):
+    nn = (pb.nx * pb.geo_order + 1) * (pb.ny * pb.geo_order + 1)
+    tr = np.ascontiguousarray(traces, dtype=np.int32)
+    sel = np.zeros(nn, dtype=np.int32)
+    x = np.zeros(2 * nn)
+    nsel = C.c_int()
+    ngeo = lib.fn("mdg_select")(C.byref(pb), _ptr(coord), len(tr), _ptr(tr), int(hyper), C.byref(nsel), _ptr(sel),
+                                _ptr(x))
+    return sel[: nsel.value].copy(), x[:ngeo].copy()
+
+
+def mdg_residual(lib, pb, coord, traces, u, x, hyper=True):
+    E, nb, N = sizes(pb)
+    sel, _ = mdg_select(lib, pb, coord, traces, hyper)
+    tr = np.ascontiguousarray(traces, dtype=np.int32)
+    ux = np.ascontiguousarray(np.concatenate([u, x]))
+    out = np.zeros(N + len(sel) * neq(pb))
+    if lib.prefix == "ref_":
+        rc = lib.fn("mdg_residual")(C.byref(pb), _ptr(coord), len(tr), _ptr(tr), int(hyper), _ptr(ux), len(ux),
+                                    _ptr(out), len(out))
+    else:
+        rc = lib.fn("mdg_residual")(C.byref(pb), _ptr(coord), len(tr), _ptr(tr), int(hyper), _ptr(ux), _ptr(out))
+    assert rc == 0, rc
+    return out
+
+
+def mdg_jacobian_dense(lib, pb, coord, traces, u, x, hyper=True):
+    E, nb, N = sizes(pb)
+    sel, _ = mdg_select(lib, pb, coord, traces, hyper)
+    tr = np.ascontiguousarray(traces, dtype=np.int32)
+    nres = N + len(sel) * neq(pb)
+    out = np.zeros(nres)
+    J = np.zeros((nres, N + len(x)))
+    u = np.ascontiguousarray(u)
+    x = np.ascontiguousarray(x)
+    if lib.prefix == "ref_":
+        rc = lib.fn("mdg_jacobian_dense")(C.byref(pb), _ptr(coord), len(tr), _ptr(tr), int(hyper), _ptr(u), _ptr(x),
+                                          len(x), _ptr(out), nres, _ptr(J))
+    else:
+        rc = lib.fn("mdg_jacobian_dense")(C.byref(pb), _ptr(coord), len(tr), _ptr(tr), int(hyper), _ptr(u), _ptr(x),
+                                          _ptr(out), _ptr(J))
+    assert rc == 0, rc
+    return out, J
