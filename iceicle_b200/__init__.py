@@ -98,6 +98,16 @@ def lib():
             "icx_form_residual_timed": (C.c_int, [vp, vp, vp, vp, dp, dp]),
             "icx_form_residual_noalloc": (C.c_int, [vp, vp, vp, vp]),
             "icx_gmres_solve": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, ip, dp, vp]),
+            "icx_mdg_select": (C.c_int, [vp, C.c_int, vp, C.c_int]),
+            "icx_mdg_info": (C.c_int, [vp, ip, ip]),
+            "icx_mdg_selected_nodes": (C.c_int, [vp, vp]),
+            "icx_mdg_get_x": (C.c_int, [vp, vp]),
+            "icx_mdg_set_x": (C.c_int, [vp, vp]),
+            "icx_form_mdg_residual": (C.c_int, [vp, vp, vp, vp]),
+            "icx_form_residual_mdg": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+            "icx_mdg_jacobian_pattern": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                                    C.POINTER(C.c_longlong), vp, vp]),
+            "icx_form_jacobian_mdg_fd": (C.c_int, [vp, vp, vp, vp, vp, C.c_double, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -269,6 +279,48 @@ class Context:
             self._check(st, "gmres_solve")
         return it.value, rr.value, st == 0
 
+    # --- MDG-ICE -----------------------------------------------------------
+    def mdg_select(self, traces, hyper_rectangle=True):
+        tr = np.ascontiguousarray(traces, dtype=np.int32)
+        self._check(lib().icx_mdg_select(self._h, len(tr), _ptr(tr), int(hyper_rectangle)), "mdg_select")
+        ns, ng = C.c_int(), C.c_int()
+        self._check(lib().icx_mdg_info(self._h, C.byref(ns), C.byref(ng)), "mdg_info")
+        self.mdg_nsel, self.mdg_ngeo = ns.value, ng.value
+        return ns.value, ng.value
+
+    def mdg_selected_nodes(self):
+        out = np.zeros(self.mdg_nsel, dtype=np.int32)
+        self._check(lib().icx_mdg_selected_nodes(self._h, _ptr(out)), "mdg_selected_nodes")
+        return out
+
+    def mdg_get_x(self):
+        x = np.zeros(self.mdg_ngeo)
+        self._check(lib().icx_mdg_get_x(self._h, _ptr(x)), "mdg_get_x")
+        return x
+
+    def mdg_set_x(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        self._check(lib().icx_mdg_set_x(self._h, _ptr(x)), "mdg_set_x")
+
+    def form_residual_mdg(self, u, x, res, ic, stream=None):
+        xp = None if x is None else _ptr(np.ascontiguousarray(x, dtype=np.float64))
+        self._check(lib().icx_form_residual_mdg(self._h, _ptr(u), xp, _ptr(res), _ptr(ic), _stream_ptr(stream)),
+                    "form_residual_mdg")
+
+    def mdg_jacobian_pattern(self):
+        nr, nc, nz = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self._check(lib().icx_mdg_jacobian_pattern(self._h, C.byref(nr), C.byref(nc), C.byref(nz), None, None),
+                    "mdg_jacobian_pattern")
+        rowptr = np.zeros(nr.value + 1, dtype=np.int32)
+        colidx = np.zeros(nz.value, dtype=np.int32)
+        self._check(lib().icx_mdg_jacobian_pattern(self._h, C.byref(nr), C.byref(nc), C.byref(nz), _ptr(rowptr),
+                                                   _ptr(colidx)), "mdg_jacobian_pattern")
+        return nr.value, nc.value, rowptr, colidx
+
+    def form_jacobian_mdg_fd(self, u, res, ic, vals, eps=0.0, stream=None):
+        self._check(lib().icx_form_jacobian_mdg_fd(self._h, _ptr(u), _ptr(res), _ptr(ic), _ptr(vals), eps,
+                                                   _stream_ptr(stream)), "form_jacobian_mdg_fd")
+
     def newton_solve(self, u, options=None):
         opt = options or default_newton_options()
         rep = NewtonReport()
@@ -289,3 +341,42 @@ def default_newton_options():
     if st != 0:
         raise IcxError(st, "newton_default_options")
     return opt
+
+
+class LMOptions(C.Structure):
+    _fields_ = [("tau_abs", C.c_double), ("tau_rel", C.c_double), ("kmax", C.c_int), ("lambda_u", C.c_double),
+                ("lambda_b", C.c_double), ("linesearch", C.c_int), ("ls_max_it", C.c_int),
+                ("ls_alpha_initial", C.c_double), ("ls_alpha_max", C.c_double), ("ls_alpha_min", C.c_double),
+                ("gmres_restart", C.c_int), ("gmres_max_it", C.c_int), ("gmres_rtol", C.c_double),
+                ("max_rejections", C.c_int), ("verbosity", C.c_int)]
+
+
+class LMReport(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("rejections", C.c_int), ("r0", C.c_double),
+                ("r_final", C.c_double), ("linear_iterations_total", C.c_int),
+                ("residual_history", C.c_double * 64), ("alpha_history", C.c_double * 64)]
+
+
+def default_lm_options():
+    o = LMOptions()
+    L = lib()
+    L.icx_lm_default_options.restype = C.c_int
+    L.icx_lm_default_options.argtypes = [C.POINTER(LMOptions)]
+    st = L.icx_lm_default_options(C.byref(o))
+    if st != 0:
+        raise IcxError(st, "lm_default_options")
+    return o
+
+
+def lm_solve(ctx, u, x, options=None):
+    """CorriganLM::solve: u (device tensor) and x (numpy, host) updated in place"""
+    L = lib()
+    L.icx_lm_solve.restype = C.c_int
+    L.icx_lm_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LMOptions), C.POINTER(LMReport)]
+    opt = options or default_lm_options()
+    rep = LMReport()
+    assert x.dtype == np.float64 and x.flags["C_CONTIGUOUS"]
+    st = L.icx_lm_solve(ctx._h, _ptr(u), _ptr(x), C.byref(opt), C.byref(rep))
+    if st not in (0, 5):
+        ctx._check(st, "lm_solve")
+    return rep

@@ -241,6 +241,16 @@ icx_status tabulate_and_geometry(icx_ctx* c) {
 
 }  // namespace
 
+namespace icx {
+icx_status refresh_geometry(icx_ctx* c) { return tabulate_and_geometry(c); }
+void lagrange_values(int pn, double x, double* N) {
+  Lagrange1D l(pn);
+  double dN[16], d2N[16];
+  l.eval(x, N, dN, d2N);
+}
+void gauss_legendre_points(int n, double* x, double* w) { gauss_legendre(n, x, w); }
+}  // namespace icx
+
 extern "C" {
 
 icx_status icx_create(icx_ctx** out, int device) {
@@ -260,6 +270,7 @@ void icx_destroy(icx_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   icx::free_solver_work(c);
+  icx::free_mdg(c);
   free_dev(c->dm);
   for (void* p : c->scratch)
     if (p) cudaFree(p);

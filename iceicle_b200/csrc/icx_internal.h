@@ -86,6 +86,7 @@ struct icx_ctx {
   // solver scratch (device), grown on demand
   std::vector<void*> scratch;
   struct icx_solver_work* sw = nullptr;  // Newton / GMRES buffers (icx_solver.cu)
+  struct icx_mdg_state* mdg = nullptr;   // MDG-ICE selection and Jacobian pattern (icx_mdg.cu)
 };
 
 namespace icx {
@@ -101,4 +102,13 @@ cudaError_t launch_bsr_spmv(const DeviceMesh& dm, const double* vals, const doub
                             cudaStream_t s);
 // releases the Newton / GMRES buffers of a context (icx_solver.cu)
 void free_solver_work(icx_ctx* c);
+// releases the MDG-ICE state of a context (icx_mdg.cu)
+void free_mdg(icx_ctx* c);
+// re-evaluates boundary/source data at the current host coordinates, uploads
+// them and recomputes the geometry factors (icx_host.cu)
+icx_status refresh_geometry(icx_ctx* c);
+// values of the pn+1 equispaced Lagrange polynomials of [-1, 1] at x (icx_host.cu)
+void lagrange_values(int pn, double x, double* N);
+// Gauss-Legendre points in the reference order (+x1, -x1, ..., 0) and weights (icx_host.cu)
+void gauss_legendre_points(int n, double* x, double* w);
 }  // namespace icx

@@ -2,6 +2,8 @@
 // (block-Jacobi preconditioner), block-ILU(0) on the element block pattern,
 // deterministic reductions and the multi-vector kernels of GMRES.
 #include <cfloat>
+#include <cmath>
+#include <vector>
 
 #include "icx_internal.h"
 #include "icx_linalg.h"
@@ -422,6 +424,122 @@ cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU,
     }
   }
   return cudaGetLastError();
+}
+
+}  // namespace icx
+
+// ------------------------------------------------------------------ GMRES
+namespace icx {
+
+double la_norm(LinalgWork& lw, long long n, const double* x, double* d_scratch, cudaStream_t s) {
+  la_mdot(lw, n, x, 0, 1, x, d_scratch, s);
+  double h = 0.0;
+  cudaMemcpyAsync(&h, d_scratch, sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  return std::sqrt(h);
+}
+
+#define GCK(expr)                                                  \
+  do {                                                             \
+    cudaError_t _e = (expr);                                       \
+    if (_e != cudaSuccess) {                                       \
+      if (err) *err = std::string(#expr) + ": " + cudaGetErrorString(_e); \
+      return ICX_ERR_CUDA;                                         \
+    }                                                              \
+  } while (0)
+
+icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit, double rtol, const double* b,
+                    double* x, int* iters, double* relres, cudaStream_t s, std::string* err) {
+  long long n = kb.n;
+  int m = kb.m;
+  if (b == kb.r || b == kb.w || b == kb.z || x == kb.r || x == kb.w || x == kb.z) {
+    if (err) *err = "gmres vectors alias its work buffers";
+    return ICX_ERR_INVALID;
+  }
+  GCK(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+  double bnorm = la_norm(*kb.lw, n, b, kb.dh, s);
+  *iters = 0;
+  *relres = 0.0;
+  if (bnorm == 0.0) return ICX_OK;
+  if (!std::isfinite(bnorm)) {
+    if (err) *err = "non-finite right-hand side";
+    return ICX_ERR_NONFINITE;
+  }
+  double tol = rtol * bnorm;
+  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hcol(m + 2), hp(m + 1);
+  GCK(cudaMemcpyAsync(kb.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  double beta = bnorm;
+  int total = 0;
+  while (true) {
+    GCK(la_axpby(n, 1.0 / beta, kb.r, 0.0, kb.V, s));
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int j = 0;
+    double resid = beta;
+    for (; j < m && total < maxit; ++j) {
+      double* vj = kb.V + (size_t)j * n;
+      double* vj1 = kb.V + (size_t)(j + 1) * n;
+      if (M) {
+        GCK((*M)(vj, kb.z));
+        GCK(A(kb.z, vj1));
+      } else {
+        GCK(A(vj, vj1));
+      }
+      // classical Gram-Schmidt, twice
+      std::fill(hcol.begin(), hcol.end(), 0.0);
+      for (int pass = 0; pass < 2; ++pass) {
+        GCK(la_mdot(*kb.lw, n, kb.V, n, j + 1, vj1, kb.dh, s));
+        GCK(la_maxpy(n, kb.V, n, j + 1, kb.dh, -1.0, vj1, s));
+        GCK(cudaMemcpyAsync(hp.data(), kb.dh, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s));
+        GCK(cudaStreamSynchronize(s));
+        for (int i = 0; i <= j; ++i) hcol[i] += hp[i];
+      }
+      double hn = la_norm(*kb.lw, n, vj1, kb.dh, s);
+      hcol[j + 1] = hn;
+      if (!std::isfinite(hn)) {
+        if (err) *err = "non-finite Krylov vector";
+        return ICX_ERR_NONFINITE;
+      }
+      if (hn > 0.0) GCK(la_axpby(n, 1.0 / hn, vj1, 0.0, vj1, s));
+      for (int i = 0; i < j; ++i) {
+        double t = cs[i] * hcol[i] + sn[i] * hcol[i + 1];
+        hcol[i + 1] = -sn[i] * hcol[i] + cs[i] * hcol[i + 1];
+        hcol[i] = t;
+      }
+      double den = std::hypot(hcol[j], hcol[j + 1]);
+      cs[j] = den == 0.0 ? 1.0 : hcol[j] / den;
+      sn[j] = den == 0.0 ? 0.0 : hcol[j + 1] / den;
+      hcol[j] = den;
+      hcol[j + 1] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hcol[i];
+      ++total;
+      resid = std::fabs(g[j + 1]);
+      if (resid <= tol || hn == 0.0) { ++j; break; }
+    }
+    for (int i = j - 1; i >= 0; --i) {
+      double sacc = g[i];
+      for (int k = i + 1; k < j; ++k) sacc -= H[(size_t)i * m + k] * y[k];
+      y[i] = sacc / H[(size_t)i * m + i];
+    }
+    GCK(cudaMemcpyAsync(kb.dh, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, s));
+    GCK(cudaMemsetAsync(kb.w, 0, sizeof(double) * n, s));
+    GCK(la_maxpy(n, kb.V, n, j, kb.dh, 1.0, kb.w, s));
+    if (M) {
+      GCK((*M)(kb.w, kb.z));
+      GCK(la_axpby(n, 1.0, kb.z, 1.0, x, s));
+    } else {
+      GCK(la_axpby(n, 1.0, kb.w, 1.0, x, s));
+    }
+    GCK(A(x, kb.w));
+    GCK(la_xpay(n, b, -1.0, kb.w, kb.r, s));
+    beta = la_norm(*kb.lw, n, kb.r, kb.dh, s);
+    *relres = beta / bnorm;
+    if (beta <= tol || total >= maxit || resid <= tol) break;
+  }
+  *iters = total;
+  return ICX_OK;
 }
 
 }  // namespace icx

@@ -28,3 +28,26 @@ cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU,
                          double* y, cudaStream_t s);
 
 }  // namespace icx
+
+#include <functional>
+#include <string>
+
+namespace icx {
+// device buffers of a restarted GMRES(m) on vectors of length n
+struct KrylovBuffers {
+  long long n = 0;
+  int m = 0;
+  double* V = nullptr;  // (m + 1) x n basis
+  double* w = nullptr;
+  double* z = nullptr;
+  double* r = nullptr;
+  double* dh = nullptr;  // >= m + 2 device doubles
+  LinalgWork* lw = nullptr;
+};
+using LinOp = std::function<cudaError_t(const double* x, double* y)>;
+double la_norm(LinalgWork& lw, long long n, const double* x, double* d_scratch, cudaStream_t s);
+// x = A^-1 b, right-preconditioned by M (null: none); classical Gram-Schmidt
+// with one re-orthogonalisation, FP64 Hessenberg/Givens on the host
+icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit, double rtol, const double* b,
+                    double* x, int* iters, double* relres, cudaStream_t s, std::string* err);
+}  // namespace icx

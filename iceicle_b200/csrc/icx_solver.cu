@@ -107,89 +107,23 @@ cudaError_t build_pc(icx_ctx* c, int kind, cudaStream_t s) {
   return cudaSuccess;
 }
 
-// x = J^-1 b by GMRES(m), right preconditioning; returns iterations, writes the
-// final relative residual estimate
+// x = J^-1 b by GMRES(m) on the BSR Jacobian, right preconditioning
 icx_status gmres(icx_ctx* c, int pc, int m, int maxit, double rtol, const double* b, double* x, int* iters,
                  double* relres, cudaStream_t s) {
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
-  long long n = w->n;
-  if (b == w->r || b == w->w || b == w->z || x == w->r || x == w->w || x == w->z)
-    return set_err(c, ICX_ERR_INVALID, "gmres vectors alias its work buffers");
-  CK(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
-  double bnorm = dev_norm(c, b, s);
-  *iters = 0;
-  *relres = 0.0;
-  if (bnorm == 0.0) return ICX_OK;
-  if (!std::isfinite(bnorm)) return set_err(c, ICX_ERR_NONFINITE, "non-finite right-hand side");
-  double tol = rtol * bnorm;
-  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hcol(m + 2);
-  CK(cudaMemcpyAsync(w->r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-  double beta = bnorm;
-  int total = 0;
-  while (true) {
-    CK(icx::la_axpby(n, 1.0 / beta, w->r, 0.0, w->V, s));
-    std::fill(g.begin(), g.end(), 0.0);
-    g[0] = beta;
-    int j = 0;
-    double resid = beta;
-    for (; j < m && total < maxit; ++j) {
-      double* vj = w->V + (size_t)j * n;
-      double* vj1 = w->V + (size_t)(j + 1) * n;
-      CK(apply_pc(c, pc, vj, w->z, s));
-      CK(icx::launch_bsr_spmv(dm, w->vals, w->z, vj1, s));
-      // classical Gram-Schmidt, twice
-      std::fill(hcol.begin(), hcol.end(), 0.0);
-      for (int pass = 0; pass < 2; ++pass) {
-        CK(icx::la_mdot(w->lw, n, w->V, n, j + 1, vj1, w->dh, s));
-        CK(icx::la_maxpy(n, w->V, n, j + 1, w->dh, -1.0, vj1, s));
-        std::vector<double> hp(j + 1);
-        CK(cudaMemcpyAsync(hp.data(), w->dh, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        for (int i = 0; i <= j; ++i) hcol[i] += hp[i];
-      }
-      double hn = dev_norm(c, vj1, s);
-      hcol[j + 1] = hn;
-      if (!std::isfinite(hn)) return set_err(c, ICX_ERR_NONFINITE, "non-finite Krylov vector");
-      if (hn > 0.0) CK(icx::la_axpby(n, 1.0 / hn, vj1, 0.0, vj1, s));
-      // apply the previous rotations, then a new one
-      for (int i = 0; i < j; ++i) {
-        double t = cs[i] * hcol[i] + sn[i] * hcol[i + 1];
-        hcol[i + 1] = -sn[i] * hcol[i] + cs[i] * hcol[i + 1];
-        hcol[i] = t;
-      }
-      double den = std::hypot(hcol[j], hcol[j + 1]);
-      cs[j] = den == 0.0 ? 1.0 : hcol[j] / den;
-      sn[j] = den == 0.0 ? 0.0 : hcol[j + 1] / den;
-      hcol[j] = den;
-      hcol[j + 1] = 0.0;
-      g[j + 1] = -sn[j] * g[j];
-      g[j] = cs[j] * g[j];
-      for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hcol[i];
-      ++total;
-      resid = std::fabs(g[j + 1]);
-      if (resid <= tol || hn == 0.0) { ++j; break; }
-    }
-    // y = H^-1 g (upper triangular j x j), x += M^-1 (V y)
-    for (int i = j - 1; i >= 0; --i) {
-      double sacc = g[i];
-      for (int k = i + 1; k < j; ++k) sacc -= H[(size_t)i * m + k] * y[k];
-      y[i] = sacc / H[(size_t)i * m + i];
-    }
-    CK(cudaMemcpyAsync(w->dh, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(w->w, 0, sizeof(double) * n, s));
-    CK(icx::la_maxpy(n, w->V, n, j, w->dh, 1.0, w->w, s));
-    CK(apply_pc(c, pc, w->w, w->z, s));
-    CK(icx::la_axpby(n, 1.0, w->z, 1.0, x, s));
-    // true residual for the restart
-    CK(icx::launch_bsr_spmv(dm, w->vals, x, w->w, s));
-    CK(icx::la_xpay(n, b, -1.0, w->w, w->r, s));
-    beta = dev_norm(c, w->r, s);
-    *relres = beta / bnorm;
-    if (beta <= tol || total >= maxit || resid <= tol) break;
-  }
-  *iters = total;
-  return ICX_OK;
+  icx::KrylovBuffers kb;
+  kb.n = w->n;
+  kb.m = m;
+  kb.V = w->V;
+  kb.w = w->w;
+  kb.z = w->z;
+  kb.r = w->r;
+  kb.dh = w->dh;
+  kb.lw = &w->lw;
+  icx::LinOp A = [&](const double* xin, double* yout) { return icx::launch_bsr_spmv(dm, w->vals, xin, yout, s); };
+  icx::LinOp M = [&](const double* xin, double* yout) { return apply_pc(c, pc, xin, yout, s); };
+  return icx::gmres_op(kb, A, pc ? &M : nullptr, maxit, rtol, b, x, iters, relres, s, &c->err);
 }
 
 // wolfe_ls / zoom / corrigan_ls of the reference (nonlinear_solver_utils.hpp:83-191)

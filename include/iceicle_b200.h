@@ -139,6 +139,63 @@ icx_status icx_form_jacobian_fd(icx_ctx* ctx, const double* d_u, double* d_res, 
 /* y = J x for the BSR Jacobian (PETSc MatMult on the AIJ matrix, PN:243) */
 icx_status icx_bsr_spmv(icx_ctx* ctx, const double* d_vals, const double* d_x, double* d_y, void* stream);
 
+/* ---- MDG-ICE (moving discontinuous Galerkin, interface condition enforcement)
+ * icx_mdg_select: geo_dof_map over the given face indices, i.e. the nodes of
+ * those faces become geometry unknowns (fe_function/geo_layouts.hpp:359-498);
+ * hyper_rectangle != 0 applies mesh_parameterizations::hyper_rectangle
+ * (geo_layouts.hpp:510-540): nodes on the box keep the coordinate they sit on
+ * and slide along it. Geometry parameters x: per selected node its free
+ * coordinates (extract_geospan / update_mesh, component_span.hpp:177-210). */
+icx_status icx_mdg_select(icx_ctx* ctx, int ntraces, const int* traces, int hyper_rectangle);
+icx_status icx_mdg_info(const icx_ctx* ctx, int* n_selected_nodes, int* n_geo);
+icx_status icx_mdg_selected_nodes(const icx_ctx* ctx, int* nodes);
+icx_status icx_mdg_get_x(const icx_ctx* ctx, double* x);        /* host */
+icx_status icx_mdg_set_x(icx_ctx* ctx, const double* x);        /* host; moves the mesh */
+/* form_mdg_residual (form_residual.hpp:335-381): d_ic[n_selected_nodes * neq] */
+icx_status icx_form_mdg_residual(icx_ctx* ctx, const double* d_u, double* d_ic, void* stream);
+/* form_residual(fespace, disc, geo_map, [u; x], [res; ic]) (form_residual.hpp:426-452);
+ * x (host) may be NULL to keep the current mesh */
+icx_status icx_form_residual_mdg(icx_ctx* ctx, const double* d_u, const double* x, double* d_res, double* d_ic,
+                                 void* stream);
+/* CSR pattern of the Jacobian of [res; ic] w.r.t. [u; x]: nrow = n_dof + n_ic,
+ * ncol = n_dof + n_geo; rowptr/colidx (host) may be NULL to query sizes */
+icx_status icx_mdg_jacobian_pattern(icx_ctx* ctx, long long* nrow, long long* ncol, long long* nnz, int* rowptr,
+                                    int* colidx);
+/* form_petsc_jacobian_fd + form_petsc_mdg_jacobian_fd (form_petsc_jacobian.hpp:55-317, 665-1049):
+ * [res; ic] and the CSR values of the full Jacobian at the current mesh */
+icx_status icx_form_jacobian_mdg_fd(icx_ctx* ctx, const double* d_u, double* d_res, double* d_ic,
+                                    double* d_csr_vals, double eps, void* stream);
+
+/* ---- regularised Gauss-Newton / Levenberg-Marquardt for MDG-ICE
+ * (CorriganLM::solve, src/solvers/include/iceicle/corrigan_lm.hpp:363-717) with
+ * the matrix-free subproblem (J^T J + D) p = J^T r, D = lambda_u |J_col| on the
+ * PDE unknowns and max(lambda_b, lambda_b |J_col|) on the geometry unknowns
+ * (corrigan_lm.hpp:68-109), solved by GMRES without preconditioner. */
+typedef struct icx_lm_options {
+  double tau_abs, tau_rel;
+  int kmax;
+  double lambda_u, lambda_b;
+  int linesearch;            /* 0 none, 2 corrigan (nonlinear_solver_utils.hpp:173-191, 236-257) */
+  int ls_max_it;
+  double ls_alpha_initial, ls_alpha_max, ls_alpha_min;
+  int gmres_restart, gmres_max_it;
+  double gmres_rtol;
+  int max_rejections;        /* bound on rejected steps in a row */
+  int verbosity;
+} icx_lm_options;
+
+typedef struct icx_lm_report {
+  int iterations, converged, rejections;
+  double r0, r_final;
+  int linear_iterations_total;
+  double residual_history[64];
+  double alpha_history[64];
+} icx_lm_report;
+
+icx_status icx_lm_default_options(icx_lm_options* opt);
+/* d_u (device) and the geometry parameters x (host, n_geo) are updated in place */
+icx_status icx_lm_solve(icx_ctx* ctx, double* d_u, double* x, const icx_lm_options* opt, icx_lm_report* rep);
+
 /* ---- Newton solver (PetscNewton, PN:37-337; ConvergenceCriteria, NU:24-60) */
 typedef struct icx_newton_options {
   double tau_abs, tau_rel;

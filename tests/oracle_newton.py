@@ -77,3 +77,62 @@ def newton(pb, coord, u0, tau_abs=1e-10, kmax=20, linesearch=None):
         r, rowptr, colidx, vals = ob.jacobian_bsr(pb, coord, u)
         hist.append(np.linalg.norm(r))
     return u, hist
+
+
+def corrigan_ls(f, alpha_max=10.0, alpha1=1.0, kmax=20, alpha_min=0.0):
+    a, b, alpha = alpha_min, alpha_max, alpha1
+    for k in range(kmax):
+        phi_0 = f(0.0)
+        if k > 0:
+            alpha = (a + b) / 2
+        phi_star = f(alpha)
+        if abs(phi_star) < abs(phi_0):
+            if alpha == alpha1:
+                break
+            a = alpha
+        else:
+            b = alpha
+    return alpha
+
+
+def lm(pb, coord, traces, u0, x0, kmax=5, lambda_u=1e-7, lambda_b=1e-2, tau_abs=1e-10, linesearch=True):
+    """CorriganLM::solve (corrigan_lm.hpp:363-717) with the matrix-free
+    subproblem solved exactly; the regularisation follows the lambda updates.
+    Returns (u, x, residual history)."""
+    u, x = np.array(u0, dtype=float), np.array(x0, dtype=float)
+    N = u.size
+    out, J = ob.mdg_jacobian_dense(ob.oracle(), pb, coord, traces, u, x)
+    hist = [np.linalg.norm(out)]
+    lu, lb, lu_min = lambda_u, lambda_b, lambda_u
+    k = 0
+    rejects = 0
+    while k < kmax and hist[-1] > tau_abs and rejects < 20:
+        cn = np.linalg.norm(J, axis=0)
+        d = np.concatenate([lu * cn[:N], np.maximum(lb, lb * cn[N:])])
+        A = J.T @ J + np.diag(d)
+        p = np.linalg.solve(A, J.T @ out)
+        alpha, accept = 1.0, True
+        if linesearch:
+            last = {}
+
+            def phi(a):
+                o = ob.mdg_residual(ob.oracle(), pb, coord, traces, u - a * p[:N], x - a * p[N:])
+                v = np.linalg.norm(o[:N]) + np.linalg.norm(o[N:])
+                last["v"] = v
+                last["x"] = x - a * p[N:]
+                return v
+            alpha = corrigan_ls(phi)
+            accept = last["v"] < 10 * hist[-1]
+            if accept:
+                lu, lb = max(lu_min, 0.55 * lu), max(last["v"], 0.55 * lb)
+            else:
+                lu, lb = lu * 1.8, lb * 1.8
+        if not accept:
+            rejects += 1
+            continue
+        rejects = 0
+        u, x = u - alpha * p[:N], x - alpha * p[N:]
+        out, J = ob.mdg_jacobian_dense(ob.oracle(), pb, coord, traces, u, x)
+        hist.append(np.linalg.norm(out))
+        k += 1
+    return u, x, hist

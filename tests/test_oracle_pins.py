@@ -116,3 +116,39 @@ def test_linear_state_has_zero_interior_jump_residual():
     r = ob.residual(ob.oracle(), pb, c, u)
     # sum of residuals = -(outflow - inflow) = 0 for a divergence-free flux
     assert abs(r.sum()) < 1e-13
+
+
+MDG_CASES = [
+    dict(nx=4, ny=4, g=1, p=1, mu=0.0, a=(0.0, 1.0), b=(1.0, 0.0), bct=(3, 3, 3, 4),
+         dirichlet=[("oblique_step", [0.4, 0.2, 1.0, -0.5])]),
+    dict(nx=3, ny=4, g=1, p=2, mu=0.0, a=(0.0, 1.0), b=(1.0, 0.0), bct=(3, 3, 3, 4),
+         dirichlet=[("oblique_step", [0.4, 0.2, 1.0, -0.5])]),
+    dict(nx=3, ny=3, g=1, p=2, mu=0.02, bct=(3, 2, 4, 3)),
+    dict(nx=3, ny=3, g=2, p=2, pde=NS, ip=True, perturb=0.05),
+]
+
+
+@needs_ref
+@pytest.mark.parametrize("kw", MDG_CASES, ids=[str(c) for c in MDG_CASES])
+def test_mdg_residual_and_jacobian_match_reference(kw):
+    """MDG-ICE with all interior traces selected and hyper_rectangle boundary
+    sliding: selection, geometry parameters, [res; ic] at moved nodes and the
+    Jacobian w.r.t. [u; x] (FD tolerance as above)"""
+    spec = Spec(**kw)
+    pb = spec.oracle_problem()
+    c = spec.coords()
+    _, faces, nint = ob.topology(ob.oracle(), pb)
+    traces = np.arange(nint)
+    s1, x1 = ob.mdg_select(ob.oracle(), pb, c, traces)
+    s2, x2 = ob.mdg_select(ob.ref(), pb, c, traces)
+    assert np.array_equal(s1, s2) and np.array_equal(x1, x2)
+    u = spec.state(np.random.default_rng(1))
+    xp = x1 + 0.01 * np.random.default_rng(2).standard_normal(x1.size) / spec.nx
+    r1 = ob.mdg_residual(ob.oracle(), pb, c, traces, u, xp)
+    r2 = ob.mdg_residual(ob.ref(), pb, c, traces, u, xp)
+    assert np.abs(r1 - r2).max() <= 1e-12 * np.abs(r2).max()
+    o1, J1 = ob.mdg_jacobian_dense(ob.oracle(), pb, c, traces, u, xp)
+    o2, J2 = ob.mdg_jacobian_dense(ob.ref(), pb, c, traces, u, xp)
+    assert np.abs(o1 - o2).max() <= 1e-12 * np.abs(o2).max()
+    assert np.abs(J1 - J2).max() <= 1e-6 * np.abs(J2).max()
+    assert np.array_equal(J1 != 0, J2 != 0)
