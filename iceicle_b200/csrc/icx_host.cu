@@ -162,7 +162,7 @@ cudaError_t upload(T** dptr, const std::vector<T>& h) {
 
 void free_dev(DeviceMesh& dm) {
   void* ptrs[] = {dm.coord, dm.el_nodes, dm.face_info, dm.el_face, dm.el_side, dm.vgeo, dm.fgeo,
-                  dm.tab_vol, dm.tab_face, dm.tab_gvol, dm.tab_gface, dm.tab_gcen, dm.qw_face,
+                  dm.tab_vol, dm.tab_face, dm.tab_1d, dm.tab_fphi, dm.tab_f1d, dm.tab_gvol, dm.tab_gface, dm.tab_gcen, dm.qw_face,
                   dm.bvals, dm.src, dm.face_flux, dm.face_grad, dm.bsr_rowptr, dm.bsr_colidx,
                   dm.bsr_diag, dm.face_blk};
   for (void* p : ptrs)
@@ -402,6 +402,9 @@ icx_status icx_disc_navier_stokes(icx_ctx* c, double gamma, double Pr, double mu
   c->phys.gamma = gamma;
   c->phys.Pr = Pr;
   c->phys.ns_mu = mu;
+  c->phys.inv_gamma = 1.0 / gamma;
+  c->phys.inv_2gam2m1 = 1.0 / (2 * (gamma * gamma - 1));
+  c->phys.mu_gamma_pr = mu * gamma / Pr;
   c->conv_flux = conv_flux;
   c->has_disc = true;
   c->ready = false;
@@ -506,6 +509,40 @@ icx_status icx_setup(icx_ctx* c) {
         tp_tab(lb, xi, &tface[((size_t)(lf * 2 + o) * dm.nqf + q) * dm.nb * 6]);
         tp_tab(lg, xi, &tgface[((size_t)(lf * 2 + o) * dm.nqf + q) * dm.ng * 6]);
       }
+  // 1D factors of the volume tabulation (sum factorisation): values, then
+  // derivatives, of the p+1 Lagrange polynomials at the nq1 Gauss points
+  std::vector<double> t1d((size_t)2 * dm.nq1 * (P + 1));
+  for (int q = 0; q < dm.nq1; ++q) {
+    double N[16], dN[16], d2N[16];
+    lb.eval(qx[q], N, dN, d2N);
+    for (int i = 0; i <= P; ++i) {
+      t1d[(size_t)q * (P + 1) + i] = N[i];
+      t1d[(size_t)(dm.nq1 + q) * (P + 1) + i] = dN[i];
+    }
+  }
+  std::vector<double> tfphi((size_t)8 * dm.nqf * dm.nb);
+  for (size_t k = 0; k < tfphi.size(); ++k) tfphi[k] = tface[k * 6];
+  // face tabulation as 1D factors: the fixed coordinate of local face lf is
+  // xi_(lf & 1) = -1 (lf < 2) or +1, the other follows the face point
+  std::vector<double> tf1d((size_t)4 * (P + 1) * 3 + (size_t)8 * dm.nqf * (P + 1) * 3);
+  for (int lf = 0; lf < 4; ++lf) {
+    double N[16], dN[16], d2N[16];
+    lb.eval(lf < 2 ? -1.0 : 1.0, N, dN, d2N);
+    for (int k = 0; k <= P; ++k) {
+      double* o = &tf1d[((size_t)lf * (P + 1) + k) * 3];
+      o[0] = N[k]; o[1] = dN[k]; o[2] = d2N[k];
+    }
+    for (int o = 0; o < 2; ++o)
+      for (int q = 0; q < dm.nqf; ++q) {
+        double xi[2];
+        face_ref(lf, o ? -qx[q] : qx[q], xi);
+        lb.eval(xi[1 - (lf & 1)], N, dN, d2N);
+        for (int j = 0; j <= P; ++j) {
+          double* t = &tf1d[(size_t)4 * (P + 1) * 3 + ((((size_t)lf * 2 + o) * dm.nqf + q) * (P + 1) + j) * 3];
+          t[0] = N[j]; t[1] = dN[j]; t[2] = d2N[j];
+        }
+      }
+  }
   std::vector<double> tgcen(dm.ng);
   {
     double xi0[2] = {0.0, 0.0};
@@ -560,6 +597,9 @@ icx_status icx_setup(icx_ctx* c) {
   errs.push_back(upload(&dm.el_side, els));
   errs.push_back(upload(&dm.tab_vol, tvol));
   errs.push_back(upload(&dm.tab_face, tface));
+  errs.push_back(upload(&dm.tab_1d, t1d));
+  errs.push_back(upload(&dm.tab_fphi, tfphi));
+  errs.push_back(upload(&dm.tab_f1d, tf1d));
   errs.push_back(upload(&dm.tab_gvol, tgvol));
   errs.push_back(upload(&dm.tab_gface, tgface));
   errs.push_back(upload(&dm.tab_gcen, tgcen));

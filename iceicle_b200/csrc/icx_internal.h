@@ -28,6 +28,7 @@ struct PhysParams {
   int pde;
   double mu, a[2], b[2];        // Burgers
   double gamma, Pr, ns_mu;      // Navier-Stokes (unit reference parameters)
+  double inv_gamma, inv_2gam2m1, mu_gamma_pr;  // 1/gamma, 1/(2(gamma^2-1)), mu*gamma/Pr
   int interior_penalty;
   double sigma_ic;
   double beta0, beta1;          // DDG coefficients (beta1 = 0 for interior penalty)
@@ -46,6 +47,12 @@ struct DeviceMesh {
   double* fgeo = nullptr;      // [NFACE_GEO][F*nqf]
   double* tab_vol = nullptr;   // [nqv][nb][3]: phi, dphi/dxi0, dphi/dxi1
   double* tab_face = nullptr;  // [4 faces][2 orient][nqf][nb][6]: phi, d0, d1, h00, h01, h11
+  double* tab_1d = nullptr;    // [2][nq1][p+1]: 1D Lagrange values, then derivatives, at the 1D Gauss points
+  double* tab_fphi = nullptr;  // [4 faces][2 orient][nqf][nb]: phi of tab_face, compact
+  // 1D factors of tab_face: [4 faces][p+1][3] value, d, d2 along the face's
+  // fixed reference direction (lf & 1) at its constant coordinate, then
+  // [4 faces][2 orient][nqf][p+1][3] along the varying direction
+  double* tab_f1d = nullptr;
   double* tab_gvol = nullptr;  // [nqv][ng][2]: geometry basis gradients at volume points
   double* tab_gface = nullptr; // [4][2][nqf][ng][6]: geometry basis phi, d0, d1, h00, h01, h11 at face points
   double* tab_gcen = nullptr;  // [ng]: geometry basis at the element centroid

@@ -50,25 +50,28 @@ template <> struct Phys<ICX_PDE_BURGERS> {
 
 // ------------------------------------------------------------ Navier-Stokes
 struct NSState {
-  double rho, mom0, mom1, rhoE, v0, v1, vv, p, c, E;
+  double rho, mom0, mom1, rhoE, v0, v1, vv, p, c, E, inv_rho;
 };
 
 constexpr double NS_RGAS = 287.052874;
 
+// Quotients by the density are taken as products with one reciprocal per
+// state (a last-bit difference from dividing each time).
 __device__ static inline NSState ns_state(const PhysParams& pp, const double* u) {
   NSState s;
   double gamma = pp.gamma;
   s.rho = fmax(1e-14, u[0]);
+  s.inv_rho = 1.0 / s.rho;
   s.mom0 = u[1];
   s.mom1 = u[2];
-  s.v0 = u[1] / s.rho;
-  s.v1 = u[2] / s.rho;
+  s.v0 = u[1] * s.inv_rho;
+  s.v1 = u[2] * s.inv_rho;
   s.vv = s.v0 * s.v0 + s.v1 * s.v1;
   s.rhoE = u[3];
-  s.E = s.rhoE / s.rho;
+  s.E = s.rhoE * s.inv_rho;
   double e = s.E - 0.5 * s.vv;
   s.p = fmax(1e-12, (gamma - 1) * s.rho * e);
-  s.c = sqrt(gamma * s.p / s.rho);
+  s.c = sqrt(gamma * s.p * s.inv_rho);
   return s;
 }
 
@@ -81,9 +84,9 @@ template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) gv[i][j] = g[2 * (1 + i) + j] / s.rho - (i == 0 ? s.v0 : s.v1) / s.rho * g[j];
+      for (int j = 0; j < 2; ++j) gv[i][j] = (g[2 * (1 + i) + j] - (i == 0 ? s.v0 : s.v1) * g[j]) * s.inv_rho;
 #pragma unroll
-    for (int j = 0; j < 2; ++j) gE[j] = (g[6 + j] - s.E * g[j]) / s.rho;
+    for (int j = 0; j < 2; ++j) gE[j] = (g[6 + j] - s.E * g[j]) * s.inv_rho;
     double mu = pp.ns_mu;
     double div = gv[0][0] + gv[1][1];
 #pragma unroll
@@ -114,7 +117,7 @@ template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
       double q = gE[j];
       q -= vel[0] * gv[0][j];
       q -= vel[1] * gv[1][j];
-      q *= mu * pp.gamma / pp.Pr;
+      q *= pp.mu_gamma_pr;
       double ef = q;
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
@@ -133,6 +136,7 @@ template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
     double vnL = L.v0 * n[0] + L.v1 * n[1];
     double vnR = R.v0 * n[0] + R.v1 * n[1];
     double mL = vnL / L.c, mR = vnR / R.c;
+    const double inv_gam = pp.inv_gamma, inv_g21 = pp.inv_2gam2m1;
     if (mL > 1) {
       f[0] = L.rho * vnL;
       f[1] = L.mom0 * vnL + L.p * n[0];
@@ -143,10 +147,10 @@ template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
     } else {
       double fmL = L.rho * L.c * (mL + 1) * (mL + 1) / 4.0;
       f[0] = fmL;
-      f[1] = fmL * (L.v0 + n[0] * (-vnL + 2 * L.c) / gam);
-      f[2] = fmL * (L.v1 + n[1] * (-vnL + 2 * L.c) / gam);
+      f[1] = fmL * (L.v0 + n[0] * (-vnL + 2 * L.c) * inv_gam);
+      f[2] = fmL * (L.v1 + n[1] * (-vnL + 2 * L.c) * inv_gam);
       double t = (gam - 1) * vnL + 2 * L.c;
-      f[3] = fmL * ((L.vv - vnL * vnL) / 2 + t * t / (2 * (gam * gam - 1)));
+      f[3] = fmL * ((L.vv - vnL * vnL) / 2 + t * t * inv_g21);
     }
     if (mR < -1) {
       f[0] += R.rho * vnR;
@@ -156,10 +160,10 @@ template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
     } else if (mR <= 1) {
       double fmR = -R.rho * R.c * (mR - 1) * (mR - 1) / 4.0;
       f[0] += fmR;
-      f[1] += fmR * (R.v0 + n[0] * (-vnR - 2 * R.c) / gam);
-      f[2] += fmR * (R.v1 + n[1] * (-vnR - 2 * R.c) / gam);
+      f[1] += fmR * (R.v0 + n[0] * (-vnR - 2 * R.c) * inv_gam);
+      f[2] += fmR * (R.v1 + n[1] * (-vnR - 2 * R.c) * inv_gam);
       double t = (gam - 1) * vnR - 2 * R.c;
-      f[3] += fmR * ((R.vv - vnR * vnR) / 2 + t * t / (2 * (gam * gam - 1)));
+      f[3] += fmR * ((R.vv - vnR * vnR) / 2 + t * t * inv_g21);
     }
   }
 
@@ -174,7 +178,7 @@ template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
     double mu = pp.ns_mu;
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      double ef = mu * pp.gamma / pp.Pr * gE[j] * n[j];
+      double ef = pp.mu_gamma_pr * gE[j] * n[j];
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         f[1 + i] += tau[i][j] * n[j];

@@ -16,14 +16,23 @@
 //                       lifts the stored face fluxes of its four faces onto
 //                       its test functions. Every residual entry is written
 //                       exactly once: no atomics and no zero fill.
+#include <atomic>
 #include <cfloat>
+#include <cstdint>
 #include <cstdio>
 
 #include "icx_internal.h"
 #include "icx_dg.cuh"
 
-namespace icx {
+// resident CTAs per SM requested for the volume and face kernels (register budget)
+#ifndef ICX_VOL_MINB
+#define ICX_VOL_MINB 4
+#endif
+#ifndef ICX_FACE_MINB
+#define ICX_FACE_MINB 5
+#endif
 
+namespace icx {
 
 __constant__ double c_dxi_ds[4][2] = {{0.0, -1.0}, {1.0, 0.0}, {0.0, 1.0}, {-1.0, 0.0}};
 
@@ -146,85 +155,325 @@ __global__ void geo_face_kernel(DeviceMesh dm) {
 }
 
 // ------------------------------------------------------------- face fluxes
+// One CTA per group of FPB consecutive faces, one thread per face point in
+// the flux stage. A side's trace at the points of local face lf factors
+// through the face's fixed reference direction a = lf & 1 (xi_a = -1 or +1 on
+// the whole face): with c(k, j) the coefficient whose index along a is k and
+// along the other direction j,
+//   T_m(j) = sum_k c(k, j) d^m b_k(xi_a)        (once per face and side, m = 0..2)
+//   u = sum_j T_0(j) b_j(s_q),  du/dxi_a = sum_j T_1(j) b_j(s_q),
+//   du/dxi_(1-a) = sum_j T_0(j) b_j'(s_q), and the second derivatives alike,
+// which replaces the (P+1)^2 terms per point by 2(P+1)^2 per face plus
+// a few (P+1) per point.
 template <int PDE, int P, int G, bool DDG>
-__global__ void face_flux_kernel(DeviceMesh dm, PhysParams pp, const double* __restrict__ u) {
+struct FaceCfg {
   using C = Cfg<PDE, P, G>;
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= dm.F * C::NQF) return;
-  int f = k / C::NQF, q = k - f * C::NQF;
-  const int* fi = dm.face_info + 8 * f;
-  int L = fi[0], R = fi[1];
-  double out[C::NEQ], gq[4];
-  face_point_flux<PDE, P, G, DDG>(dm, pp, f, q, u + (size_t)L * C::BS, u + (size_t)(R >= 0 ? R : L) * C::BS, out,
-                                  gq);
+  static constexpr int N1 = P + 1, NM = DDG ? 3 : 2;
+  static constexpr int THREADS = 128;
+  static constexpr int FPB = THREADS / C::NQF;
+  static constexpr int TAB_FIX = 4 * N1 * 3;
+  static constexpr int TAB = TAB_FIX + 8 * C::NQF * N1 * 3;
+  static constexpr int RS = N1 * C::NEQ + C::NEQ;       // padded row stride of a staged tile [i0][i1][eq]
+  static constexpr int TILE = N1 * RS;
+  static constexpr int T_F = 2 * C::NEQ * N1 * NM;       // [side][eq][j][m]
+  static constexpr int T_FP = T_F | 1;                   // odd per-face stride: faces fall in distinct banks
+  static constexpr size_t SMEM = sizeof(double) * (TAB + FPB * (2 * TILE + T_FP)) + sizeof(int) * FPB * 8;
+  // resident CTAs requested: the Navier-Stokes flux with Hessians needs more registers
+  static constexpr int MINB = (DDG && C::NEQ > 1) ? 3 : ICX_FACE_MINB;
+};
+
+// asynchronous global -> shared copy of one double (cp.async, completed by cp_async_wait_all)
+__device__ inline void cp_async_f64(double* sdst, const double* gsrc) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <int PDE, int P, int G, bool DDG>
+__global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flux_kernel(DeviceMesh dm, PhysParams pp, const double* __restrict__ u) {
+  using C = Cfg<PDE, P, G>;
+  using FC = FaceCfg<PDE, P, G, DDG>;
+  constexpr int NEQ = C::NEQ, BS = C::BS, NQF = C::NQF, N1 = FC::N1, NM = FC::NM, FPB = FC::FPB;
+  extern __shared__ double smem[];
+  double* s_tab = smem;                           // tab_f1d
+  double* s_u = s_tab + FC::TAB;                  // [FPB][2][N1][RS]
+  double* s_T = s_u + FPB * 2 * FC::TILE;         // [FPB][T_FP]: [2][NEQ][N1][NM]
+  int* s_rec = (int*)(s_T + FPB * FC::T_FP);      // [FPB][8] face records
+  const int f0 = blockIdx.x * FPB;
+  const int nf = min(FPB, dm.F - f0);
+  const int tid = threadIdx.x;
+  for (int t = tid; t < FC::TAB; t += FC::THREADS) s_tab[t] = dm.tab_f1d[t];
+  for (int t = tid; t < nf * 8; t += FC::THREADS) s_rec[t] = dm.face_info[(size_t)f0 * 8 + t];
+  __syncthreads();
+
+  // coefficient tiles of both sides (a boundary face repeats its left tile so
+  // that both sides are evaluated without branches; the copy is not used)
+  for (int t = tid; t < nf * 2 * BS; t += FC::THREADS) {
+    int fs = t / BS, k = t - fs * BS;
+    int e = s_rec[(fs >> 1) * 8 + (fs & 1)];
+    if (e < 0) e = s_rec[(fs >> 1) * 8];
+    int i = k / NEQ, eq = k - i * NEQ;
+    int i0 = i / N1, i1 = i - i0 * N1;
+    cp_async_f64(s_u + fs * FC::TILE + i0 * FC::RS + i1 * NEQ + eq, u + (size_t)e * BS + k);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  // partial sums along each side's fixed direction
+  for (int t = tid; t < nf * 2 * NEQ * N1; t += FC::THREADS) {
+    int fs = t / (NEQ * N1), r = t - fs * (NEQ * N1);
+    int eq = r / N1, j = r - eq * N1;
+    const int* rec = s_rec + (fs >> 1) * 8;
+    int side = fs & 1;
+    int lf = (side && rec[1] >= 0) ? rec[3] : rec[2];
+    const double* fx = s_tab + lf * N1 * 3;
+    const double* c = s_u + fs * FC::TILE + eq;
+    int stride_k = (lf & 1) ? NEQ : FC::RS, off_j = (lf & 1) ? j * FC::RS : j * NEQ;
+    double acc[NM];
 #pragma unroll
-  for (int eq = 0; eq < C::NEQ; ++eq) dm.face_flux[(size_t)k * C::NEQ + eq] = out[eq];
-  if (Phys<PDE>::has_ic && pp.sigma_ic != 0.0) {
-    // layout [F][side][NQF][NEQ=1][2]
-    double* fg = dm.face_grad + (size_t)f * 2 * C::NQF * 2;
-    fg[(0 * C::NQF + q) * 2 + 0] = gq[0];
-    fg[(0 * C::NQF + q) * 2 + 1] = gq[1];
-    fg[(1 * C::NQF + q) * 2 + 0] = gq[2];
-    fg[(1 * C::NQF + q) * 2 + 1] = gq[3];
+    for (int m = 0; m < NM; ++m) acc[m] = 0.0;
+#pragma unroll
+    for (int k = 0; k < N1; ++k) {
+      double cv = c[off_j + k * stride_k];
+#pragma unroll
+      for (int m = 0; m < NM; ++m) acc[m] += cv * fx[k * 3 + m];
+    }
+    double* T = s_T + (fs >> 1) * FC::T_FP + ((fs & 1) * NEQ + eq) * N1 * NM + j * NM;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) T[m] = acc[m];
+  }
+  __syncthreads();
+
+  for (int t = tid; t < nf * NQF; t += FC::THREADS) {
+    int fl = t / NQF, q = t - fl * NQF;
+    int f = f0 + fl;
+    const int* rec = s_rec + fl * 8;
+    bool interior = rec[1] >= 0;
+    int bct = rec[5], bidx = rec[7];
+    FacePt fp;
+    {
+      int nfq = dm.F * NQF, k = f * NQF + q;
+      const double* g = dm.fgeo;
+      fp.n[0] = g[FG_N0 * nfq + k];
+      fp.n[1] = g[FG_N1 * nfq + k];
+      fp.wsq = g[FG_WSQ * nfq + k];
+      fp.h = g[FG_H * nfq + k];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) fp.JiL[a] = g[(FG_JIL + a) * nfq + k];
+      if (DDG) {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) fp.HL[a] = g[(FG_HL + a) * nfq + k];
+      }
+      const int kr = interior ? k : -1;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) fp.JiR[a] = interior ? g[(FG_JIR + a) * nfq + kr] : fp.JiL[a];
+      if (DDG) {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) fp.HR[a] = interior ? g[(FG_HR + a) * nfq + kr] : fp.HL[a];
+      }
+    }
+    double us[2][NEQ], gs[2][2 * NEQ], hs[2][DDG ? 4 * NEQ : 1];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      int lf = (side && interior) ? rec[3] : rec[2], o = (side && interior) ? rec[4] : 0;
+      const double* vt = s_tab + FC::TAB_FIX + ((lf * 2 + o) * NQF + q) * N1 * 3;
+      const bool a1 = lf & 1;
+      const double* Ji = side ? fp.JiR : fp.JiL;
+      const double* Hm = side ? fp.HR : fp.HL;
+#pragma unroll
+      for (int eq = 0; eq < NEQ; ++eq) {
+        const double* T = s_T + fl * FC::T_FP + (side * NEQ + eq) * N1 * NM;
+        double v = 0.0, dfix = 0.0, dvar = 0.0, hff = 0.0, hfv = 0.0, hvv = 0.0;
+#pragma unroll
+        for (int j = 0; j < N1; ++j) {
+          double b = vt[j * 3], db = vt[j * 3 + 1];
+          v += T[j * NM] * b;
+          dfix += T[j * NM + 1] * b;
+          dvar += T[j * NM] * db;
+          if (DDG) {
+            hff += T[j * NM + NM - 1] * b;
+            hfv += T[j * NM + 1] * db;
+            hvv += T[j * NM] * vt[j * 3 + 2];
+          }
+        }
+        us[side][eq] = v;
+        double tt[6];
+        tt[0] = 0.0;
+        tt[1] = a1 ? dvar : dfix;
+        tt[2] = a1 ? dfix : dvar;
+        tt[3] = a1 ? hvv : hff;
+        tt[4] = hfv;
+        tt[5] = a1 ? hff : hvv;
+        double hx[4];
+        basis_phys<DDG>(tt, Ji, Hm, gs[side] + eq * 2, hx);
+        if (DDG) {
+#pragma unroll
+          for (int a = 0; a < 4; ++a) hs[side][eq * 4 + a] = hx[a];
+        }
+      }
+    }
+    const double* bval = interior ? nullptr : dm.bvals + ((size_t)bidx * NQF + q) * NEQ;
+    double out[NEQ], gq[4];
+    face_flux_states<PDE, DDG>(pp, fp, interior, bct, bval, us[0], gs[0], hs[0], us[1], gs[1], hs[1], out, gq);
+    size_t k = (size_t)f * NQF + q;
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) dm.face_flux[k * NEQ + eq] = out[eq];
+    if (Phys<PDE>::has_ic && pp.sigma_ic != 0.0) {
+      // layout [F][side][NQF][NEQ=1][2]
+      double* fg = dm.face_grad + (size_t)f * 2 * NQF * 2;
+      fg[(0 * NQF + q) * 2 + 0] = gq[0];
+      fg[(0 * NQF + q) * 2 + 1] = gq[1];
+      fg[(1 * NQF + q) * 2 + 0] = gq[2];
+      fg[(1 * NQF + q) * 2 + 1] = gq[3];
+    }
   }
 }
 
 // ----------------------------------------------------- volume + face lifting
+// Tensor-product sum factorisation. With basis i = (i0, i1) and volume point
+// q = (q0, q1) (dim 0 slowest on both), phi_i(q) = b[q0][i0] * b[q1][i1] and
+// the xi-derivatives replace one factor by db. The element interpolation
+//   u(q), du/dxi0(q), du/dxi1(q)  from  c[i]
+// runs as two 1D contractions (over i1, then i0), and the test-function
+// contraction
+//   r[i] = sum_q dphi_i/dxi0 G0(q) + dphi_i/dxi1 G1(q) + phi_i S(q)
+// as two more (over q1, then q0). The face lifting factors the same way: on
+// local face lf the reference coordinate xi_a (a = lf & 1) is fixed, so
+//   sum_qf phi_i(x_qf) F(qf) = bfix_lf[i_a] * L_lf[i_(1-a)],
+//   L_lf[j] = sum_qf bvar_lf[qf][j] F(qf).
+// Each stage gives a thread one row of data and loops over the 1D table
+// indices: the lanes of a warp read consecutive words of the staged data and
+// a handful of table entries, and the staged layouts below keep those
+// accesses free of bank conflicts (the 1D tables use a padded row stride).
 template <int PDE, int P, int G>
 struct VolCfg {
   using C = Cfg<PDE, P, G>;
+  static constexpr int N1 = P + 1, Q1 = G + P, NEQ = C::NEQ;
   static constexpr int THREADS = 256;
   static constexpr int EPB_RAW = THREADS / C::NQV;
   static constexpr int EPB = EPB_RAW < 1 ? 1 : EPB_RAW;
-  static constexpr int TAB = C::NQV * C::NB * 3;                     // doubles
-  static constexpr int PER_EL = C::BS + C::NQV * C::NEQ * 3;          // coef + G + S
-  static constexpr size_t SMEM = sizeof(double) * (TAB + EPB * PER_EL);
+  static constexpr int TS = N1 + 1;                 // padded row stride of b, db
+  static constexpr int US = N1 + 1;                 // padded row stride of the staged coefficients
+  static constexpr int TAB1 = 2 * Q1 * TS;          // b, db
+  static constexpr int TABF = 4 * N1;               // bfix per local face
+  static constexpr int TABV = 8 * C::NQF * N1;      // bvar per (local face, orientation, point)
+  static constexpr int U_EL = NEQ * N1 * US;        // c[eq][i0][i1]
+  static constexpr int T_EL = NEQ * 2 * N1 * Q1;    // T[eq][2][i0][q1], later AB[eq][2][q0][i1]
+  static constexpr int GS_EL = NEQ * 3 * C::NQV;    // GS[eq][3][q]
+  static constexpr int FF_EL = 4 * C::NQF * NEQ;    // signed face fluxes [lf][qf][eq]
+  static constexpr int L_EL = NEQ * 4 * N1;         // lifted face fluxes L[eq][lf][j]
+  static constexpr int PER_EL = U_EL + T_EL + GS_EL + FF_EL + L_EL;
+  static constexpr size_t SMEM = sizeof(double) * (TAB1 + TABF + TABV + EPB * PER_EL) + sizeof(int) * EPB * 8;
 };
 
 template <int PDE, int P, int G>
-__global__ void __launch_bounds__(256) vol_lift_kernel(DeviceMesh dm, PhysParams pp, const double* __restrict__ u,
-                                                       double* __restrict__ res) {
+__global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh dm, PhysParams pp,
+                                                                    const double* __restrict__ u,
+                                                                    double* __restrict__ res) {
   using C = Cfg<PDE, P, G>;
   using V = VolCfg<PDE, P, G>;
   constexpr int NEQ = C::NEQ, NB = C::NB, BS = C::BS, NQV = C::NQV, NQF = C::NQF, EPB = V::EPB;
+  constexpr int N1 = V::N1, Q1 = V::Q1, TS = V::TS, US = V::US;
   extern __shared__ double smem[];
-  double* s_tab = smem;                          // [NQV][NB][3]
-  double* s_coef = s_tab + V::TAB;               // [EPB][BS]
-  double* s_G = s_coef + EPB * BS;               // [EPB][NQV][NEQ][2]
-  double* s_S = s_G + EPB * NQV * NEQ * 2;       // [EPB][NQV][NEQ]
+  double* s_b = smem;                            // [Q1][TS]
+  double* s_db = s_b + Q1 * TS;                  // [Q1][TS]
+  double* s_tf = s_b + V::TAB1;                  // [4][N1]
+  double* s_tv = s_tf + V::TABF;                 // [4][2][NQF][N1]
+  double* s_u = s_tv + V::TABV;                  // [EPB][NEQ][N1][US]
+  double* s_T = s_u + EPB * V::U_EL;             // [EPB][NEQ][2][N1][Q1], then [EPB][NEQ][2][Q1][N1]
+  double* s_GS = s_T + EPB * V::T_EL;            // [EPB][NEQ][3][NQV]
+  double* s_ff = s_GS + EPB * V::GS_EL;          // [EPB][4][NQF][NEQ]
+  double* s_L = s_ff + EPB * V::FF_EL;           // [EPB][NEQ][4][N1]
+  int* s_fi = (int*)(s_L + EPB * V::L_EL);       // [EPB][4]: face index; [EPB][4]: side + 2 * orientation
   const int e0 = blockIdx.x * EPB;
   const int ne = min(EPB, dm.E - e0);
   const int tid = threadIdx.x;
-  for (int t = tid; t < V::TAB; t += blockDim.x) s_tab[t] = dm.tab_vol[t];
-  // element coefficient tiles are contiguous in the reference layout
-  const double* ublk = u + (size_t)e0 * BS;
-  for (int t = tid; t < ne * BS; t += blockDim.x) s_coef[t] = ublk[t];
+
+  // S0: 1D tables, coefficient tiles (contiguous in the reference layout,
+  // read coalesced and stored as [eq][i0][i1]), face records
+  for (int t = tid; t < Q1 * N1; t += V::THREADS) {
+    int q = t / N1, i = t - q * N1;
+    s_b[q * TS + i] = dm.tab_1d[t];
+    s_db[q * TS + i] = dm.tab_1d[Q1 * N1 + t];
+  }
+  for (int t = tid; t < V::TABF; t += V::THREADS) s_tf[t] = dm.tab_f1d[t * 3];
+  for (int t = tid; t < V::TABV; t += V::THREADS) s_tv[t] = dm.tab_f1d[(V::TABF + t) * 3];
+  for (int t = tid; t < ne * BS; t += V::THREADS) {
+    int el = t / BS, r = t - el * BS;
+    int i = r / NEQ, eq = r - i * NEQ;
+    int i0 = i / N1, i1 = i - i0 * N1;
+    s_u[el * V::U_EL + (eq * N1 + i0) * US + i1] = u[(size_t)e0 * BS + t];
+  }
+  for (int t = tid; t < ne * 4; t += V::THREADS) {
+    int e = e0 + t / 4;
+    int fidx = dm.el_face[e * 4 + (t & 3)];
+    int side = dm.el_side[e * 4 + (t & 3)];
+    int o = side ? dm.face_info[8 * fidx + 4] : 0;
+    s_fi[t] = fidx;
+    s_fi[EPB * 4 + t] = side + 2 * o;
+  }
   __syncthreads();
 
+  // S1: contract over i1 (thread = (el, i0, q1), all equations):
+  //     T[el][eq][0/1][i0][q1] = sum_i1 c[i0][i1] (b, db)[q1][i1];
+  //     and gather the signed face fluxes of the element's four faces
+  for (int t = tid; t < ne * N1 * Q1; t += V::THREADS) {
+    int el = t / (N1 * Q1), r = t - el * (N1 * Q1);
+    int i0 = r / Q1, q1 = r - i0 * Q1;
+    double b[N1], db[N1];
+#pragma unroll
+    for (int i1 = 0; i1 < N1; ++i1) { b[i1] = s_b[q1 * TS + i1]; db[i1] = s_db[q1 * TS + i1]; }
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) {
+      const double* c = s_u + el * V::U_EL + (eq * N1 + i0) * US;
+      double tv = 0.0, td = 0.0;
+#pragma unroll
+      for (int i1 = 0; i1 < N1; ++i1) {
+        tv += c[i1] * b[i1];
+        td += c[i1] * db[i1];
+      }
+      double* T = s_T + el * V::T_EL + eq * 2 * N1 * Q1 + i0 * Q1 + q1;
+      T[0] = tv;
+      T[N1 * Q1] = td;
+    }
+  }
+  for (int t = tid; t < ne * 4 * NQF * NEQ; t += V::THREADS) {
+    int elf = t / (NQF * NEQ), k = t - elf * (NQF * NEQ);
+    int fidx = s_fi[elf];
+    double v = dm.face_flux[(size_t)fidx * NQF * NEQ + k];
+    s_ff[t] = (s_fi[EPB * 4 + elf] & 1) ? -v : v;
+  }
+  __syncthreads();
+
+  // S2: contract over i0 (thread = (el, q0, q1)), pull back, physical flux per point
   const int nq = dm.E * NQV;
   const bool has_src = dm.src != nullptr;
-  for (int t = tid; t < ne * NQV; t += blockDim.x) {
+  for (int t = tid; t < ne * NQV; t += V::THREADS) {
     int el = t / NQV, q = t - el * NQV;
+    int q0 = q / Q1, q1 = q - q0 * Q1;
     int e = e0 + el;
-    const double* cf = s_coef + el * BS;
-    const double* tb = s_tab + q * NB * 3;
-    double uq[NEQ], gxi[NEQ][2];
-#pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) { uq[eq] = 0.0; gxi[eq][0] = gxi[eq][1] = 0.0; }
-#pragma unroll 4
-    for (int i = 0; i < NB; ++i) {
-      double phi = tb[i * 3], d0 = tb[i * 3 + 1], d1 = tb[i * 3 + 2];
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) {
-        double c = cf[i * NEQ + eq];
-        uq[eq] += c * phi;
-        gxi[eq][0] += c * d0;
-        gxi[eq][1] += c * d1;
-      }
-    }
     size_t kq = (size_t)e * NQV + q;
     double Ji[4] = {dm.vgeo[0 * nq + kq], dm.vgeo[1 * nq + kq], dm.vgeo[2 * nq + kq], dm.vgeo[3 * nq + kq]};
     double wd = dm.vgeo[4 * nq + kq];
+    double b[N1], db[N1];
+#pragma unroll
+    for (int i0 = 0; i0 < N1; ++i0) { b[i0] = s_b[q0 * TS + i0]; db[i0] = s_db[q0 * TS + i0]; }
+    double uq[NEQ], gxi[NEQ][2];
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) {
+      const double* T = s_T + el * V::T_EL + eq * 2 * N1 * Q1 + q1;
+      double v = 0.0, g0 = 0.0, g1 = 0.0;
+#pragma unroll
+      for (int i0 = 0; i0 < N1; ++i0) {
+        double tv = T[i0 * Q1], td = T[N1 * Q1 + i0 * Q1];
+        v += b[i0] * tv;
+        g0 += db[i0] * tv;
+        g1 += b[i0] * td;
+      }
+      uq[eq] = v;
+      gxi[eq][0] = g0;
+      gxi[eq][1] = g1;
+    }
     double gx[2 * NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq)
@@ -232,58 +481,106 @@ __global__ void __launch_bounds__(256) vol_lift_kernel(DeviceMesh dm, PhysParams
       for (int d = 0; d < 2; ++d) gx[eq * 2 + d] = gxi[eq][0] * Ji[0 * 2 + d] + gxi[eq][1] * Ji[1 * 2 + d];
     double F[2 * NEQ];
     Phys<PDE>::flux(pp, uq, gx, F);
-    double* Gq = s_G + (el * NQV + q) * NEQ * 2;
+    double* GS = s_GS + el * V::GS_EL + q;
 #pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq)
+    for (int eq = 0; eq < NEQ; ++eq) {
 #pragma unroll
       for (int kk = 0; kk < 2; ++kk)
-        Gq[eq * 2 + kk] = (F[eq * 2 + 0] * Ji[kk * 2 + 0] + F[eq * 2 + 1] * Ji[kk * 2 + 1]) * wd;
-    double* Sq = s_S + (el * NQV + q) * NEQ;
-    if (has_src) {
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) Sq[eq] = -dm.src[kq * NEQ + eq] * wd;
+        GS[(eq * 3 + kk) * NQV] = (F[eq * 2 + 0] * Ji[kk * 2 + 0] + F[eq * 2 + 1] * Ji[kk * 2 + 1]) * wd;
+      GS[(eq * 3 + 2) * NQV] = has_src ? -dm.src[kq * NEQ + eq] * wd : 0.0;
     }
   }
   __syncthreads();
 
+  // S3: contract over q1 (thread = (el, q0, i1)):
+  //     A = sum_q1 b[q1][i1] G0, B = sum_q1 db[q1][i1] G1 + b[q1][i1] S  -> AB[el][eq][0/1][q0][i1];
+  //     lift the face fluxes along each face (thread = (el, lf, j)): L[el][eq][lf][j]
+  for (int t = tid; t < ne * Q1 * N1; t += V::THREADS) {
+    int el = t / (Q1 * N1), r = t - el * (Q1 * N1);
+    int q0 = r / N1, i1 = r - q0 * N1;
+    double b[Q1], db[Q1];
+#pragma unroll
+    for (int q1 = 0; q1 < Q1; ++q1) { b[q1] = s_b[q1 * TS + i1]; db[q1] = s_db[q1 * TS + i1]; }
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) {
+      const double* GS = s_GS + el * V::GS_EL + eq * 3 * NQV + q0 * Q1;
+      double a = 0.0, bb = 0.0;
+#pragma unroll
+      for (int q1 = 0; q1 < Q1; ++q1) {
+        a += b[q1] * GS[q1];
+        bb += db[q1] * GS[NQV + q1] + b[q1] * GS[2 * NQV + q1];
+      }
+      double* AB = s_T + el * V::T_EL + eq * 2 * Q1 * N1 + q0 * N1 + i1;
+      AB[0] = a;
+      AB[Q1 * N1] = bb;
+    }
+  }
+  for (int t = tid; t < ne * 4 * N1; t += V::THREADS) {
+    int el = t / (4 * N1), r = t - el * (4 * N1);
+    int lf = r / N1, j = r - lf * N1;
+    int o = s_fi[EPB * 4 + el * 4 + lf] >> 1;
+    const double* tv = s_tv + (lf * 2 + o) * NQF * N1 + j;
+    const double* ff = s_ff + (el * 4 + lf) * NQF * NEQ;
+    double acc[NEQ];
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) acc[eq] = 0.0;
+#pragma unroll
+    for (int qf = 0; qf < NQF; ++qf) {
+      double w = tv[qf * N1];
+#pragma unroll
+      for (int eq = 0; eq < NEQ; ++eq) acc[eq] += w * ff[qf * NEQ + eq];
+    }
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) s_L[el * V::L_EL + (eq * 4 + lf) * N1 + j] = acc[eq];
+  }
+  __syncthreads();
+
+  // S4: contract over q0 and add the lifted face terms (thread = (el, i0, i1), all equations)
   const bool ic = Phys<PDE>::has_ic && pp.sigma_ic != 0.0;
-  for (int t = tid; t < ne * BS; t += blockDim.x) {
-    int el = t / BS, r = t - el * BS;
-    int i = r / NEQ, eq = r - i * NEQ;
+  for (int t = tid; t < ne * NB; t += V::THREADS) {
+    int el = t / NB, i = t - el * NB;
+    int i0 = i / N1, i1 = i - i0 * N1;
     int e = e0 + el;
-    const double* Gq = s_G + el * NQV * NEQ * 2;
-    double acc = 0.0;
-#pragma unroll 5
-    for (int q = 0; q < NQV; ++q) {
-      const double* tb = s_tab + (q * NB + i) * 3;
-      acc += tb[1] * Gq[(q * NEQ + eq) * 2 + 0] + tb[2] * Gq[(q * NEQ + eq) * 2 + 1];
-    }
-    if (has_src) {
-      const double* Sq = s_S + el * NQV * NEQ;
-#pragma unroll 5
-      for (int q = 0; q < NQV; ++q) acc += s_tab[(q * NB + i) * 3] * Sq[q * NEQ + eq];
-    }
+    double b[Q1], db[Q1];
 #pragma unroll
-    for (int lf = 0; lf < 4; ++lf) {
-      int fidx = dm.el_face[e * 4 + lf];
-      int side = dm.el_side[e * 4 + lf];
-      int o = side ? dm.face_info[8 * fidx + 4] : 0;
-      const double* tf = dm.tab_face + ((size_t)(lf * 2 + o) * NQF * NB + i) * 6;
-      const double* ff = dm.face_flux + (size_t)fidx * NQF * NEQ + eq;
-      double s = 0.0;
+    for (int q0 = 0; q0 < Q1; ++q0) { b[q0] = s_b[q0 * TS + i0]; db[q0] = s_db[q0 * TS + i0]; }
+    double bf[4];
 #pragma unroll
-      for (int qf = 0; qf < NQF; ++qf) s += tf[(size_t)qf * NB * 6] * ff[qf * NEQ];
-      acc += side ? -s : s;
-      if (ic) {
+    for (int lf = 0; lf < 4; ++lf) bf[lf] = s_tf[lf * N1 + ((lf & 1) ? i1 : i0)];
+    double out[NEQ];
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) {
+      const double* AB = s_T + el * V::T_EL + eq * 2 * Q1 * N1 + i1;
+      double acc = 0.0;
+#pragma unroll
+      for (int q0 = 0; q0 < Q1; ++q0) acc += db[q0] * AB[q0 * N1] + b[q0] * AB[Q1 * N1 + q0 * N1];
+      const double* L = s_L + el * V::L_EL + eq * 4 * N1;
+#pragma unroll
+      for (int lf = 0; lf < 4; ++lf) acc += bf[lf] * L[lf * N1 + ((lf & 1) ? i0 : i1)];
+      out[eq] = acc;
+    }
+    if (ic) {
+#pragma unroll
+      for (int lf = 0; lf < 4; ++lf) {
+        int so = s_fi[EPB * 4 + el * 4 + lf];
+        int fidx = s_fi[el * 4 + lf], side = so & 1;
+        const double* tg = dm.tab_face + ((size_t)(lf * 2 + (so >> 1)) * NQF * NB + i) * 6;
         const double* fg = dm.face_grad + ((size_t)(fidx * 2 + side) * NQF) * 2;
         double sg = 0.0;
 #pragma unroll
         for (int qf = 0; qf < NQF; ++qf)
-          sg += tf[(size_t)qf * NB * 6 + 1] * fg[qf * 2 + 0] + tf[(size_t)qf * NB * 6 + 2] * fg[qf * 2 + 1];
-        acc -= sg;
+          sg += tg[(size_t)qf * NB * 6 + 1] * fg[qf * 2 + 0] + tg[(size_t)qf * NB * 6 + 2] * fg[qf * 2 + 1];
+        out[0] -= sg;
       }
     }
-    res[(size_t)e * BS + r] = acc;
+    double* rp = res + (size_t)e * BS + i * NEQ;
+    if (NEQ % 2 == 0 && (reinterpret_cast<uintptr_t>(res) & 15) == 0) {
+#pragma unroll
+      for (int eq = 0; eq + 1 < NEQ; eq += 2) reinterpret_cast<double2*>(rp)[eq / 2] = make_double2(out[eq], out[eq + 1]);
+    } else {
+#pragma unroll
+      for (int eq = 0; eq < NEQ; ++eq) rp[eq] = out[eq];
+    }
   }
 }
 
@@ -306,24 +603,36 @@ cudaError_t launch_geometry(const DeviceMesh& dm, cudaStream_t s) {
   return cudaErrorInvalidValue;
 }
 
+// raises a kernel's dynamic shared memory limit once per device
+template <class K>
+static cudaError_t smem_attr_once(K kernel, size_t bytes, std::atomic<unsigned>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  unsigned bit = 1u << (dev & 31);
+  if (done.load(std::memory_order_relaxed) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done.fetch_or(bit);
+  return e;
+}
+
 template <int PDE, int P, int G>
 static cudaError_t residual_pg(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
                                cudaStream_t s, cudaEvent_t mid) {
-  using C = Cfg<PDE, P, G>;
   using V = VolCfg<PDE, P, G>;
-  int nf = dm.F * C::NQF;
-  if (pp.beta1 != 0.0)
-    face_flux_kernel<PDE, P, G, true><<<(nf + 127) / 128, 128, 0, s>>>(dm, pp, u);
-  else
-    face_flux_kernel<PDE, P, G, false><<<(nf + 127) / 128, 128, 0, s>>>(dm, pp, u);
-  if (mid) cudaEventRecord(mid, s);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(vol_lift_kernel<PDE, P, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)V::SMEM);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
+  static std::atomic<unsigned> attr_face_ddg{0}, attr_face_ip{0}, attr_vol{0};
+  cudaError_t e;
+  if (pp.beta1 != 0.0) {
+    using FC = FaceCfg<PDE, P, G, true>;
+    if ((e = smem_attr_once(face_flux_kernel<PDE, P, G, true>, FC::SMEM, attr_face_ddg)) != cudaSuccess) return e;
+    face_flux_kernel<PDE, P, G, true><<<(dm.F + FC::FPB - 1) / FC::FPB, FC::THREADS, FC::SMEM, s>>>(dm, pp, u);
+  } else {
+    using FC = FaceCfg<PDE, P, G, false>;
+    if ((e = smem_attr_once(face_flux_kernel<PDE, P, G, false>, FC::SMEM, attr_face_ip)) != cudaSuccess) return e;
+    face_flux_kernel<PDE, P, G, false><<<(dm.F + FC::FPB - 1) / FC::FPB, FC::THREADS, FC::SMEM, s>>>(dm, pp, u);
   }
+  if (mid) cudaEventRecord(mid, s);
+  if ((e = smem_attr_once(vol_lift_kernel<PDE, P, G>, V::SMEM, attr_vol)) != cudaSuccess) return e;
   int nblk = (dm.E + V::EPB - 1) / V::EPB;
   vol_lift_kernel<PDE, P, G><<<nblk, V::THREADS, V::SMEM, s>>>(dm, pp, u, res);
   return cudaGetLastError();
