@@ -1,0 +1,145 @@
+// Block-row products on the element block pattern, shared by the BSR SpMV,
+// the block-diagonal apply and the block-ILU(0) triangular solves:
+//
+//   y_e[r] = x0_e[r] + sign * sum_{blocks (e, k) selected} A_ek[r][:] . v_k
+//
+// One warp computes R consecutive rows of one block row. Lane l holds columns
+// l, l + 32, ... of every row it touches, so each load of a block row is one
+// contiguous 256-byte segment; the R partial sums are reduced across the warp
+// with butterfly shuffles and lane rr stores row r0 + rr.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace icx {
+
+enum BlockRowMode {
+  BR_ALL = 0,    // every block of the row (SpMV)
+  BR_LOWER = 1,  // blocks with column < row (forward substitution)
+  BR_UPPER = 2,  // blocks with column > row (backward substitution)
+  BR_DIAG = 3    // block-diagonal storage D[e] (one block per row, column = row)
+};
+
+// rows of one launch: either all block rows 0..nrows-1 (level < 0) or the
+// elements i + nx * j of the structured grid with i + j = level
+struct RowSet {
+  int nx, ny, level, nrows;
+  __host__ __device__ int count() const {
+    if (level < 0) return nrows;
+    int i0 = level - (ny - 1) > 0 ? level - (ny - 1) : 0;
+    int i1 = level < nx - 1 ? level : nx - 1;
+    return i1 - i0 + 1;
+  }
+  __device__ int row(int idx) const {
+    if (level < 0) return idx;
+    int i0 = level - (ny - 1) > 0 ? level - (ny - 1) : 0;
+    int i = i0 + idx;
+    return i + nx * (level - i);
+  }
+};
+
+template <int BS>
+struct BlockRowCfg {
+  static constexpr int NS = (BS + 31) / 32;                   // column chunks per lane
+  static constexpr int R = BS >= 64 ? 8 : (BS >= 32 ? 4 : 2);  // rows per warp
+  static constexpr int GROUPS = (BS + R - 1) / R;             // warps per block row
+};
+
+template <int BS, int MODE>
+__global__ void __launch_bounds__(256) block_row_kernel(RowSet rs, const int* __restrict__ rowptr,
+                                                        const int* __restrict__ colidx,
+                                                        const double* __restrict__ A,
+                                                        const double* v,
+                                                        const double* x0, double sign,
+                                                        double* y) {
+  using K = BlockRowCfg<BS>;
+  constexpr int NS = K::NS, R = K::R;
+  const int lane = threadIdx.x & 31;
+  const long long task = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (task >= (long long)rs.count() * K::GROUPS) return;
+  const int idx = (int)(task / K::GROUPS), g = (int)(task - (long long)idx * K::GROUPS);
+  const int e = rs.row(idx);
+  const int r0 = g * R;
+  double acc[R];
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr) acc[rr] = 0.0;
+  // blocks of this row: on the structured grid the lower blocks are the
+  // first (j > 0) + (i > 0) of the row (columns e - nx, e - 1) and the upper
+  // blocks the last (i < nx - 1) + (j < ny - 1) (columns e + 1, e + nx)
+  int kb0, kb1;
+  if (MODE == BR_DIAG) { kb0 = e; kb1 = e + 1; }
+  else if (MODE == BR_ALL) { kb0 = rowptr[e]; kb1 = rowptr[e + 1]; }
+  else {
+    const int gi = e % rs.nx, gj = e / rs.nx;
+    if (MODE == BR_LOWER) { kb0 = rowptr[e]; kb1 = kb0 + (gj > 0) + (gi > 0); }
+    else { kb1 = rowptr[e + 1]; kb0 = kb1 - (gi < rs.nx - 1) - (gj < rs.ny - 1); }
+    // the next level's blocks of this kind into L2 while this level computes
+    if (g == 0 && rs.level >= 0) {
+      const int nl = rs.level + (MODE == BR_LOWER ? 1 : -1);
+      if (nl >= 0 && nl <= rs.nx + rs.ny - 2) {
+        RowSet nrs{rs.nx, rs.ny, nl, 0};
+        const int ncount = nrs.count();
+        for (int pi = idx; pi < ncount && pi <= idx + (idx == rs.count() - 1 ? ncount : 0); ++pi) {
+          const int ne = nrs.row(pi);
+          const int ni = ne % rs.nx, nj = ne / rs.nx;
+          int p0, p1;
+          if (MODE == BR_LOWER) { p0 = rowptr[ne]; p1 = p0 + (nj > 0) + (ni > 0); }
+          else { p1 = rowptr[ne + 1]; p0 = p1 - (ni < rs.nx - 1) - (nj < rs.ny - 1); }
+          const char* base = reinterpret_cast<const char*>(A + (size_t)p0 * BS * BS);
+          const size_t bytes = (size_t)(p1 - p0) * BS * BS * sizeof(double);
+          for (size_t off = (size_t)lane * 128; off < bytes; off += 32 * 128)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(base + off));
+        }
+      }
+    }
+  }
+  for (int kb = kb0; kb < kb1; ++kb) {
+    const int k = MODE == BR_DIAG ? e : colidx[kb];
+    double xv[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      int c = lane + 32 * s;
+      xv[s] = c < BS ? v[(size_t)k * BS + c] : 0.0;
+    }
+    const double* Ab = A + (size_t)kb * BS * BS;
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      int r = r0 + rr;
+      if (r < BS) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          int c = lane + 32 * s;
+          if (c < BS) acc[rr] += Ab[(size_t)r * BS + c] * xv[s];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
+  }
+  double mine = 0.0;
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr)
+    if (lane == rr) mine = acc[rr];
+  const int r = r0 + lane;
+  if (lane < R && r < BS) {
+    double base = x0 ? x0[(size_t)e * BS + r] : 0.0;
+    y[(size_t)e * BS + r] = base + sign * mine;
+  }
+}
+
+// launch over a row set: 8 warps per CTA
+template <int BS, int MODE>
+inline cudaError_t launch_block_rows(const RowSet& rs, const int* rowptr, const int* colidx, const double* A,
+                                     const double* v, const double* x0, double sign, double* y, cudaStream_t s) {
+  long long tasks = (long long)rs.count() * BlockRowCfg<BS>::GROUPS;
+  if (tasks <= 0) return cudaSuccess;
+  unsigned blocks = (unsigned)((tasks + 7) / 8);
+  block_row_kernel<BS, MODE><<<blocks, 256, 0, s>>>(rs, rowptr, colidx, A, v, x0, sign, y);
+  return cudaGetLastError();
+}
+
+#define ICX_BLOCK_SIZES(X) X(4) X(9) X(16) X(25) X(36) X(64) X(100)
+
+}  // namespace icx

@@ -19,6 +19,7 @@
 #include <cfloat>
 
 #include "icx_dg.cuh"
+#include "icx_blockrow.cuh"
 
 namespace icx {
 
@@ -353,24 +354,6 @@ __global__ void __launch_bounds__(256) jac_elem_kernel(DeviceMesh dm, PhysParams
 
 // ------------------------------------------------------------------ SpMV
 // y = J x; one warp per block row, lanes over the rows of the block
-template <int BS>
-__global__ void bsr_spmv_kernel(int E, const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                                const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y) {
-  int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-  int lane = threadIdx.x & 31;
-  if (row >= E) return;
-  for (int r = lane; r < BS; r += 32) {
-    double acc = 0.0;
-    for (int k = rowptr[row]; k < rowptr[row + 1]; ++k) {
-      const double* A = vals + (size_t)k * BS * BS + (size_t)r * BS;
-      const double* xv = x + (size_t)colidx[k] * BS;
-#pragma unroll 4
-      for (int c = 0; c < BS; ++c) acc += A[c] * xv[c];
-    }
-    y[(size_t)row * BS + r] = acc;
-  }
-}
-
 template <int PDE, int P, int G>
 static cudaError_t jac_pg(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* vals, double eps,
                           cudaStream_t s) {
@@ -408,11 +391,10 @@ cudaError_t launch_jacobian_fd(const DeviceMesh& dm, const PhysParams& pp, const
 
 cudaError_t launch_bsr_spmv(const DeviceMesh& dm, const double* vals, const double* x, double* y, cudaStream_t s) {
   int bs = dm.nb * dm.neq;
-  int blocks = (dm.E + 7) / 8;
+  RowSet rs{0, 0, -1, dm.E};
 #define ICX_SPMV_CASE(B) \
-  if (bs == B) { bsr_spmv_kernel<B><<<blocks, 256, 0, s>>>(dm.E, dm.bsr_rowptr, dm.bsr_colidx, vals, x, y); return cudaGetLastError(); }
-  ICX_SPMV_CASE(4) ICX_SPMV_CASE(9) ICX_SPMV_CASE(16) ICX_SPMV_CASE(25)
-  ICX_SPMV_CASE(36) ICX_SPMV_CASE(64) ICX_SPMV_CASE(100)
+  if (bs == B) return launch_block_rows<B, BR_ALL>(rs, dm.bsr_rowptr, dm.bsr_colidx, vals, x, nullptr, 1.0, y, s);
+  ICX_BLOCK_SIZES(ICX_SPMV_CASE)
 #undef ICX_SPMV_CASE
   return cudaErrorInvalidValue;
 }

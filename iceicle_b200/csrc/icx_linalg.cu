@@ -7,100 +7,120 @@
 
 #include "icx_internal.h"
 #include "icx_linalg.h"
+#include "icx_blockrow.cuh"
 
 namespace icx {
 
 // ----------------------------------------------------- block inversion
-// In-place Gauss-Jordan inversion with partial pivoting of one bs x bs block
-// per CTA, in shared memory. A singular pivot leaves the block as identity and
-// raises *flag (the preconditioner degrades to no-op on that block).
-__global__ void block_invert_kernel(int nblk, int bs, const double* __restrict__ src, const int* __restrict__ blk_index,
-                                    double* __restrict__ dst, int* flag) {
-  extern __shared__ double a[];
-  int* perm = reinterpret_cast<int*>(a + bs * bs);
-  __shared__ int piv_row;
-  __shared__ double piv_val;
+// In-place Gauss-Jordan inversion with partial pivoting of the BS x BS block
+// `a` in shared memory by the whole CTA (blockDim.x >= 2 BS), three barriers
+// per pivot step:
+//   1. warp 0 finds the pivot row p of column k (largest |a[i][k]|, i >= k,
+//      first index on ties) and keeps a[p][k] and a[k][k];
+//   2. column threads swap rows k and p and scale row k by 1/pivot (a[k][k]
+//      becomes 1/pivot); row threads save the multipliers f_i = a[i][k];
+//   3. every entry off row k: a[i][j] -= f_i a[k][j] (j != k), a[i][k] = -f_i a[k][k].
+// The row interchanges are undone as a column permutation when the result is
+// written out (write_inverse). A zero pivot sets *singular and stops.
+template <int BS>
+__device__ void gj_invert(double* a, int* perm, double* fcol, int* singular) {
+  __shared__ int s_p;
+  __shared__ double s_pv, s_akk;
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (tid == 0) *singular = 0;
+  __syncthreads();
+  for (int k = 0; k < BS; ++k) {
+    if (tid < 32) {
+      double best = -1.0;
+      int bi = BS;
+      for (int i = k + lane; i < BS; i += 32) {
+        double v = fabs(a[i * BS + k]);
+        if (v > best) { best = v; bi = i; }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        double ov = __shfl_xor_sync(0xffffffffu, best, off);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+      }
+      if (lane == 0) {
+        s_p = bi;
+        perm[k] = bi;
+        s_pv = a[bi * BS + k];
+        s_akk = a[k * BS + k];
+        if (!(best > 0.0)) *singular = 1;
+      }
+    }
+    __syncthreads();
+    if (*singular) return;
+    const int p = s_p;
+    const double pv = s_pv;
+    if (tid < BS) {
+      const int j = tid;
+      double rk = a[k * BS + j], rp = a[p * BS + j];
+      if (p != k) a[p * BS + j] = rk;
+      a[k * BS + j] = (j == k ? 1.0 : rp) / pv;
+    } else if (tid >= 128 && tid < 128 + BS) {
+      const int i = tid - 128;
+      fcol[i] = (i == p) ? s_akk : a[i * BS + k];
+    }
+    __syncthreads();
+    const double akk = a[k * BS + k];
+    for (int t = tid; t < BS * BS; t += blockDim.x) {
+      int i = t / BS, j = t - i * BS;
+      if (i == k) continue;
+      if (j == k) a[t] = -fcol[i] * akk;
+      else a[t] -= fcol[i] * a[k * BS + j];
+    }
+    __syncthreads();
+  }
+}
+
+// dst = the inverse held in `a` after gj_invert, with the row interchanges
+// undone as column interchanges in reverse order (composed into one gather);
+// the identity if the block was singular
+template <int BS>
+__device__ void write_inverse(const double* a, const int* perm, int* colsrc, int singular, double* dst) {
+  if (threadIdx.x == 0 && !singular) {
+    for (int j = 0; j < BS; ++j) colsrc[j] = j;
+    for (int k = BS - 1; k >= 0; --k) {
+      int p = perm[k];
+      if (p != k) { int t = colsrc[k]; colsrc[k] = colsrc[p]; colsrc[p] = t; }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < BS * BS; t += blockDim.x) {
+    int i = t / BS, j = t - i * BS;
+    dst[t] = singular ? (i == j ? 1.0 : 0.0) : a[i * BS + colsrc[j]];
+  }
+}
+
+template <int BS>
+struct InvSmem {
+  static constexpr size_t BYTES = sizeof(double) * (BS * BS + BS) + sizeof(int) * 2 * BS;
+};
+
+// inverse of one diagonal block per CTA; a singular block becomes the
+// identity and raises *flag (the preconditioner degrades to no-op on it)
+template <int BS>
+__global__ void __launch_bounds__(256) block_invert_kernel(int nblk, const double* __restrict__ src,
+                                                           const int* __restrict__ blk_index,
+                                                           double* __restrict__ dst, int* flag) {
+  extern __shared__ double sh[];
+  double* a = sh;
+  double* fcol = a + BS * BS;
+  int* perm = reinterpret_cast<int*>(fcol + BS);
+  int* colsrc = perm + BS;
   __shared__ int singular;
   int b = blockIdx.x;
   if (b >= nblk) return;
-  const double* A = src + (size_t)blk_index[b] * bs * bs;
-  for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) a[t] = A[t];
-  if (threadIdx.x == 0) singular = 0;
+  const double* A = src + (size_t)blk_index[b] * BS * BS;
+  for (int t = threadIdx.x; t < BS * BS; t += blockDim.x) a[t] = A[t];
   __syncthreads();
-  for (int k = 0; k < bs; ++k) {
-    if (threadIdx.x == 0) {
-      int p = k;
-      double best = fabs(a[k * bs + k]);
-      for (int i = k + 1; i < bs; ++i) {
-        double v = fabs(a[i * bs + k]);
-        if (v > best) { best = v; p = i; }
-      }
-      piv_row = p;
-      perm[k] = p;
-      if (best == 0.0) singular = 1;
-      piv_val = a[p * bs + k];
-    }
-    __syncthreads();
-    if (singular) break;
-    int p = piv_row;
-    if (p != k)
-      for (int j = threadIdx.x; j < bs; j += blockDim.x) {
-        double t = a[k * bs + j];
-        a[k * bs + j] = a[p * bs + j];
-        a[p * bs + j] = t;
-      }
-    __syncthreads();
-    double pv = piv_val;
-    for (int j = threadIdx.x; j < bs; j += blockDim.x) a[k * bs + j] = (j == k ? 1.0 : a[k * bs + j]) / pv;
-    __syncthreads();
-    for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
-      int i = t / bs, j = t - i * bs;
-      if (i == k) continue;
-      double fct = a[i * bs + k];
-      if (j == k) continue;
-      a[t] -= fct * a[k * bs + j];
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < bs; i += blockDim.x)
-      if (i != k) a[i * bs + k] = -a[i * bs + k] * a[k * bs + k];
-    __syncthreads();
-  }
-  if (singular) {
-    if (threadIdx.x == 0) atomicExch(flag, 1);
-    for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) a[t] = (t / bs == t % bs) ? 1.0 : 0.0;
-    __syncthreads();
-  } else {
-    // undo the row interchanges as column interchanges, in reverse order
-    for (int k = bs - 1; k >= 0; --k) {
-      int p = perm[k];
-      if (p != k)
-        for (int i = threadIdx.x; i < bs; i += blockDim.x) {
-          double t = a[i * bs + k];
-          a[i * bs + k] = a[i * bs + p];
-          a[i * bs + p] = t;
-        }
-      __syncthreads();
-    }
-  }
-  double* D = dst + (size_t)b * bs * bs;
-  for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) D[t] = a[t];
-}
-
-// y_e = D_e x_e for block-diagonal D (one warp per block row)
-template <int BS>
-__global__ void block_diag_apply_kernel(int E, const double* __restrict__ D, const double* __restrict__ x,
-                                        double* __restrict__ y) {
-  int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-  int lane = threadIdx.x & 31;
-  if (row >= E) return;
-  const double* xv = x + (size_t)row * BS;
-  for (int r = lane; r < BS; r += 32) {
-    const double* A = D + (size_t)row * BS * BS + (size_t)r * BS;
-    double acc = 0.0;
-#pragma unroll 4
-    for (int c = 0; c < BS; ++c) acc += A[c] * xv[c];
-    y[(size_t)row * BS + r] = acc;
-  }
+  gj_invert<BS>(a, perm, fcol, &singular);
+  __syncthreads();
+  if (singular && threadIdx.x == 0) atomicExch(flag, 1);
+  write_inverse<BS>(a, perm, colsrc, singular, dst + (size_t)b * BS * BS);
 }
 
 // ------------------------------------------------------------ block-ILU(0)
@@ -112,163 +132,163 @@ __global__ void block_diag_apply_kernel(int E, const double* __restrict__ D, con
 // so the rows of one anti-diagonal i + j = level are independent: one launch
 // per level, one CTA per row.
 
-// Gauss-Jordan inversion of the bs x bs block in shared memory `a` (in place)
-__device__ void gj_invert_shared(double* a, int* perm, int bs, int* s_flag, double* s_pv, int* s_pr) {
-  for (int k = 0; k < bs; ++k) {
-    if (threadIdx.x == 0) {
-      int p = k;
-      double best = fabs(a[k * bs + k]);
-      for (int i = k + 1; i < bs; ++i) {
-        double v = fabs(a[i * bs + k]);
-        if (v > best) { best = v; p = i; }
-      }
-      *s_pr = p;
-      perm[k] = p;
-      if (best == 0.0) *s_flag = 1;
-      *s_pv = a[p * bs + k];
-    }
-    __syncthreads();
-    if (*s_flag) return;
-    int p = *s_pr;
-    if (p != k)
-      for (int j = threadIdx.x; j < bs; j += blockDim.x) {
-        double t = a[k * bs + j];
-        a[k * bs + j] = a[p * bs + j];
-        a[p * bs + j] = t;
-      }
-    __syncthreads();
-    double pv = *s_pv;
-    for (int j = threadIdx.x; j < bs; j += blockDim.x) a[k * bs + j] = (j == k ? 1.0 : a[k * bs + j]) / pv;
-    __syncthreads();
-    for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
-      int i = t / bs, j = t - i * bs;
-      if (i == k || j == k) continue;
-      a[t] -= a[i * bs + k] * a[k * bs + j];
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < bs; i += blockDim.x)
-      if (i != k) a[i * bs + k] = -a[i * bs + k] * a[k * bs + k];
-    __syncthreads();
-  }
-  for (int k = bs - 1; k >= 0; --k) {
-    int p = perm[k];
-    if (p != k)
-      for (int i = threadIdx.x; i < bs; i += blockDim.x) {
-        double t = a[i * bs + k];
-        a[i * bs + k] = a[i * bs + p];
-        a[i * bs + p] = t;
-      }
-    __syncthreads();
-  }
-}
-
 __device__ inline int find_block(const int* rowptr, const int* colidx, int r, int c) {
   for (int k = rowptr[r]; k < rowptr[r + 1]; ++k)
     if (colidx[k] == c) return k;
   return -1;
 }
 
-__global__ void ilu_level_kernel(int nx, int ny, int level, int bs, const int* __restrict__ rowptr,
-                                 const int* __restrict__ colidx, double* __restrict__ LU, double* __restrict__ Uinv,
-                                 int* flag) {
-  extern __shared__ double sh[];
-  double* Lek = sh;                                  // bs x bs
-  double* Ainv = sh + bs * bs;                       // bs x bs
-  int* perm = reinterpret_cast<int*>(sh + 2 * bs * bs);
-  __shared__ int s_flag, s_pr;
-  __shared__ double s_pv;
-  int i0 = max(0, level - (ny - 1));
-  int i = i0 + blockIdx.x, j = level - i;
-  if (i >= nx || j < 0) return;
-  int e = i + nx * j;
-  if (threadIdx.x == 0) s_flag = 0;
-  for (int kl = rowptr[e]; kl < rowptr[e + 1]; ++kl) {
-    int k = colidx[kl];
-    if (k >= e) break;  // columns ascend: the lower blocks come first
-    double* Aek = LU + (size_t)kl * bs * bs;
-    const double* Ui = Uinv + (size_t)k * bs * bs;
-    __syncthreads();
-    for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
-      int r = t / bs, c = t - r * bs;
-      double s = 0.0;
-      for (int m = 0; m < bs; ++m) s += Aek[r * bs + m] * Ui[m * bs + c];
-      Lek[t] = s;
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) Aek[t] = Lek[t];
-    for (int kj = rowptr[k]; kj < rowptr[k + 1]; ++kj) {
-      int jc = colidx[kj];
-      if (jc <= k) continue;
-      int ej = find_block(rowptr, colidx, e, jc);
-      if (ej < 0) continue;  // outside the pattern: dropped (level 0 fill)
-      const double* Akj = LU + (size_t)kj * bs * bs;
-      double* Aej = LU + (size_t)ej * bs * bs;
-      __syncthreads();
-      for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
-        int r = t / bs, c = t - r * bs;
-        double s = 0.0;
-        for (int m = 0; m < bs; ++m) s += Lek[r * bs + m] * Akj[m * bs + c];
-        Aej[t] -= s;
+// C = X Y for BS x BS blocks in shared memory, each thread owning 4 x 4
+// output tiles; op(tile, r0, c0, acc) consumes every finished tile
+template <int BS, class Op>
+__device__ inline void block_gemm(const double* X, const double* Y, Op op) {
+  constexpr int NT = (BS + 3) / 4;
+  for (int tt = threadIdx.x; tt < NT * NT; tt += blockDim.x) {
+    const int r0 = (tt / NT) * 4, c0 = (tt % NT) * 4;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int m = 0; m < BS; ++m) {
+      double xa[4], yb[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) xa[a] = (r0 + a < BS) ? X[(r0 + a) * BS + m] : 0.0;
+      if (BS % 4 == 0) {
+        const double2* y2 = reinterpret_cast<const double2*>(Y + m * BS + c0);
+        double2 u0 = y2[0], u1 = y2[1];
+        yb[0] = u0.x; yb[1] = u0.y; yb[2] = u1.x; yb[3] = u1.y;
+      } else {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) yb[b] = (c0 + b < BS) ? Y[m * BS + c0 + b] : 0.0;
       }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += xa[a] * yb[b];
     }
-  }
-  __syncthreads();
-  int kd = find_block(rowptr, colidx, e, e);
-  const double* Aee = LU + (size_t)kd * bs * bs;
-  for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) Ainv[t] = Aee[t];
-  __syncthreads();
-  gj_invert_shared(Ainv, perm, bs, &s_flag, &s_pv, &s_pr);
-  __syncthreads();
-  double* D = Uinv + (size_t)e * bs * bs;
-  if (s_flag) {
-    if (threadIdx.x == 0) atomicExch(flag, 1);
-    for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) D[t] = (t / bs == t % bs) ? 1.0 : 0.0;
-  } else {
-    for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) D[t] = Ainv[t];
+    op(r0, c0, acc);
   }
 }
 
-// one level of the triangular solves, one warp per block row:
-//   forward  (ascending levels):  y_e = x_e - sum_{k<e} L_ek y_k
-//   backward (descending levels): y_e = inv(U_ee) (y_e - sum_{k>e} U_ek y_k)
 template <int BS>
-__global__ void ilu_solve_level_kernel(int nx, int ny, int level, int forward, const int* __restrict__ rowptr,
-                                       const int* __restrict__ colidx, const double* __restrict__ LU,
-                                       const double* __restrict__ Uinv, const double* __restrict__ x,
-                                       double* __restrict__ y) {
-  __shared__ double tmp[4][BS];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int i0 = max(0, level - (ny - 1));
-  int i = i0 + blockIdx.x * 4 + warp;
-  int j = level - i;
-  bool active = i < nx && j >= 0;
-  int e = active ? i + nx * j : 0;
-  if (active) {
-    for (int r = lane; r < BS; r += 32) {
-      double acc = forward ? x[(size_t)e * BS + r] : y[(size_t)e * BS + r];
-      for (int k = rowptr[e]; k < rowptr[e + 1]; ++k) {
-        int c = colidx[k];
-        if (forward ? (c < e) : (c > e)) {
-          const double* A = LU + (size_t)k * BS * BS + (size_t)r * BS;
-          const double* v = y + (size_t)c * BS;
-          for (int m = 0; m < BS; ++m) acc -= A[m] * v[m];
-        }
-      }
-      tmp[warp][r] = acc;
+struct IluSmem {
+  static constexpr size_t BYTES = sizeof(double) * (2 * BS * BS + BS) + sizeof(int) * 2 * BS;
+};
+
+template <int BS>
+__global__ void __launch_bounds__(256) ilu_level_kernel(int nx, int ny, int level, const int* __restrict__ rowptr,
+                                                        const int* __restrict__ colidx, double* __restrict__ LU,
+                                                        double* __restrict__ Uinv, int* flag) {
+  extern __shared__ double sh[];
+  double* X = sh;                  // BS x BS
+  double* Y = X + BS * BS;         // BS x BS
+  double* fcol = Y + BS * BS;      // BS
+  int* perm = reinterpret_cast<int*>(fcol + BS);
+  int* colsrc = perm + BS;
+  __shared__ int singular;
+  const int i0 = max(0, level - (ny - 1));
+  const int i = i0 + blockIdx.x, j = level - i;
+  if (i >= nx || j < 0) return;
+  const int e = i + nx * j;
+  for (int kl = rowptr[e]; kl < rowptr[e + 1]; ++kl) {
+    const int k = colidx[kl];
+    if (k >= e) break;  // columns ascend: the lower blocks come first
+    double* Aek = LU + (size_t)kl * BS * BS;
+    const double* Ui = Uinv + (size_t)k * BS * BS;
+    __syncthreads();
+    for (int t = threadIdx.x; t < BS * BS; t += blockDim.x) {
+      X[t] = Aek[t];
+      Y[t] = Ui[t];
+    }
+    __syncthreads();
+    // L_ek = A_ek inv(U_kk): kept in registers until every thread has read X
+    constexpr int NT = (BS + 3) / 4;
+    constexpr int MAXT = (NT * NT + 255) / 256;
+    double keep[MAXT][4][4];
+    int slot = 0;
+    block_gemm<BS>(X, Y, [&](int r0, int c0, double (&acc)[4][4]) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) keep[slot][a][b] = acc[a][b];
+      ++slot;
+    });
+    __syncthreads();
+    slot = 0;
+    for (int tt = threadIdx.x; tt < NT * NT; tt += blockDim.x, ++slot) {
+      const int r0 = (tt / NT) * 4, c0 = (tt % NT) * 4;
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if (r0 + a < BS && c0 + b < BS) {
+            X[(r0 + a) * BS + c0 + b] = keep[slot][a][b];
+            Aek[(r0 + a) * BS + c0 + b] = keep[slot][a][b];
+          }
+    }
+    // A_ej -= L_ek U_kj for the upper blocks of row k that lie in row e's pattern
+    for (int kj = rowptr[k]; kj < rowptr[k + 1]; ++kj) {
+      const int jc = colidx[kj];
+      if (jc <= k) continue;
+      const int ej = find_block(rowptr, colidx, e, jc);
+      if (ej < 0) continue;  // outside the pattern: dropped (level 0 fill)
+      const double* Akj = LU + (size_t)kj * BS * BS;
+      double* Aej = LU + (size_t)ej * BS * BS;
+      __syncthreads();
+      for (int t = threadIdx.x; t < BS * BS; t += blockDim.x) Y[t] = Akj[t];
+      __syncthreads();
+      block_gemm<BS>(X, Y, [&](int r0, int c0, double (&acc)[4][4]) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b)
+            if (r0 + a < BS && c0 + b < BS) Aej[(r0 + a) * BS + c0 + b] -= acc[a][b];
+      });
     }
   }
-  __syncwarp();
-  if (active) {
-    if (forward) {
-      for (int r = lane; r < BS; r += 32) y[(size_t)e * BS + r] = tmp[warp][r];
-    } else {
-      for (int r = lane; r < BS; r += 32) {
-        const double* A = Uinv + (size_t)e * BS * BS + (size_t)r * BS;
-        double s = 0.0;
-        for (int m = 0; m < BS; ++m) s += A[m] * tmp[warp][m];
-        y[(size_t)e * BS + r] = s;
-      }
-    }
+  __syncthreads();
+  const int kd = find_block(rowptr, colidx, e, e);
+  const double* Aee = LU + (size_t)kd * BS * BS;
+  for (int t = threadIdx.x; t < BS * BS; t += blockDim.x) X[t] = Aee[t];
+  __syncthreads();
+  gj_invert<BS>(X, perm, fcol, &singular);
+  __syncthreads();
+  if (singular && threadIdx.x == 0) atomicExch(flag, 1);
+  write_inverse<BS>(X, perm, colsrc, singular, Uinv + (size_t)e * BS * BS);
+}
+
+// After the factorisation every upper block is scaled by the inverse of its
+// row's diagonal block, U_ek <- inv(U_ee) U_ek (k > e), so that the backward
+// substitution y_e = inv(U_ee) (f_e - sum_{k>e} U_ek y_k) becomes
+//   y_e = inv(U_ee) f_e - sum_{k>e} (inv(U_ee) U_ek) y_k,
+// a plain block-row product whose rows can be split across warps.
+// One CTA per row, both operands staged in shared memory.
+template <int BS>
+__global__ void __launch_bounds__(256) ilu_scale_upper_kernel(int E, const int* __restrict__ rowptr,
+                                                              const int* __restrict__ colidx,
+                                                              double* __restrict__ LU,
+                                                              const double* __restrict__ Uinv) {
+  extern __shared__ double sh[];
+  double* D = sh;            // BS x BS
+  double* B = sh + BS * BS;  // BS x BS
+  const int e = blockIdx.x;
+  if (e >= E) return;
+  const double* Di = Uinv + (size_t)e * BS * BS;
+  for (int t = threadIdx.x; t < BS * BS; t += blockDim.x) D[t] = Di[t];
+  for (int kb = rowptr[e]; kb < rowptr[e + 1]; ++kb) {
+    if (colidx[kb] <= e) continue;
+    double* U = LU + (size_t)kb * BS * BS;
+    __syncthreads();
+    for (int t = threadIdx.x; t < BS * BS; t += blockDim.x) B[t] = U[t];
+    __syncthreads();
+    block_gemm<BS>(D, B, [&](int r0, int c0, double (&acc)[4][4]) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if (r0 + a < BS && c0 + b < BS) U[(r0 + a) * BS + c0 + b] = acc[a][b];
+    });
   }
 }
 
@@ -359,35 +379,33 @@ cudaError_t la_xpay(long long n, const double* x, double a, const double* y, dou
   return cudaGetLastError();
 }
 
-cudaError_t la_block_invert(int nblk, int bs, const double* src, const int* blk_index, double* dst, int* flag,
-                            cudaStream_t s) {
-  size_t smem = sizeof(double) * bs * bs + sizeof(int) * bs;
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    cudaError_t e = cudaFuncSetAttribute(block_invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = smem;
-  }
-  block_invert_kernel<<<nblk, 256, smem, s>>>(nblk, bs, src, blk_index, dst, flag);
-  return cudaGetLastError();
+template <class K>
+static cudaError_t smem_attr(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-#define ICX_BS_SWITCH(bs, CALL) \
-  switch (bs) {                 \
-    case 4: { constexpr int B = 4; CALL; } break;     \
-    case 9: { constexpr int B = 9; CALL; } break;     \
-    case 16: { constexpr int B = 16; CALL; } break;   \
-    case 25: { constexpr int B = 25; CALL; } break;   \
-    case 36: { constexpr int B = 36; CALL; } break;   \
-    case 64: { constexpr int B = 64; CALL; } break;   \
-    case 100: { constexpr int B = 100; CALL; } break; \
-    default: return cudaErrorInvalidValue;            \
+cudaError_t la_block_invert(int nblk, int bs, const double* src, const int* blk_index, double* dst, int* flag,
+                            cudaStream_t s) {
+#define ICX_INV_CASE(B)                                                                        \
+  if (bs == B) {                                                                               \
+    cudaError_t e = smem_attr(block_invert_kernel<B>, InvSmem<B>::BYTES);                      \
+    if (e != cudaSuccess) return e;                                                            \
+    block_invert_kernel<B><<<nblk, 256, InvSmem<B>::BYTES, s>>>(nblk, src, blk_index, dst, flag); \
+    return cudaGetLastError();                                                                 \
   }
+  ICX_BLOCK_SIZES(ICX_INV_CASE)
+#undef ICX_INV_CASE
+  return cudaErrorInvalidValue;
+}
 
 cudaError_t la_block_diag_apply(int E, int bs, const double* D, const double* x, double* y, cudaStream_t s) {
-  int blocks = (E + 7) / 8;
-  ICX_BS_SWITCH(bs, (block_diag_apply_kernel<B><<<blocks, 256, 0, s>>>(E, D, x, y)));
-  return cudaGetLastError();
+  RowSet rs{0, 0, -1, E};
+#define ICX_DIAG_CASE(B) \
+  if (bs == B) return launch_block_rows<B, BR_DIAG>(rs, nullptr, nullptr, D, x, nullptr, 1.0, y, s);
+  ICX_BLOCK_SIZES(ICX_DIAG_CASE)
+#undef ICX_DIAG_CASE
+  return cudaErrorInvalidValue;
 }
 
 static int level_rows(int nx, int ny, int level) {
@@ -397,33 +415,41 @@ static int level_rows(int nx, int ny, int level) {
 }
 
 cudaError_t la_ilu_factor(const DeviceMesh& dm, int nx, int ny, double* LU, double* Uinv, int* flag, cudaStream_t s) {
-  int bs = dm.nb * dm.neq;
-  size_t smem = sizeof(double) * 2 * bs * bs + sizeof(int) * bs;
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    cudaError_t e = cudaFuncSetAttribute(ilu_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = smem;
+  const int bs = dm.nb * dm.neq;
+#define ICX_ILUF_CASE(B)                                                                               \
+  if (bs == B) {                                                                                       \
+    cudaError_t e = smem_attr(ilu_level_kernel<B>, IluSmem<B>::BYTES);                                 \
+    if (e == cudaSuccess) e = smem_attr(ilu_scale_upper_kernel<B>, IluSmem<B>::BYTES);                 \
+    if (e != cudaSuccess) return e;                                                                    \
+    for (int level = 0; level < nx + ny - 1; ++level)                                                  \
+      ilu_level_kernel<B><<<level_rows(nx, ny, level), 256, IluSmem<B>::BYTES, s>>>(                   \
+          nx, ny, level, dm.bsr_rowptr, dm.bsr_colidx, LU, Uinv, flag);                                \
+    ilu_scale_upper_kernel<B><<<dm.E, 256, IluSmem<B>::BYTES, s>>>(dm.E, dm.bsr_rowptr, dm.bsr_colidx, LU, Uinv); \
+    return cudaGetLastError();                                                                         \
   }
-  for (int level = 0; level < nx + ny - 1; ++level)
-    ilu_level_kernel<<<level_rows(nx, ny, level), 256, smem, s>>>(nx, ny, level, bs, dm.bsr_rowptr, dm.bsr_colidx,
-                                                                  LU, Uinv, flag);
-  return cudaGetLastError();
+  ICX_BLOCK_SIZES(ICX_ILUF_CASE)
+#undef ICX_ILUF_CASE
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU, const double* Uinv, const double* x,
-                         double* y, cudaStream_t s) {
+                         double* y, double* tmp, cudaStream_t s) {
   int bs = dm.nb * dm.neq;
-  for (int pass = 0; pass < 2; ++pass) {
-    int fwd = pass == 0;
-    for (int l = 0; l < nx + ny - 1; ++l) {
-      int level = fwd ? l : nx + ny - 2 - l;
-      int blocks = (level_rows(nx, ny, level) + 3) / 4;
-      ICX_BS_SWITCH(bs, (ilu_solve_level_kernel<B><<<blocks, 128, 0, s>>>(nx, ny, level, fwd, dm.bsr_rowptr,
-                                                                           dm.bsr_colidx, LU, Uinv, x, y)));
-    }
+  const int nl = nx + ny - 1;
+  cudaError_t e = cudaSuccess;
+#define ICX_ILU_CASE(B)                                                                                      \
+  if (bs == B) {                                                                                             \
+    for (int l = 0; l < nl && e == cudaSuccess; ++l)                                                         \
+      e = launch_block_rows<B, BR_LOWER>(RowSet{nx, ny, l, 0}, dm.bsr_rowptr, dm.bsr_colidx, LU, y, x, -1.0, y, s); \
+    if (e == cudaSuccess)                                                                                    \
+      e = launch_block_rows<B, BR_DIAG>(RowSet{0, 0, -1, dm.E}, nullptr, nullptr, Uinv, y, nullptr, 1.0, tmp, s); \
+    for (int l = nl - 1; l >= 0 && e == cudaSuccess; --l)                                                    \
+      e = launch_block_rows<B, BR_UPPER>(RowSet{nx, ny, l, 0}, dm.bsr_rowptr, dm.bsr_colidx, LU, y, tmp, -1.0, y, s); \
+    return e;                                                                                                \
   }
-  return cudaGetLastError();
+  ICX_BLOCK_SIZES(ICX_ILU_CASE)
+#undef ICX_ILU_CASE
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace icx

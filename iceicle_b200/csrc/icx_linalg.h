@@ -22,10 +22,12 @@ cudaError_t la_xpay(long long n, const double* x, double a, const double* y, dou
 cudaError_t la_block_invert(int nblk, int bs, const double* src, const int* blk_index, double* dst, int* flag,
                             cudaStream_t s);
 cudaError_t la_block_diag_apply(int E, int bs, const double* D, const double* x, double* y, cudaStream_t s);
-// block-ILU(0) on the structured element grid: LU holds a copy of the BSR values on entry
+// block-ILU(0) on the structured element grid: LU holds a copy of the BSR values on entry;
+// on exit its strictly lower blocks are L, its upper blocks inv(U_ee) U_ek and Uinv the inv(U_ee)
 cudaError_t la_ilu_factor(const DeviceMesh& dm, int nx, int ny, double* LU, double* Uinv, int* flag, cudaStream_t s);
+// y = (LU)^-1 x; tmp: n doubles of scratch (x, y, tmp distinct)
 cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU, const double* Uinv, const double* x,
-                         double* y, cudaStream_t s);
+                         double* y, double* tmp, cudaStream_t s);
 
 }  // namespace icx
 

@@ -30,6 +30,11 @@ struct icx_solver_work {
   double* du = nullptr;
   double* ustep = nullptr;
   double* rwork = nullptr;
+  double* pct = nullptr;    // scratch of the preconditioner apply
+  double* pin = nullptr;    // fixed input / output of the captured ILU apply
+  double* pout = nullptr;
+  cudaGraphExec_t ilu_exec = nullptr;  // the level launches of one ILU apply, captured once
+  cudaStream_t cap = nullptr;          // private stream for the capture
   double* dh = nullptr;     // device scalars (dot results)
   int* flag = nullptr;
   icx::LinalgWork lw;
@@ -66,7 +71,7 @@ icx_status ensure_work(icx_ctx* c, int m) {
   CK(cudaMalloc((void**)&w->pc, vb));
   CK(cudaMalloc((void**)&w->uinv, sizeof(double) * (size_t)dm.E * bs * bs));
   CK(cudaMalloc((void**)&w->V, sizeof(double) * (size_t)(m + 1) * n));
-  double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork};
+  double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork, &w->pct, &w->pin, &w->pout};
   for (double** p : vecs) CK(cudaMalloc((void**)p, sizeof(double) * n));
   CK(cudaMalloc((void**)&w->dh, sizeof(double) * 2 * (m + 2)));
   CK(cudaMalloc((void**)&w->flag, sizeof(int)));
@@ -88,7 +93,29 @@ cudaError_t apply_pc(icx_ctx* c, int kind, const double* x, double* z, cudaStrea
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
   if (kind == 1) return icx::la_block_diag_apply(dm.E, w->bs, w->pc, x, z, s);
-  if (kind == 2) return icx::la_ilu_apply(dm, c->nx, c->ny, w->pc, w->uinv, x, z, s);
+  if (kind == 2) {
+    // the 2 (nx + ny - 1) + 1 launches of one apply are replayed as a CUDA
+    // graph on fixed buffers: the level kernels are short, launch cost dominates
+    if (!w->ilu_exec) {
+      cudaError_t e;
+      if (!w->cap && (e = cudaStreamCreateWithFlags(&w->cap, cudaStreamNonBlocking)) != cudaSuccess) return e;
+      if ((e = cudaStreamBeginCapture(w->cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+      cudaError_t ea = icx::la_ilu_apply(dm, c->nx, c->ny, w->pc, w->uinv, w->pin, w->pout, w->pct, w->cap);
+      cudaGraph_t g = nullptr;
+      cudaError_t ec = cudaStreamEndCapture(w->cap, &g);
+      if (ea != cudaSuccess || ec != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return ea != cudaSuccess ? ea : ec;
+      }
+      e = cudaGraphInstantiate(&w->ilu_exec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) { w->ilu_exec = nullptr; return e; }
+    }
+    cudaError_t e = cudaMemcpyAsync(w->pin, x, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaGraphLaunch(w->ilu_exec, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(z, w->pout, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
+    return e;
+  }
   return cudaMemcpyAsync(z, x, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
 }
 
@@ -197,8 +224,10 @@ namespace icx {
 void free_solver_work(icx_ctx* c) {
   if (!c || !c->sw) return;
   icx_solver_work* w = c->sw;
-  void* ptrs[] = {w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du, w->ustep, w->rwork, w->dh, w->flag,
-                  w->lw.partial};
+  if (w->ilu_exec) cudaGraphExecDestroy(w->ilu_exec);
+  if (w->cap) cudaStreamDestroy(w->cap);
+  void* ptrs[] = {w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du, w->ustep, w->rwork, w->pct, w->pin,
+                  w->pout, w->dh, w->flag, w->lw.partial};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete w;
