@@ -44,18 +44,13 @@ struct BlockRowCfg {
   static constexpr int GROUPS = (BS + R - 1) / R;             // warps per block row
 };
 
-template <int BS, int MODE>
-__global__ void __launch_bounds__(256) block_row_kernel(RowSet rs, const int* __restrict__ rowptr,
-                                                        const int* __restrict__ colidx,
-                                                        const double* __restrict__ A,
-                                                        const double* v,
-                                                        const double* x0, double sign,
-                                                        double* y) {
+template <int BS, int MODE, bool COHERENT>
+__device__ inline void block_row_task(const RowSet& rs, long long task, const int* __restrict__ rowptr,
+                                      const int* __restrict__ colidx, const double* __restrict__ A,
+                                      const double* v, const double* x0, double sign, double* y) {
   using K = BlockRowCfg<BS>;
   constexpr int NS = K::NS, R = K::R;
   const int lane = threadIdx.x & 31;
-  const long long task = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (task >= (long long)rs.count() * K::GROUPS) return;
   const int idx = (int)(task / K::GROUPS), g = (int)(task - (long long)idx * K::GROUPS);
   const int e = rs.row(idx);
   const int r0 = g * R;
@@ -98,7 +93,7 @@ __global__ void __launch_bounds__(256) block_row_kernel(RowSet rs, const int* __
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       int c = lane + 32 * s;
-      xv[s] = c < BS ? v[(size_t)k * BS + c] : 0.0;
+      xv[s] = c < BS ? (COHERENT ? __ldcg(v + (size_t)k * BS + c) : v[(size_t)k * BS + c]) : 0.0;
     }
     const double* Ab = A + (size_t)kb * BS * BS;
 #pragma unroll
@@ -124,9 +119,19 @@ __global__ void __launch_bounds__(256) block_row_kernel(RowSet rs, const int* __
     if (lane == rr) mine = acc[rr];
   const int r = r0 + lane;
   if (lane < R && r < BS) {
-    double base = x0 ? x0[(size_t)e * BS + r] : 0.0;
+    double base = x0 ? (COHERENT ? __ldcg(x0 + (size_t)e * BS + r) : x0[(size_t)e * BS + r]) : 0.0;
     y[(size_t)e * BS + r] = base + sign * mine;
   }
+}
+
+template <int BS, int MODE>
+__global__ void __launch_bounds__(256) block_row_kernel(RowSet rs, const int* __restrict__ rowptr,
+                                                        const int* __restrict__ colidx,
+                                                        const double* __restrict__ A, const double* v,
+                                                        const double* x0, double sign, double* y) {
+  const long long task = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (task >= (long long)rs.count() * BlockRowCfg<BS>::GROUPS) return;
+  block_row_task<BS, MODE, false>(rs, task, rowptr, colidx, A, v, x0, sign, y);
 }
 
 // launch over a row set: 8 warps per CTA
@@ -138,6 +143,179 @@ inline cudaError_t launch_block_rows(const RowSet& rs, const int* rowptr, const 
   unsigned blocks = (unsigned)((tasks + 7) / 8);
   block_row_kernel<BS, MODE><<<blocks, 256, 0, s>>>(rs, rowptr, colidx, A, v, x0, sign, y);
   return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------------------------
+// Block-ILU(0) apply in one cooperative launch, scheduled by data flow:
+//   forward   f_e = x_e - sum_{k<e} L_ek f_k                      (levels ascending)
+//   backward  y_e = inv(U_ee) f_e - sum_{k>e} (inv(U_ee) U_ek) y_k  (levels descending)
+// A task is (element, group of R rows). The tasks are ordered by level (the
+// element order `order` lists the elements by anti-diagonal) and dealt to the
+// warps round-robin; every warp runs its tasks in that order, all forward
+// tasks before any backward task. A task loads its matrix rows, then waits
+// only for the elements it reads: each element has a completion counter per
+// sweep that every group increments after writing its rows, and the sweep of
+// apply number `epoch` is complete for element k when its counter reaches
+// epoch * GROUPS (the counters grow across applies and are never reset).
+// Because every dependency is a task earlier in some warp's order and all
+// warps are resident (cooperative launch), the waits always end; each is
+// nevertheless bounded by ICX_FLOW_SPINS polls, after which the warp sets
+// *err and the launch winds down (every waiting warp polls *err).
+#ifndef ICX_FLOW_SPINS
+#define ICX_FLOW_SPINS (1u << 22)
+#endif
+
+struct IluFlowArgs {
+  int nx, ny, E;
+  const int* rowptr;
+  const int* order;     // [E] elements by ascending level
+  const double* LU;     // strictly lower blocks L, upper blocks inv(U_ee) U_ek
+  const double* Uinv;   // [E] inv(U_ee)
+  const double* x;
+  double* f;            // forward result
+  double* y;            // output
+  unsigned* cnt_f;      // [E] forward completion counters
+  unsigned* cnt_b;      // [E] backward completion counters
+  unsigned epoch;
+  int* err;
+};
+
+// lane 0 polls *c with acquire loads until it reaches target (wrap-safe);
+// false on timeout or error. The acquire orders the warp's later loads of the
+// producer's data after the observation (then __syncwarp for the other lanes).
+__device__ inline unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ inline bool flow_wait(const unsigned* c, unsigned target, int* err) {
+  int ok = 1;
+  if ((threadIdx.x & 31) == 0) {
+    unsigned spins = 0;
+    while ((int)(ld_acquire_u32(c) - target) < 0) {
+      if (*reinterpret_cast<volatile int*>(err)) { ok = 0; break; }
+      if (++spins > ICX_FLOW_SPINS) { atomicExch(err, 1); ok = 0; break; }
+    }
+  }
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  __syncwarp();
+  return ok != 0;
+}
+
+// the warp's stores happen before the increment (release at gpu scope,
+// cumulative over the lanes' stores ordered by __syncwarp)
+__device__ inline void flow_signal(unsigned* c) {
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(c) : "memory");
+}
+
+// rows per task of the data-flow apply: three blocks' rows stay in registers
+template <int BS>
+struct FlowCfg {
+  static constexpr int NS = (BS + 31) / 32;
+  static constexpr int R = NS >= 3 ? 4 : (BS >= 64 ? 8 : (BS >= 32 ? 4 : 2));
+  static constexpr int GROUPS = (BS + R - 1) / R;
+};
+
+template <int BS>
+__global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs a) {
+  using K = FlowCfg<BS>;
+  constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const long long ntask = (long long)a.E * GROUPS;
+  const unsigned target = a.epoch * (unsigned)GROUPS;
+  for (int sweep = 0; sweep < 2; ++sweep) {
+    const bool fwd = sweep == 0;
+    for (long long t = gw; t < ntask; t += nw) {
+      if (*reinterpret_cast<volatile int*>(a.err)) return;
+      const long long p = t / GROUPS;
+      const int g = (int)(t - p * GROUPS);
+      const int e = a.order[fwd ? p : a.E - 1 - p];
+      const int gi = e % a.nx, gj = e / a.nx;
+      const int r0 = g * R;
+      // neighbour blocks: forward reads the lower ones (e - nx, e - 1), backward the upper (e + 1, e + nx)
+      int nbk = 0, kbs[2], ks[2];
+      if (fwd) {
+        const int b0 = a.rowptr[e];
+        if (gj > 0) { kbs[nbk] = b0 + nbk; ks[nbk] = e - a.nx; ++nbk; }
+        if (gi > 0) { kbs[nbk] = b0 + nbk; ks[nbk] = e - 1; ++nbk; }
+      } else {
+        const int nup = (gi < a.nx - 1) + (gj < a.ny - 1);
+        const int b0 = a.rowptr[e + 1] - nup;
+        if (gi < a.nx - 1) { kbs[nbk] = b0 + nbk; ks[nbk] = e + 1; ++nbk; }
+        if (gj < a.ny - 1) { kbs[nbk] = b0 + nbk; ks[nbk] = e + a.nx; ++nbk; }
+      }
+      // matrix rows first: they do not depend on other tasks
+      double am[3][R][NS];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const double* Ab = nullptr;
+        if (b < 2 && b < nbk) Ab = a.LU + (size_t)kbs[b] * BS * BS;
+        else if (b == 2 && !fwd) Ab = a.Uinv + (size_t)e * BS * BS;
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+          for (int s = 0; s < NS; ++s) {
+            const int r = r0 + rr, c = lane + 32 * s;
+            am[b][rr][s] = (Ab && r < BS && c < BS) ? Ab[(size_t)r * BS + c] : 0.0;
+          }
+      }
+      double acc[R];
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) acc[rr] = 0.0;
+      const double* vsrc = fwd ? a.f : a.y;
+      unsigned* cnt = fwd ? a.cnt_f : a.cnt_b;
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        if (b < nbk) {
+          if (!flow_wait(cnt + ks[b], target, a.err)) return;
+          double xv[NS];
+#pragma unroll
+          for (int s = 0; s < NS; ++s) {
+            const int c = lane + 32 * s;
+            xv[s] = c < BS ? __ldcg(vsrc + (size_t)ks[b] * BS + c) : 0.0;
+          }
+#pragma unroll
+          for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+            for (int s = 0; s < NS; ++s) acc[rr] -= am[b][rr][s] * xv[s];
+        }
+      }
+      if (!fwd) {
+        // y_e = inv(U_ee) f_e + acc: f_e is complete once its forward counter is
+        if (!flow_wait(a.cnt_f + e, target, a.err)) return;
+        double xv[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const int c = lane + 32 * s;
+          xv[s] = c < BS ? __ldcg(a.f + (size_t)e * BS + c) : 0.0;
+        }
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+          for (int s = 0; s < NS; ++s) acc[rr] += am[2][rr][s] * xv[s];
+      }
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
+      }
+      double mine = 0.0;
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr)
+        if (lane == rr) mine = acc[rr];
+      const int r = r0 + lane;
+      if (lane < R && r < BS) {
+        if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + mine;
+        else a.y[(size_t)e * BS + r] = mine;
+      }
+      flow_signal(cnt + e);
+    }
+  }
 }
 
 #define ICX_BLOCK_SIZES(X) X(4) X(9) X(16) X(25) X(36) X(64) X(100)

@@ -452,6 +452,35 @@ cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU,
   return cudaErrorInvalidValue;
 }
 
+// the same apply in one cooperative launch scheduled by data flow
+// (ilu_apply_flow_kernel); `epoch` numbers the applies since the counters
+// were last zeroed (1, 2, ...)
+cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, int nx, int ny, const int* order, const double* LU,
+                              const double* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
+                              unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s) {
+  const int bs = dm.nb * dm.neq;
+  int dev = 0, nsm = 0, coop = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (e != cudaSuccess) return e;
+  if (!coop) return cudaErrorNotSupported;
+  IluFlowArgs args{nx, ny, dm.E, dm.bsr_rowptr, order, LU, Uinv, x, f, y, cnt_f, cnt_b, epoch, err};
+  void* params[] = {&args};
+#define ICX_ILUF2_CASE(B)                                                                         \
+  if (bs == B) {                                                                                  \
+    int per_sm = 0;                                                                               \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ilu_apply_flow_kernel<B>, 256, 0); \
+    if (e != cudaSuccess) return e;                                                               \
+    if (per_sm < 1) return cudaErrorNotSupported;                                                 \
+    int grid = nsm * (per_sm < 2 ? per_sm : 2);                                                   \
+    return cudaLaunchCooperativeKernel((const void*)ilu_apply_flow_kernel<B>, dim3(grid), dim3(256), params, 0, s); \
+  }
+  ICX_BLOCK_SIZES(ICX_ILUF2_CASE)
+#undef ICX_ILUF2_CASE
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace icx
 
 // ------------------------------------------------------------------ GMRES

@@ -28,7 +28,14 @@ cudaError_t la_ilu_factor(const DeviceMesh& dm, int nx, int ny, double* LU, doub
 // y = (LU)^-1 x; tmp: n doubles of scratch (x, y, tmp distinct)
 cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU, const double* Uinv, const double* x,
                          double* y, double* tmp, cudaStream_t s);
-
+// the same in one cooperative launch scheduled by data flow: order = the E
+// elements by ascending anti-diagonal, f = n doubles of scratch, cnt_f /
+// cnt_b = E device counters each (zero before the first apply, never reset
+// afterwards), epoch = 1 for the first apply after zeroing and +1 per apply;
+// *err (device) is set if a dependency wait timed out
+cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, int nx, int ny, const int* order, const double* LU,
+                              const double* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
+                              unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s);
 }  // namespace icx
 
 #include <functional>

@@ -31,10 +31,10 @@ struct icx_solver_work {
   double* ustep = nullptr;
   double* rwork = nullptr;
   double* pct = nullptr;    // scratch of the preconditioner apply
-  double* pin = nullptr;    // fixed input / output of the captured ILU apply
-  double* pout = nullptr;
-  cudaGraphExec_t ilu_exec = nullptr;  // the level launches of one ILU apply, captured once
-  cudaStream_t cap = nullptr;          // private stream for the capture
+  int* order = nullptr;     // elements by ascending anti-diagonal (ILU data-flow schedule)
+  unsigned* cnt = nullptr;  // 2 x E completion counters of the ILU apply
+  unsigned epoch = 0;       // ILU applies since the counters were zeroed
+  int* pc_err = nullptr;    // set by the ILU apply if a dependency wait timed out
   double* dh = nullptr;     // device scalars (dot results)
   int* flag = nullptr;
   icx::LinalgWork lw;
@@ -71,10 +71,25 @@ icx_status ensure_work(icx_ctx* c, int m) {
   CK(cudaMalloc((void**)&w->pc, vb));
   CK(cudaMalloc((void**)&w->uinv, sizeof(double) * (size_t)dm.E * bs * bs));
   CK(cudaMalloc((void**)&w->V, sizeof(double) * (size_t)(m + 1) * n));
-  double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork, &w->pct, &w->pin, &w->pout};
+  double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork, &w->pct};
   for (double** p : vecs) CK(cudaMalloc((void**)p, sizeof(double) * n));
   CK(cudaMalloc((void**)&w->dh, sizeof(double) * 2 * (m + 2)));
   CK(cudaMalloc((void**)&w->flag, sizeof(int)));
+  CK(cudaMalloc((void**)&w->pc_err, sizeof(int)));
+  CK(cudaMemset(w->pc_err, 0, sizeof(int)));
+  CK(cudaMalloc((void**)&w->cnt, sizeof(unsigned) * 2 * dm.E));
+  CK(cudaMemset(w->cnt, 0, sizeof(unsigned) * 2 * dm.E));
+  {
+    std::vector<int> order;
+    order.reserve(dm.E);
+    for (int l = 0; l < c->nx + c->ny - 1; ++l)
+      for (int i = 0; i < c->nx; ++i) {
+        int j = l - i;
+        if (j >= 0 && j < c->ny) order.push_back(i + c->nx * j);
+      }
+    CK(cudaMalloc((void**)&w->order, sizeof(int) * dm.E));
+    CK(cudaMemcpy(w->order, order.data(), sizeof(int) * dm.E, cudaMemcpyHostToDevice));
+  }
   CK(cudaMalloc((void**)&w->lw.partial, sizeof(double) * 64 * 296));
   return ICX_OK;
 }
@@ -93,29 +108,9 @@ cudaError_t apply_pc(icx_ctx* c, int kind, const double* x, double* z, cudaStrea
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
   if (kind == 1) return icx::la_block_diag_apply(dm.E, w->bs, w->pc, x, z, s);
-  if (kind == 2) {
-    // the 2 (nx + ny - 1) + 1 launches of one apply are replayed as a CUDA
-    // graph on fixed buffers: the level kernels are short, launch cost dominates
-    if (!w->ilu_exec) {
-      cudaError_t e;
-      if (!w->cap && (e = cudaStreamCreateWithFlags(&w->cap, cudaStreamNonBlocking)) != cudaSuccess) return e;
-      if ((e = cudaStreamBeginCapture(w->cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-      cudaError_t ea = icx::la_ilu_apply(dm, c->nx, c->ny, w->pc, w->uinv, w->pin, w->pout, w->pct, w->cap);
-      cudaGraph_t g = nullptr;
-      cudaError_t ec = cudaStreamEndCapture(w->cap, &g);
-      if (ea != cudaSuccess || ec != cudaSuccess) {
-        if (g) cudaGraphDestroy(g);
-        return ea != cudaSuccess ? ea : ec;
-      }
-      e = cudaGraphInstantiate(&w->ilu_exec, g, 0);
-      cudaGraphDestroy(g);
-      if (e != cudaSuccess) { w->ilu_exec = nullptr; return e; }
-    }
-    cudaError_t e = cudaMemcpyAsync(w->pin, x, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
-    if (e == cudaSuccess) e = cudaGraphLaunch(w->ilu_exec, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(z, w->pout, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
-    return e;
-  }
+  if (kind == 2)
+    return icx::la_ilu_apply_flow(dm, c->nx, c->ny, w->order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E,
+                                  ++w->epoch, w->pc_err, s);
   return cudaMemcpyAsync(z, x, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
 }
 
@@ -150,7 +145,18 @@ icx_status gmres(icx_ctx* c, int pc, int m, int maxit, double rtol, const double
   kb.lw = &w->lw;
   icx::LinOp A = [&](const double* xin, double* yout) { return icx::launch_bsr_spmv(dm, w->vals, xin, yout, s); };
   icx::LinOp M = [&](const double* xin, double* yout) { return apply_pc(c, pc, xin, yout, s); };
-  return icx::gmres_op(kb, A, pc ? &M : nullptr, maxit, rtol, b, x, iters, relres, s, &c->err);
+  icx_status st = icx::gmres_op(kb, A, pc ? &M : nullptr, maxit, rtol, b, x, iters, relres, s, &c->err);
+  int perr = 0;
+  CK(cudaMemcpyAsync(&perr, w->pc_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (perr) {
+    // the counters are inconsistent after an abandoned apply: start over
+    cudaMemsetAsync(w->pc_err, 0, sizeof(int), s);
+    cudaMemsetAsync(w->cnt, 0, sizeof(unsigned) * 2 * dm.E, s);
+    w->epoch = 0;
+    return set_err(c, ICX_ERR_CUDA, "block-ILU apply: a dependency wait timed out");
+  }
+  return st;
 }
 
 // wolfe_ls / zoom / corrigan_ls of the reference (nonlinear_solver_utils.hpp:83-191)
@@ -224,10 +230,8 @@ namespace icx {
 void free_solver_work(icx_ctx* c) {
   if (!c || !c->sw) return;
   icx_solver_work* w = c->sw;
-  if (w->ilu_exec) cudaGraphExecDestroy(w->ilu_exec);
-  if (w->cap) cudaStreamDestroy(w->cap);
-  void* ptrs[] = {w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du, w->ustep, w->rwork, w->pct, w->pin,
-                  w->pout, w->dh, w->flag, w->lw.partial};
+  void* ptrs[] = {w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du, w->ustep, w->rwork, w->pct, w->order,
+                  w->cnt, w->pc_err, w->dh, w->flag, w->lw.partial};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete w;
