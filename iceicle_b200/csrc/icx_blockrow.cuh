@@ -44,9 +44,9 @@ struct BlockRowCfg {
   static constexpr int GROUPS = (BS + R - 1) / R;             // warps per block row
 };
 
-template <int BS, int MODE, bool COHERENT>
+template <int BS, int MODE, bool COHERENT, class TA = double>
 __device__ inline void block_row_task(const RowSet& rs, long long task, const int* __restrict__ rowptr,
-                                      const int* __restrict__ colidx, const double* __restrict__ A,
+                                      const int* __restrict__ colidx, const TA* __restrict__ A,
                                       const double* v, const double* x0, double sign, double* y) {
   using K = BlockRowCfg<BS>;
   constexpr int NS = K::NS, R = K::R;
@@ -54,9 +54,9 @@ __device__ inline void block_row_task(const RowSet& rs, long long task, const in
   const int idx = (int)(task / K::GROUPS), g = (int)(task - (long long)idx * K::GROUPS);
   const int e = rs.row(idx);
   const int r0 = g * R;
-  double acc[R];
+  TA acc[R];
 #pragma unroll
-  for (int rr = 0; rr < R; ++rr) acc[rr] = 0.0;
+  for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
   // blocks of this row: on the structured grid the lower blocks are the
   // first (j > 0) + (i > 0) of the row (columns e - nx, e - 1) and the upper
   // blocks the last (i < nx - 1) + (j < ny - 1) (columns e + 1, e + nx)
@@ -80,7 +80,7 @@ __device__ inline void block_row_task(const RowSet& rs, long long task, const in
           if (MODE == BR_LOWER) { p0 = rowptr[ne]; p1 = p0 + (nj > 0) + (ni > 0); }
           else { p1 = rowptr[ne + 1]; p0 = p1 - (ni < rs.nx - 1) - (nj < rs.ny - 1); }
           const char* base = reinterpret_cast<const char*>(A + (size_t)p0 * BS * BS);
-          const size_t bytes = (size_t)(p1 - p0) * BS * BS * sizeof(double);
+          const size_t bytes = (size_t)(p1 - p0) * BS * BS * sizeof(TA);
           for (size_t off = (size_t)lane * 128; off < bytes; off += 32 * 128)
             asm volatile("prefetch.global.L2 [%0];" ::"l"(base + off));
         }
@@ -89,13 +89,13 @@ __device__ inline void block_row_task(const RowSet& rs, long long task, const in
   }
   for (int kb = kb0; kb < kb1; ++kb) {
     const int k = MODE == BR_DIAG ? e : colidx[kb];
-    double xv[NS];
+    TA xv[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       int c = lane + 32 * s;
-      xv[s] = c < BS ? (COHERENT ? __ldcg(v + (size_t)k * BS + c) : v[(size_t)k * BS + c]) : 0.0;
+      xv[s] = c < BS ? (TA)(COHERENT ? __ldcg(v + (size_t)k * BS + c) : v[(size_t)k * BS + c]) : TA(0);
     }
-    const double* Ab = A + (size_t)kb * BS * BS;
+    const TA* Ab = A + (size_t)kb * BS * BS;
 #pragma unroll
     for (int rr = 0; rr < R; ++rr) {
       int r = r0 + rr;
@@ -113,35 +113,35 @@ __device__ inline void block_row_task(const RowSet& rs, long long task, const in
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
   }
-  double mine = 0.0;
+  TA mine = TA(0);
 #pragma unroll
   for (int rr = 0; rr < R; ++rr)
     if (lane == rr) mine = acc[rr];
   const int r = r0 + lane;
   if (lane < R && r < BS) {
     double base = x0 ? (COHERENT ? __ldcg(x0 + (size_t)e * BS + r) : x0[(size_t)e * BS + r]) : 0.0;
-    y[(size_t)e * BS + r] = base + sign * mine;
+    y[(size_t)e * BS + r] = base + sign * (double)mine;
   }
 }
 
-template <int BS, int MODE>
+template <int BS, int MODE, class TA = double>
 __global__ void __launch_bounds__(256) block_row_kernel(RowSet rs, const int* __restrict__ rowptr,
                                                         const int* __restrict__ colidx,
-                                                        const double* __restrict__ A, const double* v,
+                                                        const TA* __restrict__ A, const double* v,
                                                         const double* x0, double sign, double* y) {
   const long long task = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (task >= (long long)rs.count() * BlockRowCfg<BS>::GROUPS) return;
-  block_row_task<BS, MODE, false>(rs, task, rowptr, colidx, A, v, x0, sign, y);
+  block_row_task<BS, MODE, false, TA>(rs, task, rowptr, colidx, A, v, x0, sign, y);
 }
 
 // launch over a row set: 8 warps per CTA
-template <int BS, int MODE>
-inline cudaError_t launch_block_rows(const RowSet& rs, const int* rowptr, const int* colidx, const double* A,
+template <int BS, int MODE, class TA = double>
+inline cudaError_t launch_block_rows(const RowSet& rs, const int* rowptr, const int* colidx, const TA* A,
                                      const double* v, const double* x0, double sign, double* y, cudaStream_t s) {
   long long tasks = (long long)rs.count() * BlockRowCfg<BS>::GROUPS;
   if (tasks <= 0) return cudaSuccess;
   unsigned blocks = (unsigned)((tasks + 7) / 8);
-  block_row_kernel<BS, MODE><<<blocks, 256, 0, s>>>(rs, rowptr, colidx, A, v, x0, sign, y);
+  block_row_kernel<BS, MODE, TA><<<blocks, 256, 0, s>>>(rs, rowptr, colidx, A, v, x0, sign, y);
   return cudaGetLastError();
 }
 
@@ -166,12 +166,13 @@ inline cudaError_t launch_block_rows(const RowSet& rs, const int* rowptr, const 
 #define ICX_FLOW_SPINS (1u << 22)
 #endif
 
+template <class TA>
 struct IluFlowArgs {
   int nx, ny, E;
   const int* rowptr;
   const int* order;     // [E] elements by ascending level
-  const double* LU;     // strictly lower blocks L, upper blocks inv(U_ee) U_ek
-  const double* Uinv;   // [E] inv(U_ee)
+  const TA* LU;         // strictly lower blocks L, upper blocks inv(U_ee) U_ek
+  const TA* Uinv;       // [E] inv(U_ee)
   const double* x;
   double* f;            // forward result
   double* y;            // output
@@ -219,8 +220,8 @@ struct FlowCfg {
   static constexpr int GROUPS = (BS + R - 1) / R;
 };
 
-template <int BS>
-__global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs a) {
+template <int BS, class TA>
+__global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) {
   using K = FlowCfg<BS>;
   constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
   const int lane = threadIdx.x & 31;
@@ -250,10 +251,10 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs a) {
         if (gj < a.ny - 1) { kbs[nbk] = b0 + nbk; ks[nbk] = e + a.nx; ++nbk; }
       }
       // matrix rows first: they do not depend on other tasks
-      double am[3][R][NS];
+      TA am[3][R][NS];
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
-        const double* Ab = nullptr;
+        const TA* Ab = nullptr;
         if (b < 2 && b < nbk) Ab = a.LU + (size_t)kbs[b] * BS * BS;
         else if (b == 2 && !fwd) Ab = a.Uinv + (size_t)e * BS * BS;
 #pragma unroll
@@ -261,23 +262,23 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs a) {
 #pragma unroll
           for (int s = 0; s < NS; ++s) {
             const int r = r0 + rr, c = lane + 32 * s;
-            am[b][rr][s] = (Ab && r < BS && c < BS) ? Ab[(size_t)r * BS + c] : 0.0;
+            am[b][rr][s] = (Ab && r < BS && c < BS) ? Ab[(size_t)r * BS + c] : TA(0);
           }
       }
-      double acc[R];
+      TA acc[R];
 #pragma unroll
-      for (int rr = 0; rr < R; ++rr) acc[rr] = 0.0;
+      for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
       const double* vsrc = fwd ? a.f : a.y;
       unsigned* cnt = fwd ? a.cnt_f : a.cnt_b;
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         if (b < nbk) {
           if (!flow_wait(cnt + ks[b], target, a.err)) return;
-          double xv[NS];
+          TA xv[NS];
 #pragma unroll
           for (int s = 0; s < NS; ++s) {
             const int c = lane + 32 * s;
-            xv[s] = c < BS ? __ldcg(vsrc + (size_t)ks[b] * BS + c) : 0.0;
+            xv[s] = c < BS ? (TA)__ldcg(vsrc + (size_t)ks[b] * BS + c) : TA(0);
           }
 #pragma unroll
           for (int rr = 0; rr < R; ++rr)
@@ -288,11 +289,11 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs a) {
       if (!fwd) {
         // y_e = inv(U_ee) f_e + acc: f_e is complete once its forward counter is
         if (!flow_wait(a.cnt_f + e, target, a.err)) return;
-        double xv[NS];
+        TA xv[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
           const int c = lane + 32 * s;
-          xv[s] = c < BS ? __ldcg(a.f + (size_t)e * BS + c) : 0.0;
+          xv[s] = c < BS ? (TA)__ldcg(a.f + (size_t)e * BS + c) : TA(0);
         }
 #pragma unroll
         for (int rr = 0; rr < R; ++rr)
@@ -304,14 +305,14 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs a) {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
       }
-      double mine = 0.0;
+      TA mine = TA(0);
 #pragma unroll
       for (int rr = 0; rr < R; ++rr)
         if (lane == rr) mine = acc[rr];
       const int r = r0 + lane;
       if (lane < R && r < BS) {
-        if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + mine;
-        else a.y[(size_t)e * BS + r] = mine;
+        if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
+        else a.y[(size_t)e * BS + r] = (double)mine;
       }
       flow_signal(cnt + e);
     }

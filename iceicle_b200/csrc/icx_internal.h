@@ -107,6 +107,9 @@ cudaError_t launch_jacobian_fd(const DeviceMesh& dm, const PhysParams& pp, const
                                double* vals, double eps, cudaStream_t s);
 cudaError_t launch_bsr_spmv(const DeviceMesh& dm, const double* vals, const double* x, double* y,
                             cudaStream_t s);
+// the same with FP32 values and FP32 accumulation (x, y FP64)
+cudaError_t launch_bsr_spmv_f32(const DeviceMesh& dm, const float* vals, const double* x, double* y,
+                                cudaStream_t s);
 // releases the Newton / GMRES buffers of a context (icx_solver.cu)
 void free_solver_work(icx_ctx* c);
 // releases the MDG-ICE state of a context (icx_mdg.cu)

@@ -399,4 +399,14 @@ cudaError_t launch_bsr_spmv(const DeviceMesh& dm, const double* vals, const doub
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_bsr_spmv_f32(const DeviceMesh& dm, const float* vals, const double* x, double* y, cudaStream_t s) {
+  int bs = dm.nb * dm.neq;
+  RowSet rs{0, 0, -1, dm.E};
+#define ICX_SPMV32_CASE(B) \
+  if (bs == B) return launch_block_rows<B, BR_ALL, float>(rs, dm.bsr_rowptr, dm.bsr_colidx, vals, x, nullptr, 1.0, y, s);
+  ICX_BLOCK_SIZES(ICX_SPMV32_CASE)
+#undef ICX_SPMV32_CASE
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace icx

@@ -455,9 +455,10 @@ cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU,
 // the same apply in one cooperative launch scheduled by data flow
 // (ilu_apply_flow_kernel); `epoch` numbers the applies since the counters
 // were last zeroed (1, 2, ...)
-cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, int nx, int ny, const int* order, const double* LU,
-                              const double* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
-                              unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s) {
+template <class TA>
+static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, int nx, int ny, const int* order, const TA* LU,
+                                   const TA* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
+                                   unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s) {
   const int bs = dm.nb * dm.neq;
   int dev = 0, nsm = 0, coop = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -465,20 +466,51 @@ cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, int nx, int ny, const int* o
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   if (e != cudaSuccess) return e;
   if (!coop) return cudaErrorNotSupported;
-  IluFlowArgs args{nx, ny, dm.E, dm.bsr_rowptr, order, LU, Uinv, x, f, y, cnt_f, cnt_b, epoch, err};
+  IluFlowArgs<TA> args{nx, ny, dm.E, dm.bsr_rowptr, order, LU, Uinv, x, f, y, cnt_f, cnt_b, epoch, err};
   void* params[] = {&args};
-#define ICX_ILUF2_CASE(B)                                                                         \
-  if (bs == B) {                                                                                  \
-    int per_sm = 0;                                                                               \
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ilu_apply_flow_kernel<B>, 256, 0); \
-    if (e != cudaSuccess) return e;                                                               \
-    if (per_sm < 1) return cudaErrorNotSupported;                                                 \
-    int grid = nsm * (per_sm < 2 ? per_sm : 2);                                                   \
-    return cudaLaunchCooperativeKernel((const void*)ilu_apply_flow_kernel<B>, dim3(grid), dim3(256), params, 0, s); \
+#define ICX_ILUF2_CASE(B)                                                                             \
+  if (bs == B) {                                                                                      \
+    int per_sm = 0;                                                                                   \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ilu_apply_flow_kernel<B, TA>, 256, 0); \
+    if (e != cudaSuccess) return e;                                                                   \
+    if (per_sm < 1) return cudaErrorNotSupported;                                                     \
+    int grid = nsm * (per_sm < 2 ? per_sm : 2);                                                       \
+    return cudaLaunchCooperativeKernel((const void*)ilu_apply_flow_kernel<B, TA>, dim3(grid), dim3(256), params, 0, s); \
   }
   ICX_BLOCK_SIZES(ICX_ILUF2_CASE)
 #undef ICX_ILUF2_CASE
   return cudaErrorInvalidValue;
+}
+
+cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, int nx, int ny, const int* order, const double* LU,
+                              const double* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
+                              unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s) {
+  return ilu_apply_flow_t<double>(dm, nx, ny, order, LU, Uinv, x, y, f, cnt_f, cnt_b, epoch, err, s);
+}
+
+cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, int nx, int ny, const int* order, const float* LU,
+                                  const float* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
+                                  unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s) {
+  return ilu_apply_flow_t<float>(dm, nx, ny, order, LU, Uinv, x, y, f, cnt_f, cnt_b, epoch, err, s);
+}
+
+cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s) {
+  RowSet rs{0, 0, -1, E};
+#define ICX_DIAG32_CASE(B) \
+  if (bs == B) return launch_block_rows<B, BR_DIAG, float>(rs, nullptr, nullptr, D, x, nullptr, 1.0, y, s);
+  ICX_BLOCK_SIZES(ICX_DIAG32_CASE)
+#undef ICX_DIAG32_CASE
+  return cudaErrorInvalidValue;
+}
+
+__global__ void d2f_kernel(long long n, const double* __restrict__ x, float* __restrict__ y) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}
+
+cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s) {
+  d2f_kernel<<<grid_for(n), 256, 0, s>>>(n, x, y);
+  return cudaGetLastError();
 }
 
 }  // namespace icx

@@ -36,6 +36,12 @@ cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU,
 cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, int nx, int ny, const int* order, const double* LU,
                               const double* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
                               unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s);
+// FP32 matrix variants (FP32 values, FP32 accumulation; vectors stay FP64)
+cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, int nx, int ny, const int* order, const float* LU,
+                                  const float* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
+                                  unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s);
+cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s);
+cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s);
 }  // namespace icx
 
 #include <functional>

@@ -31,6 +31,9 @@ struct icx_solver_work {
   double* ustep = nullptr;
   double* rwork = nullptr;
   double* pct = nullptr;    // scratch of the preconditioner apply
+  float* vals32 = nullptr;  // mixed precision: FP32 copies of the Jacobian and the preconditioner
+  float* pc32 = nullptr;
+  float* uinv32 = nullptr;
   int* order = nullptr;     // elements by ascending anti-diagonal (ILU data-flow schedule)
   unsigned* cnt = nullptr;  // 2 x E completion counters of the ILU apply
   unsigned epoch = 0;       // ILU applies since the counters were zeroed
@@ -103,35 +106,60 @@ double dev_norm(icx_ctx* c, const double* x, cudaStream_t s) {
   return std::sqrt(h);
 }
 
-// z = M^-1 x
-cudaError_t apply_pc(icx_ctx* c, int kind, const double* x, double* z, cudaStream_t s) {
+// FP32 copies of the Jacobian and preconditioner (mixed precision), allocated on first use
+icx_status ensure_mixed(icx_ctx* c) {
+  icx_solver_work* w = c->sw;
+  if (w->vals32) return ICX_OK;
+  size_t nv = (size_t)w->nnzb * w->bs * w->bs;
+  CK(cudaMalloc((void**)&w->vals32, sizeof(float) * nv));
+  CK(cudaMalloc((void**)&w->pc32, sizeof(float) * nv));
+  CK(cudaMalloc((void**)&w->uinv32, sizeof(float) * (size_t)c->dm.E * w->bs * w->bs));
+  return ICX_OK;
+}
+
+// z = M^-1 x (mixed: from the FP32 copies, FP32 accumulation)
+cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* z, cudaStream_t s) {
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
-  if (kind == 1) return icx::la_block_diag_apply(dm.E, w->bs, w->pc, x, z, s);
-  if (kind == 2)
+  if (kind == 1)
+    return mixed ? icx::la_block_diag_apply_f32(dm.E, w->bs, w->pc32, x, z, s)
+                 : icx::la_block_diag_apply(dm.E, w->bs, w->pc, x, z, s);
+  if (kind == 2) {
+    if (mixed)
+      return icx::la_ilu_apply_flow_f32(dm, c->nx, c->ny, w->order, w->pc32, w->uinv32, x, z, w->pct, w->cnt,
+                                        w->cnt + dm.E, ++w->epoch, w->pc_err, s);
     return icx::la_ilu_apply_flow(dm, c->nx, c->ny, w->order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E,
                                   ++w->epoch, w->pc_err, s);
+  }
   return cudaMemcpyAsync(z, x, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
 }
 
-// builds the preconditioner from w->vals
-cudaError_t build_pc(icx_ctx* c, int kind, cudaStream_t s) {
+// builds the preconditioner from w->vals (in FP64; mixed: then rounded to FP32,
+// together with the Jacobian itself)
+cudaError_t build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
-  cudaMemsetAsync(w->flag, 0, sizeof(int), s);
-  if (kind == 1) return icx::la_block_invert(dm.E, w->bs, w->vals, dm.bsr_diag, w->pc, w->flag, s);
+  const long long nv = (long long)dm.nnzb * w->bs * w->bs, nd = (long long)dm.E * w->bs * w->bs;
+  cudaError_t e = cudaMemsetAsync(w->flag, 0, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  if (kind == 1) e = icx::la_block_invert(dm.E, w->bs, w->vals, dm.bsr_diag, w->pc, w->flag, s);
   if (kind == 2) {
-    cudaError_t e = cudaMemcpyAsync(w->pc, w->vals, sizeof(double) * (size_t)dm.nnzb * w->bs * w->bs,
-                                    cudaMemcpyDeviceToDevice, s);
-    if (e != cudaSuccess) return e;
-    return icx::la_ilu_factor(dm, c->nx, c->ny, w->pc, w->uinv, w->flag, s);
+    e = cudaMemcpyAsync(w->pc, w->vals, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = icx::la_ilu_factor(dm, c->nx, c->ny, w->pc, w->uinv, w->flag, s);
   }
-  return cudaSuccess;
+  if (e != cudaSuccess || !mixed) return e;
+  e = icx::la_d2f(nv, w->vals, w->vals32, s);
+  if (e == cudaSuccess && kind == 1) e = icx::la_d2f(nd, w->pc, w->pc32, s);
+  if (e == cudaSuccess && kind == 2) e = icx::la_d2f(nv, w->pc, w->pc32, s);
+  if (e == cudaSuccess && kind == 2) e = icx::la_d2f(nd, w->uinv, w->uinv32, s);
+  return e;
 }
 
 // x = J^-1 b by GMRES(m) on the BSR Jacobian, right preconditioning
-icx_status gmres(icx_ctx* c, int pc, int m, int maxit, double rtol, const double* b, double* x, int* iters,
-                 double* relres, cudaStream_t s) {
+// (mixed: operator and preconditioner from the FP32 copies; the Krylov
+// vectors, Hessenberg and Givens rotations stay FP64)
+icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, const double* b, double* x,
+                 int* iters, double* relres, cudaStream_t s) {
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
   icx::KrylovBuffers kb;
@@ -143,8 +171,10 @@ icx_status gmres(icx_ctx* c, int pc, int m, int maxit, double rtol, const double
   kb.r = w->r;
   kb.dh = w->dh;
   kb.lw = &w->lw;
-  icx::LinOp A = [&](const double* xin, double* yout) { return icx::launch_bsr_spmv(dm, w->vals, xin, yout, s); };
-  icx::LinOp M = [&](const double* xin, double* yout) { return apply_pc(c, pc, xin, yout, s); };
+  icx::LinOp A = [&](const double* xin, double* yout) {
+    return mixed ? icx::launch_bsr_spmv_f32(dm, w->vals32, xin, yout, s) : icx::launch_bsr_spmv(dm, w->vals, xin, yout, s);
+  };
+  icx::LinOp M = [&](const double* xin, double* yout) { return apply_pc(c, pc, mixed, xin, yout, s); };
   icx_status st = icx::gmres_op(kb, A, pc ? &M : nullptr, maxit, rtol, b, x, iters, relres, s, &c->err);
   int perr = 0;
   CK(cudaMemcpyAsync(&perr, w->pc_err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -230,7 +260,7 @@ namespace icx {
 void free_solver_work(icx_ctx* c) {
   if (!c || !c->sw) return;
   icx_solver_work* w = c->sw;
-  void* ptrs[] = {w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du, w->ustep, w->rwork, w->pct, w->order,
+  void* ptrs[] = {w->vals32, w->pc32, w->uinv32, w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du, w->ustep, w->rwork, w->pct, w->order,
                   w->cnt, w->pc_err, w->dh, w->flag, w->lw.partial};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -277,6 +307,7 @@ icx_status icx_newton_default_options(icx_newton_options* o) {
   o->gmres_rtol = 1e-5;      // PETSc KSP default relative tolerance
   o->preconditioner = 2;     // block-ILU(0)
   o->verbosity = 0;
+  o->precision = 0;          // all FP64
   return ICX_OK;
 }
 
@@ -292,10 +323,10 @@ icx_status icx_gmres_solve(icx_ctx* c, const double* d_vals, const double* d_b, 
   icx_solver_work* w = c->sw;
   CK(cudaMemcpyAsync(w->vals, d_vals, sizeof(double) * (size_t)c->dm.nnzb * w->bs * w->bs, cudaMemcpyDeviceToDevice,
                      s));
-  CK(build_pc(c, preconditioner, s));
+  CK(build_pc(c, preconditioner, false, s));
   int it = 0;
   double rr = 0.0;
-  st = gmres(c, preconditioner, restart, maxit, rtol, d_b, d_x, &it, &rr, s);
+  st = gmres(c, preconditioner, false, restart, maxit, rtol, d_b, d_x, &it, &rr, s);
   if (iterations) *iterations = it;
   if (relres) *relres = rr;
   if (st != ICX_OK) return st;
@@ -307,8 +338,11 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   if (!d_u || !opt) return set_err(c, ICX_ERR_INVALID, "null argument");
   if (opt->gmres_restart < 1 || opt->gmres_restart > 60) return set_err(c, ICX_ERR_INVALID, "restart in 1..60");
   cudaStream_t s = 0;
+  if (opt->precision < 0 || opt->precision > 1) return set_err(c, ICX_ERR_INVALID, "precision must be 0 or 1");
   icx_status st = ensure_work(c, opt->gmres_restart);
   if (st != ICX_OK) return st;
+  const bool mixed = opt->precision == 1;
+  if (mixed && (st = ensure_mixed(c)) != ICX_OK) return st;
   icx_solver_work* w = c->sw;
   long long n = w->n;
   icx_newton_report local{};
@@ -326,11 +360,11 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   int k = 0;
   bool converged = rk <= tau;
   for (; k < opt->kmax && !converged; ++k) {
-    CK(build_pc(c, opt->preconditioner, s));
+    CK(build_pc(c, opt->preconditioner, mixed, s));
     int it = 0;
     double rr = 0.0;
-    st = gmres(c, opt->preconditioner, opt->gmres_restart, opt->gmres_max_it, opt->gmres_rtol, w->res, w->du, &it, &rr,
-               s);
+    st = gmres(c, opt->preconditioner, mixed, opt->gmres_restart, opt->gmres_max_it, opt->gmres_rtol, w->res, w->du,
+               &it, &rr, s);
     if (st != ICX_OK) return st;
     R->linear_iterations_total += it;
     double alpha = 1.0;

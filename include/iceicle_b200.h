@@ -208,6 +208,12 @@ typedef struct icx_newton_options {
   double gmres_rtol;       /* relative tolerance of the linear solve */
   int preconditioner;      /* 0 none, 1 block-Jacobi, 2 block-ILU0 */
   int verbosity;
+  /* 0: all FP64. 1: mixed - the linear solves read FP32 copies of the
+   * Jacobian (SpMV) and of the preconditioner (block inverses / ILU factors,
+   * formed in FP64 then rounded) with FP32 accumulation; the Krylov vectors,
+   * Hessenberg and Givens rotations, the Newton residual, its norm and the
+   * line search stay FP64, so the converged state is judged in FP64. */
+  int precision;
 } icx_newton_options;
 
 typedef struct icx_newton_report {

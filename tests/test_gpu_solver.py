@@ -144,3 +144,53 @@ def test_newton_ns_mms_with_linesearch_converges_to_oracle_state():
     assert rep.converged and rep.r_final <= 1e-11
     u = du.cpu().numpy()
     assert np.linalg.norm(u - u_or) <= 1e-10 * np.linalg.norm(u_or)
+
+
+@pytest.mark.parametrize("pc", [1, 2])
+def test_newton_mixed_precision_converges_to_fp64_oracle_state(pc):
+    """precision = 1: SpMV and preconditioner read FP32 copies (FP32
+    accumulation) inside FP64 Newton. The Newton residual is FP64, so the
+    converged state is the FP64 one: within 1e-10 (L2, relative) of the
+    oracle's, the same bar as the all-FP64 solve; only the inner iteration
+    counts may differ."""
+    spec = Spec(pde=NS, nx=4, ny=4, p=2, g=2, ip=True, source=True, perturb=0.05)
+    c = spec.coords()
+    ctx = spec.context(c)
+    from iceicle_b200 import workload_fn
+    import ctypes as C
+    from iceicle_b200.workloads import ns_mms_params
+    prm = ns_mms_params()
+    f = workload_fn("ns_mms_state")
+    xy = ctx.basis_node_coords().reshape(-1, 2)
+    out = (C.c_double * 4)()
+    pt = (C.c_double * 2)()
+    u0 = np.zeros((len(xy), 4))
+    for k in range(len(xy)):
+        pt[0], pt[1] = xy[k]
+        f(pt, out, C.cast(prm, C.c_void_p))
+        u0[k] = out[:]
+    u0 = (u0 * (1 + 1e-2 * np.random.default_rng(2).standard_normal(u0.shape))).reshape(-1)
+    u_or, _ = on.newton(spec.oracle_problem(), c, u0, tau_abs=1e-11, kmax=20, linesearch="wolfe")
+    du = torch.from_numpy(u0.copy()).cuda()
+    rep = ctx.newton_solve(du, _newton_opts(tau_abs=1e-11, kmax=30, linesearch=1, gmres_rtol=1e-5,
+                                            gmres_max_it=5000, preconditioner=pc, precision=1))
+    assert rep.converged and rep.r_final <= 1e-11
+    u = du.cpu().numpy()
+    assert np.linalg.norm(u - u_or) <= 1e-10 * np.linalg.norm(u_or)
+
+
+def test_newton_mixed_precision_burgers_ilu():
+    """mixed precision on the 32 x 32 viscous Burgers configuration: converges
+    in FP64 and lands on the all-FP64 solution. With zero Dirichlet data and
+    no source the steady state is u = 0, so the difference is measured
+    against the initial state's norm (1e-10); both solves run to
+    |r| <= 1e-12 so that their states are comparable"""
+    from iceicle_b200.workloads import burgers_config
+    wl = burgers_config()
+    u64 = torch.from_numpy(wl.u0.copy()).cuda()
+    r64 = wl.ctx.newton_solve(u64, _newton_opts(tau_abs=1e-12))
+    u32 = torch.from_numpy(wl.u0.copy()).cuda()
+    r32 = wl.ctx.newton_solve(u32, _newton_opts(tau_abs=1e-12, precision=1))
+    assert r64.converged and r32.converged and r32.r_final <= 1e-12
+    a, b = u64.cpu().numpy(), u32.cpu().numpy()
+    assert np.linalg.norm(a - b) <= 1e-10 * np.linalg.norm(wl.u0)
