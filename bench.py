@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-newton", action="store_true", help="skip the secondary Newton solve timings")
     return ap.parse_args()
 
 
@@ -150,17 +151,64 @@ class ClockSampler:
 
 
 def residual_work(wl):
-    """algorithmic bytes and FP64 flops of the volume+lift kernel per launch"""
+    """algorithmic bytes and FP64 flops per launch of the two residual kernels.
+    Bytes: every array the kernel must touch, once (u, res, geometry, source,
+    boundary data, the face fluxes passed between the kernels). Flops: the
+    sum-factorised contractions as implemented (2 per multiply-add) plus
+    160 per Navier-Stokes physical flux and 420 per numerical flux (Van Leer
+    splitting of both states + viscous flux), counted once per point."""
     L = wl.ctx.layout
     E, nb, neq, nqv, nqf, F = L.n_elem, L.nbasis, L.neq, L.nq_vol, L.nq_face, L.n_faces
     N = L.n_dof
-    # u read, res write, per-point geometry (J^-1, w det) + source, face fluxes
+    n1 = int(round(nb ** 0.5))
+    q1 = nqf
     bytes_vol = 8 * (2 * N + E * nqv * (5 + neq) + F * nqf * neq)
-    flux_flops = 160  # NS physical flux incl. viscous terms, counted once per point
-    ph1 = nqv * (6 * nb * neq + 8 * neq + flux_flops + 8 * neq + 2 * neq)
-    ph2 = nb * neq * (4 * nqv + 2 * nqv + 4 * 2 * nqf)
-    flops_vol = E * (ph1 + ph2)
-    return bytes_vol, flops_vol
+    bytes_face = 8 * (N + F * nqf * 12 + F * nqf * neq)
+    fma_vol = (n1 * q1 * neq * 2 * n1 + nqv * neq * 3 * n1 + nqv * neq * 10 + q1 * n1 * neq * 3 * q1
+               + 4 * n1 * nqf * neq + nb * neq * (2 * q1 + 4))
+    flops_vol = E * (2 * fma_vol + nqv * 160)
+    fma_face = F * (2 * neq * n1 * 2 * n1 + nqf * 2 * neq * (3 * n1 + 4))
+    flops_face = 2 * fma_face + F * nqf * 420
+    return dict(vol=(bytes_vol, flops_vol), face=(bytes_face, flops_face))
+
+
+def newton_bench(torch, dev):
+    """Newton solve time to |r| <= 1e-10 (FP64 residual), all-FP64 vs mixed
+    precision (FP32 Jacobian and preconditioner copies): 32 x 32 viscous
+    Burgers p=2 and the 128 x 128 Navier-Stokes manufactured solution p=3,
+    both with GMRES(30) + block-ILU(0) and the Wolfe line search. Timed with
+    CUDA events around the whole solve (it synchronises internally)."""
+    import iceicle_b200 as ib
+    from iceicle_b200.workloads import burgers_config, ns_mms_config
+    out = {}
+    for name, make in (("burgers_32x32_p2", lambda: burgers_config(device=dev.index)),
+                       ("ns_mms_128x128_p3", lambda: ns_mms_config(nx=NX, ny=NY, p=3, geo_order=2,
+                                                                    device=dev.index))):
+        wl = make()
+        rows = {}
+        states = {}
+        for label, prec in (("fp64", 0), ("mixed", 1)):
+            opt = ib.default_newton_options()
+            opt.precision = prec
+            u = torch.from_numpy(wl.u0).to(dev)
+            if name.startswith("burgers"):
+                wl.ctx.newton_solve(torch.from_numpy(wl.u0).to(dev), opt)  # warm-up (one-time setup)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record()
+            rep = wl.ctx.newton_solve(u, opt)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            states[label] = u.cpu().numpy()
+            rows[label] = {"s": e0.elapsed_time(e1) * 1e-3, "newton_its": rep.iterations,
+                           "gmres_its": rep.linear_iterations_total, "r_final": rep.r_final,
+                           "converged": bool(rep.converged)}
+        a, b = states["fp64"], states["mixed"]
+        rows["mixed_vs_fp64_state_l2"] = float(np.linalg.norm(a - b) / max(np.linalg.norm(wl.u0), 1e-300))
+        rows["speedup_mixed_vs_fp64"] = rows["fp64"]["s"] / rows["mixed"]["s"]
+        out[name] = rows
+        del wl
+    return out
 
 
 def run_ours(a):
@@ -226,7 +274,7 @@ def run_ours(a):
     if rank == 0:
         value = ws * N * a.steps / (ms * 1e-3)
         e2e = ws * N * a.steps / (ms_e2e * 1e-3)
-        bytes_vol, flops_vol = residual_work(wl)
+        work = residual_work(wl)
         tv = float(np.median(t_vol)) * 1e-3
         tf = float(np.median(t_face)) * 1e-3
         peaks = {}
@@ -235,7 +283,10 @@ def run_ours(a):
         except Exception:
             pass
         hbm = peaks.get("hbm_gbs", 6650.0)
-        achieved = bytes_vol / tv / 1e9
+        dom = "vol" if tv >= tf else "face"
+        td = tv if dom == "vol" else tf
+        bytes_d, flops_d = work[dom]
+        achieved = bytes_d / td / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -243,14 +294,19 @@ def run_ours(a):
             "config": dict(WORKLOAD, parallelism=f"replicas x{ws}" if ws > 1 else "single GPU"),
             "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N},
             "gpu_launches": 2 * a.steps,
-            "roofline": {"bound": "hbm", "kernel": "vol_lift_kernel<NS,p3,g2>", "achieved": achieved,
-                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "roofline": {"bound": "hbm",
+                         "kernel": "vol_lift_kernel<NS,p3,g2>" if dom == "vol" else "face_flux_kernel<NS,p3,g2,IP>",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
                          else "fallback 6650 GB/s",
-                         "traffic": None, "algorithmic_bytes": bytes_vol,
+                         "traffic": None, "algorithmic_bytes": bytes_d,
                          "kernel_ms": {"face_flux": tf * 1e3, "vol_lift": tv * 1e3},
-                         "fp64": {"flops_per_launch": flops_vol, "achieved_tflops": flops_vol / tv / 1e12,
-                                  "nominal_peak_tflops": 37.0}},
+                         "fp64": {"flops_per_launch": flops_d, "achieved_tflops": flops_d / td / 1e12,
+                                  "nominal_peak_tflops": 37.0},
+                         "other_kernel": {"name": "face_flux" if dom == "vol" else "vol_lift",
+                                          "algorithmic_bytes": work["face" if dom == "vol" else "vol"][0],
+                                          "achieved_gbs": work["face" if dom == "vol" else "vol"][0] /
+                                          (tf if dom == "vol" else tv) / 1e9}},
             "clocks": clocks,
         }
         if not a.no_cpu_baseline and ws == 1:
@@ -262,6 +318,8 @@ def run_ours(a):
                                         "sample": "3 full 128x128 p3 residuals, 1 thread (reference is serial)"}
             else:
                 line["cpu_baseline"] = None
+        if not a.no_newton and ws == 1:
+            line["newton"] = newton_bench(torch, dev)
         print(json.dumps(line))
     if ws > 1:
         dist.destroy_process_group()

@@ -161,8 +161,8 @@ cudaError_t upload(T** dptr, const std::vector<T>& h) {
 }
 
 void free_dev(DeviceMesh& dm) {
-  void* ptrs[] = {dm.coord, dm.el_nodes, dm.face_info, dm.el_face, dm.el_side, dm.vgeo, dm.fgeo,
-                  dm.tab_vol, dm.tab_face, dm.tab_1d, dm.tab_fphi, dm.tab_f1d, dm.tab_gvol, dm.tab_gface, dm.tab_gcen, dm.qw_face,
+  void* ptrs[] = {dm.coord, dm.el_nodes, dm.face_info, dm.el_face, dm.el_side, dm.el_fso, dm.vgeo, dm.fgeo,
+                  dm.tab_vol, dm.tab_face, dm.tab_1d, dm.tab_fphi, dm.tab_f1d, dm.tab_g1d, dm.tab_gvol, dm.tab_gface, dm.tab_gcen, dm.qw_face,
                   dm.bvals, dm.src, dm.face_flux, dm.face_grad, dm.bsr_rowptr, dm.bsr_colidx,
                   dm.bsr_diag, dm.face_blk};
   for (void* p : ptrs)
@@ -520,6 +520,16 @@ icx_status icx_setup(icx_ctx* c) {
       t1d[(size_t)(dm.nq1 + q) * (P + 1) + i] = dN[i];
     }
   }
+  // 1D factors of the geometry tabulation: tab_gvol[q][n][0] = dg[q0][n0] * bg[q1][n1], ...[1] = bg[q0][n0] * dg[q1][n1]
+  std::vector<double> tg1d((size_t)2 * dm.nq1 * (g + 1));
+  for (int q = 0; q < dm.nq1; ++q) {
+    double N[16], dN[16], d2N[16];
+    lg.eval(qx[q], N, dN, d2N);
+    for (int n = 0; n <= g; ++n) {
+      tg1d[(size_t)q * (g + 1) + n] = N[n];
+      tg1d[(size_t)(dm.nq1 + q) * (g + 1) + n] = dN[n];
+    }
+  }
   std::vector<double> tfphi((size_t)8 * dm.nqf * dm.nb);
   for (size_t k = 0; k < tfphi.size(); ++k) tfphi[k] = tface[k * 6];
   // face tabulation as 1D factors: the fixed coordinate of local face lf is
@@ -595,11 +605,21 @@ icx_status icx_setup(icx_ctx* c) {
   errs.push_back(upload(&dm.face_info, finfo));
   errs.push_back(upload(&dm.el_face, elf));
   errs.push_back(upload(&dm.el_side, els));
+  {
+    std::vector<int> fso((size_t)dm.E * 4, 0);
+    for (size_t k = 0; k < fso.size(); ++k) {
+      int f = elf[k], side = els[k];
+      int o = side ? c->faces[7 * f + 4] : 0;
+      fso[k] = f * 4 + side + 2 * o;
+    }
+    errs.push_back(upload(&dm.el_fso, fso));
+  }
   errs.push_back(upload(&dm.tab_vol, tvol));
   errs.push_back(upload(&dm.tab_face, tface));
   errs.push_back(upload(&dm.tab_1d, t1d));
   errs.push_back(upload(&dm.tab_fphi, tfphi));
   errs.push_back(upload(&dm.tab_f1d, tf1d));
+  errs.push_back(upload(&dm.tab_g1d, tg1d));
   errs.push_back(upload(&dm.tab_gvol, tgvol));
   errs.push_back(upload(&dm.tab_gface, tgface));
   errs.push_back(upload(&dm.tab_gcen, tgcen));

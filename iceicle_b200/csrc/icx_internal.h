@@ -43,6 +43,7 @@ struct DeviceMesh {
   int* face_info = nullptr;    // [F][8]: elemL, elemR, fnl, fnr, orient, bctype, bcflag, boundary index
   int* el_face = nullptr;      // [E][4] face index per local face
   int* el_side = nullptr;      // [E][4] 0: element is L of that face, 1: R
+  int* el_fso = nullptr;       // [E][4] face index * 4 + side + 2 * orientation (orientation of the R side, else 0)
   double* vgeo = nullptr;      // [5][E*nqv]: Jinv00, Jinv01, Jinv10, Jinv11, w*detJ (clamped)
   double* fgeo = nullptr;      // [NFACE_GEO][F*nqf]
   double* tab_vol = nullptr;   // [nqv][nb][3]: phi, dphi/dxi0, dphi/dxi1
@@ -54,6 +55,7 @@ struct DeviceMesh {
   // [4 faces][2 orient][nqf][p+1][3] along the varying direction
   double* tab_f1d = nullptr;
   double* tab_gvol = nullptr;  // [nqv][ng][2]: geometry basis gradients at volume points
+  double* tab_g1d = nullptr;   // [2][nq1][g+1]: 1D geometry Lagrange values, then derivatives, at the 1D Gauss points
   double* tab_gface = nullptr; // [4][2][nqf][ng][6]: geometry basis phi, d0, d1, h00, h01, h11 at face points
   double* tab_gcen = nullptr;  // [ng]: geometry basis at the element centroid
   double* qw_face = nullptr;   // [nqf]

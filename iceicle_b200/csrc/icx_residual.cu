@@ -188,6 +188,11 @@ __device__ inline void cp_async_f64(double* sdst, const double* gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
 __device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// two doubles; both addresses 16-byte aligned
+__device__ inline void cp_async_f64x2(double* sdst, const double* gsrc) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
 
 template <int PDE, int P, int G, bool DDG>
 __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flux_kernel(DeviceMesh dm, PhysParams pp, const double* __restrict__ u) {
@@ -202,19 +207,51 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flu
   const int f0 = blockIdx.x * FPB;
   const int nf = min(FPB, dm.F - f0);
   const int tid = threadIdx.x;
+  static_assert(FPB * NQF <= FC::THREADS, "one face point per thread");
+  // this thread's face point geometry, loaded before the staging barriers so
+  // that its latency overlaps them (a boundary point's right-side fields are
+  // zero in the table and replaced by the left side's below)
+  FacePt fp;
+  const bool has_pt = tid < nf * NQF;
+  if (has_pt) {
+    const int nfq = dm.F * NQF, k = f0 * NQF + tid;
+    const double* g = dm.fgeo;
+    fp.n[0] = g[FG_N0 * nfq + k];
+    fp.n[1] = g[FG_N1 * nfq + k];
+    fp.wsq = g[FG_WSQ * nfq + k];
+    fp.h = g[FG_H * nfq + k];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) fp.JiL[a] = g[(FG_JIL + a) * nfq + k];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) fp.JiR[a] = g[(FG_JIR + a) * nfq + k];
+    if (DDG) {
+#pragma unroll
+      for (int a = 0; a < 6; ++a) fp.HL[a] = g[(FG_HL + a) * nfq + k];
+#pragma unroll
+      for (int a = 0; a < 6; ++a) fp.HR[a] = g[(FG_HR + a) * nfq + k];
+    }
+  }
   for (int t = tid; t < FC::TAB; t += FC::THREADS) s_tab[t] = dm.tab_f1d[t];
   for (int t = tid; t < nf * 8; t += FC::THREADS) s_rec[t] = dm.face_info[(size_t)f0 * 8 + t];
-  __syncthreads();
-
-  // coefficient tiles of both sides (a boundary face repeats its left tile so
-  // that both sides are evaluated without branches; the copy is not used)
-  for (int t = tid; t < nf * 2 * BS; t += FC::THREADS) {
-    int fs = t / BS, k = t - fs * BS;
-    int e = s_rec[(fs >> 1) * 8 + (fs & 1)];
-    if (e < 0) e = s_rec[(fs >> 1) * 8];
-    int i = k / NEQ, eq = k - i * NEQ;
-    int i0 = i / N1, i1 = i - i0 * N1;
-    cp_async_f64(s_u + fs * FC::TILE + i0 * FC::RS + i1 * NEQ + eq, u + (size_t)e * BS + k);
+  // coefficient tiles of both sides into the padded [i0][i1][eq] layout; each
+  // thread reads the record of the tile it copies (a boundary face repeats its
+  // left tile so that both sides are evaluated without branches; the copy is
+  // not used)
+  constexpr int ROW = N1 * NEQ;  // contiguous doubles of one i0 row
+  for (int t = tid; t < nf * 2 * N1; t += FC::THREADS) {
+    const int fs = t / N1, i0 = t - fs * N1;
+    const int* rec = dm.face_info + (size_t)(f0 + (fs >> 1)) * 8;
+    int e = rec[fs & 1];
+    if (e < 0) e = rec[0];
+    const double* src = u + (size_t)e * BS + i0 * ROW;
+    double* dst = s_u + fs * FC::TILE + i0 * FC::RS;
+    if (ROW % 2 == 0 && FC::RS % 2 == 0 && BS % 2 == 0 && (reinterpret_cast<uintptr_t>(u) & 15) == 0) {
+#pragma unroll
+      for (int k = 0; k < ROW; k += 2) cp_async_f64x2(dst + k, src + k);
+    } else {
+#pragma unroll
+      for (int k = 0; k < ROW; ++k) cp_async_f64(dst + k, src + k);
+    }
   }
   cp_async_wait_all();
   __syncthreads();
@@ -244,32 +281,19 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flu
   }
   __syncthreads();
 
-  for (int t = tid; t < nf * NQF; t += FC::THREADS) {
+  if (has_pt) {
+    const int t = tid;
     int fl = t / NQF, q = t - fl * NQF;
     int f = f0 + fl;
     const int* rec = s_rec + fl * 8;
     bool interior = rec[1] >= 0;
     int bct = rec[5], bidx = rec[7];
-    FacePt fp;
-    {
-      int nfq = dm.F * NQF, k = f * NQF + q;
-      const double* g = dm.fgeo;
-      fp.n[0] = g[FG_N0 * nfq + k];
-      fp.n[1] = g[FG_N1 * nfq + k];
-      fp.wsq = g[FG_WSQ * nfq + k];
-      fp.h = g[FG_H * nfq + k];
+    if (!interior) {
 #pragma unroll
-      for (int a = 0; a < 4; ++a) fp.JiL[a] = g[(FG_JIL + a) * nfq + k];
+      for (int a = 0; a < 4; ++a) fp.JiR[a] = fp.JiL[a];
       if (DDG) {
 #pragma unroll
-        for (int a = 0; a < 6; ++a) fp.HL[a] = g[(FG_HL + a) * nfq + k];
-      }
-      const int kr = interior ? k : -1;
-#pragma unroll
-      for (int a = 0; a < 4; ++a) fp.JiR[a] = interior ? g[(FG_JIR + a) * nfq + kr] : fp.JiL[a];
-      if (DDG) {
-#pragma unroll
-        for (int a = 0; a < 6; ++a) fp.HR[a] = interior ? g[(FG_HR + a) * nfq + kr] : fp.HL[a];
+        for (int a = 0; a < 6; ++a) fp.HR[a] = fp.HL[a];
       }
     }
     double us[2][NEQ], gs[2][2 * NEQ], hs[2][DDG ? 4 * NEQ : 1];
@@ -361,8 +385,9 @@ struct VolCfg {
   static constexpr int T_EL = NEQ * 2 * N1 * Q1;    // T[eq][2][i0][q1], later AB[eq][2][q0][i1]
   static constexpr int GS_EL = NEQ * 3 * C::NQV;    // GS[eq][3][q]
   static constexpr int FF_EL = 4 * C::NQF * NEQ;    // signed face fluxes [lf][qf][eq]
-  static constexpr int L_EL = NEQ * 4 * N1;         // lifted face fluxes L[eq][lf][j]
-  static constexpr int PER_EL = U_EL + T_EL + GS_EL + FF_EL + L_EL;
+  static constexpr int L_EL = NEQ * 4 * N1;         // lifted face fluxes L[eq][lf][j] (reuses the c[] area)
+  static constexpr int UL_EL = U_EL > L_EL ? U_EL : L_EL;
+  static constexpr int PER_EL = UL_EL + T_EL + GS_EL + FF_EL;
   static constexpr size_t SMEM = sizeof(double) * (TAB1 + TABF + TABV + EPB * PER_EL) + sizeof(int) * EPB * 8;
 };
 
@@ -379,15 +404,28 @@ __global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh 
   double* s_db = s_b + Q1 * TS;                  // [Q1][TS]
   double* s_tf = s_b + V::TAB1;                  // [4][N1]
   double* s_tv = s_tf + V::TABF;                 // [4][2][NQF][N1]
-  double* s_u = s_tv + V::TABV;                  // [EPB][NEQ][N1][US]
-  double* s_T = s_u + EPB * V::U_EL;             // [EPB][NEQ][2][N1][Q1], then [EPB][NEQ][2][Q1][N1]
+  double* s_u = s_tv + V::TABV;                  // [EPB][NEQ][N1][US]; later L [EPB][NEQ][4][N1]
+  double* s_L = s_u;
+  double* s_T = s_u + EPB * V::UL_EL;            // [EPB][NEQ][2][N1][Q1], then [EPB][NEQ][2][Q1][N1]
   double* s_GS = s_T + EPB * V::T_EL;            // [EPB][NEQ][3][NQV]
   double* s_ff = s_GS + EPB * V::GS_EL;          // [EPB][4][NQF][NEQ]
-  double* s_L = s_ff + EPB * V::FF_EL;           // [EPB][NEQ][4][N1]
-  int* s_fi = (int*)(s_L + EPB * V::L_EL);       // [EPB][4]: face index; [EPB][4]: side + 2 * orientation
+  int* s_fi = (int*)(s_ff + EPB * V::FF_EL);     // [EPB][4]: face index; [EPB][4]: side + 2 * orientation
   const int e0 = blockIdx.x * EPB;
   const int ne = min(EPB, dm.E - e0);
   const int tid = threadIdx.x;
+  static_assert(EPB * NQV <= V::THREADS || EPB == 1, "one volume point per thread");
+  // this thread's volume point geometry (J^-1, w det J) and source, loaded
+  // before the staging barriers so that their latency overlaps them
+  double pg[5], psrc[NEQ];
+  {
+    const int nq = dm.E * NQV;
+    const size_t kq = (size_t)e0 * NQV + tid;
+    const bool has = tid < ne * NQV;
+#pragma unroll
+    for (int a = 0; a < 5; ++a) pg[a] = has ? dm.vgeo[(size_t)a * nq + kq] : 0.0;
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) psrc[eq] = (has && dm.src) ? dm.src[kq * NEQ + eq] : 0.0;
+  }
 
   // S0: 1D tables, coefficient tiles (contiguous in the reference layout,
   // read coalesced and stored as [eq][i0][i1]), face records
@@ -402,15 +440,25 @@ __global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh 
     int el = t / BS, r = t - el * BS;
     int i = r / NEQ, eq = r - i * NEQ;
     int i0 = i / N1, i1 = i - i0 * N1;
-    s_u[el * V::U_EL + (eq * N1 + i0) * US + i1] = u[(size_t)e0 * BS + t];
+    s_u[el * V::UL_EL + (eq * N1 + i0) * US + i1] = u[(size_t)e0 * BS + t];
   }
+  // face records and the stored fluxes of the element's faces: one packed
+  // record load, then the copy, issued by the same thread (completed before
+  // the lifting stage reads them)
   for (int t = tid; t < ne * 4; t += V::THREADS) {
-    int e = e0 + t / 4;
-    int fidx = dm.el_face[e * 4 + (t & 3)];
-    int side = dm.el_side[e * 4 + (t & 3)];
-    int o = side ? dm.face_info[8 * fidx + 4] : 0;
+    int fso = dm.el_fso[(size_t)e0 * 4 + t];
+    int fidx = fso >> 2;
     s_fi[t] = fidx;
-    s_fi[EPB * 4 + t] = side + 2 * o;
+    s_fi[EPB * 4 + t] = fso & 3;
+    const double* src = dm.face_flux + (size_t)fidx * NQF * NEQ;
+    double* dst = s_ff + t * NQF * NEQ;
+    if ((NQF * NEQ) % 2 == 0) {
+#pragma unroll
+      for (int k = 0; k < NQF * NEQ; k += 2) cp_async_f64x2(dst + k, src + k);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NQF * NEQ; ++k) cp_async_f64(dst + k, src + k);
+    }
   }
   __syncthreads();
 
@@ -425,7 +473,7 @@ __global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh 
     for (int i1 = 0; i1 < N1; ++i1) { b[i1] = s_b[q1 * TS + i1]; db[i1] = s_db[q1 * TS + i1]; }
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) {
-      const double* c = s_u + el * V::U_EL + (eq * N1 + i0) * US;
+      const double* c = s_u + el * V::UL_EL + (eq * N1 + i0) * US;
       double tv = 0.0, td = 0.0;
 #pragma unroll
       for (int i1 = 0; i1 < N1; ++i1) {
@@ -437,24 +485,16 @@ __global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh 
       T[N1 * Q1] = td;
     }
   }
-  for (int t = tid; t < ne * 4 * NQF * NEQ; t += V::THREADS) {
-    int elf = t / (NQF * NEQ), k = t - elf * (NQF * NEQ);
-    int fidx = s_fi[elf];
-    double v = dm.face_flux[(size_t)fidx * NQF * NEQ + k];
-    s_ff[t] = (s_fi[EPB * 4 + elf] & 1) ? -v : v;
-  }
+  cp_async_wait_all();
   __syncthreads();
 
   // S2: contract over i0 (thread = (el, q0, q1)), pull back, physical flux per point
-  const int nq = dm.E * NQV;
   const bool has_src = dm.src != nullptr;
   for (int t = tid; t < ne * NQV; t += V::THREADS) {
     int el = t / NQV, q = t - el * NQV;
     int q0 = q / Q1, q1 = q - q0 * Q1;
-    int e = e0 + el;
-    size_t kq = (size_t)e * NQV + q;
-    double Ji[4] = {dm.vgeo[0 * nq + kq], dm.vgeo[1 * nq + kq], dm.vgeo[2 * nq + kq], dm.vgeo[3 * nq + kq]};
-    double wd = dm.vgeo[4 * nq + kq];
+    const double* Ji = pg;  // t == tid: the point loaded at the start
+    const double wd = pg[4];
     double b[N1], db[N1];
 #pragma unroll
     for (int i0 = 0; i0 < N1; ++i0) { b[i0] = s_b[q0 * TS + i0]; db[i0] = s_db[q0 * TS + i0]; }
@@ -487,7 +527,7 @@ __global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh 
 #pragma unroll
       for (int kk = 0; kk < 2; ++kk)
         GS[(eq * 3 + kk) * NQV] = (F[eq * 2 + 0] * Ji[kk * 2 + 0] + F[eq * 2 + 1] * Ji[kk * 2 + 1]) * wd;
-      GS[(eq * 3 + 2) * NQV] = has_src ? -dm.src[kq * NEQ + eq] * wd : 0.0;
+      GS[(eq * 3 + 2) * NQV] = has_src ? -psrc[eq] * wd : 0.0;
     }
   }
   __syncthreads();
@@ -521,6 +561,7 @@ __global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh 
     int o = s_fi[EPB * 4 + el * 4 + lf] >> 1;
     const double* tv = s_tv + (lf * 2 + o) * NQF * N1 + j;
     const double* ff = s_ff + (el * 4 + lf) * NQF * NEQ;
+    const double sgn = (s_fi[EPB * 4 + el * 4 + lf] & 1) ? -1.0 : 1.0;  // the right element subtracts
     double acc[NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) acc[eq] = 0.0;
@@ -531,7 +572,7 @@ __global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh 
       for (int eq = 0; eq < NEQ; ++eq) acc[eq] += w * ff[qf * NEQ + eq];
     }
 #pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) s_L[el * V::L_EL + (eq * 4 + lf) * N1 + j] = acc[eq];
+    for (int eq = 0; eq < NEQ; ++eq) s_L[el * V::UL_EL + (eq * 4 + lf) * N1 + j] = sgn * acc[eq];
   }
   __syncthreads();
 
@@ -554,7 +595,7 @@ __global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh 
       double acc = 0.0;
 #pragma unroll
       for (int q0 = 0; q0 < Q1; ++q0) acc += db[q0] * AB[q0 * N1] + b[q0] * AB[Q1 * N1 + q0 * N1];
-      const double* L = s_L + el * V::L_EL + eq * 4 * N1;
+      const double* L = s_L + el * V::UL_EL + eq * 4 * N1;
 #pragma unroll
       for (int lf = 0; lf < 4; ++lf) acc += bf[lf] * L[lf * N1 + ((lf & 1) ? i0 : i1)];
       out[eq] = acc;
