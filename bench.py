@@ -172,6 +172,13 @@ def residual_work(wl):
     return dict(vol=(bytes_vol, flops_vol), face=(bytes_face, flops_face))
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the two
+# residual kernels on this workload, from one ncu capture of
+#   ncu --set full --clock-control none -k regex:"face_flux|vol_lift" -s 10 -c 2 \
+#       python bench.py --steps 2 --warmup 3 --no-newton --no-cpu-baseline
+NCU_DRAM_BYTES = {"vol": 43.45e6 + 0.50e6, "face": 25.70e6 + 0.01e6}
+
+
 def newton_bench(torch, dev):
     """Newton solve time to |r| <= 1e-10 (FP64 residual), all-FP64 vs mixed
     precision (FP32 Jacobian and preconditioner copies): 32 x 32 viscous
@@ -299,7 +306,7 @@ def run_ours(a):
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
                          else "fallback 6650 GB/s",
-                         "traffic": None, "algorithmic_bytes": bytes_d,
+                         "traffic": NCU_DRAM_BYTES[dom], "algorithmic_bytes": bytes_d,
                          "kernel_ms": {"face_flux": tf * 1e3, "vol_lift": tv * 1e3},
                          "fp64": {"flops_per_launch": flops_d, "achieved_tflops": flops_d / td / 1e12,
                                   "nominal_peak_tflops": 37.0},
