@@ -55,6 +55,16 @@ class NewtonOptions(C.Structure):
                 ("precision", C.c_int)]
 
 
+class ExplicitOptions(C.Structure):
+    _fields_ = [("scheme", C.c_int), ("timestep", C.c_int), ("dt", C.c_double), ("cfl", C.c_double),
+                ("termination", C.c_int), ("ntime", C.c_int), ("tfinal", C.c_double)]
+
+
+class ExplicitReport(C.Structure):
+    _fields_ = [("steps", C.c_int), ("time", C.c_double), ("dt_last", C.c_double), ("lambda_max", C.c_double),
+                ("singular_elements", C.c_int)]
+
+
 class NewtonReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("r0", C.c_double), ("r_final", C.c_double),
                 ("linear_iterations_total", C.c_int), ("residual_history", C.c_double * 64),
@@ -94,6 +104,9 @@ def lib():
             "icx_form_jacobian_fd": (C.c_int, [vp, vp, vp, vp, C.c_double, vp]),
             "icx_bsr_spmv": (C.c_int, [vp, vp, vp, vp, vp]),
             "icx_newton_default_options": (C.c_int, [C.POINTER(NewtonOptions)]),
+            "icx_explicit_default_options": (C.c_int, [C.POINTER(ExplicitOptions)]),
+            "icx_explicit_solve": (C.c_int, [vp, vp, C.POINTER(ExplicitOptions), C.POINTER(ExplicitReport)]),
+            "icx_mass_inverse_apply": (C.c_int, [vp, vp, vp, vp]),
             "icx_newton_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport)]),
             "icx_basis_node_coords": (C.c_int, [vp, vp]),
             "icx_form_residual_timed": (C.c_int, [vp, vp, vp, vp, dp, dp]),
@@ -322,6 +335,19 @@ class Context:
         self._check(lib().icx_form_jacobian_mdg_fd(self._h, _ptr(u), _ptr(res), _ptr(ic), _ptr(vals), eps,
                                                    _stream_ptr(stream)), "form_jacobian_mdg_fd")
 
+    def explicit_solve(self, u, options=None):
+        """advance u (device, FP64) in place with an explicit time stepper
+        (ExplicitEuler / RK3TVD / RK3SSP); returns the ExplicitReport"""
+        opt = options or default_explicit_options()
+        rep = ExplicitReport()
+        self._check(lib().icx_explicit_solve(self._h, _ptr(u), C.byref(opt), C.byref(rep)), "explicit_solve")
+        return rep
+
+    def mass_inverse_apply(self, r, out, stream=None):
+        """out = M^-1 r element by element (device arrays)"""
+        self._check(lib().icx_mass_inverse_apply(self._h, _ptr(r), _ptr(out), _stream_ptr(stream)),
+                    "mass_inverse_apply")
+
     def newton_solve(self, u, options=None):
         opt = options or default_newton_options()
         rep = NewtonReport()
@@ -329,6 +355,16 @@ class Context:
         if st not in (0, 5):
             self._check(st, "newton_solve")
         return rep
+
+
+def default_explicit_options(**kw):
+    opt = ExplicitOptions()
+    st = lib().icx_explicit_default_options(C.byref(opt))
+    if st != 0:
+        raise IcxError(st, "explicit_default_options")
+    for k, v in kw.items():
+        setattr(opt, k, v)
+    return opt
 
 
 def workload_fn(name):

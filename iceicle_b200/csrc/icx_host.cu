@@ -248,6 +248,11 @@ void lagrange_values(int pn, double x, double* N) {
   double dN[16], d2N[16];
   l.eval(x, N, dN, d2N);
 }
+void lagrange_values_derivs(int pn, double x, double* N, double* dN) {
+  Lagrange1D l(pn);
+  double d2N[16];
+  l.eval(x, N, dN, d2N);
+}
 void gauss_legendre_points(int n, double* x, double* w) { gauss_legendre(n, x, w); }
 }  // namespace icx
 
@@ -271,6 +276,7 @@ void icx_destroy(icx_ctx* c) {
   cudaSetDevice(c->device);
   icx::free_solver_work(c);
   icx::free_mdg(c);
+  icx::free_explicit(c);
   free_dev(c->dm);
   for (void* p : c->scratch)
     if (p) cudaFree(p);

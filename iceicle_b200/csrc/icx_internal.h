@@ -96,6 +96,7 @@ struct icx_ctx {
   std::vector<void*> scratch;
   struct icx_solver_work* sw = nullptr;  // Newton / GMRES buffers (icx_solver.cu)
   struct icx_mdg_state* mdg = nullptr;   // MDG-ICE selection and Jacobian pattern (icx_mdg.cu)
+  struct icx_explicit_work* ew = nullptr; // explicit time-stepping buffers (icx_explicit.cu)
 };
 
 namespace icx {
@@ -121,6 +122,10 @@ void free_mdg(icx_ctx* c);
 icx_status refresh_geometry(icx_ctx* c);
 // values of the pn+1 equispaced Lagrange polynomials of [-1, 1] at x (icx_host.cu)
 void lagrange_values(int pn, double x, double* N);
+// the same with first derivatives
+void lagrange_values_derivs(int pn, double x, double* N, double* dN);
+// releases the explicit time-stepping buffers of a context (icx_explicit.cu)
+void free_explicit(icx_ctx* c);
 // Gauss-Legendre points in the reference order (+x1, -x1, ..., 0) and weights (icx_host.cu)
 void gauss_legendre_points(int n, double* x, double* w);
 }  // namespace icx

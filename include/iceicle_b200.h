@@ -235,6 +235,37 @@ icx_status icx_gmres_solve(icx_ctx* ctx, const double* d_vals, const double* d_b
 icx_status icx_newton_default_options(icx_newton_options* opt);
 icx_status icx_newton_solve(icx_ctx* ctx, double* d_u, const icx_newton_options* opt, icx_newton_report* rep);
 
+/* ---- explicit time stepping (ExplicitEuler explicit_euler.hpp:30-181,
+ * RK3TVD tvd_rk3.hpp:30-277, RK3SSP ssp_rk3.hpp:30-241; FixedTimestep,
+ * CFLTimestep, TimestepTermination, TfinalTermination explicit_utils.hpp:60-180).
+ * The update is u += dt M^-1 R(u) per element with M the element mass matrix.
+ * RK3SSP evaluates all three stage residuals at the step's initial state, as
+ * the reference's stage function does. The CFL timestep (Burgers only) uses
+ * the running maximum of |a + b u / 2| over the volume points of every
+ * residual evaluation of the solve, as BurgersFlux::lambda_max does. */
+typedef struct icx_explicit_options {
+  int scheme;       /* 0 ExplicitEuler, 1 RK3TVD, 2 RK3SSP */
+  int timestep;     /* 0 FixedTimestep (dt), 1 CFLTimestep (cfl) */
+  double dt, cfl;
+  int termination;  /* 0 TimestepTermination (ntime), 1 TfinalTermination (tfinal) */
+  int ntime;
+  double tfinal;
+} icx_explicit_options;
+
+typedef struct icx_explicit_report {
+  int steps;              /* itime at the end */
+  double time;            /* time at the end */
+  double dt_last;
+  double lambda_max;      /* Burgers: the running maximum wave speed */
+  int singular_elements;  /* elements whose mass matrix had no inverse (RK3TVD: 1e-8 r there) */
+} icx_explicit_report;
+
+icx_status icx_explicit_default_options(icx_explicit_options* opt);
+/* d_u (device) advanced in place */
+icx_status icx_explicit_solve(icx_ctx* ctx, double* d_u, const icx_explicit_options* opt, icx_explicit_report* rep);
+/* d_out = M^-1 d_r element by element and equation by equation */
+icx_status icx_mass_inverse_apply(icx_ctx* ctx, const double* d_r, double* d_out, void* stream);
+
 /* ---- workload callbacks (icx_point_fn) ------------------------------------
  * icx_wl_constant: user -> double[1 + n] = {n, v_0 .. v_{n-1}}: out = v
  * icx_wl_sine_product: user -> double[1] = {amp}: out[0] = amp sin(2 pi x) sin(2 pi y)

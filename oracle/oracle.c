@@ -1299,3 +1299,196 @@ int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, 
   free(cw);
   return rc;
 }
+
+/* ------------------------------------------------------------------ */
+/* explicit time stepping                                              */
+/* ------------------------------------------------------------------ */
+/* element mass matrices M[e][i][j] = sum_q B_i B_j w det J (det J not clamped)
+ * (calculate_mass_matrix, finite_element.hpp:587-610) */
+int orc_mass_matrices(const orc_problem* pb, const double* coord, double* M) {
+  disc D;
+  if (disc_init(&D, pb, coord)) return -1;
+  int nb = D.nb, E = pb->nx * pb->ny;
+  for (int e = 0; e < E; ++e) {
+    double* Me = M + (size_t)e * nb * nb;
+    memset(Me, 0, sizeof(double) * nb * nb);
+    elgeo G;
+    el_geo(pb, coord, e, &G);
+    for (int q0 = 0; q0 < D.nq1; ++q0)
+      for (int q1 = 0; q1 < D.nq1; ++q1) {
+        double xi[2] = {D.qx[q0], D.qx[q1]};
+        double w = D.qw[q0] * D.qw[q1];
+        double J[2][2], B[MAXNB], dB[2 * MAXNB];
+        el_map(&D.lg, &G, xi, NULL, J, NULL);
+        double detJ = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        tp_eval(&D.lb, xi, B, dB, NULL);
+        for (int i = 0; i < nb; ++i)
+          for (int j = 0; j < nb; ++j) Me[i * nb + j] += B[i] * B[j] * w * detJ;
+      }
+  }
+  disc_free(&D);
+  return 0;
+}
+
+/* Burgers wave speed |a + b u / 2| at every volume point of u, maximum over
+ * the mesh (BurgersFlux::operator(), burgers.hpp:65-92, is evaluated there) */
+static double burgers_lambda_max(const disc* D, const double* u) {
+  const orc_problem* pb = D->pb;
+  int nb = D->nb, E = pb->nx * pb->ny;
+  double lam = 0.0;
+  for (int e = 0; e < E; ++e)
+    for (int q0 = 0; q0 < D->nq1; ++q0)
+      for (int q1 = 0; q1 < D->nq1; ++q1) {
+        double xi[2] = {D->qx[q0], D->qx[q1]};
+        double B[MAXNB], dB[2 * MAXNB];
+        tp_eval(&D->lb, xi, B, dB, NULL);
+        double uq = 0.0;
+        for (int i = 0; i < nb; ++i) uq += u[(size_t)e * nb + i] * B[i];
+        double s = 0.0;
+        for (int d = 0; d < 2; ++d) {
+          double l = pb->a[d] + 0.5 * pb->b[d] * uq;
+          s += l * l;
+        }
+        s = sqrt(s);
+        if (s > lam) lam = s;
+      }
+  return lam;
+}
+
+/* x = M^-1 b for one element and equation: Gaussian elimination with partial
+ * pivoting (decompose_lu / sub_lu); returns -1 on a zero pivot */
+static int dense_solve(int n, const double* M, const double* b, double* x) {
+  double A[MAXNB * MAXNB], y[MAXNB];
+  int perm[MAXNB];
+  memcpy(A, M, sizeof(double) * n * n);
+  for (int i = 0; i < n; ++i) perm[i] = i;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    for (int i = k + 1; i < n; ++i)
+      if (fabs(A[i * n + k]) > fabs(A[p * n + k])) p = i;
+    if (A[p * n + k] == 0.0) return -1;
+    if (p != k) {
+      for (int j = 0; j < n; ++j) { double t = A[k * n + j]; A[k * n + j] = A[p * n + j]; A[p * n + j] = t; }
+      int t = perm[k]; perm[k] = perm[p]; perm[p] = t;
+    }
+    for (int i = k + 1; i < n; ++i) {
+      A[i * n + k] /= A[k * n + k];
+      for (int j = k + 1; j < n; ++j) A[i * n + j] -= A[i * n + k] * A[k * n + j];
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    double s = b[perm[i]];
+    for (int j = 0; j < i; ++j) s -= A[i * n + j] * y[j];
+    y[i] = s;
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double s = y[i];
+    for (int j = i + 1; j < n; ++j) s -= A[i * n + j] * x[j];
+    x[i] = s / A[i * n + i];
+  }
+  return 0;
+}
+
+/* out = M^-1 r element by element and equation by equation; a singular mass
+ * matrix contributes 1e-8 r when `tvd_fallback` (tvd_rk3.hpp:185-199) */
+static int mass_solve(int E, int nb, int neq, const double* M, const double* r, double* out, int tvd_fallback) {
+  double b[MAXNB], x[MAXNB];
+  for (int e = 0; e < E; ++e)
+    for (int k = 0; k < neq; ++k) {
+      for (int i = 0; i < nb; ++i) b[i] = r[((size_t)e * nb + i) * neq + k];
+      if (dense_solve(nb, M + (size_t)e * nb * nb, b, x)) {
+        if (!tvd_fallback) return -1;
+        for (int i = 0; i < nb; ++i) x[i] = 1e-8 * b[i];
+      }
+      for (int i = 0; i < nb; ++i) out[((size_t)e * nb + i) * neq + k] = x[i];
+    }
+  return 0;
+}
+
+/* ExplicitEuler (explicit_euler.hpp:88-137), RK3TVD (tvd_rk3.hpp:108-233),
+ * RK3SSP (ssp_rk3.hpp:107-187) with FixedTimestep / CFLTimestep and
+ * TimestepTermination / TfinalTermination (explicit_utils.hpp:69-180).
+ * scheme 0 Euler, 1 TVD-RK3, 2 SSP-RK3; dt_kind 0 fixed (dt), 1 CFL (cfl);
+ * term_kind 0 ntime steps, 1 final time tfinal. As in the reference, every
+ * SSP-RK3 stage evaluates the residual at the step's initial state, and the
+ * CFL wave speed is the running maximum over every volume point of every
+ * residual evaluation since the solve began (Burgers). */
+int orc_explicit_solve(const orc_problem* pb, const double* coord, double* u, int scheme, int dt_kind, double dt_fixed,
+                       double cfl, int term_kind, int ntime, double tfinal, int* steps_out, double* time_out) {
+  disc D;
+  if (disc_init(&D, pb, coord)) return -1;
+  int nb = D.nb, neq = D.neq, E = pb->nx * pb->ny;
+  size_t n = (size_t)E * nb * neq;
+  double* M = (double*)malloc(sizeof(double) * (size_t)E * nb * nb);
+  double* res = (double*)malloc(sizeof(double) * n);
+  double* r1 = (double*)malloc(sizeof(double) * n);
+  double* r2 = (double*)malloc(sizeof(double) * n);
+  double* r3 = (double*)malloc(sizeof(double) * n);
+  double* us = (double*)malloc(sizeof(double) * n);
+  orc_mass_matrices(pb, coord, M);
+  /* CFL reference length: min over elements of det(J at the centroid)^(1/2) */
+  double reflen = 1e8;
+  for (int e = 0; e < E; ++e) {
+    elgeo G;
+    el_geo(pb, coord, e, &G);
+    double xi[2] = {0.0, 0.0}, J[2][2];
+    el_map(&D.lg, &G, xi, NULL, J, NULL);
+    double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    double r = pow(det, 1.0 / 2);
+    if (r < reflen) reflen = r;
+  }
+  double lam = 0.0;
+  int rc = 0;
+#define ORC_RES(U)                                                   \
+  do {                                                               \
+    if ((rc = orc_form_residual(pb, coord, (U), res))) goto done;    \
+    if (pb->pde == 0) {                                              \
+      double l_ = burgers_lambda_max(&D, (U));                       \
+      if (l_ > lam) lam = l_;                                        \
+    }                                                                \
+  } while (0)
+  ORC_RES(u); /* solve(): initial residual for the wave speeds */
+  int itime = 0;
+  double time = 0.0;
+  while (term_kind == 0 ? itime < ntime : time < tfinal) {
+    double dt = dt_fixed;
+    if (dt_kind == 1) {
+      /* dt_from_cfl (burgers.hpp:104-108) / (2 Pn_max + 1) */
+      dt = (reflen * cfl) / (pb->mu / reflen + lam) / (2 * pb->p + 1);
+    }
+    if (term_kind == 1) dt = fmin(dt, tfinal - time);
+    if (scheme == 0) {
+      ORC_RES(u);
+      if ((rc = mass_solve(E, nb, neq, M, res, r1, 0))) goto done;
+      for (size_t i = 0; i < n; ++i) u[i] += dt * r1[i];
+    } else if (scheme == 1) {
+      static const double alfa[3] = {0.0, 0.75, 1.0 / 3.0}, beta[3] = {1.0, 0.25, 2.0 / 3.0};
+      memcpy(us, u, sizeof(double) * n); /* u_old */
+      for (int st = 0; st < 3; ++st) {
+        ORC_RES(u);
+        if ((rc = mass_solve(E, nb, neq, M, res, r1, 1))) goto done;
+        for (size_t i = 0; i < n; ++i) u[i] = alfa[st] * us[i] + beta[st] * u[i];
+        for (size_t i = 0; i < n; ++i) u[i] += beta[st] * dt * r1[i];
+      }
+    } else {
+      /* stage residuals at the step's initial state */
+      double* rs[3] = {r1, r2, r3};
+      for (int st = 0; st < 3; ++st) {
+        ORC_RES(u);
+        if ((rc = mass_solve(E, nb, neq, M, res, rs[st], 0))) goto done;
+      }
+      for (size_t i = 0; i < n; ++i) u[i] += 1.0 / 6.0 * dt * r1[i];
+      for (size_t i = 0; i < n; ++i) u[i] += 1.0 / 6.0 * dt * r2[i];
+      for (size_t i = 0; i < n; ++i) u[i] += 2.0 / 3.0 * dt * r3[i];
+    }
+    ++itime;
+    time += dt;
+  }
+#undef ORC_RES
+done:
+  if (steps_out) *steps_out = itime;
+  if (time_out) *time_out = time;
+  free(M); free(res); free(r1); free(r2); free(r3); free(us);
+  disc_free(&D);
+  return rc;
+}

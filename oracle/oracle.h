@@ -78,6 +78,14 @@ int orc_mdg_residual(const orc_problem* pb, const double* coord, int ntr, const 
 int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
                            const double* u, const double* x, double* res_and_ic, double* J);
 
+/* element mass matrices [E][nb][nb] (finite_element.hpp:587-610) */
+int orc_mass_matrices(const orc_problem* pb, const double* coord, double* M);
+/* explicit time stepping: scheme 0 Euler, 1 TVD-RK3, 2 SSP-RK3; dt_kind 0
+ * fixed, 1 CFL; term_kind 0 ntime steps, 1 tfinal (explicit_*.hpp, ssp_rk3.hpp,
+ * tvd_rk3.hpp, explicit_utils.hpp); u updated in place */
+int orc_explicit_solve(const orc_problem* pb, const double* coord, double* u, int scheme, int dt_kind, double dt_fixed,
+                       double cfl, int term_kind, int ntime, double tfinal, int* steps_out, double* time_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,6 +22,9 @@
 #ifdef REF_WITH_JACOBIAN
 #include "iceicle/form_petsc_jacobian.hpp"
 #endif
+#include "iceicle/explicit_euler.hpp"
+#include "iceicle/ssp_rk3.hpp"
+#include "iceicle/tvd_rk3.hpp"
 #include <cstring>
 #include <functional>
 #include <memory>
@@ -340,5 +343,60 @@ int ref_form_jacobian_dense(const ref_problem* pb, const double* coord, const do
   });
 }
 #endif
+
+
+/// element mass matrices [E][nb][nb] (calculate_mass_matrix)
+int ref_mass_matrices(const ref_problem* pb, const double* coord, double* M) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    size_t k = 0;
+    for (const auto& el : fespace.elements) {
+      auto mass = calculate_mass_matrix(el);
+      const int nb = el.nbasis();
+      for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j) M[k++] = mass[i][j];
+    }
+    return 0;
+  });
+}
+
+/// the reference's explicit solvers run to completion from u (updated in
+/// place): scheme 0 ExplicitEuler, 1 RK3TVD, 2 RK3SSP; dt_kind 0 FixedTimestep,
+/// 1 CFLTimestep (Burgers only); term_kind 0 TimestepTermination (ntime),
+/// 1 TfinalTermination (tfinal)
+int ref_explicit_solve(const ref_problem* pb, const double* coord, double* u, int scheme, int dt_kind, double dt,
+                       double cfl, int term_kind, int ntime, double tfinal, int* steps_out, double* time_out) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) -> int {
+    fe_layout_right layout{fespace.dg_map, neq_c};
+    std::vector<T> ubuf(u, u + layout.size());
+    fespan uspan{ubuf.data(), layout};
+    auto with_stop = [&](auto timestep) -> int {
+      auto with_scheme = [&](auto stop) -> int {
+        auto go = [&](auto& solver) {
+          solver.vis_callback = [](auto&) {};
+          solver.solve(fespace, disc, uspan);
+          *steps_out = solver.itime;
+          *time_out = solver.time;
+        };
+        if (scheme == 0) { solvers::ExplicitEuler solver{fespace, disc, timestep, stop}; go(solver); }
+        else if (scheme == 1) { solvers::RK3TVD solver{fespace, disc, timestep, stop}; go(solver); }
+        else { solvers::RK3SSP solver{fespace, disc, timestep, stop}; go(solver); }
+        return 0;
+      };
+      if (term_kind == 0) return with_scheme(solvers::TimestepTermination<T, IDX>{ntime});
+      solvers::TfinalTermination<T, IDX> tf{};
+      tf.tfinal = tfinal;
+      return with_scheme(tf);
+    };
+    int rc = -2;
+    if (dt_kind == 0) rc = with_stop(solvers::FixedTimestep<T, IDX>{dt});
+    else if constexpr (requires { disc.dt_from_cfl(1.0, 1.0); }) {
+      solvers::CFLTimestep<T, IDX> c{};
+      c.cfl = cfl;
+      rc = with_stop(c);
+    }
+    if (rc == 0) std::memcpy(u, ubuf.data(), sizeof(T) * ubuf.size());
+    return rc;
+  });
+}
 
 }  // extern "C"

@@ -204,3 +204,24 @@ def mdg_jacobian_dense(lib, pb, coord, traces, u, x, hyper=True):
                                           _ptr(out), _ptr(J))
     assert rc == 0, rc
     return out, J
+
+
+def mass_matrices(lib, pb, coord):
+    """element mass matrices [E][nb][nb] (oracle or reference build)"""
+    E, nb, N = sizes(pb)
+    M = np.zeros((E, nb, nb))
+    rc = lib.fn("mass_matrices")(C.byref(pb), _ptr(coord), _ptr(M))
+    assert rc == 0, rc
+    return M
+
+
+def explicit_solve(lib, pb, coord, u, scheme, dt_kind=0, dt=0.0, cfl=0.3, term_kind=0, ntime=1, tfinal=0.0):
+    """run an explicit solver (0 Euler, 1 TVD-RK3, 2 SSP-RK3) from u; returns
+    (u, steps, time)"""
+    uu = np.ascontiguousarray(u, dtype=np.float64).copy()
+    steps, t = C.c_int(), C.c_double()
+    rc = lib.fn("explicit_solve")(C.byref(pb), _ptr(coord), _ptr(uu), int(scheme), int(dt_kind), C.c_double(dt),
+                                  C.c_double(cfl), int(term_kind), int(ntime), C.c_double(tfinal), C.byref(steps),
+                                  C.byref(t))
+    assert rc == 0, rc
+    return uu, steps.value, t.value
