@@ -105,6 +105,8 @@ def lib():
             "icx_bsr_spmv": (C.c_int, [vp, vp, vp, vp, vp]),
             "icx_newton_default_options": (C.c_int, [C.POINTER(NewtonOptions)]),
             "icx_explicit_default_options": (C.c_int, [C.POINTER(ExplicitOptions)]),
+            "icx_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int, C.POINTER(vp)]),
+            "icx_batch_offsets": (C.c_int, [vp, ip]),
             "icx_explicit_solve": (C.c_int, [vp, vp, C.POINTER(ExplicitOptions), C.POINTER(ExplicitReport)]),
             "icx_mass_inverse_apply": (C.c_int, [vp, vp, vp, vp]),
             "icx_newton_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport)]),
@@ -355,6 +357,26 @@ class Context:
         if st not in (0, 5):
             self._check(st, "newton_solve")
         return rep
+
+
+def batch(parts, device=0):
+    """one Context holding the set-up Contexts `parts` side by side (the batch
+    keeps them alive); `elem_offsets` gives each part's first element, then the
+    total"""
+    b = Context.__new__(Context)
+    b._h = C.c_void_p()
+    b._keep = list(parts)
+    arr = (C.c_void_p * len(parts))(*[p._h.value for p in parts])
+    st = lib().icx_batch_create(C.byref(b._h), device, len(parts), arr)
+    if st != 0:
+        raise IcxError(st, "batch_create")
+    off = (C.c_int * (len(parts) + 1))()
+    b._check(lib().icx_batch_offsets(b._h, off), "batch_offsets")
+    b.elem_offsets = list(off)
+    lay = LayoutInfo()
+    b._check(lib().icx_get_layout(b._h, C.byref(lay)), "get_layout")
+    b.layout = lay
+    return b
 
 
 def default_explicit_options(**kw):

@@ -14,27 +14,14 @@ namespace icx {
 
 enum BlockRowMode {
   BR_ALL = 0,    // every block of the row (SpMV)
-  BR_LOWER = 1,  // blocks with column < row (forward substitution)
-  BR_UPPER = 2,  // blocks with column > row (backward substitution)
   BR_DIAG = 3    // block-diagonal storage D[e] (one block per row, column = row)
 };
 
-// rows of one launch: either all block rows 0..nrows-1 (level < 0) or the
-// elements i + nx * j of the structured grid with i + j = level
+// the block rows 0..nrows-1 of one launch
 struct RowSet {
   int nx, ny, level, nrows;
-  __host__ __device__ int count() const {
-    if (level < 0) return nrows;
-    int i0 = level - (ny - 1) > 0 ? level - (ny - 1) : 0;
-    int i1 = level < nx - 1 ? level : nx - 1;
-    return i1 - i0 + 1;
-  }
-  __device__ int row(int idx) const {
-    if (level < 0) return idx;
-    int i0 = level - (ny - 1) > 0 ? level - (ny - 1) : 0;
-    int i = i0 + idx;
-    return i + nx * (level - i);
-  }
+  __host__ __device__ int count() const { return nrows; }
+  __device__ int row(int idx) const { return idx; }
 };
 
 template <int BS>
@@ -57,36 +44,9 @@ __device__ inline void block_row_task(const RowSet& rs, long long task, const in
   TA acc[R];
 #pragma unroll
   for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
-  // blocks of this row: on the structured grid the lower blocks are the
-  // first (j > 0) + (i > 0) of the row (columns e - nx, e - 1) and the upper
-  // blocks the last (i < nx - 1) + (j < ny - 1) (columns e + 1, e + nx)
   int kb0, kb1;
   if (MODE == BR_DIAG) { kb0 = e; kb1 = e + 1; }
-  else if (MODE == BR_ALL) { kb0 = rowptr[e]; kb1 = rowptr[e + 1]; }
-  else {
-    const int gi = e % rs.nx, gj = e / rs.nx;
-    if (MODE == BR_LOWER) { kb0 = rowptr[e]; kb1 = kb0 + (gj > 0) + (gi > 0); }
-    else { kb1 = rowptr[e + 1]; kb0 = kb1 - (gi < rs.nx - 1) - (gj < rs.ny - 1); }
-    // the next level's blocks of this kind into L2 while this level computes
-    if (g == 0 && rs.level >= 0) {
-      const int nl = rs.level + (MODE == BR_LOWER ? 1 : -1);
-      if (nl >= 0 && nl <= rs.nx + rs.ny - 2) {
-        RowSet nrs{rs.nx, rs.ny, nl, 0};
-        const int ncount = nrs.count();
-        for (int pi = idx; pi < ncount && pi <= idx + (idx == rs.count() - 1 ? ncount : 0); ++pi) {
-          const int ne = nrs.row(pi);
-          const int ni = ne % rs.nx, nj = ne / rs.nx;
-          int p0, p1;
-          if (MODE == BR_LOWER) { p0 = rowptr[ne]; p1 = p0 + (nj > 0) + (ni > 0); }
-          else { p1 = rowptr[ne + 1]; p0 = p1 - (ni < rs.nx - 1) - (nj < rs.ny - 1); }
-          const char* base = reinterpret_cast<const char*>(A + (size_t)p0 * BS * BS);
-          const size_t bytes = (size_t)(p1 - p0) * BS * BS * sizeof(TA);
-          for (size_t off = (size_t)lane * 128; off < bytes; off += 32 * 128)
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(base + off));
-        }
-      }
-    }
-  }
+  else { kb0 = rowptr[e]; kb1 = rowptr[e + 1]; }
   for (int kb = kb0; kb < kb1; ++kb) {
     const int k = MODE == BR_DIAG ? e : colidx[kb];
     TA xv[NS];
@@ -151,7 +111,9 @@ inline cudaError_t launch_block_rows(const RowSet& rs, const int* rowptr, const 
 //   forward   f_e = x_e - sum_{k<e} L_ek f_k                      (levels ascending)
 //   backward  y_e = inv(U_ee) f_e - sum_{k>e} (inv(U_ee) U_ek) y_k  (levels descending)
 // A task is (element, group of R rows). The tasks are ordered by level (the
-// element order `order` lists the elements by anti-diagonal) and dealt to the
+// element order `order` lists the elements by level, the anti-diagonal i + j
+// of the element in its grid; every strictly lower neighbour of an element is
+// on a lower level) and dealt to the
 // warps round-robin; every warp runs its tasks in that order, all forward
 // tasks before any backward task. A task loads its matrix rows, then waits
 // only for the elements it reads: each element has a completion counter per
@@ -168,8 +130,10 @@ inline cudaError_t launch_block_rows(const RowSet& rs, const int* rowptr, const 
 
 template <class TA>
 struct IluFlowArgs {
-  int nx, ny, E;
+  int E, nnzb;
   const int* rowptr;
+  const int* colidx;
+  const int* diag;      // position of each row's diagonal block
   const int* order;     // [E] elements by ascending level
   const TA* LU;         // strictly lower blocks L, upper blocks inv(U_ee) U_ek
   const TA* Uinv;       // [E] inv(U_ee)
@@ -236,19 +200,28 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
       const long long p = t / GROUPS;
       const int g = (int)(t - p * GROUPS);
       const int e = a.order[fwd ? p : a.E - 1 - p];
-      const int gi = e % a.nx, gj = e / a.nx;
       const int r0 = g * R;
-      // neighbour blocks: forward reads the lower ones (e - nx, e - 1), backward the upper (e + 1, e + nx)
+      // neighbour blocks: forward reads the strictly lower ones, backward the
+      // strictly upper ones (at most two of each on quadrilateral meshes).
+      // Indices are checked before use: a bad one sets *err = 2 and ends the
+      // launch (the values are uniform over the warp, so the whole warp leaves).
       int nbk = 0, kbs[2], ks[2];
-      if (fwd) {
-        const int b0 = a.rowptr[e];
-        if (gj > 0) { kbs[nbk] = b0 + nbk; ks[nbk] = e - a.nx; ++nbk; }
-        if (gi > 0) { kbs[nbk] = b0 + nbk; ks[nbk] = e - 1; ++nbk; }
-      } else {
-        const int nup = (gi < a.nx - 1) + (gj < a.ny - 1);
-        const int b0 = a.rowptr[e + 1] - nup;
-        if (gi < a.nx - 1) { kbs[nbk] = b0 + nbk; ks[nbk] = e + 1; ++nbk; }
-        if (gj < a.ny - 1) { kbs[nbk] = b0 + nbk; ks[nbk] = e + a.nx; ++nbk; }
+      bool bad = e < 0 || e >= a.E;
+      if (!bad) {
+        const int d = a.diag[e], rb = a.rowptr[e], re = a.rowptr[e + 1];
+        bad = d < rb || d >= re || rb < 0 || re > a.nnzb;
+        const int b0 = fwd ? rb : d + 1, b1 = fwd ? d : re;
+        bad = bad || (b1 - b0) > 2;
+        for (int kb = b0; !bad && kb < b1; ++kb) {
+          kbs[nbk] = kb;
+          ks[nbk] = a.colidx[kb];
+          bad = ks[nbk] < 0 || ks[nbk] >= a.E;
+          ++nbk;
+        }
+      }
+      if (bad) {
+        if (lane == 0) atomicExch(a.err, 2);
+        return;
       }
       // matrix rows first: they do not depend on other tasks
       TA am[3][R][NS];

@@ -21,6 +21,22 @@ struct Cfg {
   static constexpr int NG = (G + 1) * (G + 1);
 };
 
+// physical parameters of element e: in a batch of independent Burgers
+// problems each element carries its problem's coefficients (mu, a, b)
+template <int PDE>
+__device__ inline PhysParams elem_params(const DeviceMesh& dm, const PhysParams& pp, int e) {
+  PhysParams q = pp;
+  if (PDE == ICX_PDE_BURGERS && dm.el_par) {
+    const double* v = dm.el_par + 5 * (size_t)e;
+    q.mu = v[0];
+    q.a[0] = v[1];
+    q.a[1] = v[2];
+    q.b[0] = v[3];
+    q.b[1] = v[4];
+  }
+  return q;
+}
+
 // physical gradient (and Hessian) of one basis function from its reference
 // derivatives t = [phi, d0, d1, h00, h01, h11]:
 //   dx = Ji^T dxi,  Hx = Ji^T (Hxi - sum_m Hm_m dx_m) Ji   (finite_element.hpp:220-398)

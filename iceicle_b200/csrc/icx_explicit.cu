@@ -131,10 +131,12 @@ __global__ void burgers_lambda_kernel(DeviceMesh dm, PhysParams pp, const double
     const int e = (int)(t / dm.nqv), q = (int)(t - (long long)e * dm.nqv);
     double uq = 0.0;
     for (int i = 0; i < dm.nb; ++i) uq += u[(size_t)e * dm.nb + i] * dm.tab_vol[((size_t)q * dm.nb + i) * 3];
+    const double* pa = dm.el_par ? dm.el_par + 5 * (size_t)e + 1 : pp.a;
+    const double* pb = dm.el_par ? dm.el_par + 5 * (size_t)e + 3 : pp.b;
     double s = 0.0;
 #pragma unroll
     for (int d = 0; d < 2; ++d) {
-      double l = pp.a[d] + 0.5 * pp.b[d] * uq;
+      double l = pa[d] + 0.5 * pb[d] * uq;
       s += l * l;
     }
     best = fmax(best, sqrt(s));
@@ -256,6 +258,8 @@ icx_status icx_explicit_solve(icx_ctx* c, double* d_u, const icx_explicit_option
     return xerr(c, ICX_ERR_INVALID, "scheme 0..2, timestep 0..1, termination 0..1");
   if (o->timestep == 1 && c->phys.pde != ICX_PDE_BURGERS)
     return xerr(c, ICX_ERR_UNSUPPORTED, "the CFL timestep needs the flux's wave speed (Burgers)");
+  if (o->timestep == 1 && !c->parts.empty())
+    return xerr(c, ICX_ERR_UNSUPPORTED, "a batch has one timestep per problem: use a fixed timestep");
   const cudaStream_t s = 0;
   icx_status st = ensure_explicit(c);
   if (st != ICX_OK) return st;

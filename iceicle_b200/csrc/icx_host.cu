@@ -1,6 +1,7 @@
 // Host side of the C ABI: mesh construction in the reference's ordering,
 // finite element space tabulations, boundary/source data through the user's
 // callbacks, device table upload and the residual entry point.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -161,8 +162,8 @@ cudaError_t upload(T** dptr, const std::vector<T>& h) {
 }
 
 void free_dev(DeviceMesh& dm) {
-  void* ptrs[] = {dm.coord, dm.el_nodes, dm.face_info, dm.el_face, dm.el_side, dm.el_fso, dm.vgeo, dm.fgeo,
-                  dm.tab_vol, dm.tab_face, dm.tab_1d, dm.tab_fphi, dm.tab_f1d, dm.tab_g1d, dm.tab_gvol, dm.tab_gface, dm.tab_gcen, dm.qw_face,
+  void* ptrs[] = {dm.coord, dm.el_nodes, dm.face_info, dm.el_face, dm.el_side, dm.el_fso, dm.el_par, dm.vgeo, dm.fgeo,
+                  dm.tab_vol, dm.tab_face, dm.tab_1d, dm.tab_fphi, dm.tab_f1d, dm.tab_gvol, dm.tab_gface, dm.tab_gcen, dm.qw_face,
                   dm.bvals, dm.src, dm.face_flux, dm.face_grad, dm.bsr_rowptr, dm.bsr_colidx,
                   dm.bsr_diag, dm.face_blk};
   for (void* p : ptrs)
@@ -170,7 +171,7 @@ void free_dev(DeviceMesh& dm) {
   dm = DeviceMesh{};
 }
 
-int n_nodes(const icx_ctx* c) { return (c->nx * c->geo_order + 1) * (c->ny * c->geo_order + 1); }
+int n_nodes(const icx_ctx* c) { return (int)(c->coord.size() / 2); }
 
 // physical point of element e at reference xi via its geometry nodes
 void el_point(const icx_ctx* c, const Lagrange1D& lg, int e, const double xi[2], double x[2]) {
@@ -185,8 +186,47 @@ void el_point(const icx_ctx* c, const Lagrange1D& lg, int e, const double xi[2],
   }
 }
 
+// a batch takes its parts' boundary and source tables (already evaluated
+// through their callbacks) in the batch's face and element order
+icx_status batch_tables(icx_ctx* c) {
+  DeviceMesh& dm = c->dm;
+  const int neq = dm.neq;
+  cudaError_t e = cudaSuccess;
+  if (dm.bvals) { cudaFree(dm.bvals); dm.bvals = nullptr; }
+  if (dm.src) { cudaFree(dm.src); dm.src = nullptr; }
+  e = cudaMalloc((void**)&dm.bvals, sizeof(double) * (size_t)std::max(dm.Fb, 1) * dm.nqf * neq);
+  if (e != cudaSuccess) return cuda_fail(c, e, "allocate boundary data");
+  bool any_src = false;
+  for (icx_ctx* pc : c->parts) any_src = any_src || pc->dm.src != nullptr;
+  if (any_src) {
+    e = cudaMalloc((void**)&dm.src, sizeof(double) * (size_t)dm.E * dm.nqv * neq);
+    if (e == cudaSuccess) e = cudaMemset(dm.src, 0, sizeof(double) * (size_t)dm.E * dm.nqv * neq);
+    if (e != cudaSuccess) return cuda_fail(c, e, "allocate source");
+  }
+  size_t boff = 0, eoff = 0;
+  for (icx_ctx* pc : c->parts) {
+    const DeviceMesh& pm = pc->dm;
+    if (pm.Fb > 0 && (e = cudaMemcpy(dm.bvals + boff * dm.nqf * neq, pm.bvals,
+                                     sizeof(double) * (size_t)pm.Fb * dm.nqf * neq, cudaMemcpyDeviceToDevice)) !=
+                         cudaSuccess)
+      return cuda_fail(c, e, "copy boundary data");
+    if (pm.src && (e = cudaMemcpy(dm.src + eoff * dm.nqv * neq, pm.src, sizeof(double) * (size_t)pm.E * dm.nqv * neq,
+                                  cudaMemcpyDeviceToDevice)) != cudaSuccess)
+      return cuda_fail(c, e, "copy source");
+    boff += pm.Fb;
+    eoff += pm.E;
+  }
+  if ((e = upload(&dm.el_par, c->el_par)) != cudaSuccess) return cuda_fail(c, e, "upload element parameters");
+  if ((e = upload(&dm.coord, c->coord)) != cudaSuccess) return cuda_fail(c, e, "upload coordinates");
+  e = icx::launch_geometry(dm, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(c, e, "geometry kernels");
+  return ICX_OK;
+}
+
 // boundary data and source through the callbacks, then geometry kernels
 icx_status tabulate_and_geometry(icx_ctx* c) {
+  if (!c->parts.empty()) return batch_tables(c);
   DeviceMesh& dm = c->dm;
   Lagrange1D lg(c->geo_order);
   double qx[16], qw[16];
@@ -351,6 +391,9 @@ icx_status icx_mesh_uniform(icx_ctx* c, int ndim, const int* nelem, const double
       c->faces.insert(c->faces.end(), rb, rb + 7);
     }
   }
+  c->n_elem = c->nx * c->ny;
+  c->el_level.resize(c->n_elem);
+  for (int e = 0; e < c->n_elem; ++e) c->el_level[e] = e % c->nx + e / c->nx;
   c->has_mesh = true;
   c->ready = false;
   return ICX_OK;
@@ -459,7 +502,7 @@ icx_status icx_setup(icx_ctx* c) {
   int g = c->geo_order, P = c->p;
   dm.P = P;
   dm.G = g;
-  dm.E = c->nx * c->ny;
+  dm.E = c->n_elem;
   dm.F = (int)c->faces.size() / 7;
   dm.Fi = c->n_interior;
   dm.Fb = dm.F - dm.Fi;
@@ -526,16 +569,6 @@ icx_status icx_setup(icx_ctx* c) {
       t1d[(size_t)(dm.nq1 + q) * (P + 1) + i] = dN[i];
     }
   }
-  // 1D factors of the geometry tabulation: tab_gvol[q][n][0] = dg[q0][n0] * bg[q1][n1], ...[1] = bg[q0][n0] * dg[q1][n1]
-  std::vector<double> tg1d((size_t)2 * dm.nq1 * (g + 1));
-  for (int q = 0; q < dm.nq1; ++q) {
-    double N[16], dN[16], d2N[16];
-    lg.eval(qx[q], N, dN, d2N);
-    for (int n = 0; n <= g; ++n) {
-      tg1d[(size_t)q * (g + 1) + n] = N[n];
-      tg1d[(size_t)(dm.nq1 + q) * (g + 1) + n] = dN[n];
-    }
-  }
   std::vector<double> tfphi((size_t)8 * dm.nqf * dm.nb);
   for (size_t k = 0; k < tfphi.size(); ++k) tfphi[k] = tface[k * 6];
   // face tabulation as 1D factors: the fixed coordinate of local face lf is
@@ -581,13 +614,20 @@ icx_status icx_setup(icx_ctx* c) {
   // blocks couple to themselves and face neighbours)
   std::vector<int> rowptr(dm.E + 1, 0), colidx, diag(dm.E), fblk((size_t)dm.F * 4, -1);
   for (int e = 0; e < dm.E; ++e) {
-    int i = e % c->nx, j = e / c->nx;
-    if (j > 0) colidx.push_back(e - c->nx);
-    if (i > 0) colidx.push_back(e - 1);
-    diag[e] = (int)colidx.size();
-    colidx.push_back(e);
-    if (i < c->nx - 1) colidx.push_back(e + 1);
-    if (j < c->ny - 1) colidx.push_back(e + c->nx);
+    // the element and its face neighbours, ascending
+    int cols[5], nc = 0;
+    cols[nc++] = e;
+    for (int lf = 0; lf < 4; ++lf) {
+      int f = elf[(size_t)e * 4 + lf];
+      if (f < 0) continue;
+      int L = c->faces[7 * f], R = c->faces[7 * f + 1];
+      if (R >= 0) cols[nc++] = (L == e) ? R : L;
+    }
+    std::sort(cols, cols + nc);
+    for (int k = 0; k < nc; ++k) {
+      if (cols[k] == e) diag[e] = (int)colidx.size();
+      colidx.push_back(cols[k]);
+    }
     rowptr[e + 1] = (int)colidx.size();
   }
   auto find_blk = [&](int r, int col) {
@@ -625,7 +665,6 @@ icx_status icx_setup(icx_ctx* c) {
   errs.push_back(upload(&dm.tab_1d, t1d));
   errs.push_back(upload(&dm.tab_fphi, tfphi));
   errs.push_back(upload(&dm.tab_f1d, tf1d));
-  errs.push_back(upload(&dm.tab_g1d, tg1d));
   errs.push_back(upload(&dm.tab_gvol, tgvol));
   errs.push_back(upload(&dm.tab_gface, tgface));
   errs.push_back(upload(&dm.tab_gcen, tgcen));
@@ -695,7 +734,7 @@ icx_status icx_form_residual_timed(icx_ctx* c, const double* d_u, double* d_res,
 icx_status icx_basis_node_coords(const icx_ctx* c, double* xy) {
   if (!c || !xy || !c->has_mesh || !c->has_space) return ICX_ERR_INVALID;
   Lagrange1D lb(c->p), lg(c->geo_order);
-  int n = c->p + 1, E = c->nx * c->ny;
+  int n = c->p + 1, E = c->n_elem;
   for (int e = 0; e < E; ++e)
     for (int i0 = 0; i0 < n; ++i0)
       for (int i1 = 0; i1 < n; ++i1) {

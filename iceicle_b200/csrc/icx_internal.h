@@ -44,6 +44,7 @@ struct DeviceMesh {
   int* el_face = nullptr;      // [E][4] face index per local face
   int* el_side = nullptr;      // [E][4] 0: element is L of that face, 1: R
   int* el_fso = nullptr;       // [E][4] face index * 4 + side + 2 * orientation (orientation of the R side, else 0)
+  double* el_par = nullptr;    // batch of independent problems: [E][5] Burgers mu, a0, a1, b0, b1 per element (else null)
   double* vgeo = nullptr;      // [5][E*nqv]: Jinv00, Jinv01, Jinv10, Jinv11, w*detJ (clamped)
   double* fgeo = nullptr;      // [NFACE_GEO][F*nqf]
   double* tab_vol = nullptr;   // [nqv][nb][3]: phi, dphi/dxi0, dphi/dxi1
@@ -55,7 +56,6 @@ struct DeviceMesh {
   // [4 faces][2 orient][nqf][p+1][3] along the varying direction
   double* tab_f1d = nullptr;
   double* tab_gvol = nullptr;  // [nqv][ng][2]: geometry basis gradients at volume points
-  double* tab_g1d = nullptr;   // [2][nq1][g+1]: 1D geometry Lagrange values, then derivatives, at the 1D Gauss points
   double* tab_gface = nullptr; // [4][2][nqf][ng][6]: geometry basis phi, d0, d1, h00, h01, h11 at face points
   double* tab_gcen = nullptr;  // [ng]: geometry basis at the element centroid
   double* qw_face = nullptr;   // [nqf]
@@ -84,6 +84,12 @@ struct icx_ctx {
   std::vector<int> el_nodes;                  // [E][ng]
   std::vector<int> faces;                     // [F][7] reference face order
   int n_interior = 0;
+  int n_elem = 0;                             // elements (nx * ny for one grid)
+  std::vector<int> el_level;                  // [E] anti-diagonal index i + j of the element in its grid
+  // a batch of independent problems (icx_batch_create): the parts it was
+  // built from (not owned) and each element's Burgers coefficients (mu, a0, a1, b0, b1)
+  std::vector<icx_ctx*> parts;
+  std::vector<double> el_par;
   int p = 0;
   icx::PhysParams phys{};
   int conv_flux = 0;

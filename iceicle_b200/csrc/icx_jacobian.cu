@@ -69,8 +69,10 @@ __device__ inline void fp_load(const double* s, FacePt& p) {
 }
 
 template <int PDE, int P, int G, bool DDG>
-__global__ void __launch_bounds__(256) jac_elem_kernel(DeviceMesh dm, PhysParams pp, const double* __restrict__ u,
+__global__ void __launch_bounds__(256) jac_elem_kernel(DeviceMesh dm, PhysParams pp_in, const double* __restrict__ u,
                                                         double* __restrict__ vals, double eps) {
+  // every face of the element joins it to the same problem: one parameter set
+  const PhysParams pp = elem_params<PDE>(dm, pp_in, blockIdx.x);
   using J = JacCfg<PDE, P, G>;
   constexpr int NEQ = J::NEQ, NB = J::NB, BS = J::BS, NQF = J::NQF, NQV = J::NQV, NST = J::NST;
   extern __shared__ double sm[];

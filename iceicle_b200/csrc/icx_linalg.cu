@@ -44,8 +44,9 @@ __global__ void __launch_bounds__(256) block_invert_kernel(int nblk, const doubl
 //   A_ek <- A_ek inv(A_kk);  A_ej -= A_ek A_kj  for every (k, j), j > k, with (e, j) in the pattern;
 // then inv(A_ee) is stored for the next rows and the backward solve. On the
 // structured element grid row (i, j) depends only on (i-1, j) and (i, j-1),
-// so the rows of one anti-diagonal i + j = level are independent: one launch
-// per level, one CTA per row.
+// so the rows of one anti-diagonal i + j = level are independent (in a batch
+// of grids, the rows of that level in every grid): one launch per level, one
+// CTA per row.
 
 __device__ inline int find_block(const int* rowptr, const int* colidx, int r, int c) {
   for (int k = rowptr[r]; k < rowptr[r + 1]; ++k)
@@ -92,7 +93,8 @@ struct IluSmem {
 };
 
 template <int BS>
-__global__ void __launch_bounds__(256) ilu_level_kernel(int nx, int ny, int level, const int* __restrict__ rowptr,
+__global__ void __launch_bounds__(256) ilu_level_kernel(int E, int nnzb, const int* __restrict__ elems,
+                                                        const int* __restrict__ rowptr,
                                                         const int* __restrict__ colidx, double* __restrict__ LU,
                                                         double* __restrict__ Uinv, int* flag) {
   extern __shared__ double sh[];
@@ -102,12 +104,19 @@ __global__ void __launch_bounds__(256) ilu_level_kernel(int nx, int ny, int leve
   int* perm = reinterpret_cast<int*>(fcol + BS);
   int* colsrc = perm + BS;
   __shared__ int singular;
-  const int i0 = max(0, level - (ny - 1));
-  const int i = i0 + blockIdx.x, j = level - i;
-  if (i >= nx || j < 0) return;
-  const int e = i + nx * j;
+  const int e = elems[blockIdx.x];
+  // block and element indices are checked before use: a bad one sets
+  // *flag = 2 and the CTA leaves (the values are uniform over the CTA)
+  if (e < 0 || e >= E || rowptr[e] < 0 || rowptr[e + 1] > nnzb) {
+    if (threadIdx.x == 0) atomicExch(flag, 2);
+    return;
+  }
   for (int kl = rowptr[e]; kl < rowptr[e + 1]; ++kl) {
     const int k = colidx[kl];
+    if (k < 0 || k >= E) {
+      if (threadIdx.x == 0) atomicExch(flag, 2);
+      return;
+    }
     if (k >= e) break;  // columns ascend: the lower blocks come first
     double* Aek = LU + (size_t)kl * BS * BS;
     const double* Ui = Uinv + (size_t)k * BS * BS;
@@ -148,6 +157,10 @@ __global__ void __launch_bounds__(256) ilu_level_kernel(int nx, int ny, int leve
       if (jc <= k) continue;
       const int ej = find_block(rowptr, colidx, e, jc);
       if (ej < 0) continue;  // outside the pattern: dropped (level 0 fill)
+      if (kj >= nnzb || ej >= nnzb) {
+        if (threadIdx.x == 0) atomicExch(flag, 2);
+        return;
+      }
       const double* Akj = LU + (size_t)kj * BS * BS;
       double* Aej = LU + (size_t)ej * BS * BS;
       __syncthreads();
@@ -164,6 +177,10 @@ __global__ void __launch_bounds__(256) ilu_level_kernel(int nx, int ny, int leve
   }
   __syncthreads();
   const int kd = find_block(rowptr, colidx, e, e);
+  if (kd < 0) {
+    if (threadIdx.x == 0) atomicExch(flag, 2);
+    return;
+  }
   const double* Aee = LU + (size_t)kd * BS * BS;
   for (int t = threadIdx.x; t < BS * BS; t += blockDim.x) X[t] = Aee[t];
   __syncthreads();
@@ -323,22 +340,21 @@ cudaError_t la_block_diag_apply(int E, int bs, const double* D, const double* x,
   return cudaErrorInvalidValue;
 }
 
-static int level_rows(int nx, int ny, int level) {
-  int i0 = level - (ny - 1) > 0 ? level - (ny - 1) : 0;
-  int i1 = level < nx - 1 ? level : nx - 1;
-  return i1 - i0 + 1;
-}
 
-cudaError_t la_ilu_factor(const DeviceMesh& dm, int nx, int ny, double* LU, double* Uinv, int* flag, cudaStream_t s) {
+cudaError_t la_ilu_factor(const DeviceMesh& dm, const int* order, const std::vector<int>& lvl_off, double* LU,
+                          double* Uinv, int* flag, cudaStream_t s) {
   const int bs = dm.nb * dm.neq;
 #define ICX_ILUF_CASE(B)                                                                               \
   if (bs == B) {                                                                                       \
     cudaError_t e = smem_attr(ilu_level_kernel<B>, IluSmem<B>::BYTES);                                 \
     if (e == cudaSuccess) e = smem_attr(ilu_scale_upper_kernel<B>, IluSmem<B>::BYTES);                 \
     if (e != cudaSuccess) return e;                                                                    \
-    for (int level = 0; level < nx + ny - 1; ++level)                                                  \
-      ilu_level_kernel<B><<<level_rows(nx, ny, level), 256, IluSmem<B>::BYTES, s>>>(                   \
-          nx, ny, level, dm.bsr_rowptr, dm.bsr_colidx, LU, Uinv, flag);                                \
+    for (size_t l = 0; l + 1 < lvl_off.size(); ++l) {                                                  \
+      const int cnt = lvl_off[l + 1] - lvl_off[l];                                                     \
+      if (cnt > 0)                                                                                     \
+        ilu_level_kernel<B><<<cnt, 256, IluSmem<B>::BYTES, s>>>(dm.E, dm.nnzb, order + lvl_off[l],     \
+                                                                dm.bsr_rowptr, dm.bsr_colidx, LU, Uinv, flag); \
+    }                                                                                                  \
     ilu_scale_upper_kernel<B><<<dm.E, 256, IluSmem<B>::BYTES, s>>>(dm.E, dm.bsr_rowptr, dm.bsr_colidx, LU, Uinv); \
     return cudaGetLastError();                                                                         \
   }
@@ -347,31 +363,8 @@ cudaError_t la_ilu_factor(const DeviceMesh& dm, int nx, int ny, double* LU, doub
   return cudaErrorInvalidValue;
 }
 
-cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU, const double* Uinv, const double* x,
-                         double* y, double* tmp, cudaStream_t s) {
-  int bs = dm.nb * dm.neq;
-  const int nl = nx + ny - 1;
-  cudaError_t e = cudaSuccess;
-#define ICX_ILU_CASE(B)                                                                                      \
-  if (bs == B) {                                                                                             \
-    for (int l = 0; l < nl && e == cudaSuccess; ++l)                                                         \
-      e = launch_block_rows<B, BR_LOWER>(RowSet{nx, ny, l, 0}, dm.bsr_rowptr, dm.bsr_colidx, LU, y, x, -1.0, y, s); \
-    if (e == cudaSuccess)                                                                                    \
-      e = launch_block_rows<B, BR_DIAG>(RowSet{0, 0, -1, dm.E}, nullptr, nullptr, Uinv, y, nullptr, 1.0, tmp, s); \
-    for (int l = nl - 1; l >= 0 && e == cudaSuccess; --l)                                                    \
-      e = launch_block_rows<B, BR_UPPER>(RowSet{nx, ny, l, 0}, dm.bsr_rowptr, dm.bsr_colidx, LU, y, tmp, -1.0, y, s); \
-    return e;                                                                                                \
-  }
-  ICX_BLOCK_SIZES(ICX_ILU_CASE)
-#undef ICX_ILU_CASE
-  return cudaErrorInvalidValue;
-}
-
-// the same apply in one cooperative launch scheduled by data flow
-// (ilu_apply_flow_kernel); `epoch` numbers the applies since the counters
-// were last zeroed (1, 2, ...)
 template <class TA>
-static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, int nx, int ny, const int* order, const TA* LU,
+static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, const int* order, const TA* LU,
                                    const TA* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
                                    unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s) {
   const int bs = dm.nb * dm.neq;
@@ -381,7 +374,8 @@ static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, int nx, int ny, const 
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   if (e != cudaSuccess) return e;
   if (!coop) return cudaErrorNotSupported;
-  IluFlowArgs<TA> args{nx, ny, dm.E, dm.bsr_rowptr, order, LU, Uinv, x, f, y, cnt_f, cnt_b, epoch, err};
+  IluFlowArgs<TA> args{dm.E, dm.nnzb, dm.bsr_rowptr, dm.bsr_colidx, dm.bsr_diag, order, LU, Uinv, x, f, y, cnt_f,
+                       cnt_b, epoch, err};
   void* params[] = {&args};
 #define ICX_ILUF2_CASE(B)                                                                             \
   if (bs == B) {                                                                                      \
@@ -397,16 +391,16 @@ static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, int nx, int ny, const 
   return cudaErrorInvalidValue;
 }
 
-cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, int nx, int ny, const int* order, const double* LU,
-                              const double* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
-                              unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s) {
-  return ilu_apply_flow_t<double>(dm, nx, ny, order, LU, Uinv, x, y, f, cnt_f, cnt_b, epoch, err, s);
+cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, const int* order, const double* LU, const double* Uinv,
+                              const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b, unsigned epoch,
+                              int* err, cudaStream_t s) {
+  return ilu_apply_flow_t<double>(dm, order, LU, Uinv, x, y, f, cnt_f, cnt_b, epoch, err, s);
 }
 
-cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, int nx, int ny, const int* order, const float* LU,
-                                  const float* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
-                                  unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s) {
-  return ilu_apply_flow_t<float>(dm, nx, ny, order, LU, Uinv, x, y, f, cnt_f, cnt_b, epoch, err, s);
+cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, const int* order, const float* LU, const float* Uinv,
+                                  const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b,
+                                  unsigned epoch, int* err, cudaStream_t s) {
+  return ilu_apply_flow_t<float>(dm, order, LU, Uinv, x, y, f, cnt_f, cnt_b, epoch, err, s);
 }
 
 cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s) {
@@ -434,10 +428,11 @@ cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s) {
 namespace icx {
 
 double la_norm(LinalgWork& lw, long long n, const double* x, double* d_scratch, cudaStream_t s) {
-  la_mdot(lw, n, x, 0, 1, x, d_scratch, s);
+  // a failed launch or copy gives NaN: callers treat a non-finite norm as an error
+  if (la_mdot(lw, n, x, 0, 1, x, d_scratch, s) != cudaSuccess) return NAN;
   double h = 0.0;
-  cudaMemcpyAsync(&h, d_scratch, sizeof(double), cudaMemcpyDeviceToHost, s);
-  cudaStreamSynchronize(s);
+  if (cudaMemcpyAsync(&h, d_scratch, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return NAN;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return NAN;
   return std::sqrt(h);
 }
 

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "icx_internal.h"
 
 namespace icx {
@@ -22,24 +24,27 @@ cudaError_t la_xpay(long long n, const double* x, double a, const double* y, dou
 cudaError_t la_block_invert(int nblk, int bs, const double* src, const int* blk_index, double* dst, int* flag,
                             cudaStream_t s);
 cudaError_t la_block_diag_apply(int E, int bs, const double* D, const double* x, double* y, cudaStream_t s);
-// block-ILU(0) on the structured element grid: LU holds a copy of the BSR values on entry;
-// on exit its strictly lower blocks are L, its upper blocks inv(U_ee) U_ek and Uinv the inv(U_ee)
-cudaError_t la_ilu_factor(const DeviceMesh& dm, int nx, int ny, double* LU, double* Uinv, int* flag, cudaStream_t s);
-// y = (LU)^-1 x; tmp: n doubles of scratch (x, y, tmp distinct)
-cudaError_t la_ilu_apply(const DeviceMesh& dm, int nx, int ny, const double* LU, const double* Uinv, const double* x,
-                         double* y, double* tmp, cudaStream_t s);
-// the same in one cooperative launch scheduled by data flow: order = the E
-// elements by ascending anti-diagonal, f = n doubles of scratch, cnt_f /
-// cnt_b = E device counters each (zero before the first apply, never reset
-// afterwards), epoch = 1 for the first apply after zeroing and +1 per apply;
-// *err (device) is set if a dependency wait timed out
-cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, int nx, int ny, const int* order, const double* LU,
-                              const double* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
-                              unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s);
+// block-ILU(0) on the element block pattern in natural order, scheduled by
+// levels: order lists the elements by ascending level (the anti-diagonal
+// i + j of the element in its grid), lvl_off[l]..lvl_off[l+1] the elements of
+// level l; every strictly lower neighbour of an element lies on a lower level.
+// LU holds a copy of the BSR values on entry; on exit its strictly lower
+// blocks are L, its upper blocks inv(U_ee) U_ek and Uinv the inv(U_ee).
+// *flag: 1 if a diagonal block was singular, 2 if an index was out of range.
+cudaError_t la_ilu_factor(const DeviceMesh& dm, const int* order, const std::vector<int>& lvl_off, double* LU,
+                          double* Uinv, int* flag, cudaStream_t s);
+// y = (LU)^-1 x in one cooperative launch scheduled by data flow: f = n
+// doubles of scratch, cnt_f / cnt_b = E device counters each (zero before the
+// first apply, never reset afterwards), epoch = 1 for the first apply after
+// zeroing and +1 per apply; *err (device) is set to 1 if a dependency wait
+// timed out, 2 if an index was out of range
+cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, const int* order, const double* LU, const double* Uinv,
+                              const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b, unsigned epoch,
+                              int* err, cudaStream_t s);
 // FP32 matrix variants (FP32 values, FP32 accumulation; vectors stay FP64)
-cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, int nx, int ny, const int* order, const float* LU,
-                                  const float* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
-                                  unsigned* cnt_b, unsigned epoch, int* err, cudaStream_t s);
+cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, const int* order, const float* LU, const float* Uinv,
+                                  const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b,
+                                  unsigned epoch, int* err, cudaStream_t s);
 cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s);
 cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s);
 }  // namespace icx

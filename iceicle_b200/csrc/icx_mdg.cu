@@ -647,6 +647,7 @@ void apply_x(icx_ctx* c, const double* x) {
 extern "C" {
 
 icx_status icx_mdg_select(icx_ctx* c, int ntraces, const int* traces, int hyper_rectangle) {
+  if (c && !c->parts.empty()) return merr(c, ICX_ERR_UNSUPPORTED, "MDG-ICE on a batch of problems");
   if (!c || !c->ready) return merr(c, ICX_ERR_INVALID, "icx_setup has not completed");
   if (ntraces < 0 || (ntraces && !traces)) return merr(c, ICX_ERR_INVALID, "bad trace list");
   const icx::DeviceMesh& dm = c->dm;

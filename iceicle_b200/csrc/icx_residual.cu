@@ -338,7 +338,8 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flu
     }
     const double* bval = interior ? nullptr : dm.bvals + ((size_t)bidx * NQF + q) * NEQ;
     double out[NEQ], gq[4];
-    face_flux_states<PDE, DDG>(pp, fp, interior, bct, bval, us[0], gs[0], hs[0], us[1], gs[1], hs[1], out, gq);
+    const PhysParams pf = elem_params<PDE>(dm, pp, rec[0]);  // both sides belong to one problem
+    face_flux_states<PDE, DDG>(pf, fp, interior, bct, bval, us[0], gs[0], hs[0], us[1], gs[1], hs[1], out, gq);
     size_t k = (size_t)f * NQF + q;
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) dm.face_flux[k * NEQ + eq] = out[eq];
@@ -520,7 +521,7 @@ __global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh 
 #pragma unroll
       for (int d = 0; d < 2; ++d) gx[eq * 2 + d] = gxi[eq][0] * Ji[0 * 2 + d] + gxi[eq][1] * Ji[1 * 2 + d];
     double F[2 * NEQ];
-    Phys<PDE>::flux(pp, uq, gx, F);
+    Phys<PDE>::flux(elem_params<PDE>(dm, pp, e0 + el), uq, gx, F);
     double* GS = s_GS + el * V::GS_EL + q;
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) {

@@ -7,6 +7,7 @@
 // preconditioning on the BSR Jacobian. Every vector operation runs on the
 // device; the host holds only the (m+1) x m Hessenberg matrix and the scalar
 // line-search logic.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -34,7 +35,8 @@ struct icx_solver_work {
   float* vals32 = nullptr;  // mixed precision: FP32 copies of the Jacobian and the preconditioner
   float* pc32 = nullptr;
   float* uinv32 = nullptr;
-  int* order = nullptr;     // elements by ascending anti-diagonal (ILU data-flow schedule)
+  int* order = nullptr;     // elements by ascending level (ILU schedule)
+  std::vector<int> lvl_off; // level l: order[lvl_off[l] .. lvl_off[l+1])
   unsigned* cnt = nullptr;  // 2 x E completion counters of the ILU apply
   unsigned epoch = 0;       // ILU applies since the counters were zeroed
   int* pc_err = nullptr;    // set by the ILU apply if a dependency wait timed out
@@ -49,6 +51,13 @@ icx_status set_err(icx_ctx* c, icx_status st, const std::string& m) {
   if (c) c->err = m;
   return st;
 }
+
+// synchronises and reports any failure of the work enqueued so far, tagged
+#define SYNC_AT(tag)                                                                            \
+  do {                                                                                          \
+    cudaError_t _e = cudaStreamSynchronize(s);                                                  \
+    if (_e != cudaSuccess) return set_err(c, ICX_ERR_CUDA, std::string(tag) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
 
 #define CK(expr)                                                                       \
   do {                                                                                 \
@@ -83,13 +92,14 @@ icx_status ensure_work(icx_ctx* c, int m) {
   CK(cudaMalloc((void**)&w->cnt, sizeof(unsigned) * 2 * dm.E));
   CK(cudaMemset(w->cnt, 0, sizeof(unsigned) * 2 * dm.E));
   {
-    std::vector<int> order;
-    order.reserve(dm.E);
-    for (int l = 0; l < c->nx + c->ny - 1; ++l)
-      for (int i = 0; i < c->nx; ++i) {
-        int j = l - i;
-        if (j >= 0 && j < c->ny) order.push_back(i + c->nx * j);
-      }
+    // elements by ascending level (anti-diagonal of the element in its grid)
+    int nl = 0;
+    for (int v : c->el_level) nl = std::max(nl, v + 1);
+    w->lvl_off.assign(nl + 1, 0);
+    for (int v : c->el_level) ++w->lvl_off[v + 1];
+    for (int l = 0; l < nl; ++l) w->lvl_off[l + 1] += w->lvl_off[l];
+    std::vector<int> order(dm.E), fill(w->lvl_off.begin(), w->lvl_off.end() - 1);
+    for (int e = 0; e < dm.E; ++e) order[fill[c->el_level[e]]++] = e;
     CK(cudaMalloc((void**)&w->order, sizeof(int) * dm.E));
     CK(cudaMemcpy(w->order, order.data(), sizeof(int) * dm.E, cudaMemcpyHostToDevice));
   }
@@ -97,12 +107,17 @@ icx_status ensure_work(icx_ctx* c, int m) {
   return ICX_OK;
 }
 
+// NaN when a launch, copy or earlier kernel failed (the CUDA message is kept in c->err)
 double dev_norm(icx_ctx* c, const double* x, cudaStream_t s) {
   icx_solver_work* w = c->sw;
-  icx::la_mdot(w->lw, w->n, x, 0, 1, x, w->dh, s);
+  cudaError_t e = icx::la_mdot(w->lw, w->n, x, 0, 1, x, w->dh, s);
   double h = 0.0;
-  cudaMemcpyAsync(&h, w->dh, sizeof(double), cudaMemcpyDeviceToHost, s);
-  cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, w->dh, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    c->err = std::string("norm: ") + cudaGetErrorString(e);
+    return NAN;
+  }
   return std::sqrt(h);
 }
 
@@ -126,10 +141,10 @@ cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* 
                  : icx::la_block_diag_apply(dm.E, w->bs, w->pc, x, z, s);
   if (kind == 2) {
     if (mixed)
-      return icx::la_ilu_apply_flow_f32(dm, c->nx, c->ny, w->order, w->pc32, w->uinv32, x, z, w->pct, w->cnt,
-                                        w->cnt + dm.E, ++w->epoch, w->pc_err, s);
-    return icx::la_ilu_apply_flow(dm, c->nx, c->ny, w->order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E,
-                                  ++w->epoch, w->pc_err, s);
+      return icx::la_ilu_apply_flow_f32(dm, w->order, w->pc32, w->uinv32, x, z, w->pct, w->cnt, w->cnt + dm.E,
+                                        ++w->epoch, w->pc_err, s);
+    return icx::la_ilu_apply_flow(dm, w->order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E, ++w->epoch,
+                                  w->pc_err, s);
   }
   return cudaMemcpyAsync(z, x, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
 }
@@ -145,7 +160,7 @@ cudaError_t build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
   if (kind == 1) e = icx::la_block_invert(dm.E, w->bs, w->vals, dm.bsr_diag, w->pc, w->flag, s);
   if (kind == 2) {
     e = cudaMemcpyAsync(w->pc, w->vals, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s);
-    if (e == cudaSuccess) e = icx::la_ilu_factor(dm, c->nx, c->ny, w->pc, w->uinv, w->flag, s);
+    if (e == cudaSuccess) e = icx::la_ilu_factor(dm, w->order, w->lvl_off, w->pc, w->uinv, w->flag, s);
   }
   if (e != cudaSuccess || !mixed) return e;
   e = icx::la_d2f(nv, w->vals, w->vals32, s);
@@ -176,6 +191,12 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
   };
   icx::LinOp M = [&](const double* xin, double* yout) { return apply_pc(c, pc, mixed, xin, yout, s); };
   icx_status st = icx::gmres_op(kb, A, pc ? &M : nullptr, maxit, rtol, b, x, iters, relres, s, &c->err);
+  if (st != ICX_OK) {
+    // a non-finite value may come from a failed kernel: report that first
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_err(c, ICX_ERR_CUDA, std::string("linear solve: ") + cudaGetErrorString(e));
+    return st;  // c->err holds the failing call
+  }
   int perr = 0;
   CK(cudaMemcpyAsync(&perr, w->pc_err, sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -184,7 +205,8 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
     cudaMemsetAsync(w->pc_err, 0, sizeof(int), s);
     cudaMemsetAsync(w->cnt, 0, sizeof(unsigned) * 2 * dm.E, s);
     w->epoch = 0;
-    return set_err(c, ICX_ERR_CUDA, "block-ILU apply: a dependency wait timed out");
+    return set_err(c, ICX_ERR_CUDA, perr == 2 ? "block-ILU apply: block index out of range"
+                                              : "block-ILU apply: a dependency wait timed out");
   }
   return st;
 }
@@ -354,13 +376,22 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   double r0 = dev_norm(c, w->res, s);
   R->r0 = r0;
   R->residual_history[0] = r0;
-  if (!std::isfinite(r0)) return set_err(c, ICX_ERR_NONFINITE, "non-finite initial residual");
+  if (!std::isfinite(r0)) {
+    SYNC_AT("initial residual");
+    return set_err(c, ICX_ERR_NONFINITE, "non-finite initial residual");
+  }
   double tau = opt->tau_abs + opt->tau_rel * r0;
   double rk = r0;
   int k = 0;
   bool converged = rk <= tau;
   for (; k < opt->kmax && !converged; ++k) {
     CK(build_pc(c, opt->preconditioner, mixed, s));
+    {
+      int fl = 0;
+      CK(cudaMemcpyAsync(&fl, w->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+      SYNC_AT("preconditioner");
+      if (fl == 2) return set_err(c, ICX_ERR_CUDA, "block-ILU factorization: block index out of range");
+    }
     int it = 0;
     double rr = 0.0;
     st = gmres(c, opt->preconditioner, mixed, opt->gmres_restart, opt->gmres_max_it, opt->gmres_rtol, w->res, w->du,
@@ -381,6 +412,7 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
       else
         alpha = corrigan_ls(phi, opt->ls_alpha_max, opt->ls_alpha_initial, opt->ls_max_it, opt->ls_alpha_min);
     }
+    SYNC_AT("line search");
     CK(icx::la_axpby(n, -alpha, w->du, 1.0, d_u, s));
     CK(icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->res, w->vals, eps, s));
     rk = dev_norm(c, w->res, s);
@@ -389,7 +421,10 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
       R->alpha_history[k] = alpha;
     }
     if (opt->verbosity > 0) std::printf("newton %d: |r| = %.6e alpha = %.4f gmres its = %d\n", k, rk, alpha, it);
-    if (!std::isfinite(rk)) return set_err(c, ICX_ERR_NONFINITE, "non-finite residual");
+    if (!std::isfinite(rk)) {
+      SYNC_AT("residual");
+      return set_err(c, ICX_ERR_NONFINITE, "non-finite residual");
+    }
     converged = rk <= tau;
   }
   CK(cudaStreamSynchronize(s));

@@ -266,6 +266,21 @@ icx_status icx_explicit_solve(icx_ctx* ctx, double* d_u, const icx_explicit_opti
 /* d_out = M^-1 d_r element by element and equation by equation */
 icx_status icx_mass_inverse_apply(icx_ctx* ctx, const double* d_r, double* d_out, void* stream);
 
+/* ---- batches of independent problems (no counterpart in the reference, which
+ * solves one problem per process). icx_batch_create lays the meshes of n_parts
+ * set-up contexts side by side in one new context: every call above then
+ * works on all parts at once (one launch per kernel), with each part's
+ * discretization unchanged. Parts must share the PDE, basis order, geometry
+ * order, interior_penalty / sigma_ic and (Navier-Stokes) the fluid constants;
+ * Burgers coefficients, mesh sizes, coordinates and boundary data may differ.
+ * The parts must outlive the batch. u / res of the batch are the parts' vectors
+ * concatenated in part order; icx_batch_offsets gives each part's first
+ * element (n_parts + 1 entries). Not available on a batch: MDG-ICE, the CFL
+ * timestep. A Newton solve on a batch uses one line search and one stopping
+ * test for the concatenated residual. */
+icx_status icx_batch_create(icx_ctx** out, int device, int n_parts, icx_ctx* const* parts);
+icx_status icx_batch_offsets(const icx_ctx* batch, int* elem_offsets);
+
 /* ---- workload callbacks (icx_point_fn) ------------------------------------
  * icx_wl_constant: user -> double[1 + n] = {n, v_0 .. v_{n-1}}: out = v
  * icx_wl_sine_product: user -> double[1] = {amp}: out[0] = amp sin(2 pi x) sin(2 pi y)
