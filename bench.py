@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-newton", action="store_true", help="skip the secondary Newton solve timings")
+    ap.add_argument("--batched", type=int, default=64, metavar="N",
+                    help="secondary timing of N seeded uneven advection-diffusion problems, batched vs one at a "
+                         "time (0: skip; the full problem set is 512)")
     return ap.parse_args()
 
 
@@ -177,6 +180,49 @@ def residual_work(wl):
 #   ncu --set full --clock-control none -k regex:"face_flux|vol_lift" -s 10 -c 2 \
 #       python bench.py --steps 2 --warmup 3 --no-newton --no-cpu-baseline
 NCU_DRAM_BYTES = {"vol": 43.45e6 + 0.50e6, "face": 25.70e6 + 0.01e6}
+
+
+def batched_bench(torch, dev, n_problems):
+    """Newton solves (FP64, GMRES(30) + block-ILU(0), |r| <= 1e-10) of the
+    seeded uneven advection-diffusion problems: grouped by basis order into one
+    batch context each (one launch per kernel for all problems of a group)
+    against the same problems solved one context at a time. CUDA events around
+    the solves; the setup of the contexts is not timed."""
+    import iceicle_b200 as ib
+    from iceicle_b200.workloads import batched_problems
+    groups = batched_problems(n_problems, device=dev.index)
+    opt = ib.default_newton_options()
+    t_batch = t_seq = 0.0
+    worst = 0.0
+    n_dof = 0
+    its = []
+    for p, (b, parts, u0, specs) in groups.items():
+        ub = torch.from_numpy(u0.copy()).to(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        rep = b.newton_solve(ub, opt)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        t_batch += e0.elapsed_time(e1) * 1e-3
+        its.append(dict(p=p, problems=len(parts), newton_its=rep.iterations, gmres_its=rep.linear_iterations_total,
+                        converged=bool(rep.converged)))
+        off = 0
+        for c in parts:
+            n = c.layout.n_dof
+            uc = torch.from_numpy(u0[off:off + n].copy()).to(dev)
+            torch.cuda.synchronize(dev)
+            e0.record()
+            c.newton_solve(uc, opt)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            t_seq += e0.elapsed_time(e1) * 1e-3
+            a, bb = uc.cpu().numpy(), ub[off:off + n].cpu().numpy()
+            worst = max(worst, float(np.linalg.norm(a - bb) / max(np.linalg.norm(a), 1e-300)))
+            off += n
+        n_dof += off
+    return {"problems": n_problems, "n_dof": n_dof, "batched_s": t_batch, "one_at_a_time_s": t_seq,
+            "speedup": t_seq / t_batch if t_batch > 0 else None, "max_state_rel_diff": worst, "groups": its}
 
 
 def newton_bench(torch, dev):
@@ -327,6 +373,8 @@ def run_ours(a):
                 line["cpu_baseline"] = None
         if not a.no_newton and ws == 1:
             line["newton"] = newton_bench(torch, dev)
+        if a.batched and ws == 1:
+            line["batched"] = batched_bench(torch, dev, a.batched)
         print(json.dumps(line))
     if ws > 1:
         dist.destroy_process_group()

@@ -11,6 +11,14 @@ no datasets for this path; every input here is generated from fixed seeds).
                      level, Van Leer convective flux with interior penalty,
                      nodes perturbed by a seeded smooth displacement of
                      amplitude 0.05 h that keeps the domain boundary.
+  batched_problems - independent 2D advection-diffusion problems of uneven
+                     size and order: n x n quads with n uniform in [8, 96],
+                     p uniform in {1, 2, 3, 4}, geometry order 1, viscosity
+                     log-uniform in [1e-4, 1e-1], advection a = (cos t, sin t)
+                     with t uniform in [0, 2 pi), Dirichlet data 1 left of the
+                     line x = 0.5 + 0.3 y and 0 right of it (a boundary layer
+                     and an interior front), seeded sinusoidal initial state;
+                     grouped by p into batches.
 """
 import ctypes as C
 
@@ -108,3 +116,55 @@ def ns_mms_config(nx=128, ny=128, p=3, geo_order=2, seed=4321, device=0, perturb
     st *= 1.0 + state_noise * rng.standard_normal(st.shape)
     return Workload(ctx, coords, np.ascontiguousarray(st.reshape(-1)), dict(prm=list(prm), p=p, g=geo_order),
                     "ns_mms", [prm])
+
+
+def batched_problem_specs(n_problems=512, seed=2024, n_range=(8, 96), orders=(1, 2, 3, 4)):
+    """the seeded problem list: dicts with n, p, mu, theta and the initial
+    state's wave numbers and phases"""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_problems):
+        out.append(dict(n=int(rng.integers(n_range[0], n_range[1] + 1)), p=int(rng.choice(orders)),
+                        mu=float(10.0 ** rng.uniform(-4.0, -1.0)), theta=float(rng.uniform(0.0, 2 * np.pi)),
+                        kx=int(rng.integers(1, 4)), ky=int(rng.integers(1, 4)),
+                        phx=float(rng.uniform(0.0, 2 * np.pi)), phy=float(rng.uniform(0.0, 2 * np.pi))))
+    return out
+
+
+def advection_diffusion_problem(spec, device=0):
+    """one problem of the list as a set-up Context and its initial state"""
+    n, p = spec["n"], spec["p"]
+    ctx = Context(device)
+    ctx.mesh_uniform((n, n), (0.0, 0.0), (1.0, 1.0), 1, (DIRICHLET,) * 4, (0,) * 4)
+    ctx.set_coords(lattice_coords((n, n), 1))
+    ctx.fespace(p)
+    a = (np.cos(spec["theta"]), np.sin(spec["theta"]))
+    ctx.disc_burgers(spec["mu"], a, (0.0, 0.0))
+    ctx.disc_options(False, 0.0)
+    step = (C.c_double * 4)(0.5, 0.3, 1.0, 0.0)
+    ctx.dirichlet(0, workload_fn("oblique_step"), C.cast(step, C.c_void_p))
+    ctx.setup()
+    ctx._keep.append(step)
+    xy = ctx.basis_node_coords()
+    u0 = np.sin(2 * np.pi * spec["kx"] * xy[..., 0] + spec["phx"]) * np.sin(2 * np.pi * spec["ky"] * xy[..., 1] +
+                                                                           spec["phy"])
+    return ctx, np.ascontiguousarray(u0.reshape(-1))
+
+
+def batched_problems(n_problems=512, seed=2024, device=0):
+    """the problem list grouped by basis order: {p: (batch Context, parts,
+    concatenated initial state, [specs])}"""
+    from . import batch
+    specs = batched_problem_specs(n_problems, seed)
+    groups = {}
+    for sp in specs:
+        groups.setdefault(sp["p"], []).append(sp)
+    out = {}
+    for p, lst in sorted(groups.items()):
+        parts, states = [], []
+        for sp in lst:
+            c, u0 = advection_diffusion_problem(sp, device)
+            parts.append(c)
+            states.append(u0)
+        out[p] = (batch(parts, device), parts, np.concatenate(states), lst)
+    return out
