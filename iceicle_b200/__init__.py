@@ -105,6 +105,7 @@ def lib():
             "icx_bsr_spmv": (C.c_int, [vp, vp, vp, vp, vp]),
             "icx_newton_default_options": (C.c_int, [C.POINTER(NewtonOptions)]),
             "icx_explicit_default_options": (C.c_int, [C.POINTER(ExplicitOptions)]),
+            "icx_mfnk_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport)]),
             "icx_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int, C.POINTER(vp)]),
             "icx_batch_offsets": (C.c_int, [vp, ip]),
             "icx_explicit_solve": (C.c_int, [vp, vp, C.POINTER(ExplicitOptions), C.POINTER(ExplicitReport)]),
@@ -349,6 +350,15 @@ class Context:
         """out = M^-1 r element by element (device arrays)"""
         self._check(lib().icx_mass_inverse_apply(self._h, _ptr(r), _ptr(out), _stream_ptr(stream)),
                     "mass_inverse_apply")
+
+    def mfnk_solve(self, u, options=None):
+        """matrix-free Newton-Krylov on u (device, FP64, in place); returns the report"""
+        opt = options or default_newton_options()
+        rep = NewtonReport()
+        st = lib().icx_mfnk_solve(self._h, _ptr(u), C.byref(opt), C.byref(rep))
+        if st not in (0, 5):
+            self._check(st, "mfnk_solve")
+        return rep
 
     def newton_solve(self, u, options=None):
         opt = options or default_newton_options()

@@ -434,3 +434,107 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   return converged ? ICX_OK : ICX_ERR_NOT_CONVERGED;
 }
 }
+
+// ---------------------------------------------------------------------------
+// Matrix-free Newton-Krylov (MFNK, src/solvers/include/iceicle/
+// matrix_free_newton_krylov.hpp:62-365) on the PDE unknowns: each Krylov
+// product is the one-sided difference J p ~ (R(u + eps p) - R(u)) / eps with
+// the fixed eps = sqrt(machine epsilon) (jacobian_mf_op), the Krylov solver
+// is GMRES without preconditioner (PCNONE), the step u <- u - alpha du takes
+// the reference's line searches with non-finite trial residuals mapped to
+// 1e100, and the stopping test |R| <= tau_abs is checked after every step
+// (the solver never sets the relative tolerance's r0, so tau_rel has no
+// effect). No Jacobian is stored.
+extern "C" icx_status icx_mfnk_solve(icx_ctx* c, double* d_u, const icx_newton_options* opt, icx_newton_report* rep) {
+  if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
+  if (!d_u || !opt) return set_err(c, ICX_ERR_INVALID, "null argument");
+  if (opt->gmres_restart < 1 || opt->gmres_restart > 60) return set_err(c, ICX_ERR_INVALID, "restart in 1..60");
+  cudaStream_t s = 0;
+  icx_status st = ensure_work(c, opt->gmres_restart);
+  if (st != ICX_OK) return st;
+  icx_solver_work* w = c->sw;
+  const icx::DeviceMesh& dm = c->dm;
+  const long long n = w->n;
+  icx_newton_report local{};
+  icx_newton_report* R = rep ? rep : &local;
+  std::memset(R, 0, sizeof(*R));
+  const double eps = std::sqrt(DBL_EPSILON);
+  // w->res = R(u); w->ustep / w->rwork are the perturbed state and residual of
+  // the Krylov products, w->z holds the line search's trial residual
+  CK(icx::launch_residual(dm, c->phys, d_u, w->res, s));
+  double rk = dev_norm(c, w->res, s);
+  if (!std::isfinite(rk)) {
+    SYNC_AT("initial residual");
+    return set_err(c, ICX_ERR_NONFINITE, "non-finite initial residual");
+  }
+  R->r0 = rk;
+  R->residual_history[0] = rk;
+  icx::KrylovBuffers kb;
+  kb.n = n;
+  kb.m = opt->gmres_restart;
+  kb.V = w->V;
+  kb.w = w->w;
+  kb.z = w->r;      // no preconditioner: gmres_op does not use z
+  kb.r = w->rwork;  // restart residual
+  kb.dh = w->dh;
+  kb.lw = &w->lw;
+  // the Krylov products need their own state/residual buffers: pct and du
+  // are free while GMRES runs (du receives the solution at the end)
+  double* up = w->pct;
+  double* rp = w->ustep;
+  icx::LinOp A = [&](const double* p, double* y) -> cudaError_t {
+    cudaError_t e = icx::la_xpay(n, d_u, eps, p, up, s);  // up = u + eps p
+    if (e == cudaSuccess) e = icx::launch_residual(dm, c->phys, up, rp, s);
+    if (e == cudaSuccess) e = icx::la_xpay(n, rp, -1.0, w->res, y, s);       // R(u + eps p) - R(u)
+    if (e == cudaSuccess) e = icx::la_axpby(n, 1.0 / eps, y, 0.0, y, s);    // / eps
+    return e;
+  };
+  bool converged = false;
+  int k = 0;
+  for (; k < opt->kmax; ++k) {
+    int it = 0;
+    double rr = 0.0;
+    st = icx::gmres_op(kb, A, nullptr, opt->gmres_max_it, opt->gmres_rtol, w->res, w->du, &it, &rr, s, &c->err);
+    if (st != ICX_OK) {
+      SYNC_AT("linear solve");
+      return st;
+    }
+    R->linear_iterations_total += it;
+    double alpha = 1.0;
+    if (opt->linesearch != 0) {
+      std::function<double(double)> phi = [&](double a) -> double {
+        icx::la_xpay(n, d_u, -a, w->du, w->ustep, s);
+        icx::launch_residual(dm, c->phys, w->ustep, w->z, s);
+        double v = dev_norm(c, w->z, s);
+        return std::isfinite(v) ? v : 1e100;
+      };
+      if (opt->linesearch == 1)
+        alpha = wolfe_ls(phi, opt->ls_alpha_max, opt->ls_alpha_initial, opt->ls_max_it, opt->ls_c1, opt->ls_c2);
+      else
+        alpha = corrigan_ls(phi, opt->ls_alpha_max, opt->ls_alpha_initial, opt->ls_max_it, opt->ls_alpha_min);
+      SYNC_AT("line search");
+    }
+    CK(icx::la_axpby(n, -alpha, w->du, 1.0, d_u, s));
+    CK(icx::launch_residual(dm, c->phys, d_u, w->res, s));
+    rk = dev_norm(c, w->res, s);
+    if (k + 1 < 64) {
+      R->residual_history[k + 1] = rk;
+      R->alpha_history[k] = alpha;
+    }
+    if (opt->verbosity > 0) std::printf("mfnk %d: |r| = %.6e alpha = %.4f gmres its = %d\n", k, rk, alpha, it);
+    if (!std::isfinite(rk)) {
+      SYNC_AT("residual");
+      return set_err(c, ICX_ERR_NONFINITE, "non-finite residual");
+    }
+    if (rk <= opt->tau_abs) {
+      converged = true;
+      ++k;
+      break;
+    }
+  }
+  SYNC_AT("mfnk");
+  R->iterations = k;
+  R->converged = converged;
+  R->r_final = rk;
+  return converged ? ICX_OK : ICX_ERR_NOT_CONVERGED;
+}

@@ -234,6 +234,14 @@ icx_status icx_gmres_solve(icx_ctx* ctx, const double* d_vals, const double* d_b
 
 icx_status icx_newton_default_options(icx_newton_options* opt);
 icx_status icx_newton_solve(icx_ctx* ctx, double* d_u, const icx_newton_options* opt, icx_newton_report* rep);
+/* MFNK (matrix_free_newton_krylov.hpp:62-365) without geometry unknowns:
+ * Newton with the Jacobian applied matrix-free as
+ * (R(u + eps p) - R(u)) / eps, eps = sqrt(machine epsilon), GMRES without
+ * preconditioner (opt->preconditioner is ignored), the line searches of
+ * icx_newton_solve (non-finite trial residuals count as 1e100) and the
+ * stopping test |R| <= tau_abs after every step, as the reference's solver
+ * applies it. rep->iterations = Newton steps taken. */
+icx_status icx_mfnk_solve(icx_ctx* ctx, double* d_u, const icx_newton_options* opt, icx_newton_report* rep);
 
 /* ---- explicit time stepping (ExplicitEuler explicit_euler.hpp:30-181,
  * RK3TVD tvd_rk3.hpp:30-277, RK3SSP ssp_rk3.hpp:30-241; FixedTimestep,

@@ -136,3 +136,37 @@ def lm(pb, coord, traces, u0, x0, kmax=5, lambda_u=1e-7, lambda_b=1e-2, tau_abs=
         hist.append(np.linalg.norm(out))
         k += 1
     return u, x, hist
+
+
+def mfnk(pb, coord, u0, tau_abs=1e-9, kmax=30, rtol=1e-6, restart=30, maxit=5000, linesearch=None, history=None):
+    """MFNK::solve (src/solvers/include/iceicle/matrix_free_newton_krylov.hpp:
+    219-365) without geometry unknowns, restated over the oracle residual: J p
+    is the one-sided difference (R(u + eps p) - R(u)) / eps with the fixed
+    eps = sqrt(machine epsilon) (jacobian_mf_op, :62-140), the Krylov solve is
+    restarted GMRES without preconditioner from a zero guess, u <- u - alpha du,
+    and the test |R| <= tau_abs runs after every step. Returns (u, steps)."""
+    u = np.array(u0, dtype=float)
+    r = ob.residual(ob.oracle(), pb, coord, u)
+    k = 0
+    for k in range(1, kmax + 1):
+        r0 = r.copy()
+        u_fix = u.copy()
+
+        def mv(p):
+            return (ob.residual(ob.oracle(), pb, coord, u_fix + SQEPS * p) - r0) / SQEPS
+
+        A = spla.LinearOperator((len(u), len(u)), matvec=mv)
+        du, _ = spla.gmres(A, r0, rtol=rtol, atol=0.0, restart=restart, maxiter=max(1, maxit // restart))
+        alpha = 1.0
+        if linesearch == "wolfe":
+            def phi(a):
+                v = np.linalg.norm(ob.residual(ob.oracle(), pb, coord, u - a * du))
+                return v if np.isfinite(v) else 1e100
+            alpha = wolfe_ls(phi)
+        u = u - alpha * du
+        r = ob.residual(ob.oracle(), pb, coord, u)
+        if history is not None:
+            history.append(float(np.linalg.norm(r)))
+        if np.linalg.norm(r) <= tau_abs:
+            break
+    return u, k

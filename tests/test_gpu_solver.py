@@ -194,3 +194,70 @@ def test_newton_mixed_precision_burgers_ilu():
     assert r64.converged and r32.converged and r32.r_final <= 1e-12
     a, b = u64.cpu().numpy(), u32.cpu().numpy()
     assert np.linalg.norm(a - b) <= 1e-10 * np.linalg.norm(wl.u0)
+
+
+def test_mfnk_matches_the_oracle_mfnk():
+    """matrix-free Newton-Krylov (no stored Jacobian, GMRES without
+    preconditioner) against the oracle's restatement of the reference MFNK on
+    a Burgers problem with nonzero boundary data. The Jacobian products are
+    one-sided differences with the fixed eps = sqrt(machine epsilon), whose
+    rounding floor (here |R| about 3e-9) bounds how far either solver can
+    drive the residual, so both stop at |R| <= 1e-8. The residual histories
+    agree while |R| is far above that floor (the two GMRES differ in their
+    last digits), and the state lands on the oracle Newton's converged state
+    to 1e-6 (L2, relative)."""
+    spec = Spec(pde=BURGERS, nx=5, ny=4, p=2, g=2, mu=1e-2, a=(0.2, 0.1), b=(1.0, 0.5),
+                dirichlet=[("constant", [1, 0.25])])
+    c = spec.coords()
+    pb = spec.oracle_problem()
+    ctx = spec.context(c)
+    u0 = 0.25 + 0.2 * np.random.default_rng(21).standard_normal(spec.N)
+    hist_or = []
+    on.mfnk(pb, c, u0, tau_abs=1e-8, kmax=30, rtol=1e-6, history=hist_or)
+    u_newton, _ = on.newton(pb, c, u0, tau_abs=1e-12, kmax=20)
+    du = torch.from_numpy(u0.copy()).cuda()
+    rep = ctx.mfnk_solve(du, _newton_opts(tau_abs=1e-8, kmax=30, linesearch=0, gmres_rtol=1e-6,
+                                          gmres_max_it=5000))
+    assert rep.converged and rep.r_final <= 1e-8
+    hist = list(rep.residual_history[1:rep.iterations + 1])
+    assert len(hist) == len(hist_or), (hist, hist_or)
+    for a_, b_ in zip(hist, hist_or):
+        if b_ > 1e-5:
+            assert abs(a_ - b_) <= 1e-3 * b_, (hist, hist_or)
+    assert np.linalg.norm(du.cpu().numpy() - u_newton) <= 1e-6 * np.linalg.norm(u_newton)
+
+
+def _ns_mms_state(ctx, noise, seed):
+    from iceicle_b200 import workload_fn
+    import ctypes as C
+    from iceicle_b200.workloads import ns_mms_params
+    prm = ns_mms_params()
+    f = workload_fn("ns_mms_state")
+    xy = ctx.basis_node_coords().reshape(-1, 2)
+    out = (C.c_double * 4)()
+    pt = (C.c_double * 2)()
+    u0 = np.zeros((len(xy), 4))
+    for k in range(len(xy)):
+        pt[0], pt[1] = xy[k]
+        f(pt, out, C.cast(prm, C.c_void_p))
+        u0[k] = out[:]
+    return (u0 * (1 + noise * np.random.default_rng(seed).standard_normal(u0.shape))).reshape(-1)
+
+
+def test_mfnk_ns_with_linesearch_matches_assembled_newton():
+    """MFNK with the Wolfe line search and the assembled-Jacobian Newton land
+    on the same Navier-Stokes state. With total energy near 25 the floor of
+    the difference products is |R| about 1e-6 here (the oracle MFNK stalls
+    between 1e-6 and 3e-7), so MFNK stops at |R| <= 5e-6, where the oracle's
+    state is 3e-8 from the converged one; the states agree to 1e-6 (L2,
+    relative)."""
+    spec = Spec(pde=NS, nx=3, ny=3, p=2, g=2, ip=True, source=True, perturb=0.05)
+    ctx = spec.context()
+    u0 = _ns_mms_state(ctx, 1e-2, 22)
+    u1 = torch.from_numpy(u0.copy()).cuda()
+    r1 = ctx.newton_solve(u1, _newton_opts(tau_abs=1e-8, kmax=30, gmres_rtol=1e-6, gmres_max_it=5000))
+    u2 = torch.from_numpy(u0.copy()).cuda()
+    r2 = ctx.mfnk_solve(u2, _newton_opts(tau_abs=5e-6, kmax=40, gmres_rtol=1e-6, gmres_max_it=5000))
+    assert r1.converged and r2.converged
+    a, b = u1.cpu().numpy(), u2.cpu().numpy()
+    assert np.linalg.norm(a - b) <= 1e-6 * np.linalg.norm(a)

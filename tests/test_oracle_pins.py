@@ -152,3 +152,19 @@ def test_mdg_residual_and_jacobian_match_reference(kw):
     assert np.abs(o1 - o2).max() <= 1e-12 * np.abs(o2).max()
     assert np.abs(J1 - J2).max() <= 1e-6 * np.abs(J2).max()
     assert np.array_equal(J1 != 0, J2 != 0)
+
+
+def test_oracle_mfnk_reaches_the_oracle_newton_state():
+    """the oracle's MFNK restatement (difference products, unpreconditioned
+    GMRES) converges to the assembled-Jacobian Newton's state down to the
+    floor of its difference products"""
+    import oracle_newton as on
+    spec = Spec(pde=BURGERS, nx=3, ny=3, p=2, g=2, mu=1e-2, a=(0.2, 0.1), b=(1.0, 0.5),
+                dirichlet=[("constant", [1, 0.25])])
+    c = spec.coords()
+    pb = spec.oracle_problem()
+    u0 = 0.25 + 0.2 * np.random.default_rng(3).standard_normal(spec.N)
+    u, k = on.mfnk(pb, c, u0, tau_abs=1e-8, kmax=30, rtol=1e-6)
+    assert np.linalg.norm(ob.residual(ob.oracle(), pb, c, u)) <= 1e-8 and k < 30
+    u_n, _ = on.newton(pb, c, u0, tau_abs=1e-12, kmax=20)
+    assert np.linalg.norm(u - u_n) <= 1e-6 * np.linalg.norm(u_n)
