@@ -112,6 +112,12 @@ def lib():
             "icx_mass_inverse_apply": (C.c_int, [vp, vp, vp, vp]),
             "icx_newton_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport)]),
             "icx_basis_node_coords": (C.c_int, [vp, vp]),
+            "icx_write_restart": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_char_p]),
+            "icx_read_restart": (C.c_int, [vp, vp, C.c_char_p, C.c_int, C.c_char_p]),
+            "icx_write_vtu": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_char_p, C.c_char_p,
+                                        C.POINTER(C.c_char_p), C.c_int]),
+            "icx_write_vtu_mdg": (C.c_int, [vp, vp, C.c_int, C.c_char_p, C.c_char_p, C.POINTER(C.c_char_p),
+                                            C.c_int]),
             "icx_form_residual_timed": (C.c_int, [vp, vp, vp, vp, dp, dp]),
             "icx_form_residual_noalloc": (C.c_int, [vp, vp, vp, vp]),
             "icx_gmres_solve": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, ip, dp, vp]),
@@ -351,6 +357,41 @@ class Context:
         self._check(lib().icx_mass_inverse_apply(self._h, _ptr(r), _ptr(out), _stream_ptr(stream)),
                     "mass_inverse_apply")
 
+    def write_restart(self, u, k, rank=0, directory=None):
+        """write_restart: <directory>/restart<k>_<rank> (directory None:
+        RESTART under the working directory) from u (device, FP64)"""
+        d = None if directory is None else str(directory).encode()
+        self._check(lib().icx_write_restart(self._h, _ptr(u), int(k), int(rank), d), "write_restart")
+
+    def read_restart(self, u, name, rank=0, directory=None):
+        """read_restart: moves the mesh nodes to the file's coordinates and
+        fills u (device, FP64) from <directory>/<name>_<rank>"""
+        d = None if directory is None else str(directory).encode()
+        self._check(lib().icx_read_restart(self._h, _ptr(u), name.encode(), int(rank), d), "read_restart")
+
+    @staticmethod
+    def _names(names):
+        if names is None:
+            return None
+        arr = (C.c_char_p * len(names))(*[n.encode() for n in names])
+        return arr
+
+    def write_vtu(self, u, itime, kind=0, directory=None, collection=None, names=None, precision=8):
+        """PVDWriter::write_vtu of u (kind VTU_SOLUTION) or of its residual
+        and the residual's domain and trace parts (kind VTU_RESIDUAL)"""
+        d = None if directory is None else str(directory).encode()
+        cn = None if collection is None else collection.encode()
+        self._check(lib().icx_write_vtu(self._h, _ptr(u), int(kind), int(itime), d, cn, self._names(names),
+                                        int(precision)), "write_vtu")
+
+    def write_vtu_mdg(self, ic, itime, directory=None, collection=None, names=None, precision=8):
+        """the MDG interface-conservation residual ic (device, [selected node][neq])
+        as an isoparametric nodal field"""
+        d = None if directory is None else str(directory).encode()
+        cn = None if collection is None else collection.encode()
+        self._check(lib().icx_write_vtu_mdg(self._h, _ptr(ic), int(itime), d, cn, self._names(names),
+                                            int(precision)), "write_vtu_mdg")
+
     def mfnk_solve(self, u, options=None):
         """matrix-free Newton-Krylov on u (device, FP64, in place); returns the report"""
         opt = options or default_newton_options()
@@ -367,6 +408,10 @@ class Context:
         if st not in (0, 5):
             self._check(st, "newton_solve")
         return rep
+
+
+VTU_SOLUTION = 0
+VTU_RESIDUAL = 1
 
 
 def batch(parts, device=0):

@@ -294,6 +294,10 @@ void lagrange_values_derivs(int pn, double x, double* N, double* dN) {
   l.eval(x, N, dN, d2N);
 }
 void gauss_legendre_points(int n, double* x, double* w) { gauss_legendre(n, x, w); }
+void element_point(const icx_ctx* c, int e, const double xi[2], double x[2]) {
+  Lagrange1D lg(c->geo_order);
+  el_point(c, lg, e, xi, x);
+}
 }  // namespace icx
 
 extern "C" {

@@ -111,6 +111,9 @@ cudaError_t launch_geometry(const DeviceMesh& dm, cudaStream_t s);
 // `mid` (optional) is recorded on s between the face and volume kernels
 cudaError_t launch_residual(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
                             cudaStream_t s, cudaEvent_t mid = nullptr);
+// the volume (domain integral) contributions alone, faces left out
+cudaError_t launch_residual_domain(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
+                                   cudaStream_t s);
 // Jacobian (icx_jacobian.cu)
 cudaError_t launch_jacobian_fd(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
                                double* vals, double eps, cudaStream_t s);
@@ -134,4 +137,6 @@ void lagrange_values_derivs(int pn, double x, double* N, double* dN);
 void free_explicit(icx_ctx* c);
 // Gauss-Legendre points in the reference order (+x1, -x1, ..., 0) and weights (icx_host.cu)
 void gauss_legendre_points(int n, double* x, double* w);
+// physical point of reference point xi in element e (geometry transformation, icx_host.cu)
+void element_point(const icx_ctx* c, int e, const double xi[2], double x[2]);
 }  // namespace icx

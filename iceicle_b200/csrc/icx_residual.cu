@@ -680,6 +680,35 @@ static cudaError_t residual_pg(const DeviceMesh& dm, const PhysParams& pp, const
   return cudaGetLastError();
 }
 
+// volume contributions only: the face kernel is skipped and its outputs are
+// zeroed, so the lifting phase of the volume kernel adds nothing
+template <int PDE, int P, int G>
+static cudaError_t residual_domain_pg(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
+                                      cudaStream_t s) {
+  using V = VolCfg<PDE, P, G>;
+  static std::atomic<unsigned> attr_vol{0};
+  cudaError_t e = cudaMemsetAsync(dm.face_flux, 0, sizeof(double) * (size_t)dm.F * dm.nqf * dm.neq, s);
+  if (e == cudaSuccess && dm.face_grad)
+    e = cudaMemsetAsync(dm.face_grad, 0, sizeof(double) * (size_t)dm.F * 2 * dm.nqf * dm.neq * 2, s);
+  if (e != cudaSuccess) return e;
+  if ((e = smem_attr_once(vol_lift_kernel<PDE, P, G>, V::SMEM, attr_vol)) != cudaSuccess) return e;
+  int nblk = (dm.E + V::EPB - 1) / V::EPB;
+  vol_lift_kernel<PDE, P, G><<<nblk, V::THREADS, V::SMEM, s>>>(dm, pp, u, res);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_residual_domain(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
+                                   cudaStream_t s) {
+#define ICX_RES_CASE(PDE, PP, GG) \
+  if (pp.pde == PDE && dm.P == PP && dm.G == GG) return residual_domain_pg<PDE, PP, GG>(dm, pp, u, res, s);
+  ICX_RES_CASE(0, 1, 1) ICX_RES_CASE(0, 2, 1) ICX_RES_CASE(0, 3, 1) ICX_RES_CASE(0, 4, 1)
+  ICX_RES_CASE(0, 1, 2) ICX_RES_CASE(0, 2, 2) ICX_RES_CASE(0, 3, 2) ICX_RES_CASE(0, 4, 2)
+  ICX_RES_CASE(1, 1, 1) ICX_RES_CASE(1, 2, 1) ICX_RES_CASE(1, 3, 1) ICX_RES_CASE(1, 4, 1)
+  ICX_RES_CASE(1, 1, 2) ICX_RES_CASE(1, 2, 2) ICX_RES_CASE(1, 3, 2) ICX_RES_CASE(1, 4, 2)
+#undef ICX_RES_CASE
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_residual(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
                             cudaStream_t s, cudaEvent_t mid) {
 #define ICX_RES_CASE(PDE, PP, GG) \

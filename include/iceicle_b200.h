@@ -289,6 +289,41 @@ icx_status icx_mass_inverse_apply(icx_ctx* ctx, const double* d_r, double* d_out
 icx_status icx_batch_create(icx_ctx** out, int device, int n_parts, icx_ctx* const* parts);
 icx_status icx_batch_offsets(const icx_ctx* batch, int* elem_offsets);
 
+/* ---- restart files and VTU output (host files; d_u and d_ic are device
+ * arrays). Not available on a batch. */
+/* write_restart (fe_function/restart.hpp:20-59): writes <dir>/restart<k>_<rank>
+ * (dir NULL: "RESTART" under the working directory, created if missing): the
+ * node coordinates "x y " per node, a newline, then u in layout order, each
+ * value followed by a space, 16 significant digits. */
+icx_status icx_write_restart(icx_ctx* ctx, const double* d_u, int k, int rank, const char* dir);
+/* read_restart (restart.hpp:68-108): reads <dir>/<name>_<rank>, moves the mesh
+ * nodes to the stored coordinates (as icx_mesh_set_coords) and fills d_u.
+ * ICX_ERR_INVALID when the file is missing or holds too few numbers (the
+ * reference leaves such values unread). */
+icx_status icx_read_restart(icx_ctx* ctx, double* d_u, const char* name, int rank, const char* dir);
+
+#define ICX_VTU_SOLUTION 0 /* PVDWriter::register_fields(u, field_names) */
+#define ICX_VTU_RESIDUAL 1 /* PVDWriter::register_residuals(u, residual_names, disc) */
+/* PVDWriter::write_vtu(itime, time) (io/pvd_writer.hpp:1095-1140): writes
+ * <dir>/<collection><itime>.vtu (dir NULL: "iceicle_data"; collection NULL:
+ * "data", or "residuals" for ICX_VTU_RESIDUAL as the reference's driver names
+ * it) in the discontinuous layout, values with `precision` significant digits
+ * (the reference prints 8). ICX_VTU_SOLUTION writes the fields of d_u;
+ * ICX_VTU_RESIDUAL the residual of d_u, then its domain-integral part
+ * ("domain_" prefix) and its face part ("trace_" prefix). names: neq names,
+ * or NULL for the reference's ("u" / "residual" for Burgers; "rho", "rhou",
+ * "rhov", "rhoe" / "density_conservation", "momentum_u_conservation",
+ * "momentum_v_conservation", "energy_conservation" for Navier-Stokes). */
+icx_status icx_write_vtu(icx_ctx* ctx, const double* d_u, int kind, int itime, const char* dir,
+                         const char* collection, const char* const* names, int precision);
+/* the MDG interface-conservation residual d_ic ([selected node][neq], the tail
+ * of icx_form_residual_mdg's output) as the reference's implicit driver writes
+ * it (solvers_lua_interface.hpp:589-632): scattered to the mesh nodes (zero at
+ * unselected nodes) and written over the isoparametric H1 space; collection
+ * NULL: "mdg_residuals"; names NULL: the field names above. */
+icx_status icx_write_vtu_mdg(icx_ctx* ctx, const double* d_ic, int itime, const char* dir, const char* collection,
+                             const char* const* names, int precision);
+
 /* ---- workload callbacks (icx_point_fn) ------------------------------------
  * icx_wl_constant: user -> double[1 + n] = {n, v_0 .. v_{n-1}}: out = v
  * icx_wl_sine_product: user -> double[1] = {amp}: out[0] = amp sin(2 pi x) sin(2 pi y)

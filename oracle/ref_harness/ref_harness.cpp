@@ -25,6 +25,9 @@
 #include "iceicle/explicit_euler.hpp"
 #include "iceicle/ssp_rk3.hpp"
 #include "iceicle/tvd_rk3.hpp"
+#include "iceicle/fe_function/restart.hpp"
+#include "iceicle/pvd_writer.hpp"
+#include <filesystem>
 #include <cstring>
 #include <functional>
 #include <memory>
@@ -151,6 +154,28 @@ int with_disc(const ref_problem& pb, const double* coord, Body&& body) {
     add_callbacks(disc, pb);
     return body(fespace, disc, std::integral_constant<std::size_t, 4>{});
   }
+}
+
+// field and residual names the reference's applications give each PDE
+// (conservation_law.cpp:246-247, ns_manufactured.cpp:246-257)
+std::vector<std::string> field_names(int pde) {
+  if (pde == 0) return {"u"};
+  return {"rho", "rhou", "rhov", "rhoe"};
+}
+std::vector<std::string> residual_names(int pde) {
+  if (pde == 0) return {"residual"};
+  return {"density_conservation", "momentum_u_conservation", "momentum_v_conservation", "energy_conservation"};
+}
+
+// runs f with the working directory set to dir (the reference's writers
+// write under std::filesystem::current_path())
+template <class F>
+int in_directory(const char* dir, F&& f) {
+  auto old = std::filesystem::current_path();
+  std::filesystem::current_path(dir);
+  int rc = f();
+  std::filesystem::current_path(old);
+  return rc;
 }
 
 template <class Body>
@@ -396,6 +421,85 @@ int ref_explicit_solve(const ref_problem* pb, const double* coord, double* u, in
     }
     if (rc == 0) std::memcpy(u, ubuf.data(), sizeof(T) * ubuf.size());
     return rc;
+  });
+}
+
+/// write_restart(fespace, u, k) (fe_function/restart.hpp:20-59) run in `dir`:
+/// writes dir/RESTART/restart<k>_0
+int ref_write_restart(const ref_problem* pb, const double* coord, const double* u, int k, const char* dir) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    fe_layout_right layout{fespace.dg_map, neq_c};
+    std::vector<T> ubuf(u, u + layout.size());
+    fespan uspan{ubuf.data(), layout};
+    return in_directory(dir, [&] { write_restart(fespace, uspan, k); return 0; });
+  });
+}
+
+/// read_restart(fespace, u, name) (restart.hpp:68-108) run in `dir`: the
+/// node coordinates it leaves in the mesh and u
+int ref_read_restart(const ref_problem* pb, const char* name, const char* dir, double* coord_out, double* u_out) {
+  return dispatch_p(*pb, nullptr, [&](auto& fespace, auto& disc, auto neq_c) {
+    fe_layout_right layout{fespace.dg_map, neq_c};
+    std::vector<T> ubuf(layout.size());
+    fespan uspan{ubuf.data(), layout};
+    int rc = in_directory(dir, [&] { read_restart(fespace, uspan, std::string{name}); return 0; });
+    const auto& c = fespace.meshptr->coord;
+    for (std::size_t i = 0; i < c.size(); ++i) { coord_out[2 * i] = c[i][0]; coord_out[2 * i + 1] = c[i][1]; }
+    std::memcpy(u_out, ubuf.data(), sizeof(T) * ubuf.size());
+    return rc;
+  });
+}
+
+/// PVDWriter::write_vtu(itime, itime) (io/pvd_writer.hpp:1095-1140) into
+/// dir/<collection><itime>.vtu: kind 0 register_fields(u, field names),
+/// kind 1 register_residuals(u, residual names, disc)
+int ref_write_vtu(const ref_problem* pb, const double* coord, const double* u, int kind, int itime,
+                  const char* dir, const char* collection) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    fe_layout_right layout{fespace.dg_map, neq_c};
+    std::vector<T> ubuf(u, u + layout.size());
+    fespan uspan{ubuf.data(), layout};
+    io::PVDWriter<T, IDX, ndim> w{};
+    w.data_directory = dir;
+    w.collection_name = collection;
+    w.register_fespace(fespace);
+    if (kind == 0) w.register_fields(uspan, field_names(pb->pde));
+    else w.register_residuals(uspan, residual_names(pb->pde), disc);
+    w.write_vtu(itime, (T)itime);
+    return 0;
+  });
+}
+
+/// the MDG interface-conservation residual as the reference's implicit
+/// driver writes it (solvers_lua_interface.hpp:589-632): ic ([selected node]
+/// [neq], geo_dof_map order) scattered into an H1 field over the mesh nodes
+/// and written by a PVDWriter on the geometry-order H1 space
+int ref_write_vtu_mdg(const ref_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                      const double* ic, int itime, const char* dir, const char* collection) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    std::vector<int> tr(traces, traces + ntr);
+    geo_dof_map geo_map{tr, fespace};
+    if (hyper)
+      mesh_parameterizations::hyper_rectangle(std::array<int, 2>{pb->nx, pb->ny},
+                                              std::array<double, 2>{pb->xmin[0], pb->xmin[1]},
+                                              std::array<double, 2>{pb->xmax[0], pb->xmax[1]}, geo_map);
+    constexpr int NEQ = (int)decltype(neq_c)::value;
+    FESpace space_h1{fespace.meshptr};
+    fe_layout_right h1_layout{fespace.cg_map, tmp::to_size<NEQ>()};
+    std::vector<T> h1_data(h1_layout.size());
+    fespan res_mdg_h1{h1_data, h1_layout};
+    ic_residual_layout<T, IDX, ndim, NEQ> ic_layout{geo_map};
+    std::vector<T> icbuf(ic, ic + ic_layout.size());
+    dofspan ic_residual{icbuf.data(), ic_layout};
+    auto view = dof_view(res_mdg_h1);
+    extract_icespan(ic_residual, view);
+    io::PVDWriter<T, IDX, ndim> w{};
+    w.data_directory = dir;
+    w.collection_name = collection;
+    w.register_fespace(space_h1);
+    w.register_fields(res_mdg_h1, field_names(pb->pde));
+    w.write_vtu(itime, (T)itime);
+    return 0;
   });
 }
 

@@ -225,3 +225,39 @@ def explicit_solve(lib, pb, coord, u, scheme, dt_kind=0, dt=0.0, cfl=0.3, term_k
                                   C.byref(t))
     assert rc == 0, rc
     return uu, steps.value, t.value
+
+
+def ref_write_restart(pb, coord, u, k, directory):
+    """the reference's write_restart run in `directory` (writes
+    directory/RESTART/restart<k>_0)"""
+    uu = np.ascontiguousarray(u, dtype=np.float64)
+    rc = ref().fn("write_restart")(C.byref(pb), _ptr(coord), _ptr(uu), int(k), str(directory).encode())
+    assert rc == 0, rc
+
+
+def ref_read_restart(pb, name, directory):
+    """the reference's read_restart run in `directory`: (coords, u)"""
+    E, nb, N = sizes(pb)
+    nn = (pb.nx * pb.geo_order + 1) * (pb.ny * pb.geo_order + 1)
+    coord = np.zeros(2 * nn)
+    u = np.zeros(N)
+    rc = ref().fn("read_restart")(C.byref(pb), name.encode(), str(directory).encode(), _ptr(coord), _ptr(u))
+    assert rc == 0, rc
+    return coord, u
+
+
+def ref_write_vtu(pb, coord, u, kind, itime, directory, collection):
+    """PVDWriter::write_vtu of the reference: kind 0 fields of u, 1 residuals"""
+    uu = np.ascontiguousarray(u, dtype=np.float64)
+    rc = ref().fn("write_vtu")(C.byref(pb), _ptr(coord), _ptr(uu), int(kind), int(itime), str(directory).encode(),
+                               collection.encode())
+    assert rc == 0, rc
+
+
+def ref_write_vtu_mdg(pb, coord, traces, hyper, ic, itime, directory, collection):
+    """the reference driver's MDG residual VTU (ic: [selected node][neq])"""
+    tr = np.ascontiguousarray(traces, dtype=np.int32)
+    icc = np.ascontiguousarray(ic, dtype=np.float64)
+    rc = ref().fn("write_vtu_mdg")(C.byref(pb), _ptr(coord), len(tr), _ptr(tr), int(hyper), _ptr(icc), int(itime),
+                                   str(directory).encode(), collection.encode())
+    assert rc == 0, rc
