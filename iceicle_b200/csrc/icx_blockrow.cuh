@@ -14,6 +14,8 @@ namespace icx {
 
 enum BlockRowMode {
   BR_ALL = 0,    // every block of the row (SpMV)
+  BR_LOWER = 1,  // the blocks left of the diagonal (column < row)
+  BR_UPPER = 2,  // the blocks right of the diagonal (column > row)
   BR_DIAG = 3    // block-diagonal storage D[e] (one block per row, column = row)
 };
 
@@ -49,6 +51,7 @@ __device__ inline void block_row_task(const RowSet& rs, long long task, const in
   else { kb0 = rowptr[e]; kb1 = rowptr[e + 1]; }
   for (int kb = kb0; kb < kb1; ++kb) {
     const int k = MODE == BR_DIAG ? e : colidx[kb];
+    if ((MODE == BR_LOWER && k >= e) || (MODE == BR_UPPER && k <= e)) continue;
     TA xv[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
@@ -94,15 +97,119 @@ __global__ void __launch_bounds__(256) block_row_kernel(RowSet rs, const int* __
   block_row_task<BS, MODE, false, TA>(rs, task, rowptr, colidx, A, v, x0, sign, y);
 }
 
+// Small blocks (BS <= 36): one warp per block row, reading each block as one
+// contiguous run of VEC-element vectors (16 bytes where BS allows): lane l
+// takes vectors l, l + 32, ..., so every load instruction of the warp moves a
+// contiguous 512-byte segment. A lane's vectors sit at the same (row, column
+// group) positions in every block of the row, so its partial sums stay in
+// registers across the row's blocks; they are combined once per block row
+// through shared memory, row r adding its BS / VEC column groups in a fixed
+// order (the result does not depend on scheduling).
+template <class TA, int BS>
+struct VecRowCfg {
+  static constexpr int VEC = (sizeof(TA) == 4 && BS % 4 == 0) ? 4 : (BS % 2 == 0 ? 2 : 1);
+  static constexpr int QR = BS / VEC;       // vectors per block row
+  static constexpr int Q = BS * QR;         // vectors per block
+  static constexpr int J = (Q + 31) / 32;   // vectors per lane
+  static constexpr int WARPS = 8;
+};
+
+template <class TA, int VEC>
+__device__ inline void load_vec(const TA* __restrict__ p, TA (&o)[VEC]) {
+  if constexpr (sizeof(TA) == 4 && VEC == 4) {
+    float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+  } else if constexpr (sizeof(TA) == 4 && VEC == 2) {
+    float2 t = __ldg(reinterpret_cast<const float2*>(p));
+    o[0] = t.x; o[1] = t.y;
+  } else if constexpr (sizeof(TA) == 8 && VEC == 2) {
+    double2 t = __ldg(reinterpret_cast<const double2*>(p));
+    o[0] = t.x; o[1] = t.y;
+  } else {
+#pragma unroll
+    for (int t = 0; t < VEC; ++t) o[t] = __ldg(p + t);
+  }
+}
+
+template <int BS, int MODE, class TA>
+__global__ void __launch_bounds__(256) block_row_vec_kernel(int nrows, const int* __restrict__ rowptr,
+                                                            const int* __restrict__ colidx,
+                                                            const TA* __restrict__ A, const double* v,
+                                                            const double* x0, double sign, double* y) {
+  using K = VecRowCfg<TA, BS>;
+  constexpr int VEC = K::VEC, QR = K::QR, Q = K::Q, J = K::J;
+  __shared__ TA xs_all[K::WARPS][BS];
+  __shared__ TA part_all[K::WARPS][Q];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = blockIdx.x * K::WARPS + wid;
+  if (e >= nrows) return;  // uniform over the warp; only warp-level barriers follow
+  TA* xs = xs_all[wid];
+  TA* part = part_all[wid];
+  TA acc[J];
+#pragma unroll
+  for (int j = 0; j < J; ++j) acc[j] = TA(0);
+  int kb0, kb1;
+  if (MODE == BR_DIAG) { kb0 = e; kb1 = e + 1; }
+  else { kb0 = rowptr[e]; kb1 = rowptr[e + 1]; }
+  for (int kb = kb0; kb < kb1; ++kb) {
+    const int k = MODE == BR_DIAG ? e : colidx[kb];
+    if ((MODE == BR_LOWER && k >= e) || (MODE == BR_UPPER && k <= e)) continue;
+    const TA* Ab = A + (size_t)kb * BS * BS;
+    TA a[J][VEC];
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const int q = lane + 32 * j;
+      if (q < Q) load_vec<TA, VEC>(Ab + (size_t)q * VEC, a[j]);
+      else {
+#pragma unroll
+        for (int t = 0; t < VEC; ++t) a[j][t] = TA(0);
+      }
+    }
+    for (int c = lane; c < BS; c += 32) xs[c] = (TA)v[(size_t)k * BS + c];
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const int q = lane + 32 * j;
+      if (q < Q) {
+        const int c0 = (q % QR) * VEC;
+#pragma unroll
+        for (int t = 0; t < VEC; ++t) acc[j] += a[j][t] * xs[c0 + t];
+      }
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int q = lane + 32 * j;
+    if (q < Q) part[q] = acc[j];
+  }
+  __syncwarp();
+  for (int r = lane; r < BS; r += 32) {
+    TA sum = TA(0);
+#pragma unroll
+    for (int g = 0; g < QR; ++g) sum += part[r * QR + g];
+    const double base = x0 ? x0[(size_t)e * BS + r] : 0.0;
+    y[(size_t)e * BS + r] = base + sign * (double)sum;
+  }
+}
+
 // launch over a row set: 8 warps per CTA
 template <int BS, int MODE, class TA = double>
 inline cudaError_t launch_block_rows(const RowSet& rs, const int* rowptr, const int* colidx, const TA* A,
                                      const double* v, const double* x0, double sign, double* y, cudaStream_t s) {
-  long long tasks = (long long)rs.count() * BlockRowCfg<BS>::GROUPS;
-  if (tasks <= 0) return cudaSuccess;
-  unsigned blocks = (unsigned)((tasks + 7) / 8);
-  block_row_kernel<BS, MODE, TA><<<blocks, 256, 0, s>>>(rs, rowptr, colidx, A, v, x0, sign, y);
-  return cudaGetLastError();
+  if constexpr (BS <= 36) {
+    const int n = rs.count();
+    if (n <= 0) return cudaSuccess;
+    constexpr int W = VecRowCfg<TA, BS>::WARPS;
+    block_row_vec_kernel<BS, MODE, TA><<<(n + W - 1) / W, W * 32, 0, s>>>(n, rowptr, colidx, A, v, x0, sign, y);
+    return cudaGetLastError();
+  } else {
+    long long tasks = (long long)rs.count() * BlockRowCfg<BS>::GROUPS;
+    if (tasks <= 0) return cudaSuccess;
+    unsigned blocks = (unsigned)((tasks + 7) / 8);
+    block_row_kernel<BS, MODE, TA><<<blocks, 256, 0, s>>>(rs, rowptr, colidx, A, v, x0, sign, y);
+    return cudaGetLastError();
+  }
 }
 
 

@@ -331,6 +331,29 @@ cudaError_t la_block_invert(int nblk, int bs, const double* src, const int* blk_
   return cudaErrorInvalidValue;
 }
 
+template <class TA>
+static cudaError_t tri_rows_t(const DeviceMesh& dm, bool lower, const TA* A, const double* v, const double* x0,
+                              double sign, double* y, cudaStream_t s) {
+  const int bs = dm.nb * dm.neq;
+  RowSet rs{0, 0, -1, dm.E};
+#define ICX_TRI_CASE(B)                                                                                          \
+  if (bs == B)                                                                                                   \
+    return lower ? launch_block_rows<B, BR_LOWER, TA>(rs, dm.bsr_rowptr, dm.bsr_colidx, A, v, x0, sign, y, s)    \
+                 : launch_block_rows<B, BR_UPPER, TA>(rs, dm.bsr_rowptr, dm.bsr_colidx, A, v, x0, sign, y, s);
+  ICX_BLOCK_SIZES(ICX_TRI_CASE)
+#undef ICX_TRI_CASE
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t la_tri_rows(const DeviceMesh& dm, bool lower, const double* A, const double* v, const double* x0,
+                        double sign, double* y, cudaStream_t s) {
+  return tri_rows_t<double>(dm, lower, A, v, x0, sign, y, s);
+}
+cudaError_t la_tri_rows_f32(const DeviceMesh& dm, bool lower, const float* A, const double* v, const double* x0,
+                            double sign, double* y, cudaStream_t s) {
+  return tri_rows_t<float>(dm, lower, A, v, x0, sign, y, s);
+}
+
 cudaError_t la_block_diag_apply(int E, int bs, const double* D, const double* x, double* y, cudaStream_t s) {
   RowSet rs{0, 0, -1, E};
 #define ICX_DIAG_CASE(B) \

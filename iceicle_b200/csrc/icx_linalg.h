@@ -23,6 +23,11 @@ cudaError_t la_xpay(long long n, const double* x, double a, const double* y, dou
 // dst[b] = inv(src[blk_index[b]]) for b < nblk (bs x bs blocks); *flag set on a singular block
 cudaError_t la_block_invert(int nblk, int bs, const double* src, const int* blk_index, double* dst, int* flag,
                             cudaStream_t s);
+// y = x0 + sign * (strictly lower (lower = true) or strictly upper block part of A) v
+cudaError_t la_tri_rows(const DeviceMesh& dm, bool lower, const double* A, const double* v, const double* x0,
+                        double sign, double* y, cudaStream_t s);
+cudaError_t la_tri_rows_f32(const DeviceMesh& dm, bool lower, const float* A, const double* v, const double* x0,
+                            double sign, double* y, cudaStream_t s);
 cudaError_t la_block_diag_apply(int E, int bs, const double* D, const double* x, double* y, cudaStream_t s);
 // block-ILU(0) on the element block pattern in natural order, scheduled by
 // levels: order lists the elements by ascending level (the anti-diagonal

@@ -32,6 +32,9 @@ struct icx_solver_work {
   double* ustep = nullptr;
   double* rwork = nullptr;
   double* pct = nullptr;    // scratch of the preconditioner apply
+  double* pct2 = nullptr;
+  double* pct3 = nullptr;
+  int sweeps = 2;           // Jacobi sweeps per triangle (preconditioner 4)
   float* vals32 = nullptr;  // mixed precision: FP32 copies of the Jacobian and the preconditioner
   float* pc32 = nullptr;
   float* uinv32 = nullptr;
@@ -83,7 +86,7 @@ icx_status ensure_work(icx_ctx* c, int m) {
   CK(cudaMalloc((void**)&w->pc, vb));
   CK(cudaMalloc((void**)&w->uinv, sizeof(double) * (size_t)dm.E * bs * bs));
   CK(cudaMalloc((void**)&w->V, sizeof(double) * (size_t)(m + 1) * n));
-  double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork, &w->pct};
+  double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork, &w->pct, &w->pct2, &w->pct3};
   for (double** p : vecs) CK(cudaMalloc((void**)p, sizeof(double) * n));
   CK(cudaMalloc((void**)&w->dh, sizeof(double) * 2 * (m + 2)));
   CK(cudaMalloc((void**)&w->flag, sizeof(int)));
@@ -132,13 +135,54 @@ icx_status ensure_mixed(icx_ctx* c) {
   return ICX_OK;
 }
 
+cudaError_t diag_apply(icx_ctx* c, bool mixed, const double* D, const float* D32, const double* x, double* z,
+                       cudaStream_t s) {
+  return mixed ? icx::la_block_diag_apply_f32(c->dm.E, c->sw->bs, D32, x, z, s)
+               : icx::la_block_diag_apply(c->dm.E, c->sw->bs, D, x, z, s);
+}
+
+cudaError_t tri_rows(icx_ctx* c, bool mixed, bool lower, const double* v, const double* x0, double* y,
+                     cudaStream_t s) {
+  icx_solver_work* w = c->sw;
+  return mixed ? icx::la_tri_rows_f32(c->dm, lower, w->pc32, v, x0, -1.0, y, s)
+               : icx::la_tri_rows(c->dm, lower, w->pc, v, x0, -1.0, y, s);
+}
+
 // z = M^-1 x (mixed: from the FP32 copies, FP32 accumulation)
 cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* z, cudaStream_t s) {
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
-  if (kind == 1)
-    return mixed ? icx::la_block_diag_apply_f32(dm.E, w->bs, w->pc32, x, z, s)
-                 : icx::la_block_diag_apply(dm.E, w->bs, w->pc, x, z, s);
+  if (kind == 1) return diag_apply(c, mixed, w->pc, w->pc32, x, z, s);
+  if (kind == 3) {
+    // one Richardson step on block-Jacobi: z = G (2x - J G x)
+    cudaError_t e = diag_apply(c, mixed, w->pc, w->pc32, x, w->pct, s);
+    if (e == cudaSuccess)
+      e = mixed ? icx::launch_bsr_spmv_f32(dm, w->vals32, w->pct, w->pct2, s)
+                : icx::launch_bsr_spmv(dm, w->vals, w->pct, w->pct2, s);
+    if (e == cudaSuccess) e = icx::la_axpby(w->n, 2.0, x, -1.0, w->pct2, s);
+    if (e == cudaSuccess) e = diag_apply(c, mixed, w->pc, w->pc32, w->pct2, z, s);
+    return e;
+  }
+  if (kind == 4) {
+    // ILU(0) factors, each triangular solve replaced by `sweeps` Jacobi sweeps:
+    // f <- x - L f, then y <- inv(U_ee) f - (inv(U_ee) U) y
+    const int sw = w->sweeps;
+    const double* cur = x;
+    cudaError_t e = cudaSuccess;
+    for (int k = 1; k <= sw && e == cudaSuccess; ++k) {
+      double* out = (k & 1) ? w->pct : w->pct2;
+      e = tri_rows(c, mixed, true, cur, x, out, s);
+      cur = out;
+    }
+    if (e == cudaSuccess) e = diag_apply(c, mixed, w->uinv, w->uinv32, cur, sw == 0 ? z : w->pct3, s);
+    cur = w->pct3;
+    for (int k = 1; k <= sw && e == cudaSuccess; ++k) {
+      double* out = k == sw ? z : ((k & 1) ? w->pct : w->pct2);
+      e = tri_rows(c, mixed, false, cur, w->pct3, out, s);
+      cur = out;
+    }
+    return e;
+  }
   if (kind == 2) {
     if (mixed)
       return icx::la_ilu_apply_flow_f32(dm, w->order, w->pc32, w->uinv32, x, z, w->pct, w->cnt, w->cnt + dm.E,
@@ -157,16 +201,17 @@ cudaError_t build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
   const long long nv = (long long)dm.nnzb * w->bs * w->bs, nd = (long long)dm.E * w->bs * w->bs;
   cudaError_t e = cudaMemsetAsync(w->flag, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
-  if (kind == 1) e = icx::la_block_invert(dm.E, w->bs, w->vals, dm.bsr_diag, w->pc, w->flag, s);
-  if (kind == 2) {
+  const bool jac = kind == 1 || kind == 3, ilu = kind == 2 || kind == 4;
+  if (jac) e = icx::la_block_invert(dm.E, w->bs, w->vals, dm.bsr_diag, w->pc, w->flag, s);
+  if (ilu) {
     e = cudaMemcpyAsync(w->pc, w->vals, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess) e = icx::la_ilu_factor(dm, w->order, w->lvl_off, w->pc, w->uinv, w->flag, s);
   }
   if (e != cudaSuccess || !mixed) return e;
   e = icx::la_d2f(nv, w->vals, w->vals32, s);
-  if (e == cudaSuccess && kind == 1) e = icx::la_d2f(nd, w->pc, w->pc32, s);
-  if (e == cudaSuccess && kind == 2) e = icx::la_d2f(nv, w->pc, w->pc32, s);
-  if (e == cudaSuccess && kind == 2) e = icx::la_d2f(nd, w->uinv, w->uinv32, s);
+  if (e == cudaSuccess && jac) e = icx::la_d2f(nd, w->pc, w->pc32, s);
+  if (e == cudaSuccess && ilu) e = icx::la_d2f(nv, w->pc, w->pc32, s);
+  if (e == cudaSuccess && ilu) e = icx::la_d2f(nd, w->uinv, w->uinv32, s);
   return e;
 }
 
@@ -330,6 +375,7 @@ icx_status icx_newton_default_options(icx_newton_options* o) {
   o->preconditioner = 2;     // block-ILU(0)
   o->verbosity = 0;
   o->precision = 0;          // all FP64
+  o->pc_sweeps = 2;
   return ICX_OK;
 }
 
@@ -337,8 +383,8 @@ icx_status icx_gmres_solve(icx_ctx* c, const double* d_vals, const double* d_b, 
                            double rtol, int preconditioner, int* iterations, double* relres, void* stream) {
   if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
   if (!d_vals || !d_b || !d_x) return set_err(c, ICX_ERR_INVALID, "null device pointer");
-  if (restart < 1 || restart > 60 || preconditioner < 0 || preconditioner > 2)
-    return set_err(c, ICX_ERR_INVALID, "restart must be in 1..60 and preconditioner in 0..2");
+  if (restart < 1 || restart > 60 || preconditioner < 0 || preconditioner > 4)
+    return set_err(c, ICX_ERR_INVALID, "restart must be in 1..60 and preconditioner in 0..4");
   cudaStream_t s = (cudaStream_t)stream;
   icx_status st = ensure_work(c, restart);
   if (st != ICX_OK) return st;
@@ -361,8 +407,12 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   if (opt->gmres_restart < 1 || opt->gmres_restart > 60) return set_err(c, ICX_ERR_INVALID, "restart in 1..60");
   cudaStream_t s = 0;
   if (opt->precision < 0 || opt->precision > 1) return set_err(c, ICX_ERR_INVALID, "precision must be 0 or 1");
+  if (opt->preconditioner < 0 || opt->preconditioner > 4) return set_err(c, ICX_ERR_INVALID, "preconditioner in 0..4");
+  if (opt->preconditioner == 4 && (opt->pc_sweeps < 0 || opt->pc_sweeps > 16))
+    return set_err(c, ICX_ERR_INVALID, "pc_sweeps in 0..16");
   icx_status st = ensure_work(c, opt->gmres_restart);
   if (st != ICX_OK) return st;
+  c->sw->sweeps = opt->pc_sweeps;
   const bool mixed = opt->precision == 1;
   if (mixed && (st = ensure_mixed(c)) != ICX_OK) return st;
   icx_solver_work* w = c->sw;

@@ -88,8 +88,8 @@ def ns_mms_params(gamma=1.4, Pr=0.72, mu=0.01, mach=0.3, A=0.1, u0=1.0, v0=0.5):
 
 
 def ns_mms_config(nx=128, ny=128, p=3, geo_order=2, seed=4321, device=0, perturb=0.05, interior_penalty=True,
-                  state_noise=1e-3):
-    prm = ns_mms_params()
+                  state_noise=1e-3, mu=0.01):
+    prm = ns_mms_params(mu=mu)
     ctx = Context(device)
     ctx.mesh_uniform((nx, ny), (0.0, 0.0), (1.0, 1.0), geo_order, (DIRICHLET,) * 4, (0,) * 4)
     coords = lattice_coords((nx, ny), geo_order)

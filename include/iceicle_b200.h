@@ -206,7 +206,8 @@ typedef struct icx_newton_options {
   int gmres_restart;       /* GMRES(m) restart length */
   int gmres_max_it;        /* total inner iterations per Newton step */
   double gmres_rtol;       /* relative tolerance of the linear solve */
-  int preconditioner;      /* 0 none, 1 block-Jacobi, 2 block-ILU0 */
+  int preconditioner;      /* 0 none, 1 block-Jacobi, 2 block-ILU0, 3 two-step block-Jacobi
+                              G (2 I - J G), 4 block-ILU0 factors with Jacobi-sweep triangular solves */
   int verbosity;
   /* 0: all FP64. 1: mixed - the linear solves read FP32 copies of the
    * Jacobian (SpMV) and of the preconditioner (block inverses / ILU factors,
@@ -214,6 +215,9 @@ typedef struct icx_newton_options {
    * Hessenberg and Givens rotations, the Newton residual, its norm and the
    * line search stay FP64, so the converged state is judged in FP64. */
   int precision;
+  /* preconditioner 4 (block-ILU(0) factors applied by Jacobi sweeps): the
+   * sweeps per triangular solve */
+  int pc_sweeps;
 } icx_newton_options;
 
 typedef struct icx_newton_report {
