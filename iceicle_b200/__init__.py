@@ -68,7 +68,18 @@ class ExplicitReport(C.Structure):
 class NewtonReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("r0", C.c_double), ("r_final", C.c_double),
                 ("linear_iterations_total", C.c_int), ("residual_history", C.c_double * 64),
-                ("alpha_history", C.c_double * 64)]
+                ("alpha_history", C.c_double * 64), ("pc_fallbacks", C.c_int),
+                ("linear_iterations", C.c_int * 64)]
+
+
+class LpcTrainOptions(C.Structure):
+    _fields_ = [("steps", C.c_int), ("batch", C.c_int), ("random", C.c_int), ("sweeps", C.c_int),
+                ("lr", C.c_double), ("seed", C.c_ulonglong)]
+
+
+class LpcTrainReport(C.Structure):
+    _fields_ = [("steps", C.c_int), ("loss_first", C.c_double), ("loss_last", C.c_double),
+                ("loss_history", C.c_double * 64)]
 
 
 _lib = None
@@ -112,6 +123,16 @@ def lib():
             "icx_mass_inverse_apply": (C.c_int, [vp, vp, vp, vp]),
             "icx_newton_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport)]),
             "icx_basis_node_coords": (C.c_int, [vp, vp]),
+            "icx_krylov_samples": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                                             vp, ip, ip, dp]),
+            "icx_lpc_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_ulonglong]),
+            "icx_lpc_destroy": (None, [vp]),
+            "icx_lpc_info": (C.c_int, [vp, ip, ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+            "icx_lpc_get_params": (C.c_int, [vp, vp]),
+            "icx_lpc_set_params": (C.c_int, [vp, vp]),
+            "icx_lpc_attach": (C.c_int, [vp, vp]),
+            "icx_lpc_forward": (C.c_int, [vp, vp, vp]),
+            "icx_lpc_train": (C.c_int, [vp, vp, C.c_int, vp, C.POINTER(LpcTrainOptions), C.POINTER(LpcTrainReport)]),
             "icx_write_restart": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_char_p]),
             "icx_read_restart": (C.c_int, [vp, vp, C.c_char_p, C.c_int, C.c_char_p]),
             "icx_write_vtu": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_char_p, C.c_char_p,
@@ -392,6 +413,34 @@ class Context:
         self._check(lib().icx_write_vtu_mdg(self._h, _ptr(ic), int(itime), d, cn, self._names(names),
                                             int(precision)), "write_vtu_mdg")
 
+    def krylov_samples(self, vals, b, x, samples, every=8, restart=30, maxit=2000, rtol=1e-5, preconditioner=2):
+        """GMRES on J = vals from a zero guess that copies restart residuals and
+        every `every`-th Arnoldi vector into samples ([cap][n_dof] FP64 device
+        tensor); returns (n_samples, iterations, relres)"""
+        ns, it, rr = C.c_int(), C.c_int(), C.c_double()
+        st = lib().icx_krylov_samples(self._h, _ptr(vals), _ptr(b), _ptr(x), restart, maxit, rtol, preconditioner,
+                                      every, samples.shape[0], _ptr(samples), C.byref(ns), C.byref(it), C.byref(rr))
+        self._check(st, "krylov_samples")
+        return ns.value, it.value, rr.value
+
+    def lpc_attach(self, model):
+        """use a LearnedPreconditioner for Newton preconditioner 5 (None: detach)"""
+        self._check(lib().icx_lpc_attach(self._h, None if model is None else model._h), "lpc_attach")
+        self._lpc = model
+
+    def lpc_forward(self, vals, corr=None):
+        """the attached model's correction blocks for Jacobian vals"""
+        self._check(lib().icx_lpc_forward(self._h, _ptr(vals), None if corr is None else _ptr(corr)), "lpc_forward")
+
+    def lpc_train(self, vals, samples, n_samples, steps=100, batch=4, random=0, sweeps=1, lr=1e-3, seed=0):
+        """Adam steps of the attached model on Jacobian vals and residual
+        samples (`random` of each batch's vectors are seeded Gaussian ones)"""
+        o = LpcTrainOptions(steps, batch, random, sweeps, lr, seed)
+        rep = LpcTrainReport()
+        self._check(lib().icx_lpc_train(self._h, _ptr(vals), int(n_samples), _ptr(samples), C.byref(o),
+                                        C.byref(rep)), "lpc_train")
+        return rep
+
     def mfnk_solve(self, u, options=None):
         """matrix-free Newton-Krylov on u (device, FP64, in place); returns the report"""
         opt = options or default_newton_options()
@@ -412,6 +461,66 @@ class Context:
 
 VTU_SOLUTION = 0
 VTU_RESIDUAL = 1
+
+
+class LearnedPreconditioner:
+    """icx_lpc: the MLP of the learned block preconditioner (block size bs,
+    `hidden` units per hidden layer) on one device."""
+
+    def __init__(self, bs, hidden=256, device=0, seed=0):
+        self._h = C.c_void_p()
+        st = lib().icx_lpc_create(C.byref(self._h), device, bs, hidden, seed)
+        if st != 0:
+            raise IcxError(st, "icx_lpc_create")
+        self.bs, self.hidden, self.device = bs, hidden, device
+
+    def close(self):
+        if self._h:
+            lib().icx_lpc_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n_params(self):
+        n = C.c_longlong()
+        lib().icx_lpc_info(self._h, None, None, C.byref(n), None)
+        return n.value
+
+    @property
+    def steps(self):
+        n = C.c_longlong()
+        lib().icx_lpc_info(self._h, None, None, None, C.byref(n))
+        return n.value
+
+    def get_params(self):
+        p = np.zeros(self.n_params, dtype=np.float32)
+        st = lib().icx_lpc_get_params(self._h, p.ctypes.data_as(C.c_void_p))
+        if st != 0:
+            raise IcxError(st, "icx_lpc_get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.n_params:
+            raise ValueError(f"{p.size} parameters, the model has {self.n_params}")
+        st = lib().icx_lpc_set_params(self._h, p.ctypes.data_as(C.c_void_p))
+        if st != 0:
+            raise IcxError(st, "icx_lpc_set_params")
+
+    def save(self, path):
+        np.savez_compressed(path, bs=self.bs, hidden=self.hidden, params=self.get_params())
+
+    @classmethod
+    def load(cls, path, device=0):
+        z = np.load(path)
+        m = cls(int(z["bs"]), int(z["hidden"]), device)
+        m.set_params(z["params"])
+        return m
 
 
 def batch(parts, device=0):

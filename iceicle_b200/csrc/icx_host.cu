@@ -321,6 +321,7 @@ void icx_destroy(icx_ctx* c) {
   icx::free_solver_work(c);
   icx::free_mdg(c);
   icx::free_explicit(c);
+  icx::free_lpc_work(c);
   free_dev(c->dm);
   for (void* p : c->scratch)
     if (p) cudaFree(p);

@@ -103,6 +103,8 @@ struct icx_ctx {
   struct icx_solver_work* sw = nullptr;  // Newton / GMRES buffers (icx_solver.cu)
   struct icx_mdg_state* mdg = nullptr;   // MDG-ICE selection and Jacobian pattern (icx_mdg.cu)
   struct icx_explicit_work* ew = nullptr; // explicit time-stepping buffers (icx_explicit.cu)
+  struct icx_lpc* lpc = nullptr;          // learned block preconditioner model (attached, not owned)
+  struct icx_lpc_work* lpcw = nullptr;    // its per-context buffers (icx_lpc.cu)
 };
 
 namespace icx {
@@ -139,4 +141,15 @@ void free_explicit(icx_ctx* c);
 void gauss_legendre_points(int n, double* x, double* w);
 // physical point of reference point xi in element e (geometry transformation, icx_host.cu)
 void element_point(const icx_ctx* c, int e, const double xi[2], double x[2]);
+// learned block preconditioner (icx_lpc.cu): features and correction from the
+// FP64 Jacobian, the correction z = (I + C) y, and the release of its buffers
+cudaError_t lpc_build(icx_ctx* c, const double* vals, cudaStream_t s);
+cudaError_t lpc_apply(icx_ctx* c, const double* y, double* z, cudaStream_t s);
+void free_lpc_work(icx_ctx* c);
+// solver internals the training uses (icx_solver.cu): copy a Jacobian into the
+// solver and build preconditioner `kind` with mixed-precision copies; apply it;
+// the FP32 copy of the Jacobian
+icx_status solver_prepare_pc(icx_ctx* c, const double* vals, int kind, int sweeps);
+cudaError_t solver_apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* z, cudaStream_t s);
+const float* solver_vals32(icx_ctx* c);
 }  // namespace icx

@@ -426,6 +426,37 @@ cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, const int* order, const 
   return ilu_apply_flow_t<float>(dm, order, LU, Uinv, x, y, f, cnt_f, cnt_b, epoch, err, s);
 }
 
+cudaError_t la_block_diag_correct_f32(int E, int bs, const float* D, const double* y, double* z, cudaStream_t s) {
+  RowSet rs{0, 0, -1, E};
+#define ICX_CORR_CASE(B) \
+  if (bs == B) return launch_block_rows<B, BR_DIAG, float>(rs, nullptr, nullptr, D, y, y, 1.0, z, s);
+  ICX_BLOCK_SIZES(ICX_CORR_CASE)
+#undef ICX_CORR_CASE
+  return cudaErrorInvalidValue;
+}
+
+__global__ void dot_to_kernel(long long n, const double* __restrict__ x, const double* __restrict__ y,
+                              double* __restrict__ out) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s += x[i] * y[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(out, red[0]);
+}
+
+cudaError_t la_dot_to(long long n, const double* x, const double* y, double* d_out, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_out, 0, sizeof(double), s);
+  if (e != cudaSuccess) return e;
+  dot_to_kernel<<<592, 256, 0, s>>>(n, x, y, d_out);
+  return cudaGetLastError();
+}
+
 cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s) {
   RowSet rs{0, 0, -1, E};
 #define ICX_DIAG32_CASE(B) \
@@ -490,6 +521,7 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
   GCK(cudaMemcpyAsync(kb.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   double beta = bnorm;
   int total = 0;
+  std::vector<double> cycle_beta{bnorm};
   while (true) {
     GCK(la_axpby(n, 1.0 / beta, kb.r, 0.0, kb.V, s));
     std::fill(g.begin(), g.end(), 0.0);
@@ -499,6 +531,10 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
     for (; j < m && total < maxit; ++j) {
       double* vj = kb.V + (size_t)j * n;
       double* vj1 = kb.V + (size_t)(j + 1) * n;
+      if (kb.samples && kb.sample_every > 0 && kb.sample_count < kb.sample_cap && j > 0 &&
+          total % kb.sample_every == 0)
+        GCK(cudaMemcpyAsync(kb.samples + (size_t)kb.sample_count++ * n, vj, sizeof(double) * n,
+                            cudaMemcpyDeviceToDevice, s));
       if (M) {
         GCK((*M)(vj, kb.z));
         GCK(A(kb.z, vj1));
@@ -554,9 +590,15 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
     }
     GCK(A(x, kb.w));
     GCK(la_xpay(n, b, -1.0, kb.w, kb.r, s));
+    if (kb.samples && kb.sample_count < kb.sample_cap)
+      GCK(cudaMemcpyAsync(kb.samples + (size_t)kb.sample_count++ * n, kb.r, sizeof(double) * n,
+                          cudaMemcpyDeviceToDevice, s));
     beta = la_norm(*kb.lw, n, kb.r, kb.dh, s);
     *relres = beta / bnorm;
     if (beta <= tol || total >= maxit || resid <= tol) break;
+    cycle_beta.push_back(beta);
+    const int nc = (int)cycle_beta.size() - 1;
+    if (kb.stall_cycles > 0 && nc >= kb.stall_cycles && beta > 0.5 * cycle_beta[nc - kb.stall_cycles]) break;
   }
   *iters = total;
   return ICX_OK;

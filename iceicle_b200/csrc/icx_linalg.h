@@ -29,6 +29,10 @@ cudaError_t la_tri_rows(const DeviceMesh& dm, bool lower, const double* A, const
 cudaError_t la_tri_rows_f32(const DeviceMesh& dm, bool lower, const float* A, const double* v, const double* x0,
                             double sign, double* y, cudaStream_t s);
 cudaError_t la_block_diag_apply(int E, int bs, const double* D, const double* x, double* y, cudaStream_t s);
+// z = y + D y, D block diagonal in FP32 (FP32 accumulation)
+cudaError_t la_block_diag_correct_f32(int E, int bs, const float* D, const double* y, double* z, cudaStream_t s);
+// *d_out = x . y (device scalar, overwritten)
+cudaError_t la_dot_to(long long n, const double* x, const double* y, double* d_out, cudaStream_t s);
 // block-ILU(0) on the element block pattern in natural order, scheduled by
 // levels: order lists the elements by ascending level (the anti-diagonal
 // i + j of the element in its grid), lvl_off[l]..lvl_off[l+1] the elements of
@@ -68,6 +72,13 @@ struct KrylovBuffers {
   double* r = nullptr;
   double* dh = nullptr;  // >= m + 2 device doubles
   LinalgWork* lw = nullptr;
+  // optional Krylov samples: the true residual at every restart and every
+  // `sample_every`-th Arnoldi vector, copied into samples[count] while count < cap
+  double* samples = nullptr;
+  int sample_cap = 0, sample_every = 0, sample_count = 0;
+  // stall test (0: off): stop when the residual after a restart cycle is above
+  // half the residual `stall_cycles` cycles earlier
+  int stall_cycles = 0;
 };
 using LinOp = std::function<cudaError_t(const double* x, double* y)>;
 double la_norm(LinalgWork& lw, long long n, const double* x, double* d_scratch, cudaStream_t s);

@@ -34,6 +34,7 @@ struct icx_solver_work {
   double* pct = nullptr;    // scratch of the preconditioner apply
   double* pct2 = nullptr;
   double* pct3 = nullptr;
+  double* pct4 = nullptr;
   int sweeps = 2;           // Jacobi sweeps per triangle (preconditioner 4)
   float* vals32 = nullptr;  // mixed precision: FP32 copies of the Jacobian and the preconditioner
   float* pc32 = nullptr;
@@ -86,7 +87,7 @@ icx_status ensure_work(icx_ctx* c, int m) {
   CK(cudaMalloc((void**)&w->pc, vb));
   CK(cudaMalloc((void**)&w->uinv, sizeof(double) * (size_t)dm.E * bs * bs));
   CK(cudaMalloc((void**)&w->V, sizeof(double) * (size_t)(m + 1) * n));
-  double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork, &w->pct, &w->pct2, &w->pct3};
+  double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork, &w->pct, &w->pct2, &w->pct3, &w->pct4};
   for (double** p : vecs) CK(cudaMalloc((void**)p, sizeof(double) * n));
   CK(cudaMalloc((void**)&w->dh, sizeof(double) * 2 * (m + 2)));
   CK(cudaMalloc((void**)&w->flag, sizeof(int)));
@@ -163,6 +164,13 @@ cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* 
     if (e == cudaSuccess) e = diag_apply(c, mixed, w->pc, w->pc32, w->pct2, z, s);
     return e;
   }
+  if (kind == 5) {
+    // learned: z = (I + C) y, y from the ILU(0) factors by `sweeps` Jacobi
+    // sweeps per triangle, or by the exact triangular solves when sweeps = 0
+    cudaError_t e = apply_pc(c, w->sweeps > 0 ? 4 : 2, mixed, x, w->pct4, s);
+    if (e == cudaSuccess) e = icx::lpc_apply(c, w->pct4, z, s);
+    return e;
+  }
   if (kind == 4) {
     // ILU(0) factors, each triangular solve replaced by `sweeps` Jacobi sweeps:
     // f <- x - L f, then y <- inv(U_ee) f - (inv(U_ee) U) y
@@ -201,7 +209,8 @@ cudaError_t build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
   const long long nv = (long long)dm.nnzb * w->bs * w->bs, nd = (long long)dm.E * w->bs * w->bs;
   cudaError_t e = cudaMemsetAsync(w->flag, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
-  const bool jac = kind == 1 || kind == 3, ilu = kind == 2 || kind == 4;
+  const bool jac = kind == 1 || kind == 3, ilu = kind == 2 || kind == 4 || kind == 5;
+  if (kind == 5 && (e = icx::lpc_build(c, w->vals, s)) != cudaSuccess) return e;
   if (jac) e = icx::la_block_invert(dm.E, w->bs, w->vals, dm.bsr_diag, w->pc, w->flag, s);
   if (ilu) {
     e = cudaMemcpyAsync(w->pc, w->vals, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s);
@@ -219,7 +228,8 @@ cudaError_t build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
 // (mixed: operator and preconditioner from the FP32 copies; the Krylov
 // vectors, Hessenberg and Givens rotations stay FP64)
 icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, const double* b, double* x,
-                 int* iters, double* relres, cudaStream_t s) {
+                 int* iters, double* relres, cudaStream_t s, double* samples = nullptr, int sample_cap = 0,
+                 int sample_every = 0, int* sample_count = nullptr) {
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
   icx::KrylovBuffers kb;
@@ -231,6 +241,17 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
   kb.r = w->r;
   kb.dh = w->dh;
   kb.lw = &w->lw;
+  kb.samples = samples;
+  kb.sample_cap = sample_cap;
+  kb.sample_every = sample_every;
+  // the parallel and learned preconditioners give up on a stalled solve
+  // (block-ILU(0) then takes the step)
+  kb.stall_cycles = pc >= 3 ? 10 : 0;
+  struct CountOut {
+    int* dst;
+    icx::KrylovBuffers* kb;
+    ~CountOut() { if (dst) *dst = kb->sample_count; }
+  } count_out{sample_count, &kb};
   icx::LinOp A = [&](const double* xin, double* yout) {
     return mixed ? icx::launch_bsr_spmv_f32(dm, w->vals32, xin, yout, s) : icx::launch_bsr_spmv(dm, w->vals, xin, yout, s);
   };
@@ -401,15 +422,42 @@ icx_status icx_gmres_solve(icx_ctx* c, const double* d_vals, const double* d_b, 
   return rr <= rtol ? ICX_OK : ICX_ERR_NOT_CONVERGED;
 }
 
+icx_status icx_krylov_samples(icx_ctx* c, const double* d_vals, const double* d_b, double* d_x, int restart, int maxit,
+                              double rtol, int preconditioner, int every, int capacity, double* d_samples,
+                              int* n_samples, int* iterations, double* relres) {
+  if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
+  if (!d_vals || !d_b || !d_x || !d_samples || capacity < 1 || every < 1)
+    return set_err(c, ICX_ERR_INVALID, "null pointer, capacity < 1 or every < 1");
+  if (restart < 1 || restart > 60 || preconditioner < 0 || preconditioner > 4)
+    return set_err(c, ICX_ERR_INVALID, "restart must be in 1..60 and preconditioner in 0..4");
+  cudaStream_t s = 0;
+  icx_status st = ensure_work(c, restart);
+  if (st != ICX_OK) return st;
+  icx_solver_work* w = c->sw;
+  CK(cudaMemcpyAsync(w->vals, d_vals, sizeof(double) * (size_t)c->dm.nnzb * w->bs * w->bs, cudaMemcpyDeviceToDevice,
+                     s));
+  CK(build_pc(c, preconditioner, false, s));
+  int it = 0, cnt = 0;
+  double rr = 0.0;
+  st = gmres(c, preconditioner, false, restart, maxit, rtol, d_b, d_x, &it, &rr, s, d_samples, capacity, every, &cnt);
+  SYNC_AT("krylov samples");
+  if (n_samples) *n_samples = cnt;
+  if (iterations) *iterations = it;
+  if (relres) *relres = rr;
+  return st;
+}
+
 icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* opt, icx_newton_report* rep) {
   if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
   if (!d_u || !opt) return set_err(c, ICX_ERR_INVALID, "null argument");
   if (opt->gmres_restart < 1 || opt->gmres_restart > 60) return set_err(c, ICX_ERR_INVALID, "restart in 1..60");
   cudaStream_t s = 0;
   if (opt->precision < 0 || opt->precision > 1) return set_err(c, ICX_ERR_INVALID, "precision must be 0 or 1");
-  if (opt->preconditioner < 0 || opt->preconditioner > 4) return set_err(c, ICX_ERR_INVALID, "preconditioner in 0..4");
-  if (opt->preconditioner == 4 && (opt->pc_sweeps < 0 || opt->pc_sweeps > 16))
+  if (opt->preconditioner < 0 || opt->preconditioner > 5) return set_err(c, ICX_ERR_INVALID, "preconditioner in 0..5");
+  if (opt->preconditioner >= 4 && (opt->pc_sweeps < 0 || opt->pc_sweeps > 16))
     return set_err(c, ICX_ERR_INVALID, "pc_sweeps in 0..16");
+  if (opt->preconditioner == 5 && !c->lpc)
+    return set_err(c, ICX_ERR_INVALID, "preconditioner 5 needs a learned model (icx_lpc_attach)");
   icx_status st = ensure_work(c, opt->gmres_restart);
   if (st != ICX_OK) return st;
   c->sw->sweeps = opt->pc_sweeps;
@@ -448,6 +496,17 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
                &it, &rr, s);
     if (st != ICX_OK) return st;
     R->linear_iterations_total += it;
+    if (k < 64) R->linear_iterations[k] = it;
+    if (opt->preconditioner >= 3 && !(rr <= opt->gmres_rtol)) {
+      // the parallel / learned preconditioner missed the linear tolerance:
+      // this step is solved again with block-ILU(0)
+      ++R->pc_fallbacks;
+      CK(build_pc(c, 2, mixed, s));
+      st = gmres(c, 2, mixed, opt->gmres_restart, opt->gmres_max_it, opt->gmres_rtol, w->res, w->du, &it, &rr, s);
+      if (st != ICX_OK) return st;
+      R->linear_iterations_total += it;
+      if (k < 64) R->linear_iterations[k] += it;
+    }
     double alpha = 1.0;
     if (opt->linesearch != 0) {
       // phi(alpha) = |R(u - alpha du)|_2, non-finite -> 1e9 (petsc_newton.hpp:262-293)
@@ -588,3 +647,26 @@ extern "C" icx_status icx_mfnk_solve(icx_ctx* c, double* d_u, const icx_newton_o
   R->r_final = rk;
   return converged ? ICX_OK : ICX_ERR_NOT_CONVERGED;
 }
+
+namespace icx {
+
+icx_status solver_prepare_pc(icx_ctx* c, const double* vals, int kind, int sweeps) {
+  icx_status st = ensure_work(c, 30);
+  if (st != ICX_OK) return st;
+  if ((st = ensure_mixed(c)) != ICX_OK) return st;
+  icx_solver_work* w = c->sw;
+  w->sweeps = sweeps;
+  cudaStream_t s = 0;
+  CK(cudaMemcpyAsync(w->vals, vals, sizeof(double) * (size_t)c->dm.nnzb * w->bs * w->bs, cudaMemcpyDeviceToDevice, s));
+  CK(build_pc(c, kind, true, s));
+  SYNC_AT("preconditioner");
+  return ICX_OK;
+}
+
+cudaError_t solver_apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* z, cudaStream_t s) {
+  return apply_pc(c, kind, mixed, x, z, s);
+}
+
+const float* solver_vals32(icx_ctx* c) { return c->sw ? c->sw->vals32 : nullptr; }
+
+}  // namespace icx

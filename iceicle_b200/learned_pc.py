@@ -1,0 +1,121 @@
+"""Training and evaluation of the learned block preconditioner (Newton
+preconditioner 5) on the 2D compressible Navier-Stokes manufactured solution:
+n x n quadrilaterals on [0,1]^2 with geometry order 2, p = 2 (9 basis
+functions x 4 conserved variables: 36 x 36 Jacobian blocks), Van Leer flux
+with interior penalty, nodes perturbed by a seeded smooth displacement, and a
+Reynolds number drawn per instance uniformly from [50, 500] (viscosity 1/Re).
+
+Training data are generated by the plain solver: at every Newton step of a
+training instance the FD Jacobian is formed and the plain GMRES(30) +
+block-ILU(0) solve of that step records Krylov residuals (its restart
+residuals and every k-th Arnoldi vector). The model then takes Adam steps on
+that Jacobian's samples before the Newton step is applied. Evaluation runs
+fresh seeds through the plain all-FP64 block-ILU(0) Newton solve and through
+the learned, mixed-precision one, both to an FP64 residual of 1e-10."""
+import time
+
+import numpy as np
+
+from . import LearnedPreconditioner, default_newton_options
+from .workloads import ns_mms_config
+
+BLOCK_SIZE = 36
+
+
+def instances(n, seed, re_range=(50.0, 500.0)):
+    """n seeded (mesh and state seed, Reynolds number) pairs"""
+    rng = np.random.default_rng(seed)
+    return [(int(rng.integers(1, 2**31 - 1)), float(rng.uniform(*re_range))) for _ in range(n)]
+
+
+def make_instance(seed, re, n=256, device=0):
+    return ns_mms_config(nx=n, ny=n, p=2, geo_order=2, seed=seed, device=device, mu=1.0 / re)
+
+
+def train(model, train_instances, n=256, samples=167, every=10, steps=150, batch=4, random=2, sweeps=2, lr=1e-3,
+          newton_steps=4, device=0, log=None):
+    """train `model` on the Newton steps of each instance; returns per-Jacobian
+    records (instance, step, |r|, samples, gmres iterations, first/last loss)"""
+    import torch
+    dev = torch.device("cuda", device)
+    out = []
+    for (seed, re) in train_instances:
+        wl = make_instance(seed, re, n, device)
+        ctx = wl.ctx
+        ctx.lpc_attach(model)
+        L = ctx.layout
+        bs = L.block_size
+        u = torch.from_numpy(wl.u0).to(dev)
+        res = torch.empty_like(u)
+        du = torch.empty_like(u)
+        vals = torch.empty(L.nnz_blocks * bs * bs, dtype=torch.float64, device=dev)
+        buf = torch.empty((samples, L.n_dof), dtype=torch.float64, device=dev)
+        for k in range(newton_steps):
+            ctx.form_jacobian_fd(u, res, vals)
+            rn = float(torch.linalg.vector_norm(res))
+            if rn <= 1e-10:
+                break
+            ns, its, rr = ctx.krylov_samples(vals, res, du, buf, every=every)
+            t0 = time.time()
+            rep = ctx.lpc_train(vals, buf, ns, steps=steps, batch=batch, random=random, sweeps=sweeps, lr=lr,
+                                seed=seed * 7919 + k)
+            rec = dict(seed=seed, re=re, newton_step=k, r=rn, samples=ns, gmres_its=its,
+                       loss_first=rep.loss_first, loss_last=rep.loss_last, train_s=time.time() - t0)
+            out.append(rec)
+            if log:
+                log(rec)
+            u -= du
+        ctx.lpc_attach(None)
+        del wl
+    return out
+
+
+def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0):
+    """one Newton solve of an instance to |r| <= 1e-10 (GMRES(30), Wolfe line
+    search), timed with CUDA events; returns (report dict, final state)"""
+    import torch
+    dev = torch.device("cuda", device)
+    opt = default_newton_options()
+    opt.preconditioner = preconditioner
+    opt.precision = precision
+    opt.pc_sweeps = sweeps
+    opt.gmres_max_it = 20000
+    if model is not None:
+        wl.ctx.lpc_attach(model)
+    u = torch.from_numpy(wl.u0).to(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    rep = wl.ctx.newton_solve(u, opt)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    if model is not None:
+        wl.ctx.lpc_attach(None)
+    return dict(s=e0.elapsed_time(e1) * 1e-3, newton_its=rep.iterations, gmres_its=rep.linear_iterations_total,
+                gmres_its_per_step=list(rep.linear_iterations[:rep.iterations]), r_final=rep.r_final,
+                converged=bool(rep.converged), pc_fallbacks=rep.pc_fallbacks), u.cpu().numpy()
+
+
+def evaluate(model, eval_instances, n=256, sweeps=2, device=0, log=None):
+    """plain all-FP64 block-ILU(0) against learned + mixed precision (and the
+    untrained parallel ILU as ablation) on fresh instances"""
+    out = []
+    for (seed, re) in eval_instances:
+        wl = make_instance(seed, re, n, device)
+        plain, u_plain = solve(wl, None, 2, 0, device=device)
+        learned, u_l = solve(wl, model, 5, 1, sweeps, device)
+        ablation, u_a = solve(wl, None, 4 if sweeps > 0 else 2, 1, sweeps, device)
+        scale = max(np.linalg.norm(u_plain), 1e-300)
+        rec = dict(seed=seed, re=re, plain_fp64_ilu0=plain, learned_mixed=learned, untrained_base_mixed=ablation,
+                   learned_vs_plain_state_l2=float(np.linalg.norm(u_l - u_plain) / scale),
+                   speedup_learned_mixed_vs_plain_fp64=plain["s"] / learned["s"],
+                   speedup_untrained_base_mixed_vs_plain_fp64=plain["s"] / ablation["s"])
+        out.append(rec)
+        if log:
+            log(rec)
+        del wl
+    return out
+
+
+def new_model(device=0, seed=0, hidden=256):
+    return LearnedPreconditioner(BLOCK_SIZE, hidden, device, seed)

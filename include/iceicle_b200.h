@@ -207,7 +207,10 @@ typedef struct icx_newton_options {
   int gmres_max_it;        /* total inner iterations per Newton step */
   double gmres_rtol;       /* relative tolerance of the linear solve */
   int preconditioner;      /* 0 none, 1 block-Jacobi, 2 block-ILU0, 3 two-step block-Jacobi
-                              G (2 I - J G), 4 block-ILU0 factors with Jacobi-sweep triangular solves */
+                              G (2 I - J G), 4 block-ILU0 factors with Jacobi-sweep triangular solves,
+                              5 learned: (I + C) times preconditioner 4, or times 2 when pc_sweeps = 0
+                              (icx_lpc_attach); a step whose linear solve misses gmres_rtol with 3-5
+                              is solved again with 2 */
   int verbosity;
   /* 0: all FP64. 1: mixed - the linear solves read FP32 copies of the
    * Jacobian (SpMV) and of the preconditioner (block inverses / ILU factors,
@@ -227,6 +230,10 @@ typedef struct icx_newton_report {
   int linear_iterations_total;
   double residual_history[64];
   double alpha_history[64];
+  int pc_fallbacks;  /* steps whose linear solve was redone with block-ILU(0) (preconditioners 3-5: the
+                        solve missed gmres_rtol, or stalled: under half the residual reduction over 10
+                        restart cycles) */
+  int linear_iterations[64]; /* GMRES iterations of each Newton step (fallback included) */
 } icx_newton_report;
 
 /* Linear solve J x = b with the BSR values d_vals (the KSPSolve of
@@ -292,6 +299,49 @@ icx_status icx_mass_inverse_apply(icx_ctx* ctx, const double* d_r, double* d_out
  * test for the concatenated residual. */
 icx_status icx_batch_create(icx_ctx** out, int device, int n_parts, icx_ctx* const* parts);
 icx_status icx_batch_offsets(const icx_ctx* batch, int* elem_offsets);
+
+/* Krylov samples for training the learned preconditioner: the GMRES solve of
+ * icx_gmres_solve (from a zero guess, FP64) that also copies the true residual
+ * at every restart and every `every`-th Arnoldi vector into d_samples
+ * ([capacity][n_dof], device) until it is full; *n_samples = copies made. */
+icx_status icx_krylov_samples(icx_ctx* ctx, const double* d_vals, const double* d_b, double* d_x, int restart, int maxit,
+                              double rtol, int preconditioner, int every, int capacity, double* d_samples,
+                              int* n_samples, int* iterations, double* relres);
+
+/* ---- learned block preconditioner (no counterpart in the reference): an MLP
+ * from each normalised Jacobian diagonal block J_ee / |J_ee|_F (bs x bs values)
+ * through two ReLU layers of `hidden` units to a bs x bs correction C_e; the
+ * Newton preconditioner 5 applies z = (I + C) y with y the block-ILU(0)
+ * factors applied by pc_sweeps Jacobi sweeps per triangle. BF16 products on
+ * the tensor cores with FP32 accumulation; FP32 master weights. */
+typedef struct icx_lpc icx_lpc;
+typedef struct icx_lpc_train_options {
+  int steps;               /* Adam steps on this Jacobian */
+  int batch;               /* residual samples per step */
+  int random;              /* of which this many are seeded Gaussian vectors instead of Krylov samples */
+  int sweeps;              /* Jacobi sweeps per triangle of the preconditioner being trained (0: exact ILU(0)) */
+  double lr;               /* Adam step size */
+  unsigned long long seed; /* sample selection */
+} icx_lpc_train_options;
+typedef struct icx_lpc_train_report {
+  int steps;
+  double loss_first, loss_last; /* mean of |r - J z(r)|^2 / |r|^2 over the step's samples */
+  double loss_history[64];
+} icx_lpc_train_report;
+icx_status icx_lpc_create(icx_lpc** out, int device, int block_size, int hidden, unsigned long long seed);
+void icx_lpc_destroy(icx_lpc* model);
+icx_status icx_lpc_info(const icx_lpc* model, int* block_size, int* hidden, long long* n_params, long long* steps);
+/* FP32 parameters W1 [hidden][bs^2], b1, W2 [hidden][hidden], b2, W3 [bs^2][hidden], b3 (host arrays) */
+icx_status icx_lpc_get_params(const icx_lpc* model, float* params);
+icx_status icx_lpc_set_params(icx_lpc* model, const float* params);
+/* use `model` (NULL: detach) for preconditioner 5 of this context; the model must outlive the attachment */
+icx_status icx_lpc_attach(icx_ctx* ctx, icx_lpc* model);
+/* the correction C ([n_elem][bs][bs] FP32, device; may be NULL) of the attached model for Jacobian d_vals */
+icx_status icx_lpc_forward(icx_ctx* ctx, const double* d_vals, float* d_corr);
+/* Adam steps of the attached model on Jacobian d_vals (FP64 BSR) and residual
+ * samples d_samples ([n_samples][n_dof], device) */
+icx_status icx_lpc_train(icx_ctx* ctx, const double* d_vals, int n_samples, const double* d_samples,
+                         const icx_lpc_train_options* opt, icx_lpc_train_report* rep);
 
 /* ---- restart files and VTU output (host files; d_u and d_ic are device
  * arrays). Not available on a batch. */

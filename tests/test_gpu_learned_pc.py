@@ -1,0 +1,146 @@
+"""The learned block preconditioner (Newton preconditioner 5) and the
+parallel preconditioners 3 and 4: the BF16 MLP against a torch FP32
+evaluation of the same network on BF16-rounded inputs, training lowering its
+loss, and Newton solves that reach the plain block-ILU(0) state."""
+import numpy as np
+import pytest
+import torch
+
+import iceicle_b200 as ib
+from specs import NS, Spec
+
+pytestmark = pytest.mark.gpu
+
+
+def _ns_ctx(nx=6, ny=5):
+    spec = Spec(pde=NS, nx=nx, ny=ny, g=2, p=2, ip=True, source=True, perturb=0.05)
+    ctx = spec.context()
+    from test_gpu_solver import _ns_mms_state
+    u0 = _ns_mms_state(ctx, 1e-2, 5)
+    return spec, ctx, u0
+
+
+def _jacobian(ctx, u):
+    L = ctx.layout
+    bs = L.block_size
+    vals = torch.empty(L.nnz_blocks * bs * bs, dtype=torch.float64, device="cuda")
+    res = torch.empty_like(u)
+    ctx.form_jacobian_fd(u, res, vals)
+    return vals, res
+
+
+def _bf(x):
+    return x.to(torch.bfloat16).to(torch.float32)
+
+
+def test_mlp_forward_matches_a_torch_fp32_evaluation():
+    """C = W3 relu(W2 relu(W1 x + b1) + b2) + b3 per element block, x = J_ee /
+    |J_ee|_F. The reference rounds x, the weights and both hidden activations
+    to BF16 as the kernels do and computes in FP32; the kernels accumulate in
+    FP32 in another order: 2e-2 of the largest output (BF16 has 8 bits)."""
+    spec, ctx, u0 = _ns_ctx()
+    m = ib.LearnedPreconditioner(36, 64, 0, seed=3)
+    p = m.get_params()
+    rng = np.random.default_rng(0)
+    D, H = 36 * 36, 64
+    oW3 = H * D + H + H * H + H
+    p[oW3:oW3 + D * H] = 0.05 * rng.standard_normal(D * H)
+    p[oW3 + D * H:] = 0.01 * rng.standard_normal(D)
+    p[H * D:H * D + H] = 0.1 * rng.standard_normal(H)
+    m.set_params(p)
+    ctx.lpc_attach(m)
+    u = torch.from_numpy(u0).cuda()
+    vals, _ = _jacobian(ctx, u)
+    E = ctx.layout.n_elem
+    corr = torch.empty(E * D, dtype=torch.float32, device="cuda")
+    ctx.lpc_forward(vals, corr)
+    torch.cuda.synchronize()
+    rp, ci = ctx.jacobian_pattern()
+    diag = np.array([rp[e] + int(np.nonzero(ci[rp[e]:rp[e + 1]] == e)[0][0]) for e in range(E)])
+    V = vals.view(-1, D)[torch.from_numpy(diag).cuda()]
+    X = _bf((V / V.norm(dim=1, keepdim=True)).float())
+    P = torch.from_numpy(p).cuda()
+    W1 = P[:H * D].view(H, D); b1 = P[H * D:H * D + H]
+    W2 = P[H * D + H:H * D + H + H * H].view(H, H); b2 = P[H * D + H + H * H:oW3]
+    W3 = P[oW3:oW3 + D * H].view(D, H); b3 = P[oW3 + D * H:]
+    h1 = _bf(torch.relu(X @ _bf(W1).T + b1))
+    h2 = _bf(torch.relu(h1 @ _bf(W2).T + b2))
+    ref = h2 @ _bf(W3).T + b3
+    got = corr.view(E, D)
+    assert (got - ref).abs().max().item() <= 2e-2 * ref.abs().max().item()
+    ctx.lpc_attach(None)
+
+
+def test_training_lowers_the_preconditioned_residual():
+    """Adam steps on Krylov residuals of one Jacobian lower the mean of
+    |r - J (I + C) ILU_1(r)|^2 / |r|^2 (first loss: the untrained model, C = 0)"""
+    spec, ctx, u0 = _ns_ctx()
+    m = ib.LearnedPreconditioner(36, 64, 0, seed=1)
+    ctx.lpc_attach(m)
+    u = torch.from_numpy(u0).cuda()
+    vals, res = _jacobian(ctx, u)
+    buf = torch.empty((48, ctx.layout.n_dof), dtype=torch.float64, device="cuda")
+    du = torch.empty_like(u)
+    ns, its, rr = ctx.krylov_samples(vals, res, du, buf, every=2, rtol=1e-8)
+    assert ns >= 8
+    rep = ctx.lpc_train(vals, buf, ns, steps=60, batch=4, sweeps=1, lr=2e-3, seed=2)
+    hist = list(rep.loss_history[:60])
+    assert np.isfinite(hist).all()
+    assert np.mean(hist[-10:]) < 0.9 * np.mean(hist[:5]), hist
+    assert m.steps == 60
+    ctx.lpc_attach(None)
+
+
+@pytest.mark.parametrize("pc,prec,sweeps", [(3, 0, 0), (4, 0, 1), (4, 1, 2), (5, 1, 1), (5, 0, 2)])
+def test_parallel_and_learned_preconditioners_reach_the_ilu0_state(pc, prec, sweeps):
+    """the Newton solve with preconditioner pc converges to the state of the
+    plain FP64 block-ILU(0) solve (both to |r| <= 1e-10; states to 1e-9,
+    relative L2) without falling back"""
+    spec, ctx, u0 = _ns_ctx()
+    m = ib.LearnedPreconditioner(36, 64, 0, seed=4)
+    if pc == 5:
+        ctx.lpc_attach(m)
+    o = ib.default_newton_options()
+    o.gmres_max_it = 5000
+    u1 = torch.from_numpy(u0.copy()).cuda()
+    r1 = ctx.newton_solve(u1, o)
+    o2 = ib.default_newton_options()
+    o2.gmres_max_it = 5000
+    o2.preconditioner, o2.precision, o2.pc_sweeps = pc, prec, sweeps
+    u2 = torch.from_numpy(u0.copy()).cuda()
+    r2 = ctx.newton_solve(u2, o2)
+    assert r1.converged and r2.converged
+    assert r2.pc_fallbacks == 0
+    a, b = u1.cpu().numpy(), u2.cpu().numpy()
+    assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(a)
+    ctx.lpc_attach(None)
+
+
+def test_missed_linear_tolerance_falls_back_to_ilu0():
+    spec, ctx, u0 = _ns_ctx()
+    o = ib.default_newton_options()
+    o.preconditioner, o.gmres_max_it, o.kmax = 3, 3, 2
+    u = torch.from_numpy(u0.copy()).cuda()
+    rep = ctx.newton_solve(u, o)
+    assert rep.pc_fallbacks >= 1
+
+
+def test_learned_preconditioner_needs_a_model():
+    spec, ctx, u0 = _ns_ctx(3, 3)
+    o = ib.default_newton_options()
+    o.preconditioner = 5
+    with pytest.raises(ib.IcxError):
+        ctx.newton_solve(torch.from_numpy(u0.copy()).cuda(), o)
+    m = ib.LearnedPreconditioner(16, 64, 0)
+    with pytest.raises(ib.IcxError):
+        ctx.lpc_attach(m)  # block size 16 on a 36 x 36 block context
+
+
+def test_model_save_and_load(tmp_path):
+    m = ib.LearnedPreconditioner(36, 64, 0, seed=9)
+    p = m.get_params()
+    p += np.random.default_rng(1).standard_normal(p.size).astype(np.float32) * 1e-3
+    m.set_params(p)
+    m.save(tmp_path / "m.npz")
+    m2 = ib.LearnedPreconditioner.load(tmp_path / "m.npz")
+    assert np.array_equal(m2.get_params(), p)
