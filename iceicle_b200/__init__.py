@@ -26,6 +26,7 @@ POINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_v
 
 # BOUNDARY_CONDITIONS values of the reference (geometry/face.hpp:23-90)
 PERIODIC, PARALLEL_COM, NEUMANN, DIRICHLET, EXTRAPOLATION = 0, 1, 2, 3, 4
+SPACETIME_PAST, SPACETIME_FUTURE = 11, 12
 SPACETIME_FUTURE, INTERIOR = 12, 13
 PDE_BURGERS, PDE_NAVIER_STOKES = 0, 1
 FLUX_UPWIND, FLUX_VANLEER = 0, 1
@@ -103,6 +104,7 @@ def lib():
             "icx_mesh_topology": (C.c_int, [vp, vp, vp, ip]),
             "icx_fespace": (C.c_int, [vp, C.c_int]),
             "icx_disc_burgers": (C.c_int, [vp, C.c_double, dp, dp]),
+            "icx_disc_spacetime_burgers": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
             "icx_disc_navier_stokes": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
             "icx_disc_options": (C.c_int, [vp, C.c_int, C.c_double]),
             "icx_disc_dirichlet": (C.c_int, [vp, C.c_int, POINT_FN, vp]),
@@ -239,6 +241,10 @@ class Context:
     def fespace(self, p):
         self._check(lib().icx_fespace(self._h, p), "fespace")
         self.p = p
+
+    def disc_spacetime_burgers(self, mu, a, b):
+        """Burgers in (x, t): the second mesh coordinate is time"""
+        self._check(lib().icx_disc_spacetime_burgers(self._h, mu, a, b), "disc_spacetime_burgers")
 
     def disc_burgers(self, mu, a, b):
         self._check(lib().icx_disc_burgers(self._h, mu, (C.c_double * 2)(*a), (C.c_double * 2)(*b)), "disc_burgers")

@@ -21,6 +21,7 @@ icx_status icx_batch_create(icx_ctx** out, int device, int n_parts, icx_ctx* con
   for (int k = 0; k < n_parts; ++k) {
     const icx_ctx* q = parts[k];
     if (!q || !q->ready || !q->parts.empty()) return ICX_ERR_INVALID;
+    if (q->phys.spacetime) return ICX_ERR_UNSUPPORTED;
     if (q->p != p0->p || q->geo_order != p0->geo_order || q->phys.pde != p0->phys.pde ||
         q->phys.interior_penalty != p0->phys.interior_penalty || q->phys.sigma_ic != p0->phys.sigma_ic ||
         q->device != device)

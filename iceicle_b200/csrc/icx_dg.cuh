@@ -29,6 +29,7 @@ __device__ inline PhysParams elem_params(const DeviceMesh& dm, const PhysParams&
   if (PDE == ICX_PDE_BURGERS && dm.el_par) {
     const double* v = dm.el_par + 5 * (size_t)e;
     q.mu = v[0];
+    q.mu_t = v[0];  // batches hold plain (not spacetime) Burgers parts
     q.a[0] = v[1];
     q.a[1] = v[2];
     q.b[0] = v[3];

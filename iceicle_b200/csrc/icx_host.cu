@@ -442,7 +442,25 @@ icx_status icx_disc_burgers(icx_ctx* c, double mu, const double* a, const double
   if (!c || !a || !b) return fail(c, ICX_ERR_INVALID, "null argument");
   c->phys.pde = ICX_PDE_BURGERS;
   c->phys.mu = mu;
+  c->phys.mu_t = mu;
+  c->phys.spacetime = 0;
   for (int d = 0; d < 2; ++d) { c->phys.a[d] = a[d]; c->phys.b[d] = b[d]; }
+  c->conv_flux = ICX_FLUX_UPWIND;
+  c->has_disc = true;
+  c->ready = false;
+  return ICX_OK;
+}
+
+icx_status icx_disc_spacetime_burgers(icx_ctx* c, double mu, double a, double b) {
+  if (!c) return ICX_ERR_INVALID;
+  c->phys.pde = ICX_PDE_BURGERS;
+  c->phys.mu = mu;
+  c->phys.mu_t = 0.0;
+  c->phys.spacetime = 1;
+  c->phys.a[0] = a;
+  c->phys.b[0] = b;
+  c->phys.a[1] = 1.0;  // time component of the flux: u
+  c->phys.b[1] = 0.0;
   c->conv_flux = ICX_FLUX_UPWIND;
   c->has_disc = true;
   c->ready = false;
@@ -529,6 +547,10 @@ icx_status icx_setup(icx_ctx* c) {
     // the Navier-Stokes diffusive flux defines no homogeneity tensor: the
     // reference skips the interface correction, so sigma_ic has no effect
   }
+  // neither does the spacetime Burgers diffusion (burgers.hpp:414-474): the
+  // kernels see sigma_ic = 0; SPACETIME_PAST faces without a connected past
+  // slab contribute nothing, as in the reference without spacetime information
+  if (c->phys.spacetime) c->phys.sigma_ic = 0.0;
   // DDG coefficients (conservation_law.hpp:511-538)
   c->phys.beta0 = std::pow(P + 1, 2);
   c->phys.beta1 = 1.0 / std::max((double)(2 * P * (P + 1)), 1.0);

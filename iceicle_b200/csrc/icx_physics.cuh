@@ -16,12 +16,14 @@ template <int PDE> struct Phys;
 template <> struct Phys<ICX_PDE_BURGERS> {
   static constexpr int NEQ = 1;
 
-  // F_d = (a_d + b_d u / 2) u - mu du/dx_d
+  // F_d = (a_d + b_d u / 2) u - mu_d du/dx_d, mu_0 = mu, mu_1 = mu_t (mu, or 0
+  // in spacetime form where the second coordinate is time: a_1 = 1, b_1 = 0
+  // give F_t = u, burgers.hpp:261-340)
   __device__ static inline void flux(const PhysParams& pp, const double* u, const double* g, double* F) {
 #pragma unroll
     for (int d = 0; d < 2; ++d) {
       double lam = pp.a[d] + 0.5 * pp.b[d] * u[0];
-      F[d] = lam * u[0] - pp.mu * g[d];
+      F[d] = lam * u[0] - (d == 0 ? pp.mu : pp.mu_t) * g[d];
     }
   }
   // upwinding on the averaged wavespeed P = n.(a + b uavg / 2)
@@ -39,10 +41,7 @@ template <> struct Phys<ICX_PDE_BURGERS> {
   }
   __device__ static inline void diff(const PhysParams& pp, const double* u, const double* g, const double* n,
                                      double* f) {
-    double fv = 0.0;
-#pragma unroll
-    for (int d = 0; d < 2; ++d) fv += pp.mu * g[d] * n[d];
-    f[0] = fv;
+    f[0] = pp.mu * g[0] * n[0] + pp.mu_t * g[1] * n[1];
   }
   __device__ static inline void neumann(const PhysParams& pp, const double* gn, double* f) { f[0] = pp.mu * gn[0]; }
   static constexpr bool has_ic = true;  // homogeneity tensor G = mu * I

@@ -39,6 +39,7 @@ typedef int icx_status;
 #define ICX_BC_NEUMANN 2
 #define ICX_BC_DIRICHLET 3
 #define ICX_BC_EXTRAPOLATION 4
+#define ICX_BC_SPACETIME_PAST 11
 #define ICX_BC_SPACETIME_FUTURE 12
 #define ICX_BC_INTERIOR 13
 
@@ -88,6 +89,15 @@ icx_status icx_fespace(icx_ctx* ctx, int basis_order);
 
 /* ---- ConservationLawDDG (CL:92-218) ------------------------------------ */
 icx_status icx_disc_burgers(icx_ctx* ctx, double mu, const double* a, const double* b);
+/* SpacetimeBurgersFlux / SpacetimeBurgersUpwind / SpacetimeBurgersDiffusion
+ * (disc/burgers.hpp:261-474) with BurgersCoefficients<T, 1>{mu, a, b}: the
+ * second mesh coordinate is time, F = ((a + b u / 2) u - mu du/dx, u), the
+ * upwind flux includes the time normal, and there is no diffusion along time.
+ * Boundaries: ICX_BC_SPACETIME_FUTURE (top of a slab) extrapolates; a
+ * SPACETIME_PAST face (bottom of a slab, value 11) without a connected past
+ * slab contributes nothing, as in the reference's discretization without
+ * spacetime information; sigma_ic is ignored (no homogeneity tensor). */
+icx_status icx_disc_spacetime_burgers(icx_ctx* ctx, double mu, double a, double b);
 icx_status icx_disc_navier_stokes(icx_ctx* ctx, double gamma, double Pr, double mu, int conv_flux);
 /* public members interior_penalty and sigma_ic (CL:137-143) */
 icx_status icx_disc_options(icx_ctx* ctx, int interior_penalty, double sigma_ic);

@@ -340,11 +340,14 @@ static void phys_hess(int nb, const double J[2][2], const double H[2][2][2], con
 /* ------------------------------------------------------------------ */
 /* physics                                                             */
 /* ------------------------------------------------------------------ */
-/* Burgers (BU:41-250) */
+/* Burgers (BU:41-250); in spacetime form (BU:261-474) the second coordinate
+ * is time: its flux is u (a[1] = 1, b[1] = 0 set by the caller) and it has no
+ * diffusion */
+static double burgers_mu(const orc_problem* pb, int d) { return (pb->spacetime && d == 1) ? 0.0 : pb->mu; }
 static void burgers_flux(const orc_problem* pb, const double* u, const double* g, double F[][2]) {
   for (int d = 0; d < 2; ++d) {
     double lam = pb->a[d] + 0.5 * pb->b[d] * u[0];
-    F[0][d] = lam * u[0] - pb->mu * g[d];
+    F[0][d] = lam * u[0] - burgers_mu(pb, d) * g[d];
   }
 }
 static void burgers_upwind(const orc_problem* pb, const double* uL, const double* uR, const double n[2],
@@ -361,7 +364,7 @@ static void burgers_diff(const orc_problem* pb, const double* u, const double* g
                          double* f) {
   (void)u;
   double fv = 0.0;
-  for (int d = 0; d < 2; ++d) fv += pb->mu * g[d] * n[d];
+  for (int d = 0; d < 2; ++d) fv += burgers_mu(pb, d) * g[d] * n[d];
   f[0] = fv;
 }
 
@@ -732,7 +735,9 @@ static void trace_integral(const disc* D, const int* F, const double* uL, const 
     for (int i = 0; i < nb; ++i)
       for (int k = 0; k < neq; ++k) resR[i * neq + k] -= (fvis[k] - fadv[k]) * BR[i];
     /* interface correction, Burgers only (homogeneity tensor, CL:580-610) */
-    if (pb->pde == 0 && pb->sigma_ic != 0.0) {
+    /* interface correction (Burgers only; the spacetime diffusion defines no
+     * homogeneity tensor, so the reference applies none there) */
+    if (pb->pde == 0 && !pb->spacetime && pb->sigma_ic != 0.0) {
       for (int i = 0; i < nb; ++i)
         for (int kd = 0; kd < 2; ++kd) {
           double jump = ur[0] - ul[0];
@@ -777,7 +782,7 @@ static int boundary_integral(const disc* D, const int* F, const double* uL, doub
       for (int k = 0; k < neq; ++k) { fadv[k] *= fq.w * fq.sqrtg; fvis[k] *= fq.w * fq.sqrtg; }
       for (int i = 0; i < nb; ++i)
         for (int k = 0; k < neq; ++k) resL[i * neq + k] += (fvis[k] - fadv[k]) * BL[i];
-      if (pb->pde == 0 && pb->sigma_ic != 0.0) {
+      if (pb->pde == 0 && !pb->spacetime && pb->sigma_ic != 0.0) {
         for (int i = 0; i < nb; ++i)
           for (int kd = 0; kd < 2; ++kd)
             resL[i] -= pb->sigma_ic * pb->mu * fq.n[kd] * dBL[2 * i + kd] * (ud[0] - ul[0]) * fq.w * fq.sqrtg;

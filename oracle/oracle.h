@@ -41,12 +41,13 @@ typedef struct orc_problem {
   void* neumann_user[8];
   orc_point_fn source;
   void* source_user;
+  int spacetime;        /* Burgers in (x, t): SpacetimeBurgersFlux/Upwind/Diffusion, no diffusion along t */
 } orc_problem;
 
 /* reference BOUNDARY_CONDITIONS enumerators used here */
 enum {
   ORC_BC_PERIODIC = 0, ORC_BC_PARALLEL_COM = 1, ORC_BC_NEUMANN = 2, ORC_BC_DIRICHLET = 3,
-  ORC_BC_EXTRAPOLATION = 4, ORC_BC_SPACETIME_FUTURE = 12, ORC_BC_INTERIOR = 13
+  ORC_BC_EXTRAPOLATION = 4, ORC_BC_SPACETIME_PAST = 11, ORC_BC_SPACETIME_FUTURE = 12, ORC_BC_INTERIOR = 13
 };
 
 int orc_n_nodes(const orc_problem* pb);

@@ -65,6 +65,7 @@ struct ref_problem {
   void* neumann_user[8];
   ref_point_fn source;
   void* source_user;
+  int spacetime;        // Burgers in (x, t): SpacetimeBurgersFlux / Upwind / Diffusion
 };
 }
 
@@ -130,7 +131,18 @@ int with_disc(const ref_problem& pb, const double* coord, Body&& body) {
   auto mesh = build_mesh(pb, coord);
   FESpace<T, IDX, ndim> fespace{mesh.get(), FESPACE_ENUMS::LAGRANGE, FESPACE_ENUMS::GAUSS_LEGENDRE,
                                 std::integral_constant<int, P>{}};
-  if (pb.pde == 0) {
+  if (pb.pde == 0 && pb.spacetime) {
+    BurgersCoefficients<T, ndim - 1> coeffs{};
+    coeffs.mu = pb.mu;
+    coeffs.a[0] = pb.a[0];
+    coeffs.b[0] = pb.b[0];
+    SpacetimeBurgersFlux<T, ndim> pf{coeffs};
+    SpacetimeBurgersUpwind<T, ndim> cf{coeffs};
+    SpacetimeBurgersDiffusion<T, ndim> df{coeffs};
+    ConservationLawDDG disc{std::move(pf), std::move(cf), std::move(df)};
+    add_callbacks(disc, pb);
+    return body(fespace, disc, std::integral_constant<std::size_t, 1>{});
+  } else if (pb.pde == 0) {
     BurgersCoefficients<T, ndim> coeffs{};
     coeffs.mu = pb.mu;
     coeffs.a[0] = pb.a[0]; coeffs.a[1] = pb.a[1];

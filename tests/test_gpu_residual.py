@@ -26,6 +26,9 @@ CASES = [
     dict(pde=NS, p=1, g=1, bct=(3, 4, 3, 4)),
     dict(pde=NS, p=4, g=2, nx=2, ny=3, ip=True),
     dict(nx=12, ny=9, p=2, perturb=0.2),
+    dict(spacetime=True, a=(0.4,), b=(1.0,), bct=(3, 11, 3, 12)),
+    dict(spacetime=True, p=3, a=(-0.3,), b=(0.5,), bct=(3, 3, 4, 12)),
+    dict(spacetime=True, p=4, nx=3, ny=4, ip=True, sigma_ic=0.5, bct=(2, 3, 3, 12)),
 ]
 
 

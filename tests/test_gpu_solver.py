@@ -72,6 +72,25 @@ def _newton_opts(**kw):
     return o
 
 
+def test_newton_spacetime_burgers_slab_matches_oracle_newton():
+    """one spacetime slab of viscous Burgers in (x, t): initial data and
+    inflow as Dirichlet data, SPACETIME_FUTURE on top. Newton without line
+    search on both sides; converged states agree to 1e-10 (L2, relative)"""
+    spec = Spec(pde=BURGERS, nx=6, ny=4, p=2, g=2, mu=2e-2, a=(0.3,), b=(1.0,), spacetime=True,
+                bct=(3, 3, 4, 12), dirichlet=[("constant", [1, 0.4])])
+    c = spec.coords()
+    ctx = spec.context(c)
+    xy = ctx.basis_node_coords().reshape(-1, 2)
+    u0 = 0.4 + 0.1 * np.sin(2 * np.pi * xy[:, 0]) + 1e-3 * np.random.default_rng(3).standard_normal(len(xy))
+    u_or, hist_or = on.newton(spec.oracle_problem(), c, u0, tau_abs=1e-12, kmax=15)
+    du = torch.from_numpy(u0.copy()).cuda()
+    rep = ctx.newton_solve(du, _newton_opts(tau_abs=1e-12, kmax=15, linesearch=0, gmres_rtol=1e-13,
+                                            gmres_max_it=5000))
+    assert rep.converged, list(rep.residual_history[:rep.iterations + 1])
+    u = du.cpu().numpy()
+    assert np.linalg.norm(u - u_or) <= 1e-10 * np.linalg.norm(u_or)
+
+
 def test_newton_burgers_matches_oracle_newton():
     """no line search, tight linear solves: both sides take the same Newton
     steps, so the residual histories agree while |r| >> roundoff and the

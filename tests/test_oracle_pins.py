@@ -22,6 +22,10 @@ CASES = [
     dict(pde=NS, p=3),
     dict(pde=NS, p=1, g=1, bct=(3, 4, 3, 4)),
     dict(pde=NS, p=2, ip=True, source=True),
+    # spacetime Burgers (x, t): past face without a connected slab, future face extrapolating
+    dict(spacetime=True, a=(0.4,), b=(1.0,), bct=(3, 11, 3, 12)),
+    dict(spacetime=True, p=3, a=(-0.3,), b=(0.5,), bct=(3, 3, 4, 12)),
+    dict(spacetime=True, ip=True, sigma_ic=0.5, bct=(2, 3, 3, 12)),
 ]
 
 
