@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-newton", action="store_true", help="skip the secondary Newton solve timings")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-preconditioner Newton comparison (256 x 256 Navier-Stokes, p = 2)")
     ap.add_argument("--batched", type=int, default=64, metavar="N",
                     help="secondary timing of N seeded uneven advection-diffusion problems, batched vs one at a "
                          "time (0: skip; the full problem set is 512)")
@@ -264,6 +266,37 @@ def newton_bench(torch, dev):
     return out
 
 
+def learned_bench(torch, dev):
+    """Newton solve time to |r| <= 1e-10 on one fresh seeded instance of the
+    256 x 256 p = 2 Navier-Stokes manufactured solution (Re drawn from
+    [50, 500]): the plain all-FP64 GMRES(30) + block-ILU(0) solve against the
+    learned preconditioner (shipped model) in mixed precision, with mixed
+    block-ILU(0) and the untrained parallel ILU as references. CUDA events
+    around each whole solve."""
+    from iceicle_b200 import LearnedPreconditioner
+    from iceicle_b200 import learned_pc as lp
+    path = os.path.join(ROOT, "iceicle_b200", "data", "learned_pc_ns_p2.npz")
+    if not os.path.exists(path):
+        return {"unavailable": "model file iceicle_b200/data/learned_pc_ns_p2.npz absent"}
+    m = LearnedPreconditioner.load(path, dev.index)
+    sw = m.sweeps if m.sweeps is not None else 2
+    seed, re = lp.instances(*lp.EVAL_INSTANCES)[0]
+    wl = lp.make_instance(seed, re, 256, dev.index)
+    plain, u_p = lp.solve(wl, None, 2, 0, device=dev.index)
+    mixed, _ = lp.solve(wl, None, 2, 1, device=dev.index)
+    learned, u_l = lp.solve(wl, m, 5, 1, sw, dev.index)
+    parallel, _ = lp.solve(wl, None, 4, 1, sw, dev.index)
+    del wl
+    return {"instance": {"seed": seed, "re": re, "mesh": "256x256", "p": 2, "n_dof": 256 * 256 * 36},
+            "model": {"params": m.n_params, "pc_sweeps": sw, "file": "iceicle_b200/data/learned_pc_ns_p2.npz"},
+            "plain_fp64_ilu0": plain, "mixed_ilu0": mixed, "learned_mixed": learned,
+            "parallel_ilu_mixed_untrained": parallel,
+            "learned_vs_plain_state_l2": float(np.linalg.norm(u_l - u_p) / np.linalg.norm(u_p)),
+            "speedup_learned_mixed_vs_plain_fp64": plain["s"] / learned["s"],
+            "speedup_mixed_ilu0_vs_plain_fp64": plain["s"] / mixed["s"],
+            "speedup_parallel_ilu_mixed_vs_plain_fp64": plain["s"] / parallel["s"]}
+
+
 def run_ours(a):
     import torch
     ws, rank, local = dist_env()
@@ -375,6 +408,8 @@ def run_ours(a):
             line["newton"] = newton_bench(torch, dev)
         if a.batched and ws == 1:
             line["batched"] = batched_bench(torch, dev, a.batched)
+        if not a.no_learned and ws == 1:
+            line["learned_pc"] = learned_bench(torch, dev)
         print(json.dumps(line))
     if ws > 1:
         dist.destroy_process_group()

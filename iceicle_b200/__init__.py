@@ -479,6 +479,7 @@ class LearnedPreconditioner:
         if st != 0:
             raise IcxError(st, "icx_lpc_create")
         self.bs, self.hidden, self.device = bs, hidden, device
+        self.sweeps = None
 
     def close(self):
         if self._h:
@@ -518,14 +519,18 @@ class LearnedPreconditioner:
         if st != 0:
             raise IcxError(st, "icx_lpc_set_params")
 
-    def save(self, path):
-        np.savez_compressed(path, bs=self.bs, hidden=self.hidden, params=self.get_params())
+    def save(self, path, sweeps=None):
+        """parameters and shape (and the Jacobi sweeps the model was trained
+        with, the pc_sweeps to run it with) as a compressed .npz"""
+        extra = {} if sweeps is None else {"sweeps": sweeps}
+        np.savez_compressed(path, bs=self.bs, hidden=self.hidden, params=self.get_params(), **extra)
 
     @classmethod
     def load(cls, path, device=0):
         z = np.load(path)
         m = cls(int(z["bs"]), int(z["hidden"]), device)
         m.set_params(z["params"])
+        m.sweeps = int(z["sweeps"]) if "sweeps" in z.files else None
         return m
 
 

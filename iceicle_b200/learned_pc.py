@@ -119,3 +119,33 @@ def evaluate(model, eval_instances, n=256, sweeps=2, device=0, log=None):
 
 def new_model(device=0, seed=0, hidden=256):
     return LearnedPreconditioner(BLOCK_SIZE, hidden, device, seed)
+
+
+# the training recipe of the shipped model (data/learned_pc_ns_p2.npz)
+RECIPE = dict(model_seed=1, train_instances=(3, 11), steps=120, batch=4, random=2, sweeps=2, lr=1e-3)
+EVAL_INSTANCES = (2, 99)
+
+
+def main(argv=None):
+    """python -m iceicle_b200.learned_pc train OUT.npz | evaluate MODEL.npz"""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cmd", choices=["train", "evaluate"])
+    ap.add_argument("path")
+    ap.add_argument("--n", type=int, default=256, help="quadrilaterals per direction")
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        r = RECIPE
+        m = new_model(seed=r["model_seed"])
+        train(m, instances(*r["train_instances"]), n=a.n, steps=r["steps"], batch=r["batch"], random=r["random"],
+              sweeps=r["sweeps"], lr=r["lr"], log=lambda x: print(json.dumps(x), flush=True))
+        m.save(a.path, sweeps=r["sweeps"])
+    else:
+        m = LearnedPreconditioner.load(a.path)
+        evaluate(m, instances(*EVAL_INSTANCES), n=a.n, sweeps=m.sweeps,
+                 log=lambda x: print(json.dumps(x), flush=True))
+
+
+if __name__ == "__main__":
+    main()
