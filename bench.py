@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-newton", action="store_true", help="skip the secondary Newton solve timings")
+    ap.add_argument("--spmv", type=int, default=0, metavar="N",
+                    help="only time the FP64 BSR SpMV of the N x N p = 2 Navier-Stokes Jacobian (36 x 36 blocks) "
+                         "and print one JSON line")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-preconditioner Newton comparison (256 x 256 Navier-Stokes, p = 2)")
     ap.add_argument("--batched", type=int, default=64, metavar="N",
@@ -266,6 +269,37 @@ def newton_bench(torch, dev):
     return out
 
 
+def spmv_bench(n):
+    """FP64 BSR SpMV of the FD Jacobian of the n x n p = 2 Navier-Stokes
+    manufactured solution (36 x 36 blocks): 3 untimed, then 20 timed launches
+    between CUDA events; inputs larger than L2 from n = 96 on"""
+    import torch
+    from iceicle_b200.workloads import ns_mms_config
+    dev = torch.device("cuda", 0)
+    wl = ns_mms_config(nx=n, ny=n, p=2, geo_order=2, mu=0.01)
+    ctx, L = wl.ctx, wl.ctx.layout
+    bs = L.block_size
+    u = torch.from_numpy(wl.u0).to(dev)
+    res = torch.empty_like(u)
+    vals = torch.empty(L.nnz_blocks * bs * bs, dtype=torch.float64, device=dev)
+    ctx.form_jacobian_fd(u, res, vals)
+    x = torch.randn(L.n_dof, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
+    y = torch.empty_like(x)
+    for _ in range(3):
+        ctx.bsr_spmv(vals, x, y)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(20):
+        ctx.bsr_spmv(vals, x, y)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / 20
+    nbytes = L.nnz_blocks * bs * bs * 8 + L.nnz_blocks * 4 + (L.n_elem + 1) * 4 + 2 * L.n_dof * 8
+    print(json.dumps({"spmv": f"ns_mms_{n}x{n}_p2", "block": bs, "ms": ms, "algorithmic_bytes": nbytes,
+                      "GBs": nbytes / ms / 1e6}))
+
+
 def learned_bench(torch, dev):
     """Newton solve time to |r| <= 1e-10 on one fresh seeded instance of the
     256 x 256 p = 2 Navier-Stokes manufactured solution (Re drawn from
@@ -417,7 +451,9 @@ def run_ours(a):
 
 def main():
     a = parse()
-    if a.impl == "reference":
+    if a.spmv:
+        spmv_bench(a.spmv)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

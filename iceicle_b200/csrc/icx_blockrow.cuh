@@ -111,6 +111,8 @@ struct VecRowCfg {
   static constexpr int QR = BS / VEC;       // vectors per block row
   static constexpr int Q = BS * QR;         // vectors per block
   static constexpr int J = (Q + 31) / 32;   // vectors per lane
+  static constexpr int NCH = (sizeof(TA) == 8 && J > 12) ? 2 : 1;  // load chunks per block
+  static constexpr int JC = (J + NCH - 1) / NCH;                   // vectors per lane per chunk
   static constexpr int WARPS = 8;
 };
 
@@ -131,8 +133,13 @@ __device__ inline void load_vec(const TA* __restrict__ p, TA (&o)[VEC]) {
   }
 }
 
+// two CTAs (16 warps) per SM at most 128 registers: without the bound the
+// 36 x 36 FP64 variant holds a whole block row's loads (170 registers, one CTA)
+template <class TA, int BS>
+constexpr int vec_row_min_blocks() { return (sizeof(TA) == 8 && BS >= 25) ? 2 : 1; }
+
 template <int BS, int MODE, class TA>
-__global__ void __launch_bounds__(256) block_row_vec_kernel(int nrows, const int* __restrict__ rowptr,
+__global__ void __launch_bounds__(256, vec_row_min_blocks<TA, BS>()) block_row_vec_kernel(int nrows, const int* __restrict__ rowptr,
                                                             const int* __restrict__ colidx,
                                                             const TA* __restrict__ A, const double* v,
                                                             const double* x0, double sign, double* y) {
@@ -155,25 +162,33 @@ __global__ void __launch_bounds__(256) block_row_vec_kernel(int nrows, const int
     const int k = MODE == BR_DIAG ? e : colidx[kb];
     if ((MODE == BR_LOWER && k >= e) || (MODE == BR_UPPER && k <= e)) continue;
     const TA* Ab = A + (size_t)kb * BS * BS;
-    TA a[J][VEC];
+    // the block's vectors in NCH chunks of JC per lane (one chunk for FP32;
+    // two for large FP64 blocks, which keeps them within 128 registers); the
+    // first chunk's loads are in flight while x_k is staged
 #pragma unroll
-    for (int j = 0; j < J; ++j) {
-      const int q = lane + 32 * j;
-      if (q < Q) load_vec<TA, VEC>(Ab + (size_t)q * VEC, a[j]);
-      else {
+    for (int ch = 0; ch < K::NCH; ++ch) {
+      TA a[K::JC][VEC];
 #pragma unroll
-        for (int t = 0; t < VEC; ++t) a[j][t] = TA(0);
+      for (int jj = 0; jj < K::JC; ++jj) {
+        const int j = ch * K::JC + jj, q = lane + 32 * j;
+        if (j < J && q < Q) load_vec<TA, VEC>(Ab + (size_t)q * VEC, a[jj]);
+        else {
+#pragma unroll
+          for (int t = 0; t < VEC; ++t) a[jj][t] = TA(0);
+        }
       }
-    }
-    for (int c = lane; c < BS; c += 32) xs[c] = (TA)v[(size_t)k * BS + c];
-    __syncwarp();
+      if (ch == 0) {
+        for (int c = lane; c < BS; c += 32) xs[c] = (TA)v[(size_t)k * BS + c];
+        __syncwarp();
+      }
 #pragma unroll
-    for (int j = 0; j < J; ++j) {
-      const int q = lane + 32 * j;
-      if (q < Q) {
-        const int c0 = (q % QR) * VEC;
+      for (int jj = 0; jj < K::JC; ++jj) {
+        const int j = ch * K::JC + jj, q = lane + 32 * j;
+        if (j < J && q < Q) {
+          const int c0 = (q % QR) * VEC;
 #pragma unroll
-        for (int t = 0; t < VEC; ++t) acc[j] += a[j][t] * xs[c0 + t];
+          for (int t = 0; t < VEC; ++t) acc[j] += a[jj][t] * xs[c0 + t];
+        }
       }
     }
     __syncwarp();
