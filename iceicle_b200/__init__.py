@@ -105,6 +105,7 @@ def lib():
             "icx_fespace": (C.c_int, [vp, C.c_int]),
             "icx_disc_burgers": (C.c_int, [vp, C.c_double, dp, dp]),
             "icx_disc_spacetime_burgers": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
+            "icx_spacetime_connect": (C.c_int, [vp, vp, vp]),
             "icx_disc_navier_stokes": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
             "icx_disc_options": (C.c_int, [vp, C.c_int, C.c_double]),
             "icx_disc_dirichlet": (C.c_int, [vp, C.c_int, POINT_FN, vp]),
@@ -245,6 +246,11 @@ class Context:
     def disc_spacetime_burgers(self, mu, a, b):
         """Burgers in (x, t): the second mesh coordinate is time"""
         self._check(lib().icx_disc_spacetime_burgers(self._h, mu, a, b), "disc_spacetime_burgers")
+
+    def spacetime_connect(self, past, u_past):
+        """take the solved slab `past` (state u_past, device) as the exterior
+        state of this slab's SPACETIME_PAST faces"""
+        self._check(lib().icx_spacetime_connect(self._h, past._h, _ptr(u_past)), "spacetime_connect")
 
     def disc_burgers(self, mu, a, b):
         self._check(lib().icx_disc_burgers(self._h, mu, (C.c_double * 2)(*a), (C.c_double * 2)(*b)), "disc_burgers")

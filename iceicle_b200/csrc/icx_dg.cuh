@@ -173,7 +173,10 @@ __device__ inline void face_flux_states(const PhysParams& pp, const FacePt& fp, 
         gq[1 * 2 + kk] = cs[0] * fp.JiR[kk * 2 + 0] + cs[1] * fp.JiR[kk * 2 + 1];
       }
     }
-  } else if (bct == ICX_BC_DIRICHLET) {
+  } else if (bct == ICX_BC_DIRICHLET || (bct == ICX_BC_SPACETIME_PAST && pp.st_connected)) {
+    // a connected SPACETIME_PAST face takes the past slab's trace as exterior
+    // state; on a slab interface at constant t the diffusive normal flux
+    // vanishes (no diffusion along t), leaving the time-upwind flux
     double ud[NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) ud[eq] = bval[eq];

@@ -259,6 +259,7 @@ icx_status tabulate_and_geometry(icx_ctx* c) {
   }
   cudaError_t e = upload(&dm.bvals, bv);
   if (e != cudaSuccess) return cuda_fail(c, e, "upload boundary data");
+  c->phys.st_connected = 0;  // a past-slab connection holds for the mesh it was made on
   if (c->source_fn) {
     std::vector<double> sv((size_t)dm.E * dm.nqv * neq, 0.0);
     for (int el = 0; el < dm.E; ++el)
@@ -283,6 +284,92 @@ icx_status tabulate_and_geometry(icx_ctx* c) {
 
 namespace icx {
 icx_status refresh_geometry(icx_ctx* c) { return tabulate_and_geometry(c); }
+}  // namespace icx
+
+extern "C" icx_status icx_spacetime_connect(icx_ctx* c, const icx_ctx* past, const double* d_u_past) {
+  if (!c || !past || !d_u_past || !c->ready || !past->ready) return fail(c, ICX_ERR_INVALID, "contexts not set up");
+  if (!c->phys.spacetime || !past->phys.spacetime || !c->parts.empty() || !past->parts.empty())
+    return fail(c, ICX_ERR_INVALID, "both contexts must be single spacetime Burgers slabs");
+  const icx::DeviceMesh& dm = c->dm;
+  const int neq = dm.neq, nqf = dm.nqf;
+  cudaSetDevice(past->device);
+  const size_t np = (size_t)past->dm.E * past->dm.nb * past->dm.neq;
+  std::vector<double> up(np);
+  if (cudaMemcpy(up.data(), d_u_past, sizeof(double) * np, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(c, ICX_ERR_CUDA, "copy of the past state");
+  // elements of the past slab on its SPACETIME_FUTURE faces (its top)
+  std::vector<int> tops;
+  for (size_t f = past->n_interior; f < past->faces.size() / 7; ++f)
+    if (past->faces[7 * f + 5] == ICX_BC_SPACETIME_FUTURE) tops.push_back(past->faces[7 * f]);
+  if (tops.empty()) return fail(c, ICX_ERR_INVALID, "the past slab has no SPACETIME_FUTURE faces");
+  Lagrange1D lg(c->geo_order), lgp(past->geo_order), lbp(past->p);
+  double qx[16], qw[16];
+  gauss_legendre(nqf, qx, qw);
+  const int nbp1 = past->p + 1;
+  cudaSetDevice(c->device);
+  int n_faces = 0;
+  for (size_t f = c->n_interior; f < c->faces.size() / 7; ++f) {
+    const int* F = &c->faces[7 * f];
+    if (F[5] != ICX_BC_SPACETIME_PAST) continue;
+    ++n_faces;
+    const int bidx = (int)f - c->n_interior;
+    // the interface must lie at constant t: the face's end points share t
+    double xa[2], xb[2], xi[2];
+    face_ref(F[2], -1.0, xi);
+    el_point(c, lg, F[0], xi, xa);
+    face_ref(F[2], 1.0, xi);
+    el_point(c, lg, F[0], xi, xb);
+    if (std::fabs(xa[1] - xb[1]) > 1e-12 * (1.0 + std::fabs(xa[1])))
+      return fail(c, ICX_ERR_UNSUPPORTED, "SPACETIME_PAST face not at constant t");
+    std::vector<double> vals((size_t)nqf * neq);
+    for (int q = 0; q < nqf; ++q) {
+      double x[2];
+      face_ref(F[2], qx[q], xi);
+      el_point(c, lg, F[0], xi, x);
+      // the past element whose top edge x(s, +1) passes through x: bisection on s
+      bool found = false;
+      for (int e : tops) {
+        double s0 = -1.0, s1 = 1.0, p0[2], p1[2], r0[2] = {-1.0, 1.0}, r1[2] = {1.0, 1.0};
+        el_point(past, lgp, e, r0, p0);
+        el_point(past, lgp, e, r1, p1);
+        const double tol = 1e-12 * (1.0 + std::fabs(x[0]));
+        if ((x[0] - p0[0]) * (x[0] - p1[0]) > 0.0 && std::fabs(x[0] - p0[0]) > tol && std::fabs(x[0] - p1[0]) > tol)
+          continue;
+        if (std::fabs(p0[1] - x[1]) > 1e-9 * (1.0 + std::fabs(x[1])))
+          return fail(c, ICX_ERR_INVALID, "the slabs do not meet: past top and current bottom differ in t");
+        const double dir = p1[0] > p0[0] ? 1.0 : -1.0;
+        for (int it = 0; it < 200 && s1 - s0 > 1e-15; ++it) {
+          double sm = 0.5 * (s0 + s1), rm[2] = {sm, 1.0}, pm[2];
+          el_point(past, lgp, e, rm, pm);
+          if (dir * (pm[0] - x[0]) < 0.0) s0 = sm;
+          else s1 = sm;
+        }
+        const double s = 0.5 * (s0 + s1);
+        double N0[16], N1[16], dN[16], d2N[16];
+        lbp.eval(s, N0, dN, d2N);
+        lbp.eval(1.0, N1, dN, d2N);
+        for (int eq = 0; eq < neq; ++eq) {
+          double v = 0.0;
+          for (int i0 = 0; i0 < nbp1; ++i0)
+            for (int i1 = 0; i1 < nbp1; ++i1)
+              v += up[((size_t)e * nbp1 * nbp1 + i0 * nbp1 + i1) * neq + eq] * N0[i0] * N1[i1];
+          vals[(size_t)q * neq + eq] = v;
+        }
+        found = true;
+        break;
+      }
+      if (!found) return fail(c, ICX_ERR_INVALID, "a SPACETIME_PAST point lies outside the past slab's top");
+    }
+    if (cudaMemcpy(dm.bvals + (size_t)bidx * nqf * neq, vals.data(), sizeof(double) * vals.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(c, ICX_ERR_CUDA, "upload of the past trace");
+  }
+  if (!n_faces) return fail(c, ICX_ERR_INVALID, "the context has no SPACETIME_PAST faces");
+  c->phys.st_connected = 1;
+  return ICX_OK;
+}
+
+namespace icx {
 void lagrange_values(int pn, double x, double* N) {
   Lagrange1D l(pn);
   double dN[16], d2N[16];

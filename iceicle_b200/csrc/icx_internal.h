@@ -29,6 +29,7 @@ struct PhysParams {
   double mu, a[2], b[2];        // Burgers
   double mu_t;                  // Burgers viscosity along the second coordinate (mu; 0 in spacetime form)
   int spacetime;                // Burgers in (x, t): second coordinate is time (a[1] = 1, b[1] = 0, mu_t = 0)
+  int st_connected;             // SPACETIME_PAST faces carry a past slab's trace in bvals (icx_spacetime_connect)
   double gamma, Pr, ns_mu;      // Navier-Stokes (unit reference parameters)
   double inv_gamma, inv_2gam2m1, mu_gamma_pr;  // 1/gamma, 1/(2(gamma^2-1)), mu*gamma/Pr
   int interior_penalty;

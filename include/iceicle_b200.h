@@ -98,6 +98,18 @@ icx_status icx_disc_burgers(icx_ctx* ctx, double mu, const double* a, const doub
  * slab contributes nothing, as in the reference's discretization without
  * spacetime information; sigma_ic is ignored (no homogeneity tensor). */
 icx_status icx_disc_spacetime_burgers(icx_ctx* ctx, double mu, double a, double b);
+/* SpacetimeConnection (disc/SpacetimeConnection.hpp:102-189) for a slab on top
+ * of a solved one: the past slab's solution d_u_past (device, `past`'s
+ * layout) is evaluated at the quadrature points of ctx's SPACETIME_PAST faces
+ * (located on the past slab's SPACETIME_FUTURE elements by their x
+ * coordinate), and those faces then take it as exterior state: time-upwind
+ * convective flux from the past trace, and DDG diffusion with it as the
+ * neighbour value, which vanishes on an interface at constant t (the only
+ * kind accepted). Both contexts must be set-up spacetime Burgers slabs whose
+ * interface lies at the same t. The connection holds until ctx's mesh or
+ * boundary data are recomputed (icx_setup, icx_mesh_set_coords); call it
+ * again after those. */
+icx_status icx_spacetime_connect(icx_ctx* ctx, const icx_ctx* past, const double* d_u_past);
 icx_status icx_disc_navier_stokes(icx_ctx* ctx, double gamma, double Pr, double mu, int conv_flux);
 /* public members interior_penalty and sigma_ic (CL:137-143) */
 icx_status icx_disc_options(icx_ctx* ctx, int interior_penalty, double sigma_ic);
