@@ -27,6 +27,7 @@ POINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_v
 # BOUNDARY_CONDITIONS values of the reference (geometry/face.hpp:23-90)
 PERIODIC, PARALLEL_COM, NEUMANN, DIRICHLET, EXTRAPOLATION = 0, 1, 2, 3, 4
 SPACETIME_PAST, SPACETIME_FUTURE = 11, 12
+BASIS_LAGRANGE, BASIS_LEGENDRE = 0, 1
 SPACETIME_FUTURE, INTERIOR = 12, 13
 PDE_BURGERS, PDE_NAVIER_STOKES = 0, 1
 FLUX_UPWIND, FLUX_VANLEER = 0, 1
@@ -106,6 +107,7 @@ def lib():
             "icx_disc_burgers": (C.c_int, [vp, C.c_double, dp, dp]),
             "icx_disc_spacetime_burgers": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
             "icx_spacetime_connect": (C.c_int, [vp, vp, vp]),
+            "icx_fespace_basis": (C.c_int, [vp, C.c_int, C.c_int]),
             "icx_disc_navier_stokes": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
             "icx_disc_options": (C.c_int, [vp, C.c_int, C.c_double]),
             "icx_disc_dirichlet": (C.c_int, [vp, C.c_int, POINT_FN, vp]),
@@ -239,9 +241,14 @@ class Context:
         self._check(lib().icx_mesh_topology(self._h, _ptr(conn), _ptr(faces), C.byref(ni)), "topology")
         return conn, faces, ni.value
 
-    def fespace(self, p):
-        self._check(lib().icx_fespace(self._h, p), "fespace")
+    def fespace(self, p, basis=0):
+        """tensor-product space of order p: basis BASIS_LAGRANGE (0) or BASIS_LEGENDRE (1)"""
+        if basis:
+            self._check(lib().icx_fespace_basis(self._h, p, basis), "fespace")
+        else:
+            self._check(lib().icx_fespace(self._h, p), "fespace")
         self.p = p
+        self.basis = basis
 
     def disc_spacetime_burgers(self, mu, a, b):
         """Burgers in (x, t): the second mesh coordinate is time"""

@@ -22,6 +22,7 @@ icx_status icx_batch_create(icx_ctx** out, int device, int n_parts, icx_ctx* con
     const icx_ctx* q = parts[k];
     if (!q || !q->ready || !q->parts.empty()) return ICX_ERR_INVALID;
     if (q->phys.spacetime) return ICX_ERR_UNSUPPORTED;
+    if (q->basis != p0->basis) return ICX_ERR_INVALID;
     if (q->p != p0->p || q->geo_order != p0->geo_order || q->phys.pde != p0->phys.pde ||
         q->phys.interior_penalty != p0->phys.interior_penalty || q->phys.sigma_ic != p0->phys.sigma_ic ||
         q->device != device)
@@ -35,6 +36,7 @@ icx_status icx_batch_create(icx_ctx** out, int device, int n_parts, icx_ctx* con
   icx_status st = icx_create(&c, device);
   if (st != ICX_OK) return st;
   c->p = p0->p;
+  c->basis = p0->basis;
   c->geo_order = p0->geo_order;
   c->phys = p0->phys;
   c->conv_flux = p0->conv_flux;

@@ -28,9 +28,14 @@ icx_status cuda_fail(icx_ctx* c, cudaError_t e, const char* where) {
 // Lagrange polynomials through pn+1 equispaced nodes of [-1, 1] (node j
 // accumulated as x_{j-1} + 2/pn, lagrange_1d.hpp:30-42), evaluated in
 // barycentric form with the node nearest to x factored out (lagrange_1d.hpp:78-118).
+// 1D basis of order pn on [-1, 1]: Lagrange polynomials through equispaced
+// nodes (kind ICX_BASIS_LAGRANGE), or the Legendre polynomials P_0..P_pn
+// (kind ICX_BASIS_LEGENDRE, unnormalised, P_k(1) = 1)
 struct Lagrange1D {
   int pn;
+  int kind = ICX_BASIS_LAGRANGE;
   double xi[16], wj[16];
+  Lagrange1D(int n, int k) : Lagrange1D(n) { kind = k; }
   explicit Lagrange1D(int n) : pn(n) {
     xi[0] = -1.0;
     double dx = 2.0 / pn;
@@ -42,7 +47,29 @@ struct Lagrange1D {
       wj[j] = 1.0 / w;
     }
   }
+  // P_0..P_pn with first and second derivatives by the three-term recurrence
+  // (k+1) P_{k+1} = (2k+1) x P_k - k P_{k-1}, differentiated once and twice
+  void legendre(double x, double* N, double* dN, double* d2N) const {
+    N[0] = 1.0;
+    dN[0] = 0.0;
+    d2N[0] = 0.0;
+    if (pn >= 1) {
+      N[1] = x;
+      dN[1] = 1.0;
+      d2N[1] = 0.0;
+    }
+    for (int k = 1; k < pn; ++k) {
+      const double a = (2.0 * k + 1.0) / (k + 1.0), b = (double)k / (k + 1.0);
+      N[k + 1] = a * x * N[k] - b * N[k - 1];
+      dN[k + 1] = a * (N[k] + x * dN[k]) - b * dN[k - 1];
+      d2N[k + 1] = a * (2.0 * dN[k] + x * d2N[k]) - b * d2N[k - 1];
+    }
+  }
   void eval(double x, double* N, double* dN, double* d2N) const {
+    if (kind == ICX_BASIS_LEGENDRE) {
+      legendre(x, N, dN, d2N);
+      return;
+    }
     if (pn == 1) {
       N[0] = 0.5 * (1 - x);
       N[1] = 1.0 - N[0];
@@ -302,7 +329,7 @@ extern "C" icx_status icx_spacetime_connect(icx_ctx* c, const icx_ctx* past, con
   for (size_t f = past->n_interior; f < past->faces.size() / 7; ++f)
     if (past->faces[7 * f + 5] == ICX_BC_SPACETIME_FUTURE) tops.push_back(past->faces[7 * f]);
   if (tops.empty()) return fail(c, ICX_ERR_INVALID, "the past slab has no SPACETIME_FUTURE faces");
-  Lagrange1D lg(c->geo_order), lgp(past->geo_order), lbp(past->p);
+  Lagrange1D lg(c->geo_order), lgp(past->geo_order), lbp(past->p, past->basis);
   double qx[16], qw[16];
   gauss_legendre(nqf, qx, qw);
   const int nbp1 = past->p + 1;
@@ -372,6 +399,11 @@ extern "C" icx_status icx_spacetime_connect(icx_ctx* c, const icx_ctx* past, con
 namespace icx {
 void lagrange_values(int pn, double x, double* N) {
   Lagrange1D l(pn);
+  double dN[16], d2N[16];
+  l.eval(x, N, dN, d2N);
+}
+void basis_values(int kind, int pn, double x, double* N) {
+  Lagrange1D l(pn, kind);
   double dN[16], d2N[16];
   l.eval(x, N, dN, d2N);
 }
@@ -520,9 +552,17 @@ icx_status icx_fespace(icx_ctx* c, int basis_order) {
   if (basis_order < 1 || basis_order > icx::MAX_P)
     return fail(c, ICX_ERR_UNSUPPORTED, "basis order must be in 1..4");
   c->p = basis_order;
+  c->basis = ICX_BASIS_LAGRANGE;
   c->has_space = true;
   c->ready = false;
   return ICX_OK;
+}
+
+icx_status icx_fespace_basis(icx_ctx* c, int basis_order, int basis) {
+  if (basis != ICX_BASIS_LAGRANGE && basis != ICX_BASIS_LEGENDRE) return fail(c, ICX_ERR_INVALID, "unknown basis");
+  icx_status st = icx_fespace(c, basis_order);
+  if (st == ICX_OK) c->basis = basis;
+  return st;
 }
 
 icx_status icx_disc_burgers(icx_ctx* c, double mu, const double* a, const double* b) {
@@ -643,7 +683,7 @@ icx_status icx_setup(icx_ctx* c) {
   c->phys.beta1 = 1.0 / std::max((double)(2 * P * (P + 1)), 1.0);
   if (c->phys.interior_penalty) c->phys.beta1 = 0.0;
 
-  Lagrange1D lb(P), lg(g);
+  Lagrange1D lb(P, c->basis), lg(g);
   double qx[16], qw[16];
   gauss_legendre(dm.nq1, qx, qw);
   // volume tabulation [nqv][nb][3] followed by the nqv weights
@@ -847,6 +887,7 @@ icx_status icx_form_residual_timed(icx_ctx* c, const double* d_u, double* d_res,
 
 icx_status icx_basis_node_coords(const icx_ctx* c, double* xy) {
   if (!c || !xy || !c->has_mesh || !c->has_space) return ICX_ERR_INVALID;
+  if (c->basis != ICX_BASIS_LAGRANGE) return ICX_ERR_UNSUPPORTED;  // a modal basis has no nodes
   Lagrange1D lb(c->p), lg(c->geo_order);
   int n = c->p + 1, E = c->n_elem;
   for (int e = 0; e < E; ++e)

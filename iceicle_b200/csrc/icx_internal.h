@@ -94,6 +94,7 @@ struct icx_ctx {
   std::vector<icx_ctx*> parts;
   std::vector<double> el_par;
   int p = 0;
+  int basis = ICX_BASIS_LAGRANGE;             // solution basis family
   icx::PhysParams phys{};
   int conv_flux = 0;
   std::vector<icx_point_fn> dirichlet_fn, neumann_fn;
@@ -138,6 +139,8 @@ icx_status refresh_geometry(icx_ctx* c);
 void lagrange_values(int pn, double x, double* N);
 // the same with first derivatives
 void lagrange_values_derivs(int pn, double x, double* N, double* dN);
+// values of the pn+1 one-dimensional functions of a basis family (ICX_BASIS_*) at x
+void basis_values(int kind, int pn, double x, double* N);
 // releases the explicit time-stepping buffers of a context (icx_explicit.cu)
 void free_explicit(icx_ctx* c);
 // Gauss-Legendre points in the reference order (+x1, -x1, ..., 0) and weights (icx_host.cu)

@@ -69,11 +69,11 @@ VtkCell vtk_cell(int order) {
   return {{-1, -1, 1, -1, 1, 1, -1, 1, 0, -1, 1, 0, 0, 1, -1, 0}, 23};
 }
 
-// tensor-product Lagrange values of order pn at xi, basis index i0 * (pn+1) + i1
-void tp_values(int pn, const double xi[2], double* phi) {
+// tensor-product values of order pn of a basis family at xi, basis index i0 * (pn+1) + i1
+void tp_values(int kind, int pn, const double xi[2], double* phi) {
   double a[16], b[16];
-  icx::lagrange_values(pn, xi[0], a);
-  icx::lagrange_values(pn, xi[1], b);
+  icx::basis_values(kind, pn, xi[0], a);
+  icx::basis_values(kind, pn, xi[1], b);
   for (int i = 0; i <= pn; ++i)
     for (int j = 0; j <= pn; ++j) phi[i * (pn + 1) + j] = a[i] * b[j];
 }
@@ -154,10 +154,10 @@ void field(std::string& o, const std::string& name, const std::vector<double>& p
 }
 
 // values at the VTK nodes of the element expansion v[e][nbasis][neq] of order pn
-std::vector<double> at_nodes(const std::vector<double>& v, int E, int pn, int neq, const VtkCell& cell) {
+std::vector<double> at_nodes(const std::vector<double>& v, int E, int kind, int pn, int neq, const VtkCell& cell) {
   const int nb = (pn + 1) * (pn + 1), nv = (int)cell.xi.size() / 2;
   std::vector<double> phi((size_t)nv * nb);
-  for (int k = 0; k < nv; ++k) tp_values(pn, &cell.xi[2 * k], &phi[(size_t)k * nb]);
+  for (int k = 0; k < nv; ++k) tp_values(kind, pn, &cell.xi[2 * k], &phi[(size_t)k * nb]);
   std::vector<double> out((size_t)E * nv * neq, 0.0);
   for (int e = 0; e < E; ++e)
     for (int k = 0; k < nv; ++k)
@@ -290,14 +290,14 @@ icx_status icx_write_vtu(icx_ctx* c, const double* d_u, int kind, int itime, con
   grid(o, c, cell, precision);
   if (kind == ICX_VTU_SOLUTION) {
     auto nm = names_or(names, neq, default_fields(c));
-    auto pv = at_nodes(v, E, P, neq, cell);
+    auto pv = at_nodes(v, E, c->basis, P, neq, cell);
     for (int q = 0; q < neq; ++q) field(o, nm[q], pv, neq, q, E, nv, precision);
   } else {
     auto nm = names_or(names, neq, default_residuals(c));
     const char* prefix[3] = {"", "domain_", "trace_"};
     for (int part = 0; part < 3; ++part) {
       std::vector<double> vp(v.begin() + part * N, v.begin() + (part + 1) * N);
-      auto pv = at_nodes(vp, E, P, neq, cell);
+      auto pv = at_nodes(vp, E, c->basis, P, neq, cell);
       for (int q = 0; q < neq; ++q) field(o, prefix[part] + nm[q], pv, neq, q, E, nv, precision);
     }
   }
@@ -341,7 +341,7 @@ icx_status icx_write_vtu_mdg(icx_ctx* c, const double* d_ic, int itime, const ch
   std::string o;
   grid(o, c, cell, precision);
   auto nm = names_or(names, neq, default_fields(c));
-  auto pv = at_nodes(v, E, G, neq, cell);
+  auto pv = at_nodes(v, E, ICX_BASIS_LAGRANGE, G, neq, cell);
   for (int q = 0; q < neq; ++q) field(o, nm[q], pv, neq, q, E, nv, precision);
   footer(o);
   std::filesystem::path d = dir ? std::filesystem::path(dir) : std::filesystem::current_path() / "iceicle_data";

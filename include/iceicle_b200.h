@@ -43,6 +43,8 @@ typedef int icx_status;
 #define ICX_BC_SPACETIME_FUTURE 12
 #define ICX_BC_INTERIOR 13
 
+#define ICX_BASIS_LAGRANGE 0 /* FESPACE_ENUMS::LAGRANGE: equispaced nodal tensor-product basis */
+#define ICX_BASIS_LEGENDRE 1 /* FESPACE_ENUMS::LEGENDRE: tensor products of Legendre polynomials */
 #define ICX_PDE_BURGERS 0
 #define ICX_PDE_NAVIER_STOKES 1
 #define ICX_FLUX_UPWIND 0  /* BurgersUpwind (burgers.hpp:114-170) */
@@ -86,6 +88,11 @@ icx_status icx_mesh_topology(const icx_ctx* ctx, int* conn, int* faces, int* n_i
 
 /* ---- FESpace (FS:200-416): tensor-product Lagrange, Gauss-Legendre ------ */
 icx_status icx_fespace(icx_ctx* ctx, int basis_order);
+/* FESpace{mesh, basis, GAUSS_LEGENDRE, p} with basis ICX_BASIS_LAGRANGE or
+ * ICX_BASIS_LEGENDRE (HypercubeLegendreBasis, basis/legendre.hpp:282-327:
+ * u = sum c_ij P_i(xi0) P_j(xi1), index i * (p+1) + j, unnormalised Legendre
+ * polynomials); icx_basis_node_coords refuses the modal Legendre basis */
+icx_status icx_fespace_basis(icx_ctx* ctx, int basis_order, int basis);
 
 /* ---- ConservationLawDDG (CL:92-218) ------------------------------------ */
 icx_status icx_disc_burgers(icx_ctx* ctx, double mu, const double* a, const double* b);

@@ -12,6 +12,7 @@
  *   FE  = src/FiniteElement/include/iceicle/element/finite_element.hpp
  *   HT  = src/FiniteElement/include/iceicle/transformations/HypercubeTransformations.hpp
  *   L1  = src/FiniteElement/include/iceicle/basis/lagrange_1d.hpp
+ *   B2  = src/FiniteElement/include/iceicle/basis/legendre.hpp
  *   Q1  = src/FiniteElement/include/iceicle/quadrature/quadrules_1d.hpp
  */
 #include "oracle.h"
@@ -31,12 +32,29 @@
 /* ------------------------------------------------------------------ */
 typedef struct {
   int pn;
+  int legendre;         /* 1: Legendre polynomials P_0..P_pn instead (B2:17-280) */
   double xi[MAXP];
   double wj[MAXP];
 } lag1d;
 
+/* Legendre polynomials of the reference's HypercubeLegendreBasis (B2:41-279):
+ * closed forms P_0 = 1, P_1 = x, P_2 = (3x^2 - 1)/2, P_3 = (5x^3 - 3x)/2,
+ * P_4 = (35x^4 - 30x^2 + 3)/8 and their first and second derivatives */
+static void leg1d(int pn, double x, double* N, double* dN, double* d2N) {
+  double x2 = x * x;
+  double v[5] = {1.0, x, (3 * x2 - 1) / 2.0, (5 * x2 * x - 3 * x) / 2.0, (35 * x2 * x2 - 30 * x2 + 3) * 0.125};
+  double d[5] = {0.0, 1.0, 3 * x, 1.5 * (5 * x2 - 1), 2.5 * x * (7 * x2 - 3)};
+  double s[5] = {0.0, 0.0, 3.0, 15 * x, 7.5 * (7 * x2 - 1)};
+  for (int k = 0; k <= pn && k < 5; ++k) {
+    if (N) N[k] = v[k];
+    if (dN) dN[k] = d[k];
+    if (d2N) d2N[k] = s[k];
+  }
+}
+
 static void lag_init(lag1d* l, int pn) {
   l->pn = pn;
+  l->legendre = 0;
   if (pn == 0) { l->xi[0] = 0.0; l->wj[0] = 1.0; return; }
   double dx = 2.0 / pn;
   l->xi[0] = -1.0;
@@ -51,6 +69,7 @@ static void lag_init(lag1d* l, int pn) {
 /* values and first derivatives (L1:126-195) */
 static void lag_deriv(const lag1d* l, double x, double* N, double* dN) {
   int pn = l->pn;
+  if (l->legendre) { leg1d(pn, x, N, dN, NULL); return; }
   if (pn == 0) { N[0] = 1.0; dN[0] = 0.0; return; }
   if (pn == 1) {
     N[0] = 0.5 * (1 - x); N[1] = 1.0 - N[0];
@@ -113,7 +132,12 @@ static void tp_eval(const lag1d* l, const double xi[2], double* B, double* dB, d
   double N0[MAXP], N1[MAXP], d0[MAXP], d1[MAXP], s0[MAXP], s1[MAXP];
   lag_deriv(l, xi[0], N0, d0);
   lag_deriv(l, xi[1], N1, d1);
-  for (int j = 0; j < n; ++j) { s0[j] = lag_d2(l->pn, j, xi[0]); s1[j] = lag_d2(l->pn, j, xi[1]); }
+  if (l->legendre) {
+    leg1d(l->pn, xi[0], NULL, NULL, s0);
+    leg1d(l->pn, xi[1], NULL, NULL, s1);
+  } else {
+    for (int j = 0; j < n; ++j) { s0[j] = lag_d2(l->pn, j, xi[0]); s1[j] = lag_d2(l->pn, j, xi[1]); }
+  }
   for (int i0 = 0; i0 < n; ++i0)
     for (int i1 = 0; i1 < n; ++i1) {
       int i = i0 * n + i1;
@@ -529,6 +553,7 @@ static int disc_init(disc* D, const orc_problem* pb, const double* coord) {
   D->coord = coord;
   if (pb->p < 1 || pb->p >= MAXP || pb->geo_order < 1 || pb->geo_order >= MAXP) return -1;
   lag_init(&D->lb, pb->p);
+  D->lb.legendre = pb->basis == 1;
   lag_init(&D->lg, pb->geo_order);
   D->nb = (pb->p + 1) * (pb->p + 1);
   D->neq = orc_neq(pb);

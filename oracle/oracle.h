@@ -42,6 +42,7 @@ typedef struct orc_problem {
   orc_point_fn source;
   void* source_user;
   int spacetime;        /* Burgers in (x, t): SpacetimeBurgersFlux/Upwind/Diffusion, no diffusion along t */
+  int basis;            /* solution basis: 0 Lagrange (equispaced nodes), 1 Legendre */
 } orc_problem;
 
 /* reference BOUNDARY_CONDITIONS enumerators used here */

@@ -66,6 +66,7 @@ struct ref_problem {
   ref_point_fn source;
   void* source_user;
   int spacetime;        // Burgers in (x, t): SpacetimeBurgersFlux / Upwind / Diffusion
+  int basis;            // FESPACE_BASIS_TYPE of the solution space (0 LAGRANGE, 1 LEGENDRE)
 };
 }
 
@@ -129,7 +130,8 @@ void add_callbacks(Disc& disc, const ref_problem& pb) {
 template <int P, class Body>
 int with_disc(const ref_problem& pb, const double* coord, Body&& body) {
   auto mesh = build_mesh(pb, coord);
-  FESpace<T, IDX, ndim> fespace{mesh.get(), FESPACE_ENUMS::LAGRANGE, FESPACE_ENUMS::GAUSS_LEGENDRE,
+  FESpace<T, IDX, ndim> fespace{mesh.get(), pb.basis == 1 ? FESPACE_ENUMS::LEGENDRE : FESPACE_ENUMS::LAGRANGE,
+                                FESPACE_ENUMS::GAUSS_LEGENDRE,
                                 std::integral_constant<int, P>{}};
   if (pb.pde == 0 && pb.spacetime) {
     BurgersCoefficients<T, ndim - 1> coeffs{};

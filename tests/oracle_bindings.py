@@ -25,7 +25,7 @@ class Problem(C.Structure):
         ("ns_mu", C.c_double),
         ("n_dirichlet", C.c_int), ("dirichlet", POINT_FN * 8), ("dirichlet_user", C.c_void_p * 8),
         ("n_neumann", C.c_int), ("neumann", POINT_FN * 8), ("neumann_user", C.c_void_p * 8),
-        ("source", POINT_FN), ("source_user", C.c_void_p), ("spacetime", C.c_int),
+        ("source", POINT_FN), ("source_user", C.c_void_p), ("spacetime", C.c_int), ("basis", C.c_int),
     ]
 
 

@@ -13,10 +13,11 @@ BURGERS, NS = 0, 1
 class Spec:
     def __init__(self, pde=BURGERS, nx=4, ny=3, g=2, p=2, bct=(3, 3, 3, 3), bcf=(0, 0, 0, 0), ip=False,
                  sigma_ic=0.0, mu=0.01, a=(0.3, -0.2), b=(1.0, 0.5), perturb=0.1, seed=7,
-                 dirichlet=None, neumann=None, source=False, spacetime=False):
+                 dirichlet=None, neumann=None, source=False, spacetime=False, basis=0):
         self.pde, self.nx, self.ny, self.g, self.p = pde, nx, ny, g, p
         self.bct, self.bcf, self.ip, self.sigma_ic = tuple(bct), tuple(bcf), ip, sigma_ic
         self.spacetime = spacetime
+        self.basis = basis
         if spacetime:  # Burgers in (x, t): the time component of the flux is u
             a, b = (a[0], 1.0), (b[0], 0.0)
         self.mu, self.a, self.b = mu, a, b
@@ -83,6 +84,7 @@ class Spec:
         pb.a[:] = list(self.a)
         pb.b[:] = list(self.b)
         pb.spacetime = int(self.spacetime)
+        pb.basis = int(self.basis)
         pb.gamma, pb.Pr, pb.ns_mu = 1.4, 0.72, 0.01
         pb.n_dirichlet = len(self.dirichlet)
         for i, (name, prm) in enumerate(self.dirichlet):
@@ -105,7 +107,7 @@ class Spec:
         ctx = ib.Context(0)
         ctx.mesh_uniform((self.nx, self.ny), (0.0, 0.0), (1.0, 1.0), self.g, self.bct, self.bcf)
         ctx.set_coords(self.coords() if coords is None else coords)
-        ctx.fespace(self.p)
+        ctx.fespace(self.p, self.basis)
         if self.pde == BURGERS and self.spacetime:
             ctx.disc_spacetime_burgers(self.mu, self.a[0], self.b[0])
         elif self.pde == BURGERS:

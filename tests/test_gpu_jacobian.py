@@ -28,6 +28,8 @@ CASES = [
     dict(pde=NS, nx=2, ny=2, p=2),
     dict(nx=3, ny=3, spacetime=True, a=(0.4,), b=(1.0,), bct=(3, 11, 3, 12)),
     dict(nx=3, ny=2, p=3, spacetime=True, a=(-0.3,), b=(0.5,), bct=(3, 3, 4, 12)),
+    dict(nx=3, ny=3, basis=1),
+    dict(pde=NS, nx=2, ny=2, p=2, ip=True, basis=1),
 ]
 
 

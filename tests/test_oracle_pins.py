@@ -26,6 +26,11 @@ CASES = [
     dict(spacetime=True, a=(0.4,), b=(1.0,), bct=(3, 11, 3, 12)),
     dict(spacetime=True, p=3, a=(-0.3,), b=(0.5,), bct=(3, 3, 4, 12)),
     dict(spacetime=True, ip=True, sigma_ic=0.5, bct=(2, 3, 3, 12)),
+    # Legendre (modal) solution basis
+    dict(basis=1),
+    dict(basis=1, p=4, nx=2, ny=2, sigma_ic=0.7),
+    dict(basis=1, pde=NS, p=3, ip=True, source=True),
+    dict(basis=1, spacetime=True, a=(0.4,), b=(1.0,), bct=(3, 11, 3, 12)),
 ]
 
 
