@@ -176,8 +176,13 @@ struct FaceCfg {
   static constexpr int RS = N1 * C::NEQ + C::NEQ;       // padded row stride of a staged tile [i0][i1][eq]
   static constexpr int TILE = N1 * RS;
   static constexpr int T_F = 2 * C::NEQ * N1 * NM;       // [side][eq][j][m]
-  static constexpr int T_FP = T_F | 1;                   // odd per-face stride: faces fall in distinct banks
-  static constexpr size_t SMEM = sizeof(double) * (TAB + FPB * (2 * TILE + T_FP)) + sizeof(int) * FPB * 8;
+  // the partial sums of a face overwrite its own two tiles once every tile has
+  // been read; consecutive faces start them at different offsets within the
+  // spare room so that the faces of a warp fall in different banks
+  static constexpr int SLACK = 2 * TILE - T_F;
+  static constexpr int SHIFT_MOD = (SLACK < 15 ? SLACK : 15) + 1;
+  static constexpr int ITEMS = (FPB * 2 * C::NEQ * N1 + THREADS - 1) / THREADS;  // partial sums per thread
+  static constexpr size_t SMEM = sizeof(double) * (TAB + FPB * 2 * TILE) + sizeof(int) * FPB * 8;
   // resident CTAs requested: the Navier-Stokes flux with Hessians needs more registers
   static constexpr int MINB = (DDG && C::NEQ > 1) ? 3 : ICX_FACE_MINB;
 };
@@ -202,8 +207,9 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flu
   extern __shared__ double smem[];
   double* s_tab = smem;                           // tab_f1d
   double* s_u = s_tab + FC::TAB;                  // [FPB][2][N1][RS]
-  double* s_T = s_u + FPB * 2 * FC::TILE;         // [FPB][T_FP]: [2][NEQ][N1][NM]
-  int* s_rec = (int*)(s_T + FPB * FC::T_FP);      // [FPB][8] face records
+  // face fl's partial sums [2][NEQ][N1][NM], over its tiles once they are read
+  auto s_T = [&](int fl) { return s_u + fl * 2 * FC::TILE + fl % FC::SHIFT_MOD; };
+  int* s_rec = (int*)(s_u + FPB * 2 * FC::TILE);  // [FPB][8] face records
   const int f0 = blockIdx.x * FPB;
   const int nf = min(FPB, dm.F - f0);
   const int tid = threadIdx.x;
@@ -256,8 +262,14 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flu
   cp_async_wait_all();
   __syncthreads();
 
-  // partial sums along each side's fixed direction
-  for (int t = tid; t < nf * 2 * NEQ * N1; t += FC::THREADS) {
+  // partial sums along each side's fixed direction, held in registers until
+  // every thread has read its tiles, then stored over the tiles
+  static_assert(FC::SLACK >= 0, "partial sums fit in a face's tiles");
+  double accs[FC::ITEMS][NM];
+#pragma unroll
+  for (int it = 0; it < FC::ITEMS; ++it) {
+    const int t = tid + it * FC::THREADS;
+    if (t >= nf * 2 * NEQ * N1) break;
     int fs = t / (NEQ * N1), r = t - fs * (NEQ * N1);
     int eq = r / N1, j = r - eq * N1;
     const int* rec = s_rec + (fs >> 1) * 8;
@@ -266,7 +278,7 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flu
     const double* fx = s_tab + lf * N1 * 3;
     const double* c = s_u + fs * FC::TILE + eq;
     int stride_k = (lf & 1) ? NEQ : FC::RS, off_j = (lf & 1) ? j * FC::RS : j * NEQ;
-    double acc[NM];
+    double* acc = accs[it];
 #pragma unroll
     for (int m = 0; m < NM; ++m) acc[m] = 0.0;
 #pragma unroll
@@ -275,9 +287,17 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flu
 #pragma unroll
       for (int m = 0; m < NM; ++m) acc[m] += cv * fx[k * 3 + m];
     }
-    double* T = s_T + (fs >> 1) * FC::T_FP + ((fs & 1) * NEQ + eq) * N1 * NM + j * NM;
+  }
+  __syncthreads();
 #pragma unroll
-    for (int m = 0; m < NM; ++m) T[m] = acc[m];
+  for (int it = 0; it < FC::ITEMS; ++it) {
+    const int t = tid + it * FC::THREADS;
+    if (t >= nf * 2 * NEQ * N1) break;
+    int fs = t / (NEQ * N1), r = t - fs * (NEQ * N1);
+    int eq = r / N1, j = r - eq * N1;
+    double* T = s_T(fs >> 1) + ((fs & 1) * NEQ + eq) * N1 * NM + j * NM;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) T[m] = accs[it][m];
   }
   __syncthreads();
 
@@ -306,7 +326,7 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flu
       const double* Hm = side ? fp.HR : fp.HL;
 #pragma unroll
       for (int eq = 0; eq < NEQ; ++eq) {
-        const double* T = s_T + fl * FC::T_FP + (side * NEQ + eq) * N1 * NM;
+        const double* T = s_T(fl) + (side * NEQ + eq) * N1 * NM;
         double v = 0.0, dfix = 0.0, dvar = 0.0, hff = 0.0, hfv = 0.0, hvv = 0.0;
 #pragma unroll
         for (int j = 0; j < N1; ++j) {
