@@ -184,7 +184,7 @@ def residual_work(wl):
 # residual kernels on this workload, from one ncu capture of
 #   ncu --set full --clock-control none -k regex:"face_flux|vol_lift" -s 10 -c 2 \
 #       python bench.py --steps 2 --warmup 3 --no-newton --no-cpu-baseline
-NCU_DRAM_BYTES = {"vol": 43.45e6 + 0.50e6, "face": 25.70e6 + 0.01e6}
+NCU_DRAM_BYTES = {"vol": 43.45e6 + 0.06e6, "face": 25.59e6 + 0.003e6}
 
 
 def batched_bench(torch, dev, n_problems):
