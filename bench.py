@@ -373,27 +373,36 @@ def run_ours(a):
         f, v = wl.ctx.form_residual_timed(u, res, stream)
         t_face.append(f)
         t_vol.append(v)
-    # end to end through the public API with host buffers
-    h_u = torch.from_numpy(wl.u0).pin_memory()
-    h_r = torch.empty(N, dtype=torch.float64).pin_memory()
+    # end to end through the public API with host buffers: one state per step,
+    # copied in from pinned host memory and its residual copied back
+    # (icx_form_residuals_host overlaps the copies of consecutive steps); the
+    # same measured one step at a time, each step's copies and kernels in turn
+    h_u = torch.from_numpy(np.tile(wl.u0, (a.steps, 1))).pin_memory()
+    h_r = torch.empty((a.steps, N), dtype=torch.float64).pin_memory()
+    for _ in range(max(a.warmup, 3) // 3):  # warm-up over the same host buffers (first touches from the GPU)
+        wl.ctx.form_residuals_host(h_u, h_r)
+    torch.cuda.synchronize(dev)
+    ms_e2e = wl.ctx.form_residuals_host(h_u, h_r)
+    h_u1, h_r1 = h_u[0], h_r[0]
     e2e_s = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     e2e_e = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     for k in range(a.steps):
         flush.zero_()
         e2e_s[k].record(stream)
-        u.copy_(h_u, non_blocking=True)
+        u.copy_(h_u1, non_blocking=True)
         wl.ctx.form_residual(u, res, stream)
-        h_r.copy_(res, non_blocking=True)
+        h_r1.copy_(res, non_blocking=True)
         e2e_e[k].record(stream)
     torch.cuda.synchronize(dev)
-    ms_e2e = sum(s.elapsed_time(e) for s, e in zip(e2e_s, e2e_e))
+    ms_e2e_seq = sum(s.elapsed_time(e) for s, e in zip(e2e_s, e2e_e))
     if ws > 1:
-        t = torch.tensor([ms, ms_e2e], device=dev, dtype=torch.float64)
+        t = torch.tensor([ms, ms_e2e, ms_e2e_seq], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e = t.tolist()
+        ms, ms_e2e, ms_e2e_seq = t.tolist()
     if rank == 0:
         value = ws * N * a.steps / (ms * 1e-3)
         e2e = ws * N * a.steps / (ms_e2e * 1e-3)
+        e2e_seq = ws * N * a.steps / (ms_e2e_seq * 1e-3)
         work = residual_work(wl)
         tv = float(np.median(t_vol)) * 1e-3
         tf = float(np.median(t_face)) * 1e-3
@@ -412,7 +421,9 @@ def run_ours(a):
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded manufactured solution)",
             "config": dict(WORKLOAD, parallelism=f"replicas x{ws}" if ws > 1 else "single GPU"),
-            "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N},
+            "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N,
+                    "api": "icx_form_residuals_host (copies of consecutive steps overlapped)",
+                    "one_step_at_a_time": e2e_seq},
             "gpu_launches": 2 * a.steps,
             "roofline": {"bound": "hbm",
                          "kernel": "vol_lift_kernel<NS,p3,g2>" if dom == "vol" else "face_flux_kernel<NS,p3,g2,IP>",

@@ -108,6 +108,7 @@ def lib():
             "icx_disc_spacetime_burgers": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
             "icx_spacetime_connect": (C.c_int, [vp, vp, vp]),
             "icx_fespace_basis": (C.c_int, [vp, C.c_int, C.c_int]),
+            "icx_form_residuals_host": (C.c_int, [vp, C.c_int, vp, vp, dp]),
             "icx_disc_navier_stokes": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
             "icx_disc_options": (C.c_int, [vp, C.c_int, C.c_double]),
             "icx_disc_dirichlet": (C.c_int, [vp, C.c_int, POINT_FN, vp]),
@@ -305,6 +306,16 @@ class Context:
 
     def form_residual(self, u, res, stream=None):
         self._check(lib().icx_form_residual(self._h, _ptr(u), _ptr(res), _stream_ptr(stream)), "form_residual")
+
+    def form_residuals_host(self, u, res):
+        """residuals of the states u[k] (host arrays or CPU tensors, [n_states][n_dof],
+        pinned for overlap) into res[k], with the copies of consecutive states
+        overlapped; returns the device time in ms"""
+        n = u.shape[0] if len(u.shape) > 1 else 1
+        ms = C.c_double()
+        self._check(lib().icx_form_residuals_host(self._h, n, _ptr(u), _ptr(res), C.byref(ms)),
+                    "form_residuals_host")
+        return ms.value
 
     def form_residual_noalloc(self, u, res, stream=None):
         """icx_form_residual_noalloc: same result, face scratch in a fixed

@@ -441,6 +441,7 @@ void icx_destroy(icx_ctx* c) {
   icx::free_mdg(c);
   icx::free_explicit(c);
   icx::free_lpc_work(c);
+  icx::free_host_pipe(c);
   free_dev(c->dm);
   for (void* p : c->scratch)
     if (p) cudaFree(p);

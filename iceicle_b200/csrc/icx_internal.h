@@ -109,6 +109,7 @@ struct icx_ctx {
   struct icx_explicit_work* ew = nullptr; // explicit time-stepping buffers (icx_explicit.cu)
   struct icx_lpc* lpc = nullptr;          // learned block preconditioner model (attached, not owned)
   struct icx_lpc_work* lpcw = nullptr;    // its per-context buffers (icx_lpc.cu)
+  struct icx_host_pipe* hp = nullptr;     // streams and staging buffers of icx_form_residuals_host (icx_pipeline.cu)
 };
 
 namespace icx {
@@ -152,6 +153,8 @@ void element_point(const icx_ctx* c, int e, const double xi[2], double x[2]);
 cudaError_t lpc_build(icx_ctx* c, const double* vals, cudaStream_t s);
 cudaError_t lpc_apply(icx_ctx* c, const double* y, double* z, cudaStream_t s);
 void free_lpc_work(icx_ctx* c);
+// releases the host-pipeline streams and buffers (icx_pipeline.cu)
+void free_host_pipe(icx_ctx* c);
 // solver internals the training uses (icx_solver.cu): copy a Jacobian into the
 // solver and build preconditioner `kind` with mixed-precision copies; apply it;
 // the FP32 copy of the Jacobian

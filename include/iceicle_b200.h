@@ -149,6 +149,16 @@ icx_status icx_form_residual(icx_ctx* ctx, const double* d_u, double* d_res, voi
  * calls that overlap on the GPU race and must be serialised by the caller. */
 icx_status icx_form_residual_noalloc(icx_ctx* ctx, const double* d_u, double* d_res, void* stream);
 
+/* form_residual (FR:56-268) for n_states states in host memory: h_u and h_res
+ * hold n_states vectors of n_dof doubles each (page-locked host memory lets
+ * the copies run asynchronously). The copy of state k+1 to the device, the
+ * kernels of state k and the copy of residual k-1 to the host overlap; the
+ * call returns when every residual is in h_res. *elapsed_ms (may be NULL)
+ * is the device time from the first copy to the last, by CUDA events. Uses
+ * the context's residual scratch: no other residual call on this context may
+ * run at the same time. */
+icx_status icx_form_residuals_host(icx_ctx* ctx, int n_states, const double* h_u, double* h_res,
+                                   double* elapsed_ms);
 /* diagnostics: the same computation as icx_form_residual, with CUDA events
  * around each kernel on `stream`; synchronises and returns the two kernel
  * durations in milliseconds (face fluxes, volume + face lifting). */
