@@ -9,6 +9,7 @@
 #include "icx_linalg.h"
 #include "icx_blockrow.cuh"
 #include "icx_blockinv.cuh"
+#include "icx_ilu_rows.cuh"
 
 namespace icx {
 
@@ -412,6 +413,47 @@ static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, const int* order, cons
   ICX_BLOCK_SIZES(ICX_ILUF2_CASE)
 #undef ICX_ILUF2_CASE
   return cudaErrorInvalidValue;
+}
+
+template <class TA>
+static cudaError_t ilu_apply_rows_t(const DeviceMesh& dm, int nx, int ny, const TA* LU, const TA* Uinv,
+                                   const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b,
+                                   unsigned epoch, int* err, cudaStream_t s) {
+  int dev = 0, nsm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  if (nx < 1 || ny < 1 || nx * ny != dm.E) return cudaErrorInvalidValue;
+  const int bs = dm.nb * dm.neq;
+  IluRowArgs<TA> a{nx, ny, dm.nnzb, dm.bsr_rowptr, dm.bsr_colidx, dm.bsr_diag, LU, Uinv, x, f, y, cnt_f, cnt_b,
+                   epoch, err};
+  void* params[] = {&a};
+#define ICX_ROWS_CASE(B)                                                                              \
+  if (bs == B) {                                                                                      \
+    using K = IluRowCfg<B, TA>;                                                                       \
+    if ((e = smem_attr(ilu_apply_rows_kernel<B, TA>, K::SMEM)) != cudaSuccess) return e;              \
+    int per_sm = 0;                                                                                   \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ilu_apply_rows_kernel<B, TA>, 128, K::SMEM); \
+    if (e != cudaSuccess) return e;                                                                   \
+    if ((long long)per_sm * nsm < ny) return cudaErrorNotSupported;                                   \
+    return cudaLaunchCooperativeKernel((const void*)ilu_apply_rows_kernel<B, TA>, dim3(ny), dim3(128), params, \
+                                       K::SMEM, s);                                                   \
+  }
+  ICX_ROWS_CASE(4) ICX_ROWS_CASE(9) ICX_ROWS_CASE(16) ICX_ROWS_CASE(25) ICX_ROWS_CASE(36) ICX_ROWS_CASE(64)
+#undef ICX_ROWS_CASE
+  return cudaErrorNotSupported;
+}
+
+cudaError_t la_ilu_apply_rows(const DeviceMesh& dm, int nx, int ny, const double* LU, const double* Uinv,
+                              const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b, unsigned epoch,
+                              int* err, cudaStream_t s) {
+  return ilu_apply_rows_t<double>(dm, nx, ny, LU, Uinv, x, y, f, cnt_f, cnt_b, epoch, err, s);
+}
+
+cudaError_t la_ilu_apply_rows_f32(const DeviceMesh& dm, int nx, int ny, const float* LU, const float* Uinv,
+                                  const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b,
+                                  unsigned epoch, int* err, cudaStream_t s) {
+  return ilu_apply_rows_t<float>(dm, nx, ny, LU, Uinv, x, y, f, cnt_f, cnt_b, epoch, err, s);
 }
 
 cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, const int* order, const double* LU, const double* Uinv,

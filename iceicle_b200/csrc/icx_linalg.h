@@ -47,6 +47,14 @@ cudaError_t la_ilu_factor(const DeviceMesh& dm, const int* order, const std::vec
 // first apply, never reset afterwards), epoch = 1 for the first apply after
 // zeroing and +1 per apply; *err (device) is set to 1 if a dependency wait
 // timed out, 2 if an index was out of range
+// block-ILU(0) apply pipelined by grid rows (one nx x ny structured grid in
+// natural order); cudaErrorNotSupported when the ny rows cannot all be resident
+cudaError_t la_ilu_apply_rows(const DeviceMesh& dm, int nx, int ny, const double* LU, const double* Uinv,
+                              const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b, unsigned epoch,
+                              int* err, cudaStream_t s);
+cudaError_t la_ilu_apply_rows_f32(const DeviceMesh& dm, int nx, int ny, const float* LU, const float* Uinv,
+                                  const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b,
+                                  unsigned epoch, int* err, cudaStream_t s);
 cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, const int* order, const double* LU, const double* Uinv,
                               const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b, unsigned epoch,
                               int* err, cudaStream_t s);

@@ -43,6 +43,12 @@ struct icx_solver_work {
   std::vector<int> lvl_off; // level l: order[lvl_off[l] .. lvl_off[l+1])
   unsigned* cnt = nullptr;  // 2 x E completion counters of the ILU apply
   unsigned epoch = 0;       // ILU applies since the counters were zeroed
+  // row-pipelined ILU apply: the context is one structured grid whose block
+  // pattern is the 5-point element stencil in natural order
+  bool rows_ok = false;
+  int schedule = 0;         // 0: rows when available, 1: data flow (icx_ilu_apply)
+  unsigned* cnt_rows = nullptr;
+  unsigned epoch_rows = 0;
   int* pc_err = nullptr;    // set by the ILU apply if a dependency wait timed out
   double* dh = nullptr;     // device scalars (dot results)
   int* flag = nullptr;
@@ -108,6 +114,28 @@ icx_status ensure_work(icx_ctx* c, int m) {
     CK(cudaMemcpy(w->order, order.data(), sizeof(int) * dm.E, cudaMemcpyHostToDevice));
   }
   CK(cudaMalloc((void**)&w->lw.partial, sizeof(double) * 64 * 296));
+  CK(cudaMalloc((void**)&w->cnt_rows, sizeof(unsigned) * 2 * dm.E));
+  CK(cudaMemset(w->cnt_rows, 0, sizeof(unsigned) * 2 * dm.E));
+  if (c->parts.empty() && c->nx > 0 && c->ny > 0 && (long long)c->nx * c->ny == dm.E) {
+    // the 5-point element stencil in natural order: row e holds e-nx, e-1, e, e+1, e+nx where they exist
+    std::vector<int> rp(dm.E + 1), ci(dm.nnzb);
+    CK(cudaMemcpy(rp.data(), dm.bsr_rowptr, sizeof(int) * rp.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ci.data(), dm.bsr_colidx, sizeof(int) * ci.size(), cudaMemcpyDeviceToHost));
+    bool ok = true;
+    const int nx = c->nx, ny = c->ny;
+    for (int e = 0; e < dm.E && ok; ++e) {
+      const int i = e % nx, j = e / nx;
+      std::vector<int> want;
+      if (j > 0) want.push_back(e - nx);
+      if (i > 0) want.push_back(e - 1);
+      want.push_back(e);
+      if (i < nx - 1) want.push_back(e + 1);
+      if (j < ny - 1) want.push_back(e + nx);
+      ok = (rp[e + 1] - rp[e]) == (int)want.size();
+      for (size_t k = 0; ok && k < want.size(); ++k) ok = ci[rp[e] + k] == want[k];
+    }
+    w->rows_ok = ok;
+  }
   return ICX_OK;
 }
 
@@ -192,6 +220,16 @@ cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* 
     return e;
   }
   if (kind == 2) {
+    if (w->rows_ok && w->schedule != 1) {
+      const unsigned ep = w->epoch_rows + 1;
+      cudaError_t e = mixed ? icx::la_ilu_apply_rows_f32(dm, c->nx, c->ny, w->pc32, w->uinv32, x, z, w->pct,
+                                                         w->cnt_rows, w->cnt_rows + dm.E, ep, w->pc_err, s)
+                            : icx::la_ilu_apply_rows(dm, c->nx, c->ny, w->pc, w->uinv, x, z, w->pct, w->cnt_rows,
+                                                     w->cnt_rows + dm.E, ep, w->pc_err, s);
+      if (e == cudaSuccess) w->epoch_rows = ep;
+      if (e != cudaErrorNotSupported) return e;
+      w->rows_ok = false;  // the rows cannot all be resident: data-flow apply from now on
+    }
     if (mixed)
       return icx::la_ilu_apply_flow_f32(dm, w->order, w->pc32, w->uinv32, x, z, w->pct, w->cnt, w->cnt + dm.E,
                                         ++w->epoch, w->pc_err, s);
@@ -270,7 +308,9 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
     // the counters are inconsistent after an abandoned apply: start over
     cudaMemsetAsync(w->pc_err, 0, sizeof(int), s);
     cudaMemsetAsync(w->cnt, 0, sizeof(unsigned) * 2 * dm.E, s);
+    cudaMemsetAsync(w->cnt_rows, 0, sizeof(unsigned) * 2 * dm.E, s);
     w->epoch = 0;
+    w->epoch_rows = 0;
     return set_err(c, ICX_ERR_CUDA, perr == 2 ? "block-ILU apply: block index out of range"
                                               : "block-ILU apply: a dependency wait timed out");
   }
@@ -348,8 +388,9 @@ namespace icx {
 void free_solver_work(icx_ctx* c) {
   if (!c || !c->sw) return;
   icx_solver_work* w = c->sw;
-  void* ptrs[] = {w->vals32, w->pc32, w->uinv32, w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du, w->ustep, w->rwork, w->pct, w->order,
-                  w->cnt, w->pc_err, w->dh, w->flag, w->lw.partial};
+  void* ptrs[] = {w->vals32, w->pc32, w->uinv32, w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du,
+                  w->ustep, w->rwork, w->pct, w->pct2, w->pct3, w->pct4, w->order, w->cnt, w->cnt_rows, w->pc_err,
+                  w->dh, w->flag, w->lw.partial};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete w;
@@ -420,6 +461,42 @@ icx_status icx_gmres_solve(icx_ctx* c, const double* d_vals, const double* d_b, 
   if (relres) *relres = rr;
   if (st != ICX_OK) return st;
   return rr <= rtol ? ICX_OK : ICX_ERR_NOT_CONVERGED;
+}
+
+icx_status icx_ilu_apply(icx_ctx* c, const double* d_vals, const double* d_x, double* d_y, int precision,
+                         int schedule) {
+  if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
+  if (!d_vals || !d_x || !d_y || d_x == d_y) return set_err(c, ICX_ERR_INVALID, "null or aliased device pointer");
+  if (precision < 0 || precision > 1 || schedule < 0 || schedule > 2)
+    return set_err(c, ICX_ERR_INVALID, "precision 0..1, schedule 0..2");
+  cudaStream_t s = 0;
+  icx_status st = ensure_work(c, 30);
+  if (st != ICX_OK) return st;
+  const bool mixed = precision == 1;
+  if (mixed && (st = ensure_mixed(c)) != ICX_OK) return st;
+  icx_solver_work* w = c->sw;
+  if (schedule == 2 && !w->rows_ok)
+    return set_err(c, ICX_ERR_UNSUPPORTED, "row-pipelined apply needs one structured grid with the 5-point pattern");
+  CK(cudaMemcpyAsync(w->vals, d_vals, sizeof(double) * (size_t)c->dm.nnzb * w->bs * w->bs, cudaMemcpyDeviceToDevice,
+                     s));
+  CK(build_pc(c, 2, mixed, s));
+  w->schedule = schedule == 1 ? 1 : 0;
+  cudaError_t e = apply_pc(c, 2, mixed, d_x, d_y, s);
+  w->schedule = 0;
+  CK(e);
+  int perr = 0;
+  CK(cudaMemcpyAsync(&perr, w->pc_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (perr) {
+    cudaMemsetAsync(w->pc_err, 0, sizeof(int), s);
+    cudaMemsetAsync(w->cnt, 0, sizeof(unsigned) * 2 * c->dm.E, s);
+    cudaMemsetAsync(w->cnt_rows, 0, sizeof(unsigned) * 2 * c->dm.E, s);
+    w->epoch = 0;
+    w->epoch_rows = 0;
+    return set_err(c, ICX_ERR_CUDA, perr == 2 ? "block-ILU apply: block index out of range"
+                                              : "block-ILU apply: a dependency wait timed out");
+  }
+  return ICX_OK;
 }
 
 icx_status icx_krylov_samples(icx_ctx* c, const double* d_vals, const double* d_b, double* d_x, int restart, int maxit,

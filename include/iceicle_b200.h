@@ -282,6 +282,14 @@ typedef struct icx_newton_report {
 icx_status icx_gmres_solve(icx_ctx* ctx, const double* d_vals, const double* d_b, double* d_x, int restart,
                            int maxit, double rtol, int preconditioner, int* iterations, double* relres, void* stream);
 
+/* y = M^-1 x for the block-ILU(0) preconditioner of the BSR matrix d_vals
+ * (the factors icx_gmres_solve / icx_newton_solve build; precision 1: from
+ * FP32 copies with FP32 accumulation). schedule 0: the solvers' choice (the
+ * row-pipelined apply on one structured grid, else the data-flow apply);
+ * 1: the data-flow apply; 2: the row-pipelined apply (ICX_ERR_UNSUPPORTED
+ * when the context is not one grid with the 5-point element pattern). */
+icx_status icx_ilu_apply(icx_ctx* ctx, const double* d_vals, const double* d_x, double* d_y, int precision,
+                         int schedule);
 icx_status icx_newton_default_options(icx_newton_options* opt);
 icx_status icx_newton_solve(icx_ctx* ctx, double* d_u, const icx_newton_options* opt, icx_newton_report* rep);
 /* MFNK (matrix_free_newton_krylov.hpp:62-365) without geometry unknowns:
