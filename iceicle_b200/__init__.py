@@ -309,8 +309,8 @@ class Context:
         self._check(lib().icx_form_residual(self._h, _ptr(u), _ptr(res), _stream_ptr(stream)), "form_residual")
 
     def ilu_apply(self, vals, x, y, precision=0, schedule=0):
-        """y = M^-1 x with the block-ILU(0) factors of vals (schedule 0 auto,
-        1 data flow, 2 row-pipelined)"""
+        """y = M^-1 x with the block-ILU(0) factors of vals (schedule 0 or 1:
+        the solvers' data-flow apply, 2: row-pipelined)"""
         self._check(lib().icx_ilu_apply(self._h, _ptr(vals), _ptr(x), _ptr(y), precision, schedule), "ilu_apply")
 
     def form_residuals_host(self, u, res):

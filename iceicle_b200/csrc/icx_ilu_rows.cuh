@@ -63,7 +63,7 @@ struct IluRowCfg {
   static constexpr int J = (Q + THREADS - 1) / THREADS; // vectors per thread and block
   static constexpr int MAXB = 3;                        // blocks per element and sweep
   static constexpr int STAGE = MAXB * BS * BS;          // TA per prefetch stage
-  static constexpr int STAGES = (2 * STAGE * sizeof(TA) <= 100 * 1024) ? 2 : 1;
+  static constexpr int STAGES = (2 * STAGE * sizeof(TA) <= 200 * 1024) ? 2 : 1;
   static constexpr size_t TA_BYTES = (sizeof(TA) * (STAGES * STAGE + Q + MAXB * BS) + 15) / 16 * 16;
   static constexpr size_t SMEM = TA_BYTES + sizeof(double) * BS + 16;
 };
@@ -113,13 +113,12 @@ __device__ inline bool row_wait(const unsigned* c, unsigned target, int* err, in
   return *reinterpret_cast<volatile int*>(s_flag) != 0;
 }
 
-// the CTA's stores of this element are complete (barrier), then one release
+// the CTA's stores of this element are ordered before thread 0's release by
+// the barrier (causality through the CTA-scope barrier and the gpu-scope
+// release / acquire pair, as the warp-level signal of the data-flow apply)
 __device__ inline void row_signal(unsigned* c) {
   __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(c) : "memory");
-  }
+  if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(c) : "memory");
 }
 
 template <int BS, class TA>

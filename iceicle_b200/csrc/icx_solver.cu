@@ -46,7 +46,7 @@ struct icx_solver_work {
   // row-pipelined ILU apply: the context is one structured grid whose block
   // pattern is the 5-point element stencil in natural order
   bool rows_ok = false;
-  int schedule = 0;         // 0: rows when available, 1: data flow (icx_ilu_apply)
+  int schedule = 0;         // 0 / 1: data flow (the solvers' apply), 2: rows (icx_ilu_apply only)
   unsigned* cnt_rows = nullptr;
   unsigned epoch_rows = 0;
   int* pc_err = nullptr;    // set by the ILU apply if a dependency wait timed out
@@ -220,7 +220,7 @@ cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* 
     return e;
   }
   if (kind == 2) {
-    if (w->rows_ok && w->schedule != 1) {
+    if (w->rows_ok && w->schedule == 2) {
       const unsigned ep = w->epoch_rows + 1;
       cudaError_t e = mixed ? icx::la_ilu_apply_rows_f32(dm, c->nx, c->ny, w->pc32, w->uinv32, x, z, w->pct,
                                                          w->cnt_rows, w->cnt_rows + dm.E, ep, w->pc_err, s)
@@ -480,7 +480,7 @@ icx_status icx_ilu_apply(icx_ctx* c, const double* d_vals, const double* d_x, do
   CK(cudaMemcpyAsync(w->vals, d_vals, sizeof(double) * (size_t)c->dm.nnzb * w->bs * w->bs, cudaMemcpyDeviceToDevice,
                      s));
   CK(build_pc(c, 2, mixed, s));
-  w->schedule = schedule == 1 ? 1 : 0;
+  w->schedule = schedule;
   cudaError_t e = apply_pc(c, 2, mixed, d_x, d_y, s);
   w->schedule = 0;
   CK(e);

@@ -284,10 +284,11 @@ icx_status icx_gmres_solve(icx_ctx* ctx, const double* d_vals, const double* d_b
 
 /* y = M^-1 x for the block-ILU(0) preconditioner of the BSR matrix d_vals
  * (the factors icx_gmres_solve / icx_newton_solve build; precision 1: from
- * FP32 copies with FP32 accumulation). schedule 0: the solvers' choice (the
- * row-pipelined apply on one structured grid, else the data-flow apply);
- * 1: the data-flow apply; 2: the row-pipelined apply (ICX_ERR_UNSUPPORTED
- * when the context is not one grid with the 5-point element pattern). */
+ * FP32 copies with FP32 accumulation). schedule 0 or 1: the data-flow apply
+ * the solvers use; 2: the row-pipelined apply, one CTA per grid row
+ * (ICX_ERR_UNSUPPORTED when the context is not one grid with the 5-point
+ * element pattern; it is slower than the data-flow apply on the measured
+ * workloads). */
 icx_status icx_ilu_apply(icx_ctx* ctx, const double* d_vals, const double* d_x, double* d_y, int precision,
                          int schedule);
 icx_status icx_newton_default_options(icx_newton_options* opt);
