@@ -365,35 +365,36 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
       for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
       const double* vsrc = fwd ? a.f : a.y;
       unsigned* cnt = fwd ? a.cnt_f : a.cnt_b;
+      // every dependency first (backward: also the element's own forward
+      // result), then all the vectors in one round of loads, so that the
+      // second neighbour's load does not add another L2 round trip
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        if (b < nbk && !flow_wait(cnt + ks[b], target, a.err)) return;
+      if (!fwd && !flow_wait(a.cnt_f + e, target, a.err)) return;
+      TA xv[3][NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int c = lane + 32 * s;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) xv[b][s] = (b < nbk && c < BS) ? (TA)__ldcg(vsrc + (size_t)ks[b] * BS + c) : TA(0);
+        xv[2][s] = (!fwd && c < BS) ? (TA)__ldcg(a.f + (size_t)e * BS + c) : TA(0);
+      }
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         if (b < nbk) {
-          if (!flow_wait(cnt + ks[b], target, a.err)) return;
-          TA xv[NS];
-#pragma unroll
-          for (int s = 0; s < NS; ++s) {
-            const int c = lane + 32 * s;
-            xv[s] = c < BS ? (TA)__ldcg(vsrc + (size_t)ks[b] * BS + c) : TA(0);
-          }
 #pragma unroll
           for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-            for (int s = 0; s < NS; ++s) acc[rr] -= am[b][rr][s] * xv[s];
+            for (int s = 0; s < NS; ++s) acc[rr] -= am[b][rr][s] * xv[b][s];
         }
       }
       if (!fwd) {
-        // y_e = inv(U_ee) f_e + acc: f_e is complete once its forward counter is
-        if (!flow_wait(a.cnt_f + e, target, a.err)) return;
-        TA xv[NS];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-          const int c = lane + 32 * s;
-          xv[s] = c < BS ? (TA)__ldcg(a.f + (size_t)e * BS + c) : TA(0);
-        }
+        // y_e = inv(U_ee) f_e + acc
 #pragma unroll
         for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-          for (int s = 0; s < NS; ++s) acc[rr] += am[2][rr][s] * xv[s];
+          for (int s = 0; s < NS; ++s) acc[rr] += am[2][rr][s] * xv[2][s];
       }
 #pragma unroll
       for (int rr = 0; rr < R; ++rr) {
