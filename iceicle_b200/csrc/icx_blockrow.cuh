@@ -291,6 +291,37 @@ __device__ inline bool flow_wait(const unsigned* c, unsigned target, int* err) {
   return ok != 0;
 }
 
+// up to three counters at once: lane k < n polls counter k with acquire loads
+// until every one has reached target (warp vote), so the waits overlap; the
+// same bound and error flag as flow_wait. __syncwarp then orders each lane's
+// acquire before the loads of every lane.
+__device__ inline bool flow_wait_n(const unsigned* c0, const unsigned* c1, const unsigned* c2, int n,
+                                   unsigned target, int* err) {
+  const int lane = threadIdx.x & 31;
+  const unsigned* c = lane == 0 ? c0 : (lane == 1 ? c1 : c2);
+  bool done = lane >= n;
+  unsigned spins = 0;
+  int ok = 1;
+  while (true) {
+    if (!done) done = (int)(ld_acquire_u32(c) - target) >= 0;
+    if (__all_sync(0xffffffffu, done)) break;
+    int stop = 0;
+    if (lane == 0) {
+      if (*reinterpret_cast<volatile int*>(err)) stop = 1;
+      else if (++spins > ICX_FLOW_SPINS) {
+        atomicExch(err, 1);
+        stop = 1;
+      }
+    }
+    if (__shfl_sync(0xffffffffu, stop, 0)) {
+      ok = 0;
+      break;
+    }
+  }
+  __syncwarp();
+  return ok != 0;
+}
+
 // the warp's stores happen before the increment (release at gpu scope,
 // cumulative over the lanes' stores ordered by __syncwarp)
 __device__ inline void flow_signal(unsigned* c) {
@@ -368,10 +399,13 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
       // every dependency first (backward: also the element's own forward
       // result), then all the vectors in one round of loads, so that the
       // second neighbour's load does not add another L2 round trip
-#pragma unroll
-      for (int b = 0; b < 2; ++b)
-        if (b < nbk && !flow_wait(cnt + ks[b], target, a.err)) return;
-      if (!fwd && !flow_wait(a.cnt_f + e, target, a.err)) return;
+      {
+        // counters: the nbk neighbours, then (backward) the element's own forward one
+        const unsigned* w0 = nbk > 0 ? cnt + ks[0] : a.cnt_f + e;
+        const unsigned* w1 = nbk > 1 ? cnt + ks[1] : a.cnt_f + e;
+        const int nw = nbk + (fwd ? 0 : 1);
+        if (nw > 0 && !flow_wait_n(w0, w1, a.cnt_f + e, nw, target, a.err)) return;
+      }
       TA xv[3][NS];
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
