@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--spmv", type=int, default=0, metavar="N",
                     help="only time the FP64 BSR SpMV of the N x N p = 2 Navier-Stokes Jacobian (36 x 36 blocks) "
                          "and print one JSON line")
+    ap.add_argument("--ilu", type=int, default=0, metavar="N",
+                    help="only time the block-ILU(0) apply (data-flow and row-pipelined, FP64 and FP32 factors) "
+                         "of the N x N p = 2 Navier-Stokes Jacobian and print one JSON line")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-preconditioner Newton comparison (256 x 256 Navier-Stokes, p = 2)")
     ap.add_argument("--batched", type=int, default=64, metavar="N",
@@ -300,6 +303,32 @@ def spmv_bench(n):
                       "GBs": nbytes / ms / 1e6}))
 
 
+def ilu_bench(n):
+    """block-ILU(0) apply of the FD Jacobian of the n x n p = 2 Navier-Stokes
+    manufactured solution: mean of 20 applies after 3 untimed ones, per
+    schedule and precision (CUDA events inside icx_ilu_apply)"""
+    import torch
+    from iceicle_b200.workloads import ns_mms_config
+    dev = torch.device("cuda", 0)
+    wl = ns_mms_config(nx=n, ny=n, p=2, geo_order=2, mu=0.01)
+    ctx, L = wl.ctx, wl.ctx.layout
+    bs = L.block_size
+    u = torch.from_numpy(wl.u0).to(dev)
+    res = torch.empty_like(u)
+    vals = torch.empty(L.nnz_blocks * bs * bs, dtype=torch.float64, device=dev)
+    ctx.form_jacobian_fd(u, res, vals)
+    x = torch.randn(L.n_dof, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
+    y = torch.empty_like(x)
+    out = {"ilu": f"ns_mms_{n}x{n}_p2", "block": bs, "levels_per_sweep": 2 * n - 1}
+    for sched, name in ((1, "data_flow"), (2, "rows")):
+        for prec, pn in ((0, "fp64"), (1, "fp32")):
+            ctx.ilu_apply(vals, x, y, prec, sched, 3)
+            out[f"{name}_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, sched, 20)
+    # bytes one apply must read: the off-diagonal factor blocks and the E diagonal inverses (one matrix's worth)
+    out["factor_bytes_fp64"] = L.nnz_blocks * bs * bs * 8
+    print(json.dumps(out))
+
+
 def learned_bench(torch, dev):
     """Newton solve time to |r| <= 1e-10 on one fresh seeded instance of the
     256 x 256 p = 2 Navier-Stokes manufactured solution (Re drawn from
@@ -464,6 +493,8 @@ def main():
     a = parse()
     if a.spmv:
         spmv_bench(a.spmv)
+    elif a.ilu:
+        ilu_bench(a.ilu)
     elif a.impl == "reference":
         run_reference(a)
     else:

@@ -109,7 +109,7 @@ def lib():
             "icx_spacetime_connect": (C.c_int, [vp, vp, vp]),
             "icx_fespace_basis": (C.c_int, [vp, C.c_int, C.c_int]),
             "icx_form_residuals_host": (C.c_int, [vp, C.c_int, vp, vp, dp]),
-            "icx_ilu_apply": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int]),
+            "icx_ilu_apply": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, dp]),
             "icx_disc_navier_stokes": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
             "icx_disc_options": (C.c_int, [vp, C.c_int, C.c_double]),
             "icx_disc_dirichlet": (C.c_int, [vp, C.c_int, POINT_FN, vp]),
@@ -308,10 +308,14 @@ class Context:
     def form_residual(self, u, res, stream=None):
         self._check(lib().icx_form_residual(self._h, _ptr(u), _ptr(res), _stream_ptr(stream)), "form_residual")
 
-    def ilu_apply(self, vals, x, y, precision=0, schedule=0):
+    def ilu_apply(self, vals, x, y, precision=0, schedule=0, repeat=1):
         """y = M^-1 x with the block-ILU(0) factors of vals (schedule 0 or 1:
-        the solvers' data-flow apply, 2: row-pipelined)"""
-        self._check(lib().icx_ilu_apply(self._h, _ptr(vals), _ptr(x), _ptr(y), precision, schedule), "ilu_apply")
+        the solvers' data-flow apply, 2: row-pipelined), applied `repeat`
+        times after one factorization; returns the mean ms per apply"""
+        ms = C.c_double()
+        self._check(lib().icx_ilu_apply(self._h, _ptr(vals), _ptr(x), _ptr(y), precision, schedule, repeat,
+                                        C.byref(ms)), "ilu_apply")
+        return ms.value
 
     def form_residuals_host(self, u, res):
         """residuals of the states u[k] (host arrays or CPU tensors, [n_states][n_dof],

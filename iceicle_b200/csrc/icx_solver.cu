@@ -464,11 +464,11 @@ icx_status icx_gmres_solve(icx_ctx* c, const double* d_vals, const double* d_b, 
 }
 
 icx_status icx_ilu_apply(icx_ctx* c, const double* d_vals, const double* d_x, double* d_y, int precision,
-                         int schedule) {
+                         int schedule, int repeat, double* ms_per_apply) {
   if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
   if (!d_vals || !d_x || !d_y || d_x == d_y) return set_err(c, ICX_ERR_INVALID, "null or aliased device pointer");
-  if (precision < 0 || precision > 1 || schedule < 0 || schedule > 2)
-    return set_err(c, ICX_ERR_INVALID, "precision 0..1, schedule 0..2");
+  if (precision < 0 || precision > 1 || schedule < 0 || schedule > 2 || repeat < 1)
+    return set_err(c, ICX_ERR_INVALID, "precision 0..1, schedule 0..2, repeat >= 1");
   cudaStream_t s = 0;
   icx_status st = ensure_work(c, 30);
   if (st != ICX_OK) return st;
@@ -481,8 +481,24 @@ icx_status icx_ilu_apply(icx_ctx* c, const double* d_vals, const double* d_x, do
                      s));
   CK(build_pc(c, 2, mixed, s));
   w->schedule = schedule;
-  cudaError_t e = apply_pc(c, 2, mixed, d_x, d_y, s);
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  if (ms_per_apply) {
+    CK(cudaEventCreate(&ev[0]));
+    CK(cudaEventCreate(&ev[1]));
+    CK(cudaEventRecord(ev[0], s));
+  }
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < repeat && e == cudaSuccess; ++k) e = apply_pc(c, 2, mixed, d_x, d_y, s);
   w->schedule = 0;
+  if (ms_per_apply && e == cudaSuccess) {
+    float ms = 0.f;
+    e = cudaEventRecord(ev[1], s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    *ms_per_apply = (double)ms / repeat;
+  }
+  for (cudaEvent_t x : ev)
+    if (x) cudaEventDestroy(x);
   CK(e);
   int perr = 0;
   CK(cudaMemcpyAsync(&perr, w->pc_err, sizeof(int), cudaMemcpyDeviceToHost, s));

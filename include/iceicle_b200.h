@@ -288,9 +288,10 @@ icx_status icx_gmres_solve(icx_ctx* ctx, const double* d_vals, const double* d_b
  * the solvers use; 2: the row-pipelined apply, one CTA per grid row
  * (ICX_ERR_UNSUPPORTED when the context is not one grid with the 5-point
  * element pattern; it is slower than the data-flow apply on the measured
- * workloads). */
+ * workloads). The apply runs `repeat` times after one factorization;
+ * *ms_per_apply (may be NULL) is its mean device time by CUDA events. */
 icx_status icx_ilu_apply(icx_ctx* ctx, const double* d_vals, const double* d_x, double* d_y, int precision,
-                         int schedule);
+                         int schedule, int repeat, double* ms_per_apply);
 icx_status icx_newton_default_options(icx_newton_options* opt);
 icx_status icx_newton_solve(icx_ctx* ctx, double* d_u, const icx_newton_options* opt, icx_newton_report* rep);
 /* MFNK (matrix_free_newton_krylov.hpp:62-365) without geometry unknowns:

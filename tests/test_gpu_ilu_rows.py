@@ -38,7 +38,7 @@ def test_row_pipelined_apply_matches_data_flow_apply(kw, precision, tol):
         x = torch.from_numpy(rng.standard_normal(L.n_dof)).cuda()
         y_flow, y_rows = torch.empty_like(x), torch.empty_like(x)
         ctx.ilu_apply(vals, x, y_flow, precision, 1)
-        ctx.ilu_apply(vals, x, y_rows, precision, 2)
+        ctx.ilu_apply(vals, x, y_rows, precision, 2, repeat=2)
         torch.cuda.synchronize()
         scale = float(y_flow.abs().max())
         assert float((y_rows - y_flow).abs().max()) <= tol * scale
