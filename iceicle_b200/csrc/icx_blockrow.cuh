@@ -268,33 +268,20 @@ struct IluFlowArgs {
   int* err;
 };
 
-// lane 0 polls *c with acquire loads until it reaches target (wrap-safe);
-// false on timeout or error. The acquire orders the warp's later loads of the
-// producer's data after the observation (then __syncwarp for the other lanes).
+// acquire load of a completion counter: the waiting warp's later loads of the
+// producer's data are ordered after the observation (__syncwarp then orders
+// them for the other lanes); counters are compared wrap-safe
 __device__ inline unsigned ld_acquire_u32(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
 
-__device__ inline bool flow_wait(const unsigned* c, unsigned target, int* err) {
-  int ok = 1;
-  if ((threadIdx.x & 31) == 0) {
-    unsigned spins = 0;
-    while ((int)(ld_acquire_u32(c) - target) < 0) {
-      if (*reinterpret_cast<volatile int*>(err)) { ok = 0; break; }
-      if (++spins > ICX_FLOW_SPINS) { atomicExch(err, 1); ok = 0; break; }
-    }
-  }
-  ok = __shfl_sync(0xffffffffu, ok, 0);
-  __syncwarp();
-  return ok != 0;
-}
-
 // up to three counters at once: lane k < n polls counter k with acquire loads
-// until every one has reached target (warp vote), so the waits overlap; the
-// same bound and error flag as flow_wait. __syncwarp then orders each lane's
-// acquire before the loads of every lane.
+// until every one has reached target (warp vote), so the waits overlap. At most
+// ICX_FLOW_SPINS polls: then *err = 1; a set *err ends the wait early. Returns
+// false in both cases. __syncwarp then orders each lane's acquire before the
+// loads of every lane.
 __device__ inline bool flow_wait_n(const unsigned* c0, const unsigned* c1, const unsigned* c2, int n,
                                    unsigned target, int* err) {
   const int lane = threadIdx.x & 31;
