@@ -559,7 +559,7 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
     return ICX_ERR_NONFINITE;
   }
   double tol = rtol * bnorm;
-  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hcol(m + 2), hp(m + 1);
+  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hcol(m + 2), hp3(3 * (m + 2));
   GCK(cudaMemcpyAsync(kb.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   double beta = bnorm;
   int total = 0;
@@ -583,16 +583,20 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
       } else {
         GCK(A(vj, vj1));
       }
-      // classical Gram-Schmidt, twice
+      // classical Gram-Schmidt, twice, and the norm of the result: the three
+      // reductions land in separate device slots [pass 1 | pass 2 | |v|^2]
+      // and come back to the host in one copy
       std::fill(hcol.begin(), hcol.end(), 0.0);
       for (int pass = 0; pass < 2; ++pass) {
-        GCK(la_mdot(*kb.lw, n, kb.V, n, j + 1, vj1, kb.dh, s));
-        GCK(la_maxpy(n, kb.V, n, j + 1, kb.dh, -1.0, vj1, s));
-        GCK(cudaMemcpyAsync(hp.data(), kb.dh, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, s));
-        GCK(cudaStreamSynchronize(s));
-        for (int i = 0; i <= j; ++i) hcol[i] += hp[i];
+        double* slot = kb.dh + (size_t)pass * (m + 2);
+        GCK(la_mdot(*kb.lw, n, kb.V, n, j + 1, vj1, slot, s));
+        GCK(la_maxpy(n, kb.V, n, j + 1, slot, -1.0, vj1, s));
       }
-      double hn = la_norm(*kb.lw, n, vj1, kb.dh, s);
+      GCK(la_mdot(*kb.lw, n, vj1, 0, 1, vj1, kb.dh + 2 * (m + 2), s));
+      GCK(cudaMemcpyAsync(hp3.data(), kb.dh, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, s));
+      GCK(cudaStreamSynchronize(s));
+      for (int i = 0; i <= j; ++i) hcol[i] += hp3[i] + hp3[(m + 2) + i];
+      double hn = std::sqrt(hp3[2 * (m + 2)]);
       hcol[j + 1] = hn;
       if (!std::isfinite(hn)) {
         if (err) *err = "non-finite Krylov vector";

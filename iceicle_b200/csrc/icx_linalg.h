@@ -78,7 +78,7 @@ struct KrylovBuffers {
   double* w = nullptr;
   double* z = nullptr;
   double* r = nullptr;
-  double* dh = nullptr;  // >= m + 2 device doubles
+  double* dh = nullptr;  // >= 3 (m + 2) device doubles
   LinalgWork* lw = nullptr;
   // optional Krylov samples: the true residual at every restart and every
   // `sample_every`-th Arnoldi vector, copied into samples[count] while count < cap

@@ -1010,7 +1010,7 @@ icx_status ensure_lm(icx_ctx* c, int m) {
   if (s.d_kV) cudaFree(s.d_kV);
   MCK(cudaMalloc((void**)&s.d_kV, sizeof(double) * (size_t)(m + 1) * n));
   if (s.d_kdh) cudaFree(s.d_kdh);
-  MCK(cudaMalloc((void**)&s.d_kdh, sizeof(double) * 2 * (m + 2)));
+  MCK(cudaMalloc((void**)&s.d_kdh, sizeof(double) * 3 * (m + 2)));
   if (!s.lw.partial) MCK(cudaMalloc((void**)&s.lw.partial, sizeof(double) * 64 * 296));
   s.kb.n = n;
   s.kb.m = m;

@@ -95,7 +95,7 @@ icx_status ensure_work(icx_ctx* c, int m) {
   CK(cudaMalloc((void**)&w->V, sizeof(double) * (size_t)(m + 1) * n));
   double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork, &w->pct, &w->pct2, &w->pct3, &w->pct4};
   for (double** p : vecs) CK(cudaMalloc((void**)p, sizeof(double) * n));
-  CK(cudaMalloc((void**)&w->dh, sizeof(double) * 2 * (m + 2)));
+  CK(cudaMalloc((void**)&w->dh, sizeof(double) * 3 * (m + 2)));
   CK(cudaMalloc((void**)&w->flag, sizeof(int)));
   CK(cudaMalloc((void**)&w->pc_err, sizeof(int)));
   CK(cudaMemset(w->pc_err, 0, sizeof(int)));
