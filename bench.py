@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--batched", type=int, default=64, metavar="N",
                     help="secondary timing of N seeded uneven advection-diffusion problems, batched vs one at a "
                          "time (0: skip; the full problem set is 512)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="time the compiled default launch shapes instead of the autotuned ones")
     return ap.parse_args()
 
 
@@ -233,12 +235,14 @@ def batched_bench(torch, dev, n_problems):
             "speedup": t_seq / t_batch if t_batch > 0 else None, "max_state_rel_diff": worst, "groups": its}
 
 
-def newton_bench(torch, dev):
+def newton_bench(torch, dev, tune=True):
     """Newton solve time to |r| <= 1e-10 (FP64 residual), all-FP64 vs mixed
     precision (FP32 Jacobian and preconditioner copies): 32 x 32 viscous
     Burgers p=2 and the 128 x 128 Navier-Stokes manufactured solution p=3,
     both with GMRES(30) + block-ILU(0) and the Wolfe line search. Timed with
-    CUDA events around the whole solve (it synchronises internally)."""
+    CUDA events around the whole solve (it synchronises internally). With
+    `tune`, the residual and ILU launch shapes are autotuned at the initial
+    state first (outside the timed solves)."""
     import iceicle_b200 as ib
     from iceicle_b200.workloads import burgers_config, ns_mms_config
     out = {}
@@ -247,6 +251,11 @@ def newton_bench(torch, dev):
                                                                     device=dev.index))):
         wl = make()
         rows = {}
+        if tune:
+            t = wl.ctx.autotune(torch.from_numpy(wl.u0).to(dev),
+                                ib.TUNE_RESIDUAL | ib.TUNE_ILU | ib.TUNE_ILU_FP32)
+            rows["autotune"] = {"chosen": t["chosen"], "from_cache": t["from_cache"],
+                                "ilu_ms_default": t["ilu_ms_default"], "ilu_ms_tuned": t["ilu_ms_tuned"]}
         states = {}
         for label, prec in (("fp64", 0), ("mixed", 1)):
             opt = ib.default_newton_options()
@@ -324,12 +333,19 @@ def ilu_bench(n):
         for prec, pn in ((0, "fp64"), (1, "fp32")):
             ctx.ilu_apply(vals, x, y, prec, sched, 3)
             out[f"{name}_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, sched, 20)
+    # the data-flow apply again with the autotuned rows per task and CTAs per SM
+    import iceicle_b200 as ib
+    t = ctx.autotune(u, ib.TUNE_ILU | ib.TUNE_ILU_FP32)
+    out["tuned_tile"] = {"ilu_rows": t["chosen"]["ilu_rows"], "ilu_ctas": t["chosen"]["ilu_ctas"]}
+    for prec, pn in ((0, "fp64"), (1, "fp32")):
+        ctx.ilu_apply(vals, x, y, prec, 1, 3)
+        out[f"data_flow_tuned_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 1, 20)
     # bytes one apply must read: the off-diagonal factor blocks and the E diagonal inverses (one matrix's worth)
     out["factor_bytes_fp64"] = L.nnz_blocks * bs * bs * 8
     print(json.dumps(out))
 
 
-def learned_bench(torch, dev):
+def learned_bench(torch, dev, tune=True):
     """Newton solve time to |r| <= 1e-10 on one fresh seeded instance of the
     256 x 256 p = 2 Navier-Stokes manufactured solution (Re drawn from
     [50, 500]): the plain all-FP64 GMRES(30) + block-ILU(0) solve against the
@@ -345,6 +361,11 @@ def learned_bench(torch, dev):
     sw = m.sweeps if m.sweeps is not None else 2
     seed, re = lp.instances(*lp.EVAL_INSTANCES)[0]
     wl = lp.make_instance(seed, re, 256, dev.index)
+    tuned = None
+    if tune:  # launch shapes for every solve below, chosen at the initial state
+        import iceicle_b200 as ib
+        t = wl.ctx.autotune(torch.from_numpy(wl.u0).to(dev), ib.TUNE_RESIDUAL | ib.TUNE_ILU | ib.TUNE_ILU_FP32)
+        tuned = {"chosen": t["chosen"], "ilu_ms_default": t["ilu_ms_default"], "ilu_ms_tuned": t["ilu_ms_tuned"]}
     plain, u_p = lp.solve(wl, None, 2, 0, device=dev.index)
     mixed, _ = lp.solve(wl, None, 2, 1, device=dev.index)
     learned, u_l = lp.solve(wl, m, 5, 1, sw, dev.index)
@@ -353,7 +374,7 @@ def learned_bench(torch, dev):
     return {"instance": {"seed": seed, "re": re, "mesh": "256x256", "p": 2, "n_dof": 256 * 256 * 36},
             "model": {"params": m.n_params, "pc_sweeps": sw, "file": "iceicle_b200/data/learned_pc_ns_p2.npz"},
             "plain_fp64_ilu0": plain, "mixed_ilu0": mixed, "learned_mixed": learned,
-            "parallel_ilu_mixed_untrained": parallel,
+            "parallel_ilu_mixed_untrained": parallel, "autotune": tuned,
             "learned_vs_plain_state_l2": float(np.linalg.norm(u_l - u_p) / np.linalg.norm(u_p)),
             "speedup_learned_mixed_vs_plain_fp64": plain["s"] / learned["s"],
             "speedup_mixed_ilu0_vs_plain_fp64": plain["s"] / mixed["s"],
@@ -376,6 +397,10 @@ def run_ours(a):
     res = torch.empty_like(u)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    # launch shapes of the face and volume kernels for this (p, neq), chosen
+    # once before any timing (every shape computes identical values)
+    import iceicle_b200 as ib
+    tune = None if a.no_tune else wl.ctx.autotune(u, ib.TUNE_RESIDUAL)
     for _ in range(max(a.warmup, 3)):
         wl.ctx.form_residual(u, res, stream)
     torch.cuda.synchronize(dev)
@@ -468,6 +493,10 @@ def run_ours(a):
                                           "achieved_gbs": work["face" if dom == "vol" else "vol"][0] /
                                           (tf if dom == "vol" else tv) / 1e9}},
             "clocks": clocks,
+            "autotune": None if tune is None else {
+                "chosen": {k: tune["chosen"][k] for k in ("face_minb", "vol_threads", "vol_minb")},
+                "residual_ms_default": tune["residual_ms_default"], "residual_ms_tuned": tune["residual_ms_tuned"],
+                "shapes_timed": tune["n_timed"], "rejected": tune["n_rejected"]},
         }
         if not a.no_cpu_baseline and ws == 1:
             sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -479,11 +508,11 @@ def run_ours(a):
             else:
                 line["cpu_baseline"] = None
         if not a.no_newton and ws == 1:
-            line["newton"] = newton_bench(torch, dev)
+            line["newton"] = newton_bench(torch, dev, not a.no_tune)
         if a.batched and ws == 1:
             line["batched"] = batched_bench(torch, dev, a.batched)
         if not a.no_learned and ws == 1:
-            line["learned_pc"] = learned_bench(torch, dev)
+            line["learned_pc"] = learned_bench(torch, dev, not a.no_tune)
         print(json.dumps(line))
     if ws > 1:
         dist.destroy_process_group()

@@ -84,6 +84,25 @@ class LpcTrainReport(C.Structure):
                 ("loss_history", C.c_double * 64)]
 
 
+class TileChoice(C.Structure):
+    """launch shapes of the tunable kernels (0: the compiled default)"""
+    _fields_ = [("face_minb", C.c_int), ("vol_threads", C.c_int), ("vol_minb", C.c_int),
+                ("ilu_rows", C.c_int * 2), ("ilu_ctas", C.c_int * 2)]
+
+    def as_dict(self):
+        return {"face_minb": self.face_minb, "vol_threads": self.vol_threads, "vol_minb": self.vol_minb,
+                "ilu_rows": list(self.ilu_rows), "ilu_ctas": list(self.ilu_ctas)}
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("chosen", TileChoice), ("from_cache", C.c_int), ("n_timed", C.c_int), ("n_rejected", C.c_int),
+                ("residual_ms_default", C.c_double), ("residual_ms_tuned", C.c_double),
+                ("ilu_ms_default", C.c_double * 2), ("ilu_ms_tuned", C.c_double * 2)]
+
+
+TUNE_RESIDUAL, TUNE_ILU, TUNE_ILU_FP32, TUNE_RETIME = 1, 2, 4, 8
+
+
 _lib = None
 
 
@@ -159,6 +178,9 @@ def lib():
             "icx_mdg_jacobian_pattern": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                                     C.POINTER(C.c_longlong), vp, vp]),
             "icx_form_jacobian_mdg_fd": (C.c_int, [vp, vp, vp, vp, vp, C.c_double, vp]),
+            "icx_autotune": (C.c_int, [vp, vp, C.c_int, C.POINTER(TuneReport)]),
+            "icx_tile_get": (C.c_int, [vp, C.POINTER(TileChoice)]),
+            "icx_tile_set": (C.c_int, [vp, C.POINTER(TileChoice)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -316,6 +338,37 @@ class Context:
         self._check(lib().icx_ilu_apply(self._h, _ptr(vals), _ptr(x), _ptr(y), precision, schedule, repeat,
                                         C.byref(ms)), "ilu_apply")
         return ms.value
+
+    def autotune(self, u, parts=TUNE_RESIDUAL | TUNE_ILU | TUNE_ILU_FP32):
+        """times every compiled launch shape of the selected kernels at the
+        device state u, keeps the fastest whose output is bit-identical to the
+        default's, and returns the report as a dict"""
+        rep = TuneReport()
+        self._check(lib().icx_autotune(self._h, _ptr(u), parts, C.byref(rep)), "autotune")
+        return {"chosen": rep.chosen.as_dict(), "from_cache": rep.from_cache, "n_timed": rep.n_timed,
+                "n_rejected": rep.n_rejected, "residual_ms_default": rep.residual_ms_default,
+                "residual_ms_tuned": rep.residual_ms_tuned, "ilu_ms_default": list(rep.ilu_ms_default),
+                "ilu_ms_tuned": list(rep.ilu_ms_tuned)}
+
+    @property
+    def tile(self):
+        """the context's launch shapes (dict of TileChoice fields)"""
+        t = TileChoice()
+        self._check(lib().icx_tile_get(self._h, C.byref(t)), "tile_get")
+        return t.as_dict()
+
+    @tile.setter
+    def tile(self, d):
+        t = TileChoice()
+        d = dict(d)
+        t.face_minb = d.get("face_minb", 0)
+        t.vol_threads = d.get("vol_threads", 0)
+        t.vol_minb = d.get("vol_minb", 0)
+        for k, v in enumerate(d.get("ilu_rows", [0, 0])):
+            t.ilu_rows[k] = v
+        for k, v in enumerate(d.get("ilu_ctas", [0, 0])):
+            t.ilu_ctas[k] = v
+        self._check(lib().icx_tile_set(self._h, C.byref(t)), "tile_set")
 
     def form_residuals_host(self, u, res):
         """residuals of the states u[k] (host arrays or CPU tensors, [n_states][n_dof],

@@ -316,20 +316,23 @@ __device__ inline void flow_signal(unsigned* c) {
   if ((threadIdx.x & 31) == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(c) : "memory");
 }
 
-// rows per task of the data-flow apply: three blocks' rows stay in registers
-template <int BS>
+// rows per task of the data-flow apply: three blocks' rows stay in registers.
+// RT = 0 takes the block size's default; the others are tile choices (every
+// row's sum is formed the same way whatever the rows per task)
+template <int BS, int RT = 0>
 struct FlowCfg {
   static constexpr int NS = (BS + 31) / 32;
-  // rows per task, measured (ms per apply): 64 x 64 blocks 1.15 with 6 rows
-  // against 1.31 with 8 and 1.36 with 12; 36 x 36 blocks 2.40 with 4 against
-  // 2.48 with 6 and 3.71 with 2
-  static constexpr int R = NS >= 3 ? 4 : (BS >= 64 ? 6 : (BS >= 32 ? 4 : 2));
+  // default rows per task, measured (ms per apply): 64 x 64 blocks 1.15 with
+  // 6 rows against 1.31 with 8 and 1.36 with 12; 36 x 36 blocks 2.40 with 4
+  // against 2.48 with 6 and 3.71 with 2
+  static constexpr int R_DEFAULT = NS >= 3 ? 4 : (BS >= 64 ? 6 : (BS >= 32 ? 4 : 2));
+  static constexpr int R = RT ? RT : R_DEFAULT;
   static constexpr int GROUPS = (BS + R - 1) / R;
 };
 
-template <int BS, class TA>
+template <int BS, int RT, class TA>
 __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) {
-  using K = FlowCfg<BS>;
+  using K = FlowCfg<BS, RT>;
   constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
   const int lane = threadIdx.x & 31;
   const long long nw = (long long)gridDim.x * (blockDim.x >> 5);

@@ -37,8 +37,40 @@ struct PhysParams {
   double beta0, beta1;          // DDG coefficients (beta1 = 0 for interior penalty)
 };
 
+// launch shapes of the tunable kernels (0: the compiled default). Every
+// choice computes the same values in the same order: the tuner only moves
+// work between threads, warps and CTAs.
+struct TileChoice {
+  int face_minb = 0;     // face_flux_kernel: CTAs per SM its register bound is compiled for
+  int vol_threads = 0;   // vol_lift_kernel: threads per CTA (128 or 256; elements per CTA follow)
+  int vol_minb = 0;      // vol_lift_kernel: CTAs per SM of its register bound
+  int flow_rows[2] = {0, 0};  // data-flow ILU apply [FP64, FP32]: block rows per warp task
+  int flow_ctas[2] = {0, 0};  // data-flow ILU apply: CTAs per SM of the persistent grid
+};
+
+// compiled volume tiles: threads per CTA and the resident CTAs per SM of the
+// register bound (64 registers for the first and third, 80 for the others);
+// the first is the default
+struct VolTile {
+  int threads, minb;
+};
+constexpr int kNumVolTiles = 4;
+constexpr VolTile kVolTiles[kNumVolTiles] = {{256, 4}, {256, 3}, {128, 8}, {128, 6}};
+// compiled rows per task of the data-flow ILU apply (0 in a TileChoice: the
+// block size's default)
+constexpr int kNumFlowRows = 4;
+constexpr int kFlowRows[kNumFlowRows] = {2, 4, 6, 8};
+// face_flux_kernel's default resident CTAs per SM; the tiles compiled beside
+// it are one below and one above
+int face_minb_default(int pde, bool ddg);
+// the data-flow apply's default rows per task for a block size, and whether
+// `rows` (0: the default) is compiled for it
+int flow_rows_default(int bs);
+bool flow_rows_compiled(int bs, int rows);
+
 // device tables of one context (all device pointers)
 struct DeviceMesh {
+  TileChoice tile;
   int E = 0, F = 0, Fi = 0, Fb = 0, n_nodes = 0;
   int P = 0, G = 0, nb = 0, neq = 0, ng = 0, nq1 = 0, nqv = 0, nqf = 0;
   double* coord = nullptr;     // [n_nodes][2]
@@ -161,4 +193,9 @@ void free_host_pipe(icx_ctx* c);
 icx_status solver_prepare_pc(icx_ctx* c, const double* vals, int kind, int sweeps);
 cudaError_t solver_apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* z, cudaStream_t s);
 const float* solver_vals32(icx_ctx* c);
+// one block-ILU(0) apply on the data-flow schedule (factors from
+// solver_prepare_pc with kind 2), and the apply's error flag (read, then
+// cleared with the completion counters when set)
+cudaError_t solver_apply_ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStream_t s);
+icx_status solver_take_pc_err(icx_ctx* c, int* err);
 }  // namespace icx

@@ -387,6 +387,30 @@ cudaError_t la_ilu_factor(const DeviceMesh& dm, const int* order, const std::vec
   return cudaErrorInvalidValue;
 }
 
+// rows per task compiled for a block size: at most the block size, and the
+// three blocks' rows a task holds (R x column chunks each) at most 24 values
+// per lane, which keeps them in registers
+constexpr bool flow_rows_fit(int bs, int ns, int r) { return r <= (bs < 2 ? 2 : bs) && r * ns <= 24; }
+
+template <int B, int R, class TA>
+static const void* flow_kernel_if_fit() {
+  if constexpr (flow_rows_fit(B, (B + 31) / 32, R)) return (const void*)ilu_apply_flow_kernel<B, R, TA>;
+  else return nullptr;
+}
+
+// the data-flow kernel for `rows` rows per task (0: the default), or null
+template <int B, class TA>
+static const void* flow_kernel_for(int rows) {
+  static_assert(kFlowRows[0] == 2 && kFlowRows[1] == 4 && kFlowRows[2] == 6 && kFlowRows[3] == 8, "tiles");
+  switch (rows ? rows : FlowCfg<B>::R_DEFAULT) {
+    case 2: return flow_kernel_if_fit<B, 2, TA>();
+    case 4: return flow_kernel_if_fit<B, 4, TA>();
+    case 6: return flow_kernel_if_fit<B, 6, TA>();
+    case 8: return flow_kernel_if_fit<B, 8, TA>();
+    default: return nullptr;
+  }
+}
+
 template <class TA>
 static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, const int* order, const TA* LU,
                                    const TA* Uinv, const double* x, double* y, double* f, unsigned* cnt_f,
@@ -400,19 +424,41 @@ static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, const int* order, cons
   if (!coop) return cudaErrorNotSupported;
   IluFlowArgs<TA> args{dm.E, dm.nnzb, dm.bsr_rowptr, dm.bsr_colidx, dm.bsr_diag, order, LU, Uinv, x, f, y, cnt_f,
                        cnt_b, epoch, err};
-  void* params[] = {&args};
-#define ICX_ILUF2_CASE(B)                                                                             \
-  if (bs == B) {                                                                                      \
-    int per_sm = 0;                                                                                   \
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ilu_apply_flow_kernel<B, TA>, 256, 0); \
-    if (e != cudaSuccess) return e;                                                                   \
-    if (per_sm < 1) return cudaErrorNotSupported;                                                     \
-    int grid = nsm * (per_sm < 2 ? per_sm : 2);                                                       \
-    return cudaLaunchCooperativeKernel((const void*)ilu_apply_flow_kernel<B, TA>, dim3(grid), dim3(256), params, 0, s); \
-  }
+  const int pi = sizeof(TA) == 8 ? 0 : 1;
+  const int rows = dm.tile.flow_rows[pi], ctas = dm.tile.flow_ctas[pi];
+  if (ctas < 0) return cudaErrorInvalidValue;
+  const void* kern = nullptr;
+#define ICX_ILUF2_CASE(B)                                                                  \
+  if (bs == B) kern = flow_kernel_for<B, TA>(rows);
   ICX_BLOCK_SIZES(ICX_ILUF2_CASE)
 #undef ICX_ILUF2_CASE
-  return cudaErrorInvalidValue;
+  if (!kern) return cudaErrorInvalidValue;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorNotSupported;
+  // the whole grid is resident (the tasks wait on one another): at most the
+  // occupancy limit per SM; two by default
+  const int want = ctas ? ctas : 2;
+  const int grid = nsm * (per_sm < want ? per_sm : want);
+  void* params[] = {&args};
+  return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(256), params, 0, s);
+}
+
+int flow_rows_default(int bs) {
+#define ICX_FLOWR_CASE(B) \
+  if (bs == B) return FlowCfg<B>::R_DEFAULT;
+  ICX_BLOCK_SIZES(ICX_FLOWR_CASE)
+#undef ICX_FLOWR_CASE
+  return 0;
+}
+
+bool flow_rows_compiled(int bs, int rows) {
+  if (rows == 0) return true;
+  const int ns = (bs + 31) / 32;
+  for (int r : kFlowRows)
+    if (r == rows) return flow_rows_fit(bs, ns, r);
+  return false;
 }
 
 template <class TA>

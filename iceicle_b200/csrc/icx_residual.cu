@@ -24,10 +24,8 @@
 #include "icx_internal.h"
 #include "icx_dg.cuh"
 
-// resident CTAs per SM requested for the volume and face kernels (register budget)
-#ifndef ICX_VOL_MINB
-#define ICX_VOL_MINB 4
-#endif
+// resident CTAs per SM requested for the face kernel (register budget); the
+// volume kernel's tiles are kVolTiles
 #ifndef ICX_FACE_MINB
 #define ICX_FACE_MINB 5
 #endif
@@ -199,8 +197,10 @@ __device__ inline void cp_async_f64x2(double* sdst, const double* gsrc) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
 
-template <int PDE, int P, int G, bool DDG>
-__global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flux_kernel(DeviceMesh dm, PhysParams pp, const double* __restrict__ u) {
+// MO shifts the register bound's resident CTAs per SM from FaceCfg::MINB (a
+// tile choice: -1, 0 or +1); the arithmetic does not depend on it
+template <int PDE, int P, int G, bool DDG, int MO = 0>
+__global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB + MO)) face_flux_kernel(DeviceMesh dm, PhysParams pp, const double* __restrict__ u) {
   using C = Cfg<PDE, P, G>;
   using FC = FaceCfg<PDE, P, G, DDG>;
   constexpr int NEQ = C::NEQ, BS = C::BS, NQF = C::NQF, N1 = FC::N1, NM = FC::NM, FPB = FC::FPB;
@@ -390,11 +390,11 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB)) face_flu
 // indices: the lanes of a warp read consecutive words of the staged data and
 // a handful of table entries, and the staged layouts below keep those
 // accesses free of bank conflicts (the 1D tables use a padded row stride).
-template <int PDE, int P, int G>
+template <int PDE, int P, int G, int T = 256>
 struct VolCfg {
   using C = Cfg<PDE, P, G>;
   static constexpr int N1 = P + 1, Q1 = G + P, NEQ = C::NEQ;
-  static constexpr int THREADS = 256;
+  static constexpr int THREADS = T;                 // a tile choice: 128 or 256 (elements per CTA follow)
   static constexpr int EPB_RAW = THREADS / C::NQV;
   static constexpr int EPB = EPB_RAW < 1 ? 1 : EPB_RAW;
   static constexpr int TS = N1 + 1;                 // padded row stride of b, db
@@ -412,12 +412,12 @@ struct VolCfg {
   static constexpr size_t SMEM = sizeof(double) * (TAB1 + TABF + TABV + EPB * PER_EL) + sizeof(int) * EPB * 8;
 };
 
-template <int PDE, int P, int G>
-__global__ void __launch_bounds__(256, ICX_VOL_MINB) vol_lift_kernel(DeviceMesh dm, PhysParams pp,
-                                                                    const double* __restrict__ u,
-                                                                    double* __restrict__ res) {
+template <int PDE, int P, int G, int NT = kVolTiles[0].threads, int MB = kVolTiles[0].minb>
+__global__ void __launch_bounds__(NT, MB) vol_lift_kernel(DeviceMesh dm, PhysParams pp,
+                                                          const double* __restrict__ u,
+                                                          double* __restrict__ res) {
   using C = Cfg<PDE, P, G>;
-  using V = VolCfg<PDE, P, G>;
+  using V = VolCfg<PDE, P, G, NT>;
   constexpr int NEQ = C::NEQ, NB = C::NB, BS = C::BS, NQV = C::NQV, NQF = C::NQF, EPB = V::EPB;
   constexpr int N1 = V::N1, Q1 = V::Q1, TS = V::TS, US = V::US;
   extern __shared__ double smem[];
@@ -665,38 +665,74 @@ cudaError_t launch_geometry(const DeviceMesh& dm, cudaStream_t s) {
   return cudaErrorInvalidValue;
 }
 
-// raises a kernel's dynamic shared memory limit once per device
-template <class K>
-static cudaError_t smem_attr_once(K kernel, size_t bytes, std::atomic<unsigned>& done) {
+// raises the dynamic shared memory limit of kernel KERN once per device
+template <auto KERN>
+static cudaError_t smem_attr_once(size_t bytes) {
+  static std::atomic<unsigned> done{0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   unsigned bit = 1u << (dev & 31);
   if (done.load(std::memory_order_relaxed) & bit) return cudaSuccess;
-  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  e = cudaFuncSetAttribute(KERN, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e == cudaSuccess) done.fetch_or(bit);
   return e;
+}
+
+int face_minb_default(int pde, bool ddg) { return (ddg && pde == ICX_PDE_NAVIER_STOKES) ? 3 : ICX_FACE_MINB; }
+
+template <int PDE, int P, int G, bool DDG, int MO>
+static cudaError_t face_launch(const DeviceMesh& dm, const PhysParams& pp, const double* u, cudaStream_t s) {
+  using FC = FaceCfg<PDE, P, G, DDG>;
+  constexpr auto K = face_flux_kernel<PDE, P, G, DDG, MO>;
+  cudaError_t e = smem_attr_once<K>(FC::SMEM);
+  if (e != cudaSuccess) return e;
+  K<<<(dm.F + FC::FPB - 1) / FC::FPB, FC::THREADS, FC::SMEM, s>>>(dm, pp, u);
+  return cudaSuccess;
+}
+
+template <int PDE, int P, int G, bool DDG>
+static cudaError_t face_pick(const DeviceMesh& dm, const PhysParams& pp, const double* u, cudaStream_t s) {
+  constexpr int D = FaceCfg<PDE, P, G, DDG>::MINB;
+  static_assert(D - 1 >= 1, "face register bound");
+  const int mb = dm.tile.face_minb ? dm.tile.face_minb : D;
+  if (mb == D) return face_launch<PDE, P, G, DDG, 0>(dm, pp, u, s);
+  if (mb == D - 1) return face_launch<PDE, P, G, DDG, -1>(dm, pp, u, s);
+  if (mb == D + 1) return face_launch<PDE, P, G, DDG, 1>(dm, pp, u, s);
+  return cudaErrorInvalidValue;
+}
+
+template <int PDE, int P, int G, int T, int MB>
+static cudaError_t vol_launch(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
+                              cudaStream_t s) {
+  using V = VolCfg<PDE, P, G, T>;
+  constexpr auto K = vol_lift_kernel<PDE, P, G, T, MB>;
+  cudaError_t e = smem_attr_once<K>(V::SMEM);
+  if (e != cudaSuccess) return e;
+  K<<<(dm.E + V::EPB - 1) / V::EPB, T, V::SMEM, s>>>(dm, pp, u, res);
+  return cudaSuccess;
+}
+
+template <int PDE, int P, int G>
+static cudaError_t vol_pick(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
+                            cudaStream_t s) {
+  const int t = dm.tile.vol_threads ? dm.tile.vol_threads : kVolTiles[0].threads;
+  const int mb = dm.tile.vol_minb ? dm.tile.vol_minb : (t == kVolTiles[0].threads ? kVolTiles[0].minb : 0);
+#define ICX_VOL_TILE(I)                                                                      \
+  if (t == kVolTiles[I].threads && mb == kVolTiles[I].minb)                                  \
+    return vol_launch<PDE, P, G, kVolTiles[I].threads, kVolTiles[I].minb>(dm, pp, u, res, s);
+  ICX_VOL_TILE(0) ICX_VOL_TILE(1) ICX_VOL_TILE(2) ICX_VOL_TILE(3)
+#undef ICX_VOL_TILE
+  return cudaErrorInvalidValue;
 }
 
 template <int PDE, int P, int G>
 static cudaError_t residual_pg(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
                                cudaStream_t s, cudaEvent_t mid) {
-  using V = VolCfg<PDE, P, G>;
-  static std::atomic<unsigned> attr_face_ddg{0}, attr_face_ip{0}, attr_vol{0};
-  cudaError_t e;
-  if (pp.beta1 != 0.0) {
-    using FC = FaceCfg<PDE, P, G, true>;
-    if ((e = smem_attr_once(face_flux_kernel<PDE, P, G, true>, FC::SMEM, attr_face_ddg)) != cudaSuccess) return e;
-    face_flux_kernel<PDE, P, G, true><<<(dm.F + FC::FPB - 1) / FC::FPB, FC::THREADS, FC::SMEM, s>>>(dm, pp, u);
-  } else {
-    using FC = FaceCfg<PDE, P, G, false>;
-    if ((e = smem_attr_once(face_flux_kernel<PDE, P, G, false>, FC::SMEM, attr_face_ip)) != cudaSuccess) return e;
-    face_flux_kernel<PDE, P, G, false><<<(dm.F + FC::FPB - 1) / FC::FPB, FC::THREADS, FC::SMEM, s>>>(dm, pp, u);
-  }
+  cudaError_t e = pp.beta1 != 0.0 ? face_pick<PDE, P, G, true>(dm, pp, u, s) : face_pick<PDE, P, G, false>(dm, pp, u, s);
+  if (e != cudaSuccess) return e;
   if (mid) cudaEventRecord(mid, s);
-  if ((e = smem_attr_once(vol_lift_kernel<PDE, P, G>, V::SMEM, attr_vol)) != cudaSuccess) return e;
-  int nblk = (dm.E + V::EPB - 1) / V::EPB;
-  vol_lift_kernel<PDE, P, G><<<nblk, V::THREADS, V::SMEM, s>>>(dm, pp, u, res);
+  if ((e = vol_pick<PDE, P, G>(dm, pp, u, res, s)) != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
@@ -705,15 +741,11 @@ static cudaError_t residual_pg(const DeviceMesh& dm, const PhysParams& pp, const
 template <int PDE, int P, int G>
 static cudaError_t residual_domain_pg(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
                                       cudaStream_t s) {
-  using V = VolCfg<PDE, P, G>;
-  static std::atomic<unsigned> attr_vol{0};
   cudaError_t e = cudaMemsetAsync(dm.face_flux, 0, sizeof(double) * (size_t)dm.F * dm.nqf * dm.neq, s);
   if (e == cudaSuccess && dm.face_grad)
     e = cudaMemsetAsync(dm.face_grad, 0, sizeof(double) * (size_t)dm.F * 2 * dm.nqf * dm.neq * 2, s);
   if (e != cudaSuccess) return e;
-  if ((e = smem_attr_once(vol_lift_kernel<PDE, P, G>, V::SMEM, attr_vol)) != cudaSuccess) return e;
-  int nblk = (dm.E + V::EPB - 1) / V::EPB;
-  vol_lift_kernel<PDE, P, G><<<nblk, V::THREADS, V::SMEM, s>>>(dm, pp, u, res);
+  if ((e = vol_pick<PDE, P, G>(dm, pp, u, res, s)) != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

@@ -43,6 +43,9 @@ struct icx_solver_work {
   std::vector<int> lvl_off; // level l: order[lvl_off[l] .. lvl_off[l+1])
   unsigned* cnt = nullptr;  // 2 x E completion counters of the ILU apply
   unsigned epoch = 0;       // ILU applies since the counters were zeroed
+  // rows per task of those applies: an element's counter grows by its task
+  // count per apply (block size / rows), so the counters restart when it changes
+  int flow_rows = 0;
   // row-pipelined ILU apply: the context is one structured grid whose block
   // pattern is the 5-point element stencil in natural order
   bool rows_ok = false;
@@ -177,6 +180,28 @@ cudaError_t tri_rows(icx_ctx* c, bool mixed, bool lower, const double* v, const 
                : icx::la_tri_rows(c->dm, lower, w->pc, v, x0, -1.0, y, s);
 }
 
+// the data-flow block-ILU(0) apply with the context's launch shape. Each
+// apply adds an element's task count to its counters and waits for
+// epoch x task count, so a change of rows per task (FP64 and FP32 applies may
+// differ) first zeroes the counters, in stream order
+cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStream_t s) {
+  icx_solver_work* w = c->sw;
+  const icx::DeviceMesh& dm = c->dm;
+  const int pi = mixed ? 1 : 0;
+  const int rows = dm.tile.flow_rows[pi] ? dm.tile.flow_rows[pi] : icx::flow_rows_default(w->bs);
+  if (rows != w->flow_rows) {
+    cudaError_t e = cudaMemsetAsync(w->cnt, 0, sizeof(unsigned) * 2 * dm.E, s);
+    if (e != cudaSuccess) return e;
+    w->epoch = 0;
+    w->flow_rows = rows;
+  }
+  if (mixed)
+    return icx::la_ilu_apply_flow_f32(dm, w->order, w->pc32, w->uinv32, x, z, w->pct, w->cnt, w->cnt + dm.E,
+                                      ++w->epoch, w->pc_err, s);
+  return icx::la_ilu_apply_flow(dm, w->order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E, ++w->epoch,
+                                w->pc_err, s);
+}
+
 // z = M^-1 x (mixed: from the FP32 copies, FP32 accumulation)
 cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* z, cudaStream_t s) {
   icx_solver_work* w = c->sw;
@@ -230,11 +255,7 @@ cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* 
       if (e != cudaErrorNotSupported) return e;
       w->rows_ok = false;  // the rows cannot all be resident: data-flow apply from now on
     }
-    if (mixed)
-      return icx::la_ilu_apply_flow_f32(dm, w->order, w->pc32, w->uinv32, x, z, w->pct, w->cnt, w->cnt + dm.E,
-                                        ++w->epoch, w->pc_err, s);
-    return icx::la_ilu_apply_flow(dm, w->order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E, ++w->epoch,
-                                  w->pc_err, s);
+    return ilu_flow(c, mixed, x, z, s);
   }
   return cudaMemcpyAsync(z, x, sizeof(double) * w->n, cudaMemcpyDeviceToDevice, s);
 }
@@ -761,5 +782,25 @@ cudaError_t solver_apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, d
 }
 
 const float* solver_vals32(icx_ctx* c) { return c->sw ? c->sw->vals32 : nullptr; }
+
+cudaError_t solver_apply_ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStream_t s) {
+  return ilu_flow(c, mixed, x, z, s);
+}
+
+icx_status solver_take_pc_err(icx_ctx* c, int* err) {
+  icx_solver_work* w = c->sw;
+  cudaStream_t s = 0;
+  *err = 0;
+  CK(cudaMemcpyAsync(err, w->pc_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (*err) {
+    // the counters are inconsistent after an abandoned apply: start over
+    CK(cudaMemsetAsync(w->pc_err, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(w->cnt, 0, sizeof(unsigned) * 2 * c->dm.E, s));
+    w->epoch = 0;
+    CK(cudaStreamSynchronize(s));
+  }
+  return ICX_OK;
+}
 
 }  // namespace icx

@@ -444,6 +444,54 @@ void icx_wl_ns_mms_source(const double* x, double* out, void* user);
  * (for nodal initial states, as the reference's nodal interpolation) */
 icx_status icx_basis_node_coords(const icx_ctx* ctx, double* xy);
 
+/* ---- launch-shape autotuner (no counterpart in the reference, whose kernels
+ * are CPU loops). The tunable kernels are compiled in several launch shapes
+ * that compute the same values in the same order, so a choice changes speed,
+ * never results. 0 in any field selects the compiled default.
+ *   face_minb   face flux kernel: resident CTAs per SM of its register bound,
+ *               the default D or D - 1 / D + 1 (D = 5; 3 for Navier-Stokes
+ *               with the DDG flux)
+ *   vol_threads, vol_minb   volume + lifting kernel: (256, 4) default,
+ *               (256, 3), (128, 8), (128, 6) (elements per CTA = threads /
+ *               volume points)
+ *   ilu_rows[k], ilu_ctas[k]   data-flow block-ILU(0) apply, k = 0 FP64 and
+ *               1 FP32 factors: block rows per warp task (2, 4, 6, 8; at most
+ *               the block size and 24 register values per lane) and CTAs per
+ *               SM of the persistent grid (1 to 4; capped by occupancy) */
+typedef struct icx_tile_choice {
+  int face_minb;
+  int vol_threads, vol_minb;
+  int ilu_rows[2];
+  int ilu_ctas[2];
+} icx_tile_choice;
+
+typedef struct icx_tune_report {
+  icx_tile_choice chosen;      /* the context's choice after the call */
+  int from_cache;              /* bit set per part (ICX_TUNE_*) taken from the process-wide cache untimed */
+  int n_timed;                 /* candidates timed */
+  int n_rejected;              /* candidates whose output was not bit-identical to the default's (never chosen) */
+  double residual_ms_default;  /* face + volume kernels, device time per residual (L2 flushed before each) */
+  double residual_ms_tuned;
+  double ilu_ms_default[2];    /* one block-ILU(0) apply, [FP64, FP32] */
+  double ilu_ms_tuned[2];
+} icx_tune_report;
+
+#define ICX_TUNE_RESIDUAL 1 /* face and volume kernels, timed at d_u */
+#define ICX_TUNE_ILU 2      /* data-flow ILU apply with FP64 factors of the FD Jacobian at d_u */
+#define ICX_TUNE_ILU_FP32 4 /* the same with FP32 factors */
+#define ICX_TUNE_RETIME 8   /* time even when the cache holds a choice for the key */
+
+/* Times every compiled shape of the selected kernels on this context's mesh
+ * at the state d_u (device, not modified), checks each output against the
+ * default shape's bit for bit, and keeps the fastest in the context. Choices
+ * are cached per process under the key (dimension, basis order p, equations
+ * neq, geometry order, viscous flux) and reused untimed by later contexts with
+ * the same key unless ICX_TUNE_RETIME is set. rep may be NULL. */
+icx_status icx_autotune(icx_ctx* ctx, const double* d_u, int parts, icx_tune_report* rep);
+icx_status icx_tile_get(const icx_ctx* ctx, icx_tile_choice* tile);
+/* ICX_ERR_INVALID for a shape that is not compiled for this context */
+icx_status icx_tile_set(icx_ctx* ctx, const icx_tile_choice* tile);
+
 #ifdef __cplusplus
 }
 #endif
