@@ -56,6 +56,9 @@ def parse():
                          "time (0: skip; the full problem set is 512)")
     ap.add_argument("--no-tune", action="store_true",
                     help="time the compiled default launch shapes instead of the autotuned ones")
+    ap.add_argument("--tile", default="", metavar="K=V,...",
+                    help="time the residual with these launch shapes instead of autotuning them, e.g. "
+                         "face_minb=4,vol_threads=128,vol_minb=8 (for profiling the shapes a plain run chose)")
     return ap.parse_args()
 
 
@@ -186,10 +189,15 @@ def residual_work(wl):
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the two
-# residual kernels on this workload, from one ncu capture of
-#   ncu --set full --clock-control none -k regex:"face_flux|vol_lift" -s 10 -c 2 \
-#       python bench.py --steps 2 --warmup 3 --no-newton --no-cpu-baseline
-NCU_DRAM_BYTES = {"vol": 43.45e6 + 0.06e6, "face": 25.59e6 + 0.003e6}
+# residual kernels on this workload in the tuned shapes (the default shapes
+# read the same: 43.45 MB and 25.59 MB), from one ncu capture of
+#   ncu --section SpeedOfLight --section MemoryWorkloadAnalysis --section Occupancy \
+#       --section WarpStateStats --section LaunchStats \
+#       --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none \
+#       -k "regex:vol_lift|face_flux" -s 4 -c 2 python bench.py --steps 2 --warmup 3 \
+#       --no-newton --no-cpu-baseline --batched 0 --no-learned \
+#       --tile face_minb=4,vol_threads=128,vol_minb=8
+NCU_DRAM_BYTES = {"vol": 43.45e6 + 0.57e6, "face": 25.42e6 + 0.0003e6}
 
 
 def batched_bench(torch, dev, n_problems):
@@ -400,7 +408,11 @@ def run_ours(a):
     # launch shapes of the face and volume kernels for this (p, neq), chosen
     # once before any timing (every shape computes identical values)
     import iceicle_b200 as ib
-    tune = None if a.no_tune else wl.ctx.autotune(u, ib.TUNE_RESIDUAL)
+    tune = None
+    if a.tile:
+        wl.ctx.tile = {k: int(v) for k, v in (kv.split("=") for kv in a.tile.split(","))}
+    elif not a.no_tune:
+        tune = wl.ctx.autotune(u, ib.TUNE_RESIDUAL)
     for _ in range(max(a.warmup, 3)):
         wl.ctx.form_residual(u, res, stream)
     torch.cuda.synchronize(dev)
@@ -467,6 +479,9 @@ def run_ours(a):
             pass
         hbm = peaks.get("hbm_gbs", 6650.0)
         dom = "vol" if tv >= tf else "face"
+        shape = wl.ctx.tile  # 0: the compiled default (face bound 5; volume 256 threads, bound 4)
+        shape = {"face_minb": shape["face_minb"] or 5, "vol_threads": shape["vol_threads"] or 256,
+                 "vol_minb": shape["vol_minb"] or 4}
         td = tv if dom == "vol" else tf
         bytes_d, flops_d = work[dom]
         achieved = bytes_d / td / 1e9
@@ -480,7 +495,9 @@ def run_ours(a):
                     "one_step_at_a_time": e2e_seq},
             "gpu_launches": 2 * a.steps,
             "roofline": {"bound": "hbm",
-                         "kernel": "vol_lift_kernel<NS,p3,g2>" if dom == "vol" else "face_flux_kernel<NS,p3,g2,IP>",
+                         "kernel": (f"vol_lift_kernel<NS,p3,g2> ({shape['vol_threads']} threads, "
+                                    f"{shape['vol_minb']} CTAs/SM bound)") if dom == "vol" else
+                                   f"face_flux_kernel<NS,p3,g2,IP> ({shape['face_minb']} CTAs/SM bound)",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
                          else "fallback 6650 GB/s",
@@ -493,7 +510,8 @@ def run_ours(a):
                                           "achieved_gbs": work["face" if dom == "vol" else "vol"][0] /
                                           (tf if dom == "vol" else tv) / 1e9}},
             "clocks": clocks,
-            "autotune": None if tune is None else {
+            "autotune": {"fixed": {k: wl.ctx.tile[k] for k in ("face_minb", "vol_threads", "vol_minb")}}
+            if tune is None else {
                 "chosen": {k: tune["chosen"][k] for k in ("face_minb", "vol_threads", "vol_minb")},
                 "residual_ms_default": tune["residual_ms_default"], "residual_ms_tuned": tune["residual_ms_tuned"],
                 "shapes_timed": tune["n_timed"], "rejected": tune["n_rejected"]},
