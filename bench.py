@@ -341,10 +341,16 @@ def ilu_bench(n):
         for prec, pn in ((0, "fp64"), (1, "fp32")):
             ctx.ilu_apply(vals, x, y, prec, sched, 3)
             out[f"{name}_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, sched, 20)
-    # the data-flow apply again with the autotuned rows per task and CTAs per SM
+    # the data-flow apply on the sentinel schedule (default rows and CTAs), then
+    # with the autotuned schedule, rows per task and CTAs per SM
+    ctx.tile = {"ilu_sched": [2, 2]}
+    for prec, pn in ((0, "fp64"), (1, "fp32")):
+        ctx.ilu_apply(vals, x, y, prec, 1, 3)
+        out[f"data_flow_sentinel_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 1, 20)
+    ctx.tile = {}
     import iceicle_b200 as ib
     t = ctx.autotune(u, ib.TUNE_ILU | ib.TUNE_ILU_FP32)
-    out["tuned_tile"] = {"ilu_rows": t["chosen"]["ilu_rows"], "ilu_ctas": t["chosen"]["ilu_ctas"]}
+    out["tuned_tile"] = {k: t["chosen"][k] for k in ("ilu_rows", "ilu_ctas", "ilu_sched")}
     for prec, pn in ((0, "fp64"), (1, "fp32")):
         ctx.ilu_apply(vals, x, y, prec, 1, 3)
         out[f"data_flow_tuned_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 1, 20)

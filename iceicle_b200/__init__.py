@@ -87,11 +87,12 @@ class LpcTrainReport(C.Structure):
 class TileChoice(C.Structure):
     """launch shapes of the tunable kernels (0: the compiled default)"""
     _fields_ = [("face_minb", C.c_int), ("vol_threads", C.c_int), ("vol_minb", C.c_int),
-                ("ilu_rows", C.c_int * 2), ("ilu_ctas", C.c_int * 2)]
+                ("ilu_rows", C.c_int * 2), ("ilu_ctas", C.c_int * 2), ("ilu_sched", C.c_int * 2)]
 
     def as_dict(self):
         return {"face_minb": self.face_minb, "vol_threads": self.vol_threads, "vol_minb": self.vol_minb,
-                "ilu_rows": list(self.ilu_rows), "ilu_ctas": list(self.ilu_ctas)}
+                "ilu_rows": list(self.ilu_rows), "ilu_ctas": list(self.ilu_ctas),
+                "ilu_sched": list(self.ilu_sched)}
 
 
 class TuneReport(C.Structure):
@@ -368,6 +369,8 @@ class Context:
             t.ilu_rows[k] = v
         for k, v in enumerate(d.get("ilu_ctas", [0, 0])):
             t.ilu_ctas[k] = v
+        for k, v in enumerate(d.get("ilu_sched", [0, 0])):
+            t.ilu_sched[k] = v
         self._check(lib().icx_tile_set(self._h, C.byref(t)), "tile_set")
 
     def form_residuals_host(self, u, res):

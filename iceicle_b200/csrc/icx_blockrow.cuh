@@ -238,10 +238,15 @@ inline cudaError_t launch_block_rows(const RowSet& rs, const int* rowptr, const 
 // on a lower level) and dealt to the
 // warps round-robin; every warp runs its tasks in that order, all forward
 // tasks before any backward task. A task loads its matrix rows, then waits
-// only for the elements it reads: each element has a completion counter per
-// sweep that every group increments after writing its rows, and the sweep of
-// apply number `epoch` is complete for element k when its counter reaches
-// epoch * GROUPS (the counters grow across applies and are never reset).
+// only for the elements it reads, on one of two schedules:
+//   sentinel (the default): the outputs are pre-filled with a sentinel value
+//     and the waiting warp polls the values it reads until none holds it
+//     (below, FLOW_SENTINEL);
+//   counters: each element has a completion counter per sweep that every
+//     group increments after writing its rows, and the sweep of apply number
+//     `epoch` is complete for element k when its counter reaches
+//     epoch * GROUPS (the counters grow across applies; the solver zeroes
+//     them when GROUPS changes).
 // Because every dependency is a task earlier in some warp's order and all
 // warps are resident (cooperative launch), the waits always end; each is
 // nevertheless bounded by ICX_FLOW_SPINS polls, after which the warp sets
@@ -316,6 +321,81 @@ __device__ inline void flow_signal(unsigned* c) {
   if ((threadIdx.x & 31) == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(c) : "memory");
 }
 
+// Sentinel schedule of the same apply: instead of counting completed tasks,
+// every output slot (f and y) is filled with FLOW_SENTINEL before the launch,
+// each task stores its rows with relaxed stores (no fence, no counter), and a
+// waiting warp loads the values it reads with relaxed loads until none holds
+// the sentinel. Each 8-byte value is observed whole, so no ordering between a
+// task's stores is needed: a level costs one store and one polled load
+// instead of a fence, a counter update, a counter poll and a load. The
+// sentinel is a NaN whose payload FP64 arithmetic never returns (results that
+// are NaN carry the canonical payload), and the outputs are always results
+// of arithmetic.
+constexpr unsigned long long FLOW_SENTINEL = 0x7FF4B7E5C0DE0001ull;
+
+__device__ inline double ld_relaxed_f64(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ inline void st_relaxed_f64(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+
+// vectors b < 3 with use[b] (BS values at p[b]) into xv, lane l holding
+// columns l, l + 32, ...: relaxed loads of the slots still holding the
+// sentinel, repeated until the whole warp has every value. Bounded like
+// flow_wait_n (ICX_FLOW_SPINS rounds, then *err = 1; a set *err ends it).
+template <int BS, int NS, class TA>
+__device__ inline bool flow_gather_ready(const double* p0, const double* p1, const double* p2, bool u0, bool u1,
+                                         bool u2, TA (&xv)[3][NS], int* err) {
+  const int lane = threadIdx.x & 31;
+  const double* p[3] = {p0, p1, p2};
+  const bool use[3] = {u0, u1, u2};
+  unsigned pending = 0;
+#pragma unroll
+  for (int b = 0; b < 3; ++b)
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      xv[b][s] = TA(0);
+      if (use[b] && lane + 32 * s < BS) pending |= 1u << (b * NS + s);
+    }
+  unsigned spins = 0;
+  while (true) {
+    double v[3][NS];
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int s = 0; s < NS; ++s)
+        if (pending & (1u << (b * NS + s))) v[b][s] = ld_relaxed_f64(p[b] + lane + 32 * s);
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const unsigned bit = 1u << (b * NS + s);
+        if ((pending & bit) && (unsigned long long)__double_as_longlong(v[b][s]) != FLOW_SENTINEL) {
+          xv[b][s] = (TA)v[b][s];
+          pending &= ~bit;
+        }
+      }
+    if (__all_sync(0xffffffffu, pending == 0)) return true;
+    int stop = 0;
+    if (lane == 0) {
+      if (*reinterpret_cast<volatile int*>(err)) stop = 1;
+      else if (++spins > ICX_FLOW_SPINS) {
+        atomicExch(err, 1);
+        stop = 1;
+      }
+    }
+    if (__shfl_sync(0xffffffffu, stop, 0)) return false;
+  }
+}
+
+// an output value of the sentinel schedule (never the sentinel itself)
+__device__ inline double flow_value(double v) {
+  return (unsigned long long)__double_as_longlong(v) == FLOW_SENTINEL ? __longlong_as_double(0x7FFFFFFFFFFFFFFFll) : v;
+}
+
 // rows per task of the data-flow apply: three blocks' rows stay in registers.
 // RT = 0 takes the block size's default; the others are tile choices (every
 // row's sum is formed the same way whatever the rows per task)
@@ -330,7 +410,9 @@ struct FlowCfg {
   static constexpr int GROUPS = (BS + R - 1) / R;
 };
 
-template <int BS, int RT, class TA>
+// SEN: the sentinel schedule (outputs pre-filled with FLOW_SENTINEL; the
+// counters, epoch and flow_signal are not used), else completion counters
+template <int BS, int RT, class TA, bool SEN>
 __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) {
   using K = FlowCfg<BS, RT>;
   constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
@@ -389,23 +471,32 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
       for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
       const double* vsrc = fwd ? a.f : a.y;
       unsigned* cnt = fwd ? a.cnt_f : a.cnt_b;
-      // every dependency first (backward: also the element's own forward
-      // result), then all the vectors in one round of loads, so that the
-      // second neighbour's load does not add another L2 round trip
-      {
-        // counters: the nbk neighbours, then (backward) the element's own forward one
-        const unsigned* w0 = nbk > 0 ? cnt + ks[0] : a.cnt_f + e;
-        const unsigned* w1 = nbk > 1 ? cnt + ks[1] : a.cnt_f + e;
-        const int nw = nbk + (fwd ? 0 : 1);
-        if (nw > 0 && !flow_wait_n(w0, w1, a.cnt_f + e, nw, target, a.err)) return;
-      }
       TA xv[3][NS];
+      if constexpr (SEN) {
+        // the neighbours' rows (backward: and the element's own forward
+        // result) as soon as none of them holds the sentinel
+        if (!flow_gather_ready<BS, NS, TA>(vsrc + (size_t)(nbk > 0 ? ks[0] : 0) * BS,
+                                           vsrc + (size_t)(nbk > 1 ? ks[1] : 0) * BS, a.f + (size_t)e * BS,
+                                           nbk > 0, nbk > 1, !fwd, xv, a.err))
+          return;
+      } else {
+        // every dependency first (backward: also the element's own forward
+        // result), then all the vectors in one round of loads, so that the
+        // second neighbour's load does not add another L2 round trip
+        {
+          // counters: the nbk neighbours, then (backward) the element's own forward one
+          const unsigned* w0 = nbk > 0 ? cnt + ks[0] : a.cnt_f + e;
+          const unsigned* w1 = nbk > 1 ? cnt + ks[1] : a.cnt_f + e;
+          const int nw = nbk + (fwd ? 0 : 1);
+          if (nw > 0 && !flow_wait_n(w0, w1, a.cnt_f + e, nw, target, a.err)) return;
+        }
 #pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        const int c = lane + 32 * s;
+        for (int s = 0; s < NS; ++s) {
+          const int c = lane + 32 * s;
 #pragma unroll
-        for (int b = 0; b < 2; ++b) xv[b][s] = (b < nbk && c < BS) ? (TA)__ldcg(vsrc + (size_t)ks[b] * BS + c) : TA(0);
-        xv[2][s] = (!fwd && c < BS) ? (TA)__ldcg(a.f + (size_t)e * BS + c) : TA(0);
+          for (int b = 0; b < 2; ++b) xv[b][s] = (b < nbk && c < BS) ? (TA)__ldcg(vsrc + (size_t)ks[b] * BS + c) : TA(0);
+          xv[2][s] = (!fwd && c < BS) ? (TA)__ldcg(a.f + (size_t)e * BS + c) : TA(0);
+        }
       }
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
@@ -433,11 +524,18 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
       for (int rr = 0; rr < R; ++rr)
         if (lane == rr) mine = acc[rr];
       const int r = r0 + lane;
-      if (lane < R && r < BS) {
-        if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
-        else a.y[(size_t)e * BS + r] = (double)mine;
+      if constexpr (SEN) {
+        if (lane < R && r < BS) {
+          if (fwd) st_relaxed_f64(a.f + (size_t)e * BS + r, flow_value(a.x[(size_t)e * BS + r] + (double)mine));
+          else st_relaxed_f64(a.y + (size_t)e * BS + r, flow_value((double)mine));
+        }
+      } else {
+        if (lane < R && r < BS) {
+          if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
+          else a.y[(size_t)e * BS + r] = (double)mine;
+        }
+        flow_signal(cnt + e);
       }
-      flow_signal(cnt + e);
     }
   }
 }

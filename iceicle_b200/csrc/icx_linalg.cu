@@ -393,21 +393,31 @@ cudaError_t la_ilu_factor(const DeviceMesh& dm, const int* order, const std::vec
 constexpr bool flow_rows_fit(int bs, int ns, int r) { return r <= (bs < 2 ? 2 : bs) && r * ns <= 24; }
 
 template <int B, int R, class TA>
-static const void* flow_kernel_if_fit() {
-  if constexpr (flow_rows_fit(B, (B + 31) / 32, R)) return (const void*)ilu_apply_flow_kernel<B, R, TA>;
+static const void* flow_kernel_if_fit(bool sen) {
+  if constexpr (flow_rows_fit(B, (B + 31) / 32, R))
+    return sen ? (const void*)ilu_apply_flow_kernel<B, R, TA, true> : (const void*)ilu_apply_flow_kernel<B, R, TA, false>;
   else return nullptr;
 }
 
-// the data-flow kernel for `rows` rows per task (0: the default), or null
+// the data-flow kernel for `rows` rows per task (0: the default) on the
+// counter or the sentinel schedule, or null
 template <int B, class TA>
-static const void* flow_kernel_for(int rows) {
+static const void* flow_kernel_for(int rows, bool sen) {
   static_assert(kFlowRows[0] == 2 && kFlowRows[1] == 4 && kFlowRows[2] == 6 && kFlowRows[3] == 8, "tiles");
   switch (rows ? rows : FlowCfg<B>::R_DEFAULT) {
-    case 2: return flow_kernel_if_fit<B, 2, TA>();
-    case 4: return flow_kernel_if_fit<B, 4, TA>();
-    case 6: return flow_kernel_if_fit<B, 6, TA>();
-    case 8: return flow_kernel_if_fit<B, 8, TA>();
+    case 2: return flow_kernel_if_fit<B, 2, TA>(sen);
+    case 4: return flow_kernel_if_fit<B, 4, TA>(sen);
+    case 6: return flow_kernel_if_fit<B, 6, TA>(sen);
+    case 8: return flow_kernel_if_fit<B, 8, TA>(sen);
     default: return nullptr;
+  }
+}
+
+__global__ void flow_fill_kernel(long long n, double* __restrict__ f, double* __restrict__ y) {
+  const double v = __longlong_as_double((long long)FLOW_SENTINEL);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    f[i] = v;
+    y[i] = v;
   }
 }
 
@@ -427,9 +437,10 @@ static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, const int* order, cons
   const int pi = sizeof(TA) == 8 ? 0 : 1;
   const int rows = dm.tile.flow_rows[pi], ctas = dm.tile.flow_ctas[pi];
   if (ctas < 0) return cudaErrorInvalidValue;
+  const bool sen = flow_sentinel(dm.tile, pi);
   const void* kern = nullptr;
 #define ICX_ILUF2_CASE(B)                                                                  \
-  if (bs == B) kern = flow_kernel_for<B, TA>(rows);
+  if (bs == B) kern = flow_kernel_for<B, TA>(rows, sen);
   ICX_BLOCK_SIZES(ICX_ILUF2_CASE)
 #undef ICX_ILUF2_CASE
   if (!kern) return cudaErrorInvalidValue;
@@ -441,6 +452,11 @@ static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, const int* order, cons
   // occupancy limit per SM; two by default
   const int want = ctas ? ctas : 2;
   const int grid = nsm * (per_sm < want ? per_sm : want);
+  if (sen) {
+    const long long n = (long long)dm.E * bs;
+    flow_fill_kernel<<<grid_for(n), 256, 0, s>>>(n, f, y);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   void* params[] = {&args};
   return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(256), params, 0, s);
 }

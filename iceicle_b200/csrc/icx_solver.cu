@@ -189,16 +189,19 @@ cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStr
   const icx::DeviceMesh& dm = c->dm;
   const int pi = mixed ? 1 : 0;
   const int rows = dm.tile.flow_rows[pi] ? dm.tile.flow_rows[pi] : icx::flow_rows_default(w->bs);
-  if (rows != w->flow_rows) {
+  // the sentinel schedule uses neither the counters nor the epoch
+  const bool sen = icx::flow_sentinel(dm.tile, pi);
+  if (!sen && rows != w->flow_rows) {
     cudaError_t e = cudaMemsetAsync(w->cnt, 0, sizeof(unsigned) * 2 * dm.E, s);
     if (e != cudaSuccess) return e;
     w->epoch = 0;
     w->flow_rows = rows;
   }
+  const unsigned epoch = sen ? w->epoch : ++w->epoch;
   if (mixed)
     return icx::la_ilu_apply_flow_f32(dm, w->order, w->pc32, w->uinv32, x, z, w->pct, w->cnt, w->cnt + dm.E,
-                                      ++w->epoch, w->pc_err, s);
-  return icx::la_ilu_apply_flow(dm, w->order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E, ++w->epoch,
+                                      epoch, w->pc_err, s);
+  return icx::la_ilu_apply_flow(dm, w->order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E, epoch,
                                 w->pc_err, s);
 }
 

@@ -3,7 +3,8 @@
 // changing any value or summation order:
 //   face_flux_kernel      the register bound's resident CTAs per SM
 //   vol_lift_kernel       threads per CTA (and so elements per CTA) and its register bound
-//   ilu_apply_flow_kernel block rows per warp task and CTAs per SM (FP64 and FP32 factors)
+//   ilu_apply_flow_kernel block rows per warp task, CTAs per SM and the schedule
+//                         (completion counters or sentinel values; FP64 and FP32 factors)
 // icx_autotune times each shape on the context's own mesh and state with CUDA
 // events, flushing L2 before every timed launch as the benchmarks do, checks
 // that its output equals the default shape's bit for bit (a shape that
@@ -181,7 +182,7 @@ struct Tuner {
   }
 
   // FD Jacobian at u, block-ILU(0) factors (FP64 and FP32), then every
-  // (rows per task, CTAs per SM) of the requested precisions
+  // (schedule, rows per task, CTAs per SM) of the requested precisions
   icx_status ilu(const double* u, bool fp64, bool fp32, double* ms_def, double* ms_tuned) {
     icx::DeviceMesh& dm = c->dm;
     const int bs = dm.nb * dm.neq;
@@ -211,21 +212,23 @@ struct Tuner {
                                                           : "ILU apply: bad block index");
         return ICX_OK;
       };
-      dm.tile.flow_rows[pi] = dm.tile.flow_ctas[pi] = 0;
+      dm.tile.flow_rows[pi] = dm.tile.flow_ctas[pi] = dm.tile.flow_sched[pi] = 0;
       TCK(apply(z0));
       TCK(cudaStreamSynchronize(s));
       if ((st = check_err()) != ICX_OK) { dm.tile = keep; return st; }
       if ((st = time([&] { return apply(z1); }, &ms_def[pi])) != ICX_OK ||
           (st = check_err()) != ICX_OK) { dm.tile = keep; return st; }
-      const int R0 = icx::flow_rows_default(bs);
+      const int R0 = icx::flow_rows_default(bs), S0 = icx::kFlowSchedDefault;
       double best = ms_def[pi];
-      int best_r = R0, best_c = 2;
+      int best_r = R0, best_c = 2, best_s = S0;
+      for (int sc = 1; sc <= 2; ++sc)
       for (int r : icx::kFlowRows) {
         if (!icx::flow_rows_compiled(bs, r)) continue;
         for (int k = 1; k <= MAX_CTAS; ++k) {
-          if (r == R0 && k == 2) continue;  // the default, timed above
+          if (r == R0 && k == 2 && sc == S0) continue;  // the default, timed above
           dm.tile.flow_rows[pi] = r;
           dm.tile.flow_ctas[pi] = k;
+          dm.tile.flow_sched[pi] = sc;
           double ms = 0;
           unsigned long long nd = 0;
           cudaError_t e = apply(z1);
@@ -237,11 +240,12 @@ struct Tuner {
             dm.tile = keep;
             return st;
           }
-          if (ms < MARGIN * best) { best = ms; best_r = r; best_c = k; }
+          if (ms < MARGIN * best) { best = ms; best_r = r; best_c = k; best_s = sc; }
         }
       }
       dm.tile.flow_rows[pi] = best_r;
       dm.tile.flow_ctas[pi] = best_c;
+      dm.tile.flow_sched[pi] = best_s;
       ms_tuned[pi] = best;
     }
     return ICX_OK;
@@ -255,6 +259,7 @@ void to_public(const TileChoice& t, icx_tile_choice* o) {
   for (int k = 0; k < 2; ++k) {
     o->ilu_rows[k] = t.flow_rows[k];
     o->ilu_ctas[k] = t.flow_ctas[k];
+    o->ilu_sched[k] = t.flow_sched[k];
   }
 }
 
@@ -286,6 +291,7 @@ icx_status icx_tile_set(icx_ctx* c, const icx_tile_choice* t) {
     if (!icx::flow_rows_compiled(bs, t->ilu_rows[k]))
       return fail(c, ICX_ERR_INVALID, "ilu_rows: not compiled for this block size");
     if (t->ilu_ctas[k] < 0 || t->ilu_ctas[k] > MAX_CTAS) return fail(c, ICX_ERR_INVALID, "ilu_ctas: 0..4");
+    if (t->ilu_sched[k] < 0 || t->ilu_sched[k] > 2) return fail(c, ICX_ERR_INVALID, "ilu_sched: 0..2");
   }
   TileChoice& d = c->dm.tile;
   d.face_minb = t->face_minb;
@@ -294,6 +300,7 @@ icx_status icx_tile_set(icx_ctx* c, const icx_tile_choice* t) {
   for (int k = 0; k < 2; ++k) {
     d.flow_rows[k] = t->ilu_rows[k];
     d.flow_ctas[k] = t->ilu_ctas[k];
+    d.flow_sched[k] = t->ilu_sched[k];
   }
   return ICX_OK;
 }
@@ -329,6 +336,7 @@ icx_status icx_autotune(icx_ctx* c, const double* d_u, int parts, icx_tune_repor
       if (hit & (pi == 0 ? ICX_TUNE_ILU : ICX_TUNE_ILU_FP32)) {
         t.flow_rows[pi] = cached.tile.flow_rows[pi];
         t.flow_ctas[pi] = cached.tile.flow_ctas[pi];
+        t.flow_sched[pi] = cached.tile.flow_sched[pi];
       }
     R->from_cache = hit;
     todo &= ~hit;
@@ -355,6 +363,7 @@ icx_status icx_autotune(icx_ctx* c, const double* d_u, int parts, icx_tune_repor
       if (todo & (pi == 0 ? ICX_TUNE_ILU : ICX_TUNE_ILU_FP32)) {
         ce.tile.flow_rows[pi] = t.flow_rows[pi];
         ce.tile.flow_ctas[pi] = t.flow_ctas[pi];
+        ce.tile.flow_sched[pi] = t.flow_sched[pi];
       }
     ce.parts |= todo;
   }

@@ -456,13 +456,16 @@ icx_status icx_basis_node_coords(const icx_ctx* ctx, double* xy);
  *               volume points)
  *   ilu_rows[k], ilu_ctas[k]   data-flow block-ILU(0) apply, k = 0 FP64 and
  *               1 FP32 factors: block rows per warp task (2, 4, 6, 8; at most
- *               the block size and 24 register values per lane) and CTAs per
- *               SM of the persistent grid (1 to 4; capped by occupancy) */
+ *               the block size and 24 register values per lane), CTAs per
+ *               SM of the persistent grid (1 to 4; capped by occupancy) and the
+ *               schedule: 1 completion counters per element, 2 outputs
+ *               pre-filled with a sentinel and polled directly (the default) */
 typedef struct icx_tile_choice {
   int face_minb;
   int vol_threads, vol_minb;
   int ilu_rows[2];
   int ilu_ctas[2];
+  int ilu_sched[2];
 } icx_tile_choice;
 
 typedef struct icx_tune_report {

@@ -66,16 +66,18 @@ def test_ilu_shapes_bit_identical(kw):
         ctx.tile = {}
         y0 = torch.empty_like(x)
         ctx.ilu_apply(vals, x, y0, precision, 0)
-        for r in rows:
-            for k in (1, 2, 3, 4):
-                t = {"ilu_rows": [0, 0], "ilu_ctas": [0, 0]}
-                t["ilu_rows"][precision] = r
-                t["ilu_ctas"][precision] = k
-                ctx.tile = t
-                y = torch.empty_like(x)
-                ctx.ilu_apply(vals, x, y, precision, 0, repeat=2)
-                torch.cuda.synchronize()
-                assert torch.equal(y.view(torch.int64), y0.view(torch.int64)), (precision, r, k)
+        for sched in (1, 2):  # completion counters, sentinel values
+            for r in rows:
+                for k in (1, 2, 3, 4):
+                    t = {"ilu_rows": [0, 0], "ilu_ctas": [0, 0], "ilu_sched": [0, 0]}
+                    t["ilu_rows"][precision] = r
+                    t["ilu_ctas"][precision] = k
+                    t["ilu_sched"][precision] = sched
+                    ctx.tile = t
+                    y = torch.empty_like(x)
+                    ctx.ilu_apply(vals, x, y, precision, 0, repeat=2)
+                    torch.cuda.synchronize()
+                    assert torch.equal(y.view(torch.int64), y0.view(torch.int64)), (precision, sched, r, k)
 
 
 def test_autotune_parity_and_cache():
@@ -85,8 +87,8 @@ def test_autotune_parity_and_cache():
     rep = ctx.autotune(du, icx.TUNE_RESIDUAL | icx.TUNE_ILU | icx.TUNE_ILU_FP32 | icx.TUNE_RETIME)
     assert rep["from_cache"] == 0 and rep["n_rejected"] == 0
     # residual: the default, two face bounds, three volume tiles; ILU, per
-    # precision: rows 2/4/6/8 x CTAs per SM 1..4 (36 x 36 blocks)
-    assert rep["n_timed"] == 6 + 2 * 16
+    # precision: 2 schedules x rows 2/4/6/8 x CTAs per SM 1..4 (36 x 36 blocks)
+    assert rep["n_timed"] == 6 + 2 * 32
     assert rep["residual_ms_tuned"] <= rep["residual_ms_default"]
     for k in range(2):
         assert 0 < rep["ilu_ms_tuned"][k] <= rep["ilu_ms_default"][k]
@@ -95,6 +97,7 @@ def test_autotune_parity_and_cache():
     assert ch["face_minb"] in (4, 5, 6)
     assert (ch["vol_threads"], ch["vol_minb"]) in VOL_TILES[1:]
     assert all(r in (2, 4, 6, 8) for r in ch["ilu_rows"]) and all(1 <= k <= 4 for k in ch["ilu_ctas"])
+    assert all(sc in (1, 2) for sc in ch["ilu_sched"])
     # the tuned residual is still the reference's residual
     r_or = ob.residual(ob.oracle(), spec.oracle_problem(), c, u)
     r = _residual(ctx, du)
@@ -109,7 +112,8 @@ def test_autotune_parity_and_cache():
 def test_tile_set_refuses_uncompiled_shapes():
     spec, c, u, ctx = _setup(dict(pde=BURGERS, nx=3, ny=3, p=1, g=1))  # 4 x 4 blocks: rows 2 and 4 only
     bad = [{"face_minb": 2}, {"face_minb": 7}, {"vol_threads": 128, "vol_minb": 4}, {"vol_threads": 512},
-           {"ilu_rows": [6, 0]}, {"ilu_rows": [0, 3]}, {"ilu_ctas": [5, 0]}, {"ilu_ctas": [0, -1]}]
+           {"ilu_rows": [6, 0]}, {"ilu_rows": [0, 3]}, {"ilu_ctas": [5, 0]}, {"ilu_ctas": [0, -1]},
+           {"ilu_sched": [3, 0]}, {"ilu_sched": [0, -1]}]
     for t in bad:
         with pytest.raises(icx.IcxError):
             ctx.tile = t
