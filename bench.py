@@ -323,7 +323,8 @@ def spmv_bench(n):
 def ilu_bench(n):
     """block-ILU(0) apply of the FD Jacobian of the n x n p = 2 Navier-Stokes
     manufactured solution: mean of 20 applies after 3 untimed ones, per
-    schedule and precision (CUDA events inside icx_ilu_apply)"""
+    schedule and precision (CUDA events inside icx_ilu_apply). The first
+    ilu_apply_flow_kernel launches are the FP64 sentinel-schedule ones."""
     import torch
     from iceicle_b200.workloads import ns_mms_config
     dev = torch.device("cuda", 0)
@@ -337,17 +338,18 @@ def ilu_bench(n):
     x = torch.randn(L.n_dof, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
     y = torch.empty_like(x)
     out = {"ilu": f"ns_mms_{n}x{n}_p2", "block": bs, "levels_per_sweep": 2 * n - 1}
-    for sched, name in ((1, "data_flow"), (2, "rows")):
+    # the data-flow apply (default rows per task and CTAs per SM) on its two
+    # schedules, then the row-pipelined apply
+    for sched, sn in ((2, "sentinel"), (1, "counters")):
+        ctx.tile = {"ilu_sched": [sched, sched]}
         for prec, pn in ((0, "fp64"), (1, "fp32")):
-            ctx.ilu_apply(vals, x, y, prec, sched, 3)
-            out[f"{name}_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, sched, 20)
-    # the data-flow apply on the sentinel schedule (default rows and CTAs), then
-    # with the autotuned schedule, rows per task and CTAs per SM
-    ctx.tile = {"ilu_sched": [2, 2]}
-    for prec, pn in ((0, "fp64"), (1, "fp32")):
-        ctx.ilu_apply(vals, x, y, prec, 1, 3)
-        out[f"data_flow_sentinel_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 1, 20)
+            ctx.ilu_apply(vals, x, y, prec, 1, 3)
+            out[f"data_flow_{sn}_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 1, 20)
     ctx.tile = {}
+    for prec, pn in ((0, "fp64"), (1, "fp32")):
+        ctx.ilu_apply(vals, x, y, prec, 2, 3)
+        out[f"rows_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 2, 20)
+    # the data-flow apply with the autotuned schedule, rows per task and CTAs per SM
     import iceicle_b200 as ib
     t = ctx.autotune(u, ib.TUNE_ILU | ib.TUNE_ILU_FP32)
     out["tuned_tile"] = {k: t["chosen"][k] for k in ("ilu_rows", "ilu_ctas", "ilu_sched")}
