@@ -54,7 +54,7 @@ class NewtonOptions(C.Structure):
                 ("ls_alpha_max", C.c_double), ("ls_alpha_min", C.c_double), ("ls_c1", C.c_double),
                 ("ls_c2", C.c_double), ("gmres_restart", C.c_int), ("gmres_max_it", C.c_int),
                 ("gmres_rtol", C.c_double), ("preconditioner", C.c_int), ("verbosity", C.c_int),
-                ("precision", C.c_int), ("pc_sweeps", C.c_int)]
+                ("precision", C.c_int), ("pc_sweeps", C.c_int), ("cuda_graphs", C.c_int)]
 
 
 class ExplicitOptions(C.Structure):
@@ -71,7 +71,7 @@ class NewtonReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("r0", C.c_double), ("r_final", C.c_double),
                 ("linear_iterations_total", C.c_int), ("residual_history", C.c_double * 64),
                 ("alpha_history", C.c_double * 64), ("pc_fallbacks", C.c_int),
-                ("linear_iterations", C.c_int * 64)]
+                ("linear_iterations", C.c_int * 64), ("graph_steps", C.c_int)]
 
 
 class LpcTrainOptions(C.Structure):

@@ -1,6 +1,7 @@
 // Device linear algebra for the Newton solver: block-diagonal inversion
 // (block-Jacobi preconditioner), block-ILU(0) on the element block pattern,
 // deterministic reductions and the multi-vector kernels of GMRES.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <vector>
@@ -269,9 +270,21 @@ __global__ void maxpy_kernel(long long n, const double* __restrict__ V, long lon
 }
 
 // y = a x + b y
+__device__ inline double axpby_val(double a, double x, double b, double y) { return a * x + b * y; }
+
 __global__ void axpby_kernel(long long n, double a, const double* __restrict__ x, double b, double* __restrict__ y) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    y[i] = a * x[i] + b * y[i];
+    y[i] = axpby_val(a, x[i], b, y[i]);
+}
+
+// v /= sqrt(*h2) when *h2 > 0, with the same operations as
+// la_axpby(n, 1 / sqrt(h2), v, 0, v) after the host has read h2
+__global__ void normalize_kernel(long long n, const double* __restrict__ h2, double* v) {
+  const double h = *h2;
+  if (!(h > 0.0)) return;
+  const double a = 1.0 / sqrt(h);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[i] = axpby_val(a, v[i], 0.0, v[i]);
 }
 
 // z = x + a y
@@ -603,6 +616,72 @@ double la_norm(LinalgWork& lw, long long n, const double* x, double* d_scratch, 
     }                                                              \
   } while (0)
 
+void ArnoldiGraphs::reset() {
+  for (cudaGraphExec_t& g : exec)
+    if (g) cudaGraphExecDestroy(g), g = nullptr;
+  std::fill(seen.begin(), seen.end(), 0);
+  failed = false;
+}
+
+void ArnoldiGraphs::release() {
+  reset();
+  exec.clear();
+  seen.clear();
+  if (cap) cudaStreamDestroy(cap), cap = nullptr;
+  if (hp) cudaFreeHost(hp), hp = nullptr;
+  key = 0;
+  m = 0;
+}
+
+// prepares the graph set for operators `key` and restart length m (drops
+// graphs of another key); false when it cannot be used
+static bool arnoldi_graphs_ready(ArnoldiGraphs& g, unsigned long long key, int m) {
+  if (g.m != m) {
+    g.release();
+    g.m = m;
+    g.exec.assign(m, nullptr);
+    g.seen.assign(m, 0);
+  }
+  if (!g.cap && cudaStreamCreateWithFlags(&g.cap, cudaStreamNonBlocking) != cudaSuccess) return false;
+  if (!g.hp && cudaMallocHost((void**)&g.hp, sizeof(double) * 3 * (m + 2)) != cudaSuccess) return false;
+  if (g.key != key) {
+    g.reset();
+    g.key = key;
+  }
+  return !g.failed;
+}
+
+// the graph of Arnoldi step j: captured on the step's second eager run under
+// the current key (the first run has done every one-time setup of the
+// kernels it launches), then replayed. Null: run the step eagerly.
+template <class Step>
+static cudaGraphExec_t arnoldi_graph(ArnoldiGraphs& g, int j, long long n, double* vj1, const double* h2, Step& step) {
+  if (g.failed) return nullptr;
+  if (g.exec[j]) return g.exec[j];
+  if (g.seen[j]++ < 1) return nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(g.cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t es = step(g.cap, g.hp);
+    if (es == cudaSuccess) {
+      normalize_kernel<<<grid_for(n), 256, 0, g.cap>>>(n, h2, vj1);
+      es = cudaGetLastError();
+    }
+    e = cudaStreamEndCapture(g.cap, &graph);
+    if (es != cudaSuccess) e = es;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g.exec[j], graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    // operators that cannot be captured: eager steps from now on under this key
+    (void)cudaGetLastError();
+    g.exec[j] = nullptr;
+    g.failed = true;
+    return nullptr;
+  }
+  return g.exec[j];
+}
+
 icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit, double rtol, const double* b,
                     double* x, int* iters, double* relres, cudaStream_t s, std::string* err) {
   long long n = kb.n;
@@ -622,6 +701,9 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
   }
   double tol = rtol * bnorm;
   std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hcol(m + 2), hp3(3 * (m + 2));
+  kb.graph_launches = 0;
+  bool use_graphs = kb.graphs && kb.graph_key != 0 && !kb.samples;
+  if (use_graphs && !arnoldi_graphs_ready(*kb.graphs, kb.graph_key, m)) use_graphs = false;
   GCK(cudaMemcpyAsync(kb.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   double beta = bnorm;
   int total = 0;
@@ -639,24 +721,35 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
           total % kb.sample_every == 0)
         GCK(cudaMemcpyAsync(kb.samples + (size_t)kb.sample_count++ * n, vj, sizeof(double) * n,
                             cudaMemcpyDeviceToDevice, s));
-      if (M) {
-        GCK((*M)(vj, kb.z));
-        GCK(A(kb.z, vj1));
+      // the step: preconditioner and operator, classical Gram-Schmidt twice
+      // and the norm of the result; the three reductions land in separate
+      // device slots [pass 1 | pass 2 | |v|^2] and come back in one copy
+      auto step = [&](cudaStream_t st, double* host_dst) -> cudaError_t {
+        cudaError_t e = M ? (*M)(vj, kb.z, st) : cudaSuccess;
+        if (e == cudaSuccess) e = A(M ? kb.z : vj, vj1, st);
+        for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
+          double* slot = kb.dh + (size_t)pass * (m + 2);
+          e = la_mdot(*kb.lw, n, kb.V, n, j + 1, vj1, slot, st);
+          if (e == cudaSuccess) e = la_maxpy(n, kb.V, n, j + 1, slot, -1.0, vj1, st);
+        }
+        if (e == cudaSuccess) e = la_mdot(*kb.lw, n, vj1, 0, 1, vj1, kb.dh + 2 * (m + 2), st);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(host_dst, kb.dh, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, st);
+        return e;
+      };
+      // replayed from a CUDA graph (which also normalises v_j+1 on the
+      // device), or launched one by one
+      cudaGraphExec_t gx = use_graphs ? arnoldi_graph(*kb.graphs, j, n, vj1, kb.dh + 2 * (m + 2), step) : nullptr;
+      if (gx) {
+        GCK(cudaGraphLaunch(gx, s));
+        GCK(cudaStreamSynchronize(s));
+        std::copy(kb.graphs->hp, kb.graphs->hp + 3 * (m + 2), hp3.begin());
+        ++kb.graph_launches;
       } else {
-        GCK(A(vj, vj1));
+        GCK(step(s, hp3.data()));
+        GCK(cudaStreamSynchronize(s));
       }
-      // classical Gram-Schmidt, twice, and the norm of the result: the three
-      // reductions land in separate device slots [pass 1 | pass 2 | |v|^2]
-      // and come back to the host in one copy
       std::fill(hcol.begin(), hcol.end(), 0.0);
-      for (int pass = 0; pass < 2; ++pass) {
-        double* slot = kb.dh + (size_t)pass * (m + 2);
-        GCK(la_mdot(*kb.lw, n, kb.V, n, j + 1, vj1, slot, s));
-        GCK(la_maxpy(n, kb.V, n, j + 1, slot, -1.0, vj1, s));
-      }
-      GCK(la_mdot(*kb.lw, n, vj1, 0, 1, vj1, kb.dh + 2 * (m + 2), s));
-      GCK(cudaMemcpyAsync(hp3.data(), kb.dh, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, s));
-      GCK(cudaStreamSynchronize(s));
       for (int i = 0; i <= j; ++i) hcol[i] += hp3[i] + hp3[(m + 2) + i];
       double hn = std::sqrt(hp3[2 * (m + 2)]);
       hcol[j + 1] = hn;
@@ -664,7 +757,7 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
         if (err) *err = "non-finite Krylov vector";
         return ICX_ERR_NONFINITE;
       }
-      if (hn > 0.0) GCK(la_axpby(n, 1.0 / hn, vj1, 0.0, vj1, s));
+      if (!gx && hn > 0.0) GCK(la_axpby(n, 1.0 / hn, vj1, 0.0, vj1, s));
       for (int i = 0; i < j; ++i) {
         double t = cs[i] * hcol[i] + sn[i] * hcol[i + 1];
         hcol[i + 1] = -sn[i] * hcol[i] + cs[i] * hcol[i + 1];
@@ -691,12 +784,12 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
     GCK(cudaMemsetAsync(kb.w, 0, sizeof(double) * n, s));
     GCK(la_maxpy(n, kb.V, n, j, kb.dh, 1.0, kb.w, s));
     if (M) {
-      GCK((*M)(kb.w, kb.z));
+      GCK((*M)(kb.w, kb.z, s));
       GCK(la_axpby(n, 1.0, kb.z, 1.0, x, s));
     } else {
       GCK(la_axpby(n, 1.0, kb.w, 1.0, x, s));
     }
-    GCK(A(x, kb.w));
+    GCK(A(x, kb.w, s));
     GCK(la_xpay(n, b, -1.0, kb.w, kb.r, s));
     if (kb.samples && kb.sample_count < kb.sample_cap)
       GCK(cudaMemcpyAsync(kb.samples + (size_t)kb.sample_count++ * n, kb.r, sizeof(double) * n,

@@ -70,6 +70,24 @@ cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s);
 #include <string>
 
 namespace icx {
+// CUDA graphs of the GMRES Arnoldi steps, one per step index j, kept by their
+// owner across solves. A graph holds every pointer and launch shape of the
+// step, so it stays valid while `key` (the owner's description of the
+// operators) is unchanged.
+struct ArnoldiGraphs {
+  unsigned long long key = 0;
+  int m = 0;
+  std::vector<cudaGraphExec_t> exec;  // [m]; null: not captured yet
+  std::vector<int> seen;              // [m] eager runs of step j under this key
+  bool failed = false;                // a capture failed under this key: eager steps only
+  cudaStream_t cap = nullptr;         // capture stream
+  double* hp = nullptr;               // pinned host copy of the step's reductions, 3 (m + 2) doubles
+  // drops the graphs (the key changed)
+  void reset();
+  // drops everything (owner teardown)
+  void release();
+};
+
 // device buffers of a restarted GMRES(m) on vectors of length n
 struct KrylovBuffers {
   long long n = 0;
@@ -87,8 +105,15 @@ struct KrylovBuffers {
   // stall test (0: off): stop when the residual after a restart cycle is above
   // half the residual `stall_cycles` cycles earlier
   int stall_cycles = 0;
+  // optional: replay the Arnoldi steps as CUDA graphs (graph_key != 0; the
+  // operators then launch only on the stream they are given, with arguments
+  // that do not change between calls). Not used while sampling.
+  ArnoldiGraphs* graphs = nullptr;
+  unsigned long long graph_key = 0;
+  int graph_launches = 0;  // out: Arnoldi steps replayed from a graph
 };
-using LinOp = std::function<cudaError_t(const double* x, double* y)>;
+// y = op(x), launched on stream s
+using LinOp = std::function<cudaError_t(const double* x, double* y, cudaStream_t s)>;
 double la_norm(LinalgWork& lw, long long n, const double* x, double* d_scratch, cudaStream_t s);
 // x = A^-1 b, right-preconditioned by M (null: none); classical Gram-Schmidt
 // with one re-orthogonalisation, FP64 Hessenberg/Givens on the host

@@ -1108,10 +1108,10 @@ icx_status icx_lm_solve(icx_ctx* c, double* d_u, double* x, const icx_lm_options
     icx::csr_rownorm_kernel<<<nb_n, 256, 0, strm>>>(n, s.d_t_rowptr, s.d_tvals, s.d_colnorm);
     icx::lm_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, strm>>>(n, N, lu, lb, s.d_colnorm, s.d_diag);
     icx::csr_spmv_kernel<<<nb_n, 256, 0, strm>>>(n, s.d_t_rowptr, s.d_t_colidx, s.d_tvals, s.d_res, s.d_jtr);
-    icx::LinOp A = [&](const double* xin, double* yout) {
-      icx::csr_spmv_kernel<<<nb_r, 256, 0, strm>>>(nr, s.d_rowptr, s.d_colidx, s.d_vals, xin, s.d_tmp);
-      icx::csr_spmv_kernel<<<nb_n, 256, 0, strm>>>(n, s.d_t_rowptr, s.d_t_colidx, s.d_tvals, s.d_tmp, yout);
-      icx::diag_axpy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, strm>>>(n, s.d_diag, xin, yout);
+    icx::LinOp A = [&](const double* xin, double* yout, cudaStream_t st) {
+      icx::csr_spmv_kernel<<<nb_r, 256, 0, st>>>(nr, s.d_rowptr, s.d_colidx, s.d_vals, xin, s.d_tmp);
+      icx::csr_spmv_kernel<<<nb_n, 256, 0, st>>>(n, s.d_t_rowptr, s.d_t_colidx, s.d_tvals, s.d_tmp, yout);
+      icx::diag_axpy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, s.d_diag, xin, yout);
       return cudaGetLastError();
     };
     int its = 0;

@@ -46,6 +46,9 @@ struct icx_solver_work {
   // rows per task of those applies: an element's counter grows by its task
   // count per apply (block size / rows), so the counters restart when it changes
   int flow_rows = 0;
+  icx::ArnoldiGraphs graphs;  // CUDA graphs of the GMRES Arnoldi steps
+  bool graphs_on = true;      // use them where the preconditioner allows (icx_newton_options.cuda_graphs)
+  long long graph_steps = 0;  // Arnoldi steps replayed from them
   // row-pipelined ILU apply: the context is one structured grid whose block
   // pattern is the 5-point element stencil in natural order
   bool rows_ok = false;
@@ -314,11 +317,30 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
     icx::KrylovBuffers* kb;
     ~CountOut() { if (dst) *dst = kb->sample_count; }
   } count_out{sample_count, &kb};
-  icx::LinOp A = [&](const double* xin, double* yout) {
-    return mixed ? icx::launch_bsr_spmv_f32(dm, w->vals32, xin, yout, s) : icx::launch_bsr_spmv(dm, w->vals, xin, yout, s);
+  icx::LinOp A = [&](const double* xin, double* yout, cudaStream_t st) {
+    return mixed ? icx::launch_bsr_spmv_f32(dm, w->vals32, xin, yout, st) : icx::launch_bsr_spmv(dm, w->vals, xin, yout, st);
   };
-  icx::LinOp M = [&](const double* xin, double* yout) { return apply_pc(c, pc, mixed, xin, yout, s); };
+  icx::LinOp M = [&](const double* xin, double* yout, cudaStream_t st) { return apply_pc(c, pc, mixed, xin, yout, st); };
+  // CUDA graphs of the Arnoldi steps where the preconditioner apply launches
+  // the same kernels with the same arguments every time: none, block-Jacobi,
+  // the two-step and sweep forms, and block-ILU(0) on the sentinel schedule
+  // (the counter schedule passes a new epoch to every apply, the row schedule
+  // likewise; the learned preconditioner is left out)
+  const bool graphable = w->graphs_on && (pc == 0 || pc == 1 || pc == 3 || pc == 4 ||
+                                    (pc == 2 && icx::flow_sentinel(dm.tile, mixed ? 1 : 0) &&
+                                     !(w->rows_ok && w->schedule == 2)));
+  if (graphable) {
+    const icx::TileChoice& t = dm.tile;
+    const int pi = mixed ? 1 : 0;
+    unsigned long long key = 1469598103934665603ull;  // FNV-1a over what the step's launches depend on
+    for (long long v : {(long long)pc, (long long)mixed, (long long)w->sweeps, (long long)m, (long long)t.flow_rows[pi],
+                        (long long)t.flow_ctas[pi], (long long)t.flow_sched[pi]})
+      key = (key ^ (unsigned long long)v) * 1099511628211ull;
+    kb.graphs = &w->graphs;
+    kb.graph_key = key | 1;
+  }
   icx_status st = icx::gmres_op(kb, A, pc ? &M : nullptr, maxit, rtol, b, x, iters, relres, s, &c->err);
+  w->graph_steps += kb.graph_launches;
   if (st != ICX_OK) {
     // a non-finite value may come from a failed kernel: report that first
     cudaError_t e = cudaStreamSynchronize(s);
@@ -415,6 +437,7 @@ void free_solver_work(icx_ctx* c) {
   void* ptrs[] = {w->vals32, w->pc32, w->uinv32, w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du,
                   w->ustep, w->rwork, w->pct, w->pct2, w->pct3, w->pct4, w->order, w->cnt, w->cnt_rows, w->pc_err,
                   w->dh, w->flag, w->lw.partial};
+  w->graphs.release();
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete w;
@@ -462,6 +485,7 @@ icx_status icx_newton_default_options(icx_newton_options* o) {
   o->verbosity = 0;
   o->precision = 0;          // all FP64
   o->pc_sweeps = 2;
+  o->cuda_graphs = 1;
   return ICX_OK;
 }
 
@@ -578,6 +602,8 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   icx_status st = ensure_work(c, opt->gmres_restart);
   if (st != ICX_OK) return st;
   c->sw->sweeps = opt->pc_sweeps;
+  c->sw->graphs_on = opt->cuda_graphs != 0;
+  const long long graph_steps0 = c->sw->graph_steps;
   const bool mixed = opt->precision == 1;
   if (mixed && (st = ensure_mixed(c)) != ICX_OK) return st;
   icx_solver_work* w = c->sw;
@@ -657,6 +683,7 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   R->iterations = k;
   R->converged = converged;
   R->r_final = rk;
+  R->graph_steps = (int)(c->sw->graph_steps - graph_steps0);
   return converged ? ICX_OK : ICX_ERR_NOT_CONVERGED;
 }
 }
@@ -708,11 +735,11 @@ extern "C" icx_status icx_mfnk_solve(icx_ctx* c, double* d_u, const icx_newton_o
   // are free while GMRES runs (du receives the solution at the end)
   double* up = w->pct;
   double* rp = w->ustep;
-  icx::LinOp A = [&](const double* p, double* y) -> cudaError_t {
-    cudaError_t e = icx::la_xpay(n, d_u, eps, p, up, s);  // up = u + eps p
-    if (e == cudaSuccess) e = icx::launch_residual(dm, c->phys, up, rp, s);
-    if (e == cudaSuccess) e = icx::la_xpay(n, rp, -1.0, w->res, y, s);       // R(u + eps p) - R(u)
-    if (e == cudaSuccess) e = icx::la_axpby(n, 1.0 / eps, y, 0.0, y, s);    // / eps
+  icx::LinOp A = [&](const double* p, double* y, cudaStream_t st) -> cudaError_t {
+    cudaError_t e = icx::la_xpay(n, d_u, eps, p, up, st);  // up = u + eps p
+    if (e == cudaSuccess) e = icx::launch_residual(dm, c->phys, up, rp, st);
+    if (e == cudaSuccess) e = icx::la_xpay(n, rp, -1.0, w->res, y, st);       // R(u + eps p) - R(u)
+    if (e == cudaSuccess) e = icx::la_axpby(n, 1.0 / eps, y, 0.0, y, st);    // / eps
     return e;
   };
   bool converged = false;

@@ -260,6 +260,12 @@ typedef struct icx_newton_options {
   /* preconditioner 4 (block-ILU(0) factors applied by Jacobi sweeps): the
    * sweeps per triangular solve */
   int pc_sweeps;
+  /* 1 (default): replay each GMRES Arnoldi step (preconditioner, operator,
+   * both Gram-Schmidt passes, norm, normalisation and the copy of the
+   * reductions) as one CUDA graph once it has run eagerly, for preconditioners
+   * 0-4 (block-ILU(0) on its default sentinel schedule). The same kernels run
+   * in the same order: results are identical with 0. */
+  int cuda_graphs;
 } icx_newton_options;
 
 typedef struct icx_newton_report {
@@ -273,6 +279,7 @@ typedef struct icx_newton_report {
                         solve missed gmres_rtol, or stalled: under half the residual reduction over 10
                         restart cycles) */
   int linear_iterations[64]; /* GMRES iterations of each Newton step (fallback included) */
+  int graph_steps;           /* Arnoldi steps replayed from CUDA graphs */
 } icx_newton_report;
 
 /* Linear solve J x = b with the BSR values d_vals (the KSPSolve of

@@ -280,3 +280,31 @@ def test_mfnk_ns_with_linesearch_matches_assembled_newton():
     assert r1.converged and r2.converged
     a, b = u1.cpu().numpy(), u2.cpu().numpy()
     assert np.linalg.norm(a - b) <= 1e-6 * np.linalg.norm(a)
+
+
+@pytest.mark.parametrize("pc,precision", [(2, 0), (2, 1), (1, 0), (4, 1), (0, 0)],
+                         ids=["ilu0_fp64", "ilu0_mixed", "jacobi_fp64", "sweeps_mixed", "none_fp64"])
+def test_newton_cuda_graphs_bit_identical(pc, precision):
+    """the Arnoldi steps replayed as CUDA graphs launch the same kernels in the
+    same order as the eager steps: the Newton iterates, GMRES counts and
+    converged state are identical bit for bit, and graphs were replayed"""
+    spec = Spec(pde=BURGERS, nx=8, ny=7, p=2, g=2, mu=1e-2, a=(0.0, 0.0), b=(1.0, 0.5),
+                dirichlet=[("constant", [1, 0.0])])
+    c = spec.coords()
+    out = {}
+    for graphs in (0, 1):
+        ctx = spec.context(c)
+        xy = ctx.basis_node_coords().reshape(-1, 2)
+        u0 = 0.5 * np.sin(2 * np.pi * xy[:, 0]) * np.sin(2 * np.pi * xy[:, 1]) + \
+            1e-3 * np.random.default_rng(8).standard_normal(len(xy))
+        du = torch.from_numpy(u0).cuda()
+        rep = ctx.newton_solve(du, _newton_opts(tau_abs=1e-11, kmax=15, preconditioner=pc, precision=precision,
+                                                gmres_restart=10, gmres_rtol=1e-6, gmres_max_it=4000,
+                                                cuda_graphs=graphs))
+        assert rep.converged, list(rep.residual_history[:rep.iterations + 1])
+        out[graphs] = (du.cpu().numpy(), rep.iterations, list(rep.linear_iterations[:rep.iterations]),
+                       list(rep.residual_history[:rep.iterations + 1]), rep.graph_steps)
+    (u0_, it0, lin0, h0, g0), (u1_, it1, lin1, h1, g1) = out[0], out[1]
+    assert g0 == 0 and g1 > 0
+    assert it0 == it1 and lin0 == lin1 and h0 == h1
+    assert np.array_equal(u0_.view(np.uint64), u1_.view(np.uint64))
