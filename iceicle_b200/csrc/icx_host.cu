@@ -648,6 +648,9 @@ icx_status icx_setup(icx_ctx* c) {
     return fail(c, ICX_ERR_INVALID, "mesh, fespace and disc must be defined before setup");
   cudaError_t e = cudaSetDevice(c->device);
   if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+  // the solver buffers (element order, ILU pattern checks, CUDA graphs of the
+  // GMRES steps) refer to the device tables rebuilt below
+  icx::free_solver_work(c);
   free_dev(c->dm);
   DeviceMesh& dm = c->dm;
   int g = c->geo_order, P = c->p;

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <functional>
 #include <vector>
@@ -334,7 +335,9 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
     const int pi = mixed ? 1 : 0;
     unsigned long long key = 1469598103934665603ull;  // FNV-1a over what the step's launches depend on
     for (long long v : {(long long)pc, (long long)mixed, (long long)w->sweeps, (long long)m, (long long)t.flow_rows[pi],
-                        (long long)t.flow_ctas[pi], (long long)t.flow_sched[pi]})
+                        (long long)t.flow_ctas[pi], (long long)t.flow_sched[pi], (long long)(uintptr_t)dm.bsr_rowptr,
+                        (long long)(uintptr_t)dm.bsr_colidx, (long long)(uintptr_t)dm.bsr_diag,
+                        (long long)(uintptr_t)w->order})
       key = (key ^ (unsigned long long)v) * 1099511628211ull;
     kb.graphs = &w->graphs;
     kb.graph_key = key | 1;
