@@ -499,7 +499,9 @@ typedef struct icx_tune_report {
  * the same key unless ICX_TUNE_RETIME is set. rep may be NULL. */
 icx_status icx_autotune(icx_ctx* ctx, const double* d_u, int parts, icx_tune_report* rep);
 icx_status icx_tile_get(const icx_ctx* ctx, icx_tile_choice* tile);
-/* ICX_ERR_INVALID for a shape that is not compiled for this context */
+/* ICX_ERR_INVALID for a shape that is not compiled for this context. icx_setup
+ * returns a context to the default shapes (call icx_autotune again after it;
+ * the cached choice then costs nothing). */
 icx_status icx_tile_set(icx_ctx* ctx, const icx_tile_choice* tile);
 
 #ifdef __cplusplus
