@@ -8,10 +8,12 @@ One step = one full residual evaluation R(u) of the whole mesh
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs under torch.distributed.run: every rank evaluates its own replica
-(weak scaling; the single-GPU path has no data-path collective), the timed
-region is bracketed by a barrier and synchronisations and the time is the
-maximum over ranks. --impl reference times the reference's own CPU
+N > 1 runs under torch.distributed.run with the mesh partitioned into
+element-row strips (iceicle_b200.partition; weak scaling: every rank owns a
+128 x 128 strip of a 128 x 128 N mesh). A step is then the halo exchange of
+one coefficient row per neighbour over NCCL plus the rank's residual. The
+timed region is bracketed by a barrier and synchronisations and the time is
+the maximum over ranks. --impl reference times the reference's own CPU
 implementation (its headers compiled as oracle/_ref) on the host cores.
 """
 import argparse
@@ -405,9 +407,23 @@ def run_ours(a):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
-    from iceicle_b200.workloads import ns_mms_config
-    wl = ns_mms_config(nx=NX, ny=NY, p=3, geo_order=2, device=local)
-    N = wl.ctx.layout.n_dof
+    from iceicle_b200.partition import StripPlan, StripResidual
+    from iceicle_b200.workloads import ns_mms_config, ns_mms_strip_config
+    if ws > 1:
+        # weak scaling over element-row strips: rank r owns rows
+        # [128 r, 128 (r + 1)) of the 128 x 128 ws mesh plus one ghost row per
+        # neighbour; a step is the halo exchange (NCCL send/recv of one row of
+        # coefficients per neighbour) and the residual of the rank's sub-mesh
+        plan = StripPlan(NX, NY * ws, ws, rank, 2)
+        wl = ns_mms_strip_config(plan, p=3, geo_order=2, device=local)
+        step_fn = StripResidual(wl.ctx, plan)
+        o0, o1 = plan.owned_dofs(wl.ctx.layout.block_size)
+    else:
+        plan = None
+        wl = ns_mms_config(nx=NX, ny=NY, p=3, geo_order=2, device=local)
+        step_fn = wl.ctx.form_residual
+        o0, o1 = 0, wl.ctx.layout.n_dof
+    N = o1 - o0  # owned DOFs of this rank
     dev = torch.device("cuda", local)
     u = torch.from_numpy(wl.u0).to(dev)
     res = torch.empty_like(u)
@@ -422,7 +438,7 @@ def run_ours(a):
     elif not a.no_tune:
         tune = wl.ctx.autotune(u, ib.TUNE_RESIDUAL)
     for _ in range(max(a.warmup, 3)):
-        wl.ctx.form_residual(u, res, stream)
+        step_fn(u, res, stream)
     torch.cuda.synchronize(dev)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
@@ -433,7 +449,7 @@ def run_ours(a):
     for k in range(a.steps):
         flush.zero_()
         starts[k].record(stream)
-        wl.ctx.form_residual(u, res, stream)
+        step_fn(u, res, stream)
         ends[k].record(stream)
     torch.cuda.synchronize(dev)
     if ws > 1:
@@ -451,24 +467,34 @@ def run_ours(a):
     # copied in from pinned host memory and its residual copied back
     # (icx_form_residuals_host overlaps the copies of consecutive steps); the
     # same measured one step at a time, each step's copies and kernels in turn
-    h_u = torch.from_numpy(np.tile(wl.u0, (a.steps, 1))).pin_memory()
-    h_r = torch.empty((a.steps, N), dtype=torch.float64).pin_memory()
-    for _ in range(max(a.warmup, 3) // 3):  # warm-up over the same host buffers (first touches from the GPU)
-        wl.ctx.form_residuals_host(h_u, h_r)
-    torch.cuda.synchronize(dev)
-    ms_e2e = wl.ctx.form_residuals_host(h_u, h_r)
-    h_u1, h_r1 = h_u[0], h_r[0]
+    # (with strips: each step copies the rank's owned rows in, exchanges the
+    # halo and copies the owned residual back, one step at a time)
+    if plan is None:
+        h_u = torch.from_numpy(np.tile(wl.u0, (a.steps, 1))).pin_memory()
+        h_r = torch.empty((a.steps, N), dtype=torch.float64).pin_memory()
+        for _ in range(max(a.warmup, 3) // 3):  # warm-up over the same host buffers (first touches from the GPU)
+            wl.ctx.form_residuals_host(h_u, h_r)
+        torch.cuda.synchronize(dev)
+        ms_e2e = wl.ctx.form_residuals_host(h_u, h_r)
+        h_u1, h_r1 = h_u[0], h_r[0]
+    else:
+        h_u1 = torch.from_numpy(wl.u0[o0:o1].copy()).pin_memory()
+        h_r1 = torch.empty(N, dtype=torch.float64).pin_memory()
     e2e_s = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     e2e_e = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
-    for k in range(a.steps):
+    for k in range(-1, a.steps):  # one untimed step first
         flush.zero_()
-        e2e_s[k].record(stream)
-        u.copy_(h_u1, non_blocking=True)
-        wl.ctx.form_residual(u, res, stream)
-        h_r1.copy_(res, non_blocking=True)
-        e2e_e[k].record(stream)
+        if k >= 0:
+            e2e_s[k].record(stream)
+        u[o0:o1].copy_(h_u1, non_blocking=True)
+        step_fn(u, res, stream)
+        h_r1.copy_(res[o0:o1], non_blocking=True)
+        if k >= 0:
+            e2e_e[k].record(stream)
     torch.cuda.synchronize(dev)
     ms_e2e_seq = sum(s.elapsed_time(e) for s, e in zip(e2e_s, e2e_e))
+    if plan is not None:
+        ms_e2e = ms_e2e_seq
     if ws > 1:
         t = torch.tensor([ms, ms_e2e, ms_e2e_seq], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -497,9 +523,12 @@ def run_ours(a):
             "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded manufactured solution)",
-            "config": dict(WORKLOAD, parallelism=f"replicas x{ws}" if ws > 1 else "single GPU"),
+            "config": dict(WORKLOAD, parallelism=(f"element-row strips x{ws}: 128 x 128 owned per GPU of a "
+                                                  f"128 x {NY * ws} mesh, one halo row per neighbour (NCCL send/recv)")
+                           if ws > 1 else "single GPU"),
             "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N,
-                    "api": "icx_form_residuals_host (copies of consecutive steps overlapped)",
+                    "api": ("icx_form_residuals_host (copies of consecutive steps overlapped)" if ws == 1 else
+                            "owned rows in, halo exchange, icx_form_residual, owned residual out; one step at a time"),
                     "one_step_at_a_time": e2e_seq},
             "gpu_launches": 2 * a.steps,
             "roofline": {"bound": "hbm",

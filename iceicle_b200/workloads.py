@@ -118,6 +118,48 @@ def ns_mms_config(nx=128, ny=128, p=3, geo_order=2, seed=4321, device=0, perturb
                     "ns_mms", [prm])
 
 
+def ns_mms_strip_config(plan, p=3, geo_order=2, seed=4321, device=0, perturb=0.05, interior_penalty=True,
+                        state_noise=1e-3, mu=0.01):
+    """one rank's part of the Navier-Stokes manufactured solution on the
+    plan.nx x plan.ny mesh of square elements over [0, 1] x [0, ny / nx]
+    (the single-rank workload is the whole of it, [0, 1]^2 when ny = nx):
+    the sub-mesh of element rows [g0, g1) (iceicle_b200.partition) on the
+    global perturbed nodes, with the state of ns_mms_config at its nodes
+    (noise seeded by seed + rank)"""
+    from .partition import sub_coords
+    nx, ny, g = plan.nx, plan.ny, geo_order
+    ymax = ny / nx
+    coords = lattice_coords((nx, ny), g, (0.0, 0.0), (1.0, ymax))
+    if perturb:
+        coords = perturb_smooth(coords, (nx, ny), perturb, seed, (0.0, 0.0), (1.0, ymax))
+    sub = sub_coords(plan, coords)
+    prm = ns_mms_params(mu=mu)
+    ctx = Context(device)
+    h = ymax / ny
+    ctx.mesh_uniform((nx, plan.rows), (0.0, plan.g0 * h), (1.0, plan.g1 * h), g, (DIRICHLET,) * 4, (0,) * 4)
+    ctx.set_coords(sub)
+    ctx.fespace(p)
+    ctx.disc_navier_stokes(prm[0], prm[1], prm[2], FLUX_VANLEER)
+    ctx.disc_options(interior_penalty, 0.0)
+    user = C.cast(prm, C.c_void_p)
+    ctx.dirichlet(0, workload_fn("ns_mms_state"), user)
+    ctx.source(workload_fn("ns_mms_source"), user)
+    ctx.setup()
+    xy = ctx.basis_node_coords().reshape(-1, 2)
+    st = np.zeros((xy.shape[0], 4))
+    f = workload_fn("ns_mms_state")
+    out = (C.c_double * 4)()
+    pt = (C.c_double * 2)()
+    for k in range(xy.shape[0]):
+        pt[0], pt[1] = xy[k, 0], xy[k, 1]
+        f(pt, out, user)
+        st[k] = out[:]
+    rng = np.random.default_rng(seed + plan.rank)
+    st *= 1.0 + state_noise * rng.standard_normal(st.shape)
+    return Workload(ctx, sub, np.ascontiguousarray(st.reshape(-1)),
+                    dict(prm=list(prm), p=p, g=geo_order, rows=(plan.g0, plan.g1)), "ns_mms_strip", [prm])
+
+
 def batched_problem_specs(n_problems=512, seed=2024, n_range=(8, 96), orders=(1, 2, 3, 4)):
     """the seeded problem list: dicts with n, p, mu, theta and the initial
     state's wave numbers and phases"""
