@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--ilu", type=int, default=0, metavar="N",
                     help="only time the block-ILU(0) apply (data-flow and row-pipelined, FP64 and FP32 factors) "
                          "of the N x N p = 2 Navier-Stokes Jacobian and print one JSON line")
+    ap.add_argument("--factor", action="store_true",
+                    help="only time the block-ILU(0) factorisation (Burgers 32 x 32 p = 2, NS 128 x 128 p = 3, "
+                         "NS 256 x 256 p = 2) and print one JSON line")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-preconditioner Newton comparison (256 x 256 Navier-Stokes, p = 2)")
     ap.add_argument("--batched", type=int, default=64, metavar="N",
@@ -363,6 +366,40 @@ def ilu_bench(n):
     print(json.dumps(out))
 
 
+def factor_bench():
+    """block-ILU(0) factorisation time (one launch per anti-diagonal level plus
+    the upper-block scaling): host wall time of one icx_ilu_apply with a single
+    apply, minus that apply's device time, best of 3 after a warm-up. The
+    first ilu_level_kernel launches are the Burgers workload's."""
+    import torch
+    from iceicle_b200.workloads import burgers_config, ns_mms_config
+    out = {"factor": "block-ILU(0), FP64"}
+    for name, make in (("burgers_32x32_p2", lambda: burgers_config()),
+                       ("ns_mms_128x128_p3", lambda: ns_mms_config(nx=128, ny=128, p=3, geo_order=2)),
+                       ("ns_mms_256x256_p2", lambda: ns_mms_config(nx=256, ny=256, p=2, geo_order=2, mu=0.01))):
+        wl = make()
+        ctx, L = wl.ctx, wl.ctx.layout
+        bs = L.block_size
+        u = torch.from_numpy(wl.u0).cuda()
+        res = torch.empty_like(u)
+        vals = torch.empty(L.nnz_blocks * bs * bs, dtype=torch.float64, device="cuda")
+        ctx.form_jacobian_fd(u, res, vals)
+        x = torch.randn(L.n_dof, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+        y = torch.empty_like(x)
+        ctx.ilu_apply(vals, x, y, 0, 1, 2)
+        ts = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ms_apply = ctx.ilu_apply(vals, x, y, 0, 1, 1)
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t0) * 1e3 - ms_apply)
+        nx = int(round((L.n_elem) ** 0.5))
+        out[name] = {"block": bs, "levels": 2 * nx - 1, "factor_ms": min(ts), "us_per_level": 1e3 * min(ts) / (2 * nx - 1)}
+        del wl
+    print(json.dumps(out))
+
+
 def learned_bench(torch, dev, tune=True):
     """Newton solve time to |r| <= 1e-10 on one fresh seeded instance of the
     256 x 256 p = 2 Navier-Stokes manufactured solution (Re drawn from
@@ -579,6 +616,8 @@ def main():
         spmv_bench(a.spmv)
     elif a.ilu:
         ilu_bench(a.ilu)
+    elif a.factor:
+        factor_bench()
     elif a.impl == "reference":
         run_reference(a)
     else:
