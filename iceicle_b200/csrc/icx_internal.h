@@ -199,6 +199,7 @@ void free_host_pipe(icx_ctx* c);
 // solver internals the training uses (icx_solver.cu): copy a Jacobian into the
 // solver and build preconditioner `kind` with mixed-precision copies; apply it;
 // the FP32 copy of the Jacobian
+// (sweeps < 0 keeps the solver's Jacobi sweeps per triangle)
 icx_status solver_prepare_pc(icx_ctx* c, const double* vals, int kind, int sweeps);
 cudaError_t solver_apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* z, cudaStream_t s);
 const float* solver_vals32(icx_ctx* c);

@@ -802,7 +802,7 @@ icx_status solver_prepare_pc(icx_ctx* c, const double* vals, int kind, int sweep
   if (st != ICX_OK) return st;
   if ((st = ensure_mixed(c)) != ICX_OK) return st;
   icx_solver_work* w = c->sw;
-  w->sweeps = sweeps;
+  if (sweeps >= 0) w->sweeps = sweeps;  // negative: keep the solver's
   cudaStream_t s = 0;
   CK(cudaMemcpyAsync(w->vals, vals, sizeof(double) * (size_t)c->dm.nnzb * w->bs * w->bs, cudaMemcpyDeviceToDevice, s));
   CK(build_pc(c, kind, true, s));

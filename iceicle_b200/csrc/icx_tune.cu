@@ -197,7 +197,7 @@ struct Tuner {
     fill_hash_kernel<<<592, 256, 0, s>>>(x, n);
     TCK(cudaGetLastError());
     TCK(cudaStreamSynchronize(s));
-    icx_status st = icx::solver_prepare_pc(c, vals, 2, 0);
+    icx_status st = icx::solver_prepare_pc(c, vals, 2, -1);
     if (st != ICX_OK) return st;
     for (int pi = 0; pi < 2; ++pi) {
       if (!(pi == 0 ? fp64 : fp32)) continue;
