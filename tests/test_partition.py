@@ -28,7 +28,7 @@ def test_strip_rows_refuses_too_many_ranks():
         strip_rows(3, 4, 0)
 
 
-@pytest.mark.parametrize("nranks", [1, 2, 3])
+@pytest.mark.parametrize("nranks", [1, 2, 3, 7])  # 7: one owned row per rank
 def test_plan_ranges(nranks):
     nx, ny, g, bs = 5, 7, 2, 36
     for r in range(nranks):
