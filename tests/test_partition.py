@@ -61,8 +61,8 @@ def _free_port():
 
 
 def _rank_main(rank, nranks, port, kw, q):
-    """one gloo rank: its sub-mesh state with ghosts zeroed, the exchange,
-    then the oracle residual of the sub-mesh against the global one"""
+    """one gloo rank: its sub-mesh state with the ghost rows set to NaN, the
+    exchange, then the oracle residual of the sub-mesh against the global one"""
     try:
         import torch
         import torch.distributed as dist
