@@ -443,6 +443,9 @@ def run_ours(a):
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        # the communicator is created by a collective of every rank before the
+        # first point-to-point batch of the halo exchange
+        dist.barrier(device_ids=[local])
     torch.cuda.set_device(local)
     from iceicle_b200.partition import StripPlan, StripResidual
     from iceicle_b200.workloads import ns_mms_config, ns_mms_strip_config
