@@ -37,3 +37,39 @@ def test_create_without_device_fails_loudly():
     h = C.c_void_p()
     st = ib.lib().icx_create(C.byref(h), 0)
     assert st == 8  # ICX_ERR_NO_DEVICE: there is no CPU fallback
+
+
+def declared_arity():
+    """number of parameters of every declared icx_* function"""
+    out = {}
+    inc = os.path.join(ROOT, "include")
+    for fn in os.listdir(inc):
+        if not fn.endswith(".h"):
+            continue
+        txt = open(os.path.join(inc, fn)).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        for m in re.finditer(r"^\s*(?:icx_status|void|const char\*)\s+(icx_\w+)\s*\(([^;]*?)\)\s*;", txt,
+                             flags=re.M | re.S):
+            params = m.group(2).strip()
+            depth, n = 0, (0 if params in ("", "void") else 1)
+            for ch in params:
+                depth += ch == "("
+                depth -= ch == ")"
+                n += ch == "," and depth == 0
+            out[m.group(1)] = n
+    return out
+
+
+def test_python_bindings_match_declared_parameters():
+    """every ctypes signature the Python mirror sets has the header's
+    parameter count (a mismatch would pass wrong arguments silently)"""
+    lib = ib.lib()
+    arity = declared_arity()
+    checked = 0
+    for name, n in arity.items():
+        f = getattr(lib, name, None)
+        if f is None or getattr(f, "argtypes", None) is None:
+            continue
+        assert len(f.argtypes) == n, (name, len(f.argtypes), n)
+        checked += 1
+    assert checked >= 40
