@@ -73,3 +73,37 @@ def test_python_bindings_match_declared_parameters():
         assert len(f.argtypes) == n, (name, len(f.argtypes), n)
         checked += 1
     assert checked >= 40
+
+
+STRUCTS = {"icx_layout_info": "LayoutInfo", "icx_newton_options": "NewtonOptions",
+           "icx_newton_report": "NewtonReport", "icx_explicit_options": "ExplicitOptions",
+           "icx_explicit_report": "ExplicitReport", "icx_lpc_train_options": "LpcTrainOptions",
+           "icx_lpc_train_report": "LpcTrainReport", "icx_tile_choice": "TileChoice",
+           "icx_tune_report": "TuneReport", "icx_lm_options": "LMOptions", "icx_lm_report": "LMReport"}
+
+
+def test_python_structs_match_c_layout():
+    """sizeof and every field's offset of the header's structs, compiled by
+    gcc, against the ctypes mirrors (same field names)"""
+    import subprocess
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "iceicle_b200.h"', "int main(void) {"]
+    for cname, pname in STRUCTS.items():
+        py = getattr(ib, pname)
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'  printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines += ["  return 0;", "}"]
+    out_dir = os.path.join(ROOT, "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    src, exe = os.path.join(out_dir, "abi_layout.c"), os.path.join(out_dir, "abi_layout")
+    open(src, "w").write("\n".join(lines) + "\n")
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+    got = {}
+    for ln in subprocess.run([exe], check=True, capture_output=True, text=True).stdout.splitlines():
+        s, key, v = ln.split()
+        got[(s, key)] = int(v)
+    for cname, pname in STRUCTS.items():
+        py = getattr(ib, pname)
+        assert got[(cname, "size")] == C.sizeof(py), (cname, got[(cname, "size")], C.sizeof(py))
+        for f in py._fields_:
+            assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])
