@@ -76,20 +76,33 @@ def dist_env():
 
 # ------------------------------------------------------------ CPU baseline
 def _ref_worker(args):
-    """time the reference's form_residual on the full workload in one process"""
-    nrep, seed = args
+    """time the reference's form_residual on the full workload in one process:
+    the same mesh nodes and initial state as the GPU arm (manufactured state
+    at the basis nodes with the seeded 1e-3 noise), built from the oracle's
+    own workload callbacks so that this process maps no product library.
+    Returns (unknowns, seconds per residual, loaded product libraries)."""
+    nrep, _ = args
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bindings as ob
     from specs import NS, Spec
     spec = Spec(pde=NS, nx=NX, ny=NY, p=3, g=2, ip=True, source=True, perturb=0.05, seed=4321)
     pb = spec.oracle_problem()
     c = spec.coords()
-    u = spec.state(np.random.default_rng(seed))
+    u = spec.mms_state(c, seed=4321, noise=1e-3)
     s = C.c_double()
     rc = ob.ref().fn("time_form_residual")(C.byref(pb), c.ctypes.data_as(C.c_void_p),
                                            u.ctypes.data_as(C.c_void_p), nrep, C.byref(s))
     assert rc == 0
-    return spec.N, s.value
+    return spec.N, s.value, _mapped_product_libs()
+
+
+def _mapped_product_libs():
+    """product shared objects mapped into this process (the reference arm must map none)"""
+    try:
+        with open("/proc/self/maps") as f:
+            return sorted({ln.split()[-1] for ln in f if "libiceicle_b200" in ln})
+    except OSError:
+        return []
 
 
 def cpu_reference(nrep, procs):
@@ -102,7 +115,7 @@ def cpu_reference(nrep, procs):
     else:
         with mp.get_context("spawn").Pool(procs) as pool:
             res = pool.map(_ref_worker, [(nrep, i) for i in range(procs)])
-    value = sum(n / t for n, t in res)
+    value = sum(r[0] / r[1] for r in res)
     return value, res
 
 
@@ -120,15 +133,17 @@ def run_reference(a):
     # each process: one untimed warm-up evaluation, then `steps` timed ones
     value, res = cpu_reference(a.steps, procs)
     wall = time.time() - t0
+    mapped = sorted({m for r in res for m in r[2]})
+    assert not mapped, f"reference arm mapped product libraries: {mapped}"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": 0,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * np.mean([t for _, t in res]),
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * np.mean([r[1] for r in res]),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded)", "config": WORKLOAD,
+        "data": "synthetic (seeded manufactured solution)", "config": WORKLOAD, "parallelism": "host processes",
         "cpu_baseline": {"value": value, "unit": "DOF/s", "cores": procs, "kind": "reference",
                          "sample": f"{procs} concurrent processes x full 128x128 p3 residual (reference headers, -O3)"},
         "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "wall_s": wall,
+        "wall_s": wall, "product_libs_mapped": mapped,
     }
     print(json.dumps(line))
 
@@ -137,10 +152,10 @@ def run_reference(a):
 class ClockSampler:
     def __init__(self, index):
         self.proc = None
-        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
         try:
-            os.makedirs(os.path.dirname(self.out), exist_ok=True)
-            self.f = open(self.out, "w")
+            self.f = tempfile.NamedTemporaryFile("w", prefix="icx_clocks_", suffix=".csv", delete=False)
+            self.out = self.f.name
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={index}", "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -157,10 +172,12 @@ class ClockSampler:
         self.proc.wait()
         self.f.close()
         rows = []
-        for line in open(self.out):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 7:
-                rows.append(parts)
+        with open(self.out) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 7:
+                    rows.append(parts)
+        os.unlink(self.out)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
@@ -563,9 +580,9 @@ def run_ours(a):
             "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded manufactured solution)",
-            "config": dict(WORKLOAD, parallelism=(f"element-row strips x{ws}: 128 x 128 owned per GPU of a "
-                                                  f"128 x {NY * ws} mesh, one halo row per neighbour (NCCL send/recv)")
-                           if ws > 1 else "single GPU"),
+            "config": WORKLOAD,
+            "parallelism": (f"element-row strips x{ws}: 128 x 128 owned per GPU of a 128 x {NY * ws} mesh, "
+                            "one halo row per neighbour (NCCL send/recv)") if ws > 1 else "single GPU",
             "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N,
                     "api": ("icx_form_residuals_host (copies of consecutive steps overlapped)" if ws == 1 else
                             "owned rows in, halo exchange, icx_form_residual, owned residual out; one step at a time"),
@@ -597,7 +614,7 @@ def run_ours(a):
             sys.path.insert(0, os.path.join(ROOT, "tests"))
             import oracle_bindings as ob
             if ob.ref_available():
-                n, t = _ref_worker((3, 0))
+                n, t, _ = _ref_worker((3, 0))
                 line["cpu_baseline"] = {"value": n / t, "unit": "DOF/s", "cores": 1, "kind": "reference",
                                         "sample": "3 full 128x128 p3 residuals, 1 thread (reference is serial)"}
             else:

@@ -79,6 +79,7 @@ extern "C" icx_status icx_form_residual_noalloc(icx_ctx* c, const double* d_u, d
   double* base = nullptr;
   if (e == cudaSuccess) e = scratch_address(c->device, &base);
   if (e != cudaSuccess) {
+    if (cur >= 0 && cur != c->device) cudaSetDevice(cur);  // leave the caller's device current
     c->err = std::string("scratch address lookup: ") + cudaGetErrorString(e);
     return ICX_ERR_CUDA;
   }

@@ -127,5 +127,14 @@ class StripResidual:
         return v[d0:d1]
 
     def __call__(self, u_local, res_local, stream=None):
-        halo_exchange(self.plan, u_local, self.bs, self.group)
-        self.ctx.form_residual(u_local, res_local, stream)
+        """exchange, then the residual on `stream` (torch's current stream when
+        None). The exchange is issued on that stream too, so its receives are
+        ordered before the residual kernels whatever stream the caller uses."""
+        import torch
+        if stream is None or not u_local.is_cuda:
+            halo_exchange(self.plan, u_local, self.bs, self.group)
+            self.ctx.form_residual(u_local, res_local, stream)
+            return
+        with torch.cuda.stream(stream):
+            halo_exchange(self.plan, u_local, self.bs, self.group)
+            self.ctx.form_residual(u_local, res_local, stream)

@@ -1522,3 +1522,26 @@ done:
   disc_free(&D);
   return rc;
 }
+
+/* ------------------------------------------------------------------ */
+/* physical coordinates of the Lagrange basis nodes, [E][nb][2], basis  */
+/* index dim 0 slowest (the points where a nodal initial state is       */
+/* sampled; tensor_product.hpp:101-126, lagrange_1d.hpp:31-53)          */
+/* ------------------------------------------------------------------ */
+int orc_basis_node_coords(const orc_problem* pb, const double* coord, double* xy) {
+  if (pb->basis != 0) return -1; /* a modal basis has no nodes */
+  lag1d lb, lg;
+  lag_init(&lb, pb->p);
+  lag_init(&lg, pb->geo_order);
+  int n = pb->p + 1, E = pb->nx * pb->ny;
+  elgeo G;
+  for (int e = 0; e < E; ++e) {
+    el_geo(pb, coord, e, &G);
+    for (int i0 = 0; i0 < n; ++i0)
+      for (int i1 = 0; i1 < n; ++i1) {
+        double xi[2] = {lb.xi[i0], lb.xi[i1]};
+        el_map(&lg, &G, xi, xy + 2 * ((size_t)e * n * n + i0 * n + i1), NULL, NULL);
+      }
+  }
+  return 0;
+}

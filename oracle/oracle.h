@@ -80,6 +80,18 @@ int orc_mdg_residual(const orc_problem* pb, const double* coord, int ntr, const 
 int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
                            const double* u, const double* x, double* res_and_ic, double* J);
 
+/* physical coordinates of the Lagrange basis nodes [E][nb][2] (basis index
+ * dim 0 slowest); -1 for a modal basis */
+int orc_basis_node_coords(const orc_problem* pb, const double* coord, double* xy);
+
+/* workload point callbacks (oracle/workloads.c; same meaning as the product's
+ * icx_wl_* exports, derived separately) */
+void orc_wl_constant(const double* x, double* out, void* user);
+void orc_wl_sine_product(const double* x, double* out, void* user);
+void orc_wl_oblique_step(const double* x, double* out, void* user);
+void orc_wl_ns_mms_state(const double* x, double* out, void* user);
+void orc_wl_ns_mms_source(const double* x, double* out, void* user);
+
 /* element mass matrices [E][nb][nb] (finite_element.hpp:587-610) */
 int orc_mass_matrices(const orc_problem* pb, const double* coord, double* M);
 /* explicit time stepping: scheme 0 Euler, 1 TVD-RK3, 2 SSP-RK3; dt_kind 0

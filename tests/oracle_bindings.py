@@ -101,6 +101,15 @@ def perturb_smooth(pb, coord, amp_frac, seed):
     return np.ascontiguousarray(out)
 
 
+def basis_node_coords(pb, coord):
+    """physical coordinates of the Lagrange basis nodes [E][nb][2] (oracle)"""
+    E, nb, N = sizes(pb)
+    xy = np.zeros((E, nb, 2))
+    rc = oracle().fn("basis_node_coords")(C.byref(pb), _ptr(np.ascontiguousarray(coord)), _ptr(xy))
+    assert rc == 0, rc
+    return xy
+
+
 def residual(lib, pb, coord, u):
     E, nb, N = sizes(pb)
     r = np.zeros(N)

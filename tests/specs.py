@@ -1,6 +1,11 @@
 """Problem specifications shared by the oracle side (orc_problem) and the GPU
 side (icx Context), so both evaluate exactly the same discretization on the
-same mesh coordinates and state. Test infrastructure only."""
+same mesh coordinates and state. Test infrastructure only.
+
+The oracle side takes everything from the oracle library: mesh coordinates
+(oracle_bindings), boundary data and sources (its own orc_wl_* callbacks)
+and basis-node coordinates. Nothing here loads the product library unless
+a GPU context is asked for (Spec.context)."""
 import ctypes as C
 
 import numpy as np
@@ -8,6 +13,13 @@ import numpy as np
 import oracle_bindings as ob
 
 BURGERS, NS = 0, 1
+
+
+def ns_mms_params(gamma=1.4, Pr=0.72, mu=0.01, mach=0.3, A=0.1, u0=1.0, v0=0.5):
+    """{gamma, Pr, mu, pinf, A, u0, v0} of the manufactured Navier-Stokes
+    solution, pinf = rho_inf |u_inf|^2 / (gamma M^2)"""
+    pinf = 1.0 * (u0 * u0 + v0 * v0) / (gamma * mach * mach)
+    return (C.c_double * 7)(gamma, Pr, mu, pinf, A, u0, v0)
 
 
 class Spec:
@@ -43,16 +55,24 @@ class Spec:
     def N(self):
         return self.E * self.nb * self.neq
 
+    def _geometry_problem(self):
+        pb = ob.Problem()
+        pb.nx, pb.ny, pb.geo_order, pb.p = self.nx, self.ny, self.g, self.p
+        pb.xmin[:] = [0.0, 0.0]
+        pb.xmax[:] = [1.0, 1.0]
+        return pb
+
     def coords(self):
-        from iceicle_b200.workloads import lattice_coords, perturb_smooth
-        c = lattice_coords((self.nx, self.ny), self.g)
+        """geometry nodes: the equispaced lattice plus the seeded smooth
+        perturbation (oracle-side copy of the workload definition)"""
+        pb = self._geometry_problem()
+        c = ob.lattice_coords(pb)
         if self.perturb:
-            c = perturb_smooth(c, (self.nx, self.ny), self.perturb, self.seed)
+            c = ob.perturb_smooth(pb, c, self.perturb, self.seed)
         return c
 
     def _params(self, name, prm):
         if name.startswith("ns_mms"):
-            from iceicle_b200.workloads import ns_mms_params
             arr = ns_mms_params()
         else:
             arr = (C.c_double * len(prm))(*prm)
@@ -60,10 +80,27 @@ class Spec:
         return arr
 
     def fn(self, name):
-        """C function pointer of an exported workload callback (from the product
-        library: it is input data, not the algorithm under test)"""
-        import iceicle_b200 as ib
-        return ib.workload_fn(name)
+        """C function pointer of the oracle's workload callback orc_wl_<name>"""
+        return C.cast(getattr(ob.oracle().lib, "orc_wl_" + name), ob.POINT_FN)
+
+    def mms_state(self, coords, seed=4321, noise=1e-3):
+        """the Navier-Stokes workload's initial state: the manufactured state at
+        the Lagrange basis nodes times (1 + noise N(0, 1)), seeded like the
+        product's workload builder"""
+        pb = self._geometry_problem()
+        xy = ob.basis_node_coords(pb, coords).reshape(-1, 2)
+        prm = ns_mms_params()
+        f = self.fn("ns_mms_state")
+        st = np.zeros((xy.shape[0], 4))
+        out = (C.c_double * 4)()
+        pt = (C.c_double * 2)()
+        for k in range(xy.shape[0]):
+            pt[0], pt[1] = xy[k, 0], xy[k, 1]
+            f(pt, out, C.cast(prm, C.c_void_p))
+            st[k] = out[:]
+        rng = np.random.default_rng(seed)
+        st *= 1.0 + noise * rng.standard_normal(st.shape)
+        return np.ascontiguousarray(st.reshape(-1))
 
     def state(self, rng):
         if self.pde == BURGERS:
@@ -103,6 +140,9 @@ class Spec:
         return pb
 
     def context(self, coords=None):
+        """the same problem as a GPU context; boundary data and sources are the
+        product's own exported callbacks (icx_wl_*), so the parity tests also
+        check them against the oracle's"""
         import iceicle_b200 as ib
         ctx = ib.Context(0)
         ctx.mesh_uniform((self.nx, self.ny), (0.0, 0.0), (1.0, 1.0), self.g, self.bct, self.bcf)
@@ -116,10 +156,10 @@ class Spec:
             ctx.disc_navier_stokes(1.4, 0.72, 0.01, ib.FLUX_VANLEER)
         ctx.disc_options(self.ip, self.sigma_ic)
         for i, (name, prm) in enumerate(self.dirichlet):
-            ctx.dirichlet(i, self.fn(name), C.cast(self._params(name, prm), C.c_void_p))
+            ctx.dirichlet(i, ib.workload_fn(name), C.cast(self._params(name, prm), C.c_void_p))
         for i, (name, prm) in enumerate(self.neumann):
-            ctx.neumann(i, self.fn(name), C.cast(self._params(name, prm), C.c_void_p))
+            ctx.neumann(i, ib.workload_fn(name), C.cast(self._params(name, prm), C.c_void_p))
         if self.source:
-            ctx.source(self.fn("ns_mms_source"), C.cast(self._params("ns_mms_source", None), C.c_void_p))
+            ctx.source(ib.workload_fn("ns_mms_source"), C.cast(self._params("ns_mms_source", None), C.c_void_p))
         ctx.setup()
         return ctx

@@ -29,3 +29,9 @@ def test_reference_arm_json_line():
     e = d["e2e"]
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    # the timed processes mapped no product library (their /proc/self/maps)
+    assert d["product_libs_mapped"] == []
+    # the same config object as the GPU arm's line
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == bench.WORKLOAD

@@ -86,13 +86,11 @@ def test_residual_repeatable_and_node_update():
 
 
 def test_full_size_ns_properties():
-    """NS manufactured-solution workload at benchmark size (128x128, p=3):
-    linearity of the face/volume split is not available for a nonlinear
-    residual, so check size-independent properties: finite, deterministic,
-    and matching the oracle on a sampled block of elements computed from a
-    small sub-mesh is not possible either; instead check that the residual of
-    the exact nodal state is small relative to that of a perturbed state
-    (consistency of the manufactured source)."""
+    """NS manufactured-solution workload at benchmark size (128x128, p=3),
+    properties beside the oracle comparison at this size
+    (test_gpu_config_parity.py): deterministic, and the residual of the exact
+    nodal state is small relative to that of a perturbed state (consistency
+    of the manufactured source)."""
     from iceicle_b200.workloads import ns_mms_config
     wl = ns_mms_config(state_noise=0.0)
     r_exact = _gpu_residual(wl.ctx, wl.u0)
