@@ -54,7 +54,7 @@ class NewtonOptions(C.Structure):
                 ("ls_alpha_max", C.c_double), ("ls_alpha_min", C.c_double), ("ls_c1", C.c_double),
                 ("ls_c2", C.c_double), ("gmres_restart", C.c_int), ("gmres_max_it", C.c_int),
                 ("gmres_rtol", C.c_double), ("preconditioner", C.c_int), ("verbosity", C.c_int),
-                ("precision", C.c_int), ("pc_sweeps", C.c_int), ("cuda_graphs", C.c_int)]
+                ("precision", C.c_int), ("pc_sweeps", C.c_int), ("cuda_graphs", C.c_int), ("ilu_tile", C.c_int)]
 
 
 class ExplicitOptions(C.Structure):
@@ -182,6 +182,10 @@ def lib():
             "icx_autotune": (C.c_int, [vp, vp, C.c_int, C.POINTER(TuneReport)]),
             "icx_tile_get": (C.c_int, [vp, C.POINTER(TileChoice)]),
             "icx_tile_set": (C.c_int, [vp, C.POINTER(TileChoice)]),
+            "icx_set_ilu_tile": (C.c_int, [vp, C.c_int]),
+            "icx_gemm_bf16_nt": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp,
+                                           C.c_int, vp, C.c_int, C.c_int, C.c_int, vp]),
+            "icx_get_ilu_tile": (C.c_int, [vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -339,6 +343,15 @@ class Context:
         self._check(lib().icx_ilu_apply(self._h, _ptr(vals), _ptr(x), _ptr(y), precision, schedule, repeat,
                                         C.byref(ms)), "ilu_apply")
         return ms.value
+
+    @property
+    def ilu_tile(self):
+        """side (in elements) of the tiles of the block-ILU(0) preconditioner; 0: the whole grid"""
+        return lib().icx_get_ilu_tile(self._h)
+
+    @ilu_tile.setter
+    def ilu_tile(self, tile):
+        self._check(lib().icx_set_ilu_tile(self._h, int(tile)), "set_ilu_tile")
 
     def autotune(self, u, parts=TUNE_RESIDUAL | TUNE_ILU | TUNE_ILU_FP32):
         """times every compiled launch shape of the selected kernels at the
@@ -570,6 +583,7 @@ class LearnedPreconditioner:
             raise IcxError(st, "icx_lpc_create")
         self.bs, self.hidden, self.device = bs, hidden, device
         self.sweeps = None
+        self.ilu_tile = None
 
     def close(self):
         if self._h:
@@ -609,10 +623,13 @@ class LearnedPreconditioner:
         if st != 0:
             raise IcxError(st, "icx_lpc_set_params")
 
-    def save(self, path, sweeps=None):
-        """parameters and shape (and the Jacobi sweeps the model was trained
-        with, the pc_sweeps to run it with) as a compressed .npz"""
+    def save(self, path, sweeps=None, ilu_tile=None):
+        """parameters and shape (and the base preconditioner the model was
+        trained on: Jacobi sweeps, i.e. the pc_sweeps to run it with, and the
+        ILU tile side) as a compressed .npz"""
         extra = {} if sweeps is None else {"sweeps": sweeps}
+        if ilu_tile is not None:
+            extra["ilu_tile"] = ilu_tile
         np.savez_compressed(path, bs=self.bs, hidden=self.hidden, params=self.get_params(), **extra)
 
     @classmethod
@@ -621,6 +638,7 @@ class LearnedPreconditioner:
         m = cls(int(z["bs"]), int(z["hidden"]), device)
         m.set_params(z["params"])
         m.sweeps = int(z["sweeps"]) if "sweeps" in z.files else None
+        m.ilu_tile = int(z["ilu_tile"]) if "ilu_tile" in z.files else None
         return m
 
 
@@ -652,6 +670,20 @@ def default_explicit_options(**kw):
     for k, v in kw.items():
         setattr(opt, k, v)
     return opt
+
+
+def gemm_bf16_nt(A, B, bias=None, relu=False, out32=None, out16=None, accumulate=False, splits=1):
+    """out = A . B^T (+ bias, ReLU) on the tensor cores; A [M, K] and B [N, K]
+    BF16 CUDA tensors, out32 FP32 and/or out16 BF16 [M, N] (accumulate: out32 +=)"""
+    M, K = A.shape
+    N = B.shape[0]
+    st = lib().icx_gemm_bf16_nt(M, N, K, _ptr(A), A.stride(0), _ptr(B), B.stride(0),
+                                _ptr(bias) if bias is not None else None, int(relu),
+                                _ptr(out32) if out32 is not None else None, out32.stride(0) if out32 is not None else 0,
+                                _ptr(out16) if out16 is not None else None, out16.stride(0) if out16 is not None else 0,
+                                int(accumulate), int(splits), None)
+    if st != 0:
+        raise IcxError(st, "gemm_bf16_nt")
 
 
 def workload_fn(name):

@@ -55,6 +55,9 @@ icx_status icx_batch_create(icx_ctx** out, int device, int n_parts, icx_ctx* con
     c->coord.insert(c->coord.end(), q->coord.begin(), q->coord.end());
     for (int v : q->el_nodes) c->el_nodes.push_back(v + node_off[k]);
     c->el_level.insert(c->el_level.end(), q->el_level.begin(), q->el_level.end());
+    c->el_i.insert(c->el_i.end(), q->el_i.begin(), q->el_i.end());
+    c->el_j.insert(c->el_j.end(), q->el_j.begin(), q->el_j.end());
+    c->el_grid.insert(c->el_grid.end(), q->n_elem, k);
     if (q->phys.pde == ICX_PDE_BURGERS)
       for (int e = 0; e < q->n_elem; ++e) {
         const double v[5] = {q->phys.mu, q->phys.a[0], q->phys.a[1], q->phys.b[0], q->phys.b[1]};

@@ -518,7 +518,14 @@ icx_status icx_mesh_uniform(icx_ctx* c, int ndim, const int* nelem, const double
   }
   c->n_elem = c->nx * c->ny;
   c->el_level.resize(c->n_elem);
-  for (int e = 0; e < c->n_elem; ++e) c->el_level[e] = e % c->nx + e / c->nx;
+  c->el_i.resize(c->n_elem);
+  c->el_j.resize(c->n_elem);
+  c->el_grid.assign(c->n_elem, 0);
+  for (int e = 0; e < c->n_elem; ++e) {
+    c->el_i[e] = e % c->nx;
+    c->el_j[e] = e / c->nx;
+    c->el_level[e] = c->el_i[e] + c->el_j[e];
+  }
   c->has_mesh = true;
   c->ready = false;
   return ICX_OK;

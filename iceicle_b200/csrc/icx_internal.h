@@ -130,6 +130,8 @@ struct icx_ctx {
   int n_interior = 0;
   int n_elem = 0;                             // elements (nx * ny for one grid)
   std::vector<int> el_level;                  // [E] anti-diagonal index i + j of the element in its grid
+  std::vector<int> el_i, el_j, el_grid;       // [E] grid position (i, j) of the element and its grid's index
+  int ilu_tile = 0;                           // block-ILU(0) on s x s element tiles (0: the whole grid)
   // a batch of independent problems (icx_batch_create): the parts it was
   // built from (not owned) and each element's Burgers coefficients (mu, a0, a1, b0, b1)
   std::vector<icx_ctx*> parts;

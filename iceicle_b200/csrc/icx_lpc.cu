@@ -1,19 +1,27 @@
 // Learned block preconditioner (preconditioner 5 of the Newton solver).
 //
 // The preconditioner is the block-ILU(0) factorisation of the Jacobian J
-// applied with Jacobi sweeps (each sweep of a triangular solve is one
-// message-passing step over the face neighbours), followed by a learned
+// (exact triangular solves, or Jacobi sweeps), followed by a learned
 // correction of every element block:
 //
-//   z = (I + C) y,  y = ILU_s(r),  C = blockdiag(C_e),  C_e = MLP(J_ee / |J_ee|_F)
+//   z = (I + C) y,  y = ILU(r),  C = blockdiag(C_e)
 //
-// The MLP maps the normalised diagonal block (bs x bs values, BF16) through two
-// hidden ReLU layers to a bs x bs correction (FP32 output). Its weights are
-// trained on the Jacobians and Krylov residuals r of the plain solver to
-// minimise the mean over residual samples of |r - J z(r)|^2 / |r|^2; the
-// output layer starts at zero, so the untrained model is ILU_s itself. All MLP
-// products run on the tensor cores in BF16 with FP32 accumulation (forward and
-// backward passes, Adam on FP32 master weights). The Newton residual, its norm
+// C_e comes from a graph network over the elements with one message-passing
+// step over the face neighbours:
+//
+//   h1_e = relu(W1 x_e + b1),           x_e = J_ee / |J_ee|_F   (bs x bs values)
+//   m_e  = mean over the face neighbours n of e of h1_n         (the message)
+//   h2_e = relu(W2 [h1_e ; m_e] + b2)
+//   C_e  = W3 h2_e + b3                                          (bs x bs values)
+//
+// The neighbours are the off-diagonal blocks of the element's block row of
+// the BSR pattern. Its weights are trained on the Jacobians and Krylov
+// residuals r of the plain solver to minimise the mean over residual samples
+// of |r - J z(r)|^2 / |r|^2; the output layer starts at zero, so the
+// untrained model is the ILU preconditioner itself. All MLP products run on
+// the tensor cores (tcgen05.mma, BF16 operands, FP32 accumulation in tensor
+// memory, TMA operand loads; icx_gemm_tc.cuh) in the forward and backward
+// passes, with Adam on FP32 master weights. The Newton residual, its norm
 // and the line search stay FP64, so the preconditioner changes iteration
 // counts but not the converged state; the solver falls back to block-ILU(0)
 // for any step whose linear solve misses its tolerance.
@@ -26,6 +34,7 @@
 
 #include "icx_internal.h"
 #include "icx_linalg.h"
+#include "icx_gemm_tc.cuh"
 #include "icx_mlp.cuh"
 
 using icx::bf16;
@@ -34,14 +43,14 @@ struct icx_lpc {
   int device = 0, bs = 0, hidden = 0, D = 0;
   size_t np = 0;
   size_t oW1 = 0, ob1 = 0, oW2 = 0, ob2 = 0, oW3 = 0, ob3 = 0;
-  float* p = nullptr;     // FP32 master parameters: W1 [H][D], b1, W2 [H][H], b2, W3 [D][H], b3
+  float* p = nullptr;     // FP32 master parameters: W1 [H][D], b1, W2 [H][2H], b2, W3 [D][H], b3
   float* grad = nullptr;
   float* m = nullptr;     // Adam moments
   float* v = nullptr;
   bf16* W1b = nullptr;    // BF16 copies for the products
   bf16* W2b = nullptr;
   bf16* W3b = nullptr;
-  bf16* W2tb = nullptr;   // transposes for the backward pass
+  bf16* W2tb = nullptr;   // transposes for the backward pass (W2^T: [2H][H])
   bf16* W3tb = nullptr;
   long long steps = 0;
 };
@@ -51,11 +60,12 @@ struct icx_lpc_work {
   int E = 0, D = 0, H = 0, B = 0;
   int Ep = 0;  // E rounded up to a multiple of 8: the row length of the transposed activations (zero padded)
   long long n = 0;
-  bf16 *X = nullptr, *H1 = nullptr, *H2 = nullptr;  // forward activations
-  float* C = nullptr;                               // [E][bs][bs] correction
+  bf16 *X = nullptr, *H2 = nullptr;  // forward activations: X [E][D], H2 [E][H]
+  bf16* H1 = nullptr;                // [E][2H]: h1 in columns 0..H-1, the neighbour mean m in H..2H-1
+  float* C = nullptr;                // [E][bs][bs] correction
   // training only
-  float *dC = nullptr, *dH = nullptr;
-  bf16 *dCb = nullptr, *dCbT = nullptr, *XT = nullptr, *H1T = nullptr, *H2T = nullptr;
+  float *dC = nullptr, *dH = nullptr, *dH1 = nullptr;  // dH [E][2H] (also [E][H]), dH1 [E][H]
+  bf16 *dCb = nullptr, *dCbT = nullptr, *XT = nullptr, *H1T = nullptr, *H2T = nullptr;  // H1T [2H][Ep]
   bf16 *dHb = nullptr, *dHT = nullptr;
   int* tpos = nullptr;      // position of the mirrored block (k, e) of each block (e, k)
   double *ys = nullptr, *as = nullptr, *t1 = nullptr, *t2 = nullptr, *rv = nullptr;
@@ -71,20 +81,10 @@ int grid_for(long long n, int threads = 256) {
   return (int)(b < 148 * 64 ? (b < 1 ? 1 : b) : 148 * 64);
 }
 
+// C = A . B^T on the tensor cores (tcgen05, icx_gemm_tc.cuh)
 cudaError_t gemm(int M, int N, int K, const bf16* A, int lda, const bf16* B, int ldb, const float* bias, bool relu,
                  float* C32, int ldc, bf16* C16, int ldc16, bool accumulate, int splits, cudaStream_t s) {
-  if (M <= 0 || N <= 0 || K <= 0) return cudaSuccess;
-  if (K % 8 || lda % 8 || ldb % 8 || ((uintptr_t)A & 15) || ((uintptr_t)B & 15)) return cudaErrorInvalidValue;
-  if (accumulate && (bias || relu || C16 || !C32)) return cudaErrorInvalidValue;
-  if (splits < 1) splits = 1;
-  int ks = (K + splits - 1) / splits;
-  ks = (ks + GEMM_BK - 1) / GEMM_BK * GEMM_BK;
-  const int nz = (K + ks - 1) / ks;
-  if (nz > 1 && !accumulate) return cudaErrorInvalidValue;
-  GemmArgs g{M, N, K, A, lda, B, ldb, bias, relu ? 1 : 0, C32, ldc, C16, ldc16, accumulate ? 1 : 0, ks};
-  dim3 grid((N + GEMM_BN - 1) / GEMM_BN, (M + GEMM_BM - 1) / GEMM_BM, nz);
-  gemm_bf16_nt_kernel<<<grid, 256, 0, s>>>(g);
-  return cudaGetLastError();
+  return icx::gemm_tc(M, N, K, A, lda, B, ldb, bias, relu, C32, ldc, C16, ldc16, accumulate, splits, s);
 }
 
 // out (cols x ldo, ldo >= rows) = in^T; columns rows..ldo-1 of out are left as they are
@@ -112,6 +112,51 @@ __global__ void features_kernel(int E, int bs, const double* __restrict__ vals, 
   }
   const double inv = red[0] > 0.0 ? 1.0 / sqrt(red[0]) : 0.0;
   for (int i = threadIdx.x; i < D; i += blockDim.x) X[(size_t)e * D + i] = __float2bfloat16_rn((float)(b[i] * inv));
+}
+
+// the message: H1[e][H + j] = mean over the face neighbours n of e of
+// H1[n][j] (zero for an element without neighbours), FP32 sums of the BF16
+// features in the pattern's column order
+__global__ void message_mean_kernel(int E, int H, const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                    bf16* __restrict__ H1) {
+  const int e = blockIdx.x;
+  if (e >= E) return;
+  const int rb = rowptr[e], re = rowptr[e + 1];
+  int deg = 0;
+  for (int kb = rb; kb < re; ++kb) deg += colidx[kb] != e;
+  const float inv = deg > 0 ? 1.f / (float)deg : 0.f;
+  for (int j = threadIdx.x; j < H; j += blockDim.x) {
+    float s = 0.f;
+    for (int kb = rb; kb < re; ++kb) {
+      const int n = colidx[kb];
+      if (n != e) s += __bfloat162float(H1[(size_t)n * 2 * H + j]);
+    }
+    H1[(size_t)e * 2 * H + H + j] = __float2bfloat16_rn(s * inv);
+  }
+}
+
+// backward of the message and of the first ReLU: with dcat = dLoss/d[h1 ; m]
+// ([E][2H]), dh1_e = dcat_e[0..H) + sum over the neighbours n of e of
+// dcat_n[H..2H) / deg(n) (the pattern is symmetric, so n's message reads e),
+// then masked by h1_e > 0; FP32 and BF16 copies
+__global__ void message_back_kernel(int E, int H, const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                    const float* __restrict__ dcat, const bf16* __restrict__ H1,
+                                    float* __restrict__ dH1, bf16* __restrict__ dH1b) {
+  const int e = blockIdx.x;
+  if (e >= E) return;
+  for (int j = threadIdx.x; j < H; j += blockDim.x) {
+    float s = dcat[(size_t)e * 2 * H + j];
+    for (int kb = rowptr[e]; kb < rowptr[e + 1]; ++kb) {
+      const int n = colidx[kb];
+      if (n == e) continue;
+      int deg = 0;
+      for (int t = rowptr[n]; t < rowptr[n + 1]; ++t) deg += colidx[t] != n;
+      s += dcat[(size_t)n * 2 * H + H + j] / (float)deg;
+    }
+    const float x = __bfloat162float(H1[(size_t)e * 2 * H + j]) > 0.f ? s : 0.f;
+    dH1[(size_t)e * H + j] = x;
+    dH1b[(size_t)e * H + j] = __float2bfloat16_rn(x);
+  }
 }
 
 // out_e = sum over the blocks (e, k) of J_ke^T a_k (the mirrored block (k, e)
@@ -215,7 +260,7 @@ __global__ void adam_kernel(long long n, float* __restrict__ p, const float* __r
 cudaError_t refresh_bf16(icx_lpc* L, cudaStream_t s) {
   const int H = L->hidden, D = L->D;
   weights_bf16_kernel<<<grid_for((long long)H * D), 256, 0, s>>>(H, D, L->p + L->oW1, L->W1b, nullptr);
-  weights_bf16_kernel<<<grid_for((long long)H * H), 256, 0, s>>>(H, H, L->p + L->oW2, L->W2b, L->W2tb);
+  weights_bf16_kernel<<<grid_for((long long)H * 2 * H), 256, 0, s>>>(H, 2 * H, L->p + L->oW2, L->W2b, L->W2tb);
   weights_bf16_kernel<<<grid_for((long long)D * H), 256, 0, s>>>(D, H, L->p + L->oW3, L->W3b, L->W3tb);
   return cudaGetLastError();
 }
@@ -244,7 +289,7 @@ cudaError_t ensure_infer(icx_ctx* c, const icx_lpc* L) {
   w->H = L->hidden;
   w->n = (long long)E * L->bs;
   cudaError_t e = grow(w->X, (size_t)E * L->D);
-  if (e == cudaSuccess) e = grow(w->H1, (size_t)E * L->hidden);
+  if (e == cudaSuccess) e = grow(w->H1, (size_t)E * 2 * L->hidden);
   if (e == cudaSuccess) e = grow(w->H2, (size_t)E * L->hidden);
   if (e == cudaSuccess) e = grow(w->C, (size_t)E * L->D);
   return e;
@@ -261,14 +306,15 @@ cudaError_t ensure_train(icx_ctx* c, const icx_lpc* L, int B) {
   if (e == cudaSuccess) e = grow(w->dCb, E * D);
   if (e == cudaSuccess) e = grow(w->dCbT, Ep * D);
   if (e == cudaSuccess) e = grow(w->XT, Ep * D);
-  if (e == cudaSuccess) e = grow(w->H1T, Ep * H);
+  if (e == cudaSuccess) e = grow(w->H1T, Ep * 2 * H);
   if (e == cudaSuccess) e = grow(w->H2T, Ep * H);
-  if (e == cudaSuccess) e = grow(w->dH, E * H);
+  if (e == cudaSuccess) e = grow(w->dH, E * 2 * H);
+  if (e == cudaSuccess) e = grow(w->dH1, E * H);
   if (e == cudaSuccess) e = grow(w->dHb, E * H);
   if (e == cudaSuccess) e = grow(w->dHT, Ep * H);
   // the padding columns of the transposes stay zero
   bf16* zp[] = {w->dCbT, w->XT, w->H1T, w->H2T, w->dHT};
-  size_t zn[] = {Ep * D, Ep * D, Ep * H, Ep * H, Ep * H};
+  size_t zn[] = {Ep * D, Ep * D, Ep * 2 * H, Ep * H, Ep * H};
   for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaMemset(zp[i], 0, sizeof(bf16) * zn[i]);
   if (e == cudaSuccess) e = grow(w->ys, (size_t)B * w->n);
   if (e == cudaSuccess) e = grow(w->as, (size_t)B * w->n);
@@ -295,17 +341,20 @@ cudaError_t ensure_train(icx_ctx* c, const icx_lpc* L, int B) {
   return e;
 }
 
-// H1 = relu(X W1^T + b1), H2 = relu(H1 W2^T + b2), C = H2 W3^T + b3
-cudaError_t mlp_forward(const icx_lpc* L, icx_lpc_work* w, cudaStream_t s) {
+// H1[:, :H] = relu(X W1^T + b1), H1[:, H:] = neighbour mean of H1[:, :H],
+// H2 = relu(H1 W2^T + b2), C = H2 W3^T + b3; rowptr / colidx: the BSR pattern
+cudaError_t mlp_forward(const icx_lpc* L, icx_lpc_work* w, const int* rowptr, const int* colidx, cudaStream_t s) {
   const int E = w->E, D = L->D, H = L->hidden;
-  cudaError_t e = gemm(E, H, D, w->X, D, L->W1b, D, L->p + L->ob1, true, nullptr, 0, w->H1, H, false, 1, s);
-  if (e == cudaSuccess) e = gemm(E, H, H, w->H1, H, L->W2b, H, L->p + L->ob2, true, nullptr, 0, w->H2, H, false, 1, s);
+  cudaError_t e = gemm(E, H, D, w->X, D, L->W1b, D, L->p + L->ob1, true, nullptr, 0, w->H1, 2 * H, false, 1, s);
+  if (e != cudaSuccess) return e;
+  message_mean_kernel<<<E, 128, 0, s>>>(E, H, rowptr, colidx, w->H1);
+  e = gemm(E, H, 2 * H, w->H1, 2 * H, L->W2b, 2 * H, L->p + L->ob2, true, nullptr, 0, w->H2, H, false, 1, s);
   if (e == cudaSuccess) e = gemm(E, D, H, w->H2, H, L->W3b, H, L->p + L->ob3, false, w->C, D, nullptr, 0, false, 1, s);
   return e;
 }
 
 // gradients of the parameters (into L->grad, which the caller zeroed) from dC = dLoss/dC
-cudaError_t mlp_backward(icx_lpc* L, icx_lpc_work* w, cudaStream_t s) {
+cudaError_t mlp_backward(icx_lpc* L, icx_lpc_work* w, const int* rowptr, const int* colidx, cudaStream_t s) {
   const int E = w->E, D = L->D, H = L->hidden, Ep = w->Ep;
   const int split = 32;
   const long long ED = (long long)E * D, EH = (long long)E * H;
@@ -313,25 +362,28 @@ cudaError_t mlp_backward(icx_lpc* L, icx_lpc_work* w, cudaStream_t s) {
   to_bf16_kernel<<<grid_for(ED), 256, 0, s>>>(ED, w->dC, w->dCb);
   if ((e = transpose(E, D, w->dCb, w->dCbT, Ep, s)) != cudaSuccess) return e;
   if ((e = transpose(E, H, w->H2, w->H2T, Ep, s)) != cudaSuccess) return e;
-  if ((e = transpose(E, H, w->H1, w->H1T, Ep, s)) != cudaSuccess) return e;
+  if ((e = transpose(E, 2 * H, w->H1, w->H1T, Ep, s)) != cudaSuccess) return e;
   // layer 3
   if ((e = gemm(D, H, Ep, w->dCbT, Ep, w->H2T, Ep, nullptr, false, L->grad + L->oW3, H, nullptr, 0, true, split, s)))
     return e;
   colsum_kernel<<<dim3((D + 255) / 256, 64), 256, 0, s>>>(E, D, w->dC, L->grad + L->ob3);
   if ((e = gemm(E, H, D, w->dCb, D, L->W3tb, D, nullptr, false, w->dH, H, nullptr, 0, false, 1, s))) return e;
   relu_back_kernel<<<grid_for(EH), 256, 0, s>>>(EH, w->dH, w->H2, w->dHb);
-  // layer 2
+  // layer 2, over [h1 ; m]
   if ((e = transpose(E, H, w->dHb, w->dHT, Ep, s)) != cudaSuccess) return e;
-  if ((e = gemm(H, H, Ep, w->dHT, Ep, w->H1T, Ep, nullptr, false, L->grad + L->oW2, H, nullptr, 0, true, split, s)))
+  if ((e = gemm(H, 2 * H, Ep, w->dHT, Ep, w->H1T, Ep, nullptr, false, L->grad + L->oW2, 2 * H, nullptr, 0, true,
+                split, s)))
     return e;
   colsum_kernel<<<dim3((H + 255) / 256, 64), 256, 0, s>>>(E, H, w->dH, L->grad + L->ob2);
-  if ((e = gemm(E, H, H, w->dHb, H, L->W2tb, H, nullptr, false, w->dH, H, nullptr, 0, false, 1, s))) return e;
-  relu_back_kernel<<<grid_for(EH), 256, 0, s>>>(EH, w->dH, w->H1, w->dHb);
+  if ((e = gemm(E, 2 * H, H, w->dHb, H, L->W2tb, H, nullptr, false, w->dH, 2 * H, nullptr, 0, false, 1, s))) return e;
+  // the message step and the first ReLU
+  message_back_kernel<<<E, 128, 0, s>>>(E, H, rowptr, colidx, w->dH, w->H1, w->dH1, w->dHb);
   // layer 1
   if ((e = transpose(E, H, w->dHb, w->dHT, Ep, s)) != cudaSuccess) return e;
   if ((e = gemm(H, D, Ep, w->dHT, Ep, w->XT, Ep, nullptr, false, L->grad + L->oW1, D, nullptr, 0, true, split, s)))
     return e;
-  colsum_kernel<<<dim3((H + 255) / 256, 64), 256, 0, s>>>(E, H, w->dH, L->grad + L->ob1);
+  colsum_kernel<<<dim3((H + 255) / 256, 64), 256, 0, s>>>(E, H, w->dH1, L->grad + L->ob1);
+  (void)EH;
   return cudaGetLastError();
 }
 
@@ -342,7 +394,7 @@ namespace icx {
 void free_lpc_work(icx_ctx* c) {
   icx_lpc_work* w = c->lpcw;
   if (!w) return;
-  void* ptrs[] = {w->X,  w->H1,  w->H2,  w->C,   w->dC,   w->dH, w->dCb, w->dCbT, w->XT, w->H1T,
+  void* ptrs[] = {w->X,  w->H1,  w->H2,  w->C,   w->dC,   w->dH, w->dH1, w->dCb, w->dCbT, w->XT, w->H1T,
                   w->H2T, w->dHb, w->dHT, w->tpos, w->ys, w->as, w->t1,  w->t2,   w->rv, w->dh};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -357,7 +409,12 @@ cudaError_t lpc_build(icx_ctx* c, const double* vals, cudaStream_t s) {
   cudaError_t e = ensure_infer(c, L);
   if (e != cudaSuccess) return e;
   features_kernel<<<c->dm.E, 256, 0, s>>>(c->dm.E, L->bs, vals, c->dm.bsr_diag, c->lpcw->X);
-  return mlp_forward(L, c->lpcw, s);
+  e = mlp_forward(L, c->lpcw, c->dm.bsr_rowptr, c->dm.bsr_colidx, s);
+  if (e != cudaSuccess) return e;
+  // a tensor-core tile that gave up on a wait leaves C incomplete: report it
+  int flag = 0;
+  e = icx::gemm_tc_status(&flag, s);
+  return e != cudaSuccess ? e : (flag ? cudaErrorLaunchTimeout : cudaSuccess);
 }
 
 // z = (I + C) y
@@ -384,7 +441,7 @@ icx_status icx_lpc_create(icx_lpc** out, int device, int block_size, int hidden,
   L->oW1 = 0;
   L->ob1 = L->oW1 + H * D;
   L->oW2 = L->ob1 + H;
-  L->ob2 = L->oW2 + H * H;
+  L->ob2 = L->oW2 + H * 2 * H;
   L->oW3 = L->ob2 + H;
   L->ob3 = L->oW3 + D * H;
   L->np = L->ob3 + D;
@@ -392,17 +449,17 @@ icx_status icx_lpc_create(icx_lpc** out, int device, int block_size, int hidden,
   std::vector<float> h(L->np, 0.f);
   std::mt19937_64 rng(seed);
   std::uniform_real_distribution<float> u(-1.f, 1.f);
-  const float a1 = std::sqrt(6.f / (float)D), a2 = std::sqrt(6.f / (float)H);
+  const float a1 = std::sqrt(6.f / (float)D), a2 = std::sqrt(6.f / (float)(2 * H));
   for (size_t i = 0; i < H * D; ++i) h[L->oW1 + i] = a1 * u(rng);
-  for (size_t i = 0; i < H * H; ++i) h[L->oW2 + i] = a2 * u(rng);
+  for (size_t i = 0; i < H * 2 * H; ++i) h[L->oW2 + i] = a2 * u(rng);
   cudaError_t e = cudaSuccess;
   float** fp[] = {&L->p, &L->grad, &L->m, &L->v};
   for (float** q : fp)
     if (e == cudaSuccess) e = cudaMalloc((void**)q, sizeof(float) * L->np);
   if (e == cudaSuccess) e = cudaMalloc((void**)&L->W1b, sizeof(bf16) * H * D);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&L->W2b, sizeof(bf16) * H * H);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&L->W2b, sizeof(bf16) * H * 2 * H);
   if (e == cudaSuccess) e = cudaMalloc((void**)&L->W3b, sizeof(bf16) * D * H);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&L->W2tb, sizeof(bf16) * H * H);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&L->W2tb, sizeof(bf16) * H * 2 * H);
   if (e == cudaSuccess) e = cudaMalloc((void**)&L->W3tb, sizeof(bf16) * D * H);
   if (e == cudaSuccess) e = cudaMemcpy(L->p, h.data(), sizeof(float) * L->np, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(L->m, 0, sizeof(float) * L->np);
@@ -494,7 +551,7 @@ icx_status icx_lpc_train(icx_ctx* c, const double* d_vals, int n_samples, const 
   std::vector<double> hnorm(2 * o->batch);
   double first = 0.0, last = 0.0;
   for (int it = 0; it < o->steps; ++it) {
-    if ((e = mlp_forward(L, w, s)) != cudaSuccess) break;
+    if ((e = mlp_forward(L, w, dm.bsr_rowptr, dm.bsr_colidx, s)) != cudaSuccess) break;
     // residual after the preconditioner, for each sample b: g = r - J (I + C) ILU_s(r)
     double loss = 0.0;
     for (int b = 0; b < o->batch && e == cudaSuccess; ++b) {
@@ -527,7 +584,7 @@ icx_status icx_lpc_train(icx_ctx* c, const double* d_vals, int n_samples, const 
     outer_kernel<<<grid_for((long long)dm.E * L->D), 256, 0, s>>>(dm.E, L->bs, o->batch, n, w->as, w->ys,
                                                                   1.0 / o->batch, w->dC);
     if ((e = cudaMemsetAsync(L->grad, 0, sizeof(float) * L->np, s)) != cudaSuccess) break;
-    if ((e = mlp_backward(L, w, s)) != cudaSuccess) break;
+    if ((e = mlp_backward(L, w, dm.bsr_rowptr, dm.bsr_colidx, s)) != cudaSuccess) break;
     ++L->steps;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - std::pow(b1, (float)L->steps), c2 = 1.f - std::pow(b2, (float)L->steps);
@@ -536,6 +593,11 @@ icx_status icx_lpc_train(icx_ctx* c, const double* d_vals, int n_samples, const 
     if ((e = refresh_bf16(L, s)) != cudaSuccess) break;
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) {
+    int flag = 0;
+    e = icx::gemm_tc_status(&flag, s);
+    if (e == cudaSuccess && flag) e = cudaErrorLaunchTimeout;
+  }
   if (e != cudaSuccess) return fail(c, ICX_ERR_CUDA, std::string("train: ") + cudaGetErrorString(e));
   if (rep) {
     rep->steps = o->steps;

@@ -18,6 +18,26 @@
 #include "icx_internal.h"
 #include "icx_linalg.h"
 
+// block-ILU(0) on s x s element tiles (icx_ctx::ilu_tile = s > 0): the
+// preconditioner keeps only the blocks that couple two elements of the same
+// tile, i.e. block-Jacobi over the tiles with ILU(0) inside each (the form of
+// PETSc's parallel default, bjacobi with ilu sub-solves, with one block per
+// tile). On a quadrilateral grid no ILU(0) update couples two face
+// neighbours, so dropping the cross-tile blocks leaves every in-tile factor
+// block exactly what ILU(0) of the tile's own matrix gives. The dependent
+// levels of the factorisation and of each triangular sweep fall from
+// nx + ny - 1 to 2s - 1.
+struct IluTilePlan {
+  int tile = 0;                 // 0: no plan (natural order over the whole grid)
+  int nnzb = 0;                 // blocks kept
+  int* rowptr = nullptr;        // [E + 1] kept pattern, columns ascending
+  int* colidx = nullptr;        // [nnzb]
+  int* diag = nullptr;          // [E] position of the diagonal block
+  int* map = nullptr;           // [nnzb] kept block -> block of the full pattern
+  int* order = nullptr;         // [E] elements by ascending in-tile level (i mod s) + (j mod s)
+  std::vector<int> lvl_off;
+};
+
 struct icx_solver_work {
   long long n = 0;
   int nnzb = 0, bs = 0, m = 0;
@@ -56,6 +76,7 @@ struct icx_solver_work {
   int schedule = 0;         // 0 / 1: data flow (the solvers' apply), 2: rows (icx_ilu_apply only)
   unsigned* cnt_rows = nullptr;
   unsigned epoch_rows = 0;
+  IluTilePlan tp;           // tiled block-ILU(0) pattern and schedule (tp.tile == c->ilu_tile once built)
   int* pc_err = nullptr;    // set by the ILU apply if a dependency wait timed out
   double* dh = nullptr;     // device scalars (dot results)
   int* flag = nullptr;
@@ -146,6 +167,89 @@ icx_status ensure_work(icx_ctx* c, int m) {
   return ICX_OK;
 }
 
+void free_tile_plan(IluTilePlan& tp) {
+  for (int* p : {tp.rowptr, tp.colidx, tp.diag, tp.map, tp.order})
+    if (p) cudaFree(p);
+  tp = IluTilePlan();
+}
+
+// builds the tiled pattern for c->ilu_tile (nothing to do when it is built or 0)
+icx_status ensure_ilu_plan(icx_ctx* c) {
+  icx_solver_work* w = c->sw;
+  const int st = c->ilu_tile;
+  if (st == w->tp.tile) return ICX_OK;
+  free_tile_plan(w->tp);
+  if (st == 0) return ICX_OK;
+  const icx::DeviceMesh& dm = c->dm;
+  if ((int)c->el_i.size() != dm.E || (int)c->el_j.size() != dm.E || (int)c->el_grid.size() != dm.E)
+    return set_err(c, ICX_ERR_UNSUPPORTED, "tiled block-ILU(0) needs the elements' grid positions");
+  std::vector<int> rp(dm.E + 1), ci(dm.nnzb);
+  CK(cudaMemcpy(rp.data(), dm.bsr_rowptr, sizeof(int) * rp.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ci.data(), dm.bsr_colidx, sizeof(int) * ci.size(), cudaMemcpyDeviceToHost));
+  auto tile_of = [&](int e) -> long long {
+    return ((long long)c->el_grid[e] << 42) | ((long long)(c->el_i[e] / st) << 21) | (long long)(c->el_j[e] / st);
+  };
+  std::vector<int> trp(dm.E + 1, 0), tci, tdiag(dm.E, -1), tmap;
+  tci.reserve(dm.nnzb);
+  tmap.reserve(dm.nnzb);
+  for (int e = 0; e < dm.E; ++e) {
+    const long long te = tile_of(e);
+    for (int kb = rp[e]; kb < rp[e + 1]; ++kb) {
+      const int k = ci[kb];
+      if (k < 0 || k >= dm.E) return set_err(c, ICX_ERR_INVALID, "block pattern column out of range");
+      if (tile_of(k) != te) continue;
+      if (k == e) tdiag[e] = (int)tci.size();
+      tci.push_back(k);
+      tmap.push_back(kb);
+    }
+    trp[e + 1] = (int)tci.size();
+    if (tdiag[e] < 0) return set_err(c, ICX_ERR_INVALID, "block pattern without a diagonal block");
+  }
+  int nl = 0;
+  std::vector<int> lvl(dm.E);
+  for (int e = 0; e < dm.E; ++e) {
+    lvl[e] = c->el_i[e] % st + c->el_j[e] % st;
+    nl = std::max(nl, lvl[e] + 1);
+  }
+  IluTilePlan tp;
+  tp.lvl_off.assign(nl + 1, 0);
+  for (int v : lvl) ++tp.lvl_off[v + 1];
+  for (int l = 0; l < nl; ++l) tp.lvl_off[l + 1] += tp.lvl_off[l];
+  std::vector<int> order(dm.E), fill(tp.lvl_off.begin(), tp.lvl_off.end() - 1);
+  for (int e = 0; e < dm.E; ++e) order[fill[lvl[e]]++] = e;
+  tp.nnzb = (int)tci.size();
+  const std::pair<int**, const std::vector<int>*> up[] = {
+      {&tp.rowptr, &trp}, {&tp.colidx, &tci}, {&tp.diag, &tdiag}, {&tp.map, &tmap}, {&tp.order, &order}};
+  for (const auto& u : up) {
+    cudaError_t e = cudaMalloc((void**)u.first, sizeof(int) * u.second->size());
+    if (e == cudaSuccess) e = cudaMemcpy(*u.first, u.second->data(), sizeof(int) * u.second->size(),
+                                         cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      free_tile_plan(tp);
+      return set_err(c, ICX_ERR_CUDA, std::string("tiled ILU plan: ") + cudaGetErrorString(e));
+    }
+  }
+  tp.tile = st;
+  w->tp = std::move(tp);
+  return ICX_OK;
+}
+
+// the mesh view the block-ILU(0) factors live on: the full pattern, or the
+// tiled one when a tile plan is built
+icx::DeviceMesh ilu_mesh(const icx_ctx* c) {
+  icx::DeviceMesh v = c->dm;
+  const IluTilePlan& tp = c->sw->tp;
+  if (tp.tile) {
+    v.bsr_rowptr = tp.rowptr;
+    v.bsr_colidx = tp.colidx;
+    v.bsr_diag = tp.diag;
+    v.nnzb = tp.nnzb;
+  }
+  return v;
+}
+
+const int* ilu_order(const icx_ctx* c) { return c->sw->tp.tile ? c->sw->tp.order : c->sw->order; }
+
 // NaN when a launch, copy or earlier kernel failed (the CUDA message is kept in c->err)
 double dev_norm(icx_ctx* c, const double* x, cudaStream_t s) {
   icx_solver_work* w = c->sw;
@@ -180,8 +284,9 @@ cudaError_t diag_apply(icx_ctx* c, bool mixed, const double* D, const float* D32
 cudaError_t tri_rows(icx_ctx* c, bool mixed, bool lower, const double* v, const double* x0, double* y,
                      cudaStream_t s) {
   icx_solver_work* w = c->sw;
-  return mixed ? icx::la_tri_rows_f32(c->dm, lower, w->pc32, v, x0, -1.0, y, s)
-               : icx::la_tri_rows(c->dm, lower, w->pc, v, x0, -1.0, y, s);
+  const icx::DeviceMesh dm = ilu_mesh(c);
+  return mixed ? icx::la_tri_rows_f32(dm, lower, w->pc32, v, x0, -1.0, y, s)
+               : icx::la_tri_rows(dm, lower, w->pc, v, x0, -1.0, y, s);
 }
 
 // the data-flow block-ILU(0) apply with the context's launch shape. Each
@@ -190,7 +295,8 @@ cudaError_t tri_rows(icx_ctx* c, bool mixed, bool lower, const double* v, const 
 // differ) first zeroes the counters, in stream order
 cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStream_t s) {
   icx_solver_work* w = c->sw;
-  const icx::DeviceMesh& dm = c->dm;
+  const icx::DeviceMesh dm = ilu_mesh(c);
+  const int* order = ilu_order(c);
   const int pi = mixed ? 1 : 0;
   const int rows = dm.tile.flow_rows[pi] ? dm.tile.flow_rows[pi] : icx::flow_rows_default(w->bs);
   // the sentinel schedule uses neither the counters nor the epoch
@@ -203,9 +309,9 @@ cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStr
   }
   const unsigned epoch = sen ? w->epoch : ++w->epoch;
   if (mixed)
-    return icx::la_ilu_apply_flow_f32(dm, w->order, w->pc32, w->uinv32, x, z, w->pct, w->cnt, w->cnt + dm.E,
+    return icx::la_ilu_apply_flow_f32(dm, order, w->pc32, w->uinv32, x, z, w->pct, w->cnt, w->cnt + dm.E,
                                       epoch, w->pc_err, s);
-  return icx::la_ilu_apply_flow(dm, w->order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E, epoch,
+  return icx::la_ilu_apply_flow(dm, order, w->pc, w->uinv, x, z, w->pct, w->cnt, w->cnt + dm.E, epoch,
                                 w->pc_err, s);
 }
 
@@ -252,7 +358,7 @@ cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* 
     return e;
   }
   if (kind == 2) {
-    if (w->rows_ok && w->schedule == 2) {
+    if (w->rows_ok && w->schedule == 2 && !w->tp.tile) {
       const unsigned ep = w->epoch_rows + 1;
       cudaError_t e = mixed ? icx::la_ilu_apply_rows_f32(dm, c->nx, c->ny, w->pc32, w->uinv32, x, z, w->pct,
                                                          w->cnt_rows, w->cnt_rows + dm.E, ep, w->pc_err, s)
@@ -269,7 +375,7 @@ cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* 
 
 // builds the preconditioner from w->vals (in FP64; mixed: then rounded to FP32,
 // together with the Jacobian itself)
-cudaError_t build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
+cudaError_t build_pc_impl(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
   icx_solver_work* w = c->sw;
   const icx::DeviceMesh& dm = c->dm;
   const long long nv = (long long)dm.nnzb * w->bs * w->bs, nd = (long long)dm.E * w->bs * w->bs;
@@ -278,16 +384,34 @@ cudaError_t build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
   const bool jac = kind == 1 || kind == 3, ilu = kind == 2 || kind == 4 || kind == 5;
   if (kind == 5 && (e = icx::lpc_build(c, w->vals, s)) != cudaSuccess) return e;
   if (jac) e = icx::la_block_invert(dm.E, w->bs, w->vals, dm.bsr_diag, w->pc, w->flag, s);
+  long long nv_pc = nv;
   if (ilu) {
-    e = cudaMemcpyAsync(w->pc, w->vals, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s);
-    if (e == cudaSuccess) e = icx::la_ilu_factor(dm, w->order, w->lvl_off, w->pc, w->uinv, w->flag, s);
+    if (w->tp.tile) {
+      // the kept blocks, compacted into the tiled pattern's order
+      const icx::DeviceMesh dt = ilu_mesh(c);
+      nv_pc = (long long)dt.nnzb * w->bs * w->bs;
+      e = icx::la_gather_blocks(dt.nnzb, w->bs, w->vals, w->tp.map, w->pc, s);
+      if (e == cudaSuccess) e = icx::la_ilu_factor(dt, w->tp.order, w->tp.lvl_off, w->pc, w->uinv, w->flag, s);
+    } else {
+      e = cudaMemcpyAsync(w->pc, w->vals, sizeof(double) * nv, cudaMemcpyDeviceToDevice, s);
+      if (e == cudaSuccess) e = icx::la_ilu_factor(dm, w->order, w->lvl_off, w->pc, w->uinv, w->flag, s);
+    }
   }
   if (e != cudaSuccess || !mixed) return e;
   e = icx::la_d2f(nv, w->vals, w->vals32, s);
   if (e == cudaSuccess && jac) e = icx::la_d2f(nd, w->pc, w->pc32, s);
-  if (e == cudaSuccess && ilu) e = icx::la_d2f(nv, w->pc, w->pc32, s);
+  if (e == cudaSuccess && ilu) e = icx::la_d2f(nv_pc, w->pc, w->pc32, s);
   if (e == cudaSuccess && ilu) e = icx::la_d2f(nd, w->uinv, w->uinv32, s);
   return e;
+}
+
+// the preconditioner for the context's current ILU tiling (the tiled plan is
+// built on the first use of a new tile size)
+cudaError_t build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
+  if (kind == 2 || kind == 4 || kind == 5) {
+    if (ensure_ilu_plan(c) != ICX_OK) return cudaErrorInvalidValue;  // c->err says why
+  }
+  return build_pc_impl(c, kind, mixed, s);
 }
 
 // x = J^-1 b by GMRES(m) on the BSR Jacobian, right preconditioning
@@ -337,7 +461,7 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
     for (long long v : {(long long)pc, (long long)mixed, (long long)w->sweeps, (long long)m, (long long)t.flow_rows[pi],
                         (long long)t.flow_ctas[pi], (long long)t.flow_sched[pi], (long long)(uintptr_t)dm.bsr_rowptr,
                         (long long)(uintptr_t)dm.bsr_colidx, (long long)(uintptr_t)dm.bsr_diag,
-                        (long long)(uintptr_t)w->order})
+                        (long long)(uintptr_t)w->order, (long long)w->tp.tile, (long long)(uintptr_t)w->tp.order})
       key = (key ^ (unsigned long long)v) * 1099511628211ull;
     kb.graphs = &w->graphs;
     kb.graph_key = key | 1;
@@ -443,6 +567,7 @@ void free_solver_work(icx_ctx* c) {
   w->graphs.release();
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  free_tile_plan(w->tp);
   delete w;
   c->sw = nullptr;
 }
@@ -489,8 +614,18 @@ icx_status icx_newton_default_options(icx_newton_options* o) {
   o->precision = 0;          // all FP64
   o->pc_sweeps = 2;
   o->cuda_graphs = 1;
+  o->ilu_tile = 0;           // block-ILU(0) over the whole grid in natural order
   return ICX_OK;
 }
+
+icx_status icx_set_ilu_tile(icx_ctx* c, int tile) {
+  if (!c) return ICX_ERR_INVALID;
+  if (tile < 0 || tile > (1 << 20)) return set_err(c, ICX_ERR_INVALID, "ILU tile side must be in 0..2^20");
+  c->ilu_tile = tile;
+  return ICX_OK;
+}
+
+int icx_get_ilu_tile(const icx_ctx* c) { return c ? c->ilu_tile : -1; }
 
 icx_status icx_gmres_solve(icx_ctx* c, const double* d_vals, const double* d_b, double* d_x, int restart, int maxit,
                            double rtol, int preconditioner, int* iterations, double* relres, void* stream) {
@@ -602,6 +737,8 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
     return set_err(c, ICX_ERR_INVALID, "pc_sweeps in 0..16");
   if (opt->preconditioner == 5 && !c->lpc)
     return set_err(c, ICX_ERR_INVALID, "preconditioner 5 needs a learned model (icx_lpc_attach)");
+  if (opt->ilu_tile > (1 << 20)) return set_err(c, ICX_ERR_INVALID, "ILU tile side must be at most 2^20");
+  if (opt->ilu_tile >= 0) c->ilu_tile = opt->ilu_tile;  // negative: keep the context's tiling
   icx_status st = ensure_work(c, opt->gmres_restart);
   if (st != ICX_OK) return st;
   c->sw->sweeps = opt->pc_sweeps;

@@ -8,10 +8,14 @@ Reynolds number drawn per instance uniformly from [50, 500] (viscosity 1/Re).
 Training data are generated by the plain solver: at every Newton step of a
 training instance the FD Jacobian is formed and the plain GMRES(30) +
 block-ILU(0) solve of that step records Krylov residuals (its restart
-residuals and every k-th Arnoldi vector). The model then takes Adam steps on
-that Jacobian's samples before the Newton step is applied. Evaluation runs
-fresh seeds through the plain all-FP64 block-ILU(0) Newton solve and through
-the learned, mixed-precision one, both to an FP64 residual of 1e-10."""
+residuals and every k-th Arnoldi vector); each (Jacobian, residual) pair is
+one training sample, and instances are drawn until the recipe's number of
+pairs is reached. The model then takes Adam steps on that Jacobian's samples
+before the Newton step is applied. The correction is trained on top of the
+base preconditioner it is run with (block-ILU(0) on element tiles, exact
+triangular solves). Evaluation runs fresh seeds through the plain all-FP64
+block-ILU(0) Newton solve and through the learned, mixed-precision one, both
+to an FP64 residual of 1e-10."""
 import time
 
 import numpy as np
@@ -33,15 +37,21 @@ def make_instance(seed, re, n=256, device=0):
 
 
 def train(model, train_instances, n=256, samples=167, every=10, steps=150, batch=4, random=2, sweeps=2, lr=1e-3,
-          newton_steps=4, device=0, log=None):
-    """train `model` on the Newton steps of each instance; returns per-Jacobian
-    records (instance, step, |r|, samples, gmres iterations, first/last loss)"""
+          newton_steps=4, device=0, log=None, pairs=None, ilu_tile=0):
+    """train `model` on the Newton steps of each instance (until `pairs`
+    Jacobian / residual pairs have been used, when given); returns
+    per-Jacobian records (instance, step, |r|, samples, gmres iterations,
+    first/last loss)"""
     import torch
     dev = torch.device("cuda", device)
     out = []
+    used = 0
     for (seed, re) in train_instances:
+        if pairs is not None and used >= pairs:
+            break
         wl = make_instance(seed, re, n, device)
         ctx = wl.ctx
+        ctx.ilu_tile = ilu_tile
         ctx.lpc_attach(model)
         L = ctx.layout
         bs = L.block_size
@@ -51,15 +61,23 @@ def train(model, train_instances, n=256, samples=167, every=10, steps=150, batch
         vals = torch.empty(L.nnz_blocks * bs * bs, dtype=torch.float64, device=dev)
         buf = torch.empty((samples, L.n_dof), dtype=torch.float64, device=dev)
         for k in range(newton_steps):
+            if pairs is not None and used >= pairs:
+                break
             ctx.form_jacobian_fd(u, res, vals)
             rn = float(torch.linalg.vector_norm(res))
             if rn <= 1e-10:
                 break
+            # the samples come from the plain solver (whole-grid block-ILU(0))
+            ctx.ilu_tile = 0
             ns, its, rr = ctx.krylov_samples(vals, res, du, buf, every=every)
+            ctx.ilu_tile = ilu_tile
+            if pairs is not None:
+                ns = min(ns, pairs - used)
+            used += ns
             t0 = time.time()
             rep = ctx.lpc_train(vals, buf, ns, steps=steps, batch=batch, random=random, sweeps=sweeps, lr=lr,
                                 seed=seed * 7919 + k)
-            rec = dict(seed=seed, re=re, newton_step=k, r=rn, samples=ns, gmres_its=its,
+            rec = dict(seed=seed, re=re, newton_step=k, r=rn, samples=ns, pairs_used=used, gmres_its=its,
                        loss_first=rep.loss_first, loss_last=rep.loss_last, train_s=time.time() - t0)
             out.append(rec)
             if log:
@@ -70,7 +88,7 @@ def train(model, train_instances, n=256, samples=167, every=10, steps=150, batch
     return out
 
 
-def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0):
+def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu_tile=0):
     """one Newton solve of an instance to |r| <= 1e-10 (GMRES(30), Wolfe line
     search), timed with CUDA events; returns (report dict, final state)"""
     import torch
@@ -79,6 +97,7 @@ def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0):
     opt.preconditioner = preconditioner
     opt.precision = precision
     opt.pc_sweeps = sweeps
+    opt.ilu_tile = ilu_tile
     opt.gmres_max_it = 20000
     if model is not None:
         wl.ctx.lpc_attach(model)
@@ -91,20 +110,21 @@ def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0):
     torch.cuda.synchronize(dev)
     if model is not None:
         wl.ctx.lpc_attach(None)
-    return dict(s=e0.elapsed_time(e1) * 1e-3, newton_its=rep.iterations, gmres_its=rep.linear_iterations_total,
+    return dict(s=e0.elapsed_time(e1) * 1e-3, ilu_tile=ilu_tile, newton_its=rep.iterations,
+                gmres_its=rep.linear_iterations_total,
                 gmres_its_per_step=list(rep.linear_iterations[:rep.iterations]), r_final=rep.r_final,
                 converged=bool(rep.converged), pc_fallbacks=rep.pc_fallbacks), u.cpu().numpy()
 
 
-def evaluate(model, eval_instances, n=256, sweeps=2, device=0, log=None):
+def evaluate(model, eval_instances, n=256, sweeps=0, device=0, log=None, ilu_tile=0):
     """plain all-FP64 block-ILU(0) against learned + mixed precision (and the
-    untrained parallel ILU as ablation) on fresh instances"""
+    untrained base preconditioner, mixed, as ablation) on fresh instances"""
     out = []
     for (seed, re) in eval_instances:
         wl = make_instance(seed, re, n, device)
         plain, u_plain = solve(wl, None, 2, 0, device=device)
-        learned, u_l = solve(wl, model, 5, 1, sweeps, device)
-        ablation, u_a = solve(wl, None, 4 if sweeps > 0 else 2, 1, sweeps, device)
+        learned, u_l = solve(wl, model, 5, 1, sweeps, device, ilu_tile)
+        ablation, u_a = solve(wl, None, 4 if sweeps > 0 else 2, 1, sweeps, device, ilu_tile)
         scale = max(np.linalg.norm(u_plain), 1e-300)
         rec = dict(seed=seed, re=re, plain_fp64_ilu0=plain, learned_mixed=learned, untrained_base_mixed=ablation,
                    learned_vs_plain_state_l2=float(np.linalg.norm(u_l - u_plain) / scale),
@@ -121,9 +141,13 @@ def new_model(device=0, seed=0, hidden=256):
     return LearnedPreconditioner(BLOCK_SIZE, hidden, device, seed)
 
 
-# the training recipe of the shipped model (data/learned_pc_ns_p2.npz)
-RECIPE = dict(model_seed=1, train_instances=(3, 11), steps=120, batch=4, random=2, sweeps=2, lr=1e-3)
-EVAL_INSTANCES = (2, 99)
+# the training recipe of the shipped model (data/learned_pc_ns_p2.npz): 2,000
+# Jacobian / residual pairs from the plain solver on seeded instances (Re
+# uniform in [50, 500]), the correction trained on top of block-ILU(0) on
+# 32 x 32 element tiles with exact triangular solves (pc_sweeps = 0)
+RECIPE = dict(model_seed=1, train_instances=(8, 11), pairs=2000, samples=167, every=5, steps=120, batch=4, random=2,
+              sweeps=0, ilu_tile=32, lr=1e-3)
+EVAL_INSTANCES = (3, 99)
 
 
 def main(argv=None):
@@ -138,12 +162,13 @@ def main(argv=None):
     if a.cmd == "train":
         r = RECIPE
         m = new_model(seed=r["model_seed"])
-        train(m, instances(*r["train_instances"]), n=a.n, steps=r["steps"], batch=r["batch"], random=r["random"],
-              sweeps=r["sweeps"], lr=r["lr"], log=lambda x: print(json.dumps(x), flush=True))
-        m.save(a.path, sweeps=r["sweeps"])
+        train(m, instances(*r["train_instances"]), n=a.n, samples=r["samples"], every=r["every"], steps=r["steps"],
+              batch=r["batch"], random=r["random"], sweeps=r["sweeps"], lr=r["lr"], pairs=r["pairs"],
+              ilu_tile=r["ilu_tile"], log=lambda x: print(json.dumps(x), flush=True))
+        m.save(a.path, sweeps=r["sweeps"], ilu_tile=r["ilu_tile"])
     else:
         m = LearnedPreconditioner.load(a.path)
-        evaluate(m, instances(*EVAL_INSTANCES), n=a.n, sweeps=m.sweeps,
+        evaluate(m, instances(*EVAL_INSTANCES), n=a.n, sweeps=m.sweeps, ilu_tile=m.ilu_tile or 0,
                  log=lambda x: print(json.dumps(x), flush=True))
 
 

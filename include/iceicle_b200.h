@@ -266,6 +266,15 @@ typedef struct icx_newton_options {
    * 0-4 (block-ILU(0) on its default sentinel schedule). The same kernels run
    * in the same order: results are identical with 0. */
   int cuda_graphs;
+  /* block-ILU(0) on ilu_tile x ilu_tile element tiles for preconditioners 2,
+   * 4 and 5: blocks that couple two tiles are dropped, which is block-Jacobi
+   * over the tiles with ILU(0) inside each (PETSc's parallel default,
+   * PCBJACOBI with PCILU sub-solves, petsc_newton.hpp:179-182, one block per
+   * tile). 0 (default): ILU(0) over the whole grid in natural order, the
+   * single-process PCILU. Negative: keep the context's setting
+   * (icx_set_ilu_tile). Changes the preconditioner and so the GMRES
+   * iterations, not the converged state. */
+  int ilu_tile;
 } icx_newton_options;
 
 typedef struct icx_newton_report {
@@ -297,6 +306,12 @@ icx_status icx_gmres_solve(icx_ctx* ctx, const double* d_vals, const double* d_b
  * element pattern; it is slower than the data-flow apply on the measured
  * workloads). The apply runs `repeat` times after one factorization;
  * *ms_per_apply (may be NULL) is its mean device time by CUDA events. */
+/* the context's block-ILU(0) tiling used by icx_gmres_solve, icx_ilu_apply,
+ * icx_krylov_samples and by icx_newton_solve when its ilu_tile < 0 (tile side
+ * in elements, 0: the whole grid; see icx_newton_options.ilu_tile). No
+ * reference counterpart: the reference selects the PC through PETSc options. */
+icx_status icx_set_ilu_tile(icx_ctx* ctx, int tile);
+int icx_get_ilu_tile(const icx_ctx* ctx);
 icx_status icx_ilu_apply(icx_ctx* ctx, const double* d_vals, const double* d_x, double* d_y, int precision,
                          int schedule, int repeat, double* ms_per_apply);
 icx_status icx_newton_default_options(icx_newton_options* opt);
@@ -370,6 +385,17 @@ icx_status icx_krylov_samples(icx_ctx* ctx, const double* d_vals, const double* 
  * Newton preconditioner 5 applies z = (I + C) y with y the block-ILU(0)
  * factors applied by pc_sweeps Jacobi sweeps per triangle. BF16 products on
  * the tensor cores with FP32 accumulation; FP32 master weights. */
+/* BF16 GEMM on the tensor cores (tcgen05.mma, TMEM accumulator, TMA operand
+ * loads): C = A . B^T with A [M][lda] and B [N][ldb] row-major BF16 (device),
+ * FP32 accumulation; optional bias [N] and ReLU, output FP32 (C32 [M][ldc])
+ * and/or BF16 (C16 [M][ldc16]); accumulate = 1 adds into C32 atomically and
+ * allows splits > 1 (split-K). K, lda, ldb multiples of 8, lda, ldb >= K,
+ * A and B 16-byte aligned. The kernel of the learned preconditioner's MLP
+ * (no reference counterpart), exported for tests. Synchronises the stream. */
+icx_status icx_gemm_bf16_nt(int M, int N, int K, const void* d_A, int lda, const void* d_B, int ldb,
+                            const float* d_bias, int relu, float* d_C32, int ldc, void* d_C16, int ldc16,
+                            int accumulate, int splits, void* stream);
+
 typedef struct icx_lpc icx_lpc;
 typedef struct icx_lpc_train_options {
   int steps;               /* Adam steps on this Jacobian */

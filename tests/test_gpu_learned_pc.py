@@ -1,7 +1,8 @@
 """The learned block preconditioner (Newton preconditioner 5) and the
-parallel preconditioners 3 and 4: the BF16 MLP against a torch FP32
-evaluation of the same network on BF16-rounded inputs, training lowering its
-loss, and Newton solves that reach the plain block-ILU(0) state."""
+parallel preconditioners 3 and 4: the BF16 graph network (MLP with one
+face-neighbour message-passing step) against a torch FP32 evaluation of the
+same network on BF16-rounded inputs, training lowering its loss, and Newton
+solves that reach the plain block-ILU(0) state."""
 import numpy as np
 import pytest
 import torch
@@ -34,16 +35,20 @@ def _bf(x):
 
 
 def test_mlp_forward_matches_a_torch_fp32_evaluation():
-    """C = W3 relu(W2 relu(W1 x + b1) + b2) + b3 per element block, x = J_ee /
-    |J_ee|_F. The reference rounds x, the weights and both hidden activations
-    to BF16 as the kernels do and computes in FP32; the kernels accumulate in
-    FP32 in another order: 2e-2 of the largest output (BF16 has 8 bits)."""
+    """h1_e = relu(W1 x_e + b1), m_e = mean of h1 over the face neighbours of e
+    (the message-passing step), h2_e = relu(W2 [h1_e ; m_e] + b2),
+    C_e = W3 h2_e + b3, x_e = J_ee / |J_ee|_F. The reference rounds x, the
+    weights, h1, m and h2 to BF16 as the kernels do and computes in FP32; the
+    kernels accumulate in FP32 in another order: 2e-2 of the largest output
+    (BF16 has 8 bits)."""
     spec, ctx, u0 = _ns_ctx()
     m = ib.LearnedPreconditioner(36, 64, 0, seed=3)
     p = m.get_params()
     rng = np.random.default_rng(0)
     D, H = 36 * 36, 64
-    oW3 = H * D + H + H * H + H
+    oW2 = H * D + H
+    oW3 = oW2 + H * 2 * H + H
+    assert p.size == oW3 + D * H + D
     p[oW3:oW3 + D * H] = 0.05 * rng.standard_normal(D * H)
     p[oW3 + D * H:] = 0.01 * rng.standard_normal(D)
     p[H * D:H * D + H] = 0.1 * rng.standard_normal(H)
@@ -60,14 +65,23 @@ def test_mlp_forward_matches_a_torch_fp32_evaluation():
     V = vals.view(-1, D)[torch.from_numpy(diag).cuda()]
     X = _bf((V / V.norm(dim=1, keepdim=True)).float())
     P = torch.from_numpy(p).cuda()
-    W1 = P[:H * D].view(H, D); b1 = P[H * D:H * D + H]
-    W2 = P[H * D + H:H * D + H + H * H].view(H, H); b2 = P[H * D + H + H * H:oW3]
+    W1 = P[:H * D].view(H, D); b1 = P[H * D:oW2]
+    W2 = P[oW2:oW2 + 2 * H * H].view(H, 2 * H); b2 = P[oW2 + 2 * H * H:oW3]
     W3 = P[oW3:oW3 + D * H].view(D, H); b3 = P[oW3 + D * H:]
     h1 = _bf(torch.relu(X @ _bf(W1).T + b1))
-    h2 = _bf(torch.relu(h1 @ _bf(W2).T + b2))
+    msg = torch.zeros_like(h1)
+    for e in range(E):
+        nb = [int(k) for k in ci[rp[e]:rp[e + 1]] if k != e]
+        if nb:
+            msg[e] = h1[nb].mean(dim=0)
+    h2 = _bf(torch.relu(torch.cat([h1, _bf(msg)], dim=1) @ _bf(W2).T + b2))
     ref = h2 @ _bf(W3).T + b3
     got = corr.view(E, D)
     assert (got - ref).abs().max().item() <= 2e-2 * ref.abs().max().item()
+    # the message matters: the same network without it gives another output
+    h2_nomsg = _bf(torch.relu(torch.cat([h1, torch.zeros_like(h1)], dim=1) @ _bf(W2).T + b2))
+    ref_nomsg = h2_nomsg @ _bf(W3).T + b3
+    assert (ref_nomsg - ref).abs().max().item() > 5e-2 * ref.abs().max().item()
     ctx.lpc_attach(None)
 
 
