@@ -26,11 +26,12 @@ POINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_v
 
 # BOUNDARY_CONDITIONS values of the reference (geometry/face.hpp:23-90)
 PERIODIC, PARALLEL_COM, NEUMANN, DIRICHLET, EXTRAPOLATION = 0, 1, 2, 3, 4
+RIEMANN, NO_SLIP_ISOTHERMAL, SLIP_WALL, WALL_GENERAL = 5, 6, 7, 8
 SPACETIME_PAST, SPACETIME_FUTURE = 11, 12
 BASIS_LAGRANGE, BASIS_LEGENDRE = 0, 1
 SPACETIME_FUTURE, INTERIOR = 12, 13
 PDE_BURGERS, PDE_NAVIER_STOKES = 0, 1
-FLUX_UPWIND, FLUX_VANLEER = 0, 1
+FLUX_UPWIND, FLUX_VANLEER, FLUX_ROE = 0, 1, 2
 
 STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "UNSUPPORTED", 4: "NONFINITE", 5: "NOT_CONVERGED",
           6: "NOMEM", 7: "SIZE", 8: "NO_DEVICE"}
@@ -131,6 +132,8 @@ def lib():
             "icx_form_residuals_host": (C.c_int, [vp, C.c_int, vp, vp, dp]),
             "icx_ilu_apply": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, dp]),
             "icx_disc_navier_stokes": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
+            "icx_disc_ns_boundary": (C.c_int, [vp, dp, C.c_int, C.c_double, C.c_double, dp, C.c_double,
+                                               C.c_double]),
             "icx_disc_options": (C.c_int, [vp, C.c_int, C.c_double]),
             "icx_disc_dirichlet": (C.c_int, [vp, C.c_int, POINT_FN, vp]),
             "icx_disc_neumann": (C.c_int, [vp, C.c_int, POINT_FN, vp]),
@@ -293,6 +296,15 @@ class Context:
 
     def disc_navier_stokes(self, gamma=1.4, Pr=0.72, mu=0.01, conv_flux=FLUX_VANLEER):
         self._check(lib().icx_disc_navier_stokes(self._h, gamma, Pr, mu, conv_flux), "disc_navier_stokes")
+
+    def disc_ns_boundary(self, wall_temperatures=(), rho_inf=1.0, u_inf=0.0, u_direction=(1.0, 0.0), T_inf=1.0,
+                         Rgas=287.052874):
+        """Navier-Stokes wall temperatures (per bcflag) and free stream of the
+        PDE-level boundaries (Physics::isothermal_temperatures / free_stream)"""
+        tw = (C.c_double * 8)(*wall_temperatures)
+        ud = (C.c_double * 2)(*u_direction)
+        self._check(lib().icx_disc_ns_boundary(self._h, tw, len(wall_temperatures), rho_inf, u_inf, ud, T_inf, Rgas),
+                    "disc_ns_boundary")
 
     def disc_options(self, interior_penalty=False, sigma_ic=0.0):
         self._check(lib().icx_disc_options(self._h, int(interior_penalty), float(sigma_ic)), "disc_options")

@@ -142,7 +142,7 @@ __device__ inline void face_flux_states(const PhysParams& pp, const FacePt& fp, 
   double fadv[NEQ], fvis[NEQ];
   const bool ic = Phys<PDE>::has_ic && pp.sigma_ic != 0.0;
   if (interior) {
-    Phys<PDE>::conv(pp, uL, uR, n, fadv);
+    Phys<PDE>::conv_sel(pp, uL, uR, n, fadv);
     double gddg[2 * NEQ], uavg[NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) {
@@ -173,14 +173,22 @@ __device__ inline void face_flux_states(const PhysParams& pp, const FacePt& fp, 
         gq[1 * 2 + kk] = cs[0] * fp.JiR[kk * 2 + 0] + cs[1] * fp.JiR[kk * 2 + 1];
       }
     }
-  } else if (bct == ICX_BC_DIRICHLET || (bct == ICX_BC_SPACETIME_PAST && pp.st_connected)) {
+  } else if (bct == ICX_BC_DIRICHLET || (bct == ICX_BC_SPACETIME_PAST && pp.st_connected) ||
+             (Phys<PDE>::has_pde_bcs && bct >= ICX_BC_RIEMANN && bct <= ICX_BC_WALL_GENERAL)) {
     // a connected SPACETIME_PAST face takes the past slab's trace as exterior
     // state; on a slab interface at constant t the diffusive normal flux
-    // vanishes (no diffusion along t), leaving the time-upwind flux
+    // vanishes (no diffusion along t), leaving the time-upwind flux. The
+    // PDE-level kinds (walls, characteristic) form the exterior state from
+    // the interior one and then take the same DDG boundary flux as a
+    // Dirichlet face with one-sided gradients (conservation_law.hpp:1043-1130)
     double ud[NEQ];
+    if (bct == ICX_BC_DIRICHLET || bct == ICX_BC_SPACETIME_PAST) {
 #pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) ud[eq] = bval[eq];
-    Phys<PDE>::conv(pp, uL, ud, n, fadv);
+      for (int eq = 0; eq < NEQ; ++eq) ud[eq] = bval[eq];
+    } else {
+      Phys<PDE>::apply_bc(pp, uL, n, bct, bval, ud);
+    }
+    Phys<PDE>::conv_sel(pp, uL, ud, n, fadv);
     double gddg[2 * NEQ], uavg[NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) {
@@ -211,7 +219,7 @@ __device__ inline void face_flux_states(const PhysParams& pp, const FacePt& fp, 
     for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq;
     if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
   } else if (bct == ICX_BC_EXTRAPOLATION || bct == ICX_BC_SPACETIME_FUTURE) {
-    Phys<PDE>::conv(pp, uL, uL, n, fadv);
+    Phys<PDE>::conv_sel(pp, uL, uL, n, fadv);
     Phys<PDE>::diff(pp, uL, gL, n, fvis);
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq - fadv[eq] * wsq;

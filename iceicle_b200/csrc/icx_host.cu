@@ -276,6 +276,15 @@ icx_status tabulate_and_geometry(icx_ctx* c) {
         return fail(c, ICX_ERR_INVALID, "missing Neumann callback for a boundary flag");
       fn = c->neumann_fn[flag]; user = c->neumann_user[flag];
     }
+    if (c->phys.pde == ICX_PDE_NAVIER_STOKES &&
+        (bct == ICX_BC_NO_SLIP_ISOTHERMAL || (bct == ICX_BC_WALL_GENERAL && c->phys.ns_viscous_wall))) {
+      // the wall temperature of the face's bcflag (Physics::isothermal_temperatures[bcflag])
+      if (flag < 0 || flag >= (int)c->wall_T.size())
+        return fail(c, ICX_ERR_INVALID, "no wall temperature for an isothermal wall's boundary flag "
+                                        "(icx_disc_ns_boundary)");
+      for (int q = 0; q < dm.nqf; ++q) bv[((size_t)bidx * dm.nqf + q) * neq] = c->wall_T[flag];
+      continue;
+    }
     if (!fn) continue;
     for (int q = 0; q < dm.nqf; ++q) {
       double xi[2], x[2];
@@ -604,7 +613,11 @@ icx_status icx_disc_spacetime_burgers(icx_ctx* c, double mu, double a, double b)
 
 icx_status icx_disc_navier_stokes(icx_ctx* c, double gamma, double Pr, double mu, int conv_flux) {
   if (!c) return ICX_ERR_INVALID;
-  if (conv_flux != ICX_FLUX_VANLEER) return fail(c, ICX_ERR_UNSUPPORTED, "Navier-Stokes supports the Van Leer flux");
+  if (conv_flux != ICX_FLUX_VANLEER && conv_flux != ICX_FLUX_ROE)
+    return fail(c, ICX_ERR_UNSUPPORTED, "Navier-Stokes convective flux: Van Leer or Roe");
+  c->phys.ns_flux = conv_flux;
+  c->phys.ns_viscous_wall = mu != 0.0;
+  if (!(c->phys.Rgas > 0.0)) c->phys.Rgas = 287.052874;  // EoS::Rgas default (navier_stokes.hpp:338)
   c->phys.pde = ICX_PDE_NAVIER_STOKES;
   c->phys.gamma = gamma;
   c->phys.Pr = Pr;
@@ -614,6 +627,22 @@ icx_status icx_disc_navier_stokes(icx_ctx* c, double gamma, double Pr, double mu
   c->phys.mu_gamma_pr = mu * gamma / Pr;
   c->conv_flux = conv_flux;
   c->has_disc = true;
+  c->ready = false;
+  return ICX_OK;
+}
+
+icx_status icx_disc_ns_boundary(icx_ctx* c, const double* wall_temperatures, int n_walls, double rho_inf,
+                                double u_inf, const double u_direction[2], double T_inf, double Rgas) {
+  if (!c) return ICX_ERR_INVALID;
+  if (n_walls < 0 || n_walls > 8 || (n_walls > 0 && !wall_temperatures))
+    return fail(c, ICX_ERR_INVALID, "wall temperatures: 0..8 values");
+  if (!(Rgas > 0.0)) return fail(c, ICX_ERR_INVALID, "the gas constant must be positive");
+  c->wall_T.assign(wall_temperatures, wall_temperatures + n_walls);
+  c->phys.fs_rho = rho_inf;
+  c->phys.fs_u[0] = u_direction ? u_direction[0] * u_inf : u_inf;
+  c->phys.fs_u[1] = u_direction ? u_direction[1] * u_inf : 0.0;
+  c->phys.fs_T = T_inf;
+  c->phys.Rgas = Rgas;
   c->ready = false;
   return ICX_OK;
 }
@@ -674,12 +703,14 @@ icx_status icx_setup(icx_ctx* c) {
   dm.nq1 = g + P;  // geometry order + basis order points per direction (reference_element.hpp:80, 240-245)
   dm.nqv = dm.nq1 * dm.nq1;
   dm.nqf = dm.nq1;
-  // NS boundary kinds implemented at the PDE level are not provided
+  // boundary kinds: INLET and OUTLET have no implementation in the
+  // reference's Navier-Stokes apply_bc (it logs "Unsupported BC" and leaves
+  // the exterior state unset), so they are refused here
   if (c->phys.pde == ICX_PDE_NAVIER_STOKES)
     for (int i = 0; i < 4; ++i) {
       int b = c->bctype[i];
-      if (b != ICX_BC_DIRICHLET && b != ICX_BC_NEUMANN && b != ICX_BC_EXTRAPOLATION && b != ICX_BC_SPACETIME_FUTURE)
-        return fail(c, ICX_ERR_UNSUPPORTED, "Navier-Stokes wall/characteristic boundaries are not implemented");
+      if (b == 9 || b == 10 || b == ICX_BC_SPACETIME_PAST)
+        return fail(c, ICX_ERR_UNSUPPORTED, "Navier-Stokes inlet/outlet/spacetime boundaries are not implemented");
     }
   if (c->phys.pde == ICX_PDE_NAVIER_STOKES && c->phys.sigma_ic != 0.0) {
     // the Navier-Stokes diffusive flux defines no homogeneity tensor: the

@@ -35,6 +35,16 @@ struct PhysParams {
   int interior_penalty;
   double sigma_ic;
   double beta0, beta1;          // DDG coefficients (beta1 = 0 for interior penalty)
+  int ns_flux;                  // Navier-Stokes convective flux: ICX_FLUX_VANLEER or ICX_FLUX_ROE
+  // Navier-Stokes PDE-level boundaries (navier_stokes.hpp:976-1189): the
+  // free stream of the characteristic (Riemann) boundary as density,
+  // velocity and temperature, the gas constant of the equation of state,
+  // and whether WALL_GENERAL is the no-slip isothermal wall (viscous) or the
+  // slip wall (inviscid); wall temperatures per bcflag go into the boundary
+  // data table at setup
+  double fs_rho, fs_u[2], fs_T;
+  double Rgas;
+  int ns_viscous_wall;
 };
 
 // launch shapes of the tunable kernels (0: the compiled default). Every
@@ -140,6 +150,7 @@ struct icx_ctx {
   int basis = ICX_BASIS_LAGRANGE;             // solution basis family
   icx::PhysParams phys{};
   int conv_flux = 0;
+  std::vector<double> wall_T;                 // Navier-Stokes isothermal wall temperature per bcflag
   std::vector<icx_point_fn> dirichlet_fn, neumann_fn;
   std::vector<void*> dirichlet_user, neumann_user;
   icx_point_fn source_fn = nullptr;

@@ -45,6 +45,16 @@ template <> struct Phys<ICX_PDE_BURGERS> {
   }
   __device__ static inline void neumann(const PhysParams& pp, const double* gn, double* f) { f[0] = pp.mu * gn[0]; }
   static constexpr bool has_ic = true;  // homogeneity tensor G = mu * I
+  __device__ static inline void conv_sel(const PhysParams& pp, const double* uL, const double* uR, const double* n,
+                                         double* f) {
+    conv(pp, uL, uR, n, f);
+  }
+  // the Burgers fluxes implement no PDE-level boundaries: those faces contribute nothing
+  static constexpr bool has_pde_bcs = false;
+  __device__ static inline void apply_bc(const PhysParams&, const double* uL, const double*, int, const double*,
+                                         double* uR) {
+    uR[0] = uL[0];
+  }
 };
 
 // ------------------------------------------------------------ Navier-Stokes
@@ -165,6 +175,109 @@ template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
       f[3] += fmR * ((R.vv - vnR * vnR) / 2 + t * t * inv_g21);
     }
   }
+
+  // Roe's approximate Riemann solver (P. L. Roe, J. Comput. Phys. 43, 1981):
+  // F = (F(uL).n + F(uR).n) / 2 - sum_k |lambda_k| alpha_k r_k / 2 over the
+  // acoustic, entropy and shear waves of the Roe-averaged state, with
+  // Harten's entropy fix on the acoustic eigenvalues
+  // (|l| < d: (l^2 + d^2) / (2 d), d = 0.1 c~). Unit reference parameters
+  // (Eu = e_coeff = 1), so the ideal-gas relations take their usual form.
+  __device__ static inline void roe(const PhysParams& pp, const double* uL, const double* uR, const double* n,
+                                    double* f) {
+    NSState L = ns_state(pp, uL), R = ns_state(pp, uR);
+    const double gam = pp.gamma;
+    const double vnL = L.v0 * n[0] + L.v1 * n[1], vnR = R.v0 * n[0] + R.v1 * n[1];
+    const double HL = L.E + L.p * L.inv_rho, HR = R.E + R.p * R.inv_rho;
+    const double sL = sqrt(L.rho), sR = sqrt(R.rho), inv = 1.0 / (sL + sR);
+    const double rt = sL * sR;
+    const double ut0 = (sL * L.v0 + sR * R.v0) * inv, ut1 = (sL * L.v1 + sR * R.v1) * inv;
+    const double Ht = (sL * HL + sR * HR) * inv;
+    const double qq = ut0 * ut0 + ut1 * ut1;
+    const double c2 = fmax((gam - 1) * (Ht - 0.5 * qq), 1e-14);
+    const double ct = sqrt(c2);
+    const double unt = ut0 * n[0] + ut1 * n[1];
+    const double drho = R.rho - L.rho, dp = R.p - L.p, dun = vnR - vnL;
+    const double dv0 = R.v0 - L.v0, dv1 = R.v1 - L.v1;
+    const double delta = 0.1 * ct;
+    double l1 = fabs(unt - ct), l2 = fabs(unt), l4 = fabs(unt + ct);
+    if (l1 < delta) l1 = (l1 * l1 + delta * delta) / (2 * delta);
+    if (l4 < delta) l4 = (l4 * l4 + delta * delta) / (2 * delta);
+    const double a1 = (dp - rt * ct * dun) / (2 * c2);
+    const double a2 = drho - dp / c2;
+    const double a4 = (dp + rt * ct * dun) / (2 * c2);
+    const double s1 = l1 * a1, s2 = l2 * a2, s4 = l4 * a4, ss = l2 * rt;
+    const double st0 = dv0 - dun * n[0], st1 = dv1 - dun * n[1];  // tangential velocity jump
+    double d[4];
+    d[0] = s1 + s2 + s4;
+    d[1] = s1 * (ut0 - ct * n[0]) + s2 * ut0 + s4 * (ut0 + ct * n[0]) + ss * st0;
+    d[2] = s1 * (ut1 - ct * n[1]) + s2 * ut1 + s4 * (ut1 + ct * n[1]) + ss * st1;
+    d[3] = s1 * (Ht - ct * unt) + s2 * 0.5 * qq + s4 * (Ht + ct * unt) + ss * (ut0 * st0 + ut1 * st1);
+    const double fL[4] = {L.rho * vnL, L.mom0 * vnL + L.p * n[0], L.mom1 * vnL + L.p * n[1], vnL * (L.rhoE + L.p)};
+    const double fR[4] = {R.rho * vnR, R.mom0 * vnR + R.p * n[0], R.mom1 * vnR + R.p * n[1], vnR * (R.rhoE + R.p)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) f[k] = 0.5 * (fL[k] + fR[k]) - 0.5 * d[k];
+  }
+
+  // the convective numerical flux the discretization selects
+  __device__ static inline void conv_sel(const PhysParams& pp, const double* uL, const double* uR, const double* n,
+                                         double* f) {
+    if (pp.ns_flux == ICX_FLUX_ROE) roe(pp, uL, uR, n, f);
+    else conv(pp, uL, uR, n, f);
+  }
+
+  // exterior state of the PDE-level boundary kinds (apply_bc,
+  // navier_stokes.hpp:976-1189). Slip wall: density and energy of the
+  // interior, momentum mirrored about the wall. No-slip isothermal wall: the
+  // interior density at rest with the wall temperature bval[0]. WALL_GENERAL:
+  // the no-slip isothermal wall for a viscous discretization, else the slip
+  // wall. Riemann (characteristic, Carlson NASA/TM-2011-217181): Riemann
+  // invariants of the interior and the free stream, restated with the
+  // reference's branches (its supersonic-outflow branch assigns a shadowing
+  // local and so changes nothing; inflow takes R+ from the free stream),
+  // then the boundary state from (rho, v, p).
+  __device__ static inline void apply_bc(const PhysParams& pp, const double* uL, const double* n, int bct,
+                                         const double* bval, double* uR) {
+    const double gam = pp.gamma;
+    const double cp = gam / (gam - 1) * pp.Rgas;  // T_coeff with unit reference parameters
+    NSState L = ns_state(pp, uL);
+    if (bct == ICX_BC_WALL_GENERAL) bct = pp.ns_viscous_wall ? ICX_BC_NO_SLIP_ISOTHERMAL : ICX_BC_SLIP_WALL;
+    if (bct == ICX_BC_SLIP_WALL) {
+      const double mn = L.mom0 * n[0] + L.mom1 * n[1];
+      uR[0] = uL[0];
+      uR[1] = L.mom0 - 2 * mn * n[0];
+      uR[2] = L.mom1 - 2 * mn * n[1];
+      uR[3] = uL[3];
+    } else if (bct == ICX_BC_NO_SLIP_ISOTHERMAL) {
+      const double rho = fmax(1e-14, L.rho);
+      const double p = fmax(1e-12, rho * (gam - 1) / gam * cp * bval[0]);
+      uR[0] = rho;
+      uR[1] = 0.0;
+      uR[2] = 0.0;
+      uR[3] = rho * (p / (gam - 1) / rho);
+    } else {  // ICX_BC_RIEMANN
+      const double rho_o = fmax(1e-14, pp.fs_rho);
+      const double p_o = fmax(1e-12, rho_o * (gam - 1) / gam * cp * pp.fs_T);
+      const double c_o = sqrt(gam * p_o / rho_o);
+      const double vn_i = L.v0 * n[0] + L.v1 * n[1];
+      const double vn_o = pp.fs_u[0] * n[0] + pp.fs_u[1] * n[1];
+      const double mach_n = vn_i / L.c;
+      double rplus = vn_i + 2 * L.c / (gam - 1);
+      const double rminus = vn_o - 2 * c_o / (gam - 1);
+      if (mach_n < 0) rplus = vn_o + 2 * c_o / (gam - 1);
+      const double ub = 0.5 * (rplus + rminus);
+      const double cb = 0.25 * (gam - 1) * (rplus - rminus);
+      const double vb0 = L.v0 + (ub - vn_i) * n[0], vb1 = L.v1 + (ub - vn_i) * n[1];
+      const double sb = L.c * L.c / (gam * pow(L.rho, gam - 1));
+      const double rhob = pow(cb * cb / (gam * sb), 1.0 / (gam - 1));
+      const double pb = rhob * cb * cb / gam;
+      const double rho = fmax(1e-14, rhob), p = fmax(1e-12, pb);
+      uR[0] = rho;
+      uR[1] = vb0 * rho;
+      uR[2] = vb1 * rho;
+      uR[3] = rho * (p / (gam - 1) / rho + 0.5 * (vb0 * vb0 + vb1 * vb1));
+    }
+  }
+  static constexpr bool has_pde_bcs = true;
 
   // viscous normal flux; the energy term is mu*gamma/Pr * dE/dx_j n_j
   __device__ static inline void diff(const PhysParams& pp, const double* u, const double* g, const double* n,

@@ -88,7 +88,7 @@ def ns_mms_params(gamma=1.4, Pr=0.72, mu=0.01, mach=0.3, A=0.1, u0=1.0, v0=0.5):
 
 
 def ns_mms_config(nx=128, ny=128, p=3, geo_order=2, seed=4321, device=0, perturb=0.05, interior_penalty=True,
-                  state_noise=1e-3, mu=0.01):
+                  state_noise=1e-3, mu=0.01, conv_flux=FLUX_VANLEER):
     prm = ns_mms_params(mu=mu)
     ctx = Context(device)
     ctx.mesh_uniform((nx, ny), (0.0, 0.0), (1.0, 1.0), geo_order, (DIRICHLET,) * 4, (0,) * 4)
@@ -97,7 +97,7 @@ def ns_mms_config(nx=128, ny=128, p=3, geo_order=2, seed=4321, device=0, perturb
         coords = perturb_smooth(coords, (nx, ny), perturb, seed)
     ctx.set_coords(coords)
     ctx.fespace(p)
-    ctx.disc_navier_stokes(prm[0], prm[1], prm[2], FLUX_VANLEER)
+    ctx.disc_navier_stokes(prm[0], prm[1], prm[2], conv_flux)
     ctx.disc_options(interior_penalty, 0.0)
     user = C.cast(prm, C.c_void_p)
     ctx.dirichlet(0, workload_fn("ns_mms_state"), user)
@@ -114,8 +114,8 @@ def ns_mms_config(nx=128, ny=128, p=3, geo_order=2, seed=4321, device=0, perturb
         st[k] = out[:]
     rng = np.random.default_rng(seed)
     st *= 1.0 + state_noise * rng.standard_normal(st.shape)
-    return Workload(ctx, coords, np.ascontiguousarray(st.reshape(-1)), dict(prm=list(prm), p=p, g=geo_order),
-                    "ns_mms", [prm])
+    return Workload(ctx, coords, np.ascontiguousarray(st.reshape(-1)),
+                    dict(prm=list(prm), p=p, g=geo_order, conv_flux=conv_flux), "ns_mms", [prm])
 
 
 def ns_mms_strip_config(plan, p=3, geo_order=2, seed=4321, device=0, perturb=0.05, interior_penalty=True,

@@ -39,6 +39,12 @@ typedef int icx_status;
 #define ICX_BC_NEUMANN 2
 #define ICX_BC_DIRICHLET 3
 #define ICX_BC_EXTRAPOLATION 4
+/* Navier-Stokes PDE-level kinds (navier_stokes.hpp:976-1189; the Burgers
+ * fluxes implement none, so such faces contribute nothing there) */
+#define ICX_BC_RIEMANN 5            /* characteristic far field against the free stream */
+#define ICX_BC_NO_SLIP_ISOTHERMAL 6 /* wall at rest at the temperature of its bcflag */
+#define ICX_BC_SLIP_WALL 7          /* inviscid wall: momentum mirrored */
+#define ICX_BC_WALL_GENERAL 8       /* no-slip isothermal when viscous (mu > 0), else slip */
 #define ICX_BC_SPACETIME_PAST 11
 #define ICX_BC_SPACETIME_FUTURE 12
 #define ICX_BC_INTERIOR 13
@@ -49,6 +55,8 @@ typedef int icx_status;
 #define ICX_PDE_NAVIER_STOKES 1
 #define ICX_FLUX_UPWIND 0  /* BurgersUpwind (burgers.hpp:114-170) */
 #define ICX_FLUX_VANLEER 1 /* navier_stokes::VanLeer (navier_stokes.hpp:776-864) */
+#define ICX_FLUX_ROE 2     /* Roe's approximate Riemann solver with Harten's entropy fix (no reference
+                              counterpart: the reference's Navier-Stokes has only Van Leer) */
 
 /* host callback x[2] -> out[neq]: the reference's std::function<void(const T*, T*)>
  * dirichlet_callbacks / neumann_callbacks / user_source (CL:145-160) */
@@ -118,6 +126,15 @@ icx_status icx_disc_spacetime_burgers(icx_ctx* ctx, double mu, double a, double 
  * again after those. */
 icx_status icx_spacetime_connect(icx_ctx* ctx, const icx_ctx* past, const double* d_u_past);
 icx_status icx_disc_navier_stokes(icx_ctx* ctx, double gamma, double Pr, double mu, int conv_flux);
+/* data of the Navier-Stokes PDE-level boundaries (Physics::isothermal_temperatures
+ * and Physics::free_stream, navier_stokes.hpp:679-682): wall temperatures
+ * indexed by the faces' bcflag (n_walls <= 8), the free stream's density,
+ * velocity magnitude, unit direction and temperature, and the gas constant
+ * of the ideal-gas equation of state (EoS::Rgas, default 287.052874). The
+ * temperature unit is the equation of state's: p = rho Rgas T with unit
+ * reference parameters. */
+icx_status icx_disc_ns_boundary(icx_ctx* ctx, const double* wall_temperatures, int n_walls, double rho_inf,
+                                double u_inf, const double u_direction[2], double T_inf, double Rgas);
 /* public members interior_penalty and sigma_ic (CL:137-143) */
 icx_status icx_disc_options(icx_ctx* ctx, int interior_penalty, double sigma_ic);
 icx_status icx_disc_dirichlet(icx_ctx* ctx, int bcflag, icx_point_fn fn, void* user);

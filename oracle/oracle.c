@@ -522,12 +522,102 @@ static void ns_diff(const orc_problem* pb, const double* u, const double* g, con
   }
 }
 
+/* Roe's approximate Riemann solver (Roe, J. Comput. Phys. 43, 1981) with
+ * Harten's entropy fix on the acoustic waves, |l| < d -> (l^2 + d^2)/(2d),
+ * d = 0.1 c of the Roe average: (F(uL).n + F(uR).n)/2 minus half the sum of
+ * |lambda_k| alpha_k r_k over the two acoustic waves, the entropy wave and
+ * the shear wave. The reference has no Roe flux; this follows the published
+ * algorithm. */
+static void ns_roe(const orc_problem* pb, const double* uL, const double* uR, const double n[2], double* f) {
+  ns_state L, R;
+  ns_thermo(pb, uL, &L);
+  ns_thermo(pb, uR, &R);
+  double g = pb->gamma;
+  double vnL = L.vel[0] * n[0] + L.vel[1] * n[1], vnR = R.vel[0] * n[0] + R.vel[1] * n[1];
+  double HL = L.E + L.p / L.rho, HR = R.E + R.p / R.rho;
+  double wL = sqrt(L.rho), wR = sqrt(R.rho);
+  double rho_a = wL * wR;
+  double u_a[2], q2 = 0.0;
+  for (int d = 0; d < 2; ++d) {
+    u_a[d] = (wL * L.vel[d] + wR * R.vel[d]) / (wL + wR);
+    q2 += u_a[d] * u_a[d];
+  }
+  double H_a = (wL * HL + wR * HR) / (wL + wR);
+  double c2 = fmax((g - 1) * (H_a - 0.5 * q2), 1e-14), c_a = sqrt(c2);
+  double un_a = u_a[0] * n[0] + u_a[1] * n[1];
+  double drho = R.rho - L.rho, dp = R.p - L.p, dun = vnR - vnL;
+  double dvt[2];
+  for (int d = 0; d < 2; ++d) dvt[d] = (R.vel[d] - L.vel[d]) - dun * n[d];
+  double lam[3] = {fabs(un_a - c_a), fabs(un_a), fabs(un_a + c_a)};
+  double delta = 0.1 * c_a;
+  for (int k = 0; k < 3; k += 2)
+    if (lam[k] < delta) lam[k] = (lam[k] * lam[k] + delta * delta) / (2 * delta);
+  double al_m = (dp - rho_a * c_a * dun) / (2 * c2), al_0 = drho - dp / c2, al_p = (dp + rho_a * c_a * dun) / (2 * c2);
+  double diss[4];
+  diss[0] = lam[0] * al_m + lam[1] * al_0 + lam[2] * al_p;
+  for (int d = 0; d < 2; ++d)
+    diss[1 + d] = lam[0] * al_m * (u_a[d] - c_a * n[d]) + lam[1] * al_0 * u_a[d] + lam[2] * al_p * (u_a[d] + c_a * n[d]) +
+                  lam[1] * rho_a * dvt[d];
+  diss[3] = lam[0] * al_m * (H_a - c_a * un_a) + lam[1] * al_0 * 0.5 * q2 + lam[2] * al_p * (H_a + c_a * un_a) +
+            lam[1] * rho_a * (u_a[0] * dvt[0] + u_a[1] * dvt[1]);
+  double FL[4] = {L.rho * vnL, L.mom[0] * vnL + L.p * n[0], L.mom[1] * vnL + L.p * n[1], vnL * (L.rhoE + L.p)};
+  double FR[4] = {R.rho * vnR, R.mom[0] * vnR + R.p * n[0], R.mom[1] * vnR + R.p * n[1], vnR * (R.rhoE + R.p)};
+  for (int k = 0; k < 4; ++k) f[k] = 0.5 * (FL[k] + FR[k]) - 0.5 * diss[k];
+}
+
+/* exterior state of the Navier-Stokes PDE-level boundaries (apply_bc,
+ * NS:976-1189), unit reference parameters, T_coeff = cp = gamma/(gamma-1) Rgas */
+static void ns_apply_bc(const orc_problem* pb, const double* uL, const double n[2], int bct, int flag, double* uR) {
+  ns_state L;
+  ns_thermo(pb, uL, &L);
+  double g = pb->gamma, cp = g / (g - 1) * NS_RGAS;
+  if (bct == ORC_BC_WALL_GENERAL) bct = pb->ns_mu != 0.0 ? ORC_BC_NO_SLIP_ISOTHERMAL : ORC_BC_SLIP_WALL;
+  if (bct == ORC_BC_SLIP_WALL) { /* NS:997-1017 */
+    double mn = L.mom[0] * n[0] + L.mom[1] * n[1];
+    uR[0] = uL[0];
+    uR[3] = uL[3];
+    for (int d = 0; d < 2; ++d) uR[1 + d] = L.mom[d] - 2 * mn * n[d];
+  } else if (bct == ORC_BC_NO_SLIP_ISOTHERMAL) { /* NS:1018-1042: (rho, 0, T_wall) in RHO_U_T */
+    double rho = fmax(1e-14, L.rho);
+    double p = fmax(1e-12, rho * (g - 1) / g * cp * pb->wall_T[flag]);
+    double e = p * 1.0 * 1.0 / (g - 1) / rho;
+    uR[0] = rho;
+    uR[1] = uR[2] = 0.0;
+    uR[3] = rho * (e + 0.5 * 1.0 * 0.0);
+  } else { /* RIEMANN, NS:1043-1128 (Carlson's characteristic state) */
+    double rho_o = fmax(1e-14, pb->fs_rho);
+    double v_o[2] = {pb->fs_dir[0] * pb->fs_u_inf, pb->fs_dir[1] * pb->fs_u_inf};
+    double p_o = fmax(1e-12, rho_o * (g - 1) / g * cp * pb->fs_T);
+    double c_o = sqrt((g * 1.0 * p_o) / rho_o);
+    double vn_i = L.vel[0] * n[0] + L.vel[1] * n[1];
+    double vn_o = v_o[0] * n[0] + v_o[1] * n[1];
+    double mach_n = vn_i / L.c;
+    double Rp = vn_i + 2 * L.c / (g - 1);
+    double Rm = vn_o - 2 * c_o / (g - 1);
+    /* the reference's supersonic-outflow branch declares a new local and leaves Rm as it is */
+    if (!(mach_n > 0) && mach_n < 0) Rp = vn_o + 2 * c_o / (g - 1);
+    double Ub = 0.5 * (Rp + Rm);
+    double cb = 0.25 * (g - 1) * (Rp - Rm);
+    double vb[2] = {L.vel[0] + (Ub - vn_i) * n[0], L.vel[1] + (Ub - vn_i) * n[1]};
+    double sb = L.c * L.c / (g * pow(L.rho, g - 1));
+    double rho_b = pow(cb * cb / (g * sb), 1.0 / (g - 1));
+    double p_b = rho_b * cb * cb / g;
+    double rho = fmax(1e-14, rho_b), p = fmax(1e-12, p_b);
+    double e = p * 1.0 * 1.0 / (g - 1) / rho;
+    double vv = vb[0] * vb[0] + vb[1] * vb[1];
+    uR[0] = rho;
+    for (int d = 0; d < 2; ++d) uR[1 + d] = vb[d] * rho;
+    uR[3] = rho * (e + 0.5 * 1.0 * vv);
+  }
+}
+
 static void phys_flux(const orc_problem* pb, const double* u, const double* g, double F[][2]) {
   if (pb->pde == 0) burgers_flux(pb, u, g, F);
   else ns_flux(pb, u, g, F);
 }
 static void conv_flux(const orc_problem* pb, const double* uL, const double* uR, const double n[2], double* f) {
   if (pb->pde == 0) burgers_upwind(pb, uL, uR, n, f);
+  else if (pb->ns_flux == 2) ns_roe(pb, uL, uR, n, f);
   else ns_vanleer(pb, uL, uR, n, f);
 }
 static void diff_flux(const orc_problem* pb, const double* u, const double* g, const double n[2], double* f) {
@@ -791,10 +881,19 @@ static int boundary_integral(const disc* D, const int* F, const double* uL, doub
     double BL[MAXNB], dBL[2 * MAXNB], ul[MAXEQ], gl[2 * MAXEQ];
     side_eval(D, &GL, fq.xiL, uL, 0, BL, dBL, ul, gl, NULL);
     double fadv[MAXEQ] = {0}, fvis[MAXEQ] = {0};
-    if (bct == ORC_BC_DIRICHLET) {
-      if (flag < 0 || flag >= pb->n_dirichlet) return -2;
+    int pde_bc = pb->pde == 1 && bct >= ORC_BC_RIEMANN && bct <= ORC_BC_WALL_GENERAL;
+    if (bct == ORC_BC_DIRICHLET || pde_bc) {
+      /* PDE-level kinds take the exterior state from apply_bc and then the
+       * same one-sided DDG flux as a Dirichlet face (CL:1043-1130) */
       double ud[MAXEQ] = {0};
-      pb->dirichlet[flag](fq.x, ud, pb->dirichlet_user[flag]);
+      if (pde_bc) {
+        int iso = bct == ORC_BC_NO_SLIP_ISOTHERMAL || (bct == ORC_BC_WALL_GENERAL && pb->ns_mu != 0.0);
+        if (iso && (flag < 0 || flag >= pb->n_wall)) return -2;
+        ns_apply_bc(pb, ul, fq.n, bct, flag, ud);
+      } else {
+        if (flag < 0 || flag >= pb->n_dirichlet) return -2;
+        pb->dirichlet[flag](fq.x, ud, pb->dirichlet_user[flag]);
+      }
       conv_flux(pb, ul, ud, fq.n, fadv);
       double h = 0.0;
       for (int d = 0; d < 2; ++d) h += fabs(fq.n[d] * (fq.x[d] - cL[d]));
@@ -829,7 +928,7 @@ static int boundary_integral(const disc* D, const int* F, const double* uL, doub
     } else if (pb->pde == 0) {
       /* Burgers implements no PDE-level boundary conditions: no contribution */
     } else {
-      return -3; /* PDE-level Navier-Stokes boundary conditions are not restated */
+      return -3; /* inlet / outlet: the reference implements neither */
     }
   }
   return 0;
@@ -1544,4 +1643,19 @@ int orc_basis_node_coords(const orc_problem* pb, const double* coord, double* xy
       }
   }
   return 0;
+}
+
+/* pointwise fluxes, exported for the consistency tests: the convective
+ * numerical flux of the problem (Van Leer or Roe for Navier-Stokes, upwind
+ * for Burgers) and the physical flux F[eq][dim] */
+void orc_numerical_flux(const orc_problem* pb, const double* uL, const double* uR, const double* n, double* f) {
+  conv_flux(pb, uL, uR, n, f);
+}
+void orc_physical_flux(const orc_problem* pb, const double* u, const double* g, double* F) {
+  phys_flux(pb, u, g, (double(*)[2])F);
+}
+/* exterior state of a Navier-Stokes PDE-level boundary at one point */
+void orc_ns_boundary_state(const orc_problem* pb, const double* uL, const double* n, int bctype, int bcflag,
+                           double* uR) {
+  ns_apply_bc(pb, uL, n, bctype, bcflag, uR);
 }

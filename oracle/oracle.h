@@ -43,12 +43,20 @@ typedef struct orc_problem {
   void* source_user;
   int spacetime;        /* Burgers in (x, t): SpacetimeBurgersFlux/Upwind/Diffusion, no diffusion along t */
   int basis;            /* solution basis: 0 Lagrange (equispaced nodes), 1 Legendre */
+  /* Navier-Stokes: convective flux (0 or 1 Van Leer, 2 Roe) and the data of
+   * the PDE-level boundaries (Physics::isothermal_temperatures and
+   * Physics::free_stream, navier_stokes.hpp:679-682) */
+  int ns_flux;
+  int n_wall;
+  double wall_T[8];
+  double fs_rho, fs_u_inf, fs_dir[2], fs_T;
 } orc_problem;
 
 /* reference BOUNDARY_CONDITIONS enumerators used here */
 enum {
   ORC_BC_PERIODIC = 0, ORC_BC_PARALLEL_COM = 1, ORC_BC_NEUMANN = 2, ORC_BC_DIRICHLET = 3,
-  ORC_BC_EXTRAPOLATION = 4, ORC_BC_SPACETIME_PAST = 11, ORC_BC_SPACETIME_FUTURE = 12, ORC_BC_INTERIOR = 13
+  ORC_BC_EXTRAPOLATION = 4, ORC_BC_RIEMANN = 5, ORC_BC_NO_SLIP_ISOTHERMAL = 6, ORC_BC_SLIP_WALL = 7,
+  ORC_BC_WALL_GENERAL = 8, ORC_BC_SPACETIME_PAST = 11, ORC_BC_SPACETIME_FUTURE = 12, ORC_BC_INTERIOR = 13
 };
 
 int orc_n_nodes(const orc_problem* pb);
@@ -91,6 +99,14 @@ void orc_wl_sine_product(const double* x, double* out, void* user);
 void orc_wl_oblique_step(const double* x, double* out, void* user);
 void orc_wl_ns_mms_state(const double* x, double* out, void* user);
 void orc_wl_ns_mms_source(const double* x, double* out, void* user);
+
+/* pointwise fluxes (consistency tests): convective numerical flux of the
+ * problem's PDE, physical flux F[eq][2] at state u with gradient g[eq][2],
+ * and the exterior state of a Navier-Stokes PDE-level boundary */
+void orc_numerical_flux(const orc_problem* pb, const double* uL, const double* uR, const double* n, double* f);
+void orc_physical_flux(const orc_problem* pb, const double* u, const double* g, double* F);
+void orc_ns_boundary_state(const orc_problem* pb, const double* uL, const double* n, int bctype, int bcflag,
+                           double* uR);
 
 /* element mass matrices [E][nb][nb] (finite_element.hpp:587-610) */
 int orc_mass_matrices(const orc_problem* pb, const double* coord, double* M);

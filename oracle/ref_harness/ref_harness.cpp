@@ -67,6 +67,10 @@ struct ref_problem {
   void* source_user;
   int spacetime;        // Burgers in (x, t): SpacetimeBurgersFlux / Upwind / Diffusion
   int basis;            // FESPACE_BASIS_TYPE of the solution space (0 LAGRANGE, 1 LEGENDRE)
+  int ns_flux;          // 0 or 1: VanLeer (the reference has no other Navier-Stokes convective flux)
+  int n_wall;           // Physics::isothermal_temperatures
+  double wall_T[8];
+  double fs_rho, fs_u_inf, fs_dir[2], fs_T;  // Physics::free_stream
 };
 }
 
@@ -156,17 +160,31 @@ int with_disc(const ref_problem& pb, const double* coord, Body&& body) {
     add_callbacks(disc, pb);
     return body(fespace, disc, std::integral_constant<std::size_t, 1>{});
   } else {
+    if (pb.ns_flux > 1) return -4;  // no Roe flux in the reference
     navier_stokes::ReferenceParameters<T> ref{};
     navier_stokes::CaloricallyPerfectEoS<T, ndim> eos{};
     eos.gamma = pb.gamma;
     navier_stokes::constant_viscosity<T> visc{pb.ns_mu};
     navier_stokes::Physics<T, ndim, navier_stokes::CaloricallyPerfectEoS<T, ndim>> physics{ref, eos, visc, pb.Pr};
-    navier_stokes::Flux flux{physics, std::true_type{}};
-    navier_stokes::VanLeer numflux{physics};
-    navier_stokes::DiffusionFlux dflux{physics, std::true_type{}};
-    ConservationLawDDG disc{std::move(flux), std::move(numflux), std::move(dflux)};
-    add_callbacks(disc, pb);
-    return body(fespace, disc, std::integral_constant<std::size_t, 4>{});
+    // boundary data before the flux objects copy the physics
+    physics.isothermal_temperatures.assign(pb.wall_T, pb.wall_T + pb.n_wall);
+    physics.free_stream.rho_inf = pb.fs_rho;
+    physics.free_stream.u_inf = pb.fs_u_inf;
+    physics.free_stream.u_direction[0] = pb.fs_dir[0];
+    physics.free_stream.u_direction[1] = pb.fs_dir[1];
+    physics.free_stream.temp_inf = pb.fs_T;
+    // the full Navier-Stokes flux for a viscous problem, the Euler one otherwise
+    // (its WALL_GENERAL is the slip wall)
+    auto run = [&](auto full_ns) {
+      navier_stokes::Flux flux{physics, full_ns};
+      navier_stokes::VanLeer numflux{physics};
+      navier_stokes::DiffusionFlux dflux{physics, full_ns};
+      ConservationLawDDG disc{std::move(flux), std::move(numflux), std::move(dflux)};
+      add_callbacks(disc, pb);
+      return body(fespace, disc, std::integral_constant<std::size_t, 4>{});
+    };
+    if (pb.ns_mu != 0.0) return run(std::true_type{});
+    return run(std::false_type{});
   }
 }
 

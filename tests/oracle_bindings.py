@@ -26,6 +26,8 @@ class Problem(C.Structure):
         ("n_dirichlet", C.c_int), ("dirichlet", POINT_FN * 8), ("dirichlet_user", C.c_void_p * 8),
         ("n_neumann", C.c_int), ("neumann", POINT_FN * 8), ("neumann_user", C.c_void_p * 8),
         ("source", POINT_FN), ("source_user", C.c_void_p), ("spacetime", C.c_int), ("basis", C.c_int),
+        ("ns_flux", C.c_int), ("n_wall", C.c_int), ("wall_T", C.c_double * 8),
+        ("fs_rho", C.c_double), ("fs_u_inf", C.c_double), ("fs_dir", C.c_double * 2), ("fs_T", C.c_double),
     ]
 
 

@@ -25,11 +25,16 @@ def ns_mms_params(gamma=1.4, Pr=0.72, mu=0.01, mach=0.3, A=0.1, u0=1.0, v0=0.5):
 class Spec:
     def __init__(self, pde=BURGERS, nx=4, ny=3, g=2, p=2, bct=(3, 3, 3, 3), bcf=(0, 0, 0, 0), ip=False,
                  sigma_ic=0.0, mu=0.01, a=(0.3, -0.2), b=(1.0, 0.5), perturb=0.1, seed=7,
-                 dirichlet=None, neumann=None, source=False, spacetime=False, basis=0):
+                 dirichlet=None, neumann=None, source=False, spacetime=False, basis=0, ns_flux=1, ns_mu=0.01,
+                 walls=(), free_stream=None):
         self.pde, self.nx, self.ny, self.g, self.p = pde, nx, ny, g, p
         self.bct, self.bcf, self.ip, self.sigma_ic = tuple(bct), tuple(bcf), ip, sigma_ic
         self.spacetime = spacetime
         self.basis = basis
+        # Navier-Stokes: convective flux (1 Van Leer, 2 Roe), viscosity, wall
+        # temperatures per bcflag, free stream (rho, |u|, (dx, dy), T)
+        self.ns_flux, self.ns_mu, self.walls = ns_flux, ns_mu, tuple(walls)
+        self.free_stream = free_stream
         if spacetime:  # Burgers in (x, t): the time component of the flux is u
             a, b = (a[0], 1.0), (b[0], 0.0)
         self.mu, self.a, self.b = mu, a, b
@@ -122,7 +127,13 @@ class Spec:
         pb.b[:] = list(self.b)
         pb.spacetime = int(self.spacetime)
         pb.basis = int(self.basis)
-        pb.gamma, pb.Pr, pb.ns_mu = 1.4, 0.72, 0.01
+        pb.gamma, pb.Pr, pb.ns_mu = 1.4, 0.72, self.ns_mu
+        pb.ns_flux = self.ns_flux
+        pb.n_wall = len(self.walls)
+        for i, t in enumerate(self.walls):
+            pb.wall_T[i] = t
+        if self.free_stream is not None:
+            pb.fs_rho, pb.fs_u_inf, (pb.fs_dir[0], pb.fs_dir[1]), pb.fs_T = self.free_stream
         pb.n_dirichlet = len(self.dirichlet)
         for i, (name, prm) in enumerate(self.dirichlet):
             arr = self._params(name, prm)
@@ -153,7 +164,10 @@ class Spec:
         elif self.pde == BURGERS:
             ctx.disc_burgers(self.mu, self.a, self.b)
         else:
-            ctx.disc_navier_stokes(1.4, 0.72, 0.01, ib.FLUX_VANLEER)
+            ctx.disc_navier_stokes(1.4, 0.72, self.ns_mu, self.ns_flux)
+            if self.walls or self.free_stream is not None:
+                fs = self.free_stream or (1.0, 0.0, (1.0, 0.0), 1.0)
+                ctx.disc_ns_boundary(self.walls, fs[0], fs[1], fs[2], fs[3])
         ctx.disc_options(self.ip, self.sigma_ic)
         for i, (name, prm) in enumerate(self.dirichlet):
             ctx.dirichlet(i, ib.workload_fn(name), C.cast(self._params(name, prm), C.c_void_p))
