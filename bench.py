@@ -265,6 +265,73 @@ def batched_bench(torch, dev, n_problems):
             "speedup": t_seq / t_batch if t_batch > 0 else None, "max_state_rel_diff": worst, "groups": its}
 
 
+def jacobian_work(L):
+    """algorithmic bytes (BSR values written once, u read) and an FP64 flop
+    count of one FD Jacobian as the element kernel computes it: per element
+    and perturbed DOF, the four faces' point states and numerical fluxes
+    (420 flops per Navier-Stokes face flux, 28 per state update) and their
+    contraction into the two blocks a face column touches; per element the
+    flux-level volume FD (1 + 3 neq physical fluxes of 160 flops per point)
+    and its contraction into the diagonal block (12 flops per entry and point)"""
+    E, nb, neq, nqv, nqf = L.n_elem, L.nbasis, L.neq, L.nq_vol, L.nq_face
+    bs = nb * neq
+    face = bs * 4 * nqf * (28 + 420) + 2 * nb * neq * bs * nqf * 4 * 2
+    vol = nqv * (1 + 3 * neq) * 160 + bs * bs * nqv * 12
+    bytes_ = L.nnz_blocks * bs * bs * 8 + L.n_dof * 8
+    return bytes_, E * (face + vol)
+
+
+def jacobian_bench(torch, dev, wl, hbm_gbs, cpu=True):
+    """FD Jacobian (form_petsc_jacobian_fd) of the residual workload into BSR:
+    mean device time of 5 launches after 2 untimed ones (CUDA events), the
+    BSR bytes it writes, GB/s against the measured HBM peak, FP64 flops; and
+    the reference's own form_petsc_jacobian_fd on one host core, timed on a
+    32 x 32 sample of the same discretization and scaled by the element count
+    (its cost is linear in the elements)"""
+    L = wl.ctx.layout
+    bs = L.block_size
+    u = torch.from_numpy(wl.u0).to(dev)
+    res = torch.empty_like(u)
+    vals = torch.empty(L.nnz_blocks * bs * bs, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        wl.ctx.form_jacobian_fd(u, res, vals)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(5):
+        wl.ctx.form_jacobian_fd(u, res, vals)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / 5
+    nbytes, flops = jacobian_work(L)
+    out = {"workload": "ns_mms 128x128 p3 (the residual workload)", "ms": ms, "bsr_bytes": L.nnz_blocks * bs * bs * 8,
+           "algorithmic_bytes": nbytes, "GBs": nbytes / ms / 1e6, "frac_of_hbm": nbytes / ms / 1e6 / hbm_gbs,
+           "fp64_flops": flops, "fp64_tflops": flops / ms / 1e9}
+    del vals
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_bindings as ob
+        if ob.ref_available():
+            from specs import NS, Spec
+            n = 32
+            spec = Spec(pde=NS, nx=n, ny=n, p=3, g=2, ip=True, source=True, perturb=0.05, seed=4321)
+            pb = spec.oracle_problem()
+            c = spec.coords()
+            us = spec.mms_state(c)
+            rp, ci = ob.bsr_pattern(pb)
+            hv = np.zeros(len(ci) * bs * bs)
+            sec = C.c_double()
+            rc = ob.ref().fn("time_jacobian_fd")(C.byref(pb), ob._ptr(c), ob._ptr(us), ob._ptr(rp), ob._ptr(ci),
+                                                 ob._ptr(hv), 1, C.byref(sec))
+            if rc == 0:
+                scale = L.n_elem / (n * n)
+                out["cpu_reference"] = {"ms": sec.value * 1e3 * scale, "cores": 1,
+                                        "sample": f"{n}x{n} p3 (same physics), 1 call after a warm-up, x{scale:g} "
+                                                  "elements (linear in the element count)"}
+                out["speedup_vs_cpu_reference"] = sec.value * 1e3 * scale / ms
+    return out
+
+
 def newton_bench(torch, dev, tune=True):
     """Newton solve time to |r| <= 1e-10 (FP64 residual), all-FP64 vs mixed
     precision (FP32 Jacobian and preconditioner copies): 32 x 32 viscous
@@ -642,6 +709,8 @@ def run_ours(a):
                                         "sample": "3 full 128x128 p3 residuals, 1 thread (reference is serial)"}
             else:
                 line["cpu_baseline"] = None
+        if ws == 1:
+            line["jacobian"] = jacobian_bench(torch, dev, wl, hbm, not a.no_cpu_baseline)
         if not a.no_newton and ws == 1:
             line["newton"] = newton_bench(torch, dev, not a.no_tune)
         if a.batched and ws == 1:

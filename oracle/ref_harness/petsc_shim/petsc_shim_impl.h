@@ -23,6 +23,13 @@ typedef enum { NOT_SET_VALUES, INSERT_VALUES, ADD_VALUES } InsertMode;
 struct _p_Mat {
   PetscInt m = 0, n = 0;
   std::map<std::pair<PetscInt, PetscInt>, double> v;
+  // preallocated block storage (set by the timing harness): entry (i, j) goes
+  // to block (i / bs, j / bs) of a block-row pattern, found by a scan of the
+  // row's few blocks, like MatSetValues into a preallocated PETSc BAIJ matrix
+  double* bsr_vals = nullptr;
+  const int* bsr_rowptr = nullptr;
+  const int* bsr_colidx = nullptr;
+  int bs = 0;
 };
 typedef _p_Mat* Mat;
 struct _p_Vec {
@@ -39,6 +46,22 @@ inline PetscErrorCode MatDestroy(Mat* A) { delete *A; *A = nullptr; return 0; }
 inline PetscErrorCode MatGetOwnershipRange(Mat, PetscInt* b, PetscInt* e) { *b = 0; *e = 0; return 0; }
 inline PetscErrorCode MatSetValues(Mat A, PetscInt m, const PetscInt* im, PetscInt n, const PetscInt* in,
                                    const PetscScalar* vals, InsertMode mode) {
+  if (A->bsr_vals) {
+    const int bs = A->bs;
+    for (PetscInt i = 0; i < m; ++i) {
+      const int ib = im[i] / bs, ir = im[i] % bs;
+      for (PetscInt j = 0; j < n; ++j) {
+        const int jb = in[j] / bs;
+        int k = A->bsr_rowptr[ib];
+        while (k < A->bsr_rowptr[ib + 1] && A->bsr_colidx[k] != jb) ++k;
+        if (k == A->bsr_rowptr[ib + 1]) continue;  // outside the preallocated pattern
+        double& dst = A->bsr_vals[((std::size_t)k * bs + ir) * bs + in[j] % bs];
+        if (mode == ADD_VALUES) dst += vals[i * n + j];
+        else dst = vals[i * n + j];
+      }
+    }
+    return 0;
+  }
   for (PetscInt i = 0; i < m; ++i)
     for (PetscInt j = 0; j < n; ++j) {
       auto key = std::make_pair(im[i], in[j]);

@@ -378,6 +378,43 @@ int ref_mdg_jacobian_dense(const ref_problem* pb, const double* coord, int ntr, 
   });
 }
 
+/// time `nrep` calls of the reference's form_petsc_jacobian_fd (with its
+/// residual) into preallocated block storage of the element pattern (rowptr
+/// [E + 1], colidx: the element and its face neighbours, ascending); the
+/// values of the last call are left in vals (nnzb blocks of bs x bs)
+int ref_time_jacobian_fd(const ref_problem* pb, const double* coord, const double* u, const int* rowptr,
+                         const int* colidx, double* vals, int nrep, double* seconds) {
+  return dispatch_p(*pb, coord, [&](auto& fespace, auto& disc, auto neq_c) {
+    fe_layout_right layout{fespace.dg_map, neq_c};
+    std::size_t n = layout.size();
+    const int E = pb->nx * pb->ny;
+    const int bs = (int)(n / (std::size_t)E);
+    std::vector<T> ubuf(u, u + n);
+    std::vector<T> rbuf(n);
+    fespan uspan{ubuf.data(), layout};
+    fespan rspan{rbuf.data(), layout};
+    Mat jac;
+    MatCreate(PETSC_COMM_WORLD, &jac);
+    MatSetSizes(jac, (PetscInt)n, (PetscInt)n, PETSC_DETERMINE, PETSC_DETERMINE);
+    jac->bsr_vals = vals;
+    jac->bsr_rowptr = rowptr;
+    jac->bsr_colidx = colidx;
+    jac->bs = bs;
+    const std::size_t nv = (std::size_t)rowptr[E] * bs * bs;
+    std::fill(vals, vals + nv, 0.0);
+    solvers::form_petsc_jacobian_fd(fespace, disc, uspan, rspan, jac);  // warm-up
+    auto t0 = std::chrono::steady_clock::now();
+    for (int r = 0; r < nrep; ++r) {
+      std::fill(vals, vals + nv, 0.0);  // MatZeroEntries
+      solvers::form_petsc_jacobian_fd(fespace, disc, uspan, rspan, jac);
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    *seconds = std::chrono::duration<double>(t1 - t0).count() / std::max(nrep, 1);
+    MatDestroy(&jac);
+    return 0;
+  });
+}
+
 /// form_petsc_jacobian_fd of the reference into a dense row-major N x N
 /// matrix (small meshes only), plus the residual
 int ref_form_jacobian_dense(const ref_problem* pb, const double* coord, const double* u, double* res,
