@@ -332,6 +332,35 @@ def jacobian_bench(torch, dev, wl, hbm_gbs, cpu=True):
     return out
 
 
+def lm_bench(torch, dev, kmax=5):
+    """MDG-ICE (CorriganLM with the explicitly formed, ILU(0)-preconditioned
+    subproblem): 64 x 64 quads, p = 1 and p = 2, oblique inviscid-Burgers
+    shock on a jittered grid, all interior traces selected; wall time of
+    `kmax` LM iterations (CUDA events around the solve), the residual history
+    and the linear iterations"""
+    import iceicle_b200 as ib
+    from iceicle_b200.workloads import mdg_ice_config
+    out = {}
+    for p in (1, 2):
+        wl, traces, x0 = mdg_ice_config(n=64, p=p, device=dev.index)
+        o = ib.default_lm_options()
+        o.kmax, o.explicit_subproblem, o.gmres_rtol = kmax, 1, 1e-8
+        u = torch.from_numpy(wl.u0.copy()).to(dev)
+        x = x0.copy()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        rep = ib.lm_solve(wl.ctx, u, x, o)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        out[f"mdg_ice_64x64_p{p}"] = {
+            "s": e0.elapsed_time(e1) * 1e-3, "iterations": rep.iterations, "rejections": rep.rejections,
+            "gmres_its": rep.linear_iterations_total, "n_geo": len(x0),
+            "residual_history": list(rep.residual_history[:rep.iterations + 1])}
+        del wl
+    return out
+
+
 def newton_bench(torch, dev, tune=True):
     """Newton solve time to |r| <= 1e-10 (FP64 residual), all-FP64 vs mixed
     precision (FP32 Jacobian and preconditioner copies): 32 x 32 viscous
@@ -713,6 +742,7 @@ def run_ours(a):
             line["jacobian"] = jacobian_bench(torch, dev, wl, hbm, not a.no_cpu_baseline)
         if not a.no_newton and ws == 1:
             line["newton"] = newton_bench(torch, dev, not a.no_tune)
+            line["mdg_ice"] = lm_bench(torch, dev)
         if a.batched and ws == 1:
             line["batched"] = batched_bench(torch, dev, a.batched)
         if not a.no_learned and ws == 1:

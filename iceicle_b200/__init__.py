@@ -716,7 +716,8 @@ class LMOptions(C.Structure):
                 ("lambda_b", C.c_double), ("linesearch", C.c_int), ("ls_max_it", C.c_int),
                 ("ls_alpha_initial", C.c_double), ("ls_alpha_max", C.c_double), ("ls_alpha_min", C.c_double),
                 ("gmres_restart", C.c_int), ("gmres_max_it", C.c_int), ("gmres_rtol", C.c_double),
-                ("max_rejections", C.c_int), ("verbosity", C.c_int)]
+                ("max_rejections", C.c_int), ("verbosity", C.c_int), ("explicit_subproblem", C.c_int),
+                ("lambda_lag", C.c_double)]
 
 
 class LMReport(C.Structure):

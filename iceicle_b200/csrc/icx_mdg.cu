@@ -72,6 +72,7 @@ struct icx_mdg_state {
   double* d_ustep = nullptr;
   double* d_rwork = nullptr;
   double* d_x = nullptr;         // current geometry parameters (device copy)
+  double* d_colnorm2 = nullptr;  // length ncol: scratch of the subproblem ILU apply
   icx::KrylovBuffers kb;
   double* d_kV = nullptr;
   double* d_kw = nullptr;
@@ -79,6 +80,33 @@ struct icx_mdg_state {
   double* d_kr = nullptr;
   double* d_kdh = nullptr;
   icx::LinalgWork lw;
+  std::vector<int> h_trowptr, h_tcolidx;  // transpose pattern (host)
+  // explicitly formed LM subproblem A = J^T J + regularisation (CSR over the
+  // unknowns [u; x]) and its scalar ILU(0), level-scheduled
+  bool a_built = false;
+  long long a_nnz = 0;
+  int* d_a_rowptr = nullptr;
+  int* d_a_colidx = nullptr;
+  int* d_a_diag = nullptr;       // position of the diagonal entry of each row
+  double* d_a_vals = nullptr;
+  double* d_a_lu = nullptr;
+  std::vector<int> lo_off, up_off;  // ILU levels: rows lo_rows[lo_off[l] .. lo_off[l + 1]) etc.
+  int* d_lo_rows = nullptr;
+  int* d_up_rows = nullptr;
+  int* d_pc_err = nullptr;
+  // Laplacian and element-wise regularisation: per element the pairs
+  // (local node i, local node j, position in A) of free coordinates of two
+  // selected nodes, and per touched position the pairs that add to it
+  int npairs = 0, npos = 0;
+  int* d_pair_ptr = nullptr;     // [E + 1]
+  int* d_pair_ij = nullptr;      // [npairs][2]
+  int* d_upos = nullptr;         // [npos] positions in A
+  int* d_upos_ptr = nullptr;     // [npos + 1] into d_upos_list
+  int* d_upos_list = nullptr;    // [npairs] pair indices, ascending
+  double* d_pair_val = nullptr;  // [npairs]
+  double* d_lam_el = nullptr;    // [E]
+  double* d_cg_tab = nullptr;    // [(g+1)^2 points][ng][2] reference gradients + [points] weights
+  double* d_detmin = nullptr;    // [E] minimum det J over the volume points
 };
 
 namespace icx {
@@ -578,7 +606,10 @@ void free_mdg(icx_ctx* c) {
                   m->d_fixval, m->d_sel, m->d_cols, m->d_items, m->d_slots, m->d_rowptr, m->d_colidx,
                   m->d_src_ptr, m->d_src, m->d_t_rowptr, m->d_t_colidx, m->d_t_perm, m->d_vals, m->d_tvals,
                   m->d_bsr, m->d_colnorm, m->d_diag, m->d_tmp, m->d_res, m->d_jtr, m->d_p, m->d_ustep,
-                  m->d_rwork, m->d_x, m->d_kV, m->d_kw, m->d_kz, m->d_kr, m->d_kdh, m->lw.partial};
+                  m->d_rwork, m->d_x, m->d_kV, m->d_kw, m->d_kz, m->d_kr, m->d_kdh, m->lw.partial,
+                  m->d_a_rowptr, m->d_a_colidx, m->d_a_diag, m->d_a_vals, m->d_a_lu, m->d_lo_rows, m->d_up_rows,
+                  m->d_pc_err, m->d_pair_ptr, m->d_pair_ij, m->d_upos, m->d_upos_ptr, m->d_upos_list,
+                  m->d_pair_val, m->d_lam_el, m->d_cg_tab, m->d_detmin, m->d_colnorm2};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete m;
@@ -897,6 +928,9 @@ icx_status build_mdg_pattern(icx_ctx* c) {
     }
   m.h_rowptr = rowptr;
   m.h_colidx = colidx;
+  m.h_trowptr = trow;
+  m.h_tcolidx = tcol;
+  m.a_built = false;
   MCK(up(&m.d_items, items));
   if (m.d_slots) cudaFree(m.d_slots);
   MCK(cudaMalloc((void**)&m.d_slots, sizeof(double) * std::max(slot, 1LL)));
@@ -989,6 +1023,178 @@ __global__ void min_det_kernel(DeviceMesh dm, int* flag) {
   if (J[0][0] * J[1][1] - J[0][1] * J[1][0] < 0.0) atomicExch(flag, 1);
 }
 
+// per element: minimum det J over the volume quadrature points (not clamped)
+template <int G>
+__global__ void elem_min_det_kernel(DeviceMesh dm, double* __restrict__ mins) {
+  constexpr int NG = (G + 1) * (G + 1);
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= dm.E) return;
+  double m = 1e100;
+  for (int q = 0; q < dm.nqv; ++q) {
+    double J[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    for (int n = 0; n < NG; ++n) {
+      int gn = dm.el_nodes[e * NG + n];
+      double d0 = dm.tab_gvol[(q * NG + n) * 2], d1 = dm.tab_gvol[(q * NG + n) * 2 + 1];
+      J[0][0] += d0 * dm.coord[2 * gn]; J[0][1] += d1 * dm.coord[2 * gn];
+      J[1][0] += d0 * dm.coord[2 * gn + 1]; J[1][1] += d1 * dm.coord[2 * gn + 1];
+    }
+    m = fmin(m, J[0][0] * J[1][1] - J[0][1] * J[1][0]);
+  }
+  mins[e] = m;
+}
+
+// A = J^T J on A's pattern: one warp per row i of A (column i of J); for each
+// entry (r, J_ri) of column i the lanes add J_ri J_rc over row r of J into
+// the positions of A's row i (binary search), rows r in ascending order
+__global__ void jtj_kernel(long long n, const int* __restrict__ t_rowptr, const int* __restrict__ t_colidx,
+                           const double* __restrict__ t_vals, const int* __restrict__ rowptr,
+                           const int* __restrict__ colidx, const double* __restrict__ vals,
+                           const int* __restrict__ a_rowptr, const int* __restrict__ a_colidx,
+                           double* __restrict__ a_vals) {
+  long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const int a0 = a_rowptr[i], a1 = a_rowptr[i + 1];
+  for (int k = a0 + lane; k < a1; k += 32) a_vals[k] = 0.0;
+  __syncwarp();
+  for (int t = t_rowptr[i]; t < t_rowptr[i + 1]; ++t) {
+    const int r = t_colidx[t];
+    const double v = t_vals[t];
+    for (int q = rowptr[r] + lane; q < rowptr[r + 1]; q += 32) {
+      const int c = colidx[q];
+      int lo = a0, hi = a1 - 1;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a_colidx[mid] < c) lo = mid + 1;
+        else hi = mid;
+      }
+      if (lo < a1 && a_colidx[lo] == c) a_vals[lo] += v * vals[q];
+    }
+    __syncwarp();
+  }
+}
+
+// the column-norm scaled diagonal of the explicit subproblem:
+// lambda_u |J_col| (PDE unknowns), lambda_b |J_col| (geometry) (corrigan_lm.hpp:429-451)
+__global__ void a_diag_kernel(long long n, long long npde, double lu, double lb, const double* __restrict__ cn,
+                              const int* __restrict__ a_diag, double* __restrict__ a_vals) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  a_vals[a_diag[i]] += (i < npde ? lu : lb) * cn[i];
+}
+
+// per element the stiffness K of the isoparametric continuous space (Lagrange
+// order G, (G + 1)^2 Gauss-Legendre points, det J not clamped;
+// DiffusionIntegrator, bilinear_integrators.hpp:11-49) and the pair values
+// K[NG-1][il] K[NG-1][jl] lag + (il == jl ? lambda_el[e] : 0): the reference's
+// K^T K loop assigns KTK[i][j] = K[k][i] K[k][j] for every k in turn, so the
+// last basis function's row remains (corrigan_lm.hpp:463-469)
+template <int G>
+__global__ void lm_pair_kernel(DeviceMesh dm, const double* __restrict__ cg_tab, const int* __restrict__ pair_ptr,
+                               const int* __restrict__ pair_ij, const double* __restrict__ lam_el, double lag,
+                               double* __restrict__ pair_val) {
+  constexpr int NG = (G + 1) * (G + 1), NQ = (G + 1) * (G + 1);
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= dm.E || pair_ptr[e] == pair_ptr[e + 1]) return;
+  double xn[NG][2];
+  for (int n = 0; n < NG; ++n) {
+    int gn = dm.el_nodes[e * NG + n];
+    xn[n][0] = dm.coord[2 * gn];
+    xn[n][1] = dm.coord[2 * gn + 1];
+  }
+  double klast[NG];
+  for (int j = 0; j < NG; ++j) klast[j] = 0.0;
+  for (int q = 0; q < NQ; ++q) {
+    const double* t = cg_tab + (size_t)q * NG * 2;
+    double J[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    for (int n = 0; n < NG; ++n) {
+      J[0][0] += t[2 * n] * xn[n][0]; J[0][1] += t[2 * n + 1] * xn[n][0];
+      J[1][0] += t[2 * n] * xn[n][1]; J[1][1] += t[2 * n + 1] * xn[n][1];
+    }
+    double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    double dd = det == 0.0 ? 1.0 : det;  // the physical-gradient guard of the reference (finite_element.hpp:235-255)
+    // grad phi_n = adj(J)^T-based reference gradient / det
+    double gl0 = (t[2 * (NG - 1)] * J[1][1] - t[2 * (NG - 1) + 1] * J[1][0]) / dd;
+    double gl1 = (-t[2 * (NG - 1)] * J[0][1] + t[2 * (NG - 1) + 1] * J[0][0]) / dd;
+    double w = cg_tab[(size_t)NQ * NG * 2 + q];
+    for (int j = 0; j < NG; ++j) {
+      double g0 = (t[2 * j] * J[1][1] - t[2 * j + 1] * J[1][0]) / dd;
+      double g1 = (-t[2 * j] * J[0][1] + t[2 * j + 1] * J[0][0]) / dd;
+      klast[j] += (gl0 * g0 + gl1 * g1) * det * w;
+    }
+  }
+  for (int pidx = pair_ptr[e]; pidx < pair_ptr[e + 1]; ++pidx) {
+    int il = pair_ij[2 * pidx], jl = pair_ij[2 * pidx + 1];
+    double v = klast[il] * klast[jl] * lag;
+    if (il == jl && lam_el[e] > 0.0) v += lam_el[e];
+    pair_val[pidx] = v;
+  }
+}
+
+// A[pos] += the pair values of that position, in ascending pair order
+__global__ void pair_gather_kernel(int npos, const int* __restrict__ upos, const int* __restrict__ upos_ptr,
+                                   const int* __restrict__ upos_list, const double* __restrict__ pair_val,
+                                   double* __restrict__ a_vals) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npos) return;
+  double s = 0.0;
+  for (int t = upos_ptr[k]; t < upos_ptr[k + 1]; ++t) s += pair_val[upos_list[t]];
+  a_vals[upos[k]] += s;
+}
+
+// scalar ILU(0) of a CSR matrix in natural order, one level of rows per
+// launch, one warp per row (IKJ): for each k < i of row i in ascending order,
+// l_ik = a_ik / u_kk, then a_ij -= l_ik u_kj for j > k of row k present in row i
+__global__ void csr_ilu_level_kernel(int nrows, const int* __restrict__ rows, const int* __restrict__ rowptr,
+                                     const int* __restrict__ colidx, const int* __restrict__ diag,
+                                     double* __restrict__ lu, int* err) {
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (w >= nrows) return;
+  const int i = rows[w];
+  const int r0 = rowptr[i], r1 = rowptr[i + 1], di = diag[i];
+  for (int p = r0; p < di; ++p) {
+    const int k = colidx[p];
+    const double ukk = lu[diag[k]];
+    if (ukk == 0.0) {
+      if (lane == 0) atomicExch(err, 1);
+      return;
+    }
+    const double l = lu[p] / ukk;
+    __syncwarp();
+    if (lane == 0) lu[p] = l;
+    for (int q = diag[k] + 1 + lane; q < rowptr[k + 1]; q += 32) {
+      const int j = colidx[q];
+      int lo = p + 1, hi = r1 - 1;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (colidx[mid] < j) lo = mid + 1;
+        else hi = mid;
+      }
+      if (lo < r1 && colidx[lo] == j) lu[lo] -= l * lu[q];
+    }
+    __syncwarp();
+  }
+}
+
+// one level of the ILU(0) triangular solves, one warp per row: forward
+// y_i = b_i - sum_{k<i} l_ik y_k; backward x_i = (y_i - sum_{j>i} u_ij x_j) / u_ii
+__global__ void csr_tri_level_kernel(int nrows, const int* __restrict__ rows, const int* __restrict__ rowptr,
+                                     const int* __restrict__ colidx, const int* __restrict__ diag,
+                                     const double* __restrict__ lu, const double* __restrict__ b,
+                                     double* __restrict__ y, int upper) {
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (w >= nrows) return;
+  const int i = rows[w];
+  const int d = diag[i];
+  const int q0 = upper ? d + 1 : rowptr[i], q1 = upper ? rowptr[i + 1] : d;
+  double s = 0.0;
+  for (int q = q0 + lane; q < q1; q += 32) s += lu[q] * y[colidx[q]];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) y[i] = upper ? (b[i] - s) / lu[d] : b[i] - s;
+}
+
 }  // namespace icx
 
 namespace {
@@ -997,7 +1203,8 @@ icx_status ensure_lm(icx_ctx* c, int m) {
   icx_mdg_state& s = *c->mdg;
   long long n = s.ncol, nr = s.nrow;
   if (s.d_kV && s.kb.m >= m && s.kb.n == n) return ICX_OK;
-  double** bufs[] = {&s.d_colnorm, &s.d_diag, &s.d_jtr, &s.d_p, &s.d_ustep, &s.d_x, &s.d_kw, &s.d_kz, &s.d_kr};
+  double** bufs[] = {&s.d_colnorm, &s.d_diag, &s.d_jtr, &s.d_p, &s.d_ustep, &s.d_x, &s.d_kw, &s.d_kz, &s.d_kr,
+                     &s.d_colnorm2};
   for (double** b : bufs) {
     if (*b) cudaFree(*b);
     MCK(cudaMalloc((void**)b, sizeof(double) * n));
@@ -1020,6 +1227,156 @@ icx_status ensure_lm(icx_ctx* c, int m) {
   s.kb.r = s.d_kr;
   s.kb.dh = s.d_kdh;
   s.kb.lw = &s.lw;
+  return ICX_OK;
+}
+
+// the explicitly formed subproblem's pattern (A = J^T J over the unknowns
+// [u; x], its diagonal, and the geometry pairs the Laplacian and the
+// element-wise regularisation add to), its ILU(0) level schedules and the
+// continuous-space tabulation; built once per selection (the pattern of J
+// does not change when the nodes move)
+icx_status build_lm_explicit(icx_ctx* c) {
+  icx_mdg_state& m = *c->mdg;
+  const icx::DeviceMesh& dm = c->dm;
+  const long long n = m.ncol;
+  const int g = c->geo_order, ng = (g + 1) * (g + 1);
+  const long long N = (long long)dm.E * dm.nb * dm.neq;
+  // geometry pairs per element: (il, jl, row, col) of the free coordinates of two selected nodes
+  std::vector<int> pair_ptr(dm.E + 1, 0), pair_ij;
+  std::vector<std::pair<long long, long long>> pair_rc;
+  auto nfree = [&](int k) { return m.cols[k + 1] - m.cols[k]; };
+  for (int e = 0; e < dm.E; ++e) {
+    for (int il = 0; il < ng; ++il) {
+      int ki = m.inv[c->el_nodes[(size_t)e * ng + il]];
+      if (ki >= m.nsel) continue;
+      for (int jl = 0; jl < ng; ++jl) {
+        int kj = m.inv[c->el_nodes[(size_t)e * ng + jl]];
+        if (kj >= m.nsel) continue;
+        for (int iv = 0; iv < nfree(ki); ++iv)
+          for (int jv = 0; jv < nfree(kj); ++jv) {
+            pair_ij.push_back(il);
+            pair_ij.push_back(jl);
+            pair_rc.push_back({N + m.cols[ki] + iv, N + m.cols[kj] + jv});
+          }
+      }
+    }
+    pair_ptr[e + 1] = (int)pair_rc.size();
+  }
+  // A's pattern: row i = the union of the rows of J that column i touches, the diagonal and the pairs
+  std::vector<std::vector<int>> extra(n);
+  for (auto& rc : pair_rc) extra[rc.first].push_back((int)rc.second);
+  std::vector<int> arow(n + 1, 0), acol, stamp(n, -1), cur;
+  for (long long i = 0; i < n; ++i) {
+    cur.clear();
+    auto add = [&](int col) {
+      if (stamp[col] != (int)i) {
+        stamp[col] = (int)i;
+        cur.push_back(col);
+      }
+    };
+    add((int)i);
+    for (int t = m.h_trowptr[i]; t < m.h_trowptr[i + 1]; ++t) {
+      int r = m.h_tcolidx[t];
+      for (int q = m.h_rowptr[r]; q < m.h_rowptr[r + 1]; ++q) add(m.h_colidx[q]);
+    }
+    for (int col : extra[i]) add(col);
+    std::sort(cur.begin(), cur.end());
+    acol.insert(acol.end(), cur.begin(), cur.end());
+    arow[i + 1] = (int)acol.size();
+  }
+  m.a_nnz = (long long)acol.size();
+  std::vector<int> adiag(n);
+  auto find = [&](long long i, int col) {
+    auto b = acol.begin() + arow[i], e = acol.begin() + arow[i + 1];
+    return (int)(std::lower_bound(b, e, col) - acol.begin());
+  };
+  for (long long i = 0; i < n; ++i) adiag[i] = find(i, (int)i);
+  // per touched position, its pairs in ascending order
+  std::vector<std::pair<int, int>> pos_pair(pair_rc.size());
+  for (size_t p = 0; p < pair_rc.size(); ++p) pos_pair[p] = {find(pair_rc[p].first, (int)pair_rc[p].second), (int)p};
+  std::sort(pos_pair.begin(), pos_pair.end());
+  std::vector<int> upos, uptr(1, 0), ulist;
+  for (size_t t = 0; t < pos_pair.size(); ++t) {
+    if (t == 0 || pos_pair[t].first != pos_pair[t - 1].first) {
+      if (t) uptr.push_back((int)ulist.size());
+      upos.push_back(pos_pair[t].first);
+    }
+    ulist.push_back(pos_pair[t].second);
+  }
+  uptr.push_back((int)ulist.size());
+  if (pos_pair.empty()) uptr.assign(1, 0);
+  m.npairs = (int)pair_rc.size();
+  m.npos = (int)upos.size();
+  // ILU(0) level schedules in natural order
+  std::vector<int> lo(n, 0), upv(n, 0);
+  int nlo = 0, nup = 0;
+  for (long long i = 0; i < n; ++i) {
+    int l = 0;
+    for (int q = arow[i]; q < adiag[i]; ++q) l = std::max(l, lo[acol[q]] + 1);
+    lo[i] = l;
+    nlo = std::max(nlo, l + 1);
+  }
+  for (long long i = n - 1; i >= 0; --i) {
+    int l = 0;
+    for (int q = adiag[i] + 1; q < arow[i + 1]; ++q) l = std::max(l, upv[acol[q]] + 1);
+    upv[i] = l;
+    nup = std::max(nup, l + 1);
+  }
+  auto schedule = [&](const std::vector<int>& lv, int nl, std::vector<int>& off, std::vector<int>& rows) {
+    off.assign(nl + 1, 0);
+    for (int v : lv) ++off[v + 1];
+    for (int l = 0; l < nl; ++l) off[l + 1] += off[l];
+    rows.assign(n, 0);
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (long long i = 0; i < n; ++i) rows[fill[lv[i]]++] = (int)i;
+  };
+  std::vector<int> lo_rows, up_rows;
+  schedule(lo, nlo, m.lo_off, lo_rows);
+  schedule(upv, nup, m.up_off, up_rows);
+  // the continuous space's reference gradients at its (g + 1)^2 Gauss points, then the weights
+  const int nq = g + 1;
+  double qx[16], qw[16];
+  icx::gauss_legendre_points(nq, qx, qw);
+  std::vector<double> tab((size_t)nq * nq * ng * 2 + nq * nq);
+  double N0[16], D0[16], N1[16], D1[16];
+  for (int q0 = 0; q0 < nq; ++q0)
+    for (int q1 = 0; q1 < nq; ++q1) {
+      icx::lagrange_values_derivs(g, qx[q0], N0, D0);
+      icx::lagrange_values_derivs(g, qx[q1], N1, D1);
+      const int q = q0 * nq + q1;
+      for (int a = 0; a <= g; ++a)
+        for (int b = 0; b <= g; ++b) {
+          const int k = a * (g + 1) + b;
+          tab[((size_t)q * ng + k) * 2] = D0[a] * N1[b];
+          tab[((size_t)q * ng + k) * 2 + 1] = N0[a] * D1[b];
+        }
+      tab[(size_t)nq * nq * ng * 2 + q] = qw[q0] * qw[q1];
+    }
+  MCK(up(&m.d_a_rowptr, arow));
+  MCK(up(&m.d_a_colidx, acol));
+  MCK(up(&m.d_a_diag, adiag));
+  MCK(up(&m.d_lo_rows, lo_rows));
+  MCK(up(&m.d_up_rows, up_rows));
+  MCK(up(&m.d_pair_ptr, pair_ptr));
+  MCK(up(&m.d_pair_ij, pair_ij.empty() ? std::vector<int>(2, 0) : pair_ij));
+  MCK(up(&m.d_upos, upos.empty() ? std::vector<int>(1, 0) : upos));
+  MCK(up(&m.d_upos_ptr, uptr));
+  MCK(up(&m.d_upos_list, ulist.empty() ? std::vector<int>(1, 0) : ulist));
+  MCK(up(&m.d_cg_tab, tab));
+  for (double** b : {&m.d_a_vals, &m.d_a_lu}) {
+    if (*b) cudaFree(*b);
+    MCK(cudaMalloc((void**)b, sizeof(double) * std::max(m.a_nnz, 1LL)));
+  }
+  for (double** b : {&m.d_pair_val}) {
+    if (*b) cudaFree(*b);
+    MCK(cudaMalloc((void**)b, sizeof(double) * std::max(m.npairs, 1)));
+  }
+  for (double** b : {&m.d_lam_el, &m.d_detmin}) {
+    if (*b) cudaFree(*b);
+    MCK(cudaMalloc((void**)b, sizeof(double) * dm.E));
+  }
+  if (!m.d_pc_err) MCK(cudaMalloc((void**)&m.d_pc_err, sizeof(int)));
+  m.a_built = true;
   return ICX_OK;
 }
 
@@ -1061,6 +1418,8 @@ icx_status icx_lm_default_options(icx_lm_options* o) {
   o->gmres_max_it = 10000;
   o->gmres_rtol = 1e-5;
   o->max_rejections = 20;
+  o->explicit_subproblem = 0;  // CorriganLM's explicitly_form_subproblem default (corrigan_lm.hpp:286)
+  o->lambda_lag = 1e-5;        // CorriganLM::lambda_lag (corrigan_lm.hpp:223)
   return ICX_OK;
 }
 
@@ -1092,11 +1451,14 @@ icx_status icx_lm_solve(icx_ctx* c, double* d_u, double* x, const icx_lm_options
   };
   st = form();
   if (st != ICX_OK) return st;
+  const bool explicit_sub = opt->explicit_subproblem != 0;
+  if (explicit_sub && !s.a_built && (st = build_lm_explicit(c)) != ICX_OK) return st;
   double rk = icx::la_norm(s.lw, nr, s.d_res, s.d_kdh, strm);
   R->r0 = rk;
   R->residual_history[0] = rk;
   double tau = opt->tau_abs + opt->tau_rel * rk;
   double lu = opt->lambda_u, lb = opt->lambda_b, lu_min = lu;
+  std::vector<double> lam_el(dm.E, 0.0), detmin(dm.E);  // element-wise regularisation (corrigan_lm.hpp:507-527)
   int k = 0, rejections = 0, hist = 0;
   bool converged = rk <= tau;
   int* d_flag = nullptr;
@@ -1106,17 +1468,73 @@ icx_status icx_lm_solve(icx_ctx* c, double* d_u, double* x, const icx_lm_options
     // J^T r and the regularisation from the column norms of J
     unsigned nb_n = (unsigned)((n * 32 + 255) / 256), nb_r = (unsigned)((nr * 32 + 255) / 256);
     icx::csr_rownorm_kernel<<<nb_n, 256, 0, strm>>>(n, s.d_t_rowptr, s.d_tvals, s.d_colnorm);
-    icx::lm_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, strm>>>(n, N, lu, lb, s.d_colnorm, s.d_diag);
     icx::csr_spmv_kernel<<<nb_n, 256, 0, strm>>>(n, s.d_t_rowptr, s.d_t_colidx, s.d_tvals, s.d_res, s.d_jtr);
-    icx::LinOp A = [&](const double* xin, double* yout, cudaStream_t st) {
-      icx::csr_spmv_kernel<<<nb_r, 256, 0, st>>>(nr, s.d_rowptr, s.d_colidx, s.d_vals, xin, s.d_tmp);
-      icx::csr_spmv_kernel<<<nb_n, 256, 0, st>>>(n, s.d_t_rowptr, s.d_t_colidx, s.d_tvals, s.d_tmp, yout);
-      icx::diag_axpy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, s.d_diag, xin, yout);
-      return cudaGetLastError();
-    };
+    icx::LinOp A, M;
+    bool use_m = false;
+    if (explicit_sub) {
+      // A = J^T J + diag(lambda |J_col|) + lambda_lag |r| K^T K + lambda_el
+      // (corrigan_lm.hpp:426-530), then its ILU(0) (the reference's PCILU)
+      icx::jtj_kernel<<<nb_n, 256, 0, strm>>>(n, s.d_t_rowptr, s.d_t_colidx, s.d_tvals, s.d_rowptr, s.d_colidx,
+                                               s.d_vals, s.d_a_rowptr, s.d_a_colidx, s.d_a_vals);
+      icx::a_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, strm>>>(n, N, lu, lb, s.d_colnorm, s.d_a_diag,
+                                                                         s.d_a_vals);
+      if (s.npairs > 0) {
+        MCK(cudaMemcpyAsync(s.d_lam_el, lam_el.data(), sizeof(double) * dm.E, cudaMemcpyHostToDevice, strm));
+        const double lag = opt->lambda_lag * rk;
+        if (dm.G == 1)
+          icx::lm_pair_kernel<1><<<(dm.E + 127) / 128, 128, 0, strm>>>(dm, s.d_cg_tab, s.d_pair_ptr, s.d_pair_ij,
+                                                                      s.d_lam_el, lag, s.d_pair_val);
+        else
+          icx::lm_pair_kernel<2><<<(dm.E + 127) / 128, 128, 0, strm>>>(dm, s.d_cg_tab, s.d_pair_ptr, s.d_pair_ij,
+                                                                      s.d_lam_el, lag, s.d_pair_val);
+        icx::pair_gather_kernel<<<(s.npos + 255) / 256, 256, 0, strm>>>(s.npos, s.d_upos, s.d_upos_ptr,
+                                                                        s.d_upos_list, s.d_pair_val, s.d_a_vals);
+      }
+      MCK(cudaMemcpyAsync(s.d_a_lu, s.d_a_vals, sizeof(double) * s.a_nnz, cudaMemcpyDeviceToDevice, strm));
+      MCK(cudaMemsetAsync(s.d_pc_err, 0, sizeof(int), strm));
+      for (size_t l = 0; l + 1 < s.lo_off.size(); ++l) {
+        const int cnt = s.lo_off[l + 1] - s.lo_off[l];
+        icx::csr_ilu_level_kernel<<<(cnt * 32 + 255) / 256, 256, 0, strm>>>(
+            cnt, s.d_lo_rows + s.lo_off[l], s.d_a_rowptr, s.d_a_colidx, s.d_a_diag, s.d_a_lu, s.d_pc_err);
+      }
+      MCK(cudaGetLastError());
+      int perr = 0;
+      MCK(cudaMemcpyAsync(&perr, s.d_pc_err, sizeof(int), cudaMemcpyDeviceToHost, strm));
+      MCK(cudaStreamSynchronize(strm));
+      if (perr) { cleanup(); return merr(c, ICX_ERR_NONFINITE, "LM subproblem ILU(0): zero pivot"); }
+      A = [&](const double* xin, double* yout, cudaStream_t st) {
+        icx::csr_spmv_kernel<<<nb_n, 256, 0, st>>>(n, s.d_a_rowptr, s.d_a_colidx, s.d_a_vals, xin, yout);
+        return cudaGetLastError();
+      };
+      M = [&](const double* xin, double* yout, cudaStream_t st) {
+        for (size_t l = 0; l + 1 < s.lo_off.size(); ++l) {
+          const int cnt = s.lo_off[l + 1] - s.lo_off[l];
+          icx::csr_tri_level_kernel<<<(cnt * 32 + 255) / 256, 256, 0, st>>>(
+              cnt, s.d_lo_rows + s.lo_off[l], s.d_a_rowptr, s.d_a_colidx, s.d_a_diag, s.d_a_lu, xin, s.d_colnorm2,
+              0);
+        }
+        for (size_t l = 0; l + 1 < s.up_off.size(); ++l) {
+          const int cnt = s.up_off[l + 1] - s.up_off[l];
+          icx::csr_tri_level_kernel<<<(cnt * 32 + 255) / 256, 256, 0, st>>>(
+              cnt, s.d_up_rows + s.up_off[l], s.d_a_rowptr, s.d_a_colidx, s.d_a_diag, s.d_a_lu, s.d_colnorm2, yout,
+              1);
+        }
+        return cudaGetLastError();
+      };
+      use_m = true;
+    } else {
+      icx::lm_diag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, strm>>>(n, N, lu, lb, s.d_colnorm, s.d_diag);
+      A = [&](const double* xin, double* yout, cudaStream_t st) {
+        icx::csr_spmv_kernel<<<nb_r, 256, 0, st>>>(nr, s.d_rowptr, s.d_colidx, s.d_vals, xin, s.d_tmp);
+        icx::csr_spmv_kernel<<<nb_n, 256, 0, st>>>(n, s.d_t_rowptr, s.d_t_colidx, s.d_tvals, s.d_tmp, yout);
+        icx::diag_axpy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, s.d_diag, xin, yout);
+        return cudaGetLastError();
+      };
+    }
     int its = 0;
     double rr = 0.0;
-    st = icx::gmres_op(s.kb, A, nullptr, opt->gmres_max_it, opt->gmres_rtol, s.d_jtr, s.d_p, &its, &rr, strm, &c->err);
+    st = icx::gmres_op(s.kb, A, use_m ? &M : nullptr, opt->gmres_max_it, opt->gmres_rtol, s.d_jtr, s.d_p, &its, &rr,
+                       strm, &c->err);
     if (st != ICX_OK) { cleanup(); return st; }
     R->linear_iterations_total += its;
     MCK(cudaMemcpy(px.data(), s.d_p + N, sizeof(double) * ngeo, cudaMemcpyDeviceToHost));
@@ -1137,16 +1555,32 @@ icx_status icx_lm_solve(icx_ctx* c, double* d_u, double* x, const icx_lm_options
         return v;
       };
       alpha = corrigan_ls_lm(phi, opt->ls_alpha_max, opt->ls_alpha_initial, opt->ls_max_it, opt->ls_alpha_min);
-      // element inversion check on the last line-search mesh (corrigan_lm.hpp:625-645)
-      cudaMemset(d_flag, 0, sizeof(int));
-      if (dm.G == 1) icx::min_det_kernel<1><<<(dm.E * dm.nqv + 255) / 256, 256, 0, strm>>>(dm, d_flag);
-      else icx::min_det_kernel<2><<<(dm.E * dm.nqv + 255) / 256, 256, 0, strm>>>(dm, d_flag);
-      int inverted = 0;
-      MCK(cudaMemcpy(&inverted, d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+      // element inversion check on the last line-search mesh, with the
+      // element-wise regularisation updates (corrigan_lm.hpp:625-666)
+      bool inverted = false;
+      if (explicit_sub) {
+        if (dm.G == 1) icx::elem_min_det_kernel<1><<<(dm.E + 127) / 128, 128, 0, strm>>>(dm, s.d_detmin);
+        else icx::elem_min_det_kernel<2><<<(dm.E + 127) / 128, 128, 0, strm>>>(dm, s.d_detmin);
+        MCK(cudaMemcpy(detmin.data(), s.d_detmin, sizeof(double) * dm.E, cudaMemcpyDeviceToHost));
+        for (int e = 0; e < dm.E; ++e)
+          if (detmin[e] < 0.0) {
+            inverted = true;
+            lam_el[e] = lam_el[e] == 0.0 ? lb : lam_el[e] * std::max(1.5, std::fabs(detmin[e]));
+          }
+      } else {
+        cudaMemset(d_flag, 0, sizeof(int));
+        if (dm.G == 1) icx::min_det_kernel<1><<<(dm.E * dm.nqv + 255) / 256, 256, 0, strm>>>(dm, d_flag);
+        else icx::min_det_kernel<2><<<(dm.E * dm.nqv + 255) / 256, 256, 0, strm>>>(dm, d_flag);
+        int fl = 0;
+        MCK(cudaMemcpy(&fl, d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+        inverted = fl != 0;
+      }
       accept = !inverted && rnorm_step < 10 * rnorm_old;
       if (accept) {
         lu = std::max(lu_min, 0.55 * lu);
         lb = std::max(rnorm_step, 0.55 * lb);
+        for (double& l : lam_el)
+          if (l > 0.0) l /= 1.5;
       } else {
         lu *= 1.8;
         lb *= 1.8;

@@ -24,7 +24,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import DIRICHLET, FLUX_VANLEER, Context, workload_fn
+from . import DIRICHLET, EXTRAPOLATION, FLUX_VANLEER, Context, workload_fn
 
 
 def lattice_coords(nelem, geo_order, xmin=(0.0, 0.0), xmax=(1.0, 1.0)):
@@ -210,3 +210,46 @@ def batched_problems(n_problems=512, seed=2024, device=0):
             states.append(u0)
         out[p] = (batch(parts, device), parts, np.concatenate(states), lst)
     return out
+
+
+def jitter_interior(coord, nelem, frac, seed):
+    """seeded uniform displacement in [-frac h, frac h] of every interior node
+    of a geometry-order-1 lattice (boundary nodes keep their place)"""
+    rng = np.random.default_rng(seed)
+    out = coord.copy()
+    nx, ny = nelem
+    h = (1.0 / nx, 1.0 / ny)
+    for k in range(out.shape[0]):
+        ix, iy = k % (nx + 1), k // (nx + 1)
+        d = rng.uniform(-frac, frac, 2)
+        if 0 < ix < nx and 0 < iy < ny:
+            out[k, 0] += d[0] * h[0]
+            out[k, 1] += d[1] * h[1]
+    return np.ascontiguousarray(out)
+
+
+def mdg_ice_config(n=64, p=1, seed=99, device=0, jitter=0.2):
+    """MDG-ICE steady inviscid Burgers with an oblique discontinuity: n x n
+    quads on [0, 1]^2, geometry order 1, (u^2 / 2)_x + u_y = 0 (a = (0, 1),
+    b = (1, 0), mu = 0), u = 1 left of x = 0.4 + 0.2 y and -0.5 right of it;
+    left, bottom and right Dirichlet with that state, top extrapolation;
+    interior nodes jittered by a seeded +-0.2 h; every interior trace
+    selected (geometry unknowns: their nodes, boundary nodes sliding along
+    the box). Returns (workload, traces, x0)."""
+    ctx = Context(device)
+    ctx.mesh_uniform((n, n), (0.0, 0.0), (1.0, 1.0), 1, (DIRICHLET, DIRICHLET, DIRICHLET, EXTRAPOLATION), (0,) * 4)
+    coords = jitter_interior(lattice_coords((n, n), 1), (n, n), jitter, seed)
+    ctx.set_coords(coords)
+    ctx.fespace(p)
+    ctx.disc_burgers(0.0, (0.0, 1.0), (1.0, 0.0))
+    ctx.disc_options(False, 0.0)
+    step = (C.c_double * 4)(0.4, 0.2, 1.0, -0.5)
+    ctx.dirichlet(0, workload_fn("oblique_step"), C.cast(step, C.c_void_p))
+    ctx.setup()
+    _, _, nint = ctx.topology()
+    traces = np.arange(nint)
+    ctx.mdg_select(traces, True)
+    xy = ctx.basis_node_coords().reshape(-1, 2)
+    u0 = np.where(xy[:, 0] < 0.4 + 0.2 * xy[:, 1], 1.0, -0.5)
+    return Workload(ctx, coords, np.ascontiguousarray(u0), dict(n=n, p=p, jitter=jitter), "mdg_ice", [step]), \
+        traces, ctx.mdg_get_x()

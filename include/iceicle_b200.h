@@ -238,6 +238,15 @@ typedef struct icx_lm_options {
   double gmres_rtol;
   int max_rejections;        /* bound on rejected steps in a row */
   int verbosity;
+  /* 1: form the subproblem matrix (explicitly_form_subproblem = true,
+   * corrigan_lm.hpp:426-530): J^T J + diag(lambda_u |J_col|, lambda_b |J_col|)
+   * + lambda_lag |r| K^T K on the isoparametric continuous space + the
+   * element-wise regularisation lambda_el of elements that inverted, solved
+   * by GMRES with its ILU(0) (PCILU). 0 (default): the matrix-free
+   * J^T J + diag(lambda_u |J_col|, max(lambda_b, lambda_b |J_col|)) operator
+   * without preconditioner (the MATSHELL path, corrigan_lm.hpp:68-109). */
+  int explicit_subproblem;
+  double lambda_lag;         /* CorriganLM::lambda_lag (default 1e-5) */
 } icx_lm_options;
 
 typedef struct icx_lm_report {

@@ -1278,8 +1278,11 @@ int orc_mdg_residual(const orc_problem* pb, const double* coord, int ntr, const 
  * dense row-major (N + nic) x (N + ngeo) array (small meshes only). dICE/dx
  * visits only the selected traces of elements around the node: the others
  * do not change when the node moves and contribute exact zeros. */
-int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
-                           const double* u, const double* x, double* res_and_ic, double* J) {
+/* the MDG Jacobian entries, each handed to emit(ctx, row, col, value); an
+ * entry may be emitted more than once (the contributions add) */
+typedef void (*orc_emit_fn)(void* ctx, size_t row, size_t col, double v);
+static int mdg_jacobian_impl(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                             const double* u, const double* x, double* res_and_ic, orc_emit_fn emit, void* ectx) {
   int nn = orc_n_nodes(pb);
   double* cw = (double*)malloc(sizeof(double) * 2 * nn);
   memcpy(cw, coord, sizeof(double) * 2 * nn);
@@ -1291,7 +1294,8 @@ int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, 
   size_t N = (size_t)E * bs, nrow = N + (size_t)M.nsel * neq, ncol = N + M.ngeo;
   const double eps = sqrt(DBL_EPSILON);
   mdg_coord_from_x(&M, x, cw);
-  memset(J, 0, sizeof(double) * nrow * ncol);
+  (void)nrow;
+  (void)ncol;
   /* DG block */
   int* rowptr = (int*)malloc(sizeof(int) * (E + 1));
   int* colidx = (int*)malloc(sizeof(int) * 5 * E);
@@ -1302,7 +1306,7 @@ int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, 
     for (int k = rowptr[r]; k < rowptr[r + 1]; ++k)
       for (int i = 0; i < bs; ++i)
         for (int j = 0; j < bs; ++j)
-          J[((size_t)r * bs + i) * ncol + (size_t)colidx[k] * bs + j] += vals[((size_t)k * bs + i) * bs + j];
+          emit(ectx, (size_t)r * bs + i, (size_t)colidx[k] * bs + j, vals[((size_t)k * bs + i) * bs + j]);
   free(vals); free(rowptr); free(colidx);
   double* ic = res_and_ic + N;
   mdg_ic_residual(&D, &M, ntr, traces, u, ic);
@@ -1327,7 +1331,7 @@ int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, 
           int k = M.inv[face_node(pb, F, i)];
           if (k == M.nsel) continue;
           for (int e = 0; e < neq; ++e)
-            J[(N + (size_t)k * neq + e) * ncol + (size_t)el * bs + c] += (r1[i * neq + e] - r0[i * neq + e]) / es;
+            emit(ectx, N + (size_t)k * neq + e, (size_t)el * bs + c, (r1[i * neq + e] - r0[i * neq + e]) / es);
         }
       }
     }
@@ -1364,7 +1368,7 @@ int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, 
         memset(rlp, 0, sizeof(double) * bs);
         domain_integral(&D, e, u + (size_t)e * bs, rlp);
         cw[2 * node] = save[0]; cw[2 * node + 1] = save[1];
-        for (int i = 0; i < bs; ++i) J[((size_t)e * bs + i) * ncol + N + c0 + is] += (rlp[i] - rl[i]) / es;
+        for (int i = 0; i < bs; ++i) emit(ectx, (size_t)e * bs + i, N + c0 + is, (rlp[i] - rl[i]) / es);
       }
     }
     /* traces of the surrounding elements, each once */
@@ -1393,9 +1397,9 @@ int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, 
         if (R >= 0) trace_integral(&D, F, u + (size_t)L * bs, u + (size_t)R * bs, rlp, rrp);
         else boundary_integral(&D, F, u + (size_t)L * bs, rlp);
         cw[2 * node] = save[0]; cw[2 * node + 1] = save[1];
-        for (int i = 0; i < bs; ++i) J[((size_t)L * bs + i) * ncol + N + c0 + is] += (rlp[i] - rl[i]) / es;
+        for (int i = 0; i < bs; ++i) emit(ectx, (size_t)L * bs + i, N + c0 + is, (rlp[i] - rl[i]) / es);
         if (R >= 0)
-          for (int i = 0; i < bs; ++i) J[((size_t)R * bs + i) * ncol + N + c0 + is] += (rrp[i] - rr[i]) / es;
+          for (int i = 0; i < bs; ++i) emit(ectx, (size_t)R * bs + i, N + c0 + is, (rrp[i] - rr[i]) / es);
       }
     }
     /* interface conservation of the selected traces among them */
@@ -1418,7 +1422,7 @@ int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, 
           int kk = M.inv[face_node(pb, F, i)];
           if (kk == M.nsel) continue;
           for (int e = 0; e < neq; ++e)
-            J[(N + (size_t)kk * neq + e) * ncol + N + c0 + is] += (r1[i * neq + e] - r0[i * neq + e]) / es;
+            emit(ectx, N + (size_t)kk * neq + e, N + c0 + is, (r1[i * neq + e] - r0[i * neq + e]) / es);
         }
       }
     }
@@ -1427,6 +1431,56 @@ int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, 
   disc_free(&D);
   free(cw);
   return rc;
+}
+
+
+typedef struct {
+  double* J;
+  size_t ncol;
+} dense_sink;
+static void emit_dense(void* c, size_t r, size_t col, double v) {
+  dense_sink* d = (dense_sink*)c;
+  d->J[r * d->ncol + col] += v;
+}
+
+int orc_mdg_jacobian_dense(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                           const double* u, const double* x, double* res_and_ic, double* J) {
+  int nsel = 0;
+  int* sel = (int*)malloc(sizeof(int) * (size_t)orc_n_nodes(pb));
+  double* xs = (double*)malloc(sizeof(double) * 2 * (size_t)orc_n_nodes(pb));
+  int ngeo = orc_mdg_select(pb, coord, ntr, traces, hyper, &nsel, sel, xs);
+  free(sel);
+  free(xs);
+  int E = pb->nx * pb->ny, bs = (pb->p + 1) * (pb->p + 1) * orc_neq(pb);
+  size_t N = (size_t)E * bs, nrow = N + (size_t)nsel * orc_neq(pb), ncol = N + (size_t)ngeo;
+  memset(J, 0, sizeof(double) * nrow * ncol);
+  dense_sink d = {J, ncol};
+  return mdg_jacobian_impl(pb, coord, ntr, traces, hyper, u, x, res_and_ic, emit_dense, &d);
+}
+
+typedef struct {
+  int* rows;
+  int* cols;
+  double* vals;
+  size_t n, cap;
+} coo_sink;
+static void emit_coo(void* c, size_t r, size_t col, double v) {
+  coo_sink* d = (coo_sink*)c;
+  if (d->n < d->cap) {
+    d->rows[d->n] = (int)r;
+    d->cols[d->n] = (int)col;
+    d->vals[d->n] = v;
+  }
+  ++d->n;
+}
+
+long long orc_mdg_jacobian_coo(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                               const double* u, const double* x, double* res_and_ic, long long cap, int* rows,
+                               int* cols, double* vals) {
+  coo_sink d = {rows, cols, vals, 0, (size_t)cap};
+  int rc = mdg_jacobian_impl(pb, coord, ntr, traces, hyper, u, x, res_and_ic, emit_coo, &d);
+  if (rc) return -1;
+  return (long long)d.n;
 }
 
 /* ------------------------------------------------------------------ */
@@ -1658,4 +1712,82 @@ void orc_physical_flux(const orc_problem* pb, const double* u, const double* g, 
 void orc_ns_boundary_state(const orc_problem* pb, const double* uL, const double* n, int bctype, int bcflag,
                            double* uR) {
   ns_apply_bc(pb, uL, n, bctype, bcflag, uR);
+}
+
+/* ------------------------------------------------------------------ */
+/* LM regularisation inputs                                            */
+/* ------------------------------------------------------------------ */
+/* stiffness of the isoparametric continuous space per element,
+ * K[e][i][j] = sum_q w_q det J grad phi_i . grad phi_j, with the geometry's
+ * own Lagrange basis (order g) and (g + 1)^2 Gauss-Legendre points, det J not
+ * clamped (DiffusionIntegrator::form_operator with lambda = 1,
+ * bilinear_integrators.hpp:11-49, on FESpace(mesh), fespace.hpp:421-457) */
+int orc_cg_stiffness(const orc_problem* pb, const double* coord, double* K) {
+  int g = pb->geo_order, ng = (g + 1) * (g + 1), nq = g + 1;
+  if (g < 1 || g >= MAXP) return -1;
+  lag1d lg;
+  lag_init(&lg, g);
+  double qx[MAXQ], qw[MAXQ];
+  gauss_legendre(nq, qx, qw);
+  int E = pb->nx * pb->ny;
+  elgeo G;
+  for (int e = 0; e < E; ++e) {
+    el_geo(pb, coord, e, &G);
+    double* Ke = K + (size_t)e * ng * ng;
+    for (int i = 0; i < ng * ng; ++i) Ke[i] = 0.0;
+    for (int q0 = 0; q0 < nq; ++q0)
+      for (int q1 = 0; q1 < nq; ++q1) {
+        double xi[2] = {qx[q0], qx[q1]}, J[2][2], B[MAXNB], dB[2 * MAXNB], dBx[2 * MAXNB];
+        el_map(&lg, &G, xi, NULL, J, NULL);
+        double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        tp_eval(&lg, xi, B, dB, NULL);
+        phys_grad(ng, J, dB, dBx);
+        double w = qw[q0] * qw[q1];
+        for (int i = 0; i < ng; ++i)
+          for (int j = 0; j < ng; ++j)
+            Ke[i * ng + j] += (dBx[2 * i] * dBx[2 * j] + dBx[2 * i + 1] * dBx[2 * j + 1]) * det * w;
+      }
+  }
+  return 0;
+}
+
+/* minimum over each element's volume quadrature points ((g + p)^2
+ * Gauss-Legendre) of det J, not clamped (the element inversion test of
+ * CorriganLM::solve, corrigan_lm.hpp:625-640) */
+int orc_min_detj(const orc_problem* pb, const double* coord, double* mins) {
+  disc D;
+  if (disc_init(&D, pb, coord)) return -1;
+  int E = pb->nx * pb->ny;
+  elgeo G;
+  for (int e = 0; e < E; ++e) {
+    el_geo(pb, coord, e, &G);
+    double m = 1e100;
+    for (int q0 = 0; q0 < D.nq1; ++q0)
+      for (int q1 = 0; q1 < D.nq1; ++q1) {
+        double xi[2] = {D.qx[q0], D.qx[q1]}, J[2][2];
+        el_map(&D.lg, &G, xi, NULL, J, NULL);
+        double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+        if (det < m) m = det;
+      }
+    mins[e] = m;
+  }
+  disc_free(&D);
+  return 0;
+}
+
+/* the geometry layout of an MDG selection: the selected nodes and, for node
+ * k, its geometry parameters x[cols[k] .. cols[k + 1]) (geo_data_layout);
+ * returns the number of selected nodes */
+int orc_mdg_layout(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper, int* sel,
+                   int* cols) {
+  disc D;
+  if (disc_init(&D, pb, coord)) return -1;
+  mdgmap M;
+  mdg_build(pb, D.faces, ntr, traces, hyper, &M);
+  for (int k = 0; k < M.nsel; ++k) sel[k] = M.sel[k];
+  for (int k = 0; k <= M.nsel; ++k) cols[k] = M.cols[k];
+  int n = M.nsel;
+  mdg_free(&M);
+  disc_free(&D);
+  return n;
 }

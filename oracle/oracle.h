@@ -108,6 +108,23 @@ void orc_physical_flux(const orc_problem* pb, const double* u, const double* g, 
 void orc_ns_boundary_state(const orc_problem* pb, const double* uL, const double* n, int bctype, int bcflag,
                            double* uR);
 
+/* the same Jacobian as (row, col, value) triplets whose duplicates add;
+ * returns the number of triplets (written up to cap), -1 on failure */
+long long orc_mdg_jacobian_coo(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper,
+                               const double* u, const double* x, double* res_and_ic, long long cap, int* rows,
+                               int* cols, double* vals);
+
+/* per-element stiffness of the isoparametric continuous space [E][ng][ng]
+ * and per-element minimum of det J over the volume quadrature points [E]
+ * (the regularisation inputs of the explicitly formed LM subproblem) */
+int orc_cg_stiffness(const orc_problem* pb, const double* coord, double* K);
+int orc_min_detj(const orc_problem* pb, const double* coord, double* mins);
+
+/* selected nodes sel[nsel] and parameter offsets cols[nsel + 1] of an MDG
+ * selection; returns nsel */
+int orc_mdg_layout(const orc_problem* pb, const double* coord, int ntr, const int* traces, int hyper, int* sel,
+                   int* cols);
+
 /* element mass matrices [E][nb][nb] (finite_element.hpp:587-610) */
 int orc_mass_matrices(const orc_problem* pb, const double* coord, double* M);
 /* explicit time stepping: scheme 0 Euler, 1 TVD-RK3, 2 SSP-RK3; dt_kind 0

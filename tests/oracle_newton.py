@@ -170,3 +170,180 @@ def mfnk(pb, coord, u0, tau_abs=1e-9, kmax=30, rtol=1e-6, restart=30, maxit=5000
         if np.linalg.norm(r) <= tau_abs:
             break
     return u, k
+
+
+def mdg_layout(pb, coord, traces, hyper=True):
+    """(selected nodes, parameter offsets cols[nsel + 1]) of an MDG selection"""
+    import ctypes as C
+    nn = (pb.nx * pb.geo_order + 1) * (pb.ny * pb.geo_order + 1)
+    tr = np.ascontiguousarray(traces, dtype=np.int32)
+    sel = np.zeros(nn, dtype=np.int32)
+    cols = np.zeros(nn + 1, dtype=np.int32)
+    f = ob.oracle().fn("mdg_layout")
+    n = f(C.byref(pb), ob._ptr(coord), len(tr), ob._ptr(tr), int(hyper), ob._ptr(sel), ob._ptr(cols))
+    assert n >= 0
+    return sel[:n].copy(), cols[:n + 1].copy()
+
+
+def mdg_jacobian_sparse(pb, coord, traces, u, x, hyper=True):
+    """[res; ic] and the sparse Jacobian (CSR) w.r.t. [u; x] of the oracle
+    (form_petsc_jacobian_fd + form_petsc_mdg_jacobian_fd)"""
+    import ctypes as C
+    E, nb, N = ob.sizes(pb)
+    neq = ob.neq(pb)
+    sel, cols = mdg_layout(pb, coord, traces, hyper)
+    nres, ncol = N + len(sel) * neq, N + len(x)
+    tr = np.ascontiguousarray(traces, dtype=np.int32)
+    bs = nb * neq
+    cap = 5 * E * bs * bs + 64 * len(sel) * (bs + 4) + 1024
+    f = ob.oracle().fn("mdg_jacobian_coo")
+    f.restype = C.c_longlong
+    while True:
+        rows = np.zeros(cap, dtype=np.int32)
+        cls = np.zeros(cap, dtype=np.int32)
+        vals = np.zeros(cap)
+        out = np.zeros(nres)
+        n = f(C.byref(pb), ob._ptr(coord), len(tr), ob._ptr(tr), int(hyper), ob._ptr(np.ascontiguousarray(u)),
+              ob._ptr(np.ascontiguousarray(x)), ob._ptr(out), C.c_longlong(cap), ob._ptr(rows), ob._ptr(cls),
+              ob._ptr(vals))
+        assert n >= 0
+        if n <= cap:
+            break
+        cap = int(n)
+    J = sp.coo_matrix((vals[:n], (rows[:n], cls[:n])), shape=(nres, ncol)).tocsr()
+    return out, J
+
+
+def _coords_from_x(pb, coord0, sel, cols, x):
+    """mesh nodes with the selected nodes' free coordinates from x (the
+    fixed coordinates of a boundary node stay where they are)"""
+    c = coord0.reshape(-1, 2).copy()
+    for k, node in enumerate(sel):
+        free = [d for d in range(2) if not _fixed(pb, node, d)]
+        for i, d in enumerate(free):
+            c[node, d] = x[cols[k] + i]
+    return c.reshape(coord0.shape)
+
+
+def _fixed(pb, node, d):
+    """hyper_rectangle: the coordinate d of a node of the order-1 lattice index on the box is fixed"""
+    if node >= (pb.nx + 1) * (pb.ny + 1):
+        return False
+    ix, iy = node % (pb.nx + 1), node // (pb.nx + 1)
+    return (ix in (0, pb.nx)) if d == 0 else (iy in (0, pb.ny))
+
+
+def lm_explicit(pb, coord, traces, u0, x0, kmax=5, lambda_u=1e-7, lambda_b=1e-2, lambda_lag=1e-5, tau_abs=1e-10,
+                max_rejections=20, history=None):
+    """CorriganLM::solve with the explicitly formed subproblem
+    (corrigan_lm.hpp:363-717, explicitly_form_subproblem = true, Corrigan line
+    search): (J^T J + diag(lambda_u |J_col|, lambda_b |J_col|)
+    + lambda_lag |r| K^T K + lambda_el) p = J^T r solved exactly (sparse LU),
+    u <- u - alpha p_u, x <- x - alpha p_x, acceptance when no element inverts
+    and |r_step| < 10 |r_old|, the lambda updates and the element-wise
+    regularisation of the reference. K^T K is formed as the reference forms it:
+    its loop assigns KTK[i, j] = K[k, i] K[k, j] for every k in turn, so the
+    last basis function's row k = ng - 1 is what remains (corrigan_lm.hpp:463-469).
+    Returns (u, x, residual norm history, alpha history)."""
+    import ctypes as C
+    u, x = np.array(u0, dtype=float), np.array(x0, dtype=float)
+    E, nb, N = ob.sizes(pb)
+    g = pb.geo_order
+    ng = (g + 1) ** 2
+    sel, cols = mdg_layout(pb, coord, traces)
+    inv = {int(n): k for k, n in enumerate(sel)}
+    free = [[d for d in range(2) if not _fixed(pb, int(n), d)] for n in sel]
+    conn, _, _ = ob.topology(ob.oracle(), pb)
+    coord0 = np.ascontiguousarray(coord)
+    ncol = N + len(x)
+
+    def state(xv):
+        return np.ascontiguousarray(_coords_from_x(pb, coord0, sel, cols, xv))
+
+    def cg_K(cw):
+        K = np.zeros((E, ng, ng))
+        assert ob.oracle().fn("cg_stiffness")(C.byref(pb), ob._ptr(cw), ob._ptr(K)) == 0
+        return K
+
+    def min_det(cw):
+        m = np.zeros(E)
+        assert ob.oracle().fn("min_detj")(C.byref(pb), ob._ptr(cw), ob._ptr(m)) == 0
+        return m
+
+    def geo_pairs(e):
+        """(row, col) positions of the free coordinates of every pair of selected nodes of element e"""
+        out = []
+        for il in range(ng):
+            ki = inv.get(int(conn[e, il]))
+            if ki is None:
+                continue
+            for jl in range(ng):
+                kj = inv.get(int(conn[e, jl]))
+                if kj is None:
+                    continue
+                for iv in range(len(free[ki])):
+                    for jv in range(len(free[kj])):
+                        out.append((il, jl, N + cols[ki] + iv, N + cols[kj] + jv))
+        return out
+
+    pairs = [geo_pairs(e) for e in range(E)]
+    out, J = mdg_jacobian_sparse(pb, state(x), traces, u, x)
+    hist = [np.linalg.norm(out)]
+    alphas = []
+    lu, lb, lu_min = lambda_u, lambda_b, lambda_u
+    lam_el = np.zeros(E)
+    k, rejects = 0, 0
+    while k < kmax and hist[-1] > tau_abs:
+        rnorm = np.linalg.norm(out)
+        Jt = J.T.tocsr()
+        A = (Jt @ J).tocoo()
+        cn = np.sqrt(np.asarray(J.multiply(J).sum(axis=0)).ravel())
+        d = np.concatenate([lu * cn[:N], lb * cn[N:]])
+        rr, cc, vv = [A.row], [A.col], [A.data]
+        rr.append(np.arange(ncol)); cc.append(np.arange(ncol)); vv.append(d)
+        Kall = cg_K(state(x))
+        ri, ci, vi = [], [], []
+        for e in range(E):
+            Kl = Kall[e]
+            KTK = np.outer(Kl[ng - 1], Kl[ng - 1])
+            for il, jl, r, c in pairs[e]:
+                ri.append(r); ci.append(c); vi.append(KTK[il, jl] * lambda_lag * rnorm)
+            if lam_el[e] > 0.0:
+                for il, jl, r, c in pairs[e]:
+                    if il == jl:
+                        ri.append(r); ci.append(c); vi.append(lam_el[e])
+        rr.append(np.array(ri, dtype=np.int64)); cc.append(np.array(ci, dtype=np.int64)); vv.append(np.array(vi))
+        M = sp.coo_matrix((np.concatenate(vv), (np.concatenate(rr), np.concatenate(cc))), shape=(ncol, ncol)).tocsc()
+        p = spla.spsolve(M, Jt @ out)
+        last = {}
+
+        def phi(a):
+            o = ob.mdg_residual(ob.oracle(), pb, state(x - a * p[N:]), traces, u - a * p[:N], x - a * p[N:])
+            v = np.linalg.norm(o[:N]) + np.linalg.norm(o[N:])
+            last["v"], last["x"] = v, x - a * p[N:]
+            return v
+        alpha = corrigan_ls(phi)
+        mins = min_det(state(last["x"]))
+        reset = False
+        for e in range(E):
+            if mins[e] < 0.0:
+                reset = True
+                lam_el[e] = lb if lam_el[e] == 0 else lam_el[e] * max(1.5, abs(mins[e]))
+        if not reset and last["v"] < 10 * rnorm:
+            u, x = u - alpha * p[:N], x - alpha * p[N:]
+            lu, lb = max(lu_min, 0.55 * lu), max(last["v"], 0.55 * lb)
+            lam_el[lam_el > 0] /= 1.5
+            rejects = 0
+            alphas.append(alpha)
+        else:
+            lu, lb = lu * 1.8, lb * 1.8
+            rejects += 1
+            if rejects > max_rejections:
+                break
+            continue
+        out, J = mdg_jacobian_sparse(pb, state(x), traces, u, x)
+        hist.append(np.linalg.norm(out))
+        if history is not None:
+            history.append((hist[-1], alpha))
+        k += 1
+    return u, x, hist, alphas
