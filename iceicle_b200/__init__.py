@@ -189,6 +189,9 @@ def lib():
             "icx_gemm_bf16_nt": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, vp,
                                            C.c_int, vp, C.c_int, C.c_int, C.c_int, vp]),
             "icx_get_ilu_tile": (C.c_int, [vp]),
+            "icx_set_ilu_groups": (C.c_int, [vp, vp]),
+            "icx_pc_factor": (C.c_int, [vp, vp, C.c_int]),
+            "icx_pc_apply": (C.c_int, [vp, vp, vp, C.c_int, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -364,6 +367,20 @@ class Context:
     @ilu_tile.setter
     def ilu_tile(self, tile):
         self._check(lib().icx_set_ilu_tile(self._h, int(tile)), "set_ilu_tile")
+
+    def set_ilu_groups(self, groups):
+        """block-ILU(0) per element group (array of E ints), None: back to the tiling"""
+        g = None if groups is None else np.ascontiguousarray(groups, dtype=np.int32)
+        self._check(lib().icx_set_ilu_groups(self._h, _ptr(g) if g is not None else None), "set_ilu_groups")
+        self._groups = g
+
+    def pc_factor(self, vals, precision=0):
+        """block-ILU(0) factors of the BSR values (the tiling / groups in force)"""
+        self._check(lib().icx_pc_factor(self._h, _ptr(vals), precision), "pc_factor")
+
+    def pc_apply(self, x, y, precision=0, stream=None):
+        """y = M^-1 x with the factors of the last pc_factor"""
+        self._check(lib().icx_pc_apply(self._h, _ptr(x), _ptr(y), precision, _stream_ptr(stream)), "pc_apply")
 
     def autotune(self, u, parts=TUNE_RESIDUAL | TUNE_ILU | TUNE_ILU_FP32):
         """times every compiled launch shape of the selected kernels at the

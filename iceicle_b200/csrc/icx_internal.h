@@ -142,6 +142,8 @@ struct icx_ctx {
   std::vector<int> el_level;                  // [E] anti-diagonal index i + j of the element in its grid
   std::vector<int> el_i, el_j, el_grid;       // [E] grid position (i, j) of the element and its grid's index
   int ilu_tile = 0;                           // block-ILU(0) on s x s element tiles (0: the whole grid)
+  std::vector<int> ilu_groups;                // block-ILU(0) per element group (set: overrides ilu_tile)
+  int ilu_plan_gen = 1;                       // changes whenever the tiling or the groups change
   // a batch of independent problems (icx_batch_create): the parts it was
   // built from (not owned) and each element's Burgers coefficients (mu, a0, a1, b0, b1)
   std::vector<icx_ctx*> parts;

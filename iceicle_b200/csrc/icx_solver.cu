@@ -28,7 +28,8 @@
 // levels of the factorisation and of each triangular sweep fall from
 // nx + ny - 1 to 2s - 1.
 struct IluTilePlan {
-  int tile = 0;                 // 0: no plan (natural order over the whole grid)
+  int tile = 0;                 // nonzero: a plan is built (s, or -1 for element groups)
+  int gen = 0;                  // icx_ctx::ilu_plan_gen it was built for
   int nnzb = 0;                 // blocks kept
   int* rowptr = nullptr;        // [E + 1] kept pattern, columns ascending
   int* colidx = nullptr;        // [nnzb]
@@ -173,20 +174,25 @@ void free_tile_plan(IluTilePlan& tp) {
   tp = IluTilePlan();
 }
 
-// builds the tiled pattern for c->ilu_tile (nothing to do when it is built or 0)
+// builds the pattern of the tiled (c->ilu_tile) or grouped (c->ilu_groups)
+// block-ILU(0); nothing to do when it is built or when neither is set
 icx_status ensure_ilu_plan(icx_ctx* c) {
   icx_solver_work* w = c->sw;
-  const int st = c->ilu_tile;
-  if (st == w->tp.tile) return ICX_OK;
+  const bool grouped = !c->ilu_groups.empty();
+  const int st = grouped ? -1 : c->ilu_tile;
+  if (st == w->tp.tile && (st == 0 || w->tp.gen == c->ilu_plan_gen)) return ICX_OK;
   free_tile_plan(w->tp);
   if (st == 0) return ICX_OK;
   const icx::DeviceMesh& dm = c->dm;
-  if ((int)c->el_i.size() != dm.E || (int)c->el_j.size() != dm.E || (int)c->el_grid.size() != dm.E)
+  if (grouped && (int)c->ilu_groups.size() != dm.E)
+    return set_err(c, ICX_ERR_INVALID, "ILU element groups: one group per element");
+  if (!grouped && ((int)c->el_i.size() != dm.E || (int)c->el_j.size() != dm.E || (int)c->el_grid.size() != dm.E))
     return set_err(c, ICX_ERR_UNSUPPORTED, "tiled block-ILU(0) needs the elements' grid positions");
   std::vector<int> rp(dm.E + 1), ci(dm.nnzb);
   CK(cudaMemcpy(rp.data(), dm.bsr_rowptr, sizeof(int) * rp.size(), cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(ci.data(), dm.bsr_colidx, sizeof(int) * ci.size(), cudaMemcpyDeviceToHost));
   auto tile_of = [&](int e) -> long long {
+    if (grouped) return c->ilu_groups[e];
     return ((long long)c->el_grid[e] << 42) | ((long long)(c->el_i[e] / st) << 21) | (long long)(c->el_j[e] / st);
   };
   std::vector<int> trp(dm.E + 1, 0), tci, tdiag(dm.E, -1), tmap;
@@ -205,10 +211,12 @@ icx_status ensure_ilu_plan(icx_ctx* c) {
     trp[e + 1] = (int)tci.size();
     if (tdiag[e] < 0) return set_err(c, ICX_ERR_INVALID, "block pattern without a diagonal block");
   }
+  // levels of the kept lower-triangular dependencies in natural order (on a
+  // tile: (i mod s) + (j mod s))
   int nl = 0;
-  std::vector<int> lvl(dm.E);
+  std::vector<int> lvl(dm.E, 0);
   for (int e = 0; e < dm.E; ++e) {
-    lvl[e] = c->el_i[e] % st + c->el_j[e] % st;
+    for (int kb = trp[e]; kb < tdiag[e]; ++kb) lvl[e] = std::max(lvl[e], lvl[tci[kb]] + 1);
     nl = std::max(nl, lvl[e] + 1);
   }
   IluTilePlan tp;
@@ -230,6 +238,7 @@ icx_status ensure_ilu_plan(icx_ctx* c) {
     }
   }
   tp.tile = st;
+  tp.gen = c->ilu_plan_gen;
   w->tp = std::move(tp);
   return ICX_OK;
 }
@@ -621,7 +630,43 @@ icx_status icx_newton_default_options(icx_newton_options* o) {
 icx_status icx_set_ilu_tile(icx_ctx* c, int tile) {
   if (!c) return ICX_ERR_INVALID;
   if (tile < 0 || tile > (1 << 20)) return set_err(c, ICX_ERR_INVALID, "ILU tile side must be in 0..2^20");
+  if (tile != c->ilu_tile) ++c->ilu_plan_gen;
   c->ilu_tile = tile;
+  return ICX_OK;
+}
+
+icx_status icx_set_ilu_groups(icx_ctx* c, const int* groups) {
+  if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
+  if (groups) c->ilu_groups.assign(groups, groups + c->dm.E);
+  else c->ilu_groups.clear();
+  ++c->ilu_plan_gen;
+  return ICX_OK;
+}
+
+icx_status icx_pc_factor(icx_ctx* c, const double* d_vals, int precision) {
+  if (!c || !c->ready || !d_vals) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed / null pointer");
+  if (precision < 0 || precision > 1) return set_err(c, ICX_ERR_INVALID, "precision 0 or 1");
+  icx_status st = ensure_work(c, 30);
+  if (st != ICX_OK) return st;
+  const bool mixed = precision == 1;
+  if (mixed && (st = ensure_mixed(c)) != ICX_OK) return st;
+  icx_solver_work* w = c->sw;
+  cudaStream_t s = 0;
+  CK(cudaMemcpyAsync(w->vals, d_vals, sizeof(double) * (size_t)c->dm.nnzb * w->bs * w->bs, cudaMemcpyDeviceToDevice,
+                     s));
+  CK(build_pc(c, 2, mixed, s));
+  int fl = 0;
+  CK(cudaMemcpyAsync(&fl, w->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SYNC_AT("preconditioner");
+  if (fl == 2) return set_err(c, ICX_ERR_CUDA, "block-ILU factorization: block index out of range");
+  if (fl == 1) return set_err(c, ICX_ERR_NONFINITE, "block-ILU factorization: singular diagonal block");
+  return ICX_OK;
+}
+
+icx_status icx_pc_apply(icx_ctx* c, const double* d_x, double* d_y, int precision, void* stream) {
+  if (!c || !c->sw || !d_x || !d_y || d_x == d_y) return set_err(c, ICX_ERR_INVALID, "no factors / bad pointers");
+  if (precision == 1 && !c->sw->vals32) return set_err(c, ICX_ERR_INVALID, "no FP32 factors (icx_pc_factor)");
+  CK(apply_pc(c, 2, precision == 1, d_x, d_y, (cudaStream_t)stream));
   return ICX_OK;
 }
 

@@ -338,6 +338,17 @@ icx_status icx_gmres_solve(icx_ctx* ctx, const double* d_vals, const double* d_b
  * reference counterpart: the reference selects the PC through PETSc options. */
 icx_status icx_set_ilu_tile(icx_ctx* ctx, int tile);
 int icx_get_ilu_tile(const icx_ctx* ctx);
+/* block-ILU(0) per element group: groups[E] (NULL: back to the tiling) - the
+ * blocks coupling two groups are dropped, e.g. a partitioned mesh's owned
+ * elements in one group and each ghost row in its own, which is the
+ * block-Jacobi across ranks of PETSc's parallel default (bjacobi + ilu)
+ * (no reference counterpart as an entry point) */
+icx_status icx_set_ilu_groups(icx_ctx* ctx, const int* groups);
+/* the block-ILU(0) preconditioner alone (PCSetUp / PCApply of
+ * petsc_newton.hpp:179-183): factor the BSR values d_vals (precision 1: also
+ * its FP32 copies), then apply y = M^-1 x on a stream, any number of times */
+icx_status icx_pc_factor(icx_ctx* ctx, const double* d_vals, int precision);
+icx_status icx_pc_apply(icx_ctx* ctx, const double* d_x, double* d_y, int precision, void* stream);
 icx_status icx_ilu_apply(icx_ctx* ctx, const double* d_vals, const double* d_x, double* d_y, int precision,
                          int schedule, int repeat, double* ms_per_apply);
 icx_status icx_newton_default_options(icx_newton_options* opt);

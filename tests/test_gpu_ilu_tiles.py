@@ -129,3 +129,52 @@ def test_newton_with_tiled_ilu_reaches_same_state(tile):
     base = out[(0, 0)][0]
     for key, (u, _) in out.items():
         assert np.linalg.norm(u - base) <= 1e-10 * np.linalg.norm(base), key
+
+
+def test_element_groups_and_separate_factor_apply():
+    """icx_set_ilu_groups + icx_pc_factor / icx_pc_apply: groups equal to the
+    2 x 2 tiles give the tiled apply bit for bit; one group holding every
+    element is the whole grid's ILU(0)"""
+    spec = Spec(pde=NS, nx=6, ny=5, p=2, ip=True)
+    ctx = spec.context()
+    vals, _, _, _ = _jacobian(ctx, spec)
+    x = torch.from_numpy(np.random.default_rng(2).standard_normal(ctx.layout.n_dof)).cuda()
+    y_tile, y_grp, y_all, y_nat = (torch.empty_like(x) for _ in range(4))
+    ctx.ilu_tile = 2
+    ctx.ilu_apply(vals, x, y_tile, 0, 1)
+    ctx.ilu_tile = 0
+    e = np.arange(30)
+    ctx.set_ilu_groups((e % 6) // 2 + 3 * ((e // 6) // 2))
+    ctx.pc_factor(vals, 0)
+    ctx.pc_apply(x, y_grp, 0)
+    ctx.set_ilu_groups(np.zeros(30))
+    ctx.pc_factor(vals, 0)
+    ctx.pc_apply(x, y_all, 0)
+    ctx.set_ilu_groups(None)
+    ctx.ilu_apply(vals, x, y_nat, 0, 1)
+    torch.cuda.synchronize()
+    assert torch.equal(y_tile.view(torch.int64), y_grp.view(torch.int64))
+    assert float((y_all - y_nat).abs().max()) <= 1e-12 * float(y_nat.abs().max())
+    ctx.close()
+
+
+def test_strip_krylov_on_one_rank_matches_gmres():
+    """the partitioned GMRES (iceicle_b200.partition.StripKrylov) over a GPU
+    context with one rank: BSR product and the owned-block ILU(0) through
+    icx_pc_factor / icx_pc_apply; the solution equals icx_gmres_solve's"""
+    from iceicle_b200.partition import StripKrylov, StripPlan
+    spec = Spec(pde=NS, nx=8, ny=8, p=2, ip=True)
+    ctx = spec.context()
+    vals, _, _, _ = _jacobian(ctx, spec)
+    b = torch.from_numpy(np.random.default_rng(6).standard_normal(ctx.layout.n_dof)).cuda()
+    plan = StripPlan(spec.nx, spec.ny, 1, 0, spec.g)
+    kry = StripKrylov.for_context(ctx, plan, vals)
+    x = torch.zeros_like(b)
+    its, rel = kry.solve(b, x, m=30, rtol=1e-12, maxit=5000)
+    ctx.set_ilu_groups(None)
+    x2 = torch.zeros_like(b)
+    ctx.gmres_solve(vals, b, x2, restart=30, maxit=5000, rtol=1e-12, preconditioner=2)
+    torch.cuda.synchronize()
+    assert rel <= 1e-12
+    assert float((x - x2).norm() / x2.norm()) <= 1e-9
+    ctx.close()
