@@ -265,6 +265,34 @@ def batched_bench(torch, dev, n_problems):
             "speedup": t_seq / t_batch if t_batch > 0 else None, "max_state_rel_diff": worst, "groups": its}
 
 
+def roe_residual_bench(torch, dev, flush, tune=True, steps=20):
+    """the residual workload with the Roe convective flux the configuration
+    names (the headline line keeps Van Leer, the flux the reference has, so
+    that both arms time the same discretization): device time per residual
+    with L2 flushed between steps"""
+    import iceicle_b200 as ib
+    from iceicle_b200.workloads import ns_mms_config
+    wl = ns_mms_config(nx=NX, ny=NY, p=3, geo_order=2, device=dev.index, conv_flux=ib.FLUX_ROE)
+    u = torch.from_numpy(wl.u0).to(dev)
+    res = torch.empty_like(u)
+    if tune:
+        wl.ctx.autotune(u, ib.TUNE_RESIDUAL)
+    for _ in range(3):
+        wl.ctx.form_residual(u, res)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize(dev)
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record()
+        wl.ctx.form_residual(u, res)
+        e1.record()
+    torch.cuda.synchronize(dev)
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / steps
+    n = wl.ctx.layout.n_dof
+    del wl
+    return {"conv_flux": "roe", "ms": ms, "dof_per_s": n / (ms * 1e-3)}
+
+
 def jacobian_work(L):
     """algorithmic bytes (BSR values written once, u read) and an FP64 flop
     count of one FD Jacobian as the element kernel computes it: per element
@@ -739,6 +767,7 @@ def run_ours(a):
             else:
                 line["cpu_baseline"] = None
         if ws == 1:
+            line["residual_roe"] = roe_residual_bench(torch, dev, flush, tune is not None)
             line["jacobian"] = jacobian_bench(torch, dev, wl, hbm, not a.no_cpu_baseline)
         if not a.no_newton and ws == 1:
             line["newton"] = newton_bench(torch, dev, not a.no_tune)

@@ -78,7 +78,7 @@ class Spec:
 
     def _params(self, name, prm):
         if name.startswith("ns_mms"):
-            arr = ns_mms_params()
+            arr = ns_mms_params(mu=self.ns_mu)
         else:
             arr = (C.c_double * len(prm))(*prm)
         self._keep.append(arr)
@@ -94,7 +94,7 @@ class Spec:
         product's workload builder"""
         pb = self._geometry_problem()
         xy = ob.basis_node_coords(pb, coords).reshape(-1, 2)
-        prm = ns_mms_params()
+        prm = ns_mms_params(mu=self.ns_mu)
         f = self.fn("ns_mms_state")
         st = np.zeros((xy.shape[0], 4))
         out = (C.c_double * 4)()

@@ -59,6 +59,39 @@ def test_ns_128x128_p3_residual_full_size():
     assert np.abs(r - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+def test_ns_128x128_p3_roe_residual_full_size():
+    """the same workload with the Roe flux the configuration names (parity
+    unpinned against the reference, which has no Roe flux: here against the
+    oracle's restatement of the published algorithm)"""
+    import iceicle_b200 as ib
+    from iceicle_b200.workloads import ns_mms_config
+    spec = Spec(pde=NS, nx=128, ny=128, p=3, g=2, ip=True, source=True, perturb=0.05, seed=4321, ns_flux=2)
+    wl = ns_mms_config(nx=128, ny=128, p=3, geo_order=2, conv_flux=ib.FLUX_ROE)
+    c, u = _same_inputs(spec, wl)
+    du = torch.from_numpy(wl.u0).cuda()
+    dr = torch.full_like(du, float("nan"))
+    wl.ctx.form_residual(du, dr)
+    torch.cuda.synchronize()
+    ref = ob.residual(ob.oracle(), spec.oracle_problem(), c, wl.u0)
+    assert np.abs(dr.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_ns_256x256_p2_residual_full_size():
+    """the learned-preconditioner workload's mesh and order (256 x 256, p = 2,
+    2,359,296 unknowns) at Re = 300"""
+    from iceicle_b200.workloads import ns_mms_config
+    spec = Spec(pde=NS, nx=256, ny=256, p=2, g=2, ip=True, source=True, perturb=0.05, seed=4321, ns_mu=1.0 / 300)
+    wl = ns_mms_config(nx=256, ny=256, p=2, geo_order=2, mu=1.0 / 300)
+    c = spec.coords()
+    assert np.array_equal(c, wl.coords)
+    du = torch.from_numpy(wl.u0).cuda()
+    dr = torch.full_like(du, float("nan"))
+    wl.ctx.form_residual(du, dr)
+    torch.cuda.synchronize()
+    ref = ob.residual(ob.oracle(), spec.oracle_problem(), c, wl.u0)
+    assert np.abs(dr.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 def test_ns_128x128_p3_newton_iterates_full_size():
     """one Newton step per call (Wolfe line search, GMRES(30) + block-ILU(0)
     to 1e-12): each iterate's residual norm as the GPU reports it equals the
