@@ -372,6 +372,11 @@ __global__ void __launch_bounds__(128, (FaceCfg<PDE, P, G, DDG>::MINB + MO)) fac
       fg[(1 * NQF + q) * 2 + 1] = gq[3];
     }
   }
+  // the volume kernel may be launched now (programmatic dependent launch): it
+  // stages its tables, geometry and coefficient tiles while the last face
+  // CTAs finish, and waits for this grid's completion before it reads the
+  // face fluxes
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 // ----------------------------------------------------- volume + face lifting
@@ -465,7 +470,11 @@ __global__ void __launch_bounds__(NT, MB) vol_lift_kernel(DeviceMesh dm, PhysPar
   }
   // face records and the stored fluxes of the element's faces: one packed
   // record load, then the copy, issued by the same thread (completed before
-  // the lifting stage reads them)
+  // the lifting stage reads them). Launched as a programmatic dependent of the
+  // face kernel, everything above overlaps that kernel's tail; the face
+  // fluxes are read only once it has completed and its stores are visible
+  // (a no-op for an ordinary launch)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   for (int t = tid; t < ne * 4; t += V::THREADS) {
     int fso = dm.el_fso[(size_t)e0 * 4 + t];
     int fidx = fso >> 2;
@@ -702,25 +711,39 @@ static cudaError_t face_pick(const DeviceMesh& dm, const PhysParams& pp, const d
   return cudaErrorInvalidValue;
 }
 
+// pdl: launch as a programmatic dependent of the face kernel just launched on s
 template <int PDE, int P, int G, int T, int MB>
 static cudaError_t vol_launch(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
-                              cudaStream_t s) {
+                              cudaStream_t s, bool pdl) {
   using V = VolCfg<PDE, P, G, T>;
   constexpr auto K = vol_lift_kernel<PDE, P, G, T, MB>;
   cudaError_t e = smem_attr_once<K>(V::SMEM);
   if (e != cudaSuccess) return e;
-  K<<<(dm.E + V::EPB - 1) / V::EPB, T, V::SMEM, s>>>(dm, pp, u, res);
-  return cudaSuccess;
+  if (!pdl) {
+    K<<<(dm.E + V::EPB - 1) / V::EPB, T, V::SMEM, s>>>(dm, pp, u, res);
+    return cudaSuccess;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((dm.E + V::EPB - 1) / V::EPB);
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = V::SMEM;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, K, dm, pp, u, res);
 }
 
 template <int PDE, int P, int G>
 static cudaError_t vol_pick(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
-                            cudaStream_t s) {
+                            cudaStream_t s, bool pdl = false) {
   const int t = dm.tile.vol_threads ? dm.tile.vol_threads : kVolTiles[0].threads;
   const int mb = dm.tile.vol_minb ? dm.tile.vol_minb : (t == kVolTiles[0].threads ? kVolTiles[0].minb : 0);
 #define ICX_VOL_TILE(I)                                                                      \
   if (t == kVolTiles[I].threads && mb == kVolTiles[I].minb)                                  \
-    return vol_launch<PDE, P, G, kVolTiles[I].threads, kVolTiles[I].minb>(dm, pp, u, res, s);
+    return vol_launch<PDE, P, G, kVolTiles[I].threads, kVolTiles[I].minb>(dm, pp, u, res, s, pdl);
   ICX_VOL_TILE(0) ICX_VOL_TILE(1) ICX_VOL_TILE(2) ICX_VOL_TILE(3)
 #undef ICX_VOL_TILE
   return cudaErrorInvalidValue;
@@ -731,8 +754,10 @@ static cudaError_t residual_pg(const DeviceMesh& dm, const PhysParams& pp, const
                                cudaStream_t s, cudaEvent_t mid) {
   cudaError_t e = pp.beta1 != 0.0 ? face_pick<PDE, P, G, true>(dm, pp, u, s) : face_pick<PDE, P, G, false>(dm, pp, u, s);
   if (e != cudaSuccess) return e;
+  // the volume kernel follows as a programmatic dependent launch, except when
+  // an event splits the two for timing
   if (mid) cudaEventRecord(mid, s);
-  if ((e = vol_pick<PDE, P, G>(dm, pp, u, res, s)) != cudaSuccess) return e;
+  if ((e = vol_pick<PDE, P, G>(dm, pp, u, res, s, mid == nullptr)) != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

@@ -43,6 +43,7 @@ PRELUDE = r'''
 #include <functional>
 #include <vector>
 #include "iceicle_b200.h"
+#include "iceicle_b200.hpp"
 // the reference-side objects the call sites name (shapes as in the reference)
 struct Coeffs { double mu; std::array<double, 2> a, b; };
 struct Disc { bool interior_penalty; double sigma_ic;
@@ -54,7 +55,10 @@ void integration_call_sites(icx_ctx* ctx_past, icx_ctx** parts, int n_parts, dou
                             double* d_samples, double* d_res_and_ic, void* stream) {
   int nx = 8, ny = 8, geometry_order = 2, basis_order = 2, p = 2, cap = 16, ns = 0, it = 0, k = 1, itime = 0;
   long long n_dof = 0;
-  double rr = 0.0, tfinal = 1.0;
+  double rr = 0.0, tfinal = 1.0, mu = 0.01, T0 = 0.004, T1 = 0.005, rho_inf = 1.0, u_inf = 0.5, T_inf = 0.004;
+  double* d_y = d_x;
+  std::vector<int> groups_v(64, 0);
+  const int* groups = groups_v.data();
   Coeffs coeffs{0.01, {0.0, 0.0}, {1.0, 0.5}}, c = coeffs;
   Disc disc{false, 0.0, {}};
   disc.dirichlet_callbacks.push_back([](const double*, double* out) { out[0] = 0.0; });
@@ -70,9 +74,11 @@ def test_integration_md_call_sites_compile(tmp_path):
     text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     blocks = re.findall(r"```cpp\n(.*?)```", text, flags=re.S)
     assert len(blocks) >= 2
-    body = "\n".join(b.replace('#include "iceicle_b200.h"', "") for b in blocks)
+    # the facade example is self-contained: its own scope (its names repeat the reference-side ones)
+    body = "\n".join(("{\n" + b.replace('#include "iceicle_b200.hpp"', "") + "\n}") if "iceicle_b200.hpp" in b
+                     else b.replace('#include "iceicle_b200.h"', "") for b in blocks)
     src = tmp_path / "call_sites.cpp"
     src.write_text(PRELUDE + body + "\n}\n")
     r = subprocess.run(["g++", "-std=c++23", "-fsyntax-only", "-Wno-unused-variable", "-I",
-                        os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
+                        os.path.join(ROOT, "include"), "-I", CUDA_INC, str(src)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-4000:]
