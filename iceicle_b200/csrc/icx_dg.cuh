@@ -126,23 +126,97 @@ __device__ inline void load_face_pt(const DeviceMesh& dm, int nqf, int f, int q,
   }
 }
 
-// numerical flux at a face point from both sides' states.
+// numerical flux at a face point from both sides' states, in two parts that
+// the face kernel may evaluate on two threads: the convective part fadv
+// (face_conv_part, also the interface-correction coefficients gq) and the
+// viscous part fvis (face_visc_part); face_flux_states runs both.
 // out[NEQ] = (f_visc - f_adv) * w * sqrt(g); with the interface correction
 // active, gq[4] = the pulled-back coefficients of dphi/dxi for the left
 // (gq[0..1]) and right (gq[2..3]) test functions.
 // bval: Dirichlet state or Neumann data at this boundary point.
+
+// the exterior state of a boundary point whose flux uses one: Dirichlet data,
+// a connected past slab, or a PDE-level boundary; false for the other kinds
+template <int PDE>
+__device__ inline bool face_exterior(const PhysParams& pp, const FacePt& fp, int bct, const double* bval,
+                                     const double* uL, double* ud) {
+  constexpr int NEQ = Phys<PDE>::NEQ;
+  if (bct == ICX_BC_DIRICHLET || (bct == ICX_BC_SPACETIME_PAST && pp.st_connected)) {
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) ud[eq] = bval[eq];
+    return true;
+  }
+  if (Phys<PDE>::has_pde_bcs && bct >= ICX_BC_RIEMANN && bct <= ICX_BC_WALL_GENERAL) {
+    Phys<PDE>::apply_bc(pp, uL, fp.n, bct, bval, ud);
+    return true;
+  }
+  return false;
+}
+
+// convective part (zero where the face has none) and the interface-correction coefficients
 template <int PDE, bool DDG>
-__device__ inline void face_flux_states(const PhysParams& pp, const FacePt& fp, bool interior, int bct,
-                                        const double* bval, const double* uL, const double* gL, const double* hL,
-                                        const double* uR, const double* gR, const double* hR, double* out,
-                                        double* gq) {
+__device__ inline void face_conv_part(const PhysParams& pp, const FacePt& fp, bool interior, int bct,
+                                      const double* bval, const double* uL, const double* uR, double* fadv,
+                                      double* gq) {
   constexpr int NEQ = Phys<PDE>::NEQ;
   const double* n = fp.n;
-  const double wsq = fp.wsq, h = fp.h;
-  double fadv[NEQ], fvis[NEQ];
+  const double wsq = fp.wsq;
   const bool ic = Phys<PDE>::has_ic && pp.sigma_ic != 0.0;
+  double ud[NEQ];
   if (interior) {
     Phys<PDE>::conv_sel(pp, uL, uR, n, fadv);
+    if (ic) {
+      // resL, resR -= sum_s (sigma mu n_s [u] w sqrt(g) / 2) dphi/dx_s   (conservation_law.hpp:580-610)
+      double cs[2];
+#pragma unroll
+      for (int s = 0; s < 2; ++s) cs[s] = 0.5 * pp.sigma_ic * pp.mu * n[s] * (uR[0] - uL[0]) * wsq;
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk) {
+        gq[0 * 2 + kk] = cs[0] * fp.JiL[kk * 2 + 0] + cs[1] * fp.JiL[kk * 2 + 1];
+        gq[1 * 2 + kk] = cs[0] * fp.JiR[kk * 2 + 0] + cs[1] * fp.JiR[kk * 2 + 1];
+      }
+    }
+  } else if (face_exterior<PDE>(pp, fp, bct, bval, uL, ud)) {
+    // a connected SPACETIME_PAST face takes the past slab's trace as exterior
+    // state; on a slab interface at constant t the diffusive normal flux
+    // vanishes (no diffusion along t), leaving the time-upwind flux. The
+    // PDE-level kinds (walls, characteristic) form the exterior state from
+    // the interior one and then take the same DDG boundary flux as a
+    // Dirichlet face with one-sided gradients (conservation_law.hpp:1043-1130)
+    Phys<PDE>::conv_sel(pp, uL, ud, n, fadv);
+    if (ic) {
+      // resL -= sum_s sigma mu n_s [u] w sqrt(g) dphi/dx_s   (conservation_law.hpp:735-760)
+      double cs[2];
+#pragma unroll
+      for (int s = 0; s < 2; ++s) cs[s] = pp.sigma_ic * pp.mu * n[s] * (ud[0] - uL[0]) * wsq;
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk) {
+        gq[0 * 2 + kk] = cs[0] * fp.JiL[kk * 2 + 0] + cs[1] * fp.JiL[kk * 2 + 1];
+        gq[1 * 2 + kk] = 0.0;
+      }
+    }
+  } else if (bct == ICX_BC_EXTRAPOLATION || bct == ICX_BC_SPACETIME_FUTURE) {
+    Phys<PDE>::conv_sel(pp, uL, uL, n, fadv);
+    if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
+  } else {
+    // Neumann faces have no convective part; boundary kinds the PDE does not
+    // implement contribute nothing
+#pragma unroll
+    for (int eq = 0; eq < NEQ; ++eq) fadv[eq] = 0.0;
+    if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
+  }
+}
+
+// viscous part (zero where the face has none)
+template <int PDE, bool DDG>
+__device__ inline void face_visc_part(const PhysParams& pp, const FacePt& fp, bool interior, int bct,
+                                      const double* bval, const double* uL, const double* gL, const double* hL,
+                                      const double* uR, const double* gR, const double* hR, double* fvis) {
+  constexpr int NEQ = Phys<PDE>::NEQ;
+  const double* n = fp.n;
+  const double h = fp.h;
+  double ud[NEQ];
+  if (interior) {
     double gddg[2 * NEQ], uavg[NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) {
@@ -160,35 +234,7 @@ __device__ inline void face_flux_states(const PhysParams& pp, const FacePt& fp, 
       uavg[eq] = 0.5 * (uL[eq] + uR[eq]);
     }
     Phys<PDE>::diff(pp, uavg, gddg, n, fvis);
-#pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq - fadv[eq] * wsq;
-    if (ic) {
-      // resL, resR -= sum_s (sigma mu n_s [u] w sqrt(g) / 2) dphi/dx_s   (conservation_law.hpp:580-610)
-      double cs[2];
-#pragma unroll
-      for (int s = 0; s < 2; ++s) cs[s] = 0.5 * pp.sigma_ic * pp.mu * n[s] * (uR[0] - uL[0]) * wsq;
-#pragma unroll
-      for (int kk = 0; kk < 2; ++kk) {
-        gq[0 * 2 + kk] = cs[0] * fp.JiL[kk * 2 + 0] + cs[1] * fp.JiL[kk * 2 + 1];
-        gq[1 * 2 + kk] = cs[0] * fp.JiR[kk * 2 + 0] + cs[1] * fp.JiR[kk * 2 + 1];
-      }
-    }
-  } else if (bct == ICX_BC_DIRICHLET || (bct == ICX_BC_SPACETIME_PAST && pp.st_connected) ||
-             (Phys<PDE>::has_pde_bcs && bct >= ICX_BC_RIEMANN && bct <= ICX_BC_WALL_GENERAL)) {
-    // a connected SPACETIME_PAST face takes the past slab's trace as exterior
-    // state; on a slab interface at constant t the diffusive normal flux
-    // vanishes (no diffusion along t), leaving the time-upwind flux. The
-    // PDE-level kinds (walls, characteristic) form the exterior state from
-    // the interior one and then take the same DDG boundary flux as a
-    // Dirichlet face with one-sided gradients (conservation_law.hpp:1043-1130)
-    double ud[NEQ];
-    if (bct == ICX_BC_DIRICHLET || bct == ICX_BC_SPACETIME_PAST) {
-#pragma unroll
-      for (int eq = 0; eq < NEQ; ++eq) ud[eq] = bval[eq];
-    } else {
-      Phys<PDE>::apply_bc(pp, uL, n, bct, bval, ud);
-    }
-    Phys<PDE>::conv_sel(pp, uL, ud, n, fadv);
+  } else if (face_exterior<PDE>(pp, fp, bct, bval, uL, ud)) {
     double gddg[2 * NEQ], uavg[NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) {
@@ -197,39 +243,35 @@ __device__ inline void face_flux_states(const PhysParams& pp, const FacePt& fp, 
       uavg[eq] = 0.5 * (uL[eq] + ud[eq]);
     }
     Phys<PDE>::diff(pp, uavg, gddg, n, fvis);
-#pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq - fadv[eq] * wsq;
-    if (ic) {
-      // resL -= sum_s sigma mu n_s [u] w sqrt(g) dphi/dx_s   (conservation_law.hpp:735-760)
-      double cs[2];
-#pragma unroll
-      for (int s = 0; s < 2; ++s) cs[s] = pp.sigma_ic * pp.mu * n[s] * (ud[0] - uL[0]) * wsq;
-#pragma unroll
-      for (int kk = 0; kk < 2; ++kk) {
-        gq[0 * 2 + kk] = cs[0] * fp.JiL[kk * 2 + 0] + cs[1] * fp.JiL[kk * 2 + 1];
-        gq[1 * 2 + kk] = 0.0;
-      }
-    }
   } else if (bct == ICX_BC_NEUMANN) {
     double gn[NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) gn[eq] = bval[eq];
     Phys<PDE>::neumann(pp, gn, fvis);
-#pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq;
-    if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
   } else if (bct == ICX_BC_EXTRAPOLATION || bct == ICX_BC_SPACETIME_FUTURE) {
-    Phys<PDE>::conv_sel(pp, uL, uL, n, fadv);
     Phys<PDE>::diff(pp, uL, gL, n, fvis);
-#pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) out[eq] = fvis[eq] * wsq - fadv[eq] * wsq;
-    if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
   } else {
-    // boundary kinds the PDE does not implement contribute nothing
 #pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) out[eq] = 0.0;
-    if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
+    for (int eq = 0; eq < NEQ; ++eq) fvis[eq] = 0.0;
   }
+}
+
+template <int PDE>
+__device__ inline void face_combine(const FacePt& fp, const double* fvis, const double* fadv, double* out) {
+#pragma unroll
+  for (int eq = 0; eq < Phys<PDE>::NEQ; ++eq) out[eq] = fvis[eq] * fp.wsq - fadv[eq] * fp.wsq;
+}
+
+template <int PDE, bool DDG>
+__device__ inline void face_flux_states(const PhysParams& pp, const FacePt& fp, bool interior, int bct,
+                                        const double* bval, const double* uL, const double* gL, const double* hL,
+                                        const double* uR, const double* gR, const double* hR, double* out,
+                                        double* gq) {
+  constexpr int NEQ = Phys<PDE>::NEQ;
+  double fadv[NEQ], fvis[NEQ];
+  face_conv_part<PDE, DDG>(pp, fp, interior, bct, bval, uL, uR, fadv, gq);
+  face_visc_part<PDE, DDG>(pp, fp, interior, bct, bval, uL, gL, hL, uR, gR, hR, fvis);
+  face_combine<PDE>(fp, fvis, fadv, out);
 }
 
 // numerical flux at face point (f, q) from the coefficient tiles of both sides

@@ -644,13 +644,16 @@ class LMSolver {
   ConvergenceCriteria& conv_criteria;
   corrigan_linesearch linesearch;
   const geo_dof_map& geo_map;
-  double lambda_u = 1e-7, lambda_b = 1e-2;
+  const bool explicitly_form_subproblem;
+  double lambda_u = 1e-7, lambda_lag = 1e-5, lambda_b = 1e-2;
   icx_lm_options options{};
   icx_lm_report report{};
   std::vector<double> x;  // the geometry parameters (extract_geospan)
 
-  LMSolver(FESpace& fs, Disc& d, ConvergenceCriteria& conv, corrigan_linesearch ls, const geo_dof_map& gm)
-      : fespace(fs), disc(d), conv_criteria(conv), linesearch(ls), geo_map(gm) {
+  LMSolver(FESpace& fs, Disc& d, ConvergenceCriteria& conv, corrigan_linesearch ls, const geo_dof_map& gm,
+           bool explicitly_form_subproblem_ = false)
+      : fespace(fs), disc(d), conv_criteria(conv), linesearch(ls), geo_map(gm),
+        explicitly_form_subproblem(explicitly_form_subproblem_) {
     check(icx_lm_default_options(&options), nullptr, "icx_lm_default_options");
   }
 
@@ -667,6 +670,8 @@ class LMSolver {
     options.kmax = conv_criteria.kmax;
     options.lambda_u = lambda_u;
     options.lambda_b = lambda_b;
+    options.lambda_lag = lambda_lag;
+    options.explicit_subproblem = explicitly_form_subproblem ? 1 : 0;
     options.linesearch = 2;
     options.ls_max_it = linesearch.max_it;
     options.ls_alpha_initial = linesearch.alpha_initial;
