@@ -391,7 +391,8 @@ def lm_bench(torch, dev, kmax=5):
 
 def newton_bench(torch, dev, tune=True):
     """Newton solve time to |r| <= 1e-10 (FP64 residual), all-FP64 vs mixed
-    precision (FP32 Jacobian and preconditioner copies): 32 x 32 viscous
+    precision (FP32 Jacobian and preconditioner copies) and FP32 flux
+    quadrature (the Jacobian itself formed in FP32): 32 x 32 viscous
     Burgers p=2 and the 128 x 128 Navier-Stokes manufactured solution p=3,
     both with GMRES(30) + block-ILU(0) and the Wolfe line search. Timed with
     CUDA events around the whole solve (it synchronises internally). With
@@ -412,7 +413,7 @@ def newton_bench(torch, dev, tune=True):
                                 "ilu_ms_default": t["ilu_ms_default"], "ilu_ms_tuned": t["ilu_ms_tuned"]}
         states = {}
         tile = 8 if name.startswith("burgers") else 32
-        for label, prec, t in (("fp64", 0, 0), ("mixed", 1, 0), ("mixed_tiled", 1, tile)):
+        for label, prec, t in (("fp64", 0, 0), ("mixed", 1, 0), ("mixed_tiled", 1, tile), ("quad32_tiled", 2, tile)):
             opt = ib.default_newton_options()
             opt.precision = prec
             opt.ilu_tile = t
@@ -430,7 +431,7 @@ def newton_bench(torch, dev, tune=True):
                            "gmres_its": rep.linear_iterations_total, "r_final": rep.r_final,
                            "converged": bool(rep.converged)}
         a = states["fp64"]
-        for label in ("mixed", "mixed_tiled"):
+        for label in ("mixed", "mixed_tiled", "quad32_tiled"):
             rows[f"{label}_vs_fp64_state_l2"] = float(np.linalg.norm(a - states[label]) /
                                                       max(np.linalg.norm(wl.u0), 1e-300))
             rows[f"speedup_{label}_vs_fp64"] = rows["fp64"]["s"] / rows[label]["s"]

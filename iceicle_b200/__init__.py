@@ -143,6 +143,7 @@ def lib():
             "icx_form_residual": (C.c_int, [vp, vp, vp, vp]),
             "icx_jacobian_pattern": (C.c_int, [vp, vp, vp]),
             "icx_form_jacobian_fd": (C.c_int, [vp, vp, vp, vp, C.c_double, vp]),
+            "icx_form_jacobian_fd_f32": (C.c_int, [vp, vp, vp, vp, vp]),
             "icx_bsr_spmv": (C.c_int, [vp, vp, vp, vp, vp]),
             "icx_newton_default_options": (C.c_int, [C.POINTER(NewtonOptions)]),
             "icx_explicit_default_options": (C.c_int, [C.POINTER(ExplicitOptions)]),
@@ -448,6 +449,12 @@ class Context:
     def form_jacobian_fd(self, u, res, vals, eps=0.0, stream=None):
         self._check(lib().icx_form_jacobian_fd(self._h, _ptr(u), _ptr(res), _ptr(vals), eps, _stream_ptr(stream)),
                     "form_jacobian_fd")
+
+    def form_jacobian_fd_f32(self, u, res, vals32, stream=None):
+        """the FD Jacobian with FP32 flux quadrature into FP32 BSR values
+        (res = R(u) in FP64)"""
+        self._check(lib().icx_form_jacobian_fd_f32(self._h, _ptr(u), _ptr(res), _ptr(vals32), _stream_ptr(stream)),
+                    "form_jacobian_fd_f32")
 
     def bsr_spmv(self, vals, x, y, stream=None):
         self._check(lib().icx_bsr_spmv(self._h, _ptr(vals), _ptr(x), _ptr(y), _stream_ptr(stream)), "bsr_spmv")

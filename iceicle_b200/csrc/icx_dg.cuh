@@ -41,20 +41,20 @@ __device__ inline PhysParams elem_params(const DeviceMesh& dm, const PhysParams&
 // physical gradient (and Hessian) of one basis function from its reference
 // derivatives t = [phi, d0, d1, h00, h01, h11]:
 //   dx = Ji^T dxi,  Hx = Ji^T (Hxi - sum_m Hm_m dx_m) Ji   (finite_element.hpp:220-398)
-template <bool WANT_H>
-__device__ inline void basis_phys(const double* t, const double* Ji, const double* Hm, double* gx, double* hx) {
+template <bool WANT_H, class T>
+__device__ inline void basis_phys(const T* t, const T* Ji, const T* Hm, T* gx, T* hx) {
 #pragma unroll
   for (int d = 0; d < 2; ++d) gx[d] = t[1] * Ji[0 * 2 + d] + t[2] * Ji[1 * 2 + d];
   if (WANT_H) {
-    double r00 = t[3] - Hm[0] * gx[0] - Hm[3] * gx[1];
-    double r01 = t[4] - Hm[1] * gx[0] - Hm[4] * gx[1];
-    double r11 = t[5] - Hm[2] * gx[0] - Hm[5] * gx[1];
-    double rhs[2][2] = {{r00, r01}, {r01, r11}};
+    T r00 = t[3] - Hm[0] * gx[0] - Hm[3] * gx[1];
+    T r01 = t[4] - Hm[1] * gx[0] - Hm[4] * gx[1];
+    T r11 = t[5] - Hm[2] * gx[0] - Hm[5] * gx[1];
+    T rhs[2][2] = {{r00, r01}, {r01, r11}};
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
-        double s = 0.0;
+        T s = T(0.0);
 #pragma unroll
         for (int l = 0; l < 2; ++l)
 #pragma unroll
@@ -66,63 +66,68 @@ __device__ inline void basis_phys(const double* t, const double* Ji, const doubl
 
 // value, physical gradient [NEQ][2] and (if WANT_H) physical Hessian
 // [NEQ][2][2] of the solution on one side of a face point.
-// tab: [NB][6] = phi, dphi/dxi0, dphi/dxi1, h00, h01, h11.
-template <int NB, int NEQ, bool WANT_H>
-__device__ inline void side_state(const double* __restrict__ ue, const double* __restrict__ tab, const double* Ji,
-                                  const double* Hm, double* u, double* gx, double* hx) {
-  double gxi[NEQ][2], hxi[NEQ][3];
+// tab: [NB][6] = phi, dphi/dxi0, dphi/dxi1, h00, h01, h11 (FP64 tables; an
+// FP32 evaluation rounds each entry once as it reads it).
+template <int NB, int NEQ, bool WANT_H, class T>
+__device__ inline void side_state(const T* __restrict__ ue, const double* __restrict__ tab, const T* Ji,
+                                  const T* Hm, T* u, T* gx, T* hx) {
+  T gxi[NEQ][2], hxi[NEQ][3];
 #pragma unroll
   for (int eq = 0; eq < NEQ; ++eq) {
-    u[eq] = 0.0;
-    gxi[eq][0] = gxi[eq][1] = 0.0;
-    hxi[eq][0] = hxi[eq][1] = hxi[eq][2] = 0.0;
+    u[eq] = T(0.0);
+    gxi[eq][0] = gxi[eq][1] = T(0.0);
+    hxi[eq][0] = hxi[eq][1] = hxi[eq][2] = T(0.0);
   }
 #pragma unroll 4
   for (int i = 0; i < NB; ++i) {
     const double* t = tab + i * 6;
-    double phi = t[0], d0 = t[1], d1 = t[2];
+    T phi = T(t[0]), d0 = T(t[1]), d1 = T(t[2]);
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) {
-      double c = ue[i * NEQ + eq];
+      T c = ue[i * NEQ + eq];
       u[eq] += c * phi;
       gxi[eq][0] += c * d0;
       gxi[eq][1] += c * d1;
       if (WANT_H) {
-        hxi[eq][0] += c * t[3];
-        hxi[eq][1] += c * t[4];
-        hxi[eq][2] += c * t[5];
+        hxi[eq][0] += c * T(t[3]);
+        hxi[eq][1] += c * T(t[4]);
+        hxi[eq][2] += c * T(t[5]);
       }
     }
   }
 #pragma unroll
   for (int eq = 0; eq < NEQ; ++eq) {
-    double tt[6] = {0.0, gxi[eq][0], gxi[eq][1], hxi[eq][0], hxi[eq][1], hxi[eq][2]};
+    T tt[6] = {T(0.0), gxi[eq][0], gxi[eq][1], hxi[eq][0], hxi[eq][1], hxi[eq][2]};
     basis_phys<WANT_H>(tt, Ji, Hm, gx + eq * 2, hx + eq * 4);
   }
 }
 
-// geometry of one face quadrature point (both sides)
-struct FacePt {
-  double n[2], wsq, h;
-  double JiL[4], HL[6], JiR[4], HR[6];
+// geometry of one face quadrature point (both sides); the FP32 form holds
+// the FP64 metrics rounded once
+template <class T>
+struct FacePtT {
+  T n[2], wsq, h;
+  T JiL[4], HL[6], JiR[4], HR[6];
 };
+using FacePt = FacePtT<double>;
 
-__device__ inline void load_face_pt(const DeviceMesh& dm, int nqf, int f, int q, bool interior, FacePt& p) {
+template <class T>
+__device__ inline void load_face_pt(const DeviceMesh& dm, int nqf, int f, int q, bool interior, FacePtT<T>& p) {
   int nfq = dm.F * nqf, k = f * nqf + q;
   const double* g = dm.fgeo;
-  p.n[0] = g[FG_N0 * nfq + k];
-  p.n[1] = g[FG_N1 * nfq + k];
-  p.wsq = g[FG_WSQ * nfq + k];
-  p.h = g[FG_H * nfq + k];
+  p.n[0] = T(g[FG_N0 * nfq + k]);
+  p.n[1] = T(g[FG_N1 * nfq + k]);
+  p.wsq = T(g[FG_WSQ * nfq + k]);
+  p.h = T(g[FG_H * nfq + k]);
 #pragma unroll
-  for (int a = 0; a < 4; ++a) p.JiL[a] = g[(FG_JIL + a) * nfq + k];
+  for (int a = 0; a < 4; ++a) p.JiL[a] = T(g[(FG_JIL + a) * nfq + k]);
 #pragma unroll
-  for (int a = 0; a < 6; ++a) p.HL[a] = g[(FG_HL + a) * nfq + k];
+  for (int a = 0; a < 6; ++a) p.HL[a] = T(g[(FG_HL + a) * nfq + k]);
   if (interior) {
 #pragma unroll
-    for (int a = 0; a < 4; ++a) p.JiR[a] = g[(FG_JIR + a) * nfq + k];
+    for (int a = 0; a < 4; ++a) p.JiR[a] = T(g[(FG_JIR + a) * nfq + k]);
 #pragma unroll
-    for (int a = 0; a < 6; ++a) p.HR[a] = g[(FG_HR + a) * nfq + k];
+    for (int a = 0; a < 6; ++a) p.HR[a] = T(g[(FG_HR + a) * nfq + k]);
   }
 }
 
@@ -137,13 +142,13 @@ __device__ inline void load_face_pt(const DeviceMesh& dm, int nqf, int f, int q,
 
 // the exterior state of a boundary point whose flux uses one: Dirichlet data,
 // a connected past slab, or a PDE-level boundary; false for the other kinds
-template <int PDE>
-__device__ inline bool face_exterior(const PhysParams& pp, const FacePt& fp, int bct, const double* bval,
-                                     const double* uL, double* ud) {
+template <int PDE, class T>
+__device__ inline bool face_exterior(const PhysParams& pp, const FacePtT<T>& fp, int bct, const double* bval,
+                                     const T* uL, T* ud) {
   constexpr int NEQ = Phys<PDE>::NEQ;
   if (bct == ICX_BC_DIRICHLET || (bct == ICX_BC_SPACETIME_PAST && pp.st_connected)) {
 #pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) ud[eq] = bval[eq];
+    for (int eq = 0; eq < NEQ; ++eq) ud[eq] = T(bval[eq]);
     return true;
   }
   if (Phys<PDE>::has_pde_bcs && bct >= ICX_BC_RIEMANN && bct <= ICX_BC_WALL_GENERAL) {
@@ -154,29 +159,28 @@ __device__ inline bool face_exterior(const PhysParams& pp, const FacePt& fp, int
 }
 
 // convective part (zero where the face has none) and the interface-correction coefficients
-template <int PDE, bool DDG>
-__device__ inline void face_conv_part(const PhysParams& pp, const FacePt& fp, bool interior, int bct,
-                                      const double* bval, const double* uL, const double* uR, double* fadv,
-                                      double* gq) {
+template <int PDE, bool DDG, class T>
+__device__ inline void face_conv_part(const PhysParams& pp, const FacePtT<T>& fp, bool interior, int bct,
+                                      const double* bval, const T* uL, const T* uR, T* fadv, T* gq) {
   constexpr int NEQ = Phys<PDE>::NEQ;
-  const double* n = fp.n;
-  const double wsq = fp.wsq;
+  const T* n = fp.n;
+  const T wsq = fp.wsq;
   const bool ic = Phys<PDE>::has_ic && pp.sigma_ic != 0.0;
-  double ud[NEQ];
+  T ud[NEQ];
   if (interior) {
     Phys<PDE>::conv_sel(pp, uL, uR, n, fadv);
     if (ic) {
       // resL, resR -= sum_s (sigma mu n_s [u] w sqrt(g) / 2) dphi/dx_s   (conservation_law.hpp:580-610)
-      double cs[2];
+      T cs[2];
 #pragma unroll
-      for (int s = 0; s < 2; ++s) cs[s] = 0.5 * pp.sigma_ic * pp.mu * n[s] * (uR[0] - uL[0]) * wsq;
+      for (int s = 0; s < 2; ++s) cs[s] = T(0.5) * T(pp.sigma_ic) * T(pp.mu) * n[s] * (uR[0] - uL[0]) * wsq;
 #pragma unroll
       for (int kk = 0; kk < 2; ++kk) {
         gq[0 * 2 + kk] = cs[0] * fp.JiL[kk * 2 + 0] + cs[1] * fp.JiL[kk * 2 + 1];
         gq[1 * 2 + kk] = cs[0] * fp.JiR[kk * 2 + 0] + cs[1] * fp.JiR[kk * 2 + 1];
       }
     }
-  } else if (face_exterior<PDE>(pp, fp, bct, bval, uL, ud)) {
+  } else if (face_exterior<PDE, T>(pp, fp, bct, bval, uL, ud)) {
     // a connected SPACETIME_PAST face takes the past slab's trace as exterior
     // state; on a slab interface at constant t the diffusive normal flux
     // vanishes (no diffusion along t), leaving the time-upwind flux. The
@@ -186,92 +190,91 @@ __device__ inline void face_conv_part(const PhysParams& pp, const FacePt& fp, bo
     Phys<PDE>::conv_sel(pp, uL, ud, n, fadv);
     if (ic) {
       // resL -= sum_s sigma mu n_s [u] w sqrt(g) dphi/dx_s   (conservation_law.hpp:735-760)
-      double cs[2];
+      T cs[2];
 #pragma unroll
-      for (int s = 0; s < 2; ++s) cs[s] = pp.sigma_ic * pp.mu * n[s] * (ud[0] - uL[0]) * wsq;
+      for (int s = 0; s < 2; ++s) cs[s] = T(pp.sigma_ic) * T(pp.mu) * n[s] * (ud[0] - uL[0]) * wsq;
 #pragma unroll
       for (int kk = 0; kk < 2; ++kk) {
         gq[0 * 2 + kk] = cs[0] * fp.JiL[kk * 2 + 0] + cs[1] * fp.JiL[kk * 2 + 1];
-        gq[1 * 2 + kk] = 0.0;
+        gq[1 * 2 + kk] = T(0.0);
       }
     }
   } else if (bct == ICX_BC_EXTRAPOLATION || bct == ICX_BC_SPACETIME_FUTURE) {
     Phys<PDE>::conv_sel(pp, uL, uL, n, fadv);
-    if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
+    if (ic) gq[0] = gq[1] = gq[2] = gq[3] = T(0.0);
   } else {
     // Neumann faces have no convective part; boundary kinds the PDE does not
     // implement contribute nothing
 #pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) fadv[eq] = 0.0;
-    if (ic) gq[0] = gq[1] = gq[2] = gq[3] = 0.0;
+    for (int eq = 0; eq < NEQ; ++eq) fadv[eq] = T(0.0);
+    if (ic) gq[0] = gq[1] = gq[2] = gq[3] = T(0.0);
   }
 }
 
 // viscous part (zero where the face has none)
-template <int PDE, bool DDG>
-__device__ inline void face_visc_part(const PhysParams& pp, const FacePt& fp, bool interior, int bct,
-                                      const double* bval, const double* uL, const double* gL, const double* hL,
-                                      const double* uR, const double* gR, const double* hR, double* fvis) {
+template <int PDE, bool DDG, class T>
+__device__ inline void face_visc_part(const PhysParams& pp, const FacePtT<T>& fp, bool interior, int bct,
+                                      const double* bval, const T* uL, const T* gL, const T* hL, const T* uR,
+                                      const T* gR, const T* hR, T* fvis) {
   constexpr int NEQ = Phys<PDE>::NEQ;
-  const double* n = fp.n;
-  const double h = fp.h;
-  double ud[NEQ];
+  const T* n = fp.n;
+  const T h = fp.h;
+  T ud[NEQ];
   if (interior) {
-    double gddg[2 * NEQ], uavg[NEQ];
+    T gddg[2 * NEQ], uavg[NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) {
-      double jump = uR[eq] - uL[eq];
+      T jump = uR[eq] - uL[eq];
 #pragma unroll
       for (int d = 0; d < 2; ++d) {
-        double v = pp.beta0 * jump / h * n[d] + 0.5 * (gL[eq * 2 + d] + gR[eq * 2 + d]);
+        T v = T(pp.beta0) * jump / h * n[d] + T(0.5) * (gL[eq * 2 + d] + gR[eq * 2 + d]);
         if (DDG) {
-          double ht = (hR[eq * 4 + 0 * 2 + d] - hL[eq * 4 + 0 * 2 + d]) * n[0] +
-                      (hR[eq * 4 + 1 * 2 + d] - hL[eq * 4 + 1 * 2 + d]) * n[1];
-          v += pp.beta1 * h * ht;
+          T ht = (hR[eq * 4 + 0 * 2 + d] - hL[eq * 4 + 0 * 2 + d]) * n[0] +
+                 (hR[eq * 4 + 1 * 2 + d] - hL[eq * 4 + 1 * 2 + d]) * n[1];
+          v += T(pp.beta1) * h * ht;
         }
         gddg[eq * 2 + d] = v;
       }
-      uavg[eq] = 0.5 * (uL[eq] + uR[eq]);
+      uavg[eq] = T(0.5) * (uL[eq] + uR[eq]);
     }
     Phys<PDE>::diff(pp, uavg, gddg, n, fvis);
-  } else if (face_exterior<PDE>(pp, fp, bct, bval, uL, ud)) {
-    double gddg[2 * NEQ], uavg[NEQ];
+  } else if (face_exterior<PDE, T>(pp, fp, bct, bval, uL, ud)) {
+    T gddg[2 * NEQ], uavg[NEQ];
 #pragma unroll
     for (int eq = 0; eq < NEQ; ++eq) {
 #pragma unroll
-      for (int d = 0; d < 2; ++d) gddg[eq * 2 + d] = pp.beta0 * (ud[eq] - uL[eq]) / h * n[d] + gL[eq * 2 + d];
-      uavg[eq] = 0.5 * (uL[eq] + ud[eq]);
+      for (int d = 0; d < 2; ++d) gddg[eq * 2 + d] = T(pp.beta0) * (ud[eq] - uL[eq]) / h * n[d] + gL[eq * 2 + d];
+      uavg[eq] = T(0.5) * (uL[eq] + ud[eq]);
     }
     Phys<PDE>::diff(pp, uavg, gddg, n, fvis);
   } else if (bct == ICX_BC_NEUMANN) {
-    double gn[NEQ];
+    T gn[NEQ];
 #pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) gn[eq] = bval[eq];
+    for (int eq = 0; eq < NEQ; ++eq) gn[eq] = T(bval[eq]);
     Phys<PDE>::neumann(pp, gn, fvis);
   } else if (bct == ICX_BC_EXTRAPOLATION || bct == ICX_BC_SPACETIME_FUTURE) {
     Phys<PDE>::diff(pp, uL, gL, n, fvis);
   } else {
 #pragma unroll
-    for (int eq = 0; eq < NEQ; ++eq) fvis[eq] = 0.0;
+    for (int eq = 0; eq < NEQ; ++eq) fvis[eq] = T(0.0);
   }
 }
 
-template <int PDE>
-__device__ inline void face_combine(const FacePt& fp, const double* fvis, const double* fadv, double* out) {
+template <int PDE, class T>
+__device__ inline void face_combine(const FacePtT<T>& fp, const T* fvis, const T* fadv, T* out) {
 #pragma unroll
   for (int eq = 0; eq < Phys<PDE>::NEQ; ++eq) out[eq] = fvis[eq] * fp.wsq - fadv[eq] * fp.wsq;
 }
 
-template <int PDE, bool DDG>
-__device__ inline void face_flux_states(const PhysParams& pp, const FacePt& fp, bool interior, int bct,
-                                        const double* bval, const double* uL, const double* gL, const double* hL,
-                                        const double* uR, const double* gR, const double* hR, double* out,
-                                        double* gq) {
+template <int PDE, bool DDG, class T>
+__device__ inline void face_flux_states(const PhysParams& pp, const FacePtT<T>& fp, bool interior, int bct,
+                                        const double* bval, const T* uL, const T* gL, const T* hL, const T* uR,
+                                        const T* gR, const T* hR, T* out, T* gq) {
   constexpr int NEQ = Phys<PDE>::NEQ;
-  double fadv[NEQ], fvis[NEQ];
-  face_conv_part<PDE, DDG>(pp, fp, interior, bct, bval, uL, uR, fadv, gq);
-  face_visc_part<PDE, DDG>(pp, fp, interior, bct, bval, uL, gL, hL, uR, gR, hR, fvis);
-  face_combine<PDE>(fp, fvis, fadv, out);
+  T fadv[NEQ], fvis[NEQ];
+  face_conv_part<PDE, DDG, T>(pp, fp, interior, bct, bval, uL, uR, fadv, gq);
+  face_visc_part<PDE, DDG, T>(pp, fp, interior, bct, bval, uL, gL, hL, uR, gR, hR, fvis);
+  face_combine<PDE, T>(fp, fvis, fadv, out);
 }
 
 // numerical flux at face point (f, q) from the coefficient tiles of both sides

@@ -180,6 +180,9 @@ cudaError_t launch_residual_domain(const DeviceMesh& dm, const PhysParams& pp, c
 // Jacobian (icx_jacobian.cu)
 cudaError_t launch_jacobian_fd(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
                                double* vals, double eps, cudaStream_t s);
+// FP64 residual, FP32-quadrature FD Jacobian (FP32 values, eps = sqrt(FLT_EPSILON))
+cudaError_t launch_jacobian_fd_f32(const DeviceMesh& dm, const PhysParams& pp, const double* u, double* res,
+                                   float* vals, cudaStream_t s);
 cudaError_t launch_bsr_spmv(const DeviceMesh& dm, const double* vals, const double* x, double* y,
                             cudaStream_t s);
 // the same with FP32 values and FP32 accumulation (x, y FP64)

@@ -593,6 +593,16 @@ cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+__global__ void f2d_kernel(long long n, const float* __restrict__ x, double* __restrict__ y) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = (double)x[i];
+}
+
+cudaError_t la_f2d(long long n, const float* x, double* y, cudaStream_t s) {
+  f2d_kernel<<<grid_for(n), 256, 0, s>>>(n, x, y);
+  return cudaGetLastError();
+}
+
 // dst block b = src block map[b]; each CTA copies whole blocks with 16-byte
 // vector loads (a block of bs x bs doubles starts on a 16-byte boundary when
 // bs * bs is even; odd sizes fall back to 8-byte copies)

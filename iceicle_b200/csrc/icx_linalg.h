@@ -64,6 +64,7 @@ cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, const int* order, const 
                                   unsigned epoch, int* err, cudaStream_t s);
 cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s);
 cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s);
+cudaError_t la_f2d(long long n, const float* x, double* y, cudaStream_t s);
 // dst block b = src block map[b] for b < nblk (bs x bs FP64 blocks)
 cudaError_t la_gather_blocks(int nblk, int bs, const double* src, const int* map, double* dst, cudaStream_t s);
 }  // namespace icx

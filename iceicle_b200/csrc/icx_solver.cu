@@ -594,6 +594,14 @@ icx_status icx_form_jacobian_fd(icx_ctx* c, const double* d_u, double* d_res, do
   return ICX_OK;
 }
 
+icx_status icx_form_jacobian_fd_f32(icx_ctx* c, const double* d_u, double* d_res, float* d_vals32, void* stream) {
+  if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
+  if (!d_u || !d_res || !d_vals32) return set_err(c, ICX_ERR_INVALID, "null device pointer");
+  cudaError_t e = icx::launch_jacobian_fd_f32(c->dm, c->phys, d_u, d_res, d_vals32, (cudaStream_t)stream);
+  if (e != cudaSuccess) return set_err(c, ICX_ERR_CUDA, std::string("jacobian kernels: ") + cudaGetErrorString(e));
+  return ICX_OK;
+}
+
 icx_status icx_bsr_spmv(icx_ctx* c, const double* d_vals, const double* d_x, double* d_y, void* stream) {
   if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
   if (!d_vals || !d_x || !d_y) return set_err(c, ICX_ERR_INVALID, "null device pointer");
@@ -776,7 +784,7 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   if (!d_u || !opt) return set_err(c, ICX_ERR_INVALID, "null argument");
   if (opt->gmres_restart < 1 || opt->gmres_restart > 60) return set_err(c, ICX_ERR_INVALID, "restart in 1..60");
   cudaStream_t s = 0;
-  if (opt->precision < 0 || opt->precision > 1) return set_err(c, ICX_ERR_INVALID, "precision must be 0 or 1");
+  if (opt->precision < 0 || opt->precision > 2) return set_err(c, ICX_ERR_INVALID, "precision must be 0, 1 or 2");
   if (opt->preconditioner < 0 || opt->preconditioner > 5) return set_err(c, ICX_ERR_INVALID, "preconditioner in 0..5");
   if (opt->preconditioner >= 4 && (opt->pc_sweeps < 0 || opt->pc_sweeps > 16))
     return set_err(c, ICX_ERR_INVALID, "pc_sweeps in 0..16");
@@ -789,7 +797,8 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   c->sw->sweeps = opt->pc_sweeps;
   c->sw->graphs_on = opt->cuda_graphs != 0;
   const long long graph_steps0 = c->sw->graph_steps;
-  const bool mixed = opt->precision == 1;
+  const bool mixed = opt->precision >= 1;
+  const bool quad32 = opt->precision == 2;
   if (mixed && (st = ensure_mixed(c)) != ICX_OK) return st;
   icx_solver_work* w = c->sw;
   long long n = w->n;
@@ -797,8 +806,16 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   icx_newton_report* R = rep ? rep : &local;
   std::memset(R, 0, sizeof(*R));
   const double eps = std::sqrt(DBL_EPSILON);
+  const size_t nvals = (size_t)w->nnzb * w->bs * w->bs;
+  // FP64 residual and the Jacobian (FP32 quadrature: formed in FP32, widened
+  // for the FP64 factorisation)
+  auto linearise = [&]() -> cudaError_t {
+    if (!quad32) return icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->res, w->vals, eps, s);
+    cudaError_t e = icx::launch_jacobian_fd_f32(c->dm, c->phys, d_u, w->res, w->vals32, s);
+    return e == cudaSuccess ? icx::la_f2d((long long)nvals, w->vals32, w->vals, s) : e;
+  };
   // residual and Jacobian at the initial state (petsc_newton.hpp:211-221)
-  CK(icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->res, w->vals, eps, s));
+  CK(linearise());
   double r0 = dev_norm(c, w->res, s);
   R->r0 = r0;
   R->residual_history[0] = r0;
@@ -851,7 +868,7 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
     }
     SYNC_AT("line search");
     CK(icx::la_axpby(n, -alpha, w->du, 1.0, d_u, s));
-    CK(icx::launch_jacobian_fd(c->dm, c->phys, d_u, w->res, w->vals, eps, s));
+    CK(linearise());
     rk = dev_norm(c, w->res, s);
     if (k + 1 < 64) {
       R->residual_history[k + 1] = rk;

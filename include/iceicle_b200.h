@@ -192,6 +192,13 @@ icx_status icx_jacobian_pattern(const icx_ctx* ctx, int* rowptr, int* colidx);
 icx_status icx_form_jacobian_fd(icx_ctx* ctx, const double* d_u, double* d_res, double* d_vals, double eps,
                                 void* stream);
 
+/* The same Jacobian with the flux quadrature in FP32 (the FP32 build of
+ * form_petsc_jacobian_fd, CMakeLists.txt:19-22 USE_SINGLE_PRECISION): states,
+ * metrics, tabulations, fluxes and sums rounded to FP32, perturbations scaled
+ * by sqrt(FLT_EPSILON), blocks written as FP32 into d_vals32; d_res = R(d_u)
+ * in FP64. */
+icx_status icx_form_jacobian_fd_f32(icx_ctx* ctx, const double* d_u, double* d_res, float* d_vals32, void* stream);
+
 /* y = J x for the BSR Jacobian (PETSc MatMult on the AIJ matrix, PN:243) */
 icx_status icx_bsr_spmv(icx_ctx* ctx, const double* d_vals, const double* d_x, double* d_y, void* stream);
 
@@ -281,7 +288,11 @@ typedef struct icx_newton_options {
    * Jacobian (SpMV) and of the preconditioner (block inverses / ILU factors,
    * formed in FP64 then rounded) with FP32 accumulation; the Krylov vectors,
    * Hessenberg and Givens rotations, the Newton residual, its norm and the
-   * line search stay FP64, so the converged state is judged in FP64. */
+   * line search stay FP64, so the converged state is judged in FP64.
+   * 2: as 1, with the Jacobian's flux quadrature itself in FP32
+   * (icx_form_jacobian_fd_f32); the preconditioner is factored in FP64 from
+   * those FP32 values. Newton is then FP64 iterative refinement around FP32
+   * linearisations: its residual, norm, line search and update stay FP64. */
   int precision;
   /* preconditioner 4 (block-ILU(0) factors applied by Jacobi sweeps): the
    * sweeps per triangular solve */

@@ -556,6 +556,16 @@ void form_jacobian_fd(FESpace& fespace, Disc& disc, const double* d_u, double* d
   check(icx_form_jacobian_fd(c, d_u, d_res, J.d_vals, eps, stream), c, "icx_form_jacobian_fd");
 }
 
+// the same Jacobian with the flux quadrature in FP32 (the reference's
+// USE_SINGLE_PRECISION build of this call): FP32 values into d_vals32
+// (nnz_blocks * bs * bs device floats), d_res = R(u) in FP64
+template <class Disc>
+void form_jacobian_fd_f32(FESpace& fespace, Disc& disc, const double* d_u, double* d_res, float* d_vals32,
+                          void* stream = nullptr) {
+  icx_ctx* c = detail::ready(fespace, disc);
+  check(icx_form_jacobian_fd_f32(c, d_u, d_res, d_vals32, stream), c, "icx_form_jacobian_fd_f32");
+}
+
 // ------------------------------------------------------------------ solvers
 // ConvergenceCriteria and the line searches (nonlinear_solver_utils.hpp:24-268)
 struct ConvergenceCriteria {

@@ -6,6 +6,7 @@
 //   residual <n> <v_0> ... <v_{n-1}>       Burgers 4 x 3 p = 2 residual at a given state
 //   ns_residual <n> <v...>                 Navier-Stokes 3 x 3 p = 2, Roe flux, walls + far field
 //   jacobian_blocks <nnzb> <bs>            BSR sizes of the Burgers Jacobian
+//   jacobian_f32_rel <d>                   max |J_fp32 - J_fp64| / max |J_fp64| (FP32 flux quadrature)
 //   newton <iterations> <|r_final|>        Burgers 8 x 8 Newton solve to 1e-10
 // Usage: facade_check <state file: Burgers 4x3 p2 state (108 doubles)> <NS state file (144 doubles)>
 #include <cuda_runtime.h>
@@ -77,6 +78,21 @@ int main(int argc, char** argv) {
     J.d_vals = vals.p;
     ib::form_jacobian_fd(fespace, disc, u.p, r.p, J);
     std::printf("jacobian_blocks %d %d\n", J.rowptr.back(), J.block_size);
+    // FP32 flux quadrature: largest block-entry difference to the FP64
+    // Jacobian, relative to the largest entry
+    float* v32 = nullptr;
+    cudaMalloc((void**)&v32, vals.n * sizeof(float));
+    ib::form_jacobian_fd_f32(fespace, disc, u.p, r.p, v32);
+    std::vector<float> h32(vals.n);
+    cudaMemcpy(h32.data(), v32, vals.n * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(v32);
+    const std::vector<double> h64 = vals.get();
+    double dmax = 0.0, vmax = 0.0;
+    for (size_t k = 0; k < h64.size(); ++k) {
+      dmax = std::fmax(dmax, std::fabs((double)h32[k] - h64[k]));
+      vmax = std::fmax(vmax, std::fabs(h64[k]));
+    }
+    std::printf("jacobian_f32_rel %.6e\n", dmax / vmax);
   }
   // Navier-Stokes 3 x 3, p = 2, Roe flux, Riemann far field left / right,
   // slip wall below, isothermal wall above (bcflag 1)

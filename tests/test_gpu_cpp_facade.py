@@ -52,6 +52,7 @@ def test_facade_burgers_residual(facade_run):
     assert np.abs(r - ref).max() <= 1e-12 * np.abs(ref).max()
     nnzb, bs = (int(x) for x in lines["jacobian_blocks"])
     assert bs == 9 and nnzb == 4 * 3 + 2 * ((4 - 1) * 3 + 4 * (3 - 1))
+    assert float(lines["jacobian_f32_rel"][0]) <= 2e-3  # FP32 flux quadrature against the FP64 blocks
 
 
 def test_facade_ns_roe_wall_residual(facade_run):
