@@ -465,8 +465,6 @@ icx_status icx_mesh_uniform(icx_ctx* c, int ndim, const int* nelem, const double
   if (ndim != 2) return fail(c, ICX_ERR_UNSUPPORTED, "only 2D meshes are implemented");
   if (geo_order < 1 || geo_order > icx::MAX_G) return fail(c, ICX_ERR_UNSUPPORTED, "geometry order must be 1 or 2");
   if (nelem[0] < 1 || nelem[1] < 1) return fail(c, ICX_ERR_INVALID, "nelem must be positive");
-  for (int i = 0; i < 4; ++i)
-    if (bctypes[i] == ICX_BC_PERIODIC) return fail(c, ICX_ERR_UNSUPPORTED, "periodic boundaries are not implemented");
   c->nx = nelem[0];
   c->ny = nelem[1];
   c->geo_order = geo_order;
@@ -521,6 +519,13 @@ icx_status icx_mesh_uniform(icx_ctx* c, int ndim, const int* nelem, const double
       int LB = idim == 0 ? c->nx * t + c->nx - 1 : t + c->nx * (c->ny - 1);
       int ra[7] = {LA, -1, idim, 0, 0, bctypes[idim], bcflags[idim]};
       int rb[7] = {LB, -1, idim + 2, 0, 0, bctypes[idim + 2], bcflags[idim + 2]};
+      if (bctypes[idim] == ICX_BC_PERIODIC) {
+        // a periodic pair's flags name each other's face index (mesh.hpp:857-866);
+        // the faces stay boundary faces of their elements
+        int fa = (int)c->faces.size() / 7;
+        ra[6] = fa + 1;
+        rb[6] = fa;
+      }
       c->faces.insert(c->faces.end(), ra, ra + 7);
       c->faces.insert(c->faces.end(), rb, rb + 7);
     }
@@ -703,14 +708,15 @@ icx_status icx_setup(icx_ctx* c) {
   dm.nq1 = g + P;  // geometry order + basis order points per direction (reference_element.hpp:80, 240-245)
   dm.nqv = dm.nq1 * dm.nq1;
   dm.nqf = dm.nq1;
-  // boundary kinds: INLET and OUTLET have no implementation in the
-  // reference's Navier-Stokes apply_bc (it logs "Unsupported BC" and leaves
-  // the exterior state unset), so they are refused here
+  // boundary kinds: PERIODIC, INLET and OUTLET have no implementation in
+  // the reference's Navier-Stokes apply_bc (it logs "Unsupported BC" and
+  // leaves the exterior state unset), so they are refused here
   if (c->phys.pde == ICX_PDE_NAVIER_STOKES)
     for (int i = 0; i < 4; ++i) {
       int b = c->bctype[i];
-      if (b == 9 || b == 10 || b == ICX_BC_SPACETIME_PAST)
-        return fail(c, ICX_ERR_UNSUPPORTED, "Navier-Stokes inlet/outlet/spacetime boundaries are not implemented");
+      if (b == ICX_BC_PERIODIC || b == 9 || b == 10 || b == ICX_BC_SPACETIME_PAST)
+        return fail(c, ICX_ERR_UNSUPPORTED,
+                    "Navier-Stokes periodic/inlet/outlet/spacetime boundaries are not implemented");
     }
   if (c->phys.pde == ICX_PDE_NAVIER_STOKES && c->phys.sigma_ic != 0.0) {
     // the Navier-Stokes diffusive flux defines no homogeneity tensor: the

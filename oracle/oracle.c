@@ -274,6 +274,11 @@ int orc_mesh_topology(const orc_problem* pb, int* conn, int* faces, int* n_inter
       F = faces + 7 * f++;
       F[0] = LB; F[1] = -1; F[2] = idim + 2; F[3] = 0; F[4] = 0; F[5] = pb->bctype[idim + 2];
       F[6] = pb->bcflag[idim + 2];
+      if (pb->bctype[idim] == ORC_BC_PERIODIC) {
+        /* the pair's flags are each other's face index (ME:857-866) */
+        F[-7 + 6] = f - 1;
+        F[6] = f - 2;
+      }
     }
   }
   return f;

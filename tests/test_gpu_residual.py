@@ -33,6 +33,8 @@ CASES = [
     dict(basis=1, p=4, nx=3, ny=2, sigma_ic=0.7),
     dict(basis=1, pde=NS, p=3, ip=True, source=True),
     dict(basis=1, g=1, p=1, bct=(3, 2, 4, 3)),
+    dict(bct=(0, 3, 0, 3)),                       # periodic pairs: no flux across them
+    dict(bct=(0, 0, 0, 0), p=3, sigma_ic=0.4),
 ]
 
 
@@ -56,8 +58,9 @@ def test_residual_parity(kw):
     assert np.abs(r - r_or).max() <= 1e-12 * np.abs(r_or).max()
 
 
-def test_topology_and_pattern_bit_exact():
-    spec = Spec(nx=5, ny=4)
+@pytest.mark.parametrize("bct", [(3, 3, 3, 3), (0, 3, 0, 3), (0, 0, 0, 0)])
+def test_topology_and_pattern_bit_exact(bct):
+    spec = Spec(nx=5, ny=4, bct=bct)
     ctx = spec.context()
     pb = spec.oracle_problem()
     c1, f1, n1 = ob.topology(ob.oracle(), pb)

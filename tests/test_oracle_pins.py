@@ -18,6 +18,8 @@ CASES = [
     dict(bct=(3, 2, 4, 3)),                   # Dirichlet / Neumann / extrapolation
     dict(nx=1, ny=1),                         # single element: boundary faces only
     dict(nx=5, ny=1),                         # one row: no y-direction interior faces
+    dict(bct=(0, 3, 0, 3)),                   # periodic in x: faces paired by flag, no flux across them
+    dict(bct=(0, 0, 0, 0), p=3, sigma_ic=0.4),
     dict(pde=NS, p=2, ip=True),
     dict(pde=NS, p=3),
     dict(pde=NS, p=1, g=1, bct=(3, 4, 3, 4)),
@@ -52,7 +54,8 @@ def test_residual_matches_reference(kw):
 
 
 @needs_ref
-@pytest.mark.parametrize("kw", [dict(), dict(g=1, p=1, nx=3, ny=5), dict(nx=1, ny=4)])
+@pytest.mark.parametrize("kw", [dict(), dict(g=1, p=1, nx=3, ny=5), dict(nx=1, ny=4), dict(bct=(0, 3, 0, 3)),
+                                dict(nx=3, ny=4, bct=(0, 0, 0, 0))])
 def test_topology_bit_exact(kw):
     spec = Spec(**kw)
     pb = spec.oracle_problem()
