@@ -132,6 +132,7 @@ def lib():
             "icx_form_residuals_host": (C.c_int, [vp, C.c_int, vp, vp, dp]),
             "icx_ilu_apply": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, dp]),
             "icx_disc_navier_stokes": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
+            "icx_disc_ns_viscosity": (C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_double]),
             "icx_disc_ns_boundary": (C.c_int, [vp, dp, C.c_int, C.c_double, C.c_double, dp, C.c_double,
                                                C.c_double]),
             "icx_disc_options": (C.c_int, [vp, C.c_int, C.c_double]),
@@ -309,6 +310,11 @@ class Context:
         ud = (C.c_double * 2)(*u_direction)
         self._check(lib().icx_disc_ns_boundary(self._h, tw, len(wall_temperatures), rho_inf, u_inf, ud, T_inf, Rgas),
                     "disc_ns_boundary")
+
+    def disc_ns_viscosity(self, kind=0, mu_ratio=0.0, T0_ratio=1.0, Ts_ratio=0.0):
+        """Navier-Stokes viscosity law: 0 constant, 1 DimensionlessSutherlands
+        with the ratios mu_0/ref.mu, T_0/ref.T, T_s/ref.T"""
+        self._check(lib().icx_disc_ns_viscosity(self._h, int(kind), mu_ratio, T0_ratio, Ts_ratio), "disc_ns_viscosity")
 
     def disc_options(self, interior_penalty=False, sigma_ic=0.0):
         self._check(lib().icx_disc_options(self._h, int(interior_penalty), float(sigma_ic)), "disc_options")

@@ -29,7 +29,9 @@ icx_status icx_batch_create(icx_ctx** out, int device, int n_parts, icx_ctx* con
       return ICX_ERR_INVALID;
     if (q->phys.pde == ICX_PDE_NAVIER_STOKES &&
         (q->phys.gamma != p0->phys.gamma || q->phys.Pr != p0->phys.Pr || q->phys.ns_mu != p0->phys.ns_mu ||
-         q->conv_flux != p0->conv_flux))
+         q->conv_flux != p0->conv_flux || q->phys.ns_visc != p0->phys.ns_visc ||
+         q->phys.suth[0] != p0->phys.suth[0] || q->phys.suth[1] != p0->phys.suth[1] ||
+         q->phys.suth[2] != p0->phys.suth[2]))
       return ICX_ERR_INVALID;
   }
   icx_ctx* c = nullptr;

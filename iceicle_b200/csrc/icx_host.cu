@@ -622,6 +622,7 @@ icx_status icx_disc_navier_stokes(icx_ctx* c, double gamma, double Pr, double mu
     return fail(c, ICX_ERR_UNSUPPORTED, "Navier-Stokes convective flux: Van Leer or Roe");
   c->phys.ns_flux = conv_flux;
   c->phys.ns_viscous_wall = mu != 0.0;
+  c->phys.ns_visc = 0;
   if (!(c->phys.Rgas > 0.0)) c->phys.Rgas = 287.052874;  // EoS::Rgas default (navier_stokes.hpp:338)
   c->phys.pde = ICX_PDE_NAVIER_STOKES;
   c->phys.gamma = gamma;
@@ -648,6 +649,28 @@ icx_status icx_disc_ns_boundary(icx_ctx* c, const double* wall_temperatures, int
   c->phys.fs_u[1] = u_direction ? u_direction[1] * u_inf : 0.0;
   c->phys.fs_T = T_inf;
   c->phys.Rgas = Rgas;
+  c->ready = false;
+  return ICX_OK;
+}
+
+icx_status icx_disc_ns_viscosity(icx_ctx* c, int kind, double mu_ratio, double T0_ratio, double Ts_ratio) {
+  if (!c) return ICX_ERR_INVALID;
+  if (!c->has_disc || c->phys.pde != ICX_PDE_NAVIER_STOKES)
+    return fail(c, ICX_ERR_INVALID, "the viscosity law follows icx_disc_navier_stokes");
+  if (kind == 0) {
+    c->phys.ns_visc = 0;
+    c->phys.ns_viscous_wall = c->phys.ns_mu != 0.0;
+  } else if (kind == 1) {
+    if (!(T0_ratio > 0.0) || !(Ts_ratio >= 0.0))
+      return fail(c, ICX_ERR_INVALID, "Sutherland temperatures: T0_ratio > 0, Ts_ratio >= 0");
+    c->phys.ns_visc = 1;
+    c->phys.suth[0] = mu_ratio;
+    c->phys.suth[1] = T0_ratio;
+    c->phys.suth[2] = Ts_ratio;
+    c->phys.ns_viscous_wall = 1;
+  } else {
+    return fail(c, ICX_ERR_INVALID, "viscosity law: 0 constant, 1 dimensionless Sutherland");
+  }
   c->ready = false;
   return ICX_OK;
 }

@@ -45,6 +45,10 @@ struct PhysParams {
   double fs_rho, fs_u[2], fs_T;
   double Rgas;
   int ns_viscous_wall;
+  // Navier-Stokes viscosity law: 0 constant (ns_mu); 1 dimensionless
+  // Sutherland mu(T) = suth[0] (T / suth[1])^1.5 (suth[1] + suth[2]) / (T + suth[2])
+  int ns_visc;
+  double suth[3];
 };
 
 // launch shapes of the tunable kernels (0: the compiled default). Every

@@ -96,17 +96,31 @@ __device__ static inline NSState<T> ns_state(const PhysParams& pp, const T* u) {
 template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
   static constexpr int NEQ = 4;
 
-  // velocity gradients gv[i][j] and total energy gradient gE[j]; shear stress
+  // the viscosity at the state's temperature T = p / rho * gamma / (gamma - 1) / cp
+  // (constant_viscosity, or DimensionlessSutherlands, navier_stokes.hpp:226-287)
+  template <class T>
+  __device__ static inline T viscosity(const PhysParams& pp, const NSState<T>& s) {
+    if (pp.ns_visc != 1) return T(pp.ns_mu);
+    const T gam = T(pp.gamma);
+    const T cp = gam / (gam - T(1)) * T(pp.Rgas);
+    const T temp = s.p * s.inv_rho * gam / (gam - T(1)) / cp;
+    const T t0 = T(pp.suth[1]), ts = T(pp.suth[2]);
+    return T(pp.suth[0]) * pow(temp / t0, T(1.5)) * (t0 + ts) / (temp + ts);
+  }
+
+  // velocity gradients gv[i][j] and total energy gradient gE[j]; shear
+  // stress; mgp = mu gamma / Pr of the heat flux
   template <class T>
   __device__ static inline void viscous(const PhysParams& pp, const NSState<T>& s, const T* g, T tau[2][2],
-                                        T gv[2][2], T gE[2]) {
+                                        T gv[2][2], T gE[2], T& mgp) {
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
       for (int j = 0; j < 2; ++j) gv[i][j] = (g[2 * (1 + i) + j] - (i == 0 ? s.v0 : s.v1) * g[j]) * s.inv_rho;
 #pragma unroll
     for (int j = 0; j < 2; ++j) gE[j] = (g[6 + j] - s.E * g[j]) * s.inv_rho;
-    T mu = T(pp.ns_mu);
+    T mu = viscosity(pp, s);
+    mgp = pp.ns_visc == 1 ? mu * T(pp.gamma) / T(pp.Pr) : T(pp.mu_gamma_pr);
     T div = gv[0][0] + gv[1][1];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -129,14 +143,14 @@ template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
       F[(1 + j) * 2 + j] += s.p;
       F[3 * 2 + j] = vel[j] * (s.rhoE + s.p);
     }
-    T tau[2][2], gv[2][2], gE[2];
-    viscous(pp, s, g, tau, gv, gE);
+    T tau[2][2], gv[2][2], gE[2], mgp;
+    viscous(pp, s, g, tau, gv, gE, mgp);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       T q = gE[j];
       q -= vel[0] * gv[0][j];
       q -= vel[1] * gv[1][j];
-      q *= T(pp.mu_gamma_pr);
+      q *= mgp;
       T ef = q;
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
@@ -294,13 +308,13 @@ template <> struct Phys<ICX_PDE_NAVIER_STOKES> {
   template <class T>
   __device__ static inline void diff(const PhysParams& pp, const T* u, const T* g, const T* n, T* f) {
     NSState<T> s = ns_state(pp, u);
-    T tau[2][2], gv[2][2], gE[2];
-    viscous(pp, s, g, tau, gv, gE);
+    T tau[2][2], gv[2][2], gE[2], mgp;
+    viscous(pp, s, g, tau, gv, gE, mgp);
     T vel[2] = {s.v0, s.v1};
     f[0] = f[1] = f[2] = f[3] = T(0.0);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      T ef = T(pp.mu_gamma_pr) * gE[j] * n[j];
+      T ef = mgp * gE[j] * n[j];
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         f[1 + i] += tau[i][j] * n[j];

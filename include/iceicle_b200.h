@@ -135,6 +135,14 @@ icx_status icx_disc_navier_stokes(icx_ctx* ctx, double gamma, double Pr, double 
  * reference parameters. */
 icx_status icx_disc_ns_boundary(icx_ctx* ctx, const double* wall_temperatures, int n_walls, double rho_inf,
                                 double u_inf, const double u_direction[2], double T_inf, double Rgas);
+/* the Navier-Stokes viscosity law (Physics' viscosity function,
+ * navier_stokes.hpp:218-287): kind 0 constant_viscosity (the mu given to
+ * icx_disc_navier_stokes, which also resets to it); kind 1
+ * DimensionlessSutherlands, mu(T) = mu_ratio (T / T0_ratio)^1.5
+ * (T0_ratio + Ts_ratio) / (T + Ts_ratio) at the state's temperature, with the
+ * ratios of its members (mu_0 / ref.mu, T_0 / ref.T, T_s / ref.T); the flux
+ * is then the full (viscous) Navier-Stokes flux. */
+icx_status icx_disc_ns_viscosity(icx_ctx* ctx, int kind, double mu_ratio, double T0_ratio, double Ts_ratio);
 /* public members interior_penalty and sigma_ic (CL:137-143) */
 icx_status icx_disc_options(icx_ctx* ctx, int interior_penalty, double sigma_ic);
 icx_status icx_disc_dirichlet(icx_ctx* ctx, int bcflag, icx_point_fn fn, void* user);

@@ -186,13 +186,28 @@ struct BurgersDiffusionFlux {
 // ----------------------------------------------------- Navier-Stokes fluxes
 namespace navier_stokes {
 
+// DimensionlessSutherlands (navier_stokes.hpp:260-287): the ratios of
+// Sutherland's constants to the reference viscosity and temperature
+struct DimensionlessSutherlands {
+  double mu_0 = 1.716e-5, T_0 = 273.1, T_s = 110.5;
+  double mu_ratio = 1.716e-5, T_0_ratio = 273.1, T_s_ratio = 110.5;  // unit reference parameters
+  DimensionlessSutherlands() = default;
+  DimensionlessSutherlands(double ref_mu, double ref_T)
+      : mu_ratio(mu_0 / ref_mu), T_0_ratio(T_0 / ref_T), T_s_ratio(T_s / ref_T) {}
+  double operator()(double That) const {
+    return mu_ratio * std::pow(That / T_0_ratio, 1.5) * (T_0_ratio + T_s_ratio) / (That + T_s_ratio);
+  }
+};
+
 // the physics of navier_stokes::Physics with unit ReferenceParameters, an
-// ideal gas (CaloricallyPerfectEoS) and constant viscosity
+// ideal gas (CaloricallyPerfectEoS) and a constant viscosity mu, or
+// Sutherland's law when `sutherland` is set
 struct Physics {
   double gamma = 1.4;
   double Pr = 0.72;
   double mu = 0.01;
   double Rgas = 287.052874;
+  std::optional<DimensionlessSutherlands> sutherland{};
   std::vector<double> isothermal_temperatures{};
   struct FreeStream {
     double rho_inf = 1.0, u_inf = 0.0;
@@ -201,8 +216,10 @@ struct Physics {
   } free_stream{};
 
   struct State {
-    double rho, v[2], vv, rhoE, E, p, c;
+    double rho, v[2], vv, rhoE, E, p, c, T;
   };
+  double viscosity(const State& s) const { return sutherland ? (*sutherland)(s.T) : mu; }
+  bool viscous() const { return sutherland.has_value() || mu != 0.0; }
   State thermo(const std::array<double, 4>& u) const {
     State s{};
     s.rho = std::max(1e-14, u[0]);
@@ -213,6 +230,7 @@ struct Physics {
     s.E = s.rhoE / s.rho;
     s.p = std::max(1e-12, (gamma - 1) * s.rho * (s.E - 0.5 * s.vv));
     s.c = std::sqrt(gamma * s.p / s.rho);
+    s.T = s.p / s.rho * gamma / (gamma - 1) / (gamma / (gamma - 1) * Rgas);
     return s;
   }
 };
@@ -229,12 +247,13 @@ struct Flux {
       for (int j = 0; j < 2; ++j) gv[i][j] = (g(1 + i, j) - s.v[i] * g(0, j)) / s.rho;
     for (int j = 0; j < 2; ++j) gE[j] = (g(3, j) - s.E * g(0, j)) / s.rho;
     const double div = gv[0][0] + gv[1][1];
+    const double mu = physics.viscosity(s);
     for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j) tau[i][j] = physics.mu * (gv[i][j] + gv[j][i]) - (i == j ? 2.0 / 3.0 * physics.mu * div : 0.0);
+      for (int j = 0; j < 2; ++j) tau[i][j] = mu * (gv[i][j] + gv[j][i]) - (i == j ? 2.0 / 3.0 * mu * div : 0.0);
     for (int j = 0; j < 2; ++j) {
       F[0][j] = u[1 + j];
       for (int i = 0; i < 2; ++i) F[1 + i][j] = u[1 + i] * s.v[j] + (i == j ? s.p : 0.0) - tau[i][j];
-      double q = physics.mu * physics.gamma / physics.Pr * (gE[j] - s.v[0] * gv[0][j] - s.v[1] * gv[1][j]);
+      double q = mu * physics.gamma / physics.Pr * (gE[j] - s.v[0] * gv[0][j] - s.v[1] * gv[1][j]);
       F[3][j] = s.v[j] * (s.rhoE + s.p) - (q + s.v[0] * tau[0][j] + s.v[1] * tau[1][j]);
     }
     return F;
@@ -246,7 +265,7 @@ struct Flux {
     const auto s = physics.thermo(uL);
     const double gam = physics.gamma, cp = gam / (gam - 1) * physics.Rgas;
     if (bct == BOUNDARY_CONDITIONS::WALL_GENERAL)
-      bct = physics.mu != 0.0 ? BOUNDARY_CONDITIONS::NO_SLIP_ISOTHERMAL : BOUNDARY_CONDITIONS::SLIP_WALL;
+      bct = physics.viscous() ? BOUNDARY_CONDITIONS::NO_SLIP_ISOTHERMAL : BOUNDARY_CONDITIONS::SLIP_WALL;
     if (bct == BOUNDARY_CONDITIONS::SLIP_WALL) {
       const double mn = uL[1] * n[0] + uL[2] * n[1];
       return {uL[0], uL[1] - 2 * mn * n[0], uL[2] - 2 * mn * n[1], uL[3]};
@@ -357,13 +376,14 @@ struct DiffusionFlux {
       for (int j = 0; j < 2; ++j) gv[i][j] = (g(1 + i, j) - s.v[i] * g(0, j)) / s.rho;
     for (int j = 0; j < 2; ++j) gE[j] = (g(3, j) - s.E * g(0, j)) / s.rho;
     const double div = gv[0][0] + gv[1][1];
+    const double mu = physics.viscosity(s);
     for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j) tau[i][j] = physics.mu * (gv[i][j] + gv[j][i]) - (i == j ? 2.0 / 3.0 * physics.mu * div : 0.0);
+      for (int j = 0; j < 2; ++j) tau[i][j] = mu * (gv[i][j] + gv[j][i]) - (i == j ? 2.0 / 3.0 * mu * div : 0.0);
     std::array<double, 4> f{};
     for (int j = 0; j < 2; ++j) {
       f[1] += tau[0][j] * n[j];
       f[2] += tau[1][j] * n[j];
-      f[3] += (physics.mu * physics.gamma / physics.Pr * gE[j] + s.v[0] * tau[0][j] + s.v[1] * tau[1][j]) * n[j];
+      f[3] += (mu * physics.gamma / physics.Pr * gE[j] + s.v[0] * tau[0][j] + s.v[1] * tau[1][j]) * n[j];
     }
     return f;
   }
@@ -389,6 +409,9 @@ struct device_physics<navier_stokes::Flux, CF, navier_stokes::DiffusionFlux> {
     const auto& ph = pf.physics;
     const int kind = std::same_as<CF, navier_stokes::Roe> ? ICX_FLUX_ROE : ICX_FLUX_VANLEER;
     check(icx_disc_navier_stokes(c, ph.gamma, ph.Pr, ph.mu, kind), c, "icx_disc_navier_stokes");
+    if (ph.sutherland)
+      check(icx_disc_ns_viscosity(c, 1, ph.sutherland->mu_ratio, ph.sutherland->T_0_ratio, ph.sutherland->T_s_ratio),
+            c, "icx_disc_ns_viscosity");
     check(icx_disc_ns_boundary(c, ph.isothermal_temperatures.data(), (int)ph.isothermal_temperatures.size(),
                                ph.free_stream.rho_inf, ph.free_stream.u_inf, ph.free_stream.u_direction.data(),
                                ph.free_stream.temp_inf, ph.Rgas),

@@ -433,8 +433,14 @@ static void ns_grads(const ns_state* s, const double* g, double gv[2][2], double
   for (int j = 0; j < 2; ++j) gE[j] = (g[2 * 3 + j] - s->E * g[2 * 0 + j]) / s->rho;
 }
 
-static void ns_tau(const orc_problem* pb, const double gv[2][2], double tau[2][2]) {
-  double mu = pb->ns_mu;
+/* the viscosity law at temperature T: constant_viscosity (NS:226-237) or
+ * DimensionlessSutherlands (NS:260-287) */
+static double ns_viscosity(const orc_problem* pb, double T) {
+  if (pb->ns_visc != 1) return pb->ns_mu;
+  return pb->suth[0] * pow(T / pb->suth[1], 1.5) * (pb->suth[1] + pb->suth[2]) / (T + pb->suth[2]);
+}
+
+static void ns_tau(double mu, const double gv[2][2], double tau[2][2]) {
   double div = gv[0][0] + gv[1][1];
   for (int i = 0; i < 2; ++i)
     for (int j = 0; j < 2; ++j) tau[i][j] = mu * (gv[i][j] + gv[j][i]);
@@ -453,8 +459,8 @@ static void ns_flux(const orc_problem* pb, const double* u, const double* g, dou
   }
   double gv[2][2], gE[2], tau[2][2], q[2];
   ns_grads(&s, g, gv, gE);
-  ns_tau(pb, gv, tau);
-  double mu = pb->ns_mu;
+  double mu = ns_viscosity(pb, s.T);
+  ns_tau(mu, gv, tau);
   for (int j = 0; j < 2; ++j) { /* heat flux (NS:724-745) */
     q[j] = gE[j] / 1.0;
     for (int k = 0; k < 2; ++k) q[j] -= s.vel[k] * gv[k][j];
@@ -513,9 +519,9 @@ static void ns_diff(const orc_problem* pb, const double* u, const double* g, con
   ns_thermo(pb, u, &s);
   double gv[2][2], gE[2], tau[2][2];
   ns_grads(&s, g, gv, gE);
-  ns_tau(pb, gv, tau);
+  double mu = ns_viscosity(pb, s.T);
+  ns_tau(mu, gv, tau);
   f[0] = f[1] = f[2] = f[3] = 0.0;
-  double mu = pb->ns_mu;
   for (int j = 0; j < 2; ++j) {
     double ef = mu * s.gamma / pb->Pr * gE[j] * n[j];
     for (int i = 0; i < 2; ++i) {
@@ -576,7 +582,8 @@ static void ns_apply_bc(const orc_problem* pb, const double* uL, const double n[
   ns_state L;
   ns_thermo(pb, uL, &L);
   double g = pb->gamma, cp = g / (g - 1) * NS_RGAS;
-  if (bct == ORC_BC_WALL_GENERAL) bct = pb->ns_mu != 0.0 ? ORC_BC_NO_SLIP_ISOTHERMAL : ORC_BC_SLIP_WALL;
+  if (bct == ORC_BC_WALL_GENERAL)
+    bct = (pb->ns_mu != 0.0 || pb->ns_visc == 1) ? ORC_BC_NO_SLIP_ISOTHERMAL : ORC_BC_SLIP_WALL;
   if (bct == ORC_BC_SLIP_WALL) { /* NS:997-1017 */
     double mn = L.mom[0] * n[0] + L.mom[1] * n[1];
     uR[0] = uL[0];
@@ -892,7 +899,8 @@ static int boundary_integral(const disc* D, const int* F, const double* uL, doub
        * same one-sided DDG flux as a Dirichlet face (CL:1043-1130) */
       double ud[MAXEQ] = {0};
       if (pde_bc) {
-        int iso = bct == ORC_BC_NO_SLIP_ISOTHERMAL || (bct == ORC_BC_WALL_GENERAL && pb->ns_mu != 0.0);
+        int iso = bct == ORC_BC_NO_SLIP_ISOTHERMAL ||
+                  (bct == ORC_BC_WALL_GENERAL && (pb->ns_mu != 0.0 || pb->ns_visc == 1));
         if (iso && (flag < 0 || flag >= pb->n_wall)) return -2;
         ns_apply_bc(pb, ul, fq.n, bct, flag, ud);
       } else {

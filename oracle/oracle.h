@@ -50,6 +50,10 @@ typedef struct orc_problem {
   int n_wall;
   double wall_T[8];
   double fs_rho, fs_u_inf, fs_dir[2], fs_T;
+  /* viscosity law: 0 constant_viscosity{ns_mu}; 1 DimensionlessSutherlands
+   * with suth = {mu_ratio, T_0_ratio, T_s_ratio} (navier_stokes.hpp:260-287) */
+  int ns_visc;
+  double suth[3];
 } orc_problem;
 
 /* reference BOUNDARY_CONDITIONS enumerators used here */

@@ -71,6 +71,8 @@ struct ref_problem {
   int n_wall;           // Physics::isothermal_temperatures
   double wall_T[8];
   double fs_rho, fs_u_inf, fs_dir[2], fs_T;  // Physics::free_stream
+  int ns_visc;                               // 0 constant_viscosity, 1 DimensionlessSutherlands
+  double suth[3];                            // mu_ratio, T_0_ratio, T_s_ratio
 };
 }
 
@@ -165,7 +167,16 @@ int with_disc(const ref_problem& pb, const double* coord, Body&& body) {
     navier_stokes::CaloricallyPerfectEoS<T, ndim> eos{};
     eos.gamma = pb.gamma;
     navier_stokes::constant_viscosity<T> visc{pb.ns_mu};
-    navier_stokes::Physics<T, ndim, navier_stokes::CaloricallyPerfectEoS<T, ndim>> physics{ref, eos, visc, pb.Pr};
+    navier_stokes::DimensionlessSutherlands<T> suth{ref};
+    suth.mu_ratio = pb.suth[0];
+    suth.T_0_ratio = pb.suth[1];
+    suth.T_s_ratio = pb.suth[2];
+    auto make_physics = [&]() {
+      if (pb.ns_visc == 1)
+        return navier_stokes::Physics<T, ndim, navier_stokes::CaloricallyPerfectEoS<T, ndim>>{ref, eos, suth, pb.Pr};
+      return navier_stokes::Physics<T, ndim, navier_stokes::CaloricallyPerfectEoS<T, ndim>>{ref, eos, visc, pb.Pr};
+    };
+    navier_stokes::Physics<T, ndim, navier_stokes::CaloricallyPerfectEoS<T, ndim>> physics = make_physics();
     // boundary data before the flux objects copy the physics
     physics.isothermal_temperatures.assign(pb.wall_T, pb.wall_T + pb.n_wall);
     physics.free_stream.rho_inf = pb.fs_rho;
@@ -183,7 +194,7 @@ int with_disc(const ref_problem& pb, const double* coord, Body&& body) {
       add_callbacks(disc, pb);
       return body(fespace, disc, std::integral_constant<std::size_t, 4>{});
     };
-    if (pb.ns_mu != 0.0) return run(std::true_type{});
+    if (pb.ns_mu != 0.0 || pb.ns_visc == 1) return run(std::true_type{});
     return run(std::false_type{});
   }
 }

@@ -95,7 +95,7 @@ int main(int argc, char** argv) {
     std::printf("jacobian_f32_rel %.6e\n", dmax / vmax);
   }
   // Navier-Stokes 3 x 3, p = 2, Roe flux, Riemann far field left / right,
-  // slip wall below, isothermal wall above (bcflag 1)
+  // slip wall below, isothermal wall above (bcflag 1), Sutherland viscosity
   {
     ib::UniformMesh mesh({0.0, 0.0}, {1.0, 1.0}, {3, 3}, 2, {BC::RIEMANN, BC::SLIP_WALL, BC::RIEMANN, BC::NO_SLIP_ISOTHERMAL},
                          {0, 0, 0, 1});
@@ -105,6 +105,11 @@ int main(int argc, char** argv) {
     ph.free_stream.rho_inf = 1.0;
     ph.free_stream.u_inf = 0.5;
     ph.free_stream.temp_inf = 0.004;
+    ib::navier_stokes::DimensionlessSutherlands su;
+    su.mu_ratio = 0.02;
+    su.T_0_ratio = 0.004;
+    su.T_s_ratio = 0.0015;
+    ph.sutherland = su;
     ib::ConservationLawDDG disc{ib::navier_stokes::Flux{ph}, ib::navier_stokes::Roe{ph},
                                 ib::navier_stokes::DiffusionFlux{ph}};
     disc.interior_penalty = true;

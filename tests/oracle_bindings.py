@@ -28,6 +28,7 @@ class Problem(C.Structure):
         ("source", POINT_FN), ("source_user", C.c_void_p), ("spacetime", C.c_int), ("basis", C.c_int),
         ("ns_flux", C.c_int), ("n_wall", C.c_int), ("wall_T", C.c_double * 8),
         ("fs_rho", C.c_double), ("fs_u_inf", C.c_double), ("fs_dir", C.c_double * 2), ("fs_T", C.c_double),
+        ("ns_visc", C.c_int), ("suth", C.c_double * 3),
     ]
 
 

@@ -26,7 +26,7 @@ class Spec:
     def __init__(self, pde=BURGERS, nx=4, ny=3, g=2, p=2, bct=(3, 3, 3, 3), bcf=(0, 0, 0, 0), ip=False,
                  sigma_ic=0.0, mu=0.01, a=(0.3, -0.2), b=(1.0, 0.5), perturb=0.1, seed=7,
                  dirichlet=None, neumann=None, source=False, spacetime=False, basis=0, ns_flux=1, ns_mu=0.01,
-                 walls=(), free_stream=None):
+                 walls=(), free_stream=None, sutherland=None):
         self.pde, self.nx, self.ny, self.g, self.p = pde, nx, ny, g, p
         self.bct, self.bcf, self.ip, self.sigma_ic = tuple(bct), tuple(bcf), ip, sigma_ic
         self.spacetime = spacetime
@@ -35,6 +35,8 @@ class Spec:
         # temperatures per bcflag, free stream (rho, |u|, (dx, dy), T)
         self.ns_flux, self.ns_mu, self.walls = ns_flux, ns_mu, tuple(walls)
         self.free_stream = free_stream
+        # DimensionlessSutherlands ratios (mu_0/ref.mu, T_0/ref.T, T_s/ref.T), or constant viscosity
+        self.sutherland = sutherland
         if spacetime:  # Burgers in (x, t): the time component of the flux is u
             a, b = (a[0], 1.0), (b[0], 0.0)
         self.mu, self.a, self.b = mu, a, b
@@ -129,6 +131,9 @@ class Spec:
         pb.basis = int(self.basis)
         pb.gamma, pb.Pr, pb.ns_mu = 1.4, 0.72, self.ns_mu
         pb.ns_flux = self.ns_flux
+        if self.sutherland is not None:
+            pb.ns_visc = 1
+            pb.suth[:] = list(self.sutherland)
         pb.n_wall = len(self.walls)
         for i, t in enumerate(self.walls):
             pb.wall_T[i] = t
@@ -165,6 +170,8 @@ class Spec:
             ctx.disc_burgers(self.mu, self.a, self.b)
         else:
             ctx.disc_navier_stokes(1.4, 0.72, self.ns_mu, self.ns_flux)
+            if self.sutherland is not None:
+                ctx.disc_ns_viscosity(1, *self.sutherland)
             if self.walls or self.free_stream is not None:
                 fs = self.free_stream or (1.0, 0.0, (1.0, 0.0), 1.0)
                 ctx.disc_ns_boundary(self.walls, fs[0], fs[1], fs[2], fs[3])

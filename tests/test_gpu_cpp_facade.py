@@ -28,7 +28,7 @@ def facade_run(tmp_path_factory):
                   dirichlet=[("constant", [1, 0.25])])
     u_b = b_spec.state(np.random.default_rng(31))
     n_spec = Spec(pde=NS, nx=3, ny=3, p=2, g=2, perturb=0.0, ip=True, ns_flux=2, bct=(5, 7, 5, 6), bcf=(0, 0, 0, 1),
-                  walls=(0.004, 0.005), free_stream=(1.0, 0.5, (1.0, 0.0), 0.004))
+                  walls=(0.004, 0.005), free_stream=(1.0, 0.5, (1.0, 0.0), 0.004), sutherland=(0.02, 0.004, 0.0015))
     u_n = n_spec.state(np.random.default_rng(32))
     np.savetxt(d / "ub.txt", u_b)
     np.savetxt(d / "un.txt", u_n)

@@ -33,6 +33,8 @@ CASES = [
     dict(basis=1, p=4, nx=3, ny=2, sigma_ic=0.7),
     dict(basis=1, pde=NS, p=3, ip=True, source=True),
     dict(basis=1, g=1, p=1, bct=(3, 2, 4, 3)),
+    dict(pde=NS, p=2, ip=True, sutherland=(0.02, 0.004, 0.0015)),  # Sutherland viscosity
+    dict(pde=NS, p=3, sutherland=(0.02, 0.004, 0.0015), ns_mu=0.0, bct=(8, 3, 8, 3), walls=(0.004,)),
     dict(bct=(0, 3, 0, 3)),                       # periodic pairs: no flux across them
     dict(bct=(0, 0, 0, 0), p=3, sigma_ic=0.4),
 ]

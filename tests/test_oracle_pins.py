@@ -24,6 +24,9 @@ CASES = [
     dict(pde=NS, p=3),
     dict(pde=NS, p=1, g=1, bct=(3, 4, 3, 4)),
     dict(pde=NS, p=2, ip=True, source=True),
+    # DimensionlessSutherlands viscosity (mu_0/ref.mu, T_0/ref.T, T_s/ref.T)
+    dict(pde=NS, p=2, ip=True, sutherland=(0.02, 0.004, 0.0015)),
+    dict(pde=NS, p=3, sutherland=(0.02, 0.004, 0.0015), ns_mu=0.0, bct=(8, 3, 8, 3), walls=(0.004,)),
     # spacetime Burgers (x, t): past face without a connected slab, future face extrapolating
     dict(spacetime=True, a=(0.4,), b=(1.0,), bct=(3, 11, 3, 12)),
     dict(spacetime=True, p=3, a=(-0.3,), b=(0.5,), bct=(3, 3, 4, 12)),
@@ -68,7 +71,8 @@ def test_topology_bit_exact(kw):
 
 @needs_ref
 @pytest.mark.parametrize("kw", [dict(nx=3, ny=3), dict(nx=3, ny=2, bct=(3, 2, 4, 3), sigma_ic=0.5),
-                                dict(pde=NS, nx=2, ny=2, p=2, ip=True)])
+                                dict(pde=NS, nx=2, ny=2, p=2, ip=True),
+                                dict(pde=NS, nx=2, ny=2, p=2, sutherland=(0.02, 0.004, 0.0015))])
 def test_fd_jacobian_matches_reference(kw):
     """One-sided FD with eps = sqrt(machine eps) amplifies the last-bit
     differences of two residual evaluations by 1/eps ~ 7e7, so FD Jacobians of
