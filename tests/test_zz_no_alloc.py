@@ -5,8 +5,9 @@ residuals (a host framework that owns the device memory pool and forbids other
 allocations during a solve; a time-critical loop that must avoid cudaMalloc's
 device-wide synchronisation). Its face scratch is a fixed 2^20-double device
 array. Checked here through the C ABI against icx_form_residual on two calls in
-a row (tolerance 1e-12 relative to the largest entry, as the other residual
-parity tests), and the size limit is checked to fail cleanly.
+a row and directly against the oracle's residual (tolerance 1e-12 relative to
+the largest entry, as the other residual parity tests), and the size limit is
+checked to fail cleanly.
 
 This file is collected last so that a run that stops at the first failure has
 already run every other test."""
@@ -17,6 +18,7 @@ import pytest
 import torch
 
 import iceicle_b200 as ib
+import oracle_bindings as ob
 from specs import BURGERS, NS, Spec
 
 pytestmark = pytest.mark.gpu
@@ -44,6 +46,25 @@ def test_noalloc_matches_residual_two_calls(kw):
         r_ref, r_new = _both(ctx, u)
         assert np.isfinite(r_new).all()
         assert np.abs(r_new - r_ref).max() <= 1e-12 * np.abs(r_ref).max()
+    ctx.close()
+
+
+@pytest.mark.parametrize("kw", [dict(pde=NS, nx=12, ny=10, p=3, ip=True, source=True),
+                                dict(pde=BURGERS, nx=9, ny=7, p=4, sigma_ic=0.5, bct=(3, 2, 4, 3))],
+                         ids=["ns_p3_12x10", "burgers_p4_ddgic"])
+def test_noalloc_matches_oracle(kw):
+    spec = Spec(**kw)
+    c = spec.coords()
+    ctx = spec.context(c)
+    u = spec.state(np.random.default_rng(23))
+    du = torch.from_numpy(u).cuda()
+    dr = torch.full_like(du, float("nan"))
+    ctx.form_residual_noalloc(du, dr)
+    torch.cuda.synchronize()
+    r = dr.cpu().numpy()
+    r_or = ob.residual(ob.oracle(), spec.oracle_problem(), c, u)
+    assert np.isfinite(r).all()
+    assert np.abs(r - r_or).max() <= 1e-12 * np.abs(r_or).max()
     ctx.close()
 
 
