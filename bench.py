@@ -56,7 +56,7 @@ def parse():
                          "NS 256 x 256 p = 2) and print one JSON line")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-preconditioner Newton comparison (256 x 256 Navier-Stokes, p = 2)")
-    ap.add_argument("--batched", type=int, default=64, metavar="N",
+    ap.add_argument("--batched", type=int, default=512, metavar="N",
                     help="secondary timing of N seeded uneven advection-diffusion problems, batched vs one at a "
                          "time (0: skip; the full problem set is 512)")
     ap.add_argument("--no-tune", action="store_true",
@@ -222,47 +222,87 @@ def residual_work(wl):
 NCU_DRAM_BYTES = {"vol": 43.45e6 + 0.57e6, "face": 25.42e6 + 0.0003e6}
 
 
-def batched_bench(torch, dev, n_problems):
-    """Newton solves (FP64, GMRES(30) + block-ILU(0), |r| <= 1e-10) of the
-    seeded uneven advection-diffusion problems: grouped by basis order into one
-    batch context each (one launch per kernel for all problems of a group)
-    against the same problems solved one context at a time. CUDA events around
-    the solves; the setup of the contexts is not timed."""
+def batched_bench(torch, dev, n_problems, sample=48):
+    """Newton solves to |r| <= 1e-10 per problem (Wolfe line search, GMRES(30)
+    + block-ILU(0)) of the seeded uneven advection-diffusion problems (meshes
+    8x8 to 96x96, orders 1-4, viscosity log-uniform in [1e-4, 1e-1], advection
+    angle uniform): all of them as one ProblemSet (each problem its own Newton
+    solve; every kernel launched once per basis order for all problems; each
+    Arnoldi step of the set one CUDA graph), in FP64 and with FP32 flux
+    quadrature (precision 2), against the problems solved one context at a
+    time. One at a time runs on a seeded sample of `sample` problems (all of
+    them would take minutes); the ratio compares it with the set of the same
+    sample. Every timing is the second of two runs (the first does the
+    one-time setup: buffers, graph capture); CUDA events around each solve;
+    contexts are built before the timed region."""
     import iceicle_b200 as ib
-    from iceicle_b200.workloads import batched_problems
-    groups = batched_problems(n_problems, device=dev.index)
-    opt = ib.default_newton_options()
-    t_batch = t_seq = 0.0
-    worst = 0.0
-    n_dof = 0
-    its = []
-    for p, (b, parts, u0, specs) in groups.items():
-        ub = torch.from_numpy(u0.copy()).to(dev)
+    import iceicle_b200.workloads as w
+    specs = w.batched_problem_specs(n_problems)
+    parts, u0 = [], []
+    for sp in specs:
+        c, u = w.advection_diffusion_problem(sp, dev.index)
+        parts.append(c)
+        u0.append(u)
+
+    def timed(fn):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fn()
         torch.cuda.synchronize(dev)
         e0.record()
-        rep = b.newton_solve(ub, opt)
+        out = fn()
         e1.record()
         torch.cuda.synchronize(dev)
-        t_batch += e0.elapsed_time(e1) * 1e-3
-        its.append(dict(p=p, problems=len(parts), newton_its=rep.iterations, gmres_its=rep.linear_iterations_total,
-                        converged=bool(rep.converged)))
-        off = 0
-        for c in parts:
-            n = c.layout.n_dof
-            uc = torch.from_numpy(u0[off:off + n].copy()).to(dev)
-            torch.cuda.synchronize(dev)
-            e0.record()
-            c.newton_solve(uc, opt)
-            e1.record()
-            torch.cuda.synchronize(dev)
-            t_seq += e0.elapsed_time(e1) * 1e-3
-            a, bb = uc.cpu().numpy(), ub[off:off + n].cpu().numpy()
-            worst = max(worst, float(np.linalg.norm(a - bb) / max(np.linalg.norm(a), 1e-300)))
-            off += n
-        n_dof += off
-    return {"problems": n_problems, "n_dof": n_dof, "batched_s": t_batch, "one_at_a_time_s": t_seq,
-            "speedup": t_seq / t_batch if t_batch > 0 else None, "max_state_rel_diff": worst, "groups": its}
+        return e0.elapsed_time(e1) * 1e-3, out
+
+    def set_solve(ps, prec):
+        opt = ib.default_newton_options()
+        opt.precision = prec
+        holder = {}
+
+        def run():
+            u = torch.from_numpy(ps.gather([u0[k] for k in ps.members])).to(dev)
+            holder["u"] = u
+            return ps.newton_solve(u, opt)
+        t, (reps, stats) = timed(run)
+        return t, holder["u"].cpu().numpy(), reps, stats
+
+    ps = ib.ProblemSet(parts, dev.index)
+    ps.members = list(range(n_problems))
+    t_all, u_all, reps, stats = set_solve(ps, 0)
+    t_q32, u_q32, reps32, _ = set_solve(ps, 2)
+    rng = np.random.default_rng(5)
+    pick = sorted(rng.choice(n_problems, size=min(sample, n_problems), replace=False).tolist())
+    sub = ib.ProblemSet([parts[k] for k in pick], dev.index)
+    sub.members = pick
+    t_sub, u_sub, _, _ = set_solve(sub, 0)
+    opt = ib.default_newton_options()
+    t_seq, worst = 0.0, 0.0
+    for i, k in enumerate(pick):
+        holder = {}
+
+        def run():
+            uk = torch.from_numpy(u0[k].copy()).to(dev)
+            holder["u"] = uk
+            return parts[k].newton_solve(uk, opt)
+        t, _ = timed(run)
+        t_seq += t
+        a, b = holder["u"].cpu().numpy(), sub.part(u_sub, i)
+        worst = max(worst, float(np.linalg.norm(a - b) / max(np.linalg.norm(a), 1e-300)))
+    q32 = max(float(np.linalg.norm(ps.part(u_all, k) - ps.part(u_q32, k)) /
+                    max(np.linalg.norm(ps.part(u_all, k)), 1e-300)) for k in range(n_problems))
+    n_dof = ps.offsets[-1]
+    out = {"problems": n_problems, "n_dof": int(n_dof), "orders": stats.orders,
+           "set_fp64_s": t_all, "set_fp32_quadrature_s": t_q32,
+           "converged": int(sum(r.converged for r in reps)), "converged_fp32_quadrature": int(sum(r.converged for r in reps32)),
+           "newton_rounds": stats.newton_rounds, "arnoldi_steps": stats.arnoldi_steps,
+           "arnoldi_graph_launches": stats.graph_launches, "line_search_rounds": stats.line_search_rounds,
+           "max_newton_its": max(r.iterations for r in reps),
+           "fp32_quadrature_vs_fp64_state_l2_max": q32,
+           "sample": {"problems": len(pick), "set_s": t_sub, "one_at_a_time_s": t_seq,
+                      "speedup": t_seq / t_sub if t_sub > 0 else None, "max_state_rel_diff": worst}}
+    sub.close()
+    ps.close()
+    return out
 
 
 def roe_residual_bench(torch, dev, flush, tune=True, steps=20):

@@ -75,6 +75,11 @@ class NewtonReport(C.Structure):
                 ("linear_iterations", C.c_int * 64), ("graph_steps", C.c_int)]
 
 
+class PsetStats(C.Structure):
+    _fields_ = [("newton_rounds", C.c_int), ("arnoldi_steps", C.c_int), ("graph_launches", C.c_int),
+                ("line_search_rounds", C.c_int), ("orders", C.c_int)]
+
+
 class LpcTrainOptions(C.Structure):
     _fields_ = [("steps", C.c_int), ("batch", C.c_int), ("random", C.c_int), ("sweeps", C.c_int),
                 ("lr", C.c_double), ("seed", C.c_ulonglong)]
@@ -151,6 +156,13 @@ def lib():
             "icx_mfnk_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport)]),
             "icx_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int, C.POINTER(vp)]),
             "icx_batch_offsets": (C.c_int, [vp, ip]),
+            "icx_pset_create": (C.c_int, [C.POINTER(vp), C.c_int, C.c_int, C.POINTER(vp)]),
+            "icx_pset_destroy": (None, [vp]),
+            "icx_pset_offsets": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
+            "icx_pset_residual": (C.c_int, [vp, vp, vp]),
+            "icx_pset_newton_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport),
+                                                C.POINTER(PsetStats)]),
+            "icx_pset_last_error": (C.c_char_p, [vp]),
             "icx_explicit_solve": (C.c_int, [vp, vp, C.POINTER(ExplicitOptions), C.POINTER(ExplicitReport)]),
             "icx_mass_inverse_apply": (C.c_int, [vp, vp, vp, vp]),
             "icx_newton_solve": (C.c_int, [vp, vp, C.POINTER(NewtonOptions), C.POINTER(NewtonReport)]),
@@ -702,6 +714,65 @@ def batch(parts, device=0):
     b._check(lib().icx_get_layout(b._h, C.byref(lay)), "get_layout")
     b.layout = lay
     return b
+
+
+class ProblemSet:
+    """icx_pset: independent problems of uneven mesh size and basis order
+    (set-up Contexts, kept alive by the set), each solved by its own Newton
+    iteration with every kernel launched once per basis order for all parts.
+    `offsets[k]` is part k's first unknown in the set's vectors, `offsets[-1]`
+    the total."""
+
+    def __init__(self, parts, device=0):
+        self._h = C.c_void_p()
+        self._keep = list(parts)
+        arr = (C.c_void_p * len(parts))(*[p._h.value for p in parts])
+        st = lib().icx_pset_create(C.byref(self._h), device, len(parts), arr)
+        if st != 0:
+            raise IcxError(st, "pset_create")
+        off = (C.c_longlong * (len(parts) + 1))()
+        self._check(lib().icx_pset_offsets(self._h, off), "pset_offsets")
+        self.offsets = list(off)
+        self.n_parts = len(parts)
+
+    def _check(self, st, what):
+        if st != 0:
+            raise IcxError(st, f"{what}: {lib().icx_pset_last_error(self._h).decode()}")
+
+    def close(self):
+        if self._h:
+            lib().icx_pset_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def gather(self, vectors):
+        """one host vector in the set's layout from the parts' vectors"""
+        out = np.zeros(self.offsets[-1])
+        for k, v in enumerate(vectors):
+            out[self.offsets[k]:self.offsets[k + 1]] = v
+        return out
+
+    def part(self, x, k):
+        return x[self.offsets[k]:self.offsets[k + 1]]
+
+    def residual(self, u, res):
+        self._check(lib().icx_pset_residual(self._h, _ptr(u), _ptr(res)), "pset_residual")
+
+    def newton_solve(self, u, options=None):
+        """(reports per part, PsetStats); a part that does not converge shows
+        in its report (the call itself raises only on other errors)"""
+        opt = options or default_newton_options()
+        reps = (NewtonReport * self.n_parts)()
+        stats = PsetStats()
+        st = lib().icx_pset_newton_solve(self._h, _ptr(u), C.byref(opt), reps, C.byref(stats))
+        if st not in (0, 5):
+            self._check(st, "pset_newton_solve")
+        return list(reps), stats
 
 
 def default_explicit_options(**kw):

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -230,4 +231,17 @@ const float* solver_vals32(icx_ctx* c);
 // cleared with the completion counters when set)
 cudaError_t solver_apply_ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStream_t s);
 icx_status solver_take_pc_err(icx_ctx* c, int* err);
+// the per-group pieces of a batch of independent solves (icx_pset.cu):
+// buffers and options, the FP64 residual with the Jacobian (precision 2: FP32
+// quadrature), the preconditioner, the Jacobian as operator, the factorisation
+// flag, whether the preconditioner apply can be captured in a graph, and the
+// reference's line searches (1 Wolfe, 2 Corrigan, else the full step)
+icx_status solver_group_ready(icx_ctx* c, int precision, int pc_sweeps, int ilu_tile, bool graphs);
+cudaError_t solver_linearise(icx_ctx* c, const double* u, double* res, int precision, cudaStream_t s);
+cudaError_t solver_build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s);
+cudaError_t solver_operator(icx_ctx* c, bool mixed, const double* x, double* y, cudaStream_t s);
+const int* solver_flag(icx_ctx* c);
+bool solver_graphable(icx_ctx* c, int pc, bool mixed);
+unsigned long long solver_graph_key(icx_ctx* c, int pc, bool mixed);
+double solver_line_search(int kind, const std::function<double(double)>& f, const icx_newton_options& o);
 }  // namespace icx

@@ -1019,6 +1019,66 @@ cudaError_t solver_apply_ilu_flow(icx_ctx* c, bool mixed, const double* x, doubl
   return ilu_flow(c, mixed, x, z, s);
 }
 
+// ---- the pieces a batch of independent solves drives per group context
+icx_status solver_group_ready(icx_ctx* c, int precision, int pc_sweeps, int ilu_tile, bool graphs) {
+  // one Krylov vector of the group's own: the batch holds the Krylov basis
+  icx_status st = ensure_work(c, 1);
+  if (st != ICX_OK) return st;
+  if (precision >= 1 && (st = ensure_mixed(c)) != ICX_OK) return st;
+  c->sw->sweeps = pc_sweeps;
+  c->sw->graphs_on = graphs;
+  if (ilu_tile >= 0) c->ilu_tile = ilu_tile;
+  return ICX_OK;
+}
+
+cudaError_t solver_linearise(icx_ctx* c, const double* u, double* res, int precision, cudaStream_t s) {
+  icx_solver_work* w = c->sw;
+  if (precision != 2) return launch_jacobian_fd(c->dm, c->phys, u, res, w->vals, std::sqrt(DBL_EPSILON), s);
+  cudaError_t e = launch_jacobian_fd_f32(c->dm, c->phys, u, res, w->vals32, s);
+  return e == cudaSuccess ? la_f2d((long long)w->nnzb * w->bs * w->bs, w->vals32, w->vals, s) : e;
+}
+
+cudaError_t solver_build_pc(icx_ctx* c, int kind, bool mixed, cudaStream_t s) { return build_pc(c, kind, mixed, s); }
+
+cudaError_t solver_operator(icx_ctx* c, bool mixed, const double* x, double* y, cudaStream_t s) {
+  icx_solver_work* w = c->sw;
+  return mixed ? launch_bsr_spmv_f32(c->dm, w->vals32, x, y, s) : launch_bsr_spmv(c->dm, w->vals, x, y, s);
+}
+
+const int* solver_flag(icx_ctx* c) { return c->sw ? c->sw->flag : nullptr; }
+
+// whether preconditioner `pc` launches the same kernels with the same
+// arguments at every apply (the condition of the Arnoldi-step graphs)
+bool solver_graphable(icx_ctx* c, int pc, bool mixed) {
+  icx_solver_work* w = c->sw;
+  return w && w->graphs_on &&
+         (pc == 0 || pc == 1 || pc == 3 || pc == 4 ||
+          (pc == 2 && flow_sentinel(c->dm.tile, mixed ? 1 : 0) && !(w->rows_ok && w->schedule == 2)));
+}
+
+// what the launches of a preconditioner apply and operator product depend on
+// (FNV-1a; a graph holding them is replayed only under the same key)
+unsigned long long solver_graph_key(icx_ctx* c, int pc, bool mixed) {
+  icx_solver_work* w = c->sw;
+  const DeviceMesh& dm = c->dm;
+  const TileChoice& t = dm.tile;
+  const int pi = mixed ? 1 : 0;
+  unsigned long long key = 1469598103934665603ull;
+  for (long long v : {(long long)pc, (long long)mixed, (long long)w->sweeps, (long long)t.flow_rows[pi],
+                      (long long)t.flow_ctas[pi], (long long)t.flow_sched[pi], (long long)(uintptr_t)dm.bsr_rowptr,
+                      (long long)(uintptr_t)dm.bsr_colidx, (long long)(uintptr_t)dm.bsr_diag,
+                      (long long)(uintptr_t)w->order, (long long)w->tp.tile, (long long)(uintptr_t)w->tp.order,
+                      (long long)(uintptr_t)w->vals, (long long)(uintptr_t)w->pc})
+    key = (key ^ (unsigned long long)v) * 1099511628211ull;
+  return key;
+}
+
+double solver_line_search(int kind, const std::function<double(double)>& f, const icx_newton_options& o) {
+  if (kind == 1) return wolfe_ls(f, o.ls_alpha_max, o.ls_alpha_initial, o.ls_max_it, o.ls_c1, o.ls_c2);
+  if (kind == 2) return corrigan_ls(f, o.ls_alpha_max, o.ls_alpha_initial, o.ls_max_it, o.ls_alpha_min);
+  return 1.0;
+}
+
 icx_status solver_take_pc_err(icx_ctx* c, int* err) {
   icx_solver_work* w = c->sw;
   cudaStream_t s = 0;

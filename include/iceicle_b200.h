@@ -427,6 +427,40 @@ icx_status icx_mass_inverse_apply(icx_ctx* ctx, const double* d_r, double* d_out
 icx_status icx_batch_create(icx_ctx** out, int device, int n_parts, icx_ctx* const* parts);
 icx_status icx_batch_offsets(const icx_ctx* batch, int* elem_offsets);
 
+/* ---- sets of independent problems of uneven mesh size and basis order (no
+ * counterpart in the reference). icx_pset_create groups n_parts set-up
+ * contexts by basis order into batches (icx_batch_create's rules hold within
+ * an order; every part has the same PDE). The set's vectors hold each order's
+ * parts side by side, orders ascending, parts in their given order within an
+ * order; icx_pset_offsets gives part k's first unknown (offsets[k], in the
+ * caller's part numbering) and offsets[n_parts] = the total. The parts must
+ * outlive the set.
+ * icx_pset_newton_solve runs one Newton solve per part, each on its own
+ * (petsc_newton.hpp:205-329): its own residual norm and stopping test, its own
+ * GMRES Krylov space, Hessenberg matrix and convergence, its own line search
+ * and step length. A Newton iteration of the set launches each kernel once
+ * per basis order for all parts; each GMRES Arnoldi step of the whole set is
+ * one CUDA graph launch (cuda_graphs = 1, preconditioners whose apply is
+ * graph-invariant). reports[k] is part k's report; the status is
+ * ICX_ERR_NOT_CONVERGED when a part did not converge. Preconditioners 0-2 and
+ * 4; precision 0-2 as icx_newton_solve. */
+typedef struct icx_pset icx_pset;
+typedef struct icx_pset_stats {
+  int newton_rounds;       /* Newton iterations of the set (the slowest part's) */
+  int arnoldi_steps;       /* Arnoldi steps of the set (each covers every part still iterating) */
+  int graph_launches;      /* of those, replayed from CUDA graphs */
+  int line_search_rounds;  /* residual evaluations of the whole set for the line searches */
+  int orders;              /* basis-order groups */
+} icx_pset_stats;
+icx_status icx_pset_create(icx_pset** out, int device, int n_parts, icx_ctx* const* parts);
+void icx_pset_destroy(icx_pset* set);
+icx_status icx_pset_offsets(const icx_pset* set, long long* offsets);
+/* every part's residual R(u_k) into d_res (the set's layout) */
+icx_status icx_pset_residual(icx_pset* set, const double* d_u, double* d_res);
+icx_status icx_pset_newton_solve(icx_pset* set, double* d_u, const icx_newton_options* opt,
+                                 icx_newton_report* reports, icx_pset_stats* stats);
+const char* icx_pset_last_error(const icx_pset* set);
+
 /* Krylov samples for training the learned preconditioner: the GMRES solve of
  * icx_gmres_solve (from a zero guess, FP64) that also copies the true residual
  * at every restart and every `every`-th Arnoldi vector into d_samples

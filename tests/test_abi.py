@@ -79,7 +79,8 @@ STRUCTS = {"icx_layout_info": "LayoutInfo", "icx_newton_options": "NewtonOptions
            "icx_newton_report": "NewtonReport", "icx_explicit_options": "ExplicitOptions",
            "icx_explicit_report": "ExplicitReport", "icx_lpc_train_options": "LpcTrainOptions",
            "icx_lpc_train_report": "LpcTrainReport", "icx_tile_choice": "TileChoice",
-           "icx_tune_report": "TuneReport", "icx_lm_options": "LMOptions", "icx_lm_report": "LMReport"}
+           "icx_tune_report": "TuneReport", "icx_lm_options": "LMOptions", "icx_lm_report": "LMReport",
+           "icx_pset_stats": "PsetStats"}
 
 
 def test_python_structs_match_c_layout():
