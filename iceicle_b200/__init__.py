@@ -177,6 +177,7 @@ def lib():
             "icx_lpc_attach": (C.c_int, [vp, vp]),
             "icx_lpc_forward": (C.c_int, [vp, vp, vp]),
             "icx_lpc_train": (C.c_int, [vp, vp, C.c_int, vp, C.POINTER(LpcTrainOptions), C.POINTER(LpcTrainReport)]),
+            "icx_lpc_calibrate": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, dp]),
             "icx_write_restart": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_char_p]),
             "icx_read_restart": (C.c_int, [vp, vp, C.c_char_p, C.c_int, C.c_char_p]),
             "icx_write_vtu": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_char_p, C.c_char_p,
@@ -603,6 +604,14 @@ class Context:
         self._check(lib().icx_lpc_train(self._h, _ptr(vals), int(n_samples), _ptr(samples), C.byref(o),
                                         C.byref(rep)), "lpc_train")
         return rep
+
+    def lpc_calibrate(self, vals, samples, n_samples, sweeps=0):
+        """(sum <a,b>/|r|^2, sum |b|^2/|r|^2, sum |a|^2/|r|^2) over the samples
+        r, with a = r - J y, b = J C y, y the base preconditioner's output"""
+        out = (C.c_double * 3)()
+        self._check(lib().icx_lpc_calibrate(self._h, _ptr(vals), int(n_samples), _ptr(samples), int(sweeps), out),
+                    "lpc_calibrate")
+        return tuple(out)
 
     def mfnk_solve(self, u, options=None):
         """matrix-free Newton-Krylov on u (device, FP64, in place); returns the report"""

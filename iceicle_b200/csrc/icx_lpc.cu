@@ -607,4 +607,51 @@ icx_status icx_lpc_train(icx_ctx* c, const double* d_vals, int n_samples, const 
   return ICX_OK;
 }
 
+icx_status icx_lpc_calibrate(icx_ctx* c, const double* d_vals, int n_samples, const double* d_samples, int sweeps,
+                             double sums[3]) {
+  if (!c || !c->ready || !c->lpc || !d_vals || !d_samples || n_samples < 1 || !sums || sweeps < 0 || sweeps > 16)
+    return fail(c, ICX_ERR_INVALID, "calibrate: bad arguments or no model attached");
+  icx_lpc* L = c->lpc;
+  cudaSetDevice(c->device);
+  cudaStream_t s = 0;
+  icx_status st = icx::solver_prepare_pc(c, d_vals, 4, sweeps);
+  if (st != ICX_OK) return st;
+  cudaError_t e = ensure_infer(c, L);
+  if (e == cudaSuccess) e = ensure_train(c, L, 1);
+  if (e == cudaSuccess) e = icx::lpc_build(c, d_vals, s);
+  if (e != cudaSuccess) return fail(c, ICX_ERR_CUDA, std::string("calibrate: ") + cudaGetErrorString(e));
+  icx_lpc_work* w = c->lpcw;
+  const long long n = w->n;
+  const float* J32 = icx::solver_vals32(c);
+  const DeviceMesh& dm = c->dm;
+  sums[0] = sums[1] = sums[2] = 0.0;
+  double h[4];
+  for (int k = 0; k < n_samples && e == cudaSuccess; ++k) {
+    // a = r - J y (the base preconditioner's residual), b = J C y (the
+    // correction's change to it): |r - J (I + g C) y|^2 = |a - g b|^2
+    const double* r = d_samples + (size_t)k * n;
+    double* y = w->ys;
+    double* a = w->as;
+    e = icx::solver_apply_pc(c, sweeps > 0 ? 4 : 2, true, r, y, s);
+    if (e == cudaSuccess) e = icx::launch_bsr_spmv_f32(dm, J32, y, w->t2, s);
+    if (e == cudaSuccess) e = icx::la_xpay(n, r, -1.0, w->t2, a, s);
+    if (e == cudaSuccess) e = icx::lpc_apply(c, y, w->t1, s);
+    if (e == cudaSuccess) e = icx::la_xpay(n, w->t1, -1.0, y, w->t1, s);  // C y
+    if (e == cudaSuccess) e = icx::launch_bsr_spmv_f32(dm, J32, w->t1, w->t2, s);
+    if (e == cudaSuccess) e = icx::la_dot_to(n, r, r, w->dh, s);
+    if (e == cudaSuccess) e = icx::la_dot_to(n, a, w->t2, w->dh + 1, s);
+    if (e == cudaSuccess) e = icx::la_dot_to(n, w->t2, w->t2, w->dh + 2, s);
+    if (e == cudaSuccess) e = icx::la_dot_to(n, a, a, w->dh + 3, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, w->dh, 4 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) break;
+    const double rr = h[0] > 0.0 ? h[0] : 1.0;
+    sums[0] += h[1] / rr;
+    sums[1] += h[2] / rr;
+    sums[2] += h[3] / rr;
+  }
+  if (e != cudaSuccess) return fail(c, ICX_ERR_CUDA, std::string("calibrate: ") + cudaGetErrorString(e));
+  return ICX_OK;
+}
+
 }  // extern "C"

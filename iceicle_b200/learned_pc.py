@@ -88,6 +88,47 @@ def train(model, train_instances, n=256, samples=167, every=10, steps=150, batch
     return out
 
 
+def calibrate(model, instance, n=256, samples=167, every=5, sweeps=0, ilu_tile=0, newton_steps=2, device=0):
+    """held-out check of a trained model: on the Krylov residuals of a fresh
+    instance's first Newton steps, the share g in [0, 1] of the correction,
+    z = (I + g C) y, that minimises the training loss (quadratic in g: the
+    loss is S_aa - 2 g S_ab + g^2 S_bb); the output layer (W3, b3), on which
+    C depends linearly, is scaled by g. Returns a record of g and the loss at
+    g = 0 (the base preconditioner), g = 1 and the chosen g."""
+    import torch
+    dev = torch.device("cuda", device)
+    wl = make_instance(*instance, n, device)
+    ctx = wl.ctx
+    L = ctx.layout
+    bs = L.block_size
+    u = torch.from_numpy(wl.u0).to(dev)
+    res, du = torch.empty_like(u), torch.empty_like(u)
+    vals = torch.empty(L.nnz_blocks * bs * bs, dtype=torch.float64, device=dev)
+    buf = torch.empty((samples, L.n_dof), dtype=torch.float64, device=dev)
+    s_ab = s_bb = s_aa = 0.0
+    for k in range(newton_steps):
+        ctx.form_jacobian_fd(u, res, vals)
+        if float(torch.linalg.vector_norm(res)) <= 1e-10:
+            break
+        ctx.ilu_tile = 0
+        ns, _, _ = ctx.krylov_samples(vals, res, du, buf, every=every)
+        ctx.ilu_tile = ilu_tile
+        ctx.lpc_attach(model)
+        ab, bb, aa = ctx.lpc_calibrate(vals, buf, ns, sweeps)
+        ctx.lpc_attach(None)
+        s_ab, s_bb, s_aa = s_ab + ab, s_bb + bb, s_aa + aa
+        u -= du
+    g = min(max(s_ab / s_bb, 0.0), 1.0) if s_bb > 0 else 0.0
+    p = model.get_params()
+    D, H = bs * bs, model.hidden
+    o_w3 = H * D + H + H * 2 * H + H
+    p[o_w3:] *= g
+    model.set_params(p)
+    del wl
+    return dict(instance=list(instance), g=g, loss_base=s_aa, loss_full=s_aa - 2 * s_ab + s_bb,
+                loss_scaled=s_aa - 2 * g * s_ab + g * g * s_bb)
+
+
 def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu_tile=0):
     """one Newton solve of an instance to |r| <= 1e-10 (GMRES(30), Wolfe line
     search), timed with CUDA events; returns (report dict, final state)"""
@@ -144,9 +185,10 @@ def new_model(device=0, seed=0, hidden=256):
 # the training recipe of the shipped model (data/learned_pc_ns_p2.npz): 2,000
 # Jacobian / residual pairs from the plain solver on seeded instances (Re
 # uniform in [50, 500]), the correction trained on top of block-ILU(0) on
-# 32 x 32 element tiles with exact triangular solves (pc_sweeps = 0)
+# 32 x 32 element tiles with exact triangular solves (pc_sweeps = 0), then
+# scaled on a held-out instance (calibrate)
 RECIPE = dict(model_seed=1, train_instances=(8, 11), pairs=2000, samples=167, every=5, steps=120, batch=4, random=2,
-              sweeps=0, ilu_tile=32, lr=1e-3)
+              sweeps=0, ilu_tile=32, lr=1e-3, holdout=(1, 5))
 EVAL_INSTANCES = (3, 99)
 
 
@@ -165,6 +207,9 @@ def main(argv=None):
         train(m, instances(*r["train_instances"]), n=a.n, samples=r["samples"], every=r["every"], steps=r["steps"],
               batch=r["batch"], random=r["random"], sweeps=r["sweeps"], lr=r["lr"], pairs=r["pairs"],
               ilu_tile=r["ilu_tile"], log=lambda x: print(json.dumps(x), flush=True))
+        rec = calibrate(m, instances(*r["holdout"])[0], n=a.n, samples=r["samples"], every=r["every"],
+                        sweeps=r["sweeps"], ilu_tile=r["ilu_tile"])
+        print(json.dumps({"calibration": rec}), flush=True)
         m.save(a.path, sweeps=r["sweeps"], ilu_tile=r["ilu_tile"])
     else:
         m = LearnedPreconditioner.load(a.path)

@@ -503,7 +503,7 @@ typedef struct icx_lpc_train_report {
 icx_status icx_lpc_create(icx_lpc** out, int device, int block_size, int hidden, unsigned long long seed);
 void icx_lpc_destroy(icx_lpc* model);
 icx_status icx_lpc_info(const icx_lpc* model, int* block_size, int* hidden, long long* n_params, long long* steps);
-/* FP32 parameters W1 [hidden][bs^2], b1, W2 [hidden][hidden], b2, W3 [bs^2][hidden], b3 (host arrays) */
+/* FP32 parameters W1 [hidden][bs^2], b1, W2 [hidden][2 hidden], b2, W3 [bs^2][hidden], b3 (host arrays) */
 icx_status icx_lpc_get_params(const icx_lpc* model, float* params);
 icx_status icx_lpc_set_params(icx_lpc* model, const float* params);
 /* use `model` (NULL: detach) for preconditioner 5 of this context; the model must outlive the attachment */
@@ -514,6 +514,14 @@ icx_status icx_lpc_forward(icx_ctx* ctx, const double* d_vals, float* d_corr);
  * samples d_samples ([n_samples][n_dof], device) */
 icx_status icx_lpc_train(icx_ctx* ctx, const double* d_vals, int n_samples, const double* d_samples,
                          const icx_lpc_train_options* opt, icx_lpc_train_report* rep);
+/* held-out check of the attached model on Jacobian d_vals and residual
+ * samples r: with y the base preconditioner's output (block-ILU(0) FP32
+ * factors; `sweeps` Jacobi sweeps per triangle, 0: exact solves),
+ * a = r - J y and b = J C y, sums[0..2] = the sums over the samples of
+ * <a, b> / |r|^2, |b|^2 / |r|^2 and |a|^2 / |r|^2. The training loss of
+ * z = (I + g C) y is then sums[2] - 2 g sums[0] + g^2 sums[1]. */
+icx_status icx_lpc_calibrate(icx_ctx* ctx, const double* d_vals, int n_samples, const double* d_samples, int sweeps,
+                             double sums[3]);
 
 /* ---- restart files and VTU output (host files; d_u and d_ic are device
  * arrays). Not available on a batch. */

@@ -105,6 +105,40 @@ def test_training_lowers_the_preconditioned_residual():
     ctx.lpc_attach(None)
 
 
+def test_calibration_sums_and_scaling():
+    """icx_lpc_calibrate after a few training steps: positive sums, the loss
+    at the chosen g is the clamped quadratic optimum (no worse than the base
+    preconditioner, g = 0, or the full correction, g = 1), and scaling the
+    output layer by a power of two scales the correction by it exactly"""
+    spec, ctx, u0 = _ns_ctx()
+    m = ib.LearnedPreconditioner(36, 64, 0, seed=4)
+    ctx.lpc_attach(m)
+    u = torch.from_numpy(u0).cuda()
+    vals, res = _jacobian(ctx, u)
+    buf = torch.empty((24, ctx.layout.n_dof), dtype=torch.float64, device="cuda")
+    du = torch.empty_like(u)
+    ns, _, _ = ctx.krylov_samples(vals, res, du, buf, every=2, rtol=1e-8)
+    ctx.lpc_train(vals, buf, ns, steps=30, batch=4, sweeps=0, lr=2e-3, seed=5)
+    ab, bb, aa = ctx.lpc_calibrate(vals, buf, ns, 0)
+    assert bb > 0 and aa > 0
+    g = min(max(ab / bb, 0.0), 1.0)
+    q = lambda t: aa - 2 * t * ab + t * t * bb
+    assert q(g) <= min(q(0.0), q(1.0)) * (1 + 1e-12)
+    E, D = ctx.layout.n_elem, 36 * 36
+    c0 = torch.empty(E * D, dtype=torch.float32, device="cuda")
+    ctx.lpc_forward(vals, c0)
+    p = m.get_params()
+    o_w3 = 64 * D + 64 + 64 * 128 + 64
+    p[o_w3:] *= 0.5
+    m.set_params(p)
+    c1 = torch.empty_like(c0)
+    ctx.lpc_forward(vals, c1)
+    torch.cuda.synchronize()
+    # BF16 rounding of W3 is exact under a scale by 1/2
+    assert torch.allclose(c1, 0.5 * c0, rtol=0, atol=1e-6 * float(c0.abs().max()))
+    ctx.lpc_attach(None)
+
+
 @pytest.mark.parametrize("pc,prec,sweeps", [(3, 0, 0), (4, 0, 1), (4, 1, 2), (5, 1, 1), (5, 0, 2)])
 def test_parallel_and_learned_preconditioners_reach_the_ilu0_state(pc, prec, sweeps):
     """the Newton solve with preconditioner pc converges to the state of the
