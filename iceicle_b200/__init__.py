@@ -833,7 +833,8 @@ class LMOptions(C.Structure):
 class LMReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("rejections", C.c_int), ("r0", C.c_double),
                 ("r_final", C.c_double), ("linear_iterations_total", C.c_int),
-                ("residual_history", C.c_double * 64), ("alpha_history", C.c_double * 64)]
+                ("residual_history", C.c_double * 64), ("alpha_history", C.c_double * 64),
+                ("linear_relres_max", C.c_double)]
 
 
 def default_lm_options():

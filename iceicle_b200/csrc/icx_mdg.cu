@@ -1537,6 +1537,7 @@ icx_status icx_lm_solve(icx_ctx* c, double* d_u, double* x, const icx_lm_options
                        strm, &c->err);
     if (st != ICX_OK) { cleanup(); return st; }
     R->linear_iterations_total += its;
+    R->linear_relres_max = std::max(R->linear_relres_max, rr);
     MCK(cudaMemcpy(px.data(), s.d_p + N, sizeof(double) * ngeo, cudaMemcpyDeviceToHost));
     double alpha = 1.0;
     bool accept = true;
@@ -1608,7 +1609,8 @@ icx_status icx_lm_solve(icx_ctx* c, double* d_u, double* x, const icx_lm_options
       R->residual_history[hist] = rk;
       R->alpha_history[hist - 1] = alpha;
     }
-    if (opt->verbosity > 0) std::printf("lm %d: |r| = %.6e alpha = %.4f gmres its = %d\n", k, rk, alpha, its);
+    if (opt->verbosity > 0)
+      std::printf("lm %d: |r| = %.6e alpha = %.4f gmres its = %d relres = %.3e\n", k, rk, alpha, its, rr);
     if (!std::isfinite(rk)) { cleanup(); return merr(c, ICX_ERR_NONFINITE, "non-finite residual"); }
     converged = rk <= tau;
   }

@@ -270,6 +270,7 @@ typedef struct icx_lm_report {
   int linear_iterations_total;
   double residual_history[64];
   double alpha_history[64];
+  double linear_relres_max;  /* the largest relative residual a subproblem solve ended with */
 } icx_lm_report;
 
 icx_status icx_lm_default_options(icx_lm_options* opt);

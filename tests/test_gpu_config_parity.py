@@ -11,7 +11,9 @@ against the C oracle on the same mesh nodes and states.
     the finite-difference accuracy of two independent Jacobians.
   * viscous Burgers 32 x 32, p = 2: the whole Newton solve (Wolfe line
     search) against the oracle Newton (sparse direct solves): residual
-    histories while |r| >> roundoff, converged state to 1e-10 (relative L2).
+    histories while |r| >> roundoff, converged state to 1e-10 of the initial
+    state's L2 norm (the steady state of this problem is u = 0, so a norm
+    relative to the converged state would compare roundoff with roundoff).
 
 The inputs are built on each side independently: the oracle side takes mesh
 nodes, basis-node coordinates and boundary/source callbacks from the oracle
@@ -78,17 +80,21 @@ def test_ns_128x128_p3_roe_residual_full_size():
 
 def test_ns_256x256_p2_residual_full_size():
     """the learned-preconditioner workload's mesh and order (256 x 256, p = 2,
-    2,359,296 unknowns) at Re = 300"""
+    2,359,296 unknowns) at Re = 300, at the workload's state with a seeded 1 %
+    multiplicative perturbation: the manufactured state itself is nearly a
+    root (its residual is ~1e-2 of the flux terms, so 1e-12 of it would be
+    below the roundoff of the terms)"""
     from iceicle_b200.workloads import ns_mms_config
     spec = Spec(pde=NS, nx=256, ny=256, p=2, g=2, ip=True, source=True, perturb=0.05, seed=4321, ns_mu=1.0 / 300)
     wl = ns_mms_config(nx=256, ny=256, p=2, geo_order=2, mu=1.0 / 300)
     c = spec.coords()
     assert np.array_equal(c, wl.coords)
-    du = torch.from_numpy(wl.u0).cuda()
+    u = wl.u0 * (1.0 + 0.01 * np.random.default_rng(17).standard_normal(wl.u0.size))
+    du = torch.from_numpy(u).cuda()
     dr = torch.full_like(du, float("nan"))
     wl.ctx.form_residual(du, dr)
     torch.cuda.synchronize()
-    ref = ob.residual(ob.oracle(), spec.oracle_problem(), c, wl.u0)
+    ref = ob.residual(ob.oracle(), spec.oracle_problem(), c, u)
     assert np.abs(dr.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
@@ -179,4 +185,5 @@ def test_burgers_32x32_p2_newton_matches_oracle_newton():
         if b > 1e-6:
             assert abs(a - b) <= 1e-5 * b, (hist, hist_or)
     u = du.cpu().numpy()
-    assert np.linalg.norm(u - u_or) <= 1e-10 * np.linalg.norm(u_or), np.linalg.norm(u - u_or) / np.linalg.norm(u_or)
+    scale = max(np.linalg.norm(u_or), np.linalg.norm(u0))
+    assert np.linalg.norm(u - u_or) <= 1e-10 * scale, np.linalg.norm(u - u_or) / scale

@@ -7,7 +7,8 @@
 * A tile at least as large as the grid is plain ILU(0): bit-identical to the
   untiled apply.
 * The preconditioner changes GMRES iterations only: Newton with tiled ILU
-  reaches the untiled converged state to 1e-10 (relative L2).
+  reaches the untiled converged state to 1e-10 of the initial state's L2
+  norm (the steady state of this Burgers problem is u = 0).
 """
 import numpy as np
 import pytest
@@ -127,8 +128,9 @@ def test_newton_with_tiled_ilu_reaches_same_state(tile):
             assert rep.converged
             out[(t, prec)] = (u.cpu().numpy(), rep.linear_iterations_total)
     base = out[(0, 0)][0]
+    scale = max(np.linalg.norm(base), np.linalg.norm(wl.u0))
     for key, (u, _) in out.items():
-        assert np.linalg.norm(u - base) <= 1e-10 * np.linalg.norm(base), key
+        assert np.linalg.norm(u - base) <= 1e-10 * scale, key
 
 
 def test_element_groups_and_separate_factor_apply():

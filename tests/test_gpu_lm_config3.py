@@ -34,6 +34,33 @@ def _jitter(coord, n, frac, seed):
     return np.ascontiguousarray(out)
 
 
+@pytest.mark.parametrize("n,p", [(10, 1), (8, 2)])
+def test_small_lm_explicit_matches_oracle(n, p):
+    """the same configuration on small meshes, where the subproblem is well
+    enough conditioned for GMRES to reach 1e-12: three LM iterations against
+    the oracle at 1e-6 (two independent FD Jacobians)"""
+    import iceicle_b200 as ib
+    from iceicle_b200.workloads import mdg_ice_config
+    wl, traces, x0 = mdg_ice_config(n=n, p=p)
+    spec = Spec(nx=n, ny=n, g=1, p=p, mu=0.0, a=(0.0, 1.0), b=(1.0, 0.0), bct=(3, 3, 3, 4),
+                dirichlet=[("oblique_step", [0.4, 0.2, 1.0, -0.5])], perturb=0.0)
+    pb = spec.oracle_problem()
+    c = _jitter(spec.coords(), n, 0.2, 99)
+    assert np.array_equal(c, wl.coords)
+    u_or, x_or, hist_or, _ = on.lm_explicit(pb, c, traces, wl.u0, x0, kmax=3)
+    o = ib.default_lm_options()
+    o.kmax, o.explicit_subproblem, o.gmres_rtol, o.gmres_max_it, o.gmres_restart = 3, 1, 1e-12, 20000, 60
+    du = torch.from_numpy(wl.u0.copy()).cuda()
+    x = x0.copy()
+    rep = ib.lm_solve(wl.ctx, du, x, o)
+    hist = list(rep.residual_history[:rep.iterations + 1])
+    assert rep.linear_relres_max <= 1e-12, rep.linear_relres_max
+    assert rep.iterations == len(hist_or) - 1, (hist, hist_or)
+    for a, b in zip(hist, hist_or):
+        assert abs(a - b) <= 1e-6 * b, (hist, hist_or)
+    assert np.linalg.norm(x - x_or) <= 1e-6 * np.linalg.norm(x_or)
+
+
 @pytest.mark.parametrize("p", [1, 2])
 def test_config3_lm_explicit_matches_oracle(p):
     import iceicle_b200 as ib

@@ -7,8 +7,9 @@ equals the same part solved alone (icx_newton_solve).
   advection-diffusion parts of orders 1-4 and nonlinear viscous Burgers parts:
   every part converges, with the Newton iteration count of its own solve, its
   GMRES iteration total within 2 of it (per-part reductions are summed in
-  another order than the single solve's), and its state within 1e-10
-  (relative L2) of its own solve's;
+  another order than the single solve's), and its state within 1e-10 of its
+  own solve's (relative to the larger L2 norm of that state and the initial
+  state: the Burgers parts' steady state is u = 0);
 * the same set in mixed precision reaches the FP64 states within 1e-10;
 * the Arnoldi steps of the set are replayed from CUDA graphs.
 """
@@ -82,7 +83,8 @@ def test_set_newton_equals_solving_each_part_alone(problem_set):
         assert reps[k].iterations == rk.iterations, (k, reps[k].iterations, rk.iterations)
         assert abs(reps[k].linear_iterations_total - rk.linear_iterations_total) <= 2, k
         ref = uk.cpu().numpy()
-        assert np.linalg.norm(ps.part(u, k) - ref) <= 1e-10 * np.linalg.norm(ref), k
+        scale = max(np.linalg.norm(ref), np.linalg.norm(u0[k]))
+        assert np.linalg.norm(ps.part(u, k) - ref) <= 1e-10 * scale, k
 
 
 def test_set_mixed_precision_reaches_fp64_states(problem_set):
@@ -92,4 +94,4 @@ def test_set_mixed_precision_reaches_fp64_states(problem_set):
     for k in range(len(parts)):
         assert reps[k].converged
         a, b = ps.part(u64, k), ps.part(u32, k)
-        assert np.linalg.norm(a - b) <= 1e-10 * np.linalg.norm(a), k
+        assert np.linalg.norm(a - b) <= 1e-10 * max(np.linalg.norm(a), np.linalg.norm(u0[k])), k
