@@ -57,6 +57,9 @@ void integration_call_sites(icx_ctx* ctx_past, icx_ctx** parts, int n_parts, dou
   long long n_dof = 0;
   double rr = 0.0, tfinal = 1.0, mu = 0.01, T0 = 0.004, T1 = 0.005, rho_inf = 1.0, u_inf = 0.5, T_inf = 0.004;
   double* d_y = d_x;
+  float* d_vals32 = nullptr;
+  double* d_u_set = d_u_all;
+  double mu_ratio = 0.02, T0_ratio = 0.004, Ts_ratio = 0.0015;
   std::vector<int> groups_v(64, 0);
   const int* groups = groups_v.data();
   Coeffs coeffs{0.01, {0.0, 0.0}, {1.0, 0.5}}, c = coeffs;
