@@ -227,15 +227,17 @@ __global__ void __launch_bounds__(256) ilu_scale_upper_kernel(int E, const int* 
 }
 
 // ------------------------------------------------------------- reductions
-// partial[j * nblocks + b] = sum over block b's rows of V_j . w (V_j = V + j*ld)
-__global__ void mdot_partial_kernel(long long n, const double* __restrict__ V, long long ld, int nvec,
+// partial[j * nblocks + b] = sum over block b's rows of V_j . w (V_j = V + j*ld;
+// an FP32 basis is widened to FP64 before the product)
+template <class TV>
+__global__ void mdot_partial_kernel(long long n, const TV* __restrict__ V, long long ld, int nvec,
                                     const double* __restrict__ w, double* __restrict__ partial) {
   __shared__ double red[256];
   int j = blockIdx.y;
-  const double* v = V + (size_t)j * ld;
+  const TV* v = V + (size_t)j * ld;
   double s = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    s += v[i] * w[i];
+    s += (double)v[i] * w[i];
   red[threadIdx.x] = s;
   __syncthreads();
   for (int off = blockDim.x / 2; off > 0; off >>= 1) {
@@ -260,13 +262,29 @@ __global__ void mdot_final_kernel(int nblocks, int nvec, const double* __restric
 }
 
 // w += sign * sum_j h[j] V_j
-__global__ void maxpy_kernel(long long n, const double* __restrict__ V, long long ld, int nvec,
+template <class TV>
+__global__ void maxpy_kernel(long long n, const TV* __restrict__ V, long long ld, int nvec,
                              const double* __restrict__ h, double sign, double* __restrict__ w) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int j = 0; j < nvec; ++j) s += h[j] * V[(size_t)j * ld + i];
+    for (int j = 0; j < nvec; ++j) s += h[j] * (double)V[(size_t)j * ld + i];
     w[i] += sign * s;
   }
+}
+
+// v32 = a x rounded to FP32
+__global__ void scale_to_f32_kernel(long long n, double a, const double* __restrict__ x, float* __restrict__ v32) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v32[i] = (float)(a * x[i]);
+}
+
+// v32 = w / sqrt(*h2) rounded to FP32 (w itself when *h2 is not positive)
+__global__ void normalize_to_f32_kernel(long long n, const double* __restrict__ h2, const double* __restrict__ w,
+                                        float* __restrict__ v32) {
+  const double h = *h2;
+  const double a = h > 0.0 ? 1.0 / sqrt(h) : 1.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v32[i] = (float)(a * w[i]);
 }
 
 // y = a x + b y
@@ -304,14 +322,29 @@ cudaError_t la_mdot(LinalgWork& w, long long n, const double* V, long long ld, i
                     double* d_out, cudaStream_t s) {
   int nb = 148 * 2;
   dim3 grid(nb, nvec);
-  mdot_partial_kernel<<<grid, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
+  mdot_partial_kernel<double><<<grid, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
+  mdot_final_kernel<<<nvec, 256, 0, s>>>(nb, nvec, w.partial, d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t la_mdot32(LinalgWork& w, long long n, const float* V, long long ld, int nvec, const double* x,
+                      double* d_out, cudaStream_t s) {
+  int nb = 148 * 2;
+  dim3 grid(nb, nvec);
+  mdot_partial_kernel<float><<<grid, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
   mdot_final_kernel<<<nvec, 256, 0, s>>>(nb, nvec, w.partial, d_out);
   return cudaGetLastError();
 }
 
 cudaError_t la_maxpy(long long n, const double* V, long long ld, int nvec, const double* d_h, double sign, double* w,
                      cudaStream_t s) {
-  maxpy_kernel<<<grid_for(n), 256, 0, s>>>(n, V, ld, nvec, d_h, sign, w);
+  maxpy_kernel<double><<<grid_for(n), 256, 0, s>>>(n, V, ld, nvec, d_h, sign, w);
+  return cudaGetLastError();
+}
+
+cudaError_t la_maxpy32(long long n, const float* V, long long ld, int nvec, const double* d_h, double sign, double* w,
+                       cudaStream_t s) {
+  maxpy_kernel<float><<<grid_for(n), 256, 0, s>>>(n, V, ld, nvec, d_h, sign, w);
   return cudaGetLastError();
 }
 
@@ -690,7 +723,8 @@ static bool arnoldi_graphs_ready(ArnoldiGraphs& g, unsigned long long key, int m
 // the current key (the first run has done every one-time setup of the
 // kernels it launches), then replayed. Null: run the step eagerly.
 template <class Step>
-static cudaGraphExec_t arnoldi_graph(ArnoldiGraphs& g, int j, long long n, double* vj1, const double* h2, Step& step) {
+static cudaGraphExec_t arnoldi_graph(ArnoldiGraphs& g, int j, long long n, double* vj1, const double* h2, Step& step,
+                                     bool append_normalize) {
   if (g.failed) return nullptr;
   if (g.exec[j]) return g.exec[j];
   if (g.seen[j]++ < 1) return nullptr;
@@ -698,7 +732,7 @@ static cudaGraphExec_t arnoldi_graph(ArnoldiGraphs& g, int j, long long n, doubl
   cudaError_t e = cudaStreamBeginCapture(g.cap, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     cudaError_t es = step(g.cap, g.hp);
-    if (es == cudaSuccess) {
+    if (es == cudaSuccess && append_normalize) {
       normalize_kernel<<<grid_for(n), 256, 0, g.cap>>>(n, h2, vj1);
       es = cudaGetLastError();
     }
@@ -743,38 +777,59 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
   double beta = bnorm;
   int total = 0;
   std::vector<double> cycle_beta{bnorm};
+  // FP32 basis: v_j is widened into vt for the operators, w = A M^-1 v_j is
+  // formed in kb.w (FP64) and stored rounded into the basis once normalised
+  const bool f32 = kb.V32 != nullptr && kb.vt != nullptr;
   while (true) {
-    GCK(la_axpby(n, 1.0 / beta, kb.r, 0.0, kb.V, s));
+    if (f32) {
+      scale_to_f32_kernel<<<grid_for(n), 256, 0, s>>>(n, 1.0 / beta, kb.r, kb.V32);
+      GCK(cudaGetLastError());
+    } else {
+      GCK(la_axpby(n, 1.0 / beta, kb.r, 0.0, kb.V, s));
+    }
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = beta;
     int j = 0;
     double resid = beta;
     for (; j < m && total < maxit; ++j) {
-      double* vj = kb.V + (size_t)j * n;
-      double* vj1 = kb.V + (size_t)(j + 1) * n;
+      double* vj = f32 ? kb.vt : kb.V + (size_t)j * n;
+      double* vj1 = f32 ? kb.w : kb.V + (size_t)(j + 1) * n;
+      const float* vj32 = f32 ? kb.V32 + (size_t)j * n : nullptr;
+      float* vj1_32 = f32 ? kb.V32 + (size_t)(j + 1) * n : nullptr;
       if (kb.samples && kb.sample_every > 0 && kb.sample_count < kb.sample_cap && j > 0 &&
-          total % kb.sample_every == 0)
-        GCK(cudaMemcpyAsync(kb.samples + (size_t)kb.sample_count++ * n, vj, sizeof(double) * n,
-                            cudaMemcpyDeviceToDevice, s));
+          total % kb.sample_every == 0) {
+        double* dst = kb.samples + (size_t)kb.sample_count++ * n;
+        if (f32) GCK(la_f2d(n, vj32, dst, s));
+        else GCK(cudaMemcpyAsync(dst, vj, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      }
       // the step: preconditioner and operator, classical Gram-Schmidt twice
       // and the norm of the result; the three reductions land in separate
       // device slots [pass 1 | pass 2 | |v|^2] and come back in one copy
       auto step = [&](cudaStream_t st, double* host_dst) -> cudaError_t {
-        cudaError_t e = M ? (*M)(vj, kb.z, st) : cudaSuccess;
+        cudaError_t e = f32 ? la_f2d(n, vj32, vj, st) : cudaSuccess;
+        if (e == cudaSuccess && M) e = (*M)(vj, kb.z, st);
         if (e == cudaSuccess) e = A(M ? kb.z : vj, vj1, st);
         for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
           double* slot = kb.dh + (size_t)pass * (m + 2);
-          e = la_mdot(*kb.lw, n, kb.V, n, j + 1, vj1, slot, st);
-          if (e == cudaSuccess) e = la_maxpy(n, kb.V, n, j + 1, slot, -1.0, vj1, st);
+          e = f32 ? la_mdot32(*kb.lw, n, kb.V32, n, j + 1, vj1, slot, st)
+                  : la_mdot(*kb.lw, n, kb.V, n, j + 1, vj1, slot, st);
+          if (e == cudaSuccess)
+            e = f32 ? la_maxpy32(n, kb.V32, n, j + 1, slot, -1.0, vj1, st)
+                    : la_maxpy(n, kb.V, n, j + 1, slot, -1.0, vj1, st);
         }
         if (e == cudaSuccess) e = la_mdot(*kb.lw, n, vj1, 0, 1, vj1, kb.dh + 2 * (m + 2), st);
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(host_dst, kb.dh, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && f32) {
+          normalize_to_f32_kernel<<<grid_for(n), 256, 0, st>>>(n, kb.dh + 2 * (m + 2), vj1, vj1_32);
+          e = cudaGetLastError();
+        }
         return e;
       };
       // replayed from a CUDA graph (which also normalises v_j+1 on the
       // device), or launched one by one
-      cudaGraphExec_t gx = use_graphs ? arnoldi_graph(*kb.graphs, j, n, vj1, kb.dh + 2 * (m + 2), step) : nullptr;
+      cudaGraphExec_t gx =
+          use_graphs ? arnoldi_graph(*kb.graphs, j, n, vj1, kb.dh + 2 * (m + 2), step, !f32) : nullptr;
       if (gx) {
         GCK(cudaGraphLaunch(gx, s));
         GCK(cudaStreamSynchronize(s));
@@ -792,7 +847,7 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
         if (err) *err = "non-finite Krylov vector";
         return ICX_ERR_NONFINITE;
       }
-      if (!gx && hn > 0.0) GCK(la_axpby(n, 1.0 / hn, vj1, 0.0, vj1, s));
+      if (!gx && !f32 && hn > 0.0) GCK(la_axpby(n, 1.0 / hn, vj1, 0.0, vj1, s));
       for (int i = 0; i < j; ++i) {
         double t = cs[i] * hcol[i] + sn[i] * hcol[i + 1];
         hcol[i + 1] = -sn[i] * hcol[i] + cs[i] * hcol[i + 1];
@@ -817,7 +872,8 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
     }
     GCK(cudaMemcpyAsync(kb.dh, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, s));
     GCK(cudaMemsetAsync(kb.w, 0, sizeof(double) * n, s));
-    GCK(la_maxpy(n, kb.V, n, j, kb.dh, 1.0, kb.w, s));
+    if (f32) GCK(la_maxpy32(n, kb.V32, n, j, kb.dh, 1.0, kb.w, s));
+    else GCK(la_maxpy(n, kb.V, n, j, kb.dh, 1.0, kb.w, s));
     if (M) {
       GCK((*M)(kb.w, kb.z, s));
       GCK(la_axpby(n, 1.0, kb.z, 1.0, x, s));

@@ -18,6 +18,11 @@ cudaError_t la_mdot(LinalgWork& w, long long n, const double* V, long long ld, i
 // w += sign * sum_j d_h[j] V_j
 cudaError_t la_maxpy(long long n, const double* V, long long ld, int nvec, const double* d_h, double sign, double* w,
                      cudaStream_t s);
+// the same two with an FP32 basis V (products and sums in FP64)
+cudaError_t la_mdot32(LinalgWork& w, long long n, const float* V, long long ld, int nvec, const double* x,
+                      double* d_out, cudaStream_t s);
+cudaError_t la_maxpy32(long long n, const float* V, long long ld, int nvec, const double* d_h, double sign, double* w,
+                       cudaStream_t s);
 cudaError_t la_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);
 cudaError_t la_xpay(long long n, const double* x, double a, const double* y, double* z, cudaStream_t s);
 // dst[b] = inv(src[blk_index[b]]) for b < nblk (bs x bs blocks); *flag set on a singular block
@@ -101,6 +106,11 @@ struct KrylovBuffers {
   double* r = nullptr;
   double* dh = nullptr;  // >= 3 (m + 2) device doubles
   LinalgWork* lw = nullptr;
+  // optional FP32 basis (mixed precision): (m + 1) x n floats in place of V,
+  // with the inner products and updates accumulated in FP64; vt is one FP64
+  // vector, the operator's input widened from the basis
+  float* V32 = nullptr;
+  double* vt = nullptr;
   // optional Krylov samples: the true residual at every restart and every
   // `sample_every`-th Arnoldi vector, copied into samples[count] while count < cap
   double* samples = nullptr;

@@ -61,6 +61,8 @@ struct icx_solver_work {
   float* vals32 = nullptr;  // mixed precision: FP32 copies of the Jacobian and the preconditioner
   float* pc32 = nullptr;
   float* uinv32 = nullptr;
+  float* V32 = nullptr;     // mixed precision: the Krylov basis in FP32, (m + 1) x n
+  double* vt = nullptr;     // the basis vector widened for the operators
   int* order = nullptr;     // elements by ascending level (ILU schedule)
   std::vector<int> lvl_off; // level l: order[lvl_off[l] .. lvl_off[l+1])
   unsigned* cnt = nullptr;  // 2 x E completion counters of the ILU apply
@@ -281,6 +283,8 @@ icx_status ensure_mixed(icx_ctx* c) {
   CK(cudaMalloc((void**)&w->vals32, sizeof(float) * nv));
   CK(cudaMalloc((void**)&w->pc32, sizeof(float) * nv));
   CK(cudaMalloc((void**)&w->uinv32, sizeof(float) * (size_t)c->dm.E * w->bs * w->bs));
+  CK(cudaMalloc((void**)&w->V32, sizeof(float) * (size_t)(w->m + 1) * w->n));
+  CK(cudaMalloc((void**)&w->vt, sizeof(double) * w->n));
   return ICX_OK;
 }
 
@@ -443,6 +447,11 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
   kb.samples = samples;
   kb.sample_cap = sample_cap;
   kb.sample_every = sample_every;
+  if (mixed && w->V32 && m <= w->m) {
+    // the Krylov basis in FP32 (inner products and updates in FP64)
+    kb.V32 = w->V32;
+    kb.vt = w->vt;
+  }
   // the parallel and learned preconditioners give up on a stalled solve
   // (block-ILU(0) then takes the step)
   kb.stall_cycles = pc >= 3 ? 10 : 0;
@@ -570,7 +579,7 @@ namespace icx {
 void free_solver_work(icx_ctx* c) {
   if (!c || !c->sw) return;
   icx_solver_work* w = c->sw;
-  void* ptrs[] = {w->vals32, w->pc32, w->uinv32, w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du,
+  void* ptrs[] = {w->V32, w->vt, w->vals32, w->pc32, w->uinv32, w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du,
                   w->ustep, w->rwork, w->pct, w->pct2, w->pct3, w->pct4, w->order, w->cnt, w->cnt_rows, w->pc_err,
                   w->dh, w->flag, w->lw.partial};
   w->graphs.release();

@@ -295,9 +295,11 @@ typedef struct icx_newton_options {
   int verbosity;
   /* 0: all FP64. 1: mixed - the linear solves read FP32 copies of the
    * Jacobian (SpMV) and of the preconditioner (block inverses / ILU factors,
-   * formed in FP64 then rounded) with FP32 accumulation; the Krylov vectors,
-   * Hessenberg and Givens rotations, the Newton residual, its norm and the
-   * line search stay FP64, so the converged state is judged in FP64.
+   * formed in FP64 then rounded) with FP32 accumulation, and keep the GMRES
+   * Krylov basis in FP32 (its inner products and updates accumulate in
+   * FP64); the Hessenberg and Givens rotations, the solution update, the
+   * Newton residual, its norm and the line search stay FP64, so the converged
+   * state is judged in FP64.
    * 2: as 1, with the Jacobian's flux quadrature itself in FP32
    * (icx_form_jacobian_fd_f32); the preconditioner is factored in FP64 from
    * those FP32 values. Newton is then FP64 iterative refinement around FP32
