@@ -59,6 +59,11 @@ def parse():
     ap.add_argument("--batched", type=int, default=512, metavar="N",
                     help="secondary timing of N seeded uneven advection-diffusion problems, batched vs one at a "
                          "time (0: skip; the full problem set is 512)")
+    ap.add_argument("--batched-sample", type=int, default=24, metavar="K",
+                    help="problems of the set also solved one at a time for the batched ratio")
+    ap.add_argument("--learned-seeds", type=int, default=1, metavar="K",
+                    help="fresh instances of the learned-preconditioner comparison (256 x 256 Navier-Stokes)")
+    ap.add_argument("--no-lm", action="store_true", help="skip the MDG-ICE (64 x 64) LM timing")
     ap.add_argument("--no-tune", action="store_true",
                     help="time the compiled default launch shapes instead of the autotuned ones")
     ap.add_argument("--tile", default="", metavar="K=V,...",
@@ -807,16 +812,24 @@ def run_ours(a):
                                         "sample": "3 full 128x128 p3 residuals, 1 thread (reference is serial)"}
             else:
                 line["cpu_baseline"] = None
+        wall = {}
+
+        def section(name, fn):
+            t0 = time.time()
+            line[name] = fn()
+            wall[name] = round(time.time() - t0, 1)
         if ws == 1:
-            line["residual_roe"] = roe_residual_bench(torch, dev, flush, tune is not None)
-            line["jacobian"] = jacobian_bench(torch, dev, wl, hbm, not a.no_cpu_baseline)
+            section("residual_roe", lambda: roe_residual_bench(torch, dev, flush, tune is not None))
+            section("jacobian", lambda: jacobian_bench(torch, dev, wl, hbm, not a.no_cpu_baseline))
         if not a.no_newton and ws == 1:
-            line["newton"] = newton_bench(torch, dev, not a.no_tune)
-            line["mdg_ice"] = lm_bench(torch, dev)
+            section("newton", lambda: newton_bench(torch, dev, not a.no_tune))
+            if not a.no_lm:
+                section("mdg_ice", lambda: lm_bench(torch, dev))
         if a.batched and ws == 1:
-            line["batched"] = batched_bench(torch, dev, a.batched)
+            section("batched", lambda: batched_bench(torch, dev, a.batched, a.batched_sample))
         if not a.no_learned and ws == 1:
-            line["learned_pc"] = learned_bench(torch, dev, not a.no_tune)
+            section("learned_pc", lambda: learned_bench(torch, dev, not a.no_tune, a.learned_seeds))
+        line["section_wall_s"] = wall
         print(json.dumps(line))
     if ws > 1:
         dist.destroy_process_group()
