@@ -64,6 +64,12 @@ def parse():
     ap.add_argument("--learned-seeds", type=int, default=1, metavar="K",
                     help="fresh instances of the learned-preconditioner comparison (256 x 256 Navier-Stokes)")
     ap.add_argument("--no-lm", action="store_true", help="skip the MDG-ICE (64 x 64) LM timing")
+    ap.add_argument("--gemm", default="", metavar="M,N,K",
+                    help="only time the tcgen05 BF16 GEMM out = A B^T (A [M, K], B [N, K], FP32 out) and print "
+                         "one JSON line")
+    ap.add_argument("--jacobian", type=int, default=0, metavar="N",
+                    help="only time the FD Jacobian (FP64 and FP32 flux quadrature) of the N x N p = 3 "
+                         "Navier-Stokes manufactured solution and print one JSON line")
     ap.add_argument("--no-tune", action="store_true",
                     help="time the compiled default launch shapes instead of the autotuned ones")
     ap.add_argument("--tile", default="", metavar="K=V,...",
@@ -835,8 +841,77 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+def gemm_mode(spec):
+    """tcgen05 BF16 GEMM alone: 20 launches after 3 untimed, CUDA events,
+    2 M N K flops per launch against the measured dense BF16 peak"""
+    import torch
+    import iceicle_b200 as ib
+    M, N, K = (int(v) for v in spec.split(","))
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    C32 = torch.empty(M, N, device="cuda", dtype=torch.float32)
+    for _ in range(3):
+        ib.gemm_bf16_nt(A, B, out32=C32)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(20):
+        ib.gemm_bf16_nt(A, B, out32=C32)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 20
+    ref = (A.float() @ B.float().T)
+    err = float((C32 - ref).abs().max() / ref.abs().max())
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("bf16_tflops", 1590.0)
+    tf = 2.0 * M * N * K / (ms * 1e-3) / 1e12
+    print(json.dumps({"mode": "gemm_bf16_nt", "M": M, "N": N, "K": K, "ms": ms, "tflops": tf, "peak_tflops": peak,
+                      "frac": tf / peak, "max_rel_err_vs_fp32_of_bf16_inputs": err}))
+
+
+def jacobian_mode(n):
+    """the FD Jacobian alone on the n x n p = 3 Navier-Stokes workload: FP64
+    and FP32 flux quadrature, mean of 5 launches after 2 untimed (CUDA events)"""
+    import torch
+    from iceicle_b200.workloads import ns_mms_config
+    wl = ns_mms_config(nx=n, ny=n, p=3, geo_order=2)
+    L = wl.ctx.layout
+    bs = L.block_size
+    u = torch.from_numpy(wl.u0).cuda()
+    res = torch.empty_like(u)
+    out = {"mode": "jacobian_fd", "mesh": f"{n}x{n}", "p": 3, "n_dof": L.n_dof}
+    for name, dt, fn in (("fp64", torch.float64, wl.ctx.form_jacobian_fd),
+                         ("fp32_quadrature", torch.float32, wl.ctx.form_jacobian_fd_f32)):
+        vals = torch.empty(L.nnz_blocks * bs * bs, dtype=dt, device="cuda")
+        for _ in range(2):
+            fn(u, res, vals)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(5):
+            fn(u, res, vals)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        written = vals.numel() * vals.element_size()
+        out[name] = {"ms_with_residual": ms, "bsr_bytes": written, "gbs_written": written / (ms * 1e-3) / 1e9}
+        del vals
+    print(json.dumps(out))
+
+
 def main():
     a = parse()
+    if a.gemm:
+        gemm_mode(a.gemm)
+        return
+    if a.jacobian:
+        jacobian_mode(a.jacobian)
+        return
     if a.spmv:
         spmv_bench(a.spmv)
     elif a.ilu:
