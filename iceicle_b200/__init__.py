@@ -729,8 +729,9 @@ class ProblemSet:
     """icx_pset: independent problems of uneven mesh size and basis order
     (set-up Contexts, kept alive by the set), each solved by its own Newton
     iteration with every kernel launched once per basis order for all parts.
-    `offsets[k]` is part k's first unknown in the set's vectors, `offsets[-1]`
-    the total."""
+    `offsets[k]` is part k's first unknown in the set's vectors (the parts
+    are stored by basis order), `lengths[k]` its unknowns, `offsets[-1]` the
+    total."""
 
     def __init__(self, parts, device=0):
         self._h = C.c_void_p()
@@ -742,6 +743,7 @@ class ProblemSet:
         off = (C.c_longlong * (len(parts) + 1))()
         self._check(lib().icx_pset_offsets(self._h, off), "pset_offsets")
         self.offsets = list(off)
+        self.lengths = [p.layout.n_dof for p in parts]
         self.n_parts = len(parts)
 
     def _check(self, st, what):
@@ -763,11 +765,11 @@ class ProblemSet:
         """one host vector in the set's layout from the parts' vectors"""
         out = np.zeros(self.offsets[-1])
         for k, v in enumerate(vectors):
-            out[self.offsets[k]:self.offsets[k + 1]] = v
+            out[self.offsets[k]:self.offsets[k] + self.lengths[k]] = v
         return out
 
     def part(self, x, k):
-        return x[self.offsets[k]:self.offsets[k + 1]]
+        return x[self.offsets[k]:self.offsets[k] + self.lengths[k]]
 
     def residual(self, u, res):
         self._check(lib().icx_pset_residual(self._h, _ptr(u), _ptr(res)), "pset_residual")

@@ -94,6 +94,12 @@ struct icx_mdg_state {
   int* d_lo_rows = nullptr;
   int* d_up_rows = nullptr;
   int* d_pc_err = nullptr;
+  // data-flow triangular solves of the subproblem's ILU(0): per-row flags,
+  // the two row counters of one apply, the wait-timeout flag, the last epoch
+  unsigned* d_tri_ready = nullptr;
+  unsigned* d_tri_next = nullptr;
+  int* d_tri_err = nullptr;
+  unsigned tri_epoch = 0;
   // Laplacian and element-wise regularisation: per element the pairs
   // (local node i, local node j, position in A) of free coordinates of two
   // selected nodes, and per touched position the pairs that add to it
@@ -609,7 +615,8 @@ void free_mdg(icx_ctx* c) {
                   m->d_rwork, m->d_x, m->d_kV, m->d_kw, m->d_kz, m->d_kr, m->d_kdh, m->lw.partial,
                   m->d_a_rowptr, m->d_a_colidx, m->d_a_diag, m->d_a_vals, m->d_a_lu, m->d_lo_rows, m->d_up_rows,
                   m->d_pc_err, m->d_pair_ptr, m->d_pair_ij, m->d_upos, m->d_upos_ptr, m->d_upos_list,
-                  m->d_pair_val, m->d_lam_el, m->d_cg_tab, m->d_detmin, m->d_colnorm2};
+                  m->d_pair_val, m->d_lam_el, m->d_cg_tab, m->d_detmin, m->d_colnorm2, m->d_tri_ready,
+                  m->d_tri_next, m->d_tri_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete m;
@@ -1195,6 +1202,52 @@ __global__ void csr_tri_level_kernel(int nrows, const int* __restrict__ rows, co
   if (lane == 0) y[i] = upper ? (b[i] - s) / lu[d] : b[i] - s;
 }
 
+// the same solves in one launch each, scheduled by data flow: warps claim
+// rows in solve order (ascending for the forward solve, descending for the
+// backward one) from a counter, wait for the rows their entries refer to
+// (which were claimed earlier, by warps that are running, so every wait
+// ends), and publish each result with a per-row flag set to this solve's
+// epoch. A wait gives up after ~2^22 polls (or at once when an earlier wait
+// has given up), sets *err and goes on, so the launch always ends.
+__global__ void csr_tri_flow_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                    const int* __restrict__ diag, const double* __restrict__ lu,
+                                    const double* __restrict__ b, double* y, int upper, unsigned* ready,
+                                    unsigned epoch, unsigned* next, int* err) {
+  const int lane = threadIdx.x & 31;
+  volatile unsigned* vr = ready;
+  volatile double* vy = y;
+  while (true) {
+    unsigned t = 0;
+    if (lane == 0) t = atomicAdd(next, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= (unsigned)n) break;
+    const int i = upper ? n - 1 - (int)t : (int)t;
+    const int d = diag[i];
+    const int q0 = upper ? d + 1 : rowptr[i], q1 = upper ? rowptr[i + 1] : d;
+    double s = 0.0;
+    for (int q = q0 + lane; q < q1; q += 32) {
+      const int k = colidx[q];
+      unsigned spins = 0;
+      while (vr[k] != epoch) {
+        if (++spins > (1u << 22) || *(volatile int*)err) {
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+      s += lu[q] * vy[k];
+    }
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) {
+      vy[i] = upper ? (b[i] - s) / lu[d] : b[i] - s;
+      __threadfence();
+      vr[i] = epoch;
+    }
+    __syncwarp();
+  }
+}
+
 }  // namespace icx
 
 namespace {
@@ -1376,6 +1429,13 @@ icx_status build_lm_explicit(icx_ctx* c) {
     MCK(cudaMalloc((void**)b, sizeof(double) * dm.E));
   }
   if (!m.d_pc_err) MCK(cudaMalloc((void**)&m.d_pc_err, sizeof(int)));
+  if (m.d_tri_ready) cudaFree(m.d_tri_ready);
+  MCK(cudaMalloc((void**)&m.d_tri_ready, sizeof(unsigned) * std::max(n, 1LL)));
+  MCK(cudaMemset(m.d_tri_ready, 0, sizeof(unsigned) * std::max(n, 1LL)));
+  m.tri_epoch = 0;
+  if (!m.d_tri_next) MCK(cudaMalloc((void**)&m.d_tri_next, 2 * sizeof(unsigned)));
+  if (!m.d_tri_err) MCK(cudaMalloc((void**)&m.d_tri_err, sizeof(int)));
+  MCK(cudaMemset(m.d_tri_err, 0, sizeof(int)));
   m.a_built = true;
   return ICX_OK;
 }
@@ -1506,19 +1566,19 @@ icx_status icx_lm_solve(icx_ctx* c, double* d_u, double* x, const icx_lm_options
         icx::csr_spmv_kernel<<<nb_n, 256, 0, st>>>(n, s.d_a_rowptr, s.d_a_colidx, s.d_a_vals, xin, yout);
         return cudaGetLastError();
       };
+      // the two triangular solves, one data-flow launch each (the level
+      // schedule would take one launch per level, ~2 x 760 at 64 x 64)
       M = [&](const double* xin, double* yout, cudaStream_t st) {
-        for (size_t l = 0; l + 1 < s.lo_off.size(); ++l) {
-          const int cnt = s.lo_off[l + 1] - s.lo_off[l];
-          icx::csr_tri_level_kernel<<<(cnt * 32 + 255) / 256, 256, 0, st>>>(
-              cnt, s.d_lo_rows + s.lo_off[l], s.d_a_rowptr, s.d_a_colidx, s.d_a_diag, s.d_a_lu, xin, s.d_colnorm2,
-              0);
-        }
-        for (size_t l = 0; l + 1 < s.up_off.size(); ++l) {
-          const int cnt = s.up_off[l + 1] - s.up_off[l];
-          icx::csr_tri_level_kernel<<<(cnt * 32 + 255) / 256, 256, 0, st>>>(
-              cnt, s.d_up_rows + s.up_off[l], s.d_a_rowptr, s.d_a_colidx, s.d_a_diag, s.d_a_lu, s.d_colnorm2, yout,
-              1);
-        }
+        const unsigned e_l = ++s.tri_epoch, e_u = ++s.tri_epoch;
+        const int nn = (int)n;
+        const unsigned grid = (unsigned)std::min<long long>((n + 7) / 8, 148LL * 8);
+        cudaError_t e = cudaMemsetAsync(s.d_tri_next, 0, 2 * sizeof(unsigned), st);
+        if (e != cudaSuccess) return e;
+        icx::csr_tri_flow_kernel<<<grid, 256, 0, st>>>(nn, s.d_a_rowptr, s.d_a_colidx, s.d_a_diag, s.d_a_lu, xin,
+                                                       s.d_colnorm2, 0, s.d_tri_ready, e_l, s.d_tri_next, s.d_tri_err);
+        icx::csr_tri_flow_kernel<<<grid, 256, 0, st>>>(nn, s.d_a_rowptr, s.d_a_colidx, s.d_a_diag, s.d_a_lu,
+                                                       s.d_colnorm2, yout, 1, s.d_tri_ready, e_u, s.d_tri_next + 1,
+                                                       s.d_tri_err);
         return cudaGetLastError();
       };
       use_m = true;
@@ -1536,6 +1596,18 @@ icx_status icx_lm_solve(icx_ctx* c, double* d_u, double* x, const icx_lm_options
     st = icx::gmres_op(s.kb, A, use_m ? &M : nullptr, opt->gmres_max_it, opt->gmres_rtol, s.d_jtr, s.d_p, &its, &rr,
                        strm, &c->err);
     if (st != ICX_OK) { cleanup(); return st; }
+    if (use_m) {
+      int terr = 0;
+      MCK(cudaMemcpyAsync(&terr, s.d_tri_err, sizeof(int), cudaMemcpyDeviceToHost, strm));
+      MCK(cudaStreamSynchronize(strm));
+      if (terr) {
+        cudaMemset(s.d_tri_err, 0, sizeof(int));
+        cudaMemset(s.d_tri_ready, 0, sizeof(unsigned) * n);
+        s.tri_epoch = 0;
+        cleanup();
+        return merr(c, ICX_ERR_CUDA, "LM subproblem ILU(0) apply: a dependency wait timed out");
+      }
+    }
     R->linear_iterations_total += its;
     R->linear_relres_max = std::max(R->linear_relres_max, rr);
     MCK(cudaMemcpy(px.data(), s.d_p + N, sizeof(double) * ngeo, cudaMemcpyDeviceToHost));

@@ -436,8 +436,8 @@ icx_status icx_batch_offsets(const icx_ctx* batch, int* elem_offsets);
  * an order; every part has the same PDE). The set's vectors hold each order's
  * parts side by side, orders ascending, parts in their given order within an
  * order; icx_pset_offsets gives part k's first unknown (offsets[k], in the
- * caller's part numbering) and offsets[n_parts] = the total. The parts must
- * outlive the set.
+ * caller's part numbering; the part's own n_dof unknowns follow) and
+ * offsets[n_parts] = the total. The parts must outlive the set.
  * icx_pset_newton_solve runs one Newton solve per part, each on its own
  * (petsc_newton.hpp:205-329): its own residual norm and stopping test, its own
  * GMRES Krylov space, Hessenberg matrix and convergence, its own line search

@@ -233,67 +233,68 @@ def _fixed(pb, node, d):
     return (ix in (0, pb.nx)) if d == 0 else (iy in (0, pb.ny))
 
 
-def lm_explicit(pb, coord, traces, u0, x0, kmax=5, lambda_u=1e-7, lambda_b=1e-2, lambda_lag=1e-5, tau_abs=1e-10,
-                max_rejections=20, history=None):
-    """CorriganLM::solve with the explicitly formed subproblem
-    (corrigan_lm.hpp:363-717, explicitly_form_subproblem = true, Corrigan line
-    search): (J^T J + diag(lambda_u |J_col|, lambda_b |J_col|)
-    + lambda_lag |r| K^T K + lambda_el) p = J^T r solved exactly (sparse LU),
-    u <- u - alpha p_u, x <- x - alpha p_x, acceptance when no element inverts
-    and |r_step| < 10 |r_old|, the lambda updates and the element-wise
-    regularisation of the reference. K^T K is formed as the reference forms it:
-    its loop assigns KTK[i, j] = K[k, i] K[k, j] for every k in turn, so the
-    last basis function's row k = ng - 1 is what remains (corrigan_lm.hpp:463-469).
-    Returns (u, x, residual norm history, alpha history)."""
-    import ctypes as C
-    u, x = np.array(u0, dtype=float), np.array(x0, dtype=float)
-    E, nb, N = ob.sizes(pb)
-    g = pb.geo_order
-    ng = (g + 1) ** 2
-    sel, cols = mdg_layout(pb, coord, traces)
-    inv = {int(n): k for k, n in enumerate(sel)}
-    free = [[d for d in range(2) if not _fixed(pb, int(n), d)] for n in sel]
-    conn, _, _ = ob.topology(ob.oracle(), pb)
-    coord0 = np.ascontiguousarray(coord)
-    ncol = N + len(x)
+class ExplicitSubproblem:
+    """the explicitly formed CorriganLM subproblem (corrigan_lm.hpp:426-530)
+    of one configuration: (J^T J + diag(lambda_u |J_col|, lambda_b |J_col|)
+    + lambda_lag |r| K^T K + lambda_el) p = J^T r, over the state unknowns and
+    the free coordinates of the selected nodes. K^T K is formed as the
+    reference forms it: its loop assigns KTK[i, j] = K[k, i] K[k, j] for every
+    k in turn, so the last basis function's row k = ng - 1 is what remains
+    (corrigan_lm.hpp:463-469)."""
 
-    def state(xv):
-        return np.ascontiguousarray(_coords_from_x(pb, coord0, sel, cols, xv))
+    def __init__(self, pb, coord, traces):
+        self.pb, self.traces = pb, traces
+        self.E, self.nb, self.N = ob.sizes(pb)
+        g = pb.geo_order
+        self.ng = (g + 1) ** 2
+        self.sel, self.cols = mdg_layout(pb, coord, traces)
+        inv = {int(n): k for k, n in enumerate(self.sel)}
+        free = [[d for d in range(2) if not _fixed(pb, int(n), d)] for n in self.sel]
+        conn, _, _ = ob.topology(ob.oracle(), pb)
+        self.coord0 = np.ascontiguousarray(coord)
+        ng, N = self.ng, self.N
 
-    def cg_K(cw):
-        K = np.zeros((E, ng, ng))
-        assert ob.oracle().fn("cg_stiffness")(C.byref(pb), ob._ptr(cw), ob._ptr(K)) == 0
+        def geo_pairs(e):
+            """(row, col) positions of the free coordinates of every pair of selected nodes of element e"""
+            out = []
+            for il in range(ng):
+                ki = inv.get(int(conn[e, il]))
+                if ki is None:
+                    continue
+                for jl in range(ng):
+                    kj = inv.get(int(conn[e, jl]))
+                    if kj is None:
+                        continue
+                    for iv in range(len(free[ki])):
+                        for jv in range(len(free[kj])):
+                            out.append((il, jl, N + self.cols[ki] + iv, N + self.cols[kj] + jv))
+            return out
+
+        self.pairs = [geo_pairs(e) for e in range(self.E)]
+
+    def state(self, xv):
+        return np.ascontiguousarray(_coords_from_x(self.pb, self.coord0, self.sel, self.cols, xv))
+
+    def linearise(self, u, x):
+        """([res; ic], J) at (u, x)"""
+        return mdg_jacobian_sparse(self.pb, self.state(x), self.traces, u, x)
+
+    def cg_K(self, cw):
+        import ctypes as C
+        K = np.zeros((self.E, self.ng, self.ng))
+        assert ob.oracle().fn("cg_stiffness")(C.byref(self.pb), ob._ptr(cw), ob._ptr(K)) == 0
         return K
 
-    def min_det(cw):
-        m = np.zeros(E)
-        assert ob.oracle().fn("min_detj")(C.byref(pb), ob._ptr(cw), ob._ptr(m)) == 0
+    def min_det(self, cw):
+        import ctypes as C
+        m = np.zeros(self.E)
+        assert ob.oracle().fn("min_detj")(C.byref(self.pb), ob._ptr(cw), ob._ptr(m)) == 0
         return m
 
-    def geo_pairs(e):
-        """(row, col) positions of the free coordinates of every pair of selected nodes of element e"""
-        out = []
-        for il in range(ng):
-            ki = inv.get(int(conn[e, il]))
-            if ki is None:
-                continue
-            for jl in range(ng):
-                kj = inv.get(int(conn[e, jl]))
-                if kj is None:
-                    continue
-                for iv in range(len(free[ki])):
-                    for jv in range(len(free[kj])):
-                        out.append((il, jl, N + cols[ki] + iv, N + cols[kj] + jv))
-        return out
-
-    pairs = [geo_pairs(e) for e in range(E)]
-    out, J = mdg_jacobian_sparse(pb, state(x), traces, u, x)
-    hist = [np.linalg.norm(out)]
-    alphas = []
-    lu, lb, lu_min = lambda_u, lambda_b, lambda_u
-    lam_el = np.zeros(E)
-    k, rejects = 0, 0
-    while k < kmax and hist[-1] > tau_abs:
+    def system(self, out, J, x, lu, lb, lambda_lag, lam_el):
+        """(M, rhs) of the subproblem at the linearisation (out, J) and nodes x"""
+        N, ng = self.N, self.ng
+        ncol = J.shape[1]
         rnorm = np.linalg.norm(out)
         Jt = J.T.tocsr()
         A = (Jt @ J).tocoo()
@@ -301,20 +302,46 @@ def lm_explicit(pb, coord, traces, u0, x0, kmax=5, lambda_u=1e-7, lambda_b=1e-2,
         d = np.concatenate([lu * cn[:N], lb * cn[N:]])
         rr, cc, vv = [A.row], [A.col], [A.data]
         rr.append(np.arange(ncol)); cc.append(np.arange(ncol)); vv.append(d)
-        Kall = cg_K(state(x))
+        Kall = self.cg_K(self.state(x))
         ri, ci, vi = [], [], []
-        for e in range(E):
+        for e in range(self.E):
             Kl = Kall[e]
             KTK = np.outer(Kl[ng - 1], Kl[ng - 1])
-            for il, jl, r, c in pairs[e]:
+            for il, jl, r, c in self.pairs[e]:
                 ri.append(r); ci.append(c); vi.append(KTK[il, jl] * lambda_lag * rnorm)
             if lam_el[e] > 0.0:
-                for il, jl, r, c in pairs[e]:
+                for il, jl, r, c in self.pairs[e]:
                     if il == jl:
                         ri.append(r); ci.append(c); vi.append(lam_el[e])
         rr.append(np.array(ri, dtype=np.int64)); cc.append(np.array(ci, dtype=np.int64)); vv.append(np.array(vi))
         M = sp.coo_matrix((np.concatenate(vv), (np.concatenate(rr), np.concatenate(cc))), shape=(ncol, ncol)).tocsc()
-        p = spla.spsolve(M, Jt @ out)
+        return M, Jt @ out
+
+
+def lm_explicit(pb, coord, traces, u0, x0, kmax=5, lambda_u=1e-7, lambda_b=1e-2, lambda_lag=1e-5, tau_abs=1e-10,
+                max_rejections=20, history=None):
+    """CorriganLM::solve with the explicitly formed subproblem
+    (corrigan_lm.hpp:363-717, explicitly_form_subproblem = true, Corrigan line
+    search): the ExplicitSubproblem system solved exactly (sparse LU),
+    u <- u - alpha p_u, x <- x - alpha p_x, acceptance when no element inverts
+    and |r_step| < 10 |r_old|, the lambda updates and the element-wise
+    regularisation of the reference. Returns (u, x, residual norm history,
+    alpha history)."""
+    u, x = np.array(u0, dtype=float), np.array(x0, dtype=float)
+    sub = ExplicitSubproblem(pb, coord, traces)
+    E, N = sub.E, sub.N
+    out, J = sub.linearise(u, x)
+    hist = [np.linalg.norm(out)]
+    alphas = []
+    lu, lb, lu_min = lambda_u, lambda_b, lambda_u
+    lam_el = np.zeros(E)
+    k, rejects = 0, 0
+    while k < kmax and hist[-1] > tau_abs:
+        rnorm = np.linalg.norm(out)
+        M, rhs = sub.system(out, J, x, lu, lb, lambda_lag, lam_el)
+        p = spla.spsolve(M, rhs)
+        state = sub.state
+        min_det = sub.min_det
         last = {}
 
         def phi(a):
@@ -341,7 +368,7 @@ def lm_explicit(pb, coord, traces, u0, x0, kmax=5, lambda_u=1e-7, lambda_b=1e-2,
             if rejects > max_rejections:
                 break
             continue
-        out, J = mdg_jacobian_sparse(pb, state(x), traces, u, x)
+        out, J = sub.linearise(u, x)
         hist.append(np.linalg.norm(out))
         if history is not None:
             history.append((hist[-1], alpha))

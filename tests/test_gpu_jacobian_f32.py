@@ -2,9 +2,13 @@
 Newton as FP64 iterative refinement around it (icx_newton_options.precision 2).
 
 * The FP32 blocks against the oracle's FP64 FD Jacobian: max |J32 - J| within
-  2e-3 of max |J| (one-sided differences in FP32 with eps = sqrt(FLT_EPSILON)
-  carry an error of order sqrt(FLT_EPSILON) = 3.5e-4 relative to the flux
-  scale), and the residual the call writes is the FP64 residual bit for bit.
+  2e-2 of max |J|. A one-sided FP32 difference with eps = sqrt(FLT_EPSILON)
+  carries a rounding error of about FLT_EPSILON |F| / eps = 3.5e-4 |F| per
+  entry, and the Navier-Stokes fluxes are an order of magnitude above the
+  Jacobian entries (the pressure is ~1 / (gamma M^2) ~ 10 at Mach 0.3):
+  about 1e-2 of the largest entry (measured 7e-3 to 9e-3; the Burgers
+  cases below 2e-3). The residual the call writes is the FP64 residual bit
+  for bit.
 * Newton with FP32 linearisations converges to the FP64 Newton's state within
   1e-10 of the L2 norm of the larger of that state and the initial state: the
   outer residual, norm, line search and update are FP64, so only the
@@ -48,7 +52,7 @@ def test_fp32_blocks_against_oracle(kw):
     assert np.array_equal(rp, rowptr) and np.array_equal(ci, colidx)
     j32 = v32.cpu().numpy().astype(np.float64).reshape(v_or.shape)
     err = np.abs(j32 - v_or).max() / np.abs(v_or).max()
-    assert err <= 2e-3, err
+    assert err <= 2e-2, err
     ctx.close()
 
 
@@ -58,9 +62,12 @@ def test_newton_fp32_quadrature_reaches_fp64_state(pde):
     from iceicle_b200.workloads import burgers_config, ns_mms_config
     wl = burgers_config(nx=16, ny=16) if pde == "burgers" else ns_mms_config(nx=12, ny=12, p=2, geo_order=2)
     out = {}
+    # Burgers: to 1e-13, so that both states are within roundoff of the root
+    # (its Jacobian's inverse amplifies a 1e-10 residual to ~1e-8 in the state)
+    tau = 1e-13 if pde == "burgers" else 1e-10
     for prec in (0, 2):
         o = ib.default_newton_options()
-        o.precision, o.gmres_rtol, o.tau_abs, o.kmax = prec, 1e-10, 1e-10, 30
+        o.precision, o.gmres_rtol, o.tau_abs, o.kmax = prec, 1e-10, tau, 30
         u = torch.from_numpy(wl.u0.copy()).cuda()
         rep = wl.ctx.newton_solve(u, o)
         assert rep.converged, (prec, list(rep.residual_history[:rep.iterations + 1]))
