@@ -59,8 +59,10 @@ def parse():
     ap.add_argument("--batched", type=int, default=512, metavar="N",
                     help="secondary timing of N seeded uneven advection-diffusion problems, batched vs one at a "
                          "time (0: skip; the full problem set is 512)")
-    ap.add_argument("--batched-sample", type=int, default=24, metavar="K",
+    ap.add_argument("--batched-sample", type=int, default=16, metavar="K",
                     help="problems of the set also solved one at a time for the batched ratio")
+    ap.add_argument("--batched-fp32q", action="store_true",
+                    help="also time the problem set with FP32 flux quadrature (precision 2)")
     ap.add_argument("--learned-seeds", type=int, default=1, metavar="K",
                     help="fresh instances of the learned-preconditioner comparison (256 x 256 Navier-Stokes)")
     ap.add_argument("--no-lm", action="store_true", help="skip the MDG-ICE (64 x 64) LM timing")
@@ -233,7 +235,7 @@ def residual_work(wl):
 NCU_DRAM_BYTES = {"vol": 43.45e6 + 0.57e6, "face": 25.42e6 + 0.0003e6}
 
 
-def batched_bench(torch, dev, n_problems, sample=48):
+def batched_bench(torch, dev, n_problems, sample=16, fp32_quadrature=False):
     """Newton solves to |r| <= 1e-10 per problem (Wolfe line search, GMRES(30)
     + block-ILU(0)) of the seeded uneven advection-diffusion problems (meshes
     8x8 to 96x96, orders 1-4, viscosity log-uniform in [1e-4, 1e-1], advection
@@ -280,7 +282,7 @@ def batched_bench(torch, dev, n_problems, sample=48):
     ps = ib.ProblemSet(parts, dev.index)
     ps.members = list(range(n_problems))
     t_all, u_all, reps, stats = set_solve(ps, 0)
-    t_q32, u_q32, reps32, _ = set_solve(ps, 2)
+    t_q32, u_q32, reps32 = (set_solve(ps, 2)[:3]) if fp32_quadrature else (None, u_all, reps)
     rng = np.random.default_rng(5)
     pick = sorted(rng.choice(n_problems, size=min(sample, n_problems), replace=False).tolist())
     sub = ib.ProblemSet([parts[k] for k in pick], dev.index)
@@ -300,11 +302,12 @@ def batched_bench(torch, dev, n_problems, sample=48):
         a, b = holder["u"].cpu().numpy(), sub.part(u_sub, i)
         worst = max(worst, float(np.linalg.norm(a - b) / max(np.linalg.norm(a), 1e-300)))
     q32 = max(float(np.linalg.norm(ps.part(u_all, k) - ps.part(u_q32, k)) /
-                    max(np.linalg.norm(ps.part(u_all, k)), 1e-300)) for k in range(n_problems))
+                    max(np.linalg.norm(ps.part(u_all, k)), 1e-300)) for k in range(n_problems)) \
+        if fp32_quadrature else None
     n_dof = ps.offsets[-1]
     out = {"problems": n_problems, "n_dof": int(n_dof), "orders": stats.orders,
            "set_fp64_s": t_all, "set_fp32_quadrature_s": t_q32,
-           "converged": int(sum(r.converged for r in reps)), "converged_fp32_quadrature": int(sum(r.converged for r in reps32)),
+           "converged": int(sum(r.converged for r in reps)), "converged_fp32_quadrature": int(sum(r.converged for r in reps32)) if fp32_quadrature else None,
            "newton_rounds": stats.newton_rounds, "arnoldi_steps": stats.arnoldi_steps,
            "arnoldi_graph_launches": stats.graph_launches, "line_search_rounds": stats.line_search_rounds,
            "max_newton_its": max(r.iterations for r in reps),
@@ -411,7 +414,7 @@ def jacobian_bench(torch, dev, wl, hbm_gbs, cpu=True):
     return out
 
 
-def lm_bench(torch, dev, kmax=3, maxit=2000):
+def lm_bench(torch, dev, kmax=1, maxit=300, orders=(1,)):
     """MDG-ICE (CorriganLM with the explicitly formed, ILU(0)-preconditioned
     subproblem): 64 x 64 quads, p = 1 and p = 2, oblique inviscid-Burgers
     shock on a jittered grid, all interior traces selected; wall time of
@@ -423,7 +426,7 @@ def lm_bench(torch, dev, kmax=3, maxit=2000):
     import iceicle_b200 as ib
     from iceicle_b200.workloads import mdg_ice_config
     out = {}
-    for p in (1, 2):
+    for p in orders:
         wl, traces, x0 = mdg_ice_config(n=64, p=p, device=dev.index)
         o = ib.default_lm_options()
         o.kmax, o.explicit_subproblem, o.gmres_rtol, o.gmres_max_it, o.gmres_restart = kmax, 1, 1e-8, maxit, 60
@@ -836,7 +839,7 @@ def run_ours(a):
             if not a.no_lm:
                 section("mdg_ice", lambda: lm_bench(torch, dev))
         if a.batched and ws == 1:
-            section("batched", lambda: batched_bench(torch, dev, a.batched, a.batched_sample))
+            section("batched", lambda: batched_bench(torch, dev, a.batched, a.batched_sample, a.batched_fp32q))
         if not a.no_learned and ws == 1:
             section("learned_pc", lambda: learned_bench(torch, dev, not a.no_tune, a.learned_seeds))
         line["section_wall_s"] = wall

@@ -829,7 +829,7 @@ class LMOptions(C.Structure):
                 ("ls_alpha_initial", C.c_double), ("ls_alpha_max", C.c_double), ("ls_alpha_min", C.c_double),
                 ("gmres_restart", C.c_int), ("gmres_max_it", C.c_int), ("gmres_rtol", C.c_double),
                 ("max_rejections", C.c_int), ("verbosity", C.c_int), ("explicit_subproblem", C.c_int),
-                ("lambda_lag", C.c_double)]
+                ("lambda_lag", C.c_double), ("step_only", C.c_int)]
 
 
 class LMReport(C.Structure):

@@ -1611,6 +1611,14 @@ icx_status icx_lm_solve(icx_ctx* c, double* d_u, double* x, const icx_lm_options
     R->linear_iterations_total += its;
     R->linear_relres_max = std::max(R->linear_relres_max, rr);
     MCK(cudaMemcpy(px.data(), s.d_p + N, sizeof(double) * ngeo, cudaMemcpyDeviceToHost));
+    if (opt->step_only) {
+      // the first subproblem's solution in place of the unknowns
+      MCK(cudaMemcpyAsync(d_u, s.d_p, sizeof(double) * N, cudaMemcpyDeviceToDevice, strm));
+      MCK(cudaStreamSynchronize(strm));
+      std::memcpy(x, px.data(), sizeof(double) * ngeo);
+      cleanup();
+      return icx_mdg_set_x(c, xh.data());  // the mesh stays at the input nodes
+    }
     double alpha = 1.0;
     bool accept = true;
     if (opt->linesearch == 2) {

@@ -262,6 +262,10 @@ typedef struct icx_lm_options {
    * without preconditioner (the MATSHELL path, corrigan_lm.hpp:68-109). */
   int explicit_subproblem;
   double lambda_lag;         /* CorriganLM::lambda_lag (default 1e-5) */
+  /* 1: return after the first subproblem solve (the KSPSolve of the first
+   * iteration) with its solution p in place of the unknowns: d_u <- p_u,
+   * x <- p_x; nothing is updated. 0 (default): the solve. */
+  int step_only;
 } icx_lm_options;
 
 typedef struct icx_lm_report {
