@@ -129,6 +129,33 @@ def calibrate(model, instance, n=256, samples=167, every=5, sweeps=0, ilu_tile=0
                 loss_scaled=s_aa - 2 * g * s_ab + g * g * s_bb)
 
 
+def select_scale(model, instance, n=256, sweeps=0, ilu_tile=0, candidates=(0.0, 0.25, 0.5, 1.0), device=0):
+    """the share g of the correction chosen by what it is for: the learned,
+    mixed-precision Newton solve of a held-out instance to |r| <= 1e-10 is
+    run with the output layer scaled by each candidate g, and the g with the
+    fewest GMRES iterations is kept (ties: the smaller g; g = 0 is the base
+    preconditioner itself). The output layer of `model` is left scaled by it.
+    Returns a record of the iterations per candidate and the choice."""
+    p0 = model.get_params()
+    D, H = model.bs * model.bs, model.hidden
+    o_w3 = H * D + H + H * 2 * H + H
+    wl = make_instance(*instance, n, device)
+    its = {}
+    for g in candidates:
+        p = p0.copy()
+        p[o_w3:] *= g
+        model.set_params(p)
+        rec, _ = solve(wl, model, 5, 1, sweeps, device, ilu_tile)
+        its[g] = (rec["gmres_its"] + (10**9 if not rec["converged"] else 0), rec["s"], rec["pc_fallbacks"])
+    best = min(candidates, key=lambda g: (its[g][0], g))
+    p = p0.copy()
+    p[o_w3:] *= best
+    model.set_params(p)
+    del wl
+    return dict(instance=list(instance), g=best,
+                candidates={str(g): dict(gmres_its=v[0], s=v[1], pc_fallbacks=v[2]) for g, v in its.items()})
+
+
 def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu_tile=0):
     """one Newton solve of an instance to |r| <= 1e-10 (GMRES(30), Wolfe line
     search), timed with CUDA events; returns (report dict, final state)"""
@@ -186,7 +213,8 @@ def new_model(device=0, seed=0, hidden=256):
 # Jacobian / residual pairs from the plain solver on seeded instances (Re
 # uniform in [50, 500]), the correction trained on top of block-ILU(0) on
 # 32 x 32 element tiles with exact triangular solves (pc_sweeps = 0), then
-# scaled on a held-out instance (calibrate)
+# scaled on a held-out instance: by the training loss (calibrate), then by the
+# GMRES iterations of its Newton solve (select_scale)
 RECIPE = dict(model_seed=1, train_instances=(8, 11), pairs=2000, samples=167, every=5, steps=120, batch=4, random=2,
               sweeps=0, ilu_tile=32, lr=1e-3, holdout=(1, 5))
 EVAL_INSTANCES = (3, 99)
@@ -207,9 +235,12 @@ def main(argv=None):
         train(m, instances(*r["train_instances"]), n=a.n, samples=r["samples"], every=r["every"], steps=r["steps"],
               batch=r["batch"], random=r["random"], sweeps=r["sweeps"], lr=r["lr"], pairs=r["pairs"],
               ilu_tile=r["ilu_tile"], log=lambda x: print(json.dumps(x), flush=True))
-        rec = calibrate(m, instances(*r["holdout"])[0], n=a.n, samples=r["samples"], every=r["every"],
-                        sweeps=r["sweeps"], ilu_tile=r["ilu_tile"])
+        hold = instances(*r["holdout"])[0]
+        rec = calibrate(m, hold, n=a.n, samples=r["samples"], every=r["every"], sweeps=r["sweeps"],
+                        ilu_tile=r["ilu_tile"])
         print(json.dumps({"calibration": rec}), flush=True)
+        rec = select_scale(m, hold, n=a.n, sweeps=r["sweeps"], ilu_tile=r["ilu_tile"])
+        print(json.dumps({"selection": rec}), flush=True)
         m.save(a.path, sweeps=r["sweeps"], ilu_tile=r["ilu_tile"])
     else:
         m = LearnedPreconditioner.load(a.path)
