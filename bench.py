@@ -472,6 +472,12 @@ def newton_bench(torch, dev, tune=True):
         states = {}
         tile = 8 if name.startswith("burgers") else 32
         for label, prec, t in (("fp64", 0, 0), ("mixed", 1, 0), ("mixed_tiled", 1, tile), ("quad32_tiled", 2, tile)):
+            if tune and t and "autotune_tiled" not in rows:
+                # the apply's launch shapes for the tiled pattern
+                wl.ctx.ilu_tile = t
+                t2 = wl.ctx.autotune(torch.from_numpy(wl.u0).to(dev), ib.TUNE_ILU | ib.TUNE_ILU_FP32)
+                rows["autotune_tiled"] = {"chosen": t2["chosen"], "ilu_ms_default": t2["ilu_ms_default"],
+                                          "ilu_ms_tuned": t2["ilu_ms_tuned"]}
             opt = ib.default_newton_options()
             opt.precision = prec
             opt.ilu_tile = t
@@ -642,6 +648,11 @@ def learned_bench(torch, dev, tune=True, n_seeds=3):
             tuned = {"chosen": t["chosen"], "ilu_ms_default": t["ilu_ms_default"], "ilu_ms_tuned": t["ilu_ms_tuned"]}
         plain, u_p = lp.solve(wl, None, 2, 0, device=dev.index)
         mixed, _ = lp.solve(wl, None, 2, 1, device=dev.index)
+        if tune and tile:  # the apply's launch shapes for the tiled pattern
+            wl.ctx.ilu_tile = tile
+            t2 = wl.ctx.autotune(torch.from_numpy(wl.u0).to(dev), ib.TUNE_ILU | ib.TUNE_ILU_FP32)
+            tuned["tiled"] = {"chosen": t2["chosen"], "ilu_ms_default": t2["ilu_ms_default"],
+                              "ilu_ms_tuned": t2["ilu_ms_tuned"]}
         tiled, _ = lp.solve(wl, None, 2, 1, 0, dev.index, tile)
         learned, u_l = lp.solve(wl, m, 5, 1, sw, dev.index, tile)
         del wl

@@ -227,24 +227,44 @@ __global__ void __launch_bounds__(256) ilu_scale_upper_kernel(int E, const int* 
 }
 
 // ------------------------------------------------------------- reductions
-// partial[j * nblocks + b] = sum over block b's rows of V_j . w (V_j = V + j*ld;
-// an FP32 basis is widened to FP64 before the product)
-template <class TV>
-__global__ void mdot_partial_kernel(long long n, const TV* __restrict__ V, long long ld, int nvec,
-                                    const double* __restrict__ w, double* __restrict__ partial) {
-  __shared__ double red[256];
-  int j = blockIdx.y;
-  const TV* v = V + (size_t)j * ld;
-  double s = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    s += (double)v[i] * w[i];
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-    if (threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
+// partial[j * nblocks + b] = sum over block b's rows of V_j . x (V_j = V + j*ld;
+// an FP32 basis is widened to FP64 before the product), G vectors per pass
+// over x: each thread holds x_i once per group of G basis vectors, so x is
+// read ceil(nvec / G) times instead of nvec times (the vectors V_j once
+// each); per block the sums are reduced by shuffles, then across the warps in
+// a fixed order
+template <class TV, int G>
+__global__ void __launch_bounds__(256) mdot_grouped_kernel(long long n, const TV* __restrict__ V, long long ld,
+                                                           int nvec, const double* __restrict__ x,
+                                                           double* __restrict__ partial) {
+  __shared__ double red[G][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int j0 = 0; j0 < nvec; j0 += G) {
+    double acc[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) acc[g] = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+      const double xi = x[i];
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+        if (j0 + g < nvec) acc[g] += (double)V[(size_t)(j0 + g) * ld + i] * xi;
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      double v = acc[g];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if (lane == 0) red[g][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < G && j0 + (int)threadIdx.x < nvec) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) s += red[threadIdx.x][w];
+      partial[(size_t)(j0 + threadIdx.x) * gridDim.x + blockIdx.x] = s;
+    }
     __syncthreads();
   }
-  if (threadIdx.x == 0) partial[(size_t)j * gridDim.x + blockIdx.x] = red[0];
 }
 
 __global__ void mdot_final_kernel(int nblocks, int nvec, const double* __restrict__ partial, double* __restrict__ out) {
@@ -320,18 +340,16 @@ static int grid_for(long long n) {
 
 cudaError_t la_mdot(LinalgWork& w, long long n, const double* V, long long ld, int nvec, const double* x,
                     double* d_out, cudaStream_t s) {
-  int nb = 148 * 2;
-  dim3 grid(nb, nvec);
-  mdot_partial_kernel<double><<<grid, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
+  const int nb = 148 * 2;
+  mdot_grouped_kernel<double, 8><<<nb, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
   mdot_final_kernel<<<nvec, 256, 0, s>>>(nb, nvec, w.partial, d_out);
   return cudaGetLastError();
 }
 
 cudaError_t la_mdot32(LinalgWork& w, long long n, const float* V, long long ld, int nvec, const double* x,
                       double* d_out, cudaStream_t s) {
-  int nb = 148 * 2;
-  dim3 grid(nb, nvec);
-  mdot_partial_kernel<float><<<grid, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
+  const int nb = 148 * 2;
+  mdot_grouped_kernel<float, 8><<<nb, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
   mdot_final_kernel<<<nvec, 256, 0, s>>>(nb, nvec, w.partial, d_out);
   return cudaGetLastError();
 }

@@ -35,7 +35,9 @@ struct CacheEntry {
   TileChoice tile;
   int parts = 0;  // ICX_TUNE_* bits whose fields hold a tuned choice
 };
-using Key = std::tuple<int, int, int, int, int>;  // dim, p, neq, geometry order, DDG flux
+// dim, p, neq, geometry order, DDG flux, and the block-ILU(0) tiling the
+// apply was timed on (tile side, 0 untiled, -1 element groups)
+using Key = std::tuple<int, int, int, int, int, int>;
 std::mutex g_mu;
 std::map<Key, CacheEntry> g_cache;
 
@@ -264,7 +266,8 @@ void to_public(const TileChoice& t, icx_tile_choice* o) {
 }
 
 Key key_of(const icx_ctx* c) {
-  return Key{2, c->dm.P, c->dm.neq, c->dm.G, c->phys.beta1 != 0.0 ? 1 : 0};
+  return Key{2, c->dm.P, c->dm.neq, c->dm.G, c->phys.beta1 != 0.0 ? 1 : 0,
+             c->ilu_groups.empty() ? c->ilu_tile : -1};
 }
 
 }  // namespace
