@@ -220,29 +220,38 @@ __global__ void __launch_bounds__(THREADS, 1)
       for (int kt = issued > STAGES ? issued - STAGES : 0; kt < issued; ++kt)
         mbar_wait(&full[kt % STAGES], (unsigned)(kt / STAGES) & 1u);
   } else if (nk > 0) {
-    const int row = m0 + warp * 32 + lane;
+    // tcgen05.ld gives lane l the 32 columns of accumulator row 32w + l; a
+    // 32 x 33 staging tile in the (now idle) operand ring turns them around
+    // so that every store of the warp covers 32 consecutive columns of one
+    // output row (one 128-byte line) instead of one word in each of 32 rows
+    float* stage = reinterpret_cast<float*>(sA) + warp * 32 * 33;
+    const int rbase = m0 + warp * 32;
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
     for (int c = 0; c < BN; c += 32) {
       if (n0 + c >= g.N) break;  // uniform over the CTA
       float v[32];
       tmem_ld32(lane_addr + (uint32_t)c, v);
-      if (row < g.M) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int col = n0 + c + j;
-          if (col >= g.N) break;
-          float x = v[j];
-          if (g.accumulate) {
-            atomicAdd(g.C32 + (size_t)row * g.ldc + col, x);
-            continue;
-          }
-          if (g.bias) x += g.bias[col];
-          if (g.relu) x = fmaxf(x, 0.f);
-          if (g.C32) g.C32[(size_t)row * g.ldc + col] = x;
-          if (g.C16) g.C16[(size_t)row * g.ldc16 + col] = __float2bfloat16_rn(x);
+      for (int j = 0; j < 32; ++j) stage[lane * 33 + j] = v[j];
+      __syncwarp();
+      const int col = n0 + c + lane;
+      const float bcol = (g.bias && col < g.N && !g.accumulate) ? g.bias[col] : 0.f;
+#pragma unroll 4
+      for (int r = 0; r < 32; ++r) {
+        const int row = rbase + r;
+        if (row >= g.M || col >= g.N) continue;
+        float x = stage[r * 33 + lane];
+        if (g.accumulate) {
+          atomicAdd(g.C32 + (size_t)row * g.ldc + col, x);
+          continue;
         }
+        if (g.bias) x += bcol;
+        if (g.relu) x = fmaxf(x, 0.f);
+        if (g.C32) g.C32[(size_t)row * g.ldc + col] = x;
+        if (g.C16) g.C16[(size_t)row * g.ldc16 + col] = __float2bfloat16_rn(x);
       }
+      __syncwarp();
     }
   }
   tc_fence_before();
