@@ -540,6 +540,140 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Block-ILU(0) apply on element groups (tiles): one CTA per group. A group's
+// factors couple none of its elements to another group, so its two sweeps
+// need nothing from outside it: the CTA runs its elements level by level
+// (levels of the kept lower dependencies, ascending for the forward sweep,
+// descending for the backward one), the tasks of one level (element, R rows)
+// spread over its warps, with a CTA barrier between levels. A task reads the
+// results of earlier levels with ordinary loads: the barrier orders the
+// CTA's own stores before them. No cross-CTA waits, so no polling.
+struct IluGroupPlan {
+  int ngroups;
+  const int* gorder;    // elements, group by group, by ascending level within a group
+  const int* glev;      // level boundaries: positions in gorder, group g's at glev[glev_ptr[g] .. glev_ptr[g + 1]]
+  const int* glev_ptr;  // [ngroups + 1]
+};
+
+template <class TA>
+struct IluGroupArgs {
+  int E, nnzb;
+  const int* rowptr;
+  const int* colidx;
+  const int* diag;
+  const TA* LU;
+  const TA* Uinv;
+  const double* x;
+  double* f;            // forward result (written and read by the group's own CTA)
+  double* y;            // output
+  int* err;
+  IluGroupPlan plan;
+};
+
+// threads per CTA of the group apply: FP32 factors keep their rows in half
+// the registers, so twice the warps fit a CTA
+template <class TA>
+constexpr int group_threads() { return sizeof(TA) == 8 ? 256 : 512; }
+
+template <int BS, int RT, class TA>
+__global__ void __launch_bounds__(group_threads<TA>()) ilu_apply_group_kernel(IluGroupArgs<TA> a) {
+  using K = FlowCfg<BS, RT>;
+  constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int g = blockIdx.x;
+  const int l0 = a.plan.glev_ptr[g], l1 = a.plan.glev_ptr[g + 1];
+  const int nlev = l1 - l0 - 1;
+  for (int sweep = 0; sweep < 2; ++sweep) {
+    const bool fwd = sweep == 0;
+    for (int li = 0; li < nlev; ++li) {
+      const int lv = fwd ? li : nlev - 1 - li;
+      const int p0 = a.plan.glev[l0 + lv], p1 = a.plan.glev[l0 + lv + 1];
+      const int ntask = (p1 - p0) * GROUPS;
+      for (int t = warp; t < ntask; t += nwarp) {
+        const int e = a.plan.gorder[p0 + t / GROUPS];
+        const int r0 = (t % GROUPS) * R;
+        int nbk = 0, kbs[2], ks[2];
+        bool bad = e < 0 || e >= a.E;
+        if (!bad) {
+          const int d = a.diag[e], rb = a.rowptr[e], re = a.rowptr[e + 1];
+          bad = d < rb || d >= re || rb < 0 || re > a.nnzb;
+          const int b0 = fwd ? rb : d + 1, b1 = fwd ? d : re;
+          bad = bad || (b1 - b0) > 2;
+          for (int kb = b0; !bad && kb < b1; ++kb) {
+            kbs[nbk] = kb;
+            ks[nbk] = a.colidx[kb];
+            bad = ks[nbk] < 0 || ks[nbk] >= a.E;
+            ++nbk;
+          }
+        }
+        if (bad) {
+          if (lane == 0) atomicExch(a.err, 2);
+          continue;  // the CTA keeps to its barriers
+        }
+        // the same arithmetic in the same order as the data-flow apply:
+        // f_e = x_e - sum L_ek f_k; y_e = inv(U_ee) f_e - sum (inv(U_ee) U_ek) y_k
+        TA am[3][R][NS];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          const TA* Ab = nullptr;
+          if (b < 2 && b < nbk) Ab = a.LU + (size_t)kbs[b] * BS * BS;
+          else if (b == 2 && !fwd) Ab = a.Uinv + (size_t)e * BS * BS;
+#pragma unroll
+          for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+              const int r = r0 + rr, c = lane + 32 * s;
+              am[b][rr][s] = (Ab && r < BS && c < BS) ? Ab[(size_t)r * BS + c] : TA(0);
+            }
+        }
+        const double* vsrc = fwd ? a.f : a.y;
+        TA xv[3][NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const int c = lane + 32 * s;
+#pragma unroll
+          for (int b = 0; b < 2; ++b) xv[b][s] = (b < nbk && c < BS) ? (TA)vsrc[(size_t)ks[b] * BS + c] : TA(0);
+          xv[2][s] = (!fwd && c < BS) ? (TA)a.f[(size_t)e * BS + c] : TA(0);
+        }
+        TA acc[R];
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          if (b < nbk) {
+#pragma unroll
+            for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+              for (int s = 0; s < NS; ++s) acc[rr] -= am[b][rr][s] * xv[b][s];
+          }
+        }
+        if (!fwd) {
+#pragma unroll
+          for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+            for (int s = 0; s < NS; ++s) acc[rr] += am[2][rr][s] * xv[2][s];
+        }
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
+        }
+        TA mine = TA(0);
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr)
+          if (lane == rr) mine = acc[rr];
+        const int r = r0 + lane;
+        if (lane < R && r < BS) {
+          if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
+          else a.y[(size_t)e * BS + r] = (double)mine;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
 #define ICX_BLOCK_SIZES(X) X(4) X(9) X(16) X(25) X(36) X(64) X(100)
 
 }  // namespace icx

@@ -525,6 +525,53 @@ static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, const int* order, cons
   return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(256), params, 0, s);
 }
 
+template <int B, int R, class TA>
+static const void* group_kernel_if_fit() {
+  if constexpr (flow_rows_fit(B, (B + 31) / 32, R)) return (const void*)ilu_apply_group_kernel<B, R, TA>;
+  else return nullptr;
+}
+
+template <int B, class TA>
+static const void* group_kernel_for(int rows) {
+  switch (rows ? rows : FlowCfg<B>::R_DEFAULT) {
+    case 2: return group_kernel_if_fit<B, 2, TA>();
+    case 4: return group_kernel_if_fit<B, 4, TA>();
+    case 6: return group_kernel_if_fit<B, 6, TA>();
+    case 8: return group_kernel_if_fit<B, 8, TA>();
+    default: return nullptr;
+  }
+}
+
+template <class TA>
+static cudaError_t ilu_apply_groups_t(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+                                      const int* glev_ptr, int rows, const TA* LU, const TA* Uinv, const double* x,
+                                      double* y, double* f, int* err, cudaStream_t s) {
+  if (ngroups <= 0) return cudaErrorInvalidValue;
+  const int bs = dm.nb * dm.neq;
+  const void* kern = nullptr;
+#define ICX_ILUG_CASE(B) \
+  if (bs == B) kern = group_kernel_for<B, TA>(rows);
+  ICX_BLOCK_SIZES(ICX_ILUG_CASE)
+#undef ICX_ILUG_CASE
+  if (!kern) return cudaErrorInvalidValue;
+  IluGroupArgs<TA> args{dm.E, dm.nnzb, dm.bsr_rowptr, dm.bsr_colidx, dm.bsr_diag, LU, Uinv, x, f, y, err,
+                        IluGroupPlan{ngroups, gorder, glev, glev_ptr}};
+  void* params[] = {&args};
+  return cudaLaunchKernel(kern, dim3(ngroups), dim3(group_threads<TA>()), params, 0, s);
+}
+
+cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+                                const int* glev_ptr, int rows, const double* LU, const double* Uinv, const double* x,
+                                double* y, double* f, int* err, cudaStream_t s) {
+  return ilu_apply_groups_t<double>(dm, ngroups, gorder, glev, glev_ptr, rows, LU, Uinv, x, y, f, err, s);
+}
+
+cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+                                    const int* glev_ptr, int rows, const float* LU, const float* Uinv,
+                                    const double* x, double* y, double* f, int* err, cudaStream_t s) {
+  return ilu_apply_groups_t<float>(dm, ngroups, gorder, glev, glev_ptr, rows, LU, Uinv, x, y, f, err, s);
+}
+
 int flow_rows_default(int bs) {
 #define ICX_FLOWR_CASE(B) \
   if (bs == B) return FlowCfg<B>::R_DEFAULT;

@@ -67,6 +67,16 @@ cudaError_t la_ilu_apply_flow(const DeviceMesh& dm, const int* order, const doub
 cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, const int* order, const float* LU, const float* Uinv,
                                   const double* x, double* y, double* f, unsigned* cnt_f, unsigned* cnt_b,
                                   unsigned epoch, int* err, cudaStream_t s);
+// the same apply on element groups (tiles) whose factors couple no two
+// groups: one CTA per group, levels of the group in turn (no cross-CTA
+// waits); gorder / glev / glev_ptr as IluGroupPlan (icx_blockrow.cuh); rows =
+// rows per warp task (0: the default); *err = 2 on an index out of range
+cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+                                const int* glev_ptr, int rows, const double* LU, const double* Uinv, const double* x,
+                                double* y, double* f, int* err, cudaStream_t s);
+cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+                                    const int* glev_ptr, int rows, const float* LU, const float* Uinv,
+                                    const double* x, double* y, double* f, int* err, cudaStream_t s);
 cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s);
 cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s);
 cudaError_t la_f2d(long long n, const float* x, double* y, cudaStream_t s);

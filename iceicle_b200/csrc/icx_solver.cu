@@ -8,11 +8,13 @@
 // device; the host holds only the (m+1) x m Hessenberg matrix and the scalar
 // line-search logic.
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <vector>
 
 #include "icx_internal.h"
@@ -37,6 +39,12 @@ struct IluTilePlan {
   int* map = nullptr;           // [nnzb] kept block -> block of the full pattern
   int* order = nullptr;         // [E] elements by ascending in-tile level (i mod s) + (j mod s)
   std::vector<int> lvl_off;
+  // the same per group (one CTA per group, la_ilu_apply_groups): elements
+  // group by group, by level within the group, and each group's level bounds
+  int ngroups = 0;
+  int* gorder = nullptr;        // [E]
+  int* glev = nullptr;          // level boundaries (positions in gorder), per group
+  int* glev_ptr = nullptr;      // [ngroups + 1] into glev
 };
 
 struct icx_solver_work {
@@ -171,7 +179,7 @@ icx_status ensure_work(icx_ctx* c, int m) {
 }
 
 void free_tile_plan(IluTilePlan& tp) {
-  for (int* p : {tp.rowptr, tp.colidx, tp.diag, tp.map, tp.order})
+  for (int* p : {tp.rowptr, tp.colidx, tp.diag, tp.map, tp.order, tp.gorder, tp.glev, tp.glev_ptr})
     if (p) cudaFree(p);
   tp = IluTilePlan();
 }
@@ -228,8 +236,30 @@ icx_status ensure_ilu_plan(icx_ctx* c) {
   std::vector<int> order(dm.E), fill(tp.lvl_off.begin(), tp.lvl_off.end() - 1);
   for (int e = 0; e < dm.E; ++e) order[fill[lvl[e]]++] = e;
   tp.nnzb = (int)tci.size();
+  // per group: its elements by (level, element), and the level bounds
+  std::map<long long, int> gid_of;
+  for (int e = 0; e < dm.E; ++e) gid_of.emplace(tile_of(e), 0);
+  int ng = 0;
+  for (auto& kv : gid_of) kv.second = ng++;
+  std::vector<std::array<int, 3>> key(dm.E);
+  for (int e = 0; e < dm.E; ++e) key[e] = {gid_of[tile_of(e)], lvl[e], e};
+  std::sort(key.begin(), key.end());
+  std::vector<int> gorder(dm.E), glev, glev_ptr(1, 0);
+  for (int p = 0; p < dm.E; ++p) {
+    gorder[p] = key[p][2];
+    const bool new_group = p == 0 || key[p][0] != key[p - 1][0];
+    if (new_group && p > 0) {
+      glev.push_back(p);  // the previous group's end
+      glev_ptr.push_back((int)glev.size());
+    }
+    if (new_group || key[p][1] != key[p - 1][1]) glev.push_back(p);
+  }
+  glev.push_back(dm.E);
+  glev_ptr.push_back((int)glev.size());
+  tp.ngroups = ng;
   const std::pair<int**, const std::vector<int>*> up[] = {
-      {&tp.rowptr, &trp}, {&tp.colidx, &tci}, {&tp.diag, &tdiag}, {&tp.map, &tmap}, {&tp.order, &order}};
+      {&tp.rowptr, &trp}, {&tp.colidx, &tci}, {&tp.diag, &tdiag}, {&tp.map, &tmap}, {&tp.order, &order},
+      {&tp.gorder, &gorder}, {&tp.glev, &glev}, {&tp.glev_ptr, &glev_ptr}};
   for (const auto& u : up) {
     cudaError_t e = cudaMalloc((void**)u.first, sizeof(int) * u.second->size());
     if (e == cudaSuccess) e = cudaMemcpy(*u.first, u.second->data(), sizeof(int) * u.second->size(),
@@ -312,6 +342,14 @@ cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStr
   const int* order = ilu_order(c);
   const int pi = mixed ? 1 : 0;
   const int rows = dm.tile.flow_rows[pi] ? dm.tile.flow_rows[pi] : icx::flow_rows_default(w->bs);
+  if (w->tp.tile && icx::ilu_schedule(dm.tile, pi, true) == 3) {
+    // tiled / grouped factors: one CTA per group, no waits across CTAs
+    const IluTilePlan& tp = w->tp;
+    return mixed ? icx::la_ilu_apply_groups_f32(dm, tp.ngroups, tp.gorder, tp.glev, tp.glev_ptr, rows, w->pc32,
+                                                w->uinv32, x, z, w->pct, w->pc_err, s)
+                 : icx::la_ilu_apply_groups(dm, tp.ngroups, tp.gorder, tp.glev, tp.glev_ptr, rows, w->pc, w->uinv,
+                                            x, z, w->pct, w->pc_err, s);
+  }
   // the sentinel schedule uses neither the counters nor the epoch
   const bool sen = icx::flow_sentinel(dm.tile, pi);
   if (!sen && rows != w->flow_rows) {
@@ -469,9 +507,7 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
   // the two-step and sweep forms, and block-ILU(0) on the sentinel schedule
   // (the counter schedule passes a new epoch to every apply, the row schedule
   // likewise; the learned preconditioner is left out)
-  const bool graphable = w->graphs_on && (pc == 0 || pc == 1 || pc == 3 || pc == 4 ||
-                                    (pc == 2 && icx::flow_sentinel(dm.tile, mixed ? 1 : 0) &&
-                                     !(w->rows_ok && w->schedule == 2)));
+  const bool graphable = icx::solver_graphable(c, pc, mixed);
   if (graphable) {
     const icx::TileChoice& t = dm.tile;
     const int pi = mixed ? 1 : 0;
@@ -1060,9 +1096,13 @@ const int* solver_flag(icx_ctx* c) { return c->sw ? c->sw->flag : nullptr; }
 // arguments at every apply (the condition of the Arnoldi-step graphs)
 bool solver_graphable(icx_ctx* c, int pc, bool mixed) {
   icx_solver_work* w = c->sw;
-  return w && w->graphs_on &&
-         (pc == 0 || pc == 1 || pc == 3 || pc == 4 ||
-          (pc == 2 && flow_sentinel(c->dm.tile, mixed ? 1 : 0) && !(w->rows_ok && w->schedule == 2)));
+  if (!w || !w->graphs_on) return false;
+  if (pc == 0 || pc == 1 || pc == 3 || pc == 4) return true;
+  if (pc != 2) return false;
+  // the group apply and the sentinel schedule launch the same arguments every time
+  const int pi = mixed ? 1 : 0;
+  if (w->tp.tile && ilu_schedule(c->dm.tile, pi, true) == 3) return true;
+  return flow_sentinel(c->dm.tile, pi) && !(w->rows_ok && w->schedule == 2);
 }
 
 // what the launches of a preconditioner apply and operator product depend on

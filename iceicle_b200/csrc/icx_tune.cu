@@ -220,13 +220,17 @@ struct Tuner {
       if ((st = check_err()) != ICX_OK) { dm.tile = keep; return st; }
       if ((st = time([&] { return apply(z1); }, &ms_def[pi])) != ICX_OK ||
           (st = check_err()) != ICX_OK) { dm.tile = keep; return st; }
-      const int R0 = icx::flow_rows_default(bs), S0 = icx::kFlowSchedDefault;
+      // tiled / grouped factors: the per-group apply (schedule 3, whose
+      // launch has no CTAs-per-SM choice) is the default and a candidate
+      const bool grouped = c->ilu_tile != 0 || !c->ilu_groups.empty();
+      const int R0 = icx::flow_rows_default(bs), S0 = grouped ? 3 : icx::kFlowSchedDefault;
       double best = ms_def[pi];
       int best_r = R0, best_c = 2, best_s = S0;
-      for (int sc = 1; sc <= 2; ++sc)
+      for (int sc = 1; sc <= (grouped ? 3 : 2); ++sc)
       for (int r : icx::kFlowRows) {
         if (!icx::flow_rows_compiled(bs, r)) continue;
         for (int k = 1; k <= MAX_CTAS; ++k) {
+          if (sc == 3 && k != 2) continue;
           if (r == R0 && k == 2 && sc == S0) continue;  // the default, timed above
           dm.tile.flow_rows[pi] = r;
           dm.tile.flow_ctas[pi] = k;
