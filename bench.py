@@ -571,12 +571,16 @@ def ilu_bench(n):
     for prec, pn in ((0, "fp64"), (1, "fp32")):
         ctx.ilu_apply(vals, x, y, prec, 1, 3)
         out[f"data_flow_tuned_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 1, 20)
-    # block-ILU(0) on element tiles (block-Jacobi over the tiles): fewer dependent levels, dropped couplings
-    for tile in (16, 32, 64):
+    # block-ILU(0) on element tiles (block-Jacobi over the tiles): fewer dependent levels, dropped couplings;
+    # the per-tile apply (one CTA per tile, the default) and the data-flow apply on the tiled factors
+    for tile in (8, 16, 32, 64):
         ctx.ilu_tile = tile
-        for prec, pn in ((0, "fp64"), (1, "fp32")):
-            ctx.ilu_apply(vals, x, y, prec, 1, 3)
-            out[f"tiled{tile}_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 1, 20)
+        for sched, sn in ((3, "tiles"), (2, "data_flow")):
+            ctx.tile = {"ilu_sched": [sched, sched]}
+            for prec, pn in ((0, "fp64"), (1, "fp32")):
+                ctx.ilu_apply(vals, x, y, prec, 0, 3)
+                out[f"tiled{tile}_{sn}_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 0, 20)
+    ctx.tile = {}
     ctx.ilu_tile = 0
     # bytes one apply must read: the off-diagonal factor blocks and the E diagonal inverses (one matrix's worth)
     out["factor_bytes_fp64"] = L.nnz_blocks * bs * bs * 8

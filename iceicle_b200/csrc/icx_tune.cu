@@ -298,7 +298,7 @@ icx_status icx_tile_set(icx_ctx* c, const icx_tile_choice* t) {
     if (!icx::flow_rows_compiled(bs, t->ilu_rows[k]))
       return fail(c, ICX_ERR_INVALID, "ilu_rows: not compiled for this block size");
     if (t->ilu_ctas[k] < 0 || t->ilu_ctas[k] > MAX_CTAS) return fail(c, ICX_ERR_INVALID, "ilu_ctas: 0..4");
-    if (t->ilu_sched[k] < 0 || t->ilu_sched[k] > 2) return fail(c, ICX_ERR_INVALID, "ilu_sched: 0..2");
+    if (t->ilu_sched[k] < 0 || t->ilu_sched[k] > 3) return fail(c, ICX_ERR_INVALID, "ilu_sched: 0..3");
   }
   TileChoice& d = c->dm.tile;
   d.face_minb = t->face_minb;

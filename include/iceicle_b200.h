@@ -597,7 +597,10 @@ icx_status icx_basis_node_coords(const icx_ctx* ctx, double* xy);
  *               the block size and 24 register values per lane), CTAs per
  *               SM of the persistent grid (1 to 4; capped by occupancy) and the
  *               schedule: 1 completion counters per element, 2 outputs
- *               pre-filled with a sentinel and polled directly (the default) */
+ *               pre-filled with a sentinel and polled directly (the default
+ *               on whole-grid factors), 3 on tiled or grouped factors one CTA
+ *               per tile running the tile's levels between CTA barriers (the
+ *               default there; 2 on whole-grid factors) */
 typedef struct icx_tile_choice {
   int face_minb;
   int vol_threads, vol_minb;
