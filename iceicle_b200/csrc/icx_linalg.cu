@@ -366,6 +366,16 @@ cudaError_t la_maxpy32(long long n, const float* V, long long ld, int nvec, cons
   return cudaGetLastError();
 }
 
+__global__ void scale_kernel(long long n, double a, const double* __restrict__ x, double* __restrict__ y) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = a * x[i];
+}
+
+cudaError_t la_scale(long long n, double a, const double* x, double* y, cudaStream_t s) {
+  scale_kernel<<<grid_for(n), 256, 0, s>>>(n, a, x, y);
+  return cudaGetLastError();
+}
+
 cudaError_t la_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s) {
   axpby_kernel<<<grid_for(n), 256, 0, s>>>(n, a, x, b, y);
   return cudaGetLastError();
@@ -850,7 +860,9 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
       scale_to_f32_kernel<<<grid_for(n), 256, 0, s>>>(n, 1.0 / beta, kb.r, kb.V32);
       GCK(cudaGetLastError());
     } else {
-      GCK(la_axpby(n, 1.0 / beta, kb.r, 0.0, kb.V, s));
+      // v_0 = r / beta, written without reading the basis (a fresh
+      // allocation may hold NaN bit patterns, and 0 * NaN is NaN)
+      GCK(la_scale(n, 1.0 / beta, kb.r, kb.V, s));
     }
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = beta;
@@ -955,7 +967,7 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
     if (beta <= tol || total >= maxit || resid <= tol) break;
     cycle_beta.push_back(beta);
     const int nc = (int)cycle_beta.size() - 1;
-    if (kb.stall_cycles > 0 && nc >= kb.stall_cycles && beta > 0.5 * cycle_beta[nc - kb.stall_cycles]) break;
+    if (kb.stall_cycles > 0 && nc >= kb.stall_cycles && beta > 0.9 * cycle_beta[nc - kb.stall_cycles]) break;
   }
   *iters = total;
   return ICX_OK;

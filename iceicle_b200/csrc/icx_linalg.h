@@ -24,6 +24,8 @@ cudaError_t la_mdot32(LinalgWork& w, long long n, const float* V, long long ld, 
 cudaError_t la_maxpy32(long long n, const float* V, long long ld, int nvec, const double* d_h, double sign, double* w,
                        cudaStream_t s);
 cudaError_t la_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);
+// y = a x (y is not read)
+cudaError_t la_scale(long long n, double a, const double* x, double* y, cudaStream_t s);
 cudaError_t la_xpay(long long n, const double* x, double a, const double* y, double* z, cudaStream_t s);
 // dst[b] = inv(src[blk_index[b]]) for b < nblk (bs x bs blocks); *flag set on a singular block
 cudaError_t la_block_invert(int nblk, int bs, const double* src, const int* blk_index, double* dst, int* flag,
@@ -126,7 +128,7 @@ struct KrylovBuffers {
   double* samples = nullptr;
   int sample_cap = 0, sample_every = 0, sample_count = 0;
   // stall test (0: off): stop when the residual after a restart cycle is above
-  // half the residual `stall_cycles` cycles earlier
+  // 0.9 of the residual `stall_cycles` cycles earlier
   int stall_cycles = 0;
   // optional: replay the Arnoldi steps as CUDA graphs (graph_key != 0; the
   // operators then launch only on the stream they are given, with arguments

@@ -491,8 +491,9 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
     kb.vt = w->vt;
   }
   // the parallel and learned preconditioners give up on a stalled solve
-  // (block-ILU(0) then takes the step)
-  kb.stall_cycles = pc >= 3 ? 10 : 0;
+  // (block-ILU(0) then takes the step): under 10 % residual reduction over
+  // 20 restart cycles
+  kb.stall_cycles = pc >= 3 ? 20 : 0;
   struct CountOut {
     int* dst;
     icx::KrylovBuffers* kb;

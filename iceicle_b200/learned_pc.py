@@ -5,12 +5,12 @@ functions x 4 conserved variables: 36 x 36 Jacobian blocks), Van Leer flux
 with interior penalty, nodes perturbed by a seeded smooth displacement, and a
 Reynolds number drawn per instance uniformly from [50, 500] (viscosity 1/Re).
 
-Training data are generated by the plain solver: at every Newton step of a
-training instance the FD Jacobian is formed and the plain GMRES(30) +
-block-ILU(0) solve of that step records Krylov residuals (its restart
-residuals and every k-th Arnoldi vector); each (Jacobian, residual) pair is
-one training sample, and instances are drawn until the recipe's number of
-pairs is reached. The model then takes Adam steps on that Jacobian's samples
+Training data are generated by the solver the correction is trained for: at
+every Newton step of a training instance the FD Jacobian is formed and the
+GMRES(30) solve of that step with the base preconditioner (block-ILU(0) on
+element tiles) records Krylov residuals (its restart residuals and every
+k-th Arnoldi vector); each (Jacobian, residual) pair is one training sample,
+and instances are drawn until the recipe's number of pairs is reached. The model then takes Adam steps on that Jacobian's samples
 before the Newton step is applied. The correction is trained on top of the
 base preconditioner it is run with (block-ILU(0) on element tiles, exact
 triangular solves). Evaluation runs fresh seeds through the plain all-FP64
@@ -67,10 +67,10 @@ def train(model, train_instances, n=256, samples=167, every=10, steps=150, batch
             rn = float(torch.linalg.vector_norm(res))
             if rn <= 1e-10:
                 break
-            # the samples come from the plain solver (whole-grid block-ILU(0))
-            ctx.ilu_tile = 0
-            ns, its, rr = ctx.krylov_samples(vals, res, du, buf, every=every)
+            # the samples come from the solver the correction is trained for:
+            # GMRES with the base preconditioner (block-ILU(0) on the tiles)
             ctx.ilu_tile = ilu_tile
+            ns, its, rr = ctx.krylov_samples(vals, res, du, buf, every=every)
             if pairs is not None:
                 ns = min(ns, pairs - used)
             used += ns
@@ -110,9 +110,8 @@ def calibrate(model, instance, n=256, samples=167, every=5, sweeps=0, ilu_tile=0
         ctx.form_jacobian_fd(u, res, vals)
         if float(torch.linalg.vector_norm(res)) <= 1e-10:
             break
-        ctx.ilu_tile = 0
-        ns, _, _ = ctx.krylov_samples(vals, res, du, buf, every=every)
         ctx.ilu_tile = ilu_tile
+        ns, _, _ = ctx.krylov_samples(vals, res, du, buf, every=every)
         ctx.lpc_attach(model)
         ab, bb, aa = ctx.lpc_calibrate(vals, buf, ns, sweeps)
         ctx.lpc_attach(None)

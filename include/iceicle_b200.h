@@ -337,7 +337,7 @@ typedef struct icx_newton_report {
   double residual_history[64];
   double alpha_history[64];
   int pc_fallbacks;  /* steps whose linear solve was redone with block-ILU(0) (preconditioners 3-5: the
-                        solve missed gmres_rtol, or stalled: under half the residual reduction over 10
+                        solve missed gmres_rtol, or stalled: under 10 % residual reduction over 20
                         restart cycles) */
   int linear_iterations[64]; /* GMRES iterations of each Newton step (fallback included) */
   int graph_steps;           /* Arnoldi steps replayed from CUDA graphs */
