@@ -340,7 +340,7 @@ static int grid_for(long long n) {
 
 cudaError_t la_mdot(LinalgWork& w, long long n, const double* V, long long ld, int nvec, const double* x,
                     double* d_out, cudaStream_t s) {
-  const int nb = 148 * 2;
+  const int nb = kMdotBlocks;
   mdot_grouped_kernel<double, 8><<<nb, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
   mdot_final_kernel<<<nvec, 256, 0, s>>>(nb, nvec, w.partial, d_out);
   return cudaGetLastError();
@@ -348,7 +348,7 @@ cudaError_t la_mdot(LinalgWork& w, long long n, const double* V, long long ld, i
 
 cudaError_t la_mdot32(LinalgWork& w, long long n, const float* V, long long ld, int nvec, const double* x,
                       double* d_out, cudaStream_t s) {
-  const int nb = 148 * 2;
+  const int nb = kMdotBlocks;
   mdot_grouped_kernel<float, 8><<<nb, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
   mdot_final_kernel<<<nvec, 256, 0, s>>>(nb, nvec, w.partial, d_out);
   return cudaGetLastError();

@@ -8,8 +8,12 @@
 
 namespace icx {
 
+// CTAs of the multi-dot's first stage (8 per SM: enough warps in flight to
+// stream the basis at full bandwidth)
+constexpr int kMdotBlocks = 148 * 8;
+
 struct LinalgWork {
-  double* partial = nullptr;  // [32 vectors][296 blocks] partial dot products
+  double* partial = nullptr;  // [64 vectors][kMdotBlocks] partial dot products
 };
 
 // d_out[j] = V_j . x for j < nvec, V_j = V + j * ld (deterministic two-stage reduction)

@@ -1271,7 +1271,7 @@ icx_status ensure_lm(icx_ctx* c, int m) {
   MCK(cudaMalloc((void**)&s.d_kV, sizeof(double) * (size_t)(m + 1) * n));
   if (s.d_kdh) cudaFree(s.d_kdh);
   MCK(cudaMalloc((void**)&s.d_kdh, sizeof(double) * 3 * (m + 2)));
-  if (!s.lw.partial) MCK(cudaMalloc((void**)&s.lw.partial, sizeof(double) * 64 * 296));
+  if (!s.lw.partial) MCK(cudaMalloc((void**)&s.lw.partial, sizeof(double) * 64 * icx::kMdotBlocks));
   s.kb.n = n;
   s.kb.m = m;
   s.kb.V = s.d_kV;

@@ -152,7 +152,7 @@ icx_status ensure_work(icx_ctx* c, int m) {
     CK(cudaMalloc((void**)&w->order, sizeof(int) * dm.E));
     CK(cudaMemcpy(w->order, order.data(), sizeof(int) * dm.E, cudaMemcpyHostToDevice));
   }
-  CK(cudaMalloc((void**)&w->lw.partial, sizeof(double) * 64 * 296));
+  CK(cudaMalloc((void**)&w->lw.partial, sizeof(double) * 64 * icx::kMdotBlocks));
   CK(cudaMalloc((void**)&w->cnt_rows, sizeof(unsigned) * 2 * dm.E));
   CK(cudaMemset(w->cnt_rows, 0, sizeof(unsigned) * 2 * dm.E));
   if (c->parts.empty() && c->nx > 0 && c->ny > 0 && (long long)c->nx * c->ny == dm.E) {
