@@ -576,98 +576,139 @@ struct IluGroupArgs {
 template <class TA>
 constexpr int group_threads() { return sizeof(TA) == 8 ? 256 : 512; }
 
+// one task's element, rows and neighbour blocks, and its matrix rows
+template <int R, int NS, class TA>
+struct GroupTask {
+  int e, r0, nbk, ks[2];
+  bool live;
+  TA am[3][R][NS];
+};
+
+template <int BS, int R, int NS, int GROUPS, class TA>
+__device__ inline void group_task_load(const IluGroupArgs<TA>& a, bool fwd, int p0, int t, int ntask,
+                                       GroupTask<R, NS, TA>& T) {
+  const int lane = threadIdx.x & 31;
+  T.live = t < ntask;
+  T.nbk = 0;
+  if (!T.live) return;
+  T.e = a.plan.gorder[p0 + t / GROUPS];
+  T.r0 = (t % GROUPS) * R;
+  int b0 = 0;
+  T.ks[0] = T.ks[1] = 0;
+  bool bad = T.e < 0 || T.e >= a.E;
+  if (!bad) {
+    const int d = a.diag[T.e], rb = a.rowptr[T.e], re = a.rowptr[T.e + 1];
+    bad = d < rb || d >= re || rb < 0 || re > a.nnzb;
+    b0 = fwd ? rb : d + 1;
+    T.nbk = (fwd ? d : re) - b0;
+    bad = bad || T.nbk > 2;
+  }
+  // no dynamic indexing, so the task stays in registers
+  if (!bad && T.nbk > 0) {
+    T.ks[0] = a.colidx[b0];
+    bad = T.ks[0] < 0 || T.ks[0] >= a.E;
+  }
+  if (!bad && T.nbk > 1) {
+    T.ks[1] = a.colidx[b0 + 1];
+    bad = T.ks[1] < 0 || T.ks[1] >= a.E;
+  }
+  if (bad) {
+    if (lane == 0) atomicExch(a.err, 2);
+    T.live = false;
+    return;
+  }
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    const TA* Ab = nullptr;
+    if (b < 2 && b < T.nbk) Ab = a.LU + (size_t)(b0 + b) * BS * BS;
+    else if (b == 2 && !fwd) Ab = a.Uinv + (size_t)T.e * BS * BS;
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int r = T.r0 + rr, c = lane + 32 * s;
+        T.am[b][rr][s] = (Ab && r < BS && c < BS) ? Ab[(size_t)r * BS + c] : TA(0);
+      }
+  }
+}
+
+// the same arithmetic in the same order as the data-flow apply:
+// f_e = x_e - sum L_ek f_k; y_e = inv(U_ee) f_e - sum (inv(U_ee) U_ek) y_k
+template <int BS, int R, int NS, class TA>
+__device__ inline void group_task_run(const IluGroupArgs<TA>& a, bool fwd, const GroupTask<R, NS, TA>& T) {
+  if (!T.live) return;  // uniform over the warp
+  const int lane = threadIdx.x & 31;
+  const double* vsrc = fwd ? a.f : a.y;
+  TA xv[3][NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int c = lane + 32 * s;
+#pragma unroll
+    for (int b = 0; b < 2; ++b) xv[b][s] = (b < T.nbk && c < BS) ? (TA)vsrc[(size_t)T.ks[b] * BS + c] : TA(0);
+    xv[2][s] = (!fwd && c < BS) ? (TA)a.f[(size_t)T.e * BS + c] : TA(0);
+  }
+  TA acc[R];
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    if (b < T.nbk) {
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+        for (int s = 0; s < NS; ++s) acc[rr] -= T.am[b][rr][s] * xv[b][s];
+    }
+  }
+  if (!fwd) {
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+      for (int s = 0; s < NS; ++s) acc[rr] += T.am[2][rr][s] * xv[2][s];
+  }
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
+  }
+  TA mine = TA(0);
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr)
+    if (lane == rr) mine = acc[rr];
+  const int r = T.r0 + lane;
+  if (lane < R && r < BS) {
+    if (fwd) a.f[(size_t)T.e * BS + r] = a.x[(size_t)T.e * BS + r] + (double)mine;
+    else a.y[(size_t)T.e * BS + r] = (double)mine;
+  }
+}
+
+// a warp's tasks of one level run two deep: the matrix rows of its next task
+// (which depend on nothing) load while the current one waits for and
+// combines the vectors of earlier levels
 template <int BS, int RT, class TA>
 __global__ void __launch_bounds__(group_threads<TA>()) ilu_apply_group_kernel(IluGroupArgs<TA> a) {
   using K = FlowCfg<BS, RT>;
   constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int g = blockIdx.x;
   const int l0 = a.plan.glev_ptr[g], l1 = a.plan.glev_ptr[g + 1];
   const int nlev = l1 - l0 - 1;
+  GroupTask<R, NS, TA> TA_, TB_;
   for (int sweep = 0; sweep < 2; ++sweep) {
     const bool fwd = sweep == 0;
     for (int li = 0; li < nlev; ++li) {
       const int lv = fwd ? li : nlev - 1 - li;
       const int p0 = a.plan.glev[l0 + lv], p1 = a.plan.glev[l0 + lv + 1];
       const int ntask = (p1 - p0) * GROUPS;
-      for (int t = warp; t < ntask; t += nwarp) {
-        const int e = a.plan.gorder[p0 + t / GROUPS];
-        const int r0 = (t % GROUPS) * R;
-        int nbk = 0, kbs[2], ks[2];
-        bool bad = e < 0 || e >= a.E;
-        if (!bad) {
-          const int d = a.diag[e], rb = a.rowptr[e], re = a.rowptr[e + 1];
-          bad = d < rb || d >= re || rb < 0 || re > a.nnzb;
-          const int b0 = fwd ? rb : d + 1, b1 = fwd ? d : re;
-          bad = bad || (b1 - b0) > 2;
-          for (int kb = b0; !bad && kb < b1; ++kb) {
-            kbs[nbk] = kb;
-            ks[nbk] = a.colidx[kb];
-            bad = ks[nbk] < 0 || ks[nbk] >= a.E;
-            ++nbk;
-          }
-        }
-        if (bad) {
-          if (lane == 0) atomicExch(a.err, 2);
-          continue;  // the CTA keeps to its barriers
-        }
-        // the same arithmetic in the same order as the data-flow apply:
-        // f_e = x_e - sum L_ek f_k; y_e = inv(U_ee) f_e - sum (inv(U_ee) U_ek) y_k
-        TA am[3][R][NS];
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          const TA* Ab = nullptr;
-          if (b < 2 && b < nbk) Ab = a.LU + (size_t)kbs[b] * BS * BS;
-          else if (b == 2 && !fwd) Ab = a.Uinv + (size_t)e * BS * BS;
-#pragma unroll
-          for (int rr = 0; rr < R; ++rr)
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-              const int r = r0 + rr, c = lane + 32 * s;
-              am[b][rr][s] = (Ab && r < BS && c < BS) ? Ab[(size_t)r * BS + c] : TA(0);
-            }
-        }
-        const double* vsrc = fwd ? a.f : a.y;
-        TA xv[3][NS];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-          const int c = lane + 32 * s;
-#pragma unroll
-          for (int b = 0; b < 2; ++b) xv[b][s] = (b < nbk && c < BS) ? (TA)vsrc[(size_t)ks[b] * BS + c] : TA(0);
-          xv[2][s] = (!fwd && c < BS) ? (TA)a.f[(size_t)e * BS + c] : TA(0);
-        }
-        TA acc[R];
-#pragma unroll
-        for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-          if (b < nbk) {
-#pragma unroll
-            for (int rr = 0; rr < R; ++rr)
-#pragma unroll
-              for (int s = 0; s < NS; ++s) acc[rr] -= am[b][rr][s] * xv[b][s];
-          }
-        }
-        if (!fwd) {
-#pragma unroll
-          for (int rr = 0; rr < R; ++rr)
-#pragma unroll
-            for (int s = 0; s < NS; ++s) acc[rr] += am[2][rr][s] * xv[2][s];
-        }
-#pragma unroll
-        for (int rr = 0; rr < R; ++rr) {
-#pragma unroll
-          for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
-        }
-        TA mine = TA(0);
-#pragma unroll
-        for (int rr = 0; rr < R; ++rr)
-          if (lane == rr) mine = acc[rr];
-        const int r = r0 + lane;
-        if (lane < R && r < BS) {
-          if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
-          else a.y[(size_t)e * BS + r] = (double)mine;
-        }
+      int t = warp;
+      group_task_load<BS, R, NS, GROUPS, TA>(a, fwd, p0, t, ntask, TA_);
+      while (t < ntask) {
+        group_task_load<BS, R, NS, GROUPS, TA>(a, fwd, p0, t + nwarp, ntask, TB_);
+        group_task_run<BS, R, NS, TA>(a, fwd, TA_);
+        t += nwarp;
+        if (t >= ntask) break;
+        group_task_load<BS, R, NS, GROUPS, TA>(a, fwd, p0, t + nwarp, ntask, TA_);
+        group_task_run<BS, R, NS, TA>(a, fwd, TB_);
+        t += nwarp;
       }
       __syncthreads();
     }
