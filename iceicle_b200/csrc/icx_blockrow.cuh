@@ -551,17 +551,15 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
 // CTA's own stores before them. No cross-CTA waits, so no polling.
 struct IluGroupPlan {
   int ngroups;
-  const int* gorder;    // elements, group by group, by ascending level within a group
-  const int* glev;      // level boundaries: positions in gorder, group g's at glev[glev_ptr[g] .. glev_ptr[g + 1]]
+  const int4* task;     // [2 E] per position in the group order: {element, first block, k0, k1} of its
+                        // forward (first E) and backward (last E) sweep rows; k = -1: no such block
+  const int* glev;      // level boundaries: positions in the group order, group g's at glev[glev_ptr[g] .. glev_ptr[g + 1]]
   const int* glev_ptr;  // [ngroups + 1]
 };
 
 template <class TA>
 struct IluGroupArgs {
   int E, nnzb;
-  const int* rowptr;
-  const int* colidx;
-  const int* diag;
   const TA* LU;
   const TA* Uinv;
   const double* x;
@@ -576,94 +574,62 @@ struct IluGroupArgs {
 template <class TA>
 constexpr int group_threads() { return sizeof(TA) == 8 ? 256 : 512; }
 
-// one task's element, rows and neighbour blocks, and its matrix rows
-template <int R, int NS, class TA>
-struct GroupTask {
-  int e, r0, nbk, ks[2];
-  bool live;
-  TA am[3][R][NS];
-};
+// levels of a group kept in shared memory (more: read from global memory)
+constexpr int kGroupLevelsSmem = 256;
 
-template <int BS, int R, int NS, int GROUPS, class TA>
-__device__ inline void group_task_load(const IluGroupArgs<TA>& a, bool fwd, int p0, int t, int ntask,
-                                       GroupTask<R, NS, TA>& T) {
+// one task: rows r0 .. r0 + R - 1 of the element's sweep row, with the same
+// arithmetic in the same order as the data-flow apply:
+// f_e = x_e - sum L_ek f_k; y_e = inv(U_ee) f_e - sum (inv(U_ee) U_ek) y_k
+template <int BS, int R, int NS, class TA>
+__device__ inline void group_task_run(const IluGroupArgs<TA>& a, bool fwd, int4 inf, int r0) {
   const int lane = threadIdx.x & 31;
-  T.live = t < ntask;
-  T.nbk = 0;
-  if (!T.live) return;
-  T.e = a.plan.gorder[p0 + t / GROUPS];
-  T.r0 = (t % GROUPS) * R;
-  int b0 = 0;
-  T.ks[0] = T.ks[1] = 0;
-  bool bad = T.e < 0 || T.e >= a.E;
-  if (!bad) {
-    const int d = a.diag[T.e], rb = a.rowptr[T.e], re = a.rowptr[T.e + 1];
-    bad = d < rb || d >= re || rb < 0 || re > a.nnzb;
-    b0 = fwd ? rb : d + 1;
-    T.nbk = (fwd ? d : re) - b0;
-    bad = bad || T.nbk > 2;
-  }
-  // no dynamic indexing, so the task stays in registers
-  if (!bad && T.nbk > 0) {
-    T.ks[0] = a.colidx[b0];
-    bad = T.ks[0] < 0 || T.ks[0] >= a.E;
-  }
-  if (!bad && T.nbk > 1) {
-    T.ks[1] = a.colidx[b0 + 1];
-    bad = T.ks[1] < 0 || T.ks[1] >= a.E;
-  }
-  if (bad) {
+  const int e = inf.x, b0 = inf.y, k0 = inf.z, k1 = inf.w;
+  const int nbk = (k0 >= 0) + (k1 >= 0);
+  const bool bad = e < 0 || e >= a.E || b0 < 0 || b0 + nbk > a.nnzb || k0 >= a.E || k1 >= a.E || (k1 >= 0 && k0 < 0);
+  if (bad) {  // uniform over the warp
     if (lane == 0) atomicExch(a.err, 2);
-    T.live = false;
     return;
   }
+  TA am[3][R][NS];
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
     const TA* Ab = nullptr;
-    if (b < 2 && b < T.nbk) Ab = a.LU + (size_t)(b0 + b) * BS * BS;
-    else if (b == 2 && !fwd) Ab = a.Uinv + (size_t)T.e * BS * BS;
+    if (b < 2 && b < nbk) Ab = a.LU + (size_t)(b0 + b) * BS * BS;
+    else if (b == 2 && !fwd) Ab = a.Uinv + (size_t)e * BS * BS;
 #pragma unroll
     for (int rr = 0; rr < R; ++rr)
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        const int r = T.r0 + rr, c = lane + 32 * s;
-        T.am[b][rr][s] = (Ab && r < BS && c < BS) ? Ab[(size_t)r * BS + c] : TA(0);
+        const int r = r0 + rr, c = lane + 32 * s;
+        am[b][rr][s] = (Ab && r < BS && c < BS) ? Ab[(size_t)r * BS + c] : TA(0);
       }
   }
-}
-
-// the same arithmetic in the same order as the data-flow apply:
-// f_e = x_e - sum L_ek f_k; y_e = inv(U_ee) f_e - sum (inv(U_ee) U_ek) y_k
-template <int BS, int R, int NS, class TA>
-__device__ inline void group_task_run(const IluGroupArgs<TA>& a, bool fwd, const GroupTask<R, NS, TA>& T) {
-  if (!T.live) return;  // uniform over the warp
-  const int lane = threadIdx.x & 31;
   const double* vsrc = fwd ? a.f : a.y;
   TA xv[3][NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     const int c = lane + 32 * s;
-#pragma unroll
-    for (int b = 0; b < 2; ++b) xv[b][s] = (b < T.nbk && c < BS) ? (TA)vsrc[(size_t)T.ks[b] * BS + c] : TA(0);
-    xv[2][s] = (!fwd && c < BS) ? (TA)a.f[(size_t)T.e * BS + c] : TA(0);
+    xv[0][s] = (nbk > 0 && c < BS) ? (TA)vsrc[(size_t)k0 * BS + c] : TA(0);
+    xv[1][s] = (nbk > 1 && c < BS) ? (TA)vsrc[(size_t)k1 * BS + c] : TA(0);
+    xv[2][s] = (!fwd && c < BS) ? (TA)a.f[(size_t)e * BS + c] : TA(0);
   }
   TA acc[R];
 #pragma unroll
   for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
 #pragma unroll
   for (int b = 0; b < 2; ++b) {
-    if (b < T.nbk) {
+    if (b < nbk) {
 #pragma unroll
       for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-        for (int s = 0; s < NS; ++s) acc[rr] -= T.am[b][rr][s] * xv[b][s];
+        for (int s = 0; s < NS; ++s) acc[rr] -= am[b][rr][s] * xv[b][s];
     }
   }
   if (!fwd) {
 #pragma unroll
     for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-      for (int s = 0; s < NS; ++s) acc[rr] += T.am[2][rr][s] * xv[2][s];
+      for (int s = 0; s < NS; ++s) acc[rr] += am[2][rr][s] * xv[2][s];
   }
 #pragma unroll
   for (int rr = 0; rr < R; ++rr) {
@@ -674,44 +640,62 @@ __device__ inline void group_task_run(const IluGroupArgs<TA>& a, bool fwd, const
 #pragma unroll
   for (int rr = 0; rr < R; ++rr)
     if (lane == rr) mine = acc[rr];
-  const int r = T.r0 + lane;
+  const int r = r0 + lane;
   if (lane < R && r < BS) {
-    if (fwd) a.f[(size_t)T.e * BS + r] = a.x[(size_t)T.e * BS + r] + (double)mine;
-    else a.y[(size_t)T.e * BS + r] = (double)mine;
+    if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
+    else a.y[(size_t)e * BS + r] = (double)mine;
   }
 }
 
-// a warp's tasks of one level run two deep: the matrix rows of its next task
-// (which depend on nothing) load while the current one waits for and
-// combines the vectors of earlier levels
+// the group's levels in sweep order: q < nlev forward level q, then the
+// backward levels from the last one down. Each warp's tasks of a level are
+// t = warp, warp + nwarp, ...; the task-table entry of a warp's next task
+// (in this level or, after its last one, its first of the next level) is
+// loaded before the current task runs, so a task costs one dependent trip
+// to memory (its matrix rows and neighbour vectors, loaded together)
 template <int BS, int RT, class TA>
 __global__ void __launch_bounds__(group_threads<TA>()) ilu_apply_group_kernel(IluGroupArgs<TA> a) {
   using K = FlowCfg<BS, RT>;
   constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
+  __shared__ int slev[kGroupLevelsSmem + 1];
   const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int g = blockIdx.x;
   const int l0 = a.plan.glev_ptr[g], l1 = a.plan.glev_ptr[g + 1];
   const int nlev = l1 - l0 - 1;
-  GroupTask<R, NS, TA> TA_, TB_;
-  for (int sweep = 0; sweep < 2; ++sweep) {
-    const bool fwd = sweep == 0;
-    for (int li = 0; li < nlev; ++li) {
-      const int lv = fwd ? li : nlev - 1 - li;
-      const int p0 = a.plan.glev[l0 + lv], p1 = a.plan.glev[l0 + lv + 1];
-      const int ntask = (p1 - p0) * GROUPS;
-      int t = warp;
-      group_task_load<BS, R, NS, GROUPS, TA>(a, fwd, p0, t, ntask, TA_);
-      while (t < ntask) {
-        group_task_load<BS, R, NS, GROUPS, TA>(a, fwd, p0, t + nwarp, ntask, TB_);
-        group_task_run<BS, R, NS, TA>(a, fwd, TA_);
-        t += nwarp;
-        if (t >= ntask) break;
-        group_task_load<BS, R, NS, GROUPS, TA>(a, fwd, p0, t + nwarp, ntask, TA_);
-        group_task_run<BS, R, NS, TA>(a, fwd, TB_);
-        t += nwarp;
+  const bool in_smem = nlev <= kGroupLevelsSmem;
+  if (in_smem)
+    for (int i = threadIdx.x; i <= nlev; i += blockDim.x) slev[i] = a.plan.glev[l0 + i];
+  __syncthreads();
+  auto lev = [&](int i) { return in_smem ? slev[i] : a.plan.glev[l0 + i]; };
+  const int nq = 2 * nlev;
+  int4 inf = make_int4(-1, 0, -1, -1);
+  bool have = false;
+  for (int q = 0; q < nq; ++q) {
+    const bool fwd = q < nlev;
+    const int lv = fwd ? q : nq - 1 - q;
+    const int p0 = lev(lv), ntask = (lev(lv + 1) - p0) * GROUPS;
+    const int4* tk = a.plan.task + (fwd ? 0 : a.E);
+    if (!have && warp < ntask) inf = tk[p0 + warp / GROUPS];
+    have = false;
+    for (int t = warp; t < ntask; t += nwarp) {
+      int4 nxt = inf;
+      const int tn = t + nwarp;
+      if (tn < ntask) {
+        nxt = tk[p0 + tn / GROUPS];
+        have = true;
+      } else if (q + 1 < nq) {
+        const bool fn = q + 1 < nlev;
+        const int ln = fn ? q + 1 : nq - 2 - q;
+        const int pn = lev(ln), nn = (lev(ln + 1) - pn) * GROUPS;
+        if (warp < nn) {
+          nxt = a.plan.task[(fn ? 0 : a.E) + pn + warp / GROUPS];
+          have = true;
+        }
       }
-      __syncthreads();
+      group_task_run<BS, R, NS, TA>(a, fwd, inf, (t % GROUPS) * R);
+      inf = nxt;
     }
+    __syncthreads();
   }
 }
 

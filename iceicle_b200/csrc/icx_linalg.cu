@@ -553,7 +553,7 @@ static const void* group_kernel_for(int rows) {
 }
 
 template <class TA>
-static cudaError_t ilu_apply_groups_t(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+static cudaError_t ilu_apply_groups_t(const DeviceMesh& dm, int ngroups, const int* task, const int* glev,
                                       const int* glev_ptr, int rows, const TA* LU, const TA* Uinv, const double* x,
                                       double* y, double* f, int* err, cudaStream_t s) {
   if (ngroups <= 0) return cudaErrorInvalidValue;
@@ -564,22 +564,22 @@ static cudaError_t ilu_apply_groups_t(const DeviceMesh& dm, int ngroups, const i
   ICX_BLOCK_SIZES(ICX_ILUG_CASE)
 #undef ICX_ILUG_CASE
   if (!kern) return cudaErrorInvalidValue;
-  IluGroupArgs<TA> args{dm.E, dm.nnzb, dm.bsr_rowptr, dm.bsr_colidx, dm.bsr_diag, LU, Uinv, x, f, y, err,
-                        IluGroupPlan{ngroups, gorder, glev, glev_ptr}};
+  IluGroupArgs<TA> args{dm.E, dm.nnzb, LU, Uinv, x, f, y, err,
+                        IluGroupPlan{ngroups, reinterpret_cast<const int4*>(task), glev, glev_ptr}};
   void* params[] = {&args};
   return cudaLaunchKernel(kern, dim3(ngroups), dim3(group_threads<TA>()), params, 0, s);
 }
 
-cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, int ngroups, const int* task, const int* glev,
                                 const int* glev_ptr, int rows, const double* LU, const double* Uinv, const double* x,
                                 double* y, double* f, int* err, cudaStream_t s) {
-  return ilu_apply_groups_t<double>(dm, ngroups, gorder, glev, glev_ptr, rows, LU, Uinv, x, y, f, err, s);
+  return ilu_apply_groups_t<double>(dm, ngroups, task, glev, glev_ptr, rows, LU, Uinv, x, y, f, err, s);
 }
 
-cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, int ngroups, const int* task, const int* glev,
                                     const int* glev_ptr, int rows, const float* LU, const float* Uinv,
                                     const double* x, double* y, double* f, int* err, cudaStream_t s) {
-  return ilu_apply_groups_t<float>(dm, ngroups, gorder, glev, glev_ptr, rows, LU, Uinv, x, y, f, err, s);
+  return ilu_apply_groups_t<float>(dm, ngroups, task, glev, glev_ptr, rows, LU, Uinv, x, y, f, err, s);
 }
 
 int flow_rows_default(int bs) {

@@ -75,12 +75,13 @@ cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, const int* order, const 
                                   unsigned epoch, int* err, cudaStream_t s);
 // the same apply on element groups (tiles) whose factors couple no two
 // groups: one CTA per group, levels of the group in turn (no cross-CTA
-// waits); gorder / glev / glev_ptr as IluGroupPlan (icx_blockrow.cuh); rows =
+// waits); task (4 ints per entry, 16-byte aligned) / glev / glev_ptr as
+// IluGroupPlan (icx_blockrow.cuh); rows =
 // rows per warp task (0: the default); *err = 2 on an index out of range
-cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, int ngroups, const int* task, const int* glev,
                                 const int* glev_ptr, int rows, const double* LU, const double* Uinv, const double* x,
                                 double* y, double* f, int* err, cudaStream_t s);
-cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, int ngroups, const int* gorder, const int* glev,
+cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, int ngroups, const int* task, const int* glev,
                                     const int* glev_ptr, int rows, const float* LU, const float* Uinv,
                                     const double* x, double* y, double* f, int* err, cudaStream_t s);
 cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s);

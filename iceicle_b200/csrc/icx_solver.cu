@@ -42,8 +42,9 @@ struct IluTilePlan {
   // the same per group (one CTA per group, la_ilu_apply_groups): elements
   // group by group, by level within the group, and each group's level bounds
   int ngroups = 0;
-  int* gorder = nullptr;        // [E]
-  int* glev = nullptr;          // level boundaries (positions in gorder), per group
+  bool group_ok = true;         // no sweep row has more than two off-diagonal blocks
+  int* gtask = nullptr;         // [2 E] x 4: IluGroupPlan::task, in group order (group, level, element)
+  int* glev = nullptr;          // level boundaries (positions in the group order), per group
   int* glev_ptr = nullptr;      // [ngroups + 1] into glev
 };
 
@@ -179,7 +180,7 @@ icx_status ensure_work(icx_ctx* c, int m) {
 }
 
 void free_tile_plan(IluTilePlan& tp) {
-  for (int* p : {tp.rowptr, tp.colidx, tp.diag, tp.map, tp.order, tp.gorder, tp.glev, tp.glev_ptr})
+  for (int* p : {tp.rowptr, tp.colidx, tp.diag, tp.map, tp.order, tp.gtask, tp.glev, tp.glev_ptr})
     if (p) cudaFree(p);
   tp = IluTilePlan();
 }
@@ -244,9 +245,22 @@ icx_status ensure_ilu_plan(icx_ctx* c) {
   std::vector<std::array<int, 3>> key(dm.E);
   for (int e = 0; e < dm.E; ++e) key[e] = {gid_of[tile_of(e)], lvl[e], e};
   std::sort(key.begin(), key.end());
-  std::vector<int> gorder(dm.E), glev, glev_ptr(1, 0);
+  std::vector<int> gtask(8 * (size_t)dm.E), glev, glev_ptr(1, 0);
   for (int p = 0; p < dm.E; ++p) {
-    gorder[p] = key[p][2];
+    // each sweep row's off-diagonal blocks (kept pattern): forward the ones
+    // before the diagonal, backward the ones after it; at most two of each
+    // (more: the entry is marked invalid, and the data-flow apply runs instead)
+    const int e = key[p][2];
+    const int sweeps[2][2] = {{trp[e], tdiag[e]}, {tdiag[e] + 1, trp[e + 1]}};
+    for (int sw = 0; sw < 2; ++sw) {
+      int* t = &gtask[4 * ((size_t)sw * dm.E + p)];
+      const int b0 = sweeps[sw][0], nb = sweeps[sw][1] - b0;
+      t[0] = nb > 2 ? -1 : e;
+      tp.group_ok = tp.group_ok && nb <= 2;
+      t[1] = b0;
+      t[2] = nb > 0 ? tci[b0] : -1;
+      t[3] = nb > 1 ? tci[b0 + 1] : -1;
+    }
     const bool new_group = p == 0 || key[p][0] != key[p - 1][0];
     if (new_group && p > 0) {
       glev.push_back(p);  // the previous group's end
@@ -259,7 +273,7 @@ icx_status ensure_ilu_plan(icx_ctx* c) {
   tp.ngroups = ng;
   const std::pair<int**, const std::vector<int>*> up[] = {
       {&tp.rowptr, &trp}, {&tp.colidx, &tci}, {&tp.diag, &tdiag}, {&tp.map, &tmap}, {&tp.order, &order},
-      {&tp.gorder, &gorder}, {&tp.glev, &glev}, {&tp.glev_ptr, &glev_ptr}};
+      {&tp.gtask, &gtask}, {&tp.glev, &glev}, {&tp.glev_ptr, &glev_ptr}};
   for (const auto& u : up) {
     cudaError_t e = cudaMalloc((void**)u.first, sizeof(int) * u.second->size());
     if (e == cudaSuccess) e = cudaMemcpy(*u.first, u.second->data(), sizeof(int) * u.second->size(),
@@ -342,12 +356,12 @@ cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStr
   const int* order = ilu_order(c);
   const int pi = mixed ? 1 : 0;
   const int rows = dm.tile.flow_rows[pi] ? dm.tile.flow_rows[pi] : icx::flow_rows_default(w->bs);
-  if (w->tp.tile && icx::ilu_schedule(dm.tile, pi, true) == 3) {
+  if (w->tp.tile && w->tp.group_ok && icx::ilu_schedule(dm.tile, pi, true) == 3) {
     // tiled / grouped factors: one CTA per group, no waits across CTAs
     const IluTilePlan& tp = w->tp;
-    return mixed ? icx::la_ilu_apply_groups_f32(dm, tp.ngroups, tp.gorder, tp.glev, tp.glev_ptr, rows, w->pc32,
+    return mixed ? icx::la_ilu_apply_groups_f32(dm, tp.ngroups, tp.gtask, tp.glev, tp.glev_ptr, rows, w->pc32,
                                                 w->uinv32, x, z, w->pct, w->pc_err, s)
-                 : icx::la_ilu_apply_groups(dm, tp.ngroups, tp.gorder, tp.glev, tp.glev_ptr, rows, w->pc, w->uinv,
+                 : icx::la_ilu_apply_groups(dm, tp.ngroups, tp.gtask, tp.glev, tp.glev_ptr, rows, w->pc, w->uinv,
                                             x, z, w->pct, w->pc_err, s);
   }
   // the sentinel schedule uses neither the counters nor the epoch
@@ -1102,7 +1116,7 @@ bool solver_graphable(icx_ctx* c, int pc, bool mixed) {
   if (pc != 2) return false;
   // the group apply and the sentinel schedule launch the same arguments every time
   const int pi = mixed ? 1 : 0;
-  if (w->tp.tile && ilu_schedule(c->dm.tile, pi, true) == 3) return true;
+  if (w->tp.tile && w->tp.group_ok && ilu_schedule(c->dm.tile, pi, true) == 3) return true;
   return flow_sentinel(c->dm.tile, pi) && !(w->rows_ok && w->schedule == 2);
 }
 

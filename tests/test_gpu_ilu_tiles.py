@@ -6,6 +6,9 @@
   (FP64 factors) and 1e-5 (FP32 factors).
 * A tile at least as large as the grid is plain ILU(0): bit-identical to the
   untiled apply.
+* The per-tile apply (one CTA per tile, levels in turn) and the data-flow
+  apply of the same tiled factors are bit-identical for every compiled rows
+  per task, in FP64 and FP32 factors, on ragged tiles.
 * The preconditioner changes GMRES iterations only: Newton with tiled ILU
   reaches the untiled converged state to 1e-10 of the initial state's L2
   norm (the steady state of this Burgers problem is u = 0).
@@ -95,6 +98,30 @@ def test_tiled_apply_matches_numpy(kw, tile):
             torch.cuda.synchronize()
             err = np.abs(y.cpu().numpy() - y_ref).max()
             assert err <= tol * np.abs(y_ref).max(), (precision, err)
+    ctx.close()
+
+
+@pytest.mark.parametrize("kw,tile", [(dict(pde=NS, nx=13, ny=11, p=2, ip=True), 4),
+                                     (dict(pde=NS, nx=9, ny=10, p=2, ip=True), 8),
+                                     (dict(pde=BURGERS, nx=12, ny=7, p=3, ip=True), 5)])
+def test_tile_apply_equals_data_flow_apply_bitwise(kw, tile):
+    spec = Spec(**kw)
+    ctx = spec.context()
+    vals, _, _, _ = _jacobian(ctx, spec)
+    ctx.ilu_tile = tile
+    x = torch.from_numpy(np.random.default_rng(11).standard_normal(ctx.layout.n_dof)).cuda()
+    for precision in (0, 1):
+        for rows in (2, 4, 6, 8):
+            ys = []
+            for sched in (3, 2):
+                ctx.tile = {"ilu_sched": [sched, sched], "ilu_rows": [rows, rows]}
+                y = torch.full_like(x, float("nan"))
+                ctx.ilu_apply(vals, x, y, precision, 1, repeat=2)
+                ys.append(y)
+            torch.cuda.synchronize()
+            assert torch.isfinite(ys[0]).all()
+            assert torch.equal(ys[0].view(torch.int64), ys[1].view(torch.int64)), (precision, rows)
+    ctx.tile = {}
     ctx.close()
 
 
