@@ -575,7 +575,7 @@ def ilu_bench(n):
     # the per-tile apply (one CTA per tile, the default) and the data-flow apply on the tiled factors
     for tile in (8, 16, 32, 64):
         ctx.ilu_tile = tile
-        for sched, sn in ((3, "tiles"), (2, "data_flow")):
+        for sched, sn in ((4, "staged"), (3, "tiles"), (2, "data_flow")):
             ctx.tile = {"ilu_sched": [sched, sched]}
             for prec, pn in ((0, "fp64"), (1, "fp32")):
                 ctx.ilu_apply(vals, x, y, prec, 0, 3)

@@ -555,6 +555,7 @@ struct IluGroupPlan {
                         // forward (first E) and backward (last E) sweep rows; k = -1: no such block
   const int* glev;      // level boundaries: positions in the group order, group g's at glev[glev_ptr[g] .. glev_ptr[g + 1]]
   const int* glev_ptr;  // [ngroups + 1]
+  int gmax;             // elements of the largest group
 };
 
 template <class TA>
@@ -697,6 +698,180 @@ __global__ void __launch_bounds__(group_threads<TA>()) ilu_apply_group_kernel(Il
     }
     __syncthreads();
   }
+}
+
+// the group apply with the matrix rows staged in shared memory: each warp
+// copies the rows of its next D tasks (cp.async, no registers held) into its
+// own ring of D slots while it runs the current one, across level barriers
+// (the factors are read-only), so a task waits only for its neighbours'
+// vectors; the group's task-table entries are staged once at the start.
+// Dynamic shared memory: 2 gmax entries (int4), then nwarp x D slots of
+// group_slot_bytes<BS, R, TA>() bytes. Same arithmetic in the same order as
+// ilu_apply_group_kernel (bit-identical results).
+template <int BS, int R, class TA>
+__host__ __device__ constexpr int group_slot_bytes() {
+  return ((3 * R * BS * (int)sizeof(TA)) + 15) / 16 * 16;
+}
+
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ inline void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// copies n bytes (a multiple of CH, both addresses CH-aligned) over the warp
+template <int CH>
+__device__ inline void cp_async_span(void* sdst, const void* gsrc, int n) {
+  const int lane = threadIdx.x & 31;
+  const unsigned d0 = (unsigned)__cvta_generic_to_shared(sdst);
+  const char* s0 = (const char*)gsrc;
+  for (int o = lane * CH; o < n; o += 32 * CH) {
+    if constexpr (CH == 16)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d0 + o), "l"(s0 + o) : "memory");
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d0 + o), "l"(s0 + o), "n"(CH) : "memory");
+  }
+}
+
+template <int BS, int R, class TA>
+__device__ inline bool group_task_ok(const IluGroupArgs<TA>& a, int4 inf) {
+  const int nbk = (inf.z >= 0) + (inf.w >= 0);
+  return !(inf.x < 0 || inf.x >= a.E || inf.y < 0 || inf.y + nbk > a.nnzb || inf.z >= a.E || inf.w >= a.E ||
+           (inf.w >= 0 && inf.z < 0));
+}
+
+template <int BS, int RT, class TA, int D>
+__global__ void __launch_bounds__(group_threads<TA>()) ilu_apply_group_async_kernel(IluGroupArgs<TA> a) {
+  using K = FlowCfg<BS, RT>;
+  constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
+  constexpr int SLOT = group_slot_bytes<BS, R, TA>();
+  constexpr int CH = (BS * (int)sizeof(TA)) % 16 == 0 ? 16 : (int)sizeof(TA);
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ int slev[kGroupLevelsSmem + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int g = blockIdx.x;
+  const int l0 = a.plan.glev_ptr[g], l1 = a.plan.glev_ptr[g + 1];
+  const int nlev = l1 - l0 - 1;
+  const int pg0 = a.plan.glev[l0], G = a.plan.glev[l1 - 1] - pg0;
+  // the launch guarantees G <= gmax and nlev <= kGroupLevelsSmem; a plan
+  // that breaks either is reported, not run
+  if (nlev > kGroupLevelsSmem || G > a.plan.gmax || G < 0) {
+    if (threadIdx.x == 0) atomicExch(a.err, 2);
+    return;
+  }
+  int4* sinfo = reinterpret_cast<int4*>(dsm);
+  unsigned char* ring = dsm + (size_t)2 * a.plan.gmax * sizeof(int4) + (size_t)warp * D * SLOT;
+  for (int i = threadIdx.x; i <= nlev; i += blockDim.x) slev[i] = a.plan.glev[l0 + i];
+  for (int i = threadIdx.x; i < G; i += blockDim.x) {
+    sinfo[i] = a.plan.task[pg0 + i];
+    sinfo[G + i] = a.plan.task[a.E + pg0 + i];
+  }
+  __syncthreads();
+  const int nq = 2 * nlev;
+  auto ntask = [&](int q) {
+    const int lv = q < nlev ? q : nq - 1 - q;
+    return (slev[lv + 1] - slev[lv]) * GROUPS;
+  };
+  auto info = [&](int q, int t) {
+    const bool fwd = q < nlev;
+    const int lv = fwd ? q : nq - 1 - q;
+    return sinfo[(fwd ? 0 : G) + slev[lv] - pg0 + t / GROUPS];
+  };
+  // the issue cursor: the warp's next task whose rows are not yet requested
+  int qi = 0, ti = warp;
+  while (qi < nq && ti >= ntask(qi)) ++qi;
+  auto issue = [&](int slot) {
+    if (qi < nq) {
+      const bool fwd = qi < nlev;
+      const int4 inf = info(qi, ti);
+      if (group_task_ok<BS, R, TA>(a, inf)) {
+        const int r0 = (ti % GROUPS) * R;
+        const int nr = BS - r0 < R ? BS - r0 : R;
+        const int nbk = (inf.z >= 0) + (inf.w >= 0);
+        unsigned char* dst = ring + (size_t)slot * SLOT;
+        for (int b = 0; b < 3; ++b) {
+          const TA* src = nullptr;
+          if (b < 2 && b < nbk) src = a.LU + (size_t)(inf.y + b) * BS * BS;
+          else if (b == 2 && !fwd) src = a.Uinv + (size_t)inf.x * BS * BS;
+          if (src) cp_async_span<CH>(dst + (size_t)b * R * BS * sizeof(TA), src + (size_t)r0 * BS,
+                                     nr * BS * (int)sizeof(TA));
+        }
+      }
+      ti += nwarp;
+      while (qi < nq && ti >= ntask(qi)) {
+        ++qi;
+        ti = warp;
+      }
+    }
+    cp_async_commit();  // possibly empty: one group per task keeps the count
+  };
+#pragma unroll
+  for (int d = 0; d < D; ++d) issue(d);
+  int n = 0;
+  for (int q = 0; q < nq; ++q) {
+    const bool fwd = q < nlev;
+    const int nt = ntask(q);
+    for (int t = warp; t < nt; t += nwarp, ++n) {
+      cp_async_wait<D - 1>();
+      __syncwarp();
+      const int4 inf = info(q, t);
+      const int slot = n % D;
+      if (!group_task_ok<BS, R, TA>(a, inf)) {
+        if (lane == 0) atomicExch(a.err, 2);
+      } else {
+        const TA* am = reinterpret_cast<const TA*>(ring + (size_t)slot * SLOT);
+        const int e = inf.x, k0 = inf.z, k1 = inf.w, r0 = (t % GROUPS) * R;
+        const int nbk = (k0 >= 0) + (k1 >= 0);
+        const double* vsrc = fwd ? a.f : a.y;
+        TA xv[3][NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const int c = lane + 32 * s;
+          xv[0][s] = (nbk > 0 && c < BS) ? (TA)vsrc[(size_t)k0 * BS + c] : TA(0);
+          xv[1][s] = (nbk > 1 && c < BS) ? (TA)vsrc[(size_t)k1 * BS + c] : TA(0);
+          xv[2][s] = (!fwd && c < BS) ? (TA)a.f[(size_t)e * BS + c] : TA(0);
+        }
+        auto mat = [&](int b, int rr, int s) {
+          const int c = lane + 32 * s;
+          return (r0 + rr < BS && c < BS) ? am[(b * R + rr) * BS + c] : TA(0);
+        };
+        TA acc[R];
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) acc[rr] = TA(0);
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          if (b < nbk) {
+#pragma unroll
+            for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+              for (int s = 0; s < NS; ++s) acc[rr] -= mat(b, rr, s) * xv[b][s];
+          }
+        }
+        if (!fwd) {
+#pragma unroll
+          for (int rr = 0; rr < R; ++rr)
+#pragma unroll
+            for (int s = 0; s < NS; ++s) acc[rr] += mat(2, rr, s) * xv[2][s];
+        }
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
+        }
+        TA mine = TA(0);
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr)
+          if (lane == rr) mine = acc[rr];
+        const int r = r0 + lane;
+        if (lane < R && r < BS) {
+          if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
+          else a.y[(size_t)e * BS + r] = (double)mine;
+        }
+      }
+      __syncwarp();  // the slot is read by every lane before it is refilled
+      issue(slot);
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
 }
 
 #define ICX_BLOCK_SIZES(X) X(4) X(9) X(16) X(25) X(36) X(64) X(100)

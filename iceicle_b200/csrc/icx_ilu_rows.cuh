@@ -80,9 +80,7 @@ __device__ inline void cp_async_16(void* sdst, const void* gsrc) {
   unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
-__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ inline void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+// cp_async_commit / cp_async_wait<N>: icx_blockrow.cuh
 
 // copy `count` TA values (a multiple of 16 bytes when `vec16`) from global to shared
 template <class TA>

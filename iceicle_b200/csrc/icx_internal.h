@@ -71,11 +71,13 @@ constexpr int kFlowSchedDefault = 2;
 inline bool flow_sentinel(const TileChoice& t, int pi) {
   return (t.flow_sched[pi] ? t.flow_sched[pi] : kFlowSchedDefault) == 2;
 }
-// schedule 3: the apply on element tiles / groups with one CTA per group
-// (la_ilu_apply_groups), the default when the factors are tiled or grouped
+// schedules 3 and 4: the apply on element tiles / groups with one CTA per
+// group (la_ilu_apply_groups), 4 with the matrix rows staged in shared
+// memory where they fit; 4 is the default when the factors are tiled or grouped
+constexpr int kGroupSchedDefault = 4;
 inline int ilu_schedule(const TileChoice& t, int pi, bool grouped) {
-  const int sc = t.flow_sched[pi] ? t.flow_sched[pi] : (grouped ? 3 : kFlowSchedDefault);
-  return (sc == 3 && !grouped) ? kFlowSchedDefault : sc;
+  const int sc = t.flow_sched[pi] ? t.flow_sched[pi] : (grouped ? kGroupSchedDefault : kFlowSchedDefault);
+  return (sc >= 3 && !grouped) ? kFlowSchedDefault : sc;
 }
 
 // compiled volume tiles: threads per CTA and the resident CTAs per SM of the

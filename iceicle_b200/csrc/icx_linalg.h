@@ -78,12 +78,20 @@ cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, const int* order, const 
 // waits); task (4 ints per entry, 16-byte aligned) / glev / glev_ptr as
 // IluGroupPlan (icx_blockrow.cuh); rows =
 // rows per warp task (0: the default); *err = 2 on an index out of range
-cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, int ngroups, const int* task, const int* glev,
+// the plan's shape: groups, elements of the largest group, most levels of
+// a group, and whether the staged kernel (matrix rows in shared memory) may
+// run where it fits
+struct IluGroupShape {
+  int ngroups, gmax, nlev_max;
+  bool staged;
+};
+cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, const IluGroupShape& gs, const int* task, const int* glev,
                                 const int* glev_ptr, int rows, const double* LU, const double* Uinv, const double* x,
                                 double* y, double* f, int* err, cudaStream_t s);
-cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, int ngroups, const int* task, const int* glev,
-                                    const int* glev_ptr, int rows, const float* LU, const float* Uinv,
-                                    const double* x, double* y, double* f, int* err, cudaStream_t s);
+cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, const IluGroupShape& gs, const int* task,
+                                    const int* glev, const int* glev_ptr, int rows, const float* LU,
+                                    const float* Uinv, const double* x, double* y, double* f, int* err,
+                                    cudaStream_t s);
 cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s);
 cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s);
 cudaError_t la_f2d(long long n, const float* x, double* y, cudaStream_t s);

@@ -42,6 +42,8 @@ struct IluTilePlan {
   // the same per group (one CTA per group, la_ilu_apply_groups): elements
   // group by group, by level within the group, and each group's level bounds
   int ngroups = 0;
+  int gmax = 0;                 // elements of the largest group
+  int nlev_max = 0;             // most levels of a group
   bool group_ok = true;         // no sweep row has more than two off-diagonal blocks
   int* gtask = nullptr;         // [2 E] x 4: IluGroupPlan::task, in group order (group, level, element)
   int* glev = nullptr;          // level boundaries (positions in the group order), per group
@@ -271,6 +273,10 @@ icx_status ensure_ilu_plan(icx_ctx* c) {
   glev.push_back(dm.E);
   glev_ptr.push_back((int)glev.size());
   tp.ngroups = ng;
+  for (int g = 0; g < ng; ++g) {
+    tp.gmax = std::max(tp.gmax, glev[glev_ptr[g + 1] - 1] - glev[glev_ptr[g]]);
+    tp.nlev_max = std::max(tp.nlev_max, glev_ptr[g + 1] - glev_ptr[g] - 1);
+  }
   const std::pair<int**, const std::vector<int>*> up[] = {
       {&tp.rowptr, &trp}, {&tp.colidx, &tci}, {&tp.diag, &tdiag}, {&tp.map, &tmap}, {&tp.order, &order},
       {&tp.gtask, &gtask}, {&tp.glev, &glev}, {&tp.glev_ptr, &glev_ptr}};
@@ -356,12 +362,14 @@ cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStr
   const int* order = ilu_order(c);
   const int pi = mixed ? 1 : 0;
   const int rows = dm.tile.flow_rows[pi] ? dm.tile.flow_rows[pi] : icx::flow_rows_default(w->bs);
-  if (w->tp.tile && w->tp.group_ok && icx::ilu_schedule(dm.tile, pi, true) == 3) {
+  const int gsched = icx::ilu_schedule(dm.tile, pi, true);
+  if (w->tp.tile && w->tp.group_ok && gsched >= 3) {
     // tiled / grouped factors: one CTA per group, no waits across CTAs
     const IluTilePlan& tp = w->tp;
-    return mixed ? icx::la_ilu_apply_groups_f32(dm, tp.ngroups, tp.gtask, tp.glev, tp.glev_ptr, rows, w->pc32,
+    const icx::IluGroupShape gs{tp.ngroups, tp.gmax, tp.nlev_max, gsched == 4};
+    return mixed ? icx::la_ilu_apply_groups_f32(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, w->pc32,
                                                 w->uinv32, x, z, w->pct, w->pc_err, s)
-                 : icx::la_ilu_apply_groups(dm, tp.ngroups, tp.gtask, tp.glev, tp.glev_ptr, rows, w->pc, w->uinv,
+                 : icx::la_ilu_apply_groups(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, w->pc, w->uinv,
                                             x, z, w->pct, w->pc_err, s);
   }
   // the sentinel schedule uses neither the counters nor the epoch
@@ -1116,7 +1124,7 @@ bool solver_graphable(icx_ctx* c, int pc, bool mixed) {
   if (pc != 2) return false;
   // the group apply and the sentinel schedule launch the same arguments every time
   const int pi = mixed ? 1 : 0;
-  if (w->tp.tile && w->tp.group_ok && ilu_schedule(c->dm.tile, pi, true) == 3) return true;
+  if (w->tp.tile && w->tp.group_ok && ilu_schedule(c->dm.tile, pi, true) >= 3) return true;
   return flow_sentinel(c->dm.tile, pi) && !(w->rows_ok && w->schedule == 2);
 }
 

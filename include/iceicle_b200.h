@@ -599,8 +599,10 @@ icx_status icx_basis_node_coords(const icx_ctx* ctx, double* xy);
  *               schedule: 1 completion counters per element, 2 outputs
  *               pre-filled with a sentinel and polled directly (the default
  *               on whole-grid factors), 3 on tiled or grouped factors one CTA
- *               per tile running the tile's levels between CTA barriers (the
- *               default there; 2 on whole-grid factors) */
+ *               per tile running the tile's levels between CTA barriers, 4 the
+ *               same with each warp's next task rows copied ahead into shared
+ *               memory (the default there; 3 where they do not fit; both 2 on
+ *               whole-grid factors) */
 typedef struct icx_tile_choice {
   int face_minb;
   int vol_threads, vol_minb;

@@ -6,9 +6,10 @@
   (FP64 factors) and 1e-5 (FP32 factors).
 * A tile at least as large as the grid is plain ILU(0): bit-identical to the
   untiled apply.
-* The per-tile apply (one CTA per tile, levels in turn) and the data-flow
-  apply of the same tiled factors are bit-identical for every compiled rows
-  per task, in FP64 and FP32 factors, on ragged tiles.
+* The per-tile applies (one CTA per tile, levels in turn; matrix rows in
+  registers or staged in shared memory) and the data-flow apply of the same
+  tiled factors are bit-identical for every compiled rows per task, in FP64
+  and FP32 factors, on ragged tiles.
 * The preconditioner changes GMRES iterations only: Newton with tiled ILU
   reaches the untiled converged state to 1e-10 of the initial state's L2
   norm (the steady state of this Burgers problem is u = 0).
@@ -113,14 +114,15 @@ def test_tile_apply_equals_data_flow_apply_bitwise(kw, tile):
     for precision in (0, 1):
         for rows in (2, 4, 6, 8):
             ys = []
-            for sched in (3, 2):
+            for sched in (4, 3, 2):
                 ctx.tile = {"ilu_sched": [sched, sched], "ilu_rows": [rows, rows]}
                 y = torch.full_like(x, float("nan"))
                 ctx.ilu_apply(vals, x, y, precision, 1, repeat=2)
                 ys.append(y)
             torch.cuda.synchronize()
             assert torch.isfinite(ys[0]).all()
-            assert torch.equal(ys[0].view(torch.int64), ys[1].view(torch.int64)), (precision, rows)
+            for y in ys[1:]:
+                assert torch.equal(ys[0].view(torch.int64), y.view(torch.int64)), (precision, rows)
     ctx.tile = {}
     ctx.close()
 
