@@ -19,6 +19,12 @@ enum BlockRowMode {
   BR_DIAG = 3    // block-diagonal storage D[e] (one block per row, column = row)
 };
 
+// a * b + c rounded once: the ILU applies state every product-sum as an
+// explicit fused multiply-add, so their variants round alike whatever the
+// compiler would contract
+__device__ inline float fused_madd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ inline double fused_madd(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // the block rows 0..nrows-1 of one launch
 struct RowSet {
   int nx, ny, level, nrows;
@@ -504,7 +510,7 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
 #pragma unroll
           for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-            for (int s = 0; s < NS; ++s) acc[rr] -= am[b][rr][s] * xv[b][s];
+            for (int s = 0; s < NS; ++s) acc[rr] = fused_madd(-am[b][rr][s], xv[b][s], acc[rr]);
         }
       }
       if (!fwd) {
@@ -512,7 +518,7 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
 #pragma unroll
         for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-          for (int s = 0; s < NS; ++s) acc[rr] += am[2][rr][s] * xv[2][s];
+          for (int s = 0; s < NS; ++s) acc[rr] = fused_madd(am[2][rr][s], xv[2][s], acc[rr]);
       }
 #pragma unroll
       for (int rr = 0; rr < R; ++rr) {
@@ -623,14 +629,14 @@ __device__ inline void group_task_run(const IluGroupArgs<TA>& a, bool fwd, int4 
 #pragma unroll
       for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-        for (int s = 0; s < NS; ++s) acc[rr] -= am[b][rr][s] * xv[b][s];
+        for (int s = 0; s < NS; ++s) acc[rr] = fused_madd(-am[b][rr][s], xv[b][s], acc[rr]);
     }
   }
   if (!fwd) {
 #pragma unroll
     for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-      for (int s = 0; s < NS; ++s) acc[rr] += am[2][rr][s] * xv[2][s];
+      for (int s = 0; s < NS; ++s) acc[rr] = fused_madd(am[2][rr][s], xv[2][s], acc[rr]);
   }
 #pragma unroll
   for (int rr = 0; rr < R; ++rr) {
@@ -842,14 +848,14 @@ __global__ void __launch_bounds__(group_threads<TA>()) ilu_apply_group_async_ker
 #pragma unroll
             for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-              for (int s = 0; s < NS; ++s) acc[rr] -= mat(b, rr, s) * xv[b][s];
+              for (int s = 0; s < NS; ++s) acc[rr] = fused_madd(-mat(b, rr, s), xv[b][s], acc[rr]);
           }
         }
         if (!fwd) {
 #pragma unroll
           for (int rr = 0; rr < R; ++rr)
 #pragma unroll
-            for (int s = 0; s < NS; ++s) acc[rr] += mat(2, rr, s) * xv[2][s];
+            for (int s = 0; s < NS; ++s) acc[rr] = fused_madd(mat(2, rr, s), xv[2][s], acc[rr]);
         }
 #pragma unroll
         for (int rr = 0; rr < R; ++rr) {

@@ -111,18 +111,22 @@ def test_tile_apply_equals_data_flow_apply_bitwise(kw, tile):
     vals, _, _, _ = _jacobian(ctx, spec)
     ctx.ilu_tile = tile
     x = torch.from_numpy(np.random.default_rng(11).standard_normal(ctx.layout.n_dof)).cuda()
+    bad = []
     for precision in (0, 1):
         for rows in (2, 4, 6, 8):
-            ys = []
+            ys = {}
             for sched in (4, 3, 2):
                 ctx.tile = {"ilu_sched": [sched, sched], "ilu_rows": [rows, rows]}
                 y = torch.full_like(x, float("nan"))
                 ctx.ilu_apply(vals, x, y, precision, 1, repeat=2)
-                ys.append(y)
+                ys[sched] = y
             torch.cuda.synchronize()
-            assert torch.isfinite(ys[0]).all()
-            for y in ys[1:]:
-                assert torch.equal(ys[0].view(torch.int64), y.view(torch.int64)), (precision, rows)
+            assert torch.isfinite(ys[2]).all()
+            for sched in (4, 3):
+                if not torch.equal(ys[2].view(torch.int64), ys[sched].view(torch.int64)):
+                    d = (ys[sched] - ys[2]).abs()
+                    bad.append((precision, rows, sched, int((d > 0).sum()), float(d.max())))
+    assert not bad, bad
     ctx.tile = {}
     ctx.close()
 
