@@ -575,8 +575,11 @@ def ilu_bench(n):
     # the per-tile apply (one CTA per tile, the default) and the data-flow apply on the tiled factors
     for tile in (8, 16, 32, 64):
         ctx.ilu_tile = tile
-        for sched, sn in ((4, "staged"), (3, "tiles"), (2, "data_flow")):
-            ctx.tile = {"ilu_sched": [sched, sched]}
+        # per-tile applies: matrix rows staged in shared memory or in registers, with
+        # 512 / 256 / 128 threads per CTA (k = 1 / 2 / 3; 0 the default); the data-flow apply
+        shapes = [(4, k, f"staged_k{k}") for k in (0, 1, 2, 3)] + [(3, 0, "tiles"), (2, 0, "data_flow")]
+        for sched, k, sn in shapes:
+            ctx.tile = {"ilu_sched": [sched, sched], "ilu_ctas": [k, k]}
             for prec, pn in ((0, "fp64"), (1, "fp32")):
                 ctx.ilu_apply(vals, x, y, prec, 0, 3)
                 out[f"tiled{tile}_{sn}_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 0, 20)

@@ -8,7 +8,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libiceicle_b200.so")
 SOURCES = ["icx_host.cu", "icx_residual.cu", "icx_jacobian.cu", "icx_linalg.cu", "icx_solver.cu", "icx_workloads.cu", "icx_noalloc.cu",
            "icx_mdg.cu", "icx_explicit.cu", "icx_batch.cu", "icx_io.cu", "icx_lpc.cu", "icx_pipeline.cu",
-           "icx_tune.cu", "icx_gemm_tc.cu", "icx_pset.cu"]
+           "icx_tune.cu", "icx_gemm_tc.cu", "icx_pset.cu", "icx_ilu_group.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

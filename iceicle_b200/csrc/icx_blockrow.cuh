@@ -405,6 +405,10 @@ __device__ inline double flow_value(double v) {
 // rows per task of the data-flow apply: three blocks' rows stay in registers.
 // RT = 0 takes the block size's default; the others are tile choices (every
 // row's sum is formed the same way whatever the rows per task)
+// whether a task of r rows fits: at most the block size, and r x (values
+// per lane per row) <= 24 register values
+constexpr bool flow_rows_fit(int bs, int ns, int r) { return r <= (bs < 2 ? 2 : bs) && r * ns <= 24; }
+
 template <int BS, int RT = 0>
 struct FlowCfg {
   static constexpr int NS = (BS + 31) / 32;
@@ -576,8 +580,8 @@ struct IluGroupArgs {
   IluGroupPlan plan;
 };
 
-// threads per CTA of the group apply: FP32 factors keep their rows in half
-// the registers, so twice the warps fit a CTA
+// threads per CTA of the group applies by default: FP32 factors keep their
+// rows in half the registers, so twice the warps fit a CTA
 template <class TA>
 constexpr int group_threads() { return sizeof(TA) == 8 ? 256 : 512; }
 
@@ -660,12 +664,12 @@ __device__ inline void group_task_run(const IluGroupArgs<TA>& a, bool fwd, int4 
 // (in this level or, after its last one, its first of the next level) is
 // loaded before the current task runs, so a task costs one dependent trip
 // to memory (its matrix rows and neighbour vectors, loaded together)
-template <int BS, int RT, class TA>
-__global__ void __launch_bounds__(group_threads<TA>()) ilu_apply_group_kernel(IluGroupArgs<TA> a) {
+template <int BS, int RT, class TA, int NT>
+__global__ void __launch_bounds__(NT) ilu_apply_group_kernel(IluGroupArgs<TA> a) {
   using K = FlowCfg<BS, RT>;
   constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
   __shared__ int slev[kGroupLevelsSmem + 1];
-  const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, nwarp = NT / 32;
   const int g = blockIdx.x;
   const int l0 = a.plan.glev_ptr[g], l1 = a.plan.glev_ptr[g + 1];
   const int nlev = l1 - l0 - 1;
@@ -744,15 +748,15 @@ __device__ inline bool group_task_ok(const IluGroupArgs<TA>& a, int4 inf) {
            (inf.w >= 0 && inf.z < 0));
 }
 
-template <int BS, int RT, class TA, int D>
-__global__ void __launch_bounds__(group_threads<TA>()) ilu_apply_group_async_kernel(IluGroupArgs<TA> a) {
+template <int BS, int RT, class TA, int NT, int D>
+__global__ void __launch_bounds__(NT) ilu_apply_group_async_kernel(IluGroupArgs<TA> a) {
   using K = FlowCfg<BS, RT>;
   constexpr int NS = K::NS, R = K::R, GROUPS = K::GROUPS;
   constexpr int SLOT = group_slot_bytes<BS, R, TA>();
   constexpr int CH = (BS * (int)sizeof(TA)) % 16 == 0 ? 16 : (int)sizeof(TA);
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ int slev[kGroupLevelsSmem + 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = NT / 32;
   const int g = blockIdx.x;
   const int l0 = a.plan.glev_ptr[g], l1 = a.plan.glev_ptr[g + 1];
   const int nlev = l1 - l0 - 1;

@@ -464,7 +464,6 @@ cudaError_t la_ilu_factor(const DeviceMesh& dm, const int* order, const std::vec
 // rows per task compiled for a block size: at most the block size, and the
 // three blocks' rows a task holds (R x column chunks each) at most 24 values
 // per lane, which keeps them in registers
-constexpr bool flow_rows_fit(int bs, int ns, int r) { return r <= (bs < 2 ? 2 : bs) && r * ns <= 24; }
 
 template <int B, int R, class TA>
 static const void* flow_kernel_if_fit(bool sen) {
@@ -533,109 +532,6 @@ static cudaError_t ilu_apply_flow_t(const DeviceMesh& dm, const int* order, cons
   }
   void* params[] = {&args};
   return cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(256), params, 0, s);
-}
-
-template <int B, int R, class TA>
-static const void* group_kernel_if_fit() {
-  if constexpr (flow_rows_fit(B, (B + 31) / 32, R)) return (const void*)ilu_apply_group_kernel<B, R, TA>;
-  else return nullptr;
-}
-
-template <int B, class TA>
-static const void* group_kernel_for(int rows) {
-  switch (rows ? rows : FlowCfg<B>::R_DEFAULT) {
-    case 2: return group_kernel_if_fit<B, 2, TA>();
-    case 4: return group_kernel_if_fit<B, 4, TA>();
-    case 6: return group_kernel_if_fit<B, 6, TA>();
-    case 8: return group_kernel_if_fit<B, 8, TA>();
-    default: return nullptr;
-  }
-}
-
-// the staged (shared-memory) group kernel with the deepest ring that fits
-// beside the group's task-table entries, with its dynamic shared memory; a
-// null kernel when not even two slots per warp fit
-struct StagedKernel {
-  const void* kern;
-  size_t smem;
-};
-
-static int smem_optin_bytes() {
-  static int v = -1;
-  if (v < 0) {
-    int dev = 0, b = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&b, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
-      b = 0;
-    v = b;
-  }
-  return v;
-}
-
-template <int B, int R, class TA>
-static StagedKernel staged_kernel_if_fit(int gmax, int nlev_max) {
-  if constexpr (flow_rows_fit(B, (B + 31) / 32, R)) {
-    if (nlev_max > kGroupLevelsSmem) return {nullptr, 0};
-    const size_t info = (size_t)2 * gmax * sizeof(int4);
-    const size_t ring = (size_t)(group_threads<TA>() / 32) * group_slot_bytes<B, R, TA>();
-    // the kernel's static shared memory (level bounds) and a margin
-    const size_t avail = (size_t)smem_optin_bytes() > 2048 ? (size_t)smem_optin_bytes() - 2048 : 0;
-    if (info + 3 * ring <= avail) return {(const void*)ilu_apply_group_async_kernel<B, R, TA, 3>, info + 3 * ring};
-    if (info + 2 * ring <= avail) return {(const void*)ilu_apply_group_async_kernel<B, R, TA, 2>, info + 2 * ring};
-  }
-  return {nullptr, 0};
-}
-
-template <int B, class TA>
-static StagedKernel staged_kernel_for(int rows, int gmax, int nlev_max) {
-  switch (rows ? rows : FlowCfg<B>::R_DEFAULT) {
-    case 2: return staged_kernel_if_fit<B, 2, TA>(gmax, nlev_max);
-    case 4: return staged_kernel_if_fit<B, 4, TA>(gmax, nlev_max);
-    case 6: return staged_kernel_if_fit<B, 6, TA>(gmax, nlev_max);
-    case 8: return staged_kernel_if_fit<B, 8, TA>(gmax, nlev_max);
-    default: return {nullptr, 0};
-  }
-}
-
-template <class TA>
-static cudaError_t ilu_apply_groups_t(const DeviceMesh& dm, const IluGroupShape& gs, const int* task,
-                                      const int* glev, const int* glev_ptr, int rows, const TA* LU, const TA* Uinv,
-                                      const double* x, double* y, double* f, int* err, cudaStream_t s) {
-  if (gs.ngroups <= 0) return cudaErrorInvalidValue;
-  const int bs = dm.nb * dm.neq;
-  const void* kern = nullptr;
-  StagedKernel st{nullptr, 0};
-#define ICX_ILUG_CASE(B)                                                 \
-  if (bs == B) {                                                         \
-    if (gs.staged) st = staged_kernel_for<B, TA>(rows, gs.gmax, gs.nlev_max); \
-    kern = group_kernel_for<B, TA>(rows);                                \
-  }
-  ICX_BLOCK_SIZES(ICX_ILUG_CASE)
-#undef ICX_ILUG_CASE
-  if (!kern) return cudaErrorInvalidValue;
-  size_t smem = 0;
-  if (st.kern) {
-    cudaError_t e = smem_attr(st.kern, st.smem);
-    if (e != cudaSuccess) return e;
-    kern = st.kern;
-    smem = st.smem;
-  }
-  IluGroupArgs<TA> args{dm.E, dm.nnzb, LU, Uinv, x, f, y, err,
-                        IluGroupPlan{gs.ngroups, reinterpret_cast<const int4*>(task), glev, glev_ptr, gs.gmax}};
-  void* params[] = {&args};
-  return cudaLaunchKernel(kern, dim3(gs.ngroups), dim3(group_threads<TA>()), params, smem, s);
-}
-
-cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, const IluGroupShape& gs, const int* task, const int* glev,
-                                const int* glev_ptr, int rows, const double* LU, const double* Uinv, const double* x,
-                                double* y, double* f, int* err, cudaStream_t s) {
-  return ilu_apply_groups_t<double>(dm, gs, task, glev, glev_ptr, rows, LU, Uinv, x, y, f, err, s);
-}
-
-cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, const IluGroupShape& gs, const int* task,
-                                    const int* glev, const int* glev_ptr, int rows, const float* LU,
-                                    const float* Uinv, const double* x, double* y, double* f, int* err,
-                                    cudaStream_t s) {
-  return ilu_apply_groups_t<float>(dm, gs, task, glev, glev_ptr, rows, LU, Uinv, x, y, f, err, s);
 }
 
 int flow_rows_default(int bs) {

@@ -85,11 +85,13 @@ struct IluGroupShape {
   int ngroups, gmax, nlev_max;
   bool staged;
 };
+// ctas: threads per CTA, 0 the default (256 FP64, 512 FP32), 1 / 2 / 3
+// 512 / 256 / 128 (icx_ilu_group.cu)
 cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, const IluGroupShape& gs, const int* task, const int* glev,
-                                const int* glev_ptr, int rows, const double* LU, const double* Uinv, const double* x,
-                                double* y, double* f, int* err, cudaStream_t s);
+                                const int* glev_ptr, int rows, int ctas, const double* LU, const double* Uinv,
+                                const double* x, double* y, double* f, int* err, cudaStream_t s);
 cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, const IluGroupShape& gs, const int* task,
-                                    const int* glev, const int* glev_ptr, int rows, const float* LU,
+                                    const int* glev, const int* glev_ptr, int rows, int ctas, const float* LU,
                                     const float* Uinv, const double* x, double* y, double* f, int* err,
                                     cudaStream_t s);
 cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s);

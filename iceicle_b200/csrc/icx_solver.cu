@@ -367,9 +367,10 @@ cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStr
     // tiled / grouped factors: one CTA per group, no waits across CTAs
     const IluTilePlan& tp = w->tp;
     const icx::IluGroupShape gs{tp.ngroups, tp.gmax, tp.nlev_max, gsched == 4};
-    return mixed ? icx::la_ilu_apply_groups_f32(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, w->pc32,
+    const int ctas = dm.tile.flow_ctas[pi];
+    return mixed ? icx::la_ilu_apply_groups_f32(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, ctas, w->pc32,
                                                 w->uinv32, x, z, w->pct, w->pc_err, s)
-                 : icx::la_ilu_apply_groups(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, w->pc, w->uinv,
+                 : icx::la_ilu_apply_groups(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, ctas, w->pc, w->uinv,
                                             x, z, w->pct, w->pc_err, s);
   }
   // the sentinel schedule uses neither the counters nor the epoch

@@ -230,7 +230,7 @@ struct Tuner {
       for (int r : icx::kFlowRows) {
         if (!icx::flow_rows_compiled(bs, r)) continue;
         for (int k = 1; k <= MAX_CTAS; ++k) {
-          if (sc >= 3 && k != 2) continue;
+          if (sc >= 3 && k > 3) continue;  // 512 / 256 / 128 threads per group CTA
           if (r == R0 && k == 2 && sc == S0) continue;  // the default, timed above
           dm.tile.flow_rows[pi] = r;
           dm.tile.flow_ctas[pi] = k;
@@ -299,6 +299,8 @@ icx_status icx_tile_set(icx_ctx* c, const icx_tile_choice* t) {
       return fail(c, ICX_ERR_INVALID, "ilu_rows: not compiled for this block size");
     if (t->ilu_ctas[k] < 0 || t->ilu_ctas[k] > MAX_CTAS) return fail(c, ICX_ERR_INVALID, "ilu_ctas: 0..4");
     if (t->ilu_sched[k] < 0 || t->ilu_sched[k] > 4) return fail(c, ICX_ERR_INVALID, "ilu_sched: 0..4");
+    if (t->ilu_sched[k] >= 3 && t->ilu_ctas[k] > 3)
+      return fail(c, ICX_ERR_INVALID, "ilu_ctas: 0..3 for the group applies (512 / 256 / 128 threads per CTA)");
   }
   TileChoice& d = c->dm.tile;
   d.face_minb = t->face_minb;

@@ -602,7 +602,9 @@ icx_status icx_basis_node_coords(const icx_ctx* ctx, double* xy);
  *               per tile running the tile's levels between CTA barriers, 4 the
  *               same with each warp's next task rows copied ahead into shared
  *               memory (the default there; 3 where they do not fit; both 2 on
- *               whole-grid factors) */
+ *               whole-grid factors); for 3 and 4 ilu_ctas picks the threads
+ *               per CTA instead: 0 the default (256 FP64, 512 FP32 factors),
+ *               1 / 2 / 3 512 / 256 / 128 */
 typedef struct icx_tile_choice {
   int face_minb;
   int vol_threads, vol_minb;

@@ -115,17 +115,19 @@ def test_tile_apply_equals_data_flow_apply_bitwise(kw, tile):
     for precision in (0, 1):
         for rows in (2, 4, 6, 8):
             ys = {}
-            for sched in (4, 3, 2):
-                ctx.tile = {"ilu_sched": [sched, sched], "ilu_rows": [rows, rows]}
+            # data flow; per-tile applies in registers / staged, 512 / 256 / 128 threads per CTA
+            for sched, k in ((2, 0), (4, 0), (3, 0), (4, 1), (4, 2), (4, 3), (3, 1), (3, 3)):
+                ctx.tile = {"ilu_sched": [sched, sched], "ilu_rows": [rows, rows], "ilu_ctas": [k, k]}
                 y = torch.full_like(x, float("nan"))
                 ctx.ilu_apply(vals, x, y, precision, 1, repeat=2)
-                ys[sched] = y
+                ys[(sched, k)] = y
             torch.cuda.synchronize()
-            assert torch.isfinite(ys[2]).all()
-            for sched in (4, 3):
-                if not torch.equal(ys[2].view(torch.int64), ys[sched].view(torch.int64)):
-                    d = (ys[sched] - ys[2]).abs()
-                    bad.append((precision, rows, sched, int((d > 0).sum()), float(d.max())))
+            y0 = ys.pop((2, 0))
+            assert torch.isfinite(y0).all()
+            for key, y in ys.items():
+                if not torch.equal(y0.view(torch.int64), y.view(torch.int64)):
+                    d = (y - y0).abs()
+                    bad.append((precision, rows, key, int((d > 0).sum()), float(d.max())))
     assert not bad, bad
     ctx.tile = {}
     ctx.close()
