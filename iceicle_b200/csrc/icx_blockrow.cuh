@@ -25,6 +25,46 @@ enum BlockRowMode {
 __device__ inline float fused_madd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ inline double fused_madd(double a, double b, double c) { return __fma_rn(a, b, c); }
 
+// Warp sums of R per-lane partial rows by a butterfly reduce-scatter: at
+// distance 16, 8, ... each lane keeps half of its rows, adding its partner's
+// copy of them, until one row is left, then finishes with the plain
+// butterfly. Every addition is one the full butterfly (acc += shfl_xor(acc,
+// d), d = 16 .. 1, on every row) also makes, so each row's sum is the same
+// value, with about R + 5 shuffles instead of 5 R. Lane l ends with the sum
+// of row `row` (from its bits 4, 3, ...); `owner` marks one lane per row
+// below R.
+template <class T>
+struct RowSum {
+  T v;
+  int row;
+  bool owner;
+};
+
+template <int R, class T>
+__device__ inline RowSum<T> warp_row_sums(const T (&acc)[R]) {
+  static_assert(R >= 1 && R <= 32, "rows per warp task");
+  constexpr int RP = R <= 1 ? 1 : R <= 2 ? 2 : R <= 4 ? 4 : R <= 8 ? 8 : R <= 16 ? 16 : 32;
+  const int lane = threadIdx.x & 31;
+  T v[RP];
+#pragma unroll
+  for (int i = 0; i < RP; ++i) v[i] = i < R ? acc[i] : T(0);
+  int row = 0, d = 16;
+#pragma unroll
+  for (int m = RP; m > 1; m >>= 1, d >>= 1) {
+    const bool hi = (lane & d) != 0;
+#pragma unroll
+    for (int i = 0; i < m / 2; ++i) {
+      const T send = hi ? v[i] : v[i + m / 2];
+      const T keep = hi ? v[i + m / 2] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
+    }
+    if (hi) row += m / 2;
+  }
+#pragma unroll
+  for (; d > 0; d >>= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], d);
+  return {v[0], row, row < R && (lane & (32 / RP - 1)) == 0};
+}
+
 // the block rows 0..nrows-1 of one launch
 struct RowSet {
   int nx, ny, level, nrows;
@@ -77,17 +117,10 @@ __device__ inline void block_row_task(const RowSet& rs, long long task, const in
       }
     }
   }
-#pragma unroll
-  for (int rr = 0; rr < R; ++rr) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
-  }
-  TA mine = TA(0);
-#pragma unroll
-  for (int rr = 0; rr < R; ++rr)
-    if (lane == rr) mine = acc[rr];
-  const int r = r0 + lane;
-  if (lane < R && r < BS) {
+  const RowSum<TA> sum = warp_row_sums<R>(acc);
+  const TA mine = sum.v;
+  const int r = r0 + sum.row;
+  if (sum.owner && r < BS) {
     double base = x0 ? (COHERENT ? __ldcg(x0 + (size_t)e * BS + r) : x0[(size_t)e * BS + r]) : 0.0;
     y[(size_t)e * BS + r] = base + sign * (double)mine;
   }
@@ -524,23 +557,16 @@ __global__ void __launch_bounds__(256) ilu_apply_flow_kernel(IluFlowArgs<TA> a) 
 #pragma unroll
           for (int s = 0; s < NS; ++s) acc[rr] = fused_madd(am[2][rr][s], xv[2][s], acc[rr]);
       }
-#pragma unroll
-      for (int rr = 0; rr < R; ++rr) {
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
-      }
-      TA mine = TA(0);
-#pragma unroll
-      for (int rr = 0; rr < R; ++rr)
-        if (lane == rr) mine = acc[rr];
-      const int r = r0 + lane;
+      const RowSum<TA> rs = warp_row_sums<R>(acc);
+      const TA mine = rs.v;
+      const int r = r0 + rs.row;
       if constexpr (SEN) {
-        if (lane < R && r < BS) {
+        if (rs.owner && r < BS) {
           if (fwd) st_relaxed_f64(a.f + (size_t)e * BS + r, flow_value(a.x[(size_t)e * BS + r] + (double)mine));
           else st_relaxed_f64(a.y + (size_t)e * BS + r, flow_value((double)mine));
         }
       } else {
-        if (lane < R && r < BS) {
+        if (rs.owner && r < BS) {
           if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
           else a.y[(size_t)e * BS + r] = (double)mine;
         }
@@ -642,17 +668,10 @@ __device__ inline void group_task_run(const IluGroupArgs<TA>& a, bool fwd, int4 
 #pragma unroll
       for (int s = 0; s < NS; ++s) acc[rr] = fused_madd(am[2][rr][s], xv[2][s], acc[rr]);
   }
-#pragma unroll
-  for (int rr = 0; rr < R; ++rr) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
-  }
-  TA mine = TA(0);
-#pragma unroll
-  for (int rr = 0; rr < R; ++rr)
-    if (lane == rr) mine = acc[rr];
-  const int r = r0 + lane;
-  if (lane < R && r < BS) {
+  const RowSum<TA> rs = warp_row_sums<R>(acc);
+  const TA mine = rs.v;
+  const int r = r0 + rs.row;
+  if (rs.owner && r < BS) {
     if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
     else a.y[(size_t)e * BS + r] = (double)mine;
   }
@@ -861,17 +880,10 @@ __global__ void __launch_bounds__(NT) ilu_apply_group_async_kernel(IluGroupArgs<
 #pragma unroll
             for (int s = 0; s < NS; ++s) acc[rr] = fused_madd(mat(2, rr, s), xv[2][s], acc[rr]);
         }
-#pragma unroll
-        for (int rr = 0; rr < R; ++rr) {
-#pragma unroll
-          for (int off = 16; off > 0; off >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], off);
-        }
-        TA mine = TA(0);
-#pragma unroll
-        for (int rr = 0; rr < R; ++rr)
-          if (lane == rr) mine = acc[rr];
-        const int r = r0 + lane;
-        if (lane < R && r < BS) {
+        const RowSum<TA> rs = warp_row_sums<R>(acc);
+        const TA mine = rs.v;
+        const int r = r0 + rs.row;
+        if (rs.owner && r < BS) {
           if (fwd) a.f[(size_t)e * BS + r] = a.x[(size_t)e * BS + r] + (double)mine;
           else a.y[(size_t)e * BS + r] = (double)mine;
         }
