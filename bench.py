@@ -72,6 +72,12 @@ def parse():
     ap.add_argument("--jacobian", type=int, default=0, metavar="N",
                     help="only time the FD Jacobian (FP64 and FP32 flux quadrature) of the N x N p = 3 "
                          "Navier-Stokes manufactured solution and print one JSON line")
+    ap.add_argument("--solve", type=int, default=-1, metavar="TILE",
+                    help="only run one Newton solve of the first evaluation instance of the 256 x 256 p = 2 "
+                         "Navier-Stokes problem (autotuned shapes) with block-ILU(0) on TILE x TILE element "
+                         "tiles (0: the whole grid) and print one JSON line")
+    ap.add_argument("--solve-precision", type=int, default=1, metavar="P",
+                    help="Newton precision of --solve (0 FP64, 1 mixed, 2 FP32 flux quadrature)")
     ap.add_argument("--no-tune", action="store_true",
                     help="time the compiled default launch shapes instead of the autotuned ones")
     ap.add_argument("--tile", default="", metavar="K=V,...",
@@ -575,9 +581,10 @@ def ilu_bench(n):
     # the per-tile apply (one CTA per tile, the default) and the data-flow apply on the tiled factors
     for tile in (8, 16, 32, 64):
         ctx.ilu_tile = tile
-        # per-tile applies: matrix rows staged in shared memory or in registers, with
-        # 512 / 256 / 128 threads per CTA (k = 1 / 2 / 3; 0 the default); the data-flow apply
-        shapes = [(4, k, f"staged_k{k}") for k in (0, 1, 2, 3)] + [(3, 0, "tiles"), (2, 0, "data_flow")]
+        # per-tile applies: one lane per row, matrix rows staged in shared memory or in registers,
+        # with 512 / 256 / 128 threads per CTA (k = 1 / 2 / 3; 0 the default); the data-flow apply
+        shapes = ([(5, k, f"rowpar_k{k}") for k in (0, 1, 2, 3)] + [(4, k, f"staged_k{k}") for k in (0, 1, 3)] +
+                  [(3, 0, "tiles"), (2, 0, "data_flow")])
         for sched, k, sn in shapes:
             ctx.tile = {"ilu_sched": [sched, sched], "ilu_ctas": [k, k]}
             for prec, pn in ((0, "fp64"), (1, "fp32")):
@@ -929,8 +936,41 @@ def jacobian_mode(n):
     print(json.dumps(out))
 
 
+def solve_mode(tile, precision):
+    """one Newton solve (|r| <= 1e-10, GMRES(30)) of the first evaluation
+    instance of the 256 x 256 p = 2 Navier-Stokes problem, launch shapes
+    autotuned at the initial state for the chosen tiling; CUDA events around
+    the solve"""
+    import torch
+    import iceicle_b200 as ib
+    from iceicle_b200 import learned_pc as lp
+    dev = torch.device("cuda", 0)
+    seed, re = lp.instances(*lp.EVAL_INSTANCES)[0]
+    wl = lp.make_instance(seed, re, 256, dev.index)
+    u0 = torch.from_numpy(wl.u0).to(dev)
+    wl.ctx.ilu_tile = tile
+    wl.ctx.autotune(u0, ib.TUNE_RESIDUAL | ib.TUNE_ILU | ib.TUNE_ILU_FP32)
+    opt = ib.default_newton_options()
+    opt.precision, opt.ilu_tile, opt.gmres_max_it = precision, tile, 20000
+    u = u0.clone()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    rep = wl.ctx.newton_solve(u, opt)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    s = e0.elapsed_time(e1) * 1e-3
+    its = rep.linear_iterations_total
+    print(json.dumps({"solve": "ns_256x256_p2", "seed": seed, "re": re, "ilu_tile": tile, "precision": precision,
+                      "converged": bool(rep.converged), "s": s, "newton_its": rep.iterations, "gmres_its": its,
+                      "ms_per_gmres_it": 1e3 * s / max(its, 1), "tile_choice": wl.ctx.tile}))
+
+
 def main():
     a = parse()
+    if a.solve >= 0:
+        solve_mode(a.solve, a.solve_precision)
+        return
     if a.gemm:
         gemm_mode(a.gemm)
         return

@@ -592,6 +592,8 @@ struct IluGroupPlan {
   const int* glev;      // level boundaries: positions in the group order, group g's at glev[glev_ptr[g] .. glev_ptr[g + 1]]
   const int* glev_ptr;  // [ngroups + 1]
   int gmax;             // elements of the largest group
+  const int4* loc;      // [2 E] the same entries by position within the group: {element, k0, k1, 0}
+                        // (ilu_apply_group_rows_kernel only)
 };
 
 template <class TA>
@@ -894,6 +896,118 @@ __global__ void __launch_bounds__(NT) ilu_apply_group_async_kernel(IluGroupArgs<
     __syncthreads();
   }
   cp_async_wait<0>();
+}
+
+// The group apply with one lane per matrix row: the tasks of a level are
+// its (element, row) pairs, 32 to a warp, and a lane forms its row's sums
+// over the columns in order, reading the factor row with 16-byte loads where
+// rows are 16-byte aligned. The group's forward and backward vectors stay in
+// shared memory (rounded to TA, as the other applies round them on load), so
+// a task's only reads from memory are its factor rows and x; the forward
+// vector is not written back. No warp reductions. The column order of the
+// sums differs from the other applies (not bit-identical to them; identical
+// across thread counts). Dynamic shared memory: 4 gmax entries (int4), then
+// 2 gmax BS values of TA.
+template <int BS, class TA>
+__host__ __device__ constexpr int group_rows_vec() {
+  return (BS * (int)sizeof(TA)) % 16 == 0 ? 16 / (int)sizeof(TA) : 1;
+}
+
+template <class TA>
+__host__ __device__ constexpr size_t group_rows_smem(int gmax, int bs) {
+  return (size_t)4 * gmax * sizeof(int4) + (size_t)2 * gmax * bs * sizeof(TA);
+}
+
+template <class TA, int VEC>
+struct VecOf;
+template <> struct VecOf<float, 4> { using type = float4; };
+template <> struct VecOf<double, 2> { using type = double2; };
+template <class TA> struct VecOf<TA, 1> { using type = TA; };
+
+template <class V, class TA>
+__device__ inline TA vec_at(const V& v, int i) {
+  if constexpr (sizeof(V) == sizeof(TA)) return v;
+  else return reinterpret_cast<const TA*>(&v)[i];
+}
+
+// acc += sign * A_row . x over the BS columns, in column order
+template <int BS, int VEC, bool NEG, class TA>
+__device__ inline TA row_dot(const TA* __restrict__ arow, const TA* xs, TA acc) {
+  using V = typename VecOf<TA, VEC>::type;
+#pragma unroll
+  for (int c = 0; c < BS; c += VEC) {
+    const V av = *reinterpret_cast<const V*>(arow + c);
+    const V xv = *reinterpret_cast<const V*>(xs + c);
+#pragma unroll
+    for (int i = 0; i < VEC; ++i)
+      acc = fused_madd(NEG ? -vec_at<V, TA>(av, i) : vec_at<V, TA>(av, i), vec_at<V, TA>(xv, i), acc);
+  }
+  return acc;
+}
+
+template <int BS, class TA, int NT>
+__global__ void __launch_bounds__(NT) ilu_apply_group_rows_kernel(IluGroupArgs<TA> a) {
+  constexpr int VEC = group_rows_vec<BS, TA>();
+  constexpr int NW = NT / 32;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ int slev[kGroupLevelsSmem + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = blockIdx.x;
+  const int l0 = a.plan.glev_ptr[g], l1 = a.plan.glev_ptr[g + 1];
+  const int nlev = l1 - l0 - 1;
+  const int gm = a.plan.gmax;
+  const int pg0 = a.plan.glev[l0], G = a.plan.glev[l1 - 1] - pg0;
+  if (nlev > kGroupLevelsSmem || G > gm || G < 0) {  // uniform over the CTA
+    if (threadIdx.x == 0) atomicExch(a.err, 2);
+    return;
+  }
+  int4* sinfo = reinterpret_cast<int4*>(dsm);  // [fwd gmax | bwd gmax]
+  int4* sloc = sinfo + 2 * gm;                 // [fwd gmax | bwd gmax]
+  TA* fs = reinterpret_cast<TA*>(sloc + 2 * gm);
+  TA* ys = fs + (size_t)gm * BS;
+  for (int i = threadIdx.x; i <= nlev; i += NT) slev[i] = a.plan.glev[l0 + i];
+  for (int i = threadIdx.x; i < G; i += NT) {
+    sinfo[i] = a.plan.task[pg0 + i];
+    sinfo[gm + i] = a.plan.task[a.E + pg0 + i];
+    sloc[i] = a.plan.loc[pg0 + i];
+    sloc[gm + i] = a.plan.loc[a.E + pg0 + i];
+  }
+  __syncthreads();
+  const int nq = 2 * nlev;
+  for (int q = 0; q < nq; ++q) {
+    const bool fwd = q < nlev;
+    const int lv = fwd ? q : nq - 1 - q;
+    const int p0 = slev[lv] - pg0, npair = (slev[lv + 1] - slev[lv]) * BS;
+    const int4* ti = sinfo + (fwd ? 0 : gm);
+    const int4* tl = sloc + (fwd ? 0 : gm);
+    for (int t = warp; t * 32 < npair; t += NW) {
+      const int p = t * 32 + lane;
+      if (p >= npair) continue;
+      const int ei = p / BS, r = p - ei * BS;
+      const int4 inf = ti[p0 + ei], loc = tl[p0 + ei];
+      const int nbk = (inf.z >= 0) + (inf.w >= 0);
+      const bool bad = !group_task_ok<BS, 1, TA>(a, inf) || loc.x < 0 || loc.x >= G || loc.y >= G ||
+                       loc.z >= G || (nbk > 0 && loc.y < 0) || (nbk > 1 && loc.z < 0);
+      if (bad) {
+        atomicExch(a.err, 2);
+        continue;
+      }
+      TA acc = TA(0);
+      const TA* xs = fwd ? fs : ys;
+      if (nbk > 0) acc = row_dot<BS, VEC, true>(a.LU + ((size_t)inf.y * BS + r) * BS, xs + (size_t)loc.y * BS, acc);
+      if (nbk > 1)
+        acc = row_dot<BS, VEC, true>(a.LU + ((size_t)(inf.y + 1) * BS + r) * BS, xs + (size_t)loc.z * BS, acc);
+      if (fwd) {
+        const double fd = a.x[(size_t)inf.x * BS + r] + (double)acc;
+        fs[(size_t)loc.x * BS + r] = (TA)fd;
+      } else {
+        acc = row_dot<BS, VEC, false>(a.Uinv + ((size_t)inf.x * BS + r) * BS, fs + (size_t)loc.x * BS, acc);
+        a.y[(size_t)inf.x * BS + r] = (double)acc;
+        ys[(size_t)loc.x * BS + r] = acc;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 #define ICX_BLOCK_SIZES(X) X(4) X(9) X(16) X(25) X(36) X(64) X(100)

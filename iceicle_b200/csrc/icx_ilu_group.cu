@@ -1,7 +1,8 @@
 // Launchers of the block-ILU(0) applies on element groups (tiles): one CTA
-// per group, the register form (schedule 3) and the shared-memory staged
-// form (schedule 4), for every compiled block size, rows per task and CTA
-// size. The kernels are in icx_blockrow.cuh.
+// per group, the register form (schedule 3), the shared-memory staged form
+// (schedule 4) and the one-lane-per-row form (schedule 5), for every
+// compiled block size, rows per task and CTA size. The kernels are in
+// icx_blockrow.cuh.
 #include <cuda_runtime.h>
 
 #include "icx_internal.h"
@@ -37,6 +38,11 @@ int smem_optin_bytes() {
   return v;
 }
 
+size_t smem_avail() {
+  const size_t optin = (size_t)smem_optin_bytes();
+  return optin > 2048 ? optin - 2048 : 0;  // less the kernels' static shared memory and a margin
+}
+
 struct GroupKernel {
   const void* kern;
   size_t smem;
@@ -47,11 +53,9 @@ GroupKernel group_kernel_if_fit(bool staged, int gmax, int nlev_max) {
   if constexpr (flow_rows_fit(B, (B + 31) / 32, R)) {
     if (staged && nlev_max <= kGroupLevelsSmem) {
       // the deepest ring that fits beside the group's task-table entries
-      // (less the kernel's static shared memory and a margin)
       const size_t info = (size_t)2 * gmax * sizeof(int4);
       const size_t ring = (size_t)(NT / 32) * group_slot_bytes<B, R, TA>();
-      const size_t optin = (size_t)smem_optin_bytes();
-      const size_t avail = optin > 2048 ? optin - 2048 : 0;
+      const size_t avail = smem_avail();
       if (info + 3 * ring <= avail) return {(const void*)ilu_apply_group_async_kernel<B, R, TA, NT, 3>, info + 3 * ring};
       if (info + 2 * ring <= avail) return {(const void*)ilu_apply_group_async_kernel<B, R, TA, NT, 2>, info + 2 * ring};
     }
@@ -66,6 +70,19 @@ GroupKernel group_kernel_nt(int nt, bool staged, int gmax, int nlev_max) {
     case 128: return group_kernel_if_fit<B, R, TA, 128>(staged, gmax, nlev_max);
     case 256: return group_kernel_if_fit<B, R, TA, 256>(staged, gmax, nlev_max);
     case 512: return group_kernel_if_fit<B, R, TA, 512>(staged, gmax, nlev_max);
+    default: return {nullptr, 0};
+  }
+}
+
+// schedule 5: one lane per row, where the group's vectors fit
+template <int B, class TA>
+GroupKernel group_rows_kernel(int nt, int gmax, int nlev_max) {
+  const size_t sm = group_rows_smem<TA>(gmax, B);
+  if (nlev_max > kGroupLevelsSmem || sm > smem_avail()) return {nullptr, 0};
+  switch (nt) {
+    case 128: return {(const void*)ilu_apply_group_rows_kernel<B, TA, 128>, sm};
+    case 256: return {(const void*)ilu_apply_group_rows_kernel<B, TA, 256>, sm};
+    case 512: return {(const void*)ilu_apply_group_rows_kernel<B, TA, 512>, sm};
     default: return {nullptr, 0};
   }
 }
@@ -89,8 +106,11 @@ cudaError_t ilu_apply_groups_t(const DeviceMesh& dm, const IluGroupShape& gs, co
   const int bs = dm.nb * dm.neq;
   const int nt = group_threads_for<TA>(ctas);
   GroupKernel k{nullptr, 0};
-#define ICX_ILUG_CASE(B) \
-  if (bs == B) k = group_kernel_for<B, TA>(rows, nt, gs.staged, gs.gmax, gs.nlev_max);
+#define ICX_ILUG_CASE(B)                                                                  \
+  if (bs == B) {                                                                          \
+    if (gs.sched == 5 && gs.loc) k = group_rows_kernel<B, TA>(nt, gs.gmax, gs.nlev_max);  \
+    if (!k.kern) k = group_kernel_for<B, TA>(rows, nt, gs.sched >= 4, gs.gmax, gs.nlev_max); \
+  }
   ICX_BLOCK_SIZES(ICX_ILUG_CASE)
 #undef ICX_ILUG_CASE
   if (!k.kern) return cudaErrorInvalidValue;
@@ -99,7 +119,8 @@ cudaError_t ilu_apply_groups_t(const DeviceMesh& dm, const IluGroupShape& gs, co
     if (e != cudaSuccess) return e;
   }
   IluGroupArgs<TA> args{dm.E, dm.nnzb, LU, Uinv, x, f, y, err,
-                        IluGroupPlan{gs.ngroups, reinterpret_cast<const int4*>(task), glev, glev_ptr, gs.gmax}};
+                        IluGroupPlan{gs.ngroups, reinterpret_cast<const int4*>(task), glev, glev_ptr, gs.gmax,
+                                     reinterpret_cast<const int4*>(gs.loc)}};
   void* params[] = {&args};
   return cudaLaunchKernel(k.kern, dim3(gs.ngroups), dim3(nt), params, k.smem, s);
 }

@@ -71,10 +71,11 @@ constexpr int kFlowSchedDefault = 2;
 inline bool flow_sentinel(const TileChoice& t, int pi) {
   return (t.flow_sched[pi] ? t.flow_sched[pi] : kFlowSchedDefault) == 2;
 }
-// schedules 3 and 4: the apply on element tiles / groups with one CTA per
-// group (la_ilu_apply_groups), 4 with the matrix rows staged in shared
-// memory where they fit; 4 is the default when the factors are tiled or grouped
-constexpr int kGroupSchedDefault = 4;
+// schedules 3, 4 and 5: the apply on element tiles / groups with one CTA
+// per group (la_ilu_apply_groups), 4 with the matrix rows staged in shared
+// memory, 5 with one lane per row and the group's vectors in shared memory,
+// each where it fits; 5 is the default when the factors are tiled or grouped
+constexpr int kGroupSchedDefault = 5;
 inline int ilu_schedule(const TileChoice& t, int pi, bool grouped) {
   const int sc = t.flow_sched[pi] ? t.flow_sched[pi] : (grouped ? kGroupSchedDefault : kFlowSchedDefault);
   return (sc >= 3 && !grouped) ? kFlowSchedDefault : sc;

@@ -79,11 +79,13 @@ cudaError_t la_ilu_apply_flow_f32(const DeviceMesh& dm, const int* order, const 
 // IluGroupPlan (icx_blockrow.cuh); rows =
 // rows per warp task (0: the default); *err = 2 on an index out of range
 // the plan's shape: groups, elements of the largest group, most levels of
-// a group, and whether the staged kernel (matrix rows in shared memory) may
-// run where it fits
+// a group, the schedule (3 registers, 4 matrix rows staged in shared memory,
+// 5 one lane per row with the group's vectors in shared memory; 5 and 4 fall
+// back to the next lower one where their shared memory does not fit) and
+// the entries by position within the group (IluGroupPlan::loc)
 struct IluGroupShape {
-  int ngroups, gmax, nlev_max;
-  bool staged;
+  int ngroups, gmax, nlev_max, sched;
+  const int* loc;
 };
 // ctas: threads per CTA, 0 the default (256 FP64, 512 FP32), 1 / 2 / 3
 // 512 / 256 / 128 (icx_ilu_group.cu)

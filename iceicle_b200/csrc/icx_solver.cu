@@ -46,6 +46,7 @@ struct IluTilePlan {
   int nlev_max = 0;             // most levels of a group
   bool group_ok = true;         // no sweep row has more than two off-diagonal blocks
   int* gtask = nullptr;         // [2 E] x 4: IluGroupPlan::task, in group order (group, level, element)
+  int* gloc = nullptr;          // [2 E] x 4: IluGroupPlan::loc
   int* glev = nullptr;          // level boundaries (positions in the group order), per group
   int* glev_ptr = nullptr;      // [ngroups + 1] into glev
 };
@@ -182,7 +183,7 @@ icx_status ensure_work(icx_ctx* c, int m) {
 }
 
 void free_tile_plan(IluTilePlan& tp) {
-  for (int* p : {tp.rowptr, tp.colidx, tp.diag, tp.map, tp.order, tp.gtask, tp.glev, tp.glev_ptr})
+  for (int* p : {tp.rowptr, tp.colidx, tp.diag, tp.map, tp.order, tp.gtask, tp.gloc, tp.glev, tp.glev_ptr})
     if (p) cudaFree(p);
   tp = IluTilePlan();
 }
@@ -273,13 +274,31 @@ icx_status ensure_ilu_plan(icx_ctx* c) {
   glev.push_back(dm.E);
   glev_ptr.push_back((int)glev.size());
   tp.ngroups = ng;
+  // the same entries by position within the group: {element, k0, k1, 0}
+  // (k = -1: no such block); the kept pattern couples only elements of one group
+  std::vector<int> gloc(8 * (size_t)dm.E, -1), pos(dm.E), gstart(dm.E);
+  for (int p = 0; p < dm.E; ++p) pos[key[p][2]] = p;
+  for (int g = 0; g < ng; ++g)
+    for (int p = glev[glev_ptr[g]]; p < glev[glev_ptr[g + 1] - 1]; ++p) gstart[p] = glev[glev_ptr[g]];
+  for (int sw = 0; sw < 2; ++sw)
+    for (int p = 0; p < dm.E; ++p) {
+      const int* t = &gtask[4 * ((size_t)sw * dm.E + p)];
+      int* l = &gloc[4 * ((size_t)sw * dm.E + p)];
+      l[0] = p - gstart[p];
+      l[3] = 0;
+      for (int j = 0; j < 2; ++j) {
+        const int k = t[2 + j];
+        l[1 + j] = k < 0 ? -1 : pos[k] - gstart[p];
+        if (k >= 0 && gstart[pos[k]] != gstart[p]) tp.group_ok = false;
+      }
+    }
   for (int g = 0; g < ng; ++g) {
     tp.gmax = std::max(tp.gmax, glev[glev_ptr[g + 1] - 1] - glev[glev_ptr[g]]);
     tp.nlev_max = std::max(tp.nlev_max, glev_ptr[g + 1] - glev_ptr[g] - 1);
   }
   const std::pair<int**, const std::vector<int>*> up[] = {
       {&tp.rowptr, &trp}, {&tp.colidx, &tci}, {&tp.diag, &tdiag}, {&tp.map, &tmap}, {&tp.order, &order},
-      {&tp.gtask, &gtask}, {&tp.glev, &glev}, {&tp.glev_ptr, &glev_ptr}};
+      {&tp.gtask, &gtask}, {&tp.gloc, &gloc}, {&tp.glev, &glev}, {&tp.glev_ptr, &glev_ptr}};
   for (const auto& u : up) {
     cudaError_t e = cudaMalloc((void**)u.first, sizeof(int) * u.second->size());
     if (e == cudaSuccess) e = cudaMemcpy(*u.first, u.second->data(), sizeof(int) * u.second->size(),
@@ -366,7 +385,7 @@ cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStr
   if (w->tp.tile && w->tp.group_ok && gsched >= 3) {
     // tiled / grouped factors: one CTA per group, no waits across CTAs
     const IluTilePlan& tp = w->tp;
-    const icx::IluGroupShape gs{tp.ngroups, tp.gmax, tp.nlev_max, gsched == 4};
+    const icx::IluGroupShape gs{tp.ngroups, tp.gmax, tp.nlev_max, gsched, tp.gloc};
     const int ctas = dm.tile.flow_ctas[pi];
     return mixed ? icx::la_ilu_apply_groups_f32(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, ctas, w->pc32,
                                                 w->uinv32, x, z, w->pct, w->pc_err, s)

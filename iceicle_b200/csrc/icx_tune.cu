@@ -220,17 +220,18 @@ struct Tuner {
       if ((st = check_err()) != ICX_OK) { dm.tile = keep; return st; }
       if ((st = time([&] { return apply(z1); }, &ms_def[pi])) != ICX_OK ||
           (st = check_err()) != ICX_OK) { dm.tile = keep; return st; }
-      // tiled / grouped factors: the per-group applies (schedules 3 and 4,
-      // whose launch has no CTAs-per-SM choice) are candidates, 4 the default
+      // tiled / grouped factors: the per-group applies (schedules 3 to 5,
+      // whose launch has no CTAs-per-SM choice) are candidates, 5 the default
       const bool grouped = c->ilu_tile != 0 || !c->ilu_groups.empty();
       const int R0 = icx::flow_rows_default(bs), S0 = grouped ? icx::kGroupSchedDefault : icx::kFlowSchedDefault;
       double best = ms_def[pi];
       int best_r = R0, best_c = 2, best_s = S0;
-      for (int sc = 1; sc <= (grouped ? 4 : 2); ++sc)
+      for (int sc = 1; sc <= (grouped ? 5 : 2); ++sc)
       for (int r : icx::kFlowRows) {
         if (!icx::flow_rows_compiled(bs, r)) continue;
         for (int k = 1; k <= MAX_CTAS; ++k) {
           if (sc >= 3 && k > 3) continue;  // 512 / 256 / 128 threads per group CTA
+          if (sc == 5 && r != R0) continue;  // one lane per row: no rows-per-task choice
           if (r == R0 && k == 2 && sc == S0) continue;  // the default, timed above
           dm.tile.flow_rows[pi] = r;
           dm.tile.flow_ctas[pi] = k;
@@ -298,7 +299,7 @@ icx_status icx_tile_set(icx_ctx* c, const icx_tile_choice* t) {
     if (!icx::flow_rows_compiled(bs, t->ilu_rows[k]))
       return fail(c, ICX_ERR_INVALID, "ilu_rows: not compiled for this block size");
     if (t->ilu_ctas[k] < 0 || t->ilu_ctas[k] > MAX_CTAS) return fail(c, ICX_ERR_INVALID, "ilu_ctas: 0..4");
-    if (t->ilu_sched[k] < 0 || t->ilu_sched[k] > 4) return fail(c, ICX_ERR_INVALID, "ilu_sched: 0..4");
+    if (t->ilu_sched[k] < 0 || t->ilu_sched[k] > 5) return fail(c, ICX_ERR_INVALID, "ilu_sched: 0..5");
     if (t->ilu_sched[k] >= 3 && t->ilu_ctas[k] > 3)
       return fail(c, ICX_ERR_INVALID, "ilu_ctas: 0..3 for the group applies (512 / 256 / 128 threads per CTA)");
   }

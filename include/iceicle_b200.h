@@ -601,10 +601,13 @@ icx_status icx_basis_node_coords(const icx_ctx* ctx, double* xy);
  *               on whole-grid factors), 3 on tiled or grouped factors one CTA
  *               per tile running the tile's levels between CTA barriers, 4 the
  *               same with each warp's next task rows copied ahead into shared
- *               memory (the default there; 3 where they do not fit; both 2 on
- *               whole-grid factors); for 3 and 4 ilu_ctas picks the threads
- *               per CTA instead: 0 the default (256 FP64, 512 FP32 factors),
- *               1 / 2 / 3 512 / 256 / 128 */
+ *               memory, 5 one lane per matrix row with the tile's vectors in
+ *               shared memory (the default there; each falls back to the one
+ *               below where its shared memory does not fit; 3 to 5 are 2 on
+ *               whole-grid factors; 5 sums each row's columns in order, so
+ *               its results differ from the others' in rounding); for 3 to 5
+ *               ilu_ctas picks the threads per CTA instead: 0 the default
+ *               (256 FP64, 512 FP32 factors), 1 / 2 / 3 512 / 256 / 128 */
 typedef struct icx_tile_choice {
   int face_minb;
   int vol_threads, vol_minb;

@@ -5,11 +5,15 @@
   tile's own blocks), then the two triangular solves, at 1e-12 of the result
   (FP64 factors) and 1e-5 (FP32 factors).
 * A tile at least as large as the grid is plain ILU(0): bit-identical to the
-  untiled apply.
+  untiled apply with the per-tile apply that sums like the data-flow apply
+  (schedule 4), within 1e-14 of it with the one-lane-per-row apply (5, the
+  default on tiles).
 * The per-tile applies (one CTA per tile, levels in turn; matrix rows in
   registers or staged in shared memory) and the data-flow apply of the same
   tiled factors are bit-identical for every compiled rows per task, in FP64
-  and FP32 factors, on ragged tiles.
+  and FP32 factors, on ragged tiles; the one-lane-per-row apply is
+  bit-identical across its CTA sizes and within 1e-13 (FP64) / 1e-5 (FP32)
+  of the others.
 * The preconditioner changes GMRES iterations only: Newton with tiled ILU
   reaches the untiled converged state to 1e-10 of the initial state's L2
   norm (the steady state of this Burgers problem is u = 0).
@@ -116,7 +120,8 @@ def test_tile_apply_equals_data_flow_apply_bitwise(kw, tile):
         for rows in (2, 4, 6, 8):
             ys = {}
             # data flow; per-tile applies in registers / staged, 512 / 256 / 128 threads per CTA
-            for sched, k in ((2, 0), (4, 0), (3, 0), (4, 1), (4, 2), (4, 3), (3, 1), (3, 3)):
+            for sched, k in ((2, 0), (4, 0), (3, 0), (4, 1), (4, 2), (4, 3), (3, 1), (3, 3),
+                             (5, 0), (5, 1), (5, 2), (5, 3)):
                 ctx.tile = {"ilu_sched": [sched, sched], "ilu_rows": [rows, rows], "ilu_ctas": [k, k]}
                 y = torch.full_like(x, float("nan"))
                 ctx.ilu_apply(vals, x, y, precision, 1, repeat=2)
@@ -125,9 +130,12 @@ def test_tile_apply_equals_data_flow_apply_bitwise(kw, tile):
             y0 = ys.pop((2, 0))
             assert torch.isfinite(y0).all()
             for key, y in ys.items():
-                if not torch.equal(y0.view(torch.int64), y.view(torch.int64)):
-                    d = (y - y0).abs()
+                ref = ys[(5, 0)] if key[0] == 5 else y0
+                if not torch.equal(ref.view(torch.int64), y.view(torch.int64)):
+                    d = (y - ref).abs()
                     bad.append((precision, rows, key, int((d > 0).sum()), float(d.max())))
+            tol = 1e-13 if precision == 0 else 1e-5
+            assert float((ys[(5, 0)] - y0).abs().max()) <= tol * float(y0.abs().max()), (precision, rows)
     assert not bad, bad
     ctx.tile = {}
     ctx.close()
@@ -139,12 +147,17 @@ def test_tile_covering_grid_is_plain_ilu():
     vals, _, _, _ = _jacobian(ctx, spec)
     x = torch.from_numpy(np.random.default_rng(9).standard_normal(ctx.layout.n_dof)).cuda()
     y0, y1 = torch.empty_like(x), torch.empty_like(x)
+    y5 = torch.empty_like(x)
     ctx.ilu_tile = 0
     ctx.ilu_apply(vals, x, y0, 0, 1)
     ctx.ilu_tile = 8
+    ctx.ilu_apply(vals, x, y5, 0, 1)
+    ctx.tile = {"ilu_sched": [4, 4]}
     ctx.ilu_apply(vals, x, y1, 0, 1)
+    ctx.tile = {}
     torch.cuda.synchronize()
     assert torch.equal(y0.view(torch.int64), y1.view(torch.int64))
+    assert float((y5 - y0).abs().max()) <= 1e-14 * float(y0.abs().max())
     ctx.close()
 
 
