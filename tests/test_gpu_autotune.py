@@ -113,7 +113,7 @@ def test_tile_set_refuses_uncompiled_shapes():
     spec, c, u, ctx = _setup(dict(pde=BURGERS, nx=3, ny=3, p=1, g=1))  # 4 x 4 blocks: rows 2 and 4 only
     bad = [{"face_minb": 2}, {"face_minb": 7}, {"vol_threads": 128, "vol_minb": 4}, {"vol_threads": 512},
            {"ilu_rows": [6, 0]}, {"ilu_rows": [0, 3]}, {"ilu_ctas": [5, 0]}, {"ilu_ctas": [0, -1]},
-           {"ilu_sched": [5, 0]}, {"ilu_sched": [0, -1]}]
+           {"ilu_sched": [6, 0]}, {"ilu_sched": [0, -1]}, {"ilu_sched": [5, 0], "ilu_ctas": [4, 0]}]
     for t in bad:
         with pytest.raises(icx.IcxError):
             ctx.tile = t
