@@ -930,24 +930,32 @@ __device__ inline TA vec_at(const V& v, int i) {
   else return reinterpret_cast<const TA*>(&v)[i];
 }
 
-// acc += sign * A_row . x over the BS columns, in column order
-template <int BS, int VEC, bool NEG, class TA>
-__device__ inline TA row_dot(const TA* __restrict__ arow, const TA* xs, TA acc) {
+// one factor row, held in registers (all its loads issued before any use)
+template <int BS, class TA>
+struct FactorRow {
+  static constexpr int VEC = group_rows_vec<BS, TA>();
   using V = typename VecOf<TA, VEC>::type;
+  V v[BS / VEC];
+  __device__ inline void load(const TA* __restrict__ arow) {
 #pragma unroll
-  for (int c = 0; c < BS; c += VEC) {
-    const V av = *reinterpret_cast<const V*>(arow + c);
-    const V xv = *reinterpret_cast<const V*>(xs + c);
-#pragma unroll
-    for (int i = 0; i < VEC; ++i)
-      acc = fused_madd(NEG ? -vec_at<V, TA>(av, i) : vec_at<V, TA>(av, i), vec_at<V, TA>(xv, i), acc);
+    for (int c = 0; c < BS / VEC; ++c) v[c] = __ldg(reinterpret_cast<const V*>(arow) + c);
   }
-  return acc;
-}
+  // acc += sign * row . x over the BS columns, in column order
+  template <bool NEG>
+  __device__ inline TA dot(const TA* xs, TA acc) const {
+#pragma unroll
+    for (int c = 0; c < BS / VEC; ++c) {
+      const V xv = reinterpret_cast<const V*>(xs)[c];
+#pragma unroll
+      for (int i = 0; i < VEC; ++i)
+        acc = fused_madd(NEG ? -vec_at<V, TA>(v[c], i) : vec_at<V, TA>(v[c], i), vec_at<V, TA>(xv, i), acc);
+    }
+    return acc;
+  }
+};
 
 template <int BS, class TA, int NT>
 __global__ void __launch_bounds__(NT) ilu_apply_group_rows_kernel(IluGroupArgs<TA> a) {
-  constexpr int VEC = group_rows_vec<BS, TA>();
   constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ int slev[kGroupLevelsSmem + 1];
@@ -994,14 +1002,23 @@ __global__ void __launch_bounds__(NT) ilu_apply_group_rows_kernel(IluGroupArgs<T
       }
       TA acc = TA(0);
       const TA* xs = fwd ? fs : ys;
-      if (nbk > 0) acc = row_dot<BS, VEC, true>(a.LU + ((size_t)inf.y * BS + r) * BS, xs + (size_t)loc.y * BS, acc);
-      if (nbk > 1)
-        acc = row_dot<BS, VEC, true>(a.LU + ((size_t)(inf.y + 1) * BS + r) * BS, xs + (size_t)loc.z * BS, acc);
+      // both off-diagonal rows in flight together (the second block's row
+      // loads the diagonal inverse's row on a backward row with one block)
+      FactorRow<BS, TA> r0, r1;
+      if (nbk > 0) r0.load(a.LU + ((size_t)inf.y * BS + r) * BS);
+      if (nbk > 1) r1.load(a.LU + ((size_t)(inf.y + 1) * BS + r) * BS);
+      else if (!fwd) r1.load(a.Uinv + ((size_t)inf.x * BS + r) * BS);
+      const double xe = fwd ? a.x[(size_t)inf.x * BS + r] : 0.0;
+      if (nbk > 0) acc = r0.template dot<true>(xs + (size_t)loc.y * BS, acc);
+      if (nbk > 1) {
+        acc = r1.template dot<true>(xs + (size_t)loc.z * BS, acc);
+        if (!fwd) r1.load(a.Uinv + ((size_t)inf.x * BS + r) * BS);
+      }
       if (fwd) {
-        const double fd = a.x[(size_t)inf.x * BS + r] + (double)acc;
+        const double fd = xe + (double)acc;
         fs[(size_t)loc.x * BS + r] = (TA)fd;
       } else {
-        acc = row_dot<BS, VEC, false>(a.Uinv + ((size_t)inf.x * BS + r) * BS, fs + (size_t)loc.x * BS, acc);
+        acc = r1.template dot<false>(fs + (size_t)loc.x * BS, acc);
         a.y[(size_t)inf.x * BS + r] = (double)acc;
         ys[(size_t)loc.x * BS + r] = acc;
       }

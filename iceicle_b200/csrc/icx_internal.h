@@ -74,10 +74,12 @@ inline bool flow_sentinel(const TileChoice& t, int pi) {
 // schedules 3, 4 and 5: the apply on element tiles / groups with one CTA
 // per group (la_ilu_apply_groups), 4 with the matrix rows staged in shared
 // memory, 5 with one lane per row and the group's vectors in shared memory,
-// each where it fits; 5 is the default when the factors are tiled or grouped
-constexpr int kGroupSchedDefault = 5;
+// each where it fits; when the factors are tiled or grouped the default is
+// 5 for FP32 factors (pi = 1) and 4 for FP64 ones (whose rows of 16-byte
+// pairs need twice the registers)
+inline int group_sched_default(int pi) { return pi == 1 ? 5 : 4; }
 inline int ilu_schedule(const TileChoice& t, int pi, bool grouped) {
-  const int sc = t.flow_sched[pi] ? t.flow_sched[pi] : (grouped ? kGroupSchedDefault : kFlowSchedDefault);
+  const int sc = t.flow_sched[pi] ? t.flow_sched[pi] : (grouped ? group_sched_default(pi) : kFlowSchedDefault);
   return (sc >= 3 && !grouped) ? kFlowSchedDefault : sc;
 }
 

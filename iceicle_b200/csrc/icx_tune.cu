@@ -221,9 +221,10 @@ struct Tuner {
       if ((st = time([&] { return apply(z1); }, &ms_def[pi])) != ICX_OK ||
           (st = check_err()) != ICX_OK) { dm.tile = keep; return st; }
       // tiled / grouped factors: the per-group applies (schedules 3 to 5,
-      // whose launch has no CTAs-per-SM choice) are candidates, 5 the default
+      // whose launch has no CTAs-per-SM choice) are candidates, 5 (FP32) or
+      // 4 (FP64) the default
       const bool grouped = c->ilu_tile != 0 || !c->ilu_groups.empty();
-      const int R0 = icx::flow_rows_default(bs), S0 = grouped ? icx::kGroupSchedDefault : icx::kFlowSchedDefault;
+      const int R0 = icx::flow_rows_default(bs), S0 = grouped ? icx::group_sched_default(pi) : icx::kFlowSchedDefault;
       double best = ms_def[pi];
       int best_r = R0, best_c = 2, best_s = S0;
       for (int sc = 1; sc <= (grouped ? 5 : 2); ++sc)

@@ -602,7 +602,8 @@ icx_status icx_basis_node_coords(const icx_ctx* ctx, double* xy);
  *               per tile running the tile's levels between CTA barriers, 4 the
  *               same with each warp's next task rows copied ahead into shared
  *               memory, 5 one lane per matrix row with the tile's vectors in
- *               shared memory (the default there; each falls back to the one
+ *               shared memory (the defaults there: 5 for FP32 factors, 4 for
+ *               FP64 ones; each falls back to the one
  *               below where its shared memory does not fit; 3 to 5 are 2 on
  *               whole-grid factors; 5 sums each row's columns in order, so
  *               its results differ from the others' in rounding); for 3 to 5

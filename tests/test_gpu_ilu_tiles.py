@@ -6,8 +6,8 @@
   (FP64 factors) and 1e-5 (FP32 factors).
 * A tile at least as large as the grid is plain ILU(0): bit-identical to the
   untiled apply with the per-tile apply that sums like the data-flow apply
-  (schedule 4), within 1e-14 of it with the one-lane-per-row apply (5, the
-  default on tiles).
+  (schedule 4, the FP64 default on tiles), within 1e-14 of it with the
+  one-lane-per-row apply (5, the FP32 default).
 * The per-tile applies (one CTA per tile, levels in turn; matrix rows in
   registers or staged in shared memory) and the data-flow apply of the same
   tiled factors are bit-identical for every compiled rows per task, in FP64
@@ -151,9 +151,9 @@ def test_tile_covering_grid_is_plain_ilu():
     ctx.ilu_tile = 0
     ctx.ilu_apply(vals, x, y0, 0, 1)
     ctx.ilu_tile = 8
-    ctx.ilu_apply(vals, x, y5, 0, 1)
-    ctx.tile = {"ilu_sched": [4, 4]}
     ctx.ilu_apply(vals, x, y1, 0, 1)
+    ctx.tile = {"ilu_sched": [5, 5]}
+    ctx.ilu_apply(vals, x, y5, 0, 1)
     ctx.tile = {}
     torch.cuda.synchronize()
     assert torch.equal(y0.view(torch.int64), y1.view(torch.int64))
