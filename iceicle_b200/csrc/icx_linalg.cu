@@ -292,56 +292,6 @@ __global__ void maxpy_kernel(long long n, const TV* __restrict__ V, long long ld
   }
 }
 
-// A classical Gram-Schmidt update fused with the reductions of the next
-// pass: w[i] -= sum_j h_j V_j[i] (the sum in j order, as maxpy_kernel
-// forms it), then with DOTS the per-block partial dots V_j . w of the
-// updated w (j < nvec <= G), else the partial |w|^2. One read of the basis
-// from memory per pass instead of two: the dots reload V_j[i] from L1
-// (__ldca) rather than hold G values per thread.
-template <class TV, int G, bool DOTS>
-__global__ void __launch_bounds__(256, sizeof(TV) == 4 ? 2 : 1) orth_update_kernel(long long n, const TV* __restrict__ V, long long ld,
-                                                          int nvec, const double* __restrict__ h,
-                                                          double* __restrict__ w, double* __restrict__ partial) {
-  constexpr int NA = DOTS ? G : 1;
-  __shared__ double sh[G];
-  __shared__ double red[NA][8];
-  for (int j = threadIdx.x; j < G; j += blockDim.x) sh[j] = j < nvec ? h[j] : 0.0;
-  __syncthreads();
-  double acc[NA];
-#pragma unroll
-  for (int g = 0; g < NA; ++g) acc[g] = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    double sum = 0.0;
-#pragma unroll
-    for (int j = 0; j < G; ++j)
-      if (j < nvec) sum += sh[j] * (double)__ldca(V + (size_t)j * ld + i);
-    const double wn = w[i] + (-1.0) * sum;
-    w[i] = wn;
-    if constexpr (DOTS) {
-#pragma unroll
-      for (int j = 0; j < G; ++j)
-        if (j < nvec) acc[j] += (double)__ldca(V + (size_t)j * ld + i) * wn;
-    } else {
-      acc[0] += wn * wn;
-    }
-  }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-  for (int g = 0; g < NA; ++g) {
-    double v = acc[g];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    if (lane == 0) red[g][warp] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < NA && (!DOTS || (int)threadIdx.x < nvec)) {
-    double t = 0.0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) t += red[threadIdx.x][k];
-    partial[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
-  }
-}
-
 // v32 = a x rounded to FP32
 __global__ void scale_to_f32_kernel(long long n, double a, const double* __restrict__ x, float* __restrict__ v32) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -414,44 +364,6 @@ cudaError_t la_maxpy32(long long n, const float* V, long long ld, int nvec, cons
                        cudaStream_t s) {
   maxpy_kernel<float><<<grid_for(n), 256, 0, s>>>(n, V, ld, nvec, d_h, sign, w);
   return cudaGetLastError();
-}
-
-// classical Gram-Schmidt twice against the nvec basis vectors V (stride
-// ld), then |x|^2: d_h1 = V^T x, x -= V d_h1, d_h2 = V^T x, x -= V d_h2,
-// *d_norm2 = |x|^2. Up to kOrthFused vectors the updates carry the next
-// pass's reductions (three reads of the basis); more: the plain sequence
-template <class TV>
-static cudaError_t cgs2_t(LinalgWork& w, long long n, const TV* V, long long ld, int nvec, double* x, double* d_h1,
-                          double* d_h2, double* d_norm2, cudaStream_t s) {
-  const int nb = kMdotBlocks;
-  if (nvec > kOrthFused) {
-    for (int pass = 0; pass < 2; ++pass) {
-      double* h = pass == 0 ? d_h1 : d_h2;
-      mdot_grouped_kernel<TV, 8><<<nb, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
-      mdot_final_kernel<<<nvec, 256, 0, s>>>(nb, nvec, w.partial, h);
-      maxpy_kernel<TV><<<grid_for(n), 256, 0, s>>>(n, V, ld, nvec, h, -1.0, x);
-    }
-    mdot_grouped_kernel<double, 8><<<nb, 256, 0, s>>>(n, x, 0, 1, x, w.partial);
-    mdot_final_kernel<<<1, 256, 0, s>>>(nb, 1, w.partial, d_norm2);
-    return cudaGetLastError();
-  }
-  mdot_grouped_kernel<TV, kOrthFused><<<nb, 256, 0, s>>>(n, V, ld, nvec, x, w.partial);
-  mdot_final_kernel<<<nvec, 256, 0, s>>>(nb, nvec, w.partial, d_h1);
-  orth_update_kernel<TV, kOrthFused, true><<<nb, 256, 0, s>>>(n, V, ld, nvec, d_h1, x, w.partial);
-  mdot_final_kernel<<<nvec, 256, 0, s>>>(nb, nvec, w.partial, d_h2);
-  orth_update_kernel<TV, kOrthFused, false><<<nb, 256, 0, s>>>(n, V, ld, nvec, d_h2, x, w.partial);
-  mdot_final_kernel<<<1, 256, 0, s>>>(nb, 1, w.partial, d_norm2);
-  return cudaGetLastError();
-}
-
-cudaError_t la_cgs2(LinalgWork& w, long long n, const double* V, long long ld, int nvec, double* x, double* d_h1,
-                    double* d_h2, double* d_norm2, cudaStream_t s) {
-  return cgs2_t<double>(w, n, V, ld, nvec, x, d_h1, d_h2, d_norm2, s);
-}
-
-cudaError_t la_cgs2_32(LinalgWork& w, long long n, const float* V, long long ld, int nvec, double* x, double* d_h1,
-                       double* d_h2, double* d_norm2, cudaStream_t s) {
-  return cgs2_t<float>(w, n, V, ld, nvec, x, d_h1, d_h2, d_norm2, s);
 }
 
 __global__ void scale_kernel(long long n, double a, const double* __restrict__ x, double* __restrict__ y) {
@@ -926,9 +838,15 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
         cudaError_t e = f32 ? la_f2d(n, vj32, vj, st) : cudaSuccess;
         if (e == cudaSuccess && M) e = (*M)(vj, kb.z, st);
         if (e == cudaSuccess) e = A(M ? kb.z : vj, vj1, st);
-        if (e == cudaSuccess)
-          e = f32 ? la_cgs2_32(*kb.lw, n, kb.V32, n, j + 1, vj1, kb.dh, kb.dh + (m + 2), kb.dh + 2 * (m + 2), st)
-                  : la_cgs2(*kb.lw, n, kb.V, n, j + 1, vj1, kb.dh, kb.dh + (m + 2), kb.dh + 2 * (m + 2), st);
+        for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
+          double* slot = kb.dh + (size_t)pass * (m + 2);
+          e = f32 ? la_mdot32(*kb.lw, n, kb.V32, n, j + 1, vj1, slot, st)
+                  : la_mdot(*kb.lw, n, kb.V, n, j + 1, vj1, slot, st);
+          if (e == cudaSuccess)
+            e = f32 ? la_maxpy32(n, kb.V32, n, j + 1, slot, -1.0, vj1, st)
+                    : la_maxpy(n, kb.V, n, j + 1, slot, -1.0, vj1, st);
+        }
+        if (e == cudaSuccess) e = la_mdot(*kb.lw, n, vj1, 0, 1, vj1, kb.dh + 2 * (m + 2), st);
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(host_dst, kb.dh, sizeof(double) * 3 * (m + 2), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess && f32) {

@@ -23,14 +23,6 @@ cudaError_t la_mdot(LinalgWork& w, long long n, const double* V, long long ld, i
 cudaError_t la_maxpy(long long n, const double* V, long long ld, int nvec, const double* d_h, double sign, double* w,
                      cudaStream_t s);
 // the same two with an FP32 basis V (products and sums in FP64)
-// classical Gram-Schmidt twice of x against nvec basis vectors, then |x|^2:
-// d_h1 = V^T x, x -= V d_h1, d_h2 = V^T x, x -= V d_h2, *d_norm2 = |x|^2; up
-// to kOrthFused vectors each update carries the next pass's reductions
-constexpr int kOrthFused = 32;
-cudaError_t la_cgs2(LinalgWork& w, long long n, const double* V, long long ld, int nvec, double* x, double* d_h1,
-                    double* d_h2, double* d_norm2, cudaStream_t s);
-cudaError_t la_cgs2_32(LinalgWork& w, long long n, const float* V, long long ld, int nvec, double* x, double* d_h1,
-                       double* d_h2, double* d_norm2, cudaStream_t s);
 cudaError_t la_mdot32(LinalgWork& w, long long n, const float* V, long long ld, int nvec, const double* x,
                       double* d_out, cudaStream_t s);
 cudaError_t la_maxpy32(long long n, const float* V, long long ld, int nvec, const double* d_h, double sign, double* w,
