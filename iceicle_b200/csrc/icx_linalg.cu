@@ -724,6 +724,8 @@ void ArnoldiGraphs::release() {
   seen.clear();
   if (cap) cudaStreamDestroy(cap), cap = nullptr;
   if (hp) cudaFreeHost(hp), hp = nullptr;
+  for (cudaEvent_t& ev : done)
+    if (ev) cudaEventDestroy(ev), ev = nullptr;
   key = 0;
   m = 0;
 }
@@ -738,7 +740,9 @@ static bool arnoldi_graphs_ready(ArnoldiGraphs& g, unsigned long long key, int m
     g.seen.assign(m, 0);
   }
   if (!g.cap && cudaStreamCreateWithFlags(&g.cap, cudaStreamNonBlocking) != cudaSuccess) return false;
-  if (!g.hp && cudaMallocHost((void**)&g.hp, sizeof(double) * 3 * (m + 2)) != cudaSuccess) return false;
+  if (!g.hp && cudaMallocHost((void**)&g.hp, sizeof(double) * 6 * (m + 2)) != cudaSuccess) return false;
+  for (cudaEvent_t& ev : g.done)
+    if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return false;
   if (g.key != key) {
     g.reset();
     g.key = key;
@@ -748,7 +752,8 @@ static bool arnoldi_graphs_ready(ArnoldiGraphs& g, unsigned long long key, int m
 
 // the graph of Arnoldi step j: captured on the step's second eager run under
 // the current key (the first run has done every one-time setup of the
-// kernels it launches), then replayed. Null: run the step eagerly.
+// kernels it launches), then replayed; it copies its reductions to host
+// half j % 2. Null: run the step eagerly.
 template <class Step>
 static cudaGraphExec_t arnoldi_graph(ArnoldiGraphs& g, int j, long long n, double* vj1, const double* h2, Step& step,
                                      bool append_normalize) {
@@ -758,7 +763,7 @@ static cudaGraphExec_t arnoldi_graph(ArnoldiGraphs& g, int j, long long n, doubl
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamBeginCapture(g.cap, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    cudaError_t es = step(g.cap, g.hp);
+    cudaError_t es = step(g.cap, g.hp + (size_t)(j & 1) * 3 * (g.m + 2));
     if (es == cudaSuccess && append_normalize) {
       normalize_kernel<<<grid_for(n), 256, 0, g.cap>>>(n, h2, vj1);
       es = cudaGetLastError();
@@ -820,6 +825,11 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
     g[0] = beta;
     int j = 0;
     double resid = beta;
+    // replayed steps run one ahead: step j + 1 (whose inputs the device
+    // forms: v_j+1 is normalised inside step j's graph) is launched before
+    // the host waits for step j, so the host's rotations overlap it; a step
+    // launched past convergence only writes scratch the solve overwrites
+    bool ahead = false;
     for (; j < m && total < maxit; ++j) {
       double* vj = f32 ? kb.vt : kb.V + (size_t)j * n;
       double* vj1 = f32 ? kb.w : kb.V + (size_t)(j + 1) * n;
@@ -860,10 +870,22 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
       cudaGraphExec_t gx =
           use_graphs ? arnoldi_graph(*kb.graphs, j, n, vj1, kb.dh + 2 * (m + 2), step, !f32) : nullptr;
       if (gx) {
-        GCK(cudaGraphLaunch(gx, s));
-        GCK(cudaStreamSynchronize(s));
-        std::copy(kb.graphs->hp, kb.graphs->hp + 3 * (m + 2), hp3.begin());
-        ++kb.graph_launches;
+        ArnoldiGraphs& ag = *kb.graphs;
+        if (!ahead) {
+          GCK(cudaGraphLaunch(gx, s));
+          GCK(cudaEventRecord(ag.done[j & 1], s));
+          ++kb.graph_launches;
+        }
+        ahead = false;
+        if (j + 1 < m && total + 1 < maxit && ag.exec[j + 1]) {
+          GCK(cudaGraphLaunch(ag.exec[j + 1], s));
+          GCK(cudaEventRecord(ag.done[(j + 1) & 1], s));
+          ++kb.graph_launches;
+          ahead = true;
+        }
+        GCK(cudaEventSynchronize(ag.done[j & 1]));
+        const double* hj = ag.hp + (size_t)(j & 1) * 3 * (m + 2);
+        std::copy(hj, hj + 3 * (m + 2), hp3.begin());
       } else {
         GCK(step(s, hp3.data()));
         GCK(cudaStreamSynchronize(s));

@@ -118,7 +118,9 @@ struct ArnoldiGraphs {
   std::vector<int> seen;              // [m] eager runs of step j under this key
   bool failed = false;                // a capture failed under this key: eager steps only
   cudaStream_t cap = nullptr;         // capture stream
-  double* hp = nullptr;               // pinned host copy of the step's reductions, 3 (m + 2) doubles
+  double* hp = nullptr;               // pinned host copies of the steps' reductions, 2 x 3 (m + 2) doubles:
+                                      // step j writes half j % 2, so step j + 1 may run while the host reads j
+  cudaEvent_t done[2] = {nullptr, nullptr};  // completion of the last step launched into each half
   // drops the graphs (the key changed)
   void reset();
   // drops everything (owner teardown)
