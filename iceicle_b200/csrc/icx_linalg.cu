@@ -366,6 +366,38 @@ cudaError_t la_maxpy32(long long n, const float* V, long long ld, int nvec, cons
   return cudaGetLastError();
 }
 
+// matrix-free products: slot = {|v|^2, c}, h = c / |v| (c when v = 0)
+__device__ inline double fd_step(const double* slot) {
+  const double v2 = slot[0];
+  return v2 > 0.0 ? slot[1] / sqrt(v2) : slot[1];
+}
+
+__global__ void fd_perturb_kernel(long long n, const double* __restrict__ u, const double* __restrict__ v,
+                                  const double* __restrict__ slot, double* __restrict__ up) {
+  const double h = fd_step(slot);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    up[i] = u[i] + h * v[i];
+}
+
+__global__ void fd_diff_kernel(long long n, const double* __restrict__ rp, const double* __restrict__ r0,
+                               const double* __restrict__ slot, double* __restrict__ y) {
+  const double h = fd_step(slot);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = (rp[i] - r0[i]) / h;
+}
+
+cudaError_t la_fd_perturb(long long n, const double* u, const double* v, const double* slot, double* up,
+                          cudaStream_t s) {
+  fd_perturb_kernel<<<grid_for(n), 256, 0, s>>>(n, u, v, slot, up);
+  return cudaGetLastError();
+}
+
+cudaError_t la_fd_diff(long long n, const double* rp, const double* r0, const double* slot, double* y,
+                       cudaStream_t s) {
+  fd_diff_kernel<<<grid_for(n), 256, 0, s>>>(n, rp, r0, slot, y);
+  return cudaGetLastError();
+}
+
 __global__ void scale_kernel(long long n, double a, const double* __restrict__ x, double* __restrict__ y) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     y[i] = a * x[i];

@@ -23,6 +23,12 @@ cudaError_t la_mdot(LinalgWork& w, long long n, const double* V, long long ld, i
 cudaError_t la_maxpy(long long n, const double* V, long long ld, int nvec, const double* d_h, double sign, double* w,
                      cudaStream_t s);
 // the same two with an FP32 basis V (products and sums in FP64)
+// matrix-free Jacobian products with slot = {|v|^2, c} on the device and
+// h = c / |v|: up = u + h v, then y = (rp - r0) / h
+cudaError_t la_fd_perturb(long long n, const double* u, const double* v, const double* slot, double* up,
+                          cudaStream_t s);
+cudaError_t la_fd_diff(long long n, const double* rp, const double* r0, const double* slot, double* y,
+                       cudaStream_t s);
 cudaError_t la_mdot32(LinalgWork& w, long long n, const float* V, long long ld, int nvec, const double* x,
                       double* d_out, cudaStream_t s);
 cudaError_t la_maxpy32(long long n, const float* V, long long ld, int nvec, const double* d_h, double sign, double* w,

@@ -94,6 +94,12 @@ struct icx_solver_work {
   IluTilePlan tp;           // tiled block-ILU(0) pattern and schedule (tp.tile == c->ilu_tile once built)
   int* pc_err = nullptr;    // set by the ILU apply if a dependency wait timed out
   double* dh = nullptr;     // device scalars (dot results)
+  // the matrix-free operator (icx_newton_options.matrix_free) while a Newton
+  // step's linear solve runs: state, its residual, {|v|^2, c} (in dh)
+  bool fd_on = false;
+  const double* fd_u = nullptr;
+  const double* fd_r = nullptr;
+  double* fd_slot = nullptr;
   int* flag = nullptr;
   icx::LinalgWork lw;
 };
@@ -138,7 +144,8 @@ icx_status ensure_work(icx_ctx* c, int m) {
   CK(cudaMalloc((void**)&w->V, sizeof(double) * (size_t)(m + 1) * n));
   double** vecs[] = {&w->w, &w->z, &w->r, &w->res, &w->du, &w->ustep, &w->rwork, &w->pct, &w->pct2, &w->pct3, &w->pct4};
   for (double** p : vecs) CK(cudaMalloc((void**)p, sizeof(double) * n));
-  CK(cudaMalloc((void**)&w->dh, sizeof(double) * 3 * (m + 2)));
+  // 3 (m + 2) GMRES reductions, then the matrix-free products' {|v|^2, c}
+  CK(cudaMalloc((void**)&w->dh, sizeof(double) * (3 * (m + 2) + 2)));
   CK(cudaMalloc((void**)&w->flag, sizeof(int)));
   CK(cudaMalloc((void**)&w->pc_err, sizeof(int)));
   CK(cudaMemset(w->pc_err, 0, sizeof(int)));
@@ -541,7 +548,16 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
     icx::KrylovBuffers* kb;
     ~CountOut() { if (dst) *dst = kb->sample_count; }
   } count_out{sample_count, &kb};
-  icx::LinOp A = [&](const double* xin, double* yout, cudaStream_t st) {
+  icx::LinOp A = [&](const double* xin, double* yout, cudaStream_t st) -> cudaError_t {
+    if (w->fd_on) {
+      // (R(u + h v) - R(u)) / h, h from |v| on the device; the perturbed
+      // state and residual in ustep / rwork (free while the solve runs)
+      cudaError_t e = icx::la_mdot(w->lw, w->n, xin, 0, 1, xin, w->fd_slot, st);
+      if (e == cudaSuccess) e = icx::la_fd_perturb(w->n, w->fd_u, xin, w->fd_slot, w->ustep, st);
+      if (e == cudaSuccess) e = icx::launch_residual(dm, c->phys, w->ustep, w->rwork, st);
+      if (e == cudaSuccess) e = icx::la_fd_diff(w->n, w->rwork, w->fd_r, w->fd_slot, yout, st);
+      return e;
+    }
     return mixed ? icx::launch_bsr_spmv_f32(dm, w->vals32, xin, yout, st) : icx::launch_bsr_spmv(dm, w->vals, xin, yout, st);
   };
   icx::LinOp M = [&](const double* xin, double* yout, cudaStream_t st) { return apply_pc(c, pc, mixed, xin, yout, st); };
@@ -558,7 +574,8 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
     for (long long v : {(long long)pc, (long long)mixed, (long long)w->sweeps, (long long)m, (long long)t.flow_rows[pi],
                         (long long)t.flow_ctas[pi], (long long)t.flow_sched[pi], (long long)(uintptr_t)dm.bsr_rowptr,
                         (long long)(uintptr_t)dm.bsr_colidx, (long long)(uintptr_t)dm.bsr_diag,
-                        (long long)(uintptr_t)w->order, (long long)w->tp.tile, (long long)(uintptr_t)w->tp.order})
+                        (long long)(uintptr_t)w->order, (long long)w->tp.tile, (long long)(uintptr_t)w->tp.order,
+                        (long long)w->fd_on, (long long)(uintptr_t)w->fd_u, (long long)(uintptr_t)w->fd_r})
       key = (key ^ (unsigned long long)v) * 1099511628211ull;
     kb.graphs = &w->graphs;
     kb.graph_key = key | 1;
@@ -720,6 +737,7 @@ icx_status icx_newton_default_options(icx_newton_options* o) {
   o->pc_sweeps = 2;
   o->cuda_graphs = 1;
   o->ilu_tile = 0;           // block-ILU(0) over the whole grid in natural order
+  o->matrix_free = 0;        // the assembled Jacobian's BSR product
   return ICX_OK;
 }
 
@@ -922,6 +940,20 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
       CK(cudaMemcpyAsync(&fl, w->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
       SYNC_AT("preconditioner");
       if (fl == 2) return set_err(c, ICX_ERR_CUDA, "block-ILU factorization: block index out of range");
+    }
+    // the matrix-free operator at this state: c = sqrt(eps) (sqrt(n) + |u|)
+    struct FdScope {
+      icx_solver_work* w;
+      ~FdScope() { w->fd_on = false; }
+    } fd_scope{w};
+    if (opt->matrix_free) {
+      const double cval = eps * (std::sqrt((double)n) + dev_norm(c, d_u, s));
+      w->fd_slot = w->dh + 3 * (w->m + 2);
+      CK(cudaMemcpyAsync(w->fd_slot + 1, &cval, sizeof(double), cudaMemcpyHostToDevice, s));
+      CK(cudaStreamSynchronize(s));
+      w->fd_u = d_u;
+      w->fd_r = w->res;
+      w->fd_on = true;
     }
     int it = 0;
     double rr = 0.0;

@@ -327,6 +327,14 @@ typedef struct icx_newton_options {
    * (icx_set_ilu_tile). Changes the preconditioner and so the GMRES
    * iterations, not the converged state. */
   int ilu_tile;
+  /* 1: the GMRES operator is the directional difference of the FP64
+   * residual, J v ~ (R(u + h v) - R(u)) / h with h = sqrt(DBL_EPSILON)
+   * (sqrt(n) + |u|) / |v| (the matrix-free products of icx_mfnk_solve); the
+   * assembled FD Jacobian then serves the preconditioner only (PETSc's
+   * -snes_mf_operator). One residual evaluation per Krylov step instead of
+   * the BSR product, in every precision mode. 0 (default): the assembled
+   * Jacobian's BSR product. */
+  int matrix_free;
 } icx_newton_options;
 
 typedef struct icx_newton_report {
