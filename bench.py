@@ -78,6 +78,8 @@ def parse():
                          "tiles (0: the whole grid) and print one JSON line")
     ap.add_argument("--solve-precision", type=int, default=1, metavar="P",
                     help="Newton precision of --solve (0 FP64, 1 mixed, 2 FP32 flux quadrature)")
+    ap.add_argument("--solve-matrix-free", action="store_true",
+                    help="--solve with the matrix-free GMRES operator (residual differences)")
     ap.add_argument("--no-tune", action="store_true",
                     help="time the compiled default launch shapes instead of the autotuned ones")
     ap.add_argument("--tile", default="", metavar="K=V,...",
@@ -477,7 +479,8 @@ def newton_bench(torch, dev, tune=True):
                                 "ilu_ms_default": t["ilu_ms_default"], "ilu_ms_tuned": t["ilu_ms_tuned"]}
         states = {}
         tile = 8 if name.startswith("burgers") else 32
-        for label, prec, t in (("fp64", 0, 0), ("mixed", 1, 0), ("mixed_tiled", 1, tile), ("quad32_tiled", 2, tile)):
+        for label, prec, t, mf in (("fp64", 0, 0, 0), ("mixed", 1, 0, 0), ("mixed_tiled", 1, tile, 0),
+                                   ("quad32_tiled", 2, tile, 0), ("mixed_tiled_matrix_free", 1, tile, 1)):
             if tune and t and "autotune_tiled" not in rows:
                 # the apply's launch shapes for the tiled pattern
                 wl.ctx.ilu_tile = t
@@ -487,6 +490,7 @@ def newton_bench(torch, dev, tune=True):
             opt = ib.default_newton_options()
             opt.precision = prec
             opt.ilu_tile = t
+            opt.matrix_free = mf
             u = torch.from_numpy(wl.u0).to(dev)
             if name.startswith("burgers"):
                 wl.ctx.newton_solve(torch.from_numpy(wl.u0).to(dev), opt)  # warm-up (one-time setup)
@@ -497,11 +501,11 @@ def newton_bench(torch, dev, tune=True):
             e1.record()
             torch.cuda.synchronize(dev)
             states[label] = u.cpu().numpy()
-            rows[label] = {"s": e0.elapsed_time(e1) * 1e-3, "ilu_tile": t, "newton_its": rep.iterations,
+            rows[label] = {"s": e0.elapsed_time(e1) * 1e-3, "ilu_tile": t, "matrix_free": mf, "newton_its": rep.iterations,
                            "gmres_its": rep.linear_iterations_total, "r_final": rep.r_final,
                            "converged": bool(rep.converged)}
         a = states["fp64"]
-        for label in ("mixed", "mixed_tiled", "quad32_tiled"):
+        for label in ("mixed", "mixed_tiled", "quad32_tiled", "mixed_tiled_matrix_free"):
             rows[f"{label}_vs_fp64_state_l2"] = float(np.linalg.norm(a - states[label]) /
                                                       max(np.linalg.norm(wl.u0), 1e-300))
             rows[f"speedup_{label}_vs_fp64"] = rows["fp64"]["s"] / rows[label]["s"]
@@ -650,9 +654,12 @@ def learned_bench(torch, dev, tune=True, n_seeds=3):
         return {"unavailable": f"model file does not fit the network: {exc}"}
     sw = m.sweeps if m.sweeps is not None else 0
     tile = m.ilu_tile if m.ilu_tile is not None else 0
+    # a held-out selection that kept none of the correction leaves the output
+    # layer zero: preconditioner 5 is then its base (the tiled block-ILU(0))
     out = {"model": {"params": m.n_params, "pc_sweeps": sw, "ilu_tile": tile,
+                     "correction_zero": bool(lp.correction_is_zero(m)),
                      "file": "iceicle_b200/data/learned_pc_ns_p2.npz"}, "instances": []}
-    speed = []
+    speed, speed_mf = [], []
     for seed, re in lp.instances(*lp.EVAL_INSTANCES)[:n_seeds]:
         wl = lp.make_instance(seed, re, 256, dev.index)
         tuned = None
@@ -669,18 +676,28 @@ def learned_bench(torch, dev, tune=True, n_seeds=3):
                               "ilu_ms_tuned": t2["ilu_ms_tuned"]}
         tiled, _ = lp.solve(wl, None, 2, 1, 0, dev.index, tile)
         learned, u_l = lp.solve(wl, m, 5, 1, sw, dev.index, tile)
+        # the same with the matrix-free operator (assembled Jacobian for the preconditioner only)
+        tiled_mf, _ = lp.solve(wl, None, 2, 1, 0, dev.index, tile, matrix_free=1)
+        learned_mf, u_lm = lp.solve(wl, m, 5, 1, sw, dev.index, tile, matrix_free=1)
         del wl
         rec = {"seed": seed, "re": re, "mesh": "256x256", "p": 2, "n_dof": 256 * 256 * 36,
                "plain_fp64_ilu0": plain, "mixed_ilu0": mixed, "mixed_ilu0_tiled": tiled, "learned_mixed": learned,
+               "mixed_ilu0_tiled_matrix_free": tiled_mf, "learned_mixed_matrix_free": learned_mf,
                "autotune": tuned,
                "learned_vs_plain_state_l2": float(np.linalg.norm(u_l - u_p) / np.linalg.norm(u_p)),
+               "learned_matrix_free_vs_plain_state_l2": float(np.linalg.norm(u_lm - u_p) / np.linalg.norm(u_p)),
                "speedup_learned_mixed_vs_plain_fp64": plain["s"] / learned["s"],
+               "speedup_learned_mixed_matrix_free_vs_plain_fp64": plain["s"] / learned_mf["s"],
                "speedup_mixed_ilu0_vs_plain_fp64": plain["s"] / mixed["s"],
-               "speedup_mixed_ilu0_tiled_vs_plain_fp64": plain["s"] / tiled["s"]}
+               "speedup_mixed_ilu0_tiled_vs_plain_fp64": plain["s"] / tiled["s"],
+               "speedup_mixed_ilu0_tiled_matrix_free_vs_plain_fp64": plain["s"] / tiled_mf["s"]}
         out["instances"].append(rec)
         speed.append(rec["speedup_learned_mixed_vs_plain_fp64"])
+        speed_mf.append(rec["speedup_learned_mixed_matrix_free_vs_plain_fp64"])
     out["speedup_learned_mixed_vs_plain_fp64"] = {"per_seed": speed, "min": min(speed), "mean": float(np.mean(speed)),
                                                   "target": 3.0}
+    out["speedup_learned_mixed_matrix_free_vs_plain_fp64"] = {"per_seed": speed_mf, "min": min(speed_mf),
+                                                              "mean": float(np.mean(speed_mf)), "target": 3.0}
     return out
 
 
@@ -936,7 +953,7 @@ def jacobian_mode(n):
     print(json.dumps(out))
 
 
-def solve_mode(tile, precision):
+def solve_mode(tile, precision, matrix_free=0):
     """one Newton solve (|r| <= 1e-10, GMRES(30)) of the first evaluation
     instance of the 256 x 256 p = 2 Navier-Stokes problem, launch shapes
     autotuned at the initial state for the chosen tiling; CUDA events around
@@ -951,7 +968,7 @@ def solve_mode(tile, precision):
     wl.ctx.ilu_tile = tile
     wl.ctx.autotune(u0, ib.TUNE_RESIDUAL | ib.TUNE_ILU | ib.TUNE_ILU_FP32)
     opt = ib.default_newton_options()
-    opt.precision, opt.ilu_tile, opt.gmres_max_it = precision, tile, 20000
+    opt.precision, opt.ilu_tile, opt.gmres_max_it, opt.matrix_free = precision, tile, 20000, matrix_free
     u = u0.clone()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
@@ -962,6 +979,7 @@ def solve_mode(tile, precision):
     s = e0.elapsed_time(e1) * 1e-3
     its = rep.linear_iterations_total
     print(json.dumps({"solve": "ns_256x256_p2", "seed": seed, "re": re, "ilu_tile": tile, "precision": precision,
+                      "matrix_free": matrix_free,
                       "converged": bool(rep.converged), "s": s, "newton_its": rep.iterations, "gmres_its": its,
                       "ms_per_gmres_it": 1e3 * s / max(its, 1), "tile_choice": wl.ctx.tile}))
 
@@ -969,7 +987,7 @@ def solve_mode(tile, precision):
 def main():
     a = parse()
     if a.solve >= 0:
-        solve_mode(a.solve, a.solve_precision)
+        solve_mode(a.solve, a.solve_precision, int(a.solve_matrix_free))
         return
     if a.gemm:
         gemm_mode(a.gemm)

@@ -227,6 +227,8 @@ void element_point(const icx_ctx* c, int e, const double xi[2], double x[2]);
 // FP64 Jacobian, the correction z = (I + C) y, and the release of its buffers
 cudaError_t lpc_build(icx_ctx* c, const double* vals, cudaStream_t s);
 cudaError_t lpc_apply(icx_ctx* c, const double* y, double* z, cudaStream_t s);
+// the attached model's output layer is all zero (its correction C = 0)
+bool lpc_zero_correction(const icx_ctx* c);
 void free_lpc_work(icx_ctx* c);
 // releases the host-pipeline streams and buffers (icx_pipeline.cu)
 void free_host_pipe(icx_ctx* c);

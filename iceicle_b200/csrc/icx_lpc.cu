@@ -53,6 +53,9 @@ struct icx_lpc {
   bf16* W2tb = nullptr;   // transposes for the backward pass (W2^T: [2H][H])
   bf16* W3tb = nullptr;
   long long steps = 0;
+  // the output layer (W3, b3) is all zero: C = 0, the preconditioner is its
+  // base (set from host parameters; training clears it)
+  bool zero_correction = false;
 };
 
 // per-context buffers of the learned preconditioner (grown on demand)
@@ -417,6 +420,8 @@ cudaError_t lpc_build(icx_ctx* c, const double* vals, cudaStream_t s) {
   return e != cudaSuccess ? e : (flag ? cudaErrorLaunchTimeout : cudaSuccess);
 }
 
+bool lpc_zero_correction(const icx_ctx* c) { return c->lpc && c->lpc->zero_correction; }
+
 // z = (I + C) y
 cudaError_t lpc_apply(icx_ctx* c, const double* y, double* z, cudaStream_t s) {
   if (!c->lpcw || !c->lpcw->C) return cudaErrorInvalidValue;
@@ -503,6 +508,8 @@ icx_status icx_lpc_set_params(icx_lpc* L, const float* host) {
   cudaSetDevice(L->device);
   if (cudaMemcpy(L->p, host, sizeof(float) * L->np, cudaMemcpyHostToDevice) != cudaSuccess) return ICX_ERR_CUDA;
   if (refresh_bf16(L, 0) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return ICX_ERR_CUDA;
+  L->zero_correction = true;
+  for (size_t i = L->oW3; i < L->np && L->zero_correction; ++i) L->zero_correction = host[i] == 0.0f;
   return ICX_OK;
 }
 
@@ -535,6 +542,7 @@ icx_status icx_lpc_train(icx_ctx* c, const double* d_vals, int n_samples, const 
   icx_lpc* L = c->lpc;
   cudaSetDevice(c->device);
   cudaStream_t s = 0;
+  if (o->steps > 0) L->zero_correction = false;
   // the ILU(0) factors (FP32 copies) of this Jacobian, as preconditioner 5 applies them
   icx_status st = icx::solver_prepare_pc(c, d_vals, 4, o->sweeps);
   if (st != ICX_OK) return st;

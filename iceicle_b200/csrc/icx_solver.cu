@@ -432,7 +432,9 @@ cudaError_t apply_pc(icx_ctx* c, int kind, bool mixed, const double* x, double* 
   }
   if (kind == 5) {
     // learned: z = (I + C) y, y from the ILU(0) factors by `sweeps` Jacobi
-    // sweeps per triangle, or by the exact triangular solves when sweeps = 0
+    // sweeps per triangle, or by the exact triangular solves when sweeps = 0;
+    // a model whose output layer is zero (C = 0) is its base
+    if (icx::lpc_zero_correction(c)) return apply_pc(c, w->sweeps > 0 ? 4 : 2, mixed, x, z, s);
     cudaError_t e = apply_pc(c, w->sweeps > 0 ? 4 : 2, mixed, x, w->pct4, s);
     if (e == cudaSuccess) e = icx::lpc_apply(c, w->pct4, z, s);
     return e;
@@ -482,7 +484,7 @@ cudaError_t build_pc_impl(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(w->flag, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
   const bool jac = kind == 1 || kind == 3, ilu = kind == 2 || kind == 4 || kind == 5;
-  if (kind == 5 && (e = icx::lpc_build(c, w->vals, s)) != cudaSuccess) return e;
+  if (kind == 5 && !icx::lpc_zero_correction(c) && (e = icx::lpc_build(c, w->vals, s)) != cudaSuccess) return e;
   if (jac) e = icx::la_block_invert(dm.E, w->bs, w->vals, dm.bsr_diag, w->pc, w->flag, s);
   long long nv_pc = nv;
   if (ilu) {
@@ -1173,6 +1175,7 @@ bool solver_graphable(icx_ctx* c, int pc, bool mixed) {
   icx_solver_work* w = c->sw;
   if (!w || !w->graphs_on) return false;
   if (pc == 0 || pc == 1 || pc == 3 || pc == 4) return true;
+  if (pc == 5 && icx::lpc_zero_correction(c)) return solver_graphable(c, w->sweeps > 0 ? 4 : 2, mixed);
   if (pc != 2) return false;
   // the group apply and the sentinel schedule launch the same arguments every time
   const int pi = mixed ? 1 : 0;

@@ -128,6 +128,14 @@ def calibrate(model, instance, n=256, samples=167, every=5, sweeps=0, ilu_tile=0
                 loss_scaled=s_aa - 2 * g * s_ab + g * g * s_bb)
 
 
+def correction_is_zero(model):
+    """whether the model's output layer (W3, b3) is all zero: its correction
+    C is then 0 and preconditioner 5 applies its base alone"""
+    D, H = model.bs * model.bs, model.hidden
+    o_w3 = H * D + H + H * 2 * H + H
+    return not np.any(model.get_params()[o_w3:])
+
+
 def select_scale(model, instance, n=256, sweeps=0, ilu_tile=0, candidates=(0.0, 0.25, 0.5, 1.0), device=0):
     """the share g of the correction chosen by what it is for: the learned,
     mixed-precision Newton solve of a held-out instance to |r| <= 1e-10 is
@@ -155,9 +163,11 @@ def select_scale(model, instance, n=256, sweeps=0, ilu_tile=0, candidates=(0.0, 
                 candidates={str(g): dict(gmres_its=v[0], s=v[1], pc_fallbacks=v[2]) for g, v in its.items()})
 
 
-def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu_tile=0):
+def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu_tile=0, matrix_free=0):
     """one Newton solve of an instance to |r| <= 1e-10 (GMRES(30), Wolfe line
-    search), timed with CUDA events; returns (report dict, final state)"""
+    search), timed with CUDA events; matrix_free = 1: the GMRES operator is
+    the residual's directional difference (the assembled Jacobian then only
+    preconditions); returns (report dict, final state)"""
     import torch
     dev = torch.device("cuda", device)
     opt = default_newton_options()
@@ -165,6 +175,7 @@ def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu
     opt.precision = precision
     opt.pc_sweeps = sweeps
     opt.ilu_tile = ilu_tile
+    opt.matrix_free = matrix_free
     opt.gmres_max_it = 20000
     if model is not None:
         wl.ctx.lpc_attach(model)
@@ -177,7 +188,7 @@ def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu
     torch.cuda.synchronize(dev)
     if model is not None:
         wl.ctx.lpc_attach(None)
-    return dict(s=e0.elapsed_time(e1) * 1e-3, ilu_tile=ilu_tile, newton_its=rep.iterations,
+    return dict(s=e0.elapsed_time(e1) * 1e-3, ilu_tile=ilu_tile, matrix_free=matrix_free, newton_its=rep.iterations,
                 gmres_its=rep.linear_iterations_total,
                 gmres_its_per_step=list(rep.linear_iterations[:rep.iterations]), r_final=rep.r_final,
                 converged=bool(rep.converged), pc_fallbacks=rep.pc_fallbacks), u.cpu().numpy()
@@ -215,7 +226,7 @@ def new_model(device=0, seed=0, hidden=256):
 # scaled on a held-out instance: by the training loss (calibrate), then by the
 # GMRES iterations of its Newton solve (select_scale)
 RECIPE = dict(model_seed=1, train_instances=(8, 11), pairs=2000, samples=167, every=5, steps=120, batch=4, random=2,
-              sweeps=0, ilu_tile=32, lr=1e-3, holdout=(1, 5))
+              sweeps=0, ilu_tile=16, lr=1e-3, holdout=(1, 5))
 EVAL_INSTANCES = (3, 99)
 
 

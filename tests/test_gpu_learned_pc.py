@@ -192,3 +192,32 @@ def test_model_save_and_load(tmp_path):
     m.save(tmp_path / "m.npz")
     m2 = ib.LearnedPreconditioner.load(tmp_path / "m.npz")
     assert np.array_equal(m2.get_params(), p)
+
+
+@pytest.mark.parametrize("prec,tile", [(1, 0), (1, 2), (0, 0)])
+def test_zero_output_layer_is_its_base_preconditioner(prec, tile):
+    """a model whose output layer (W3, b3) is zero has C = 0: preconditioner 5
+    is then its base (block-ILU(0), sweeps = 0) without the network's
+    products, and the Newton solve is the base's bit for bit (iterations,
+    GMRES counts, state), its Arnoldi steps replayed as graphs"""
+    from iceicle_b200 import learned_pc as lp
+    spec, ctx, u0 = _ns_ctx()
+    m = ib.LearnedPreconditioner(36, 64, 0, seed=4)
+    p = m.get_params()
+    D, H = 36 * 36, 64
+    p[H * D + H + H * 2 * H + H:] = 0
+    m.set_params(p)
+    assert lp.correction_is_zero(m)
+    out = {}
+    for pc in (2, 5):
+        ctx.lpc_attach(m if pc == 5 else None)
+        o = ib.default_newton_options()
+        o.gmres_max_it, o.preconditioner, o.precision, o.pc_sweeps, o.ilu_tile = 5000, pc, prec, 0, tile
+        u = torch.from_numpy(u0.copy()).cuda()
+        r = ctx.newton_solve(u, o)
+        assert r.converged
+        out[pc] = (u.cpu().numpy(), r.iterations, list(r.linear_iterations[:r.iterations]), r.graph_steps)
+    ctx.lpc_attach(None)
+    (a, ia, la, ga), (b, ib_, lb, gb) = out[2], out[5]
+    assert ia == ib_ and la == lb and gb > 0
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
