@@ -591,7 +591,8 @@ def ilu_bench(n):
                   [(3, 0, "tiles"), (2, 0, "data_flow")])
         for sched, k, sn in shapes:
             ctx.tile = {"ilu_sched": [sched, sched], "ilu_ctas": [k, k]}
-            for prec, pn in ((0, "fp64"), (1, "fp32")):
+            # BF16 factors (FP32 arithmetic) only in the one-lane-per-row form
+            for prec, pn in ((0, "fp64"), (1, "fp32")) + (((2, "bf16"),) if sched == 5 else ()):
                 ctx.ilu_apply(vals, x, y, prec, 0, 3)
                 out[f"tiled{tile}_{sn}_{pn}_ms"] = ctx.ilu_apply(vals, x, y, prec, 0, 20)
     ctx.tile = {}

@@ -8,7 +8,10 @@
 // contiguous 256-byte segment; the R partial sums are reduced across the warp
 // with butterfly shuffles and lane rr stores row r0 + rr.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 namespace icx {
 
@@ -900,62 +903,82 @@ __global__ void __launch_bounds__(NT) ilu_apply_group_async_kernel(IluGroupArgs<
 
 // The group apply with one lane per matrix row: the tasks of a level are
 // its (element, row) pairs, 32 to a warp, and a lane forms its row's sums
-// over the columns in order, reading the factor row with 16-byte loads where
-// rows are 16-byte aligned. The group's forward and backward vectors stay in
-// shared memory (rounded to TA, as the other applies round them on load), so
-// a task's only reads from memory are its factor rows and x; the forward
-// vector is not written back. No warp reductions. The column order of the
-// sums differs from the other applies (not bit-identical to them; identical
-// across thread counts). Dynamic shared memory: 4 gmax entries (int4), then
-// 2 gmax BS values of TA.
-template <int BS, class TA>
-__host__ __device__ constexpr int group_rows_vec() {
-  return (BS * (int)sizeof(TA)) % 16 == 0 ? 16 / (int)sizeof(TA) : 1;
+// over the columns in order, reading the factor row with the widest loads
+// (up to 16 bytes) its alignment allows. The group's forward and backward
+// vectors stay in shared memory (rounded to the arithmetic type, as the
+// other applies round them on load), so a task's only reads from memory are
+// its factor rows and x; the forward vector is not written back. No warp
+// reductions. The column order of the sums differs from the other applies
+// (not bit-identical to them; identical across thread counts). TS is the
+// factors' storage type: double and float are also the arithmetic type,
+// BF16 factors are widened to FP32. Dynamic shared memory: 4 gmax entries
+// (int4), then 2 gmax BS values of the arithmetic type.
+template <class TS>
+struct ComputeOf {
+  using type = TS;
+};
+template <>
+struct ComputeOf<__nv_bfloat16> {
+  using type = float;
+};
+
+// bytes per factor-row load: the widest of 16 / 8 / 4 / 2 dividing a row
+template <int BS, class TS>
+__host__ __device__ constexpr int group_rows_load_bytes() {
+  constexpr int row = BS * (int)sizeof(TS);
+  return row % 16 == 0 ? 16 : row % 8 == 0 ? 8 : row % 4 == 0 ? 4 : (int)sizeof(TS);
 }
 
-template <class TA>
+template <class TC>
 __host__ __device__ constexpr size_t group_rows_smem(int gmax, int bs) {
-  return (size_t)4 * gmax * sizeof(int4) + (size_t)2 * gmax * bs * sizeof(TA);
+  return (size_t)4 * gmax * sizeof(int4) + (size_t)2 * gmax * bs * sizeof(TC);
 }
 
-template <class TA, int VEC>
-struct VecOf;
-template <> struct VecOf<float, 4> { using type = float4; };
-template <> struct VecOf<double, 2> { using type = double2; };
-template <class TA> struct VecOf<TA, 1> { using type = TA; };
+template <int BYTES>
+struct RawLoad;
+template <> struct RawLoad<16> { using type = uint4; };
+template <> struct RawLoad<8> { using type = uint2; };
+template <> struct RawLoad<4> { using type = unsigned; };
+template <> struct RawLoad<2> { using type = unsigned short; };
 
-template <class V, class TA>
-__device__ inline TA vec_at(const V& v, int i) {
-  if constexpr (sizeof(V) == sizeof(TA)) return v;
-  else return reinterpret_cast<const TA*>(&v)[i];
+template <class TS>
+__device__ inline typename ComputeOf<TS>::type widen(TS v) {
+  if constexpr (std::is_same<TS, __nv_bfloat16>::value) return __bfloat162float(v);
+  else return v;
 }
 
 // one factor row, held in registers (all its loads issued before any use)
-template <int BS, class TA>
+template <int BS, class TS>
 struct FactorRow {
-  static constexpr int VEC = group_rows_vec<BS, TA>();
-  using V = typename VecOf<TA, VEC>::type;
+  using TC = typename ComputeOf<TS>::type;
+  static constexpr int LB = group_rows_load_bytes<BS, TS>();
+  static constexpr int VEC = LB / (int)sizeof(TS);  // factor values per load
+  using V = typename RawLoad<LB>::type;
   V v[BS / VEC];
-  __device__ inline void load(const TA* __restrict__ arow) {
+  __device__ inline void load(const TS* __restrict__ arow) {
 #pragma unroll
     for (int c = 0; c < BS / VEC; ++c) v[c] = __ldg(reinterpret_cast<const V*>(arow) + c);
   }
-  // acc += sign * row . x over the BS columns, in column order
+  // acc += sign * row . x over the BS columns, in column order (x in shared
+  // memory, arithmetic type)
   template <bool NEG>
-  __device__ inline TA dot(const TA* xs, TA acc) const {
+  __device__ inline TC dot(const TC* xs, TC acc) const {
 #pragma unroll
     for (int c = 0; c < BS / VEC; ++c) {
-      const V xv = reinterpret_cast<const V*>(xs)[c];
+      const TS* av = reinterpret_cast<const TS*>(&v[c]);
 #pragma unroll
-      for (int i = 0; i < VEC; ++i)
-        acc = fused_madd(NEG ? -vec_at<V, TA>(v[c], i) : vec_at<V, TA>(v[c], i), vec_at<V, TA>(xv, i), acc);
+      for (int i = 0; i < VEC; ++i) {
+        const TC aw = widen(av[i]);
+        acc = fused_madd(NEG ? -aw : aw, xs[c * VEC + i], acc);
+      }
     }
     return acc;
   }
 };
 
-template <int BS, class TA, int NT>
-__global__ void __launch_bounds__(NT) ilu_apply_group_rows_kernel(IluGroupArgs<TA> a) {
+template <int BS, class TS, int NT>
+__global__ void __launch_bounds__(NT) ilu_apply_group_rows_kernel(IluGroupArgs<TS> a) {
+  using TC = typename ComputeOf<TS>::type;
   constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ int slev[kGroupLevelsSmem + 1];
@@ -971,8 +994,8 @@ __global__ void __launch_bounds__(NT) ilu_apply_group_rows_kernel(IluGroupArgs<T
   }
   int4* sinfo = reinterpret_cast<int4*>(dsm);  // [fwd gmax | bwd gmax]
   int4* sloc = sinfo + 2 * gm;                 // [fwd gmax | bwd gmax]
-  TA* fs = reinterpret_cast<TA*>(sloc + 2 * gm);
-  TA* ys = fs + (size_t)gm * BS;
+  TC* fs = reinterpret_cast<TC*>(sloc + 2 * gm);
+  TC* ys = fs + (size_t)gm * BS;
   for (int i = threadIdx.x; i <= nlev; i += NT) slev[i] = a.plan.glev[l0 + i];
   for (int i = threadIdx.x; i < G; i += NT) {
     sinfo[i] = a.plan.task[pg0 + i];
@@ -994,17 +1017,17 @@ __global__ void __launch_bounds__(NT) ilu_apply_group_rows_kernel(IluGroupArgs<T
       const int ei = p / BS, r = p - ei * BS;
       const int4 inf = ti[p0 + ei], loc = tl[p0 + ei];
       const int nbk = (inf.z >= 0) + (inf.w >= 0);
-      const bool bad = !group_task_ok<BS, 1, TA>(a, inf) || loc.x < 0 || loc.x >= G || loc.y >= G ||
+      const bool bad = !group_task_ok<BS, 1, TS>(a, inf) || loc.x < 0 || loc.x >= G || loc.y >= G ||
                        loc.z >= G || (nbk > 0 && loc.y < 0) || (nbk > 1 && loc.z < 0);
       if (bad) {
         atomicExch(a.err, 2);
         continue;
       }
-      TA acc = TA(0);
-      const TA* xs = fwd ? fs : ys;
+      TC acc = TC(0);
+      const TC* xs = fwd ? fs : ys;
       // both off-diagonal rows in flight together (the second block's row
       // loads the diagonal inverse's row on a backward row with one block)
-      FactorRow<BS, TA> r0, r1;
+      FactorRow<BS, TS> r0, r1;
       if (nbk > 0) r0.load(a.LU + ((size_t)inf.y * BS + r) * BS);
       if (nbk > 1) r1.load(a.LU + ((size_t)(inf.y + 1) * BS + r) * BS);
       else if (!fwd) r1.load(a.Uinv + ((size_t)inf.x * BS + r) * BS);
@@ -1016,7 +1039,7 @@ __global__ void __launch_bounds__(NT) ilu_apply_group_rows_kernel(IluGroupArgs<T
       }
       if (fwd) {
         const double fd = xe + (double)acc;
-        fs[(size_t)loc.x * BS + r] = (TA)fd;
+        fs[(size_t)loc.x * BS + r] = (TC)fd;
       } else {
         acc = r1.template dot<false>(fs + (size_t)loc.x * BS, acc);
         a.y[(size_t)inf.x * BS + r] = (double)acc;

@@ -77,7 +77,7 @@ GroupKernel group_kernel_nt(int nt, bool staged, int gmax, int nlev_max) {
 // schedule 5: one lane per row, where the group's vectors fit
 template <int B, class TA>
 GroupKernel group_rows_kernel(int nt, int gmax, int nlev_max) {
-  const size_t sm = group_rows_smem<TA>(gmax, B);
+  const size_t sm = group_rows_smem<typename ComputeOf<TA>::type>(gmax, B);
   if (nlev_max > kGroupLevelsSmem || sm > smem_avail()) return {nullptr, 0};
   switch (nt) {
     case 128: return {(const void*)ilu_apply_group_rows_kernel<B, TA, 128>, sm};
@@ -126,6 +126,36 @@ cudaError_t ilu_apply_groups_t(const DeviceMesh& dm, const IluGroupShape& gs, co
 }
 
 }  // namespace
+
+cudaError_t la_ilu_apply_groups_bf16(const DeviceMesh& dm, const IluGroupShape& gs, const int* task,
+                                     const int* glev, const int* glev_ptr, int ctas, const __nv_bfloat16* LU,
+                                     const __nv_bfloat16* Uinv, const double* x, double* y, double* f, int* err,
+                                     cudaStream_t s) {
+  if (gs.ngroups <= 0 || !gs.loc) return cudaErrorInvalidValue;
+  const int bs = dm.nb * dm.neq;
+  const int nt = group_threads_for<float>(ctas);
+  GroupKernel k{nullptr, 0};
+#define ICX_ILUG16_CASE(B) \
+  if (bs == B) k = group_rows_kernel<B, __nv_bfloat16>(nt, gs.gmax, gs.nlev_max);
+  ICX_BLOCK_SIZES(ICX_ILUG16_CASE)
+#undef ICX_ILUG16_CASE
+  if (!k.kern) return cudaErrorNotSupported;  // the one-lane-per-row form does not fit
+  if (k.smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+    if (e != cudaSuccess) return e;
+  }
+  IluGroupArgs<__nv_bfloat16> args{dm.E, dm.nnzb, LU, Uinv, x, f, y, err,
+                                   IluGroupPlan{gs.ngroups, reinterpret_cast<const int4*>(task), glev, glev_ptr,
+                                                gs.gmax, reinterpret_cast<const int4*>(gs.loc)}};
+  void* params[] = {&args};
+  return cudaLaunchKernel(k.kern, dim3(gs.ngroups), dim3(nt), params, k.smem, s);
+}
+
+bool group_rows_bf16_fits(const DeviceMesh& dm, const IluGroupShape& gs) {
+  const int bs = dm.nb * dm.neq;
+  const size_t sm = group_rows_smem<float>(gs.gmax, bs);
+  return gs.loc && gs.nlev_max <= kGroupLevelsSmem && sm <= smem_avail();
+}
 
 cudaError_t la_ilu_apply_groups(const DeviceMesh& dm, const IluGroupShape& gs, const int* task, const int* glev,
                                 const int* glev_ptr, int rows, int ctas, const double* LU, const double* Uinv,

@@ -685,6 +685,16 @@ cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+__global__ void d2bf_kernel(long long n, const double* __restrict__ x, __nv_bfloat16* __restrict__ y) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = __double2bfloat16(x[i]);
+}
+
+cudaError_t la_d2bf(long long n, const double* x, __nv_bfloat16* y, cudaStream_t s) {
+  d2bf_kernel<<<grid_for(n), 256, 0, s>>>(n, x, y);
+  return cudaGetLastError();
+}
+
 __global__ void f2d_kernel(long long n, const float* __restrict__ x, double* __restrict__ y) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     y[i] = (double)x[i];

@@ -1,5 +1,6 @@
 // Device linear algebra used by the Newton solver (icx_linalg.cu).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -102,6 +103,16 @@ cudaError_t la_ilu_apply_groups_f32(const DeviceMesh& dm, const IluGroupShape& g
                                     const int* glev, const int* glev_ptr, int rows, int ctas, const float* LU,
                                     const float* Uinv, const double* x, double* y, double* f, int* err,
                                     cudaStream_t s);
+// the one-lane-per-row group apply (schedule 5) on BF16 factors (FP32
+// arithmetic); cudaErrorNotSupported where its shared memory does not fit
+// (group_rows_bf16_fits says beforehand)
+cudaError_t la_ilu_apply_groups_bf16(const DeviceMesh& dm, const IluGroupShape& gs, const int* task,
+                                     const int* glev, const int* glev_ptr, int ctas, const __nv_bfloat16* LU,
+                                     const __nv_bfloat16* Uinv, const double* x, double* y, double* f, int* err,
+                                     cudaStream_t s);
+bool group_rows_bf16_fits(const DeviceMesh& dm, const IluGroupShape& gs);
+// y = x rounded to BF16
+cudaError_t la_d2bf(long long n, const double* x, __nv_bfloat16* y, cudaStream_t s);
 cudaError_t la_block_diag_apply_f32(int E, int bs, const float* D, const double* x, double* y, cudaStream_t s);
 cudaError_t la_d2f(long long n, const double* x, float* y, cudaStream_t s);
 cudaError_t la_f2d(long long n, const float* x, double* y, cudaStream_t s);

@@ -73,6 +73,11 @@ struct icx_solver_work {
   float* vals32 = nullptr;  // mixed precision: FP32 copies of the Jacobian and the preconditioner
   float* pc32 = nullptr;
   float* uinv32 = nullptr;
+  // BF16 copies of the ILU factors (Newton precision 3: the tiled apply's
+  // one-lane-per-row form reads them, widening to FP32)
+  bool bf16 = false;
+  __nv_bfloat16* pc16 = nullptr;
+  __nv_bfloat16* uinv16 = nullptr;
   float* V32 = nullptr;     // mixed precision: the Krylov basis in FP32, (m + 1) x n
   double* vt = nullptr;     // the basis vector widened for the operators
   int* order = nullptr;     // elements by ascending level (ILU schedule)
@@ -364,6 +369,15 @@ icx_status ensure_mixed(icx_ctx* c) {
   return ICX_OK;
 }
 
+icx_status ensure_bf16(icx_ctx* c) {
+  icx_solver_work* w = c->sw;
+  if (w->pc16) return ICX_OK;
+  size_t nv = (size_t)w->nnzb * w->bs * w->bs;
+  CK(cudaMalloc((void**)&w->pc16, sizeof(__nv_bfloat16) * nv));
+  CK(cudaMalloc((void**)&w->uinv16, sizeof(__nv_bfloat16) * (size_t)c->dm.E * w->bs * w->bs));
+  return ICX_OK;
+}
+
 cudaError_t diag_apply(icx_ctx* c, bool mixed, const double* D, const float* D32, const double* x, double* z,
                        cudaStream_t s) {
   return mixed ? icx::la_block_diag_apply_f32(c->dm.E, c->sw->bs, D32, x, z, s)
@@ -394,6 +408,10 @@ cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStr
     const IluTilePlan& tp = w->tp;
     const icx::IluGroupShape gs{tp.ngroups, tp.gmax, tp.nlev_max, gsched, tp.gloc};
     const int ctas = dm.tile.flow_ctas[pi];
+    // BF16 factors: the one-lane-per-row form where it fits, else the FP32 copies
+    if (mixed && w->bf16 && w->pc16 && icx::group_rows_bf16_fits(dm, gs))
+      return icx::la_ilu_apply_groups_bf16(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, ctas, w->pc16, w->uinv16, x, z,
+                                           w->pct, w->pc_err, s);
     return mixed ? icx::la_ilu_apply_groups_f32(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, ctas, w->pc32,
                                                 w->uinv32, x, z, w->pct, w->pc_err, s)
                  : icx::la_ilu_apply_groups(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, ctas, w->pc, w->uinv,
@@ -504,6 +522,10 @@ cudaError_t build_pc_impl(icx_ctx* c, int kind, bool mixed, cudaStream_t s) {
   if (e == cudaSuccess && jac) e = icx::la_d2f(nd, w->pc, w->pc32, s);
   if (e == cudaSuccess && ilu) e = icx::la_d2f(nv_pc, w->pc, w->pc32, s);
   if (e == cudaSuccess && ilu) e = icx::la_d2f(nd, w->uinv, w->uinv32, s);
+  if (e == cudaSuccess && ilu && w->bf16 && w->pc16) {
+    e = icx::la_d2bf(nv_pc, w->pc, w->pc16, s);
+    if (e == cudaSuccess) e = icx::la_d2bf(nd, w->uinv, w->uinv16, s);
+  }
   return e;
 }
 
@@ -577,7 +599,8 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
                         (long long)t.flow_ctas[pi], (long long)t.flow_sched[pi], (long long)(uintptr_t)dm.bsr_rowptr,
                         (long long)(uintptr_t)dm.bsr_colidx, (long long)(uintptr_t)dm.bsr_diag,
                         (long long)(uintptr_t)w->order, (long long)w->tp.tile, (long long)(uintptr_t)w->tp.order,
-                        (long long)w->fd_on, (long long)(uintptr_t)w->fd_u, (long long)(uintptr_t)w->fd_r})
+                        (long long)w->fd_on, (long long)(uintptr_t)w->fd_u, (long long)(uintptr_t)w->fd_r,
+                        (long long)w->bf16})
       key = (key ^ (unsigned long long)v) * 1099511628211ull;
     kb.graphs = &w->graphs;
     kb.graph_key = key | 1;
@@ -677,7 +700,7 @@ namespace icx {
 void free_solver_work(icx_ctx* c) {
   if (!c || !c->sw) return;
   icx_solver_work* w = c->sw;
-  void* ptrs[] = {w->V32, w->vt, w->vals32, w->pc32, w->uinv32, w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du,
+  void* ptrs[] = {w->pc16, w->uinv16, w->V32, w->vt, w->vals32, w->pc32, w->uinv32, w->vals, w->pc, w->uinv, w->V, w->w, w->z, w->r, w->res, w->du,
                   w->ustep, w->rwork, w->pct, w->pct2, w->pct3, w->pct4, w->order, w->cnt, w->cnt_rows, w->pc_err,
                   w->dh, w->flag, w->lw.partial};
   w->graphs.release();
@@ -814,14 +837,20 @@ icx_status icx_ilu_apply(icx_ctx* c, const double* d_vals, const double* d_x, do
                          int schedule, int repeat, double* ms_per_apply) {
   if (!c || !c->ready) return set_err(c, ICX_ERR_INVALID, "icx_setup has not completed");
   if (!d_vals || !d_x || !d_y || d_x == d_y) return set_err(c, ICX_ERR_INVALID, "null or aliased device pointer");
-  if (precision < 0 || precision > 1 || schedule < 0 || schedule > 2 || repeat < 1)
-    return set_err(c, ICX_ERR_INVALID, "precision 0..1, schedule 0..2, repeat >= 1");
+  if (precision < 0 || precision > 2 || schedule < 0 || schedule > 2 || repeat < 1)
+    return set_err(c, ICX_ERR_INVALID, "precision 0..2, schedule 0..2, repeat >= 1");
   cudaStream_t s = 0;
   icx_status st = ensure_work(c, 30);
   if (st != ICX_OK) return st;
-  const bool mixed = precision == 1;
+  const bool mixed = precision >= 1;
   if (mixed && (st = ensure_mixed(c)) != ICX_OK) return st;
+  if (precision == 2 && (st = ensure_bf16(c)) != ICX_OK) return st;
   icx_solver_work* w = c->sw;
+  struct Bf16Scope {
+    icx_solver_work* w;
+    ~Bf16Scope() { w->bf16 = false; }
+  } bf16_scope{w};
+  w->bf16 = precision == 2;
   if (schedule == 2 && !w->rows_ok)
     return set_err(c, ICX_ERR_UNSUPPORTED, "row-pipelined apply needs one structured grid with the 5-point pattern");
   CK(cudaMemcpyAsync(w->vals, d_vals, sizeof(double) * (size_t)c->dm.nnzb * w->bs * w->bs, cudaMemcpyDeviceToDevice,
@@ -892,7 +921,7 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   if (!d_u || !opt) return set_err(c, ICX_ERR_INVALID, "null argument");
   if (opt->gmres_restart < 1 || opt->gmres_restart > 60) return set_err(c, ICX_ERR_INVALID, "restart in 1..60");
   cudaStream_t s = 0;
-  if (opt->precision < 0 || opt->precision > 2) return set_err(c, ICX_ERR_INVALID, "precision must be 0, 1 or 2");
+  if (opt->precision < 0 || opt->precision > 3) return set_err(c, ICX_ERR_INVALID, "precision must be 0 to 3");
   if (opt->preconditioner < 0 || opt->preconditioner > 5) return set_err(c, ICX_ERR_INVALID, "preconditioner in 0..5");
   if (opt->preconditioner >= 4 && (opt->pc_sweeps < 0 || opt->pc_sweeps > 16))
     return set_err(c, ICX_ERR_INVALID, "pc_sweeps in 0..16");
@@ -908,7 +937,14 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   const bool mixed = opt->precision >= 1;
   const bool quad32 = opt->precision == 2;
   if (mixed && (st = ensure_mixed(c)) != ICX_OK) return st;
+  if (opt->precision == 3 && (st = ensure_bf16(c)) != ICX_OK) return st;
   icx_solver_work* w = c->sw;
+  // precision 3: BF16 copies of the ILU factors for this solve
+  struct Bf16Scope {
+    icx_solver_work* w;
+    ~Bf16Scope() { w->bf16 = false; }
+  } bf16_scope{w};
+  w->bf16 = opt->precision == 3;
   long long n = w->n;
   icx_newton_report local{};
   icx_newton_report* R = rep ? rep : &local;

@@ -307,7 +307,13 @@ typedef struct icx_newton_options {
    * 2: as 1, with the Jacobian's flux quadrature itself in FP32
    * (icx_form_jacobian_fd_f32); the preconditioner is factored in FP64 from
    * those FP32 values. Newton is then FP64 iterative refinement around FP32
-   * linearisations: its residual, norm, line search and update stay FP64. */
+   * linearisations: its residual, norm, line search and update stay FP64.
+   * 3: as 1, with the block-ILU(0) factors of a tiled or grouped
+   * preconditioner (ilu_tile, icx_set_ilu_groups) stored in BF16 and widened
+   * to FP32 in the apply (the one-lane-per-row form, ilu_sched 5; where its
+   * shared memory does not fit, and on whole-grid factors, the FP32 copies
+   * of 1). The preconditioner only changes GMRES iterations: the converged
+   * state is judged in FP64 as in 1. */
   int precision;
   /* preconditioner 4 (block-ILU(0) factors applied by Jacobi sweeps): the
    * sweeps per triangular solve */
@@ -360,7 +366,9 @@ icx_status icx_gmres_solve(icx_ctx* ctx, const double* d_vals, const double* d_b
 
 /* y = M^-1 x for the block-ILU(0) preconditioner of the BSR matrix d_vals
  * (the factors icx_gmres_solve / icx_newton_solve build; precision 1: from
- * FP32 copies with FP32 accumulation). schedule 0 or 1: the data-flow apply
+ * FP32 copies with FP32 accumulation; 2: tiled or grouped factors from BF16
+ * copies in the one-lane-per-row apply with FP32 arithmetic, as Newton
+ * precision 3, the FP32 copies where it does not fit). schedule 0 or 1: the data-flow apply
  * the solvers use; 2: the row-pipelined apply, one CTA per grid row
  * (ICX_ERR_UNSUPPORTED when the context is not one grid with the 5-point
  * element pattern; it is slower than the data-flow apply on the measured

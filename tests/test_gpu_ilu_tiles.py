@@ -228,3 +228,34 @@ def test_strip_krylov_on_one_rank_matches_gmres():
     assert rel <= 1e-12
     assert float((x - x2).norm() / x2.norm()) <= 1e-9
     ctx.close()
+
+
+@pytest.mark.parametrize("kw,tile", [(dict(pde=NS, nx=13, ny=11, p=2, ip=True), 4),
+                                     (dict(pde=BURGERS, nx=12, ny=7, p=3, ip=True), 5)])
+def test_bf16_factors_apply(kw, tile):
+    """precision 2 of icx_ilu_apply: the tiled factors rounded to BF16, widened
+    to FP32 in the one-lane-per-row apply. Against the FP64 apply of the same
+    factors the result differs by the factors' rounding (2^-9 relative per
+    value): within 5e-2 of the result's largest entry, and identical across
+    CTA sizes"""
+    spec = Spec(**kw)
+    ctx = spec.context()
+    vals, _, _, _ = _jacobian(ctx, spec)
+    ctx.ilu_tile = tile
+    x = torch.from_numpy(np.random.default_rng(12).standard_normal(ctx.layout.n_dof)).cuda()
+    y64 = torch.empty_like(x)
+    ctx.ilu_apply(vals, x, y64, 0, 1)
+    ys = []
+    for k in (0, 1, 2, 3):
+        ctx.tile = {"ilu_sched": [5, 5], "ilu_ctas": [k, k]}
+        y = torch.full_like(x, float("nan"))
+        ctx.ilu_apply(vals, x, y, 2, 1, repeat=2)
+        ys.append(y)
+    ctx.tile = {}
+    torch.cuda.synchronize()
+    assert torch.isfinite(ys[0]).all()
+    for y in ys[1:]:
+        assert torch.equal(ys[0].view(torch.int64), y.view(torch.int64))
+    err = float((ys[0] - y64).abs().max()) / float(y64.abs().max())
+    assert err <= 5e-2, err
+    ctx.close()

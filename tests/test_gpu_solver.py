@@ -336,3 +336,23 @@ def test_newton_matrix_free_operator_reaches_the_assembled_state(precision, tile
     assert np.linalg.norm(um - ua) <= 1e-10 * np.linalg.norm(ua)
     assert abs(itm - ita) <= 0.5 * ita + 2, (itm, ita)
     assert gm > 0
+
+
+def test_newton_bf16_factors_reach_the_fp64_state():
+    """precision 3: tiled block-ILU(0) factors in BF16 (FP32 arithmetic), the
+    rest as precision 1; with the matrix-free operator and without, Newton
+    converges to the FP64 solve's state within 1e-10 (L2, relative)"""
+    spec = Spec(pde=NS, nx=6, ny=5, p=2, g=2, ip=True, source=True, perturb=0.05)
+    ctx = spec.context()
+    u0 = _ns_mms_state(ctx, 1e-2, 23)
+    du = torch.from_numpy(u0.copy()).cuda()
+    r0 = ctx.newton_solve(du, _newton_opts(tau_abs=1e-11, kmax=20, linesearch=1, gmres_rtol=1e-6, gmres_max_it=5000))
+    assert r0.converged
+    ua = du.cpu().numpy()
+    for mf in (0, 1):
+        du = torch.from_numpy(u0.copy()).cuda()
+        rep = ctx.newton_solve(du, _newton_opts(tau_abs=1e-11, kmax=20, linesearch=1, gmres_rtol=1e-6,
+                                                gmres_max_it=5000, precision=3, ilu_tile=3, matrix_free=mf))
+        assert rep.converged and rep.r_final <= 1e-11, (mf, list(rep.residual_history[:rep.iterations + 1]))
+        assert np.linalg.norm(du.cpu().numpy() - ua) <= 1e-10 * np.linalg.norm(ua)
+        assert rep.graph_steps > 0
