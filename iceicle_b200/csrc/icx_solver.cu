@@ -408,10 +408,15 @@ cudaError_t ilu_flow(icx_ctx* c, bool mixed, const double* x, double* z, cudaStr
     const IluTilePlan& tp = w->tp;
     const icx::IluGroupShape gs{tp.ngroups, tp.gmax, tp.nlev_max, gsched, tp.gloc};
     const int ctas = dm.tile.flow_ctas[pi];
-    // BF16 factors: the one-lane-per-row form where it fits, else the FP32 copies
-    if (mixed && w->bf16 && w->pc16 && icx::group_rows_bf16_fits(dm, gs))
-      return icx::la_ilu_apply_groups_bf16(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, ctas, w->pc16, w->uinv16, x, z,
-                                           w->pct, w->pc_err, s);
+    // BF16 factors: the one-lane-per-row form where it fits, else the FP32
+    // copies. Its CTA size follows the group size (measured at 256 x 256,
+    // p = 2: 8 x 8 tiles 0.159 ms with 128 threads against 0.191 with 256;
+    // 16 x 16 tiles 0.240 ms with 256 against 0.322 with 128)
+    if (mixed && w->bf16 && w->pc16 && icx::group_rows_bf16_fits(dm, gs)) {
+      const int ctas16 = tp.gmax <= 64 ? 3 : tp.gmax <= 256 ? 2 : 1;
+      return icx::la_ilu_apply_groups_bf16(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, ctas16, w->pc16, w->uinv16, x,
+                                           z, w->pct, w->pc_err, s);
+    }
     return mixed ? icx::la_ilu_apply_groups_f32(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, ctas, w->pc32,
                                                 w->uinv32, x, z, w->pct, w->pc_err, s)
                  : icx::la_ilu_apply_groups(dm, gs, tp.gtask, tp.glev, tp.glev_ptr, rows, ctas, w->pc, w->uinv,

@@ -226,7 +226,7 @@ def new_model(device=0, seed=0, hidden=256):
 # scaled on a held-out instance: by the training loss (calibrate), then by the
 # GMRES iterations of its Newton solve (select_scale)
 RECIPE = dict(model_seed=1, train_instances=(8, 11), pairs=2000, samples=167, every=5, steps=120, batch=4, random=2,
-              sweeps=0, ilu_tile=16, lr=1e-3, holdout=(1, 5))
+              sweeps=0, ilu_tile=8, lr=1e-3, holdout=(1, 5))
 EVAL_INSTANCES = (3, 99)
 
 
