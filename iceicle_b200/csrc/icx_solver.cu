@@ -950,6 +950,12 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
     ~Bf16Scope() { w->bf16 = false; }
   } bf16_scope{w};
   w->bf16 = opt->precision == 3;
+  // a learned model whose output layer is zero is its base preconditioner,
+  // so the solve is the base's: block-ILU(0) (sweeps = 0) or its Jacobi-sweep
+  // form, without the stall test and fallback kept for a correction that
+  // may not converge
+  const int pc_kind = opt->preconditioner == 5 && icx::lpc_zero_correction(c) ? (opt->pc_sweeps > 0 ? 4 : 2)
+                                                                             : opt->preconditioner;
   long long n = w->n;
   icx_newton_report local{};
   icx_newton_report* R = rep ? rep : &local;
@@ -977,7 +983,7 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   int k = 0;
   bool converged = rk <= tau;
   for (; k < opt->kmax && !converged; ++k) {
-    CK(build_pc(c, opt->preconditioner, mixed, s));
+    CK(build_pc(c, pc_kind, mixed, s));
     {
       int fl = 0;
       CK(cudaMemcpyAsync(&fl, w->flag, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1000,12 +1006,12 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
     }
     int it = 0;
     double rr = 0.0;
-    st = gmres(c, opt->preconditioner, mixed, opt->gmres_restart, opt->gmres_max_it, opt->gmres_rtol, w->res, w->du,
+    st = gmres(c, pc_kind, mixed, opt->gmres_restart, opt->gmres_max_it, opt->gmres_rtol, w->res, w->du,
                &it, &rr, s);
     if (st != ICX_OK) return st;
     R->linear_iterations_total += it;
     if (k < 64) R->linear_iterations[k] = it;
-    if (opt->preconditioner >= 3 && !(rr <= opt->gmres_rtol)) {
+    if (pc_kind >= 3 && !(rr <= opt->gmres_rtol)) {
       // the parallel / learned preconditioner missed the linear tolerance:
       // this step is solved again with block-ILU(0)
       ++R->pc_fallbacks;

@@ -295,7 +295,8 @@ typedef struct icx_newton_options {
                               G (2 I - J G), 4 block-ILU0 factors with Jacobi-sweep triangular solves,
                               5 learned: (I + C) times preconditioner 4, or times 2 when pc_sweeps = 0
                               (icx_lpc_attach); a step whose linear solve misses gmres_rtol with 3-5
-                              is solved again with 2 */
+                              is solved again with 2. A model whose output layer is all zero (C = 0)
+                              makes 5 its base exactly: the solve is then 2 (or 4), fallback rule included */
   int verbosity;
   /* 0: all FP64. 1: mixed - the linear solves read FP32 copies of the
    * Jacobian (SpMV) and of the preconditioner (block inverses / ILU factors,
