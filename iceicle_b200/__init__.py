@@ -56,7 +56,7 @@ class NewtonOptions(C.Structure):
                 ("ls_c2", C.c_double), ("gmres_restart", C.c_int), ("gmres_max_it", C.c_int),
                 ("gmres_rtol", C.c_double), ("preconditioner", C.c_int), ("verbosity", C.c_int),
                 ("precision", C.c_int), ("pc_sweeps", C.c_int), ("cuda_graphs", C.c_int), ("ilu_tile", C.c_int),
-                ("matrix_free", C.c_int)]
+                ("matrix_free", C.c_int), ("gmres_cgs_refine", C.c_int)]
 
 
 class ExplicitOptions(C.Structure):

@@ -884,13 +884,15 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
         else GCK(cudaMemcpyAsync(dst, vj, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
       }
       // the step: preconditioner and operator, classical Gram-Schmidt twice
-      // and the norm of the result; the three reductions land in separate
-      // device slots [pass 1 | pass 2 | |v|^2] and come back in one copy
+      // (once with cgs_passes = 1) and the norm of the result; the
+      // reductions land in separate device slots [pass 1 | pass 2 | |v|^2]
+      // and come back in one copy
       auto step = [&](cudaStream_t st, double* host_dst) -> cudaError_t {
         cudaError_t e = f32 ? la_f2d(n, vj32, vj, st) : cudaSuccess;
         if (e == cudaSuccess && M) e = (*M)(vj, kb.z, st);
         if (e == cudaSuccess) e = A(M ? kb.z : vj, vj1, st);
-        for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
+        const int passes = kb.cgs_passes == 1 ? 1 : 2;
+        for (int pass = 0; pass < passes && e == cudaSuccess; ++pass) {
           double* slot = kb.dh + (size_t)pass * (m + 2);
           e = f32 ? la_mdot32(*kb.lw, n, kb.V32, n, j + 1, vj1, slot, st)
                   : la_mdot(*kb.lw, n, kb.V, n, j + 1, vj1, slot, st);
@@ -933,7 +935,7 @@ icx_status gmres_op(KrylovBuffers& kb, const LinOp& A, const LinOp* M, int maxit
         GCK(cudaStreamSynchronize(s));
       }
       std::fill(hcol.begin(), hcol.end(), 0.0);
-      for (int i = 0; i <= j; ++i) hcol[i] += hp3[i] + hp3[(m + 2) + i];
+      for (int i = 0; i <= j; ++i) hcol[i] += hp3[i] + (kb.cgs_passes == 1 ? 0.0 : hp3[(m + 2) + i]);
       double hn = std::sqrt(hp3[2 * (m + 2)]);
       hcol[j + 1] = hn;
       if (!std::isfinite(hn)) {

@@ -166,6 +166,9 @@ struct KrylovBuffers {
   // stall test (0: off): stop when the residual after a restart cycle is above
   // 0.9 of the residual `stall_cycles` cycles earlier
   int stall_cycles = 0;
+  // classical Gram-Schmidt passes per Arnoldi step: 2 (a second pass every
+  // step) or 1 (PETSc's default GMRES orthogonalisation, refinement never)
+  int cgs_passes = 2;
   // optional: replay the Arnoldi steps as CUDA graphs (graph_key != 0; the
   // operators then launch only on the stream they are given, with arguments
   // that do not change between calls). Not used while sampling.

@@ -143,14 +143,14 @@ __global__ void seg_axpy_kernel(const long long* __restrict__ cbeg, const long l
   for (long long k = cbeg[c] + threadIdx.x; k < cend[c]; k += blockDim.x) y[k] = s * x[k] + 1.0 * y[k];
 }
 
-// the Hessenberg column of step j per part: both Gram-Schmidt passes summed,
-// then |v_j+1|^2 (the host takes the root)
+// the Hessenberg column of step j per part: both Gram-Schmidt passes summed
+// (d1 null: one pass), then |v_j+1|^2 (the host takes the root)
 __global__ void seg_hcol_kernel(int n_parts, int j, const double* __restrict__ d0, const double* __restrict__ d1,
                                 const double* __restrict__ d2, int ld, double* __restrict__ hcol) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_parts * (j + 2)) return;
   const int p = t / (j + 2), i = t - p * (j + 2);
-  hcol[(size_t)p * ld + i] = i <= j ? d0[(size_t)p * ld + i] + d1[(size_t)p * ld + i] : d2[(size_t)p * ld];
+  hcol[(size_t)p * ld + i] = i <= j ? d0[(size_t)p * ld + i] + (d1 ? d1[(size_t)p * ld + i] : 0.0) : d2[(size_t)p * ld];
 }
 
 struct NeedEval {
@@ -289,7 +289,7 @@ struct Kry {
 // right-preconditioned GMRES(m) of each part, all parts in the same launches
 icx_status pset_gmres(icx_pset* S, int pc, bool mixed, int m, int maxit, double rtol, const double* b, double* x,
                       const std::vector<char>& want, std::vector<int>& iters, std::vector<double>& relres,
-                      icx_pset_stats& st, cudaStream_t s) {
+                      icx_pset_stats& st, cudaStream_t s, int passes = 2) {
   const int P = S->n_parts, ld = m + 2;
   const long long N = S->N;
   PCK(cudaMemsetAsync(x, 0, sizeof(double) * N, s));
@@ -318,6 +318,7 @@ icx_status pset_gmres(icx_pset* S, int pc, bool mixed, int m, int maxit, double 
     key = (key ^ icx::solver_graph_key(g, pc, mixed)) * 1099511628211ull;
   }
   key = (key ^ (unsigned long long)m) * 1099511628211ull;
+  key = (key ^ (unsigned long long)passes) * 1099511628211ull;
   if (key != S->key) {
     release_graphs(S);
     S->key = key;
@@ -353,7 +354,7 @@ icx_status pset_gmres(icx_pset* S, int pc, bool mixed, int m, int maxit, double 
           if (ee == cudaSuccess) ee = icx::solver_operator(g, mixed, (pc ? S->z : vj) + off, vj1 + off, q);
           return ee;
         });
-        for (int pass = 0; pass < 2 && e == cudaSuccess; ++pass) {
+        for (int pass = 0; pass < passes && e == cudaSuccess; ++pass) {
           double* slot = S->dots + (size_t)pass * P * ld;
           e = seg_dots(S, S->V, N, j + 1, vj1, slot, ld, q);
           if (e == cudaSuccess) {
@@ -365,8 +366,8 @@ icx_status pset_gmres(icx_pset* S, int pc, bool mixed, int m, int maxit, double 
         double* nrm = S->dots + (size_t)2 * P * ld;
         if (e == cudaSuccess) e = seg_dots(S, vj1, 0, 1, vj1, nrm, ld, q);
         if (e == cudaSuccess) {
-          seg_hcol_kernel<<<(P * (j + 2) + 255) / 256, 256, 0, q>>>(P, j, S->dots, S->dots + (size_t)P * ld, nrm, ld,
-                                                                   S->hcol);
+          seg_hcol_kernel<<<(P * (j + 2) + 255) / 256, 256, 0, q>>>(
+              P, j, S->dots, passes == 2 ? S->dots + (size_t)P * ld : nullptr, nrm, ld, S->hcol);
           seg_normalize_kernel<<<S->n_chunks, kThreads, 0, q>>>(S->d_cbeg, S->d_cend, S->d_cpart, nrm, ld, vj1);
           e = cudaGetLastError();
         }
@@ -655,7 +656,8 @@ icx_status icx_pset_newton_solve(icx_pset* S, double* d_u, const icx_newton_opti
       PCK(cudaStreamSynchronize(s));
       if (fl == 2) return perr(S, ICX_ERR_CUDA, "block-ILU factorization: block index out of range");
     }
-    st = pset_gmres(S, pc, mixed, m, opt->gmres_max_it, opt->gmres_rtol, S->res, S->du, active, its, rel, stt, s);
+    st = pset_gmres(S, pc, mixed, m, opt->gmres_max_it, opt->gmres_rtol, S->res, S->du, active, its, rel, stt, s,
+                    opt->gmres_cgs_refine ? 2 : 1);
     if (st != ICX_OK) return st;
     for (int p = 0; p < P; ++p) {
       if (!active[p]) continue;

@@ -101,6 +101,7 @@ struct icx_solver_work {
   double* dh = nullptr;     // device scalars (dot results)
   // the matrix-free operator (icx_newton_options.matrix_free) while a Newton
   // step's linear solve runs: state, its residual, {|v|^2, c} (in dh)
+  int cgs_passes = 2;       // Gram-Schmidt passes of the GMRES run by a Newton step
   bool fd_on = false;
   const double* fd_u = nullptr;
   const double* fd_r = nullptr;
@@ -572,6 +573,7 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
   // (block-ILU(0) then takes the step): under 10 % residual reduction over
   // 20 restart cycles
   kb.stall_cycles = pc >= 3 ? 20 : 0;
+  kb.cgs_passes = w->cgs_passes;
   struct CountOut {
     int* dst;
     icx::KrylovBuffers* kb;
@@ -605,7 +607,7 @@ icx_status gmres(icx_ctx* c, int pc, bool mixed, int m, int maxit, double rtol, 
                         (long long)(uintptr_t)dm.bsr_colidx, (long long)(uintptr_t)dm.bsr_diag,
                         (long long)(uintptr_t)w->order, (long long)w->tp.tile, (long long)(uintptr_t)w->tp.order,
                         (long long)w->fd_on, (long long)(uintptr_t)w->fd_u, (long long)(uintptr_t)w->fd_r,
-                        (long long)w->bf16})
+                        (long long)w->bf16, (long long)w->cgs_passes})
       key = (key ^ (unsigned long long)v) * 1099511628211ull;
     kb.graphs = &w->graphs;
     kb.graph_key = key | 1;
@@ -768,6 +770,7 @@ icx_status icx_newton_default_options(icx_newton_options* o) {
   o->cuda_graphs = 1;
   o->ilu_tile = 0;           // block-ILU(0) over the whole grid in natural order
   o->matrix_free = 0;        // the assembled Jacobian's BSR product
+  o->gmres_cgs_refine = 1;   // classical Gram-Schmidt with a second pass every step
   return ICX_OK;
 }
 
@@ -947,9 +950,13 @@ icx_status icx_newton_solve(icx_ctx* c, double* d_u, const icx_newton_options* o
   // precision 3: BF16 copies of the ILU factors for this solve
   struct Bf16Scope {
     icx_solver_work* w;
-    ~Bf16Scope() { w->bf16 = false; }
+    ~Bf16Scope() {
+      w->bf16 = false;
+      w->cgs_passes = 2;
+    }
   } bf16_scope{w};
   w->bf16 = opt->precision == 3;
+  w->cgs_passes = opt->gmres_cgs_refine ? 2 : 1;
   // a learned model whose output layer is zero is its base preconditioner,
   // so the solve is the base's: block-ILU(0) (sweeps = 0) or its Jacobi-sweep
   // form, without the stall test and fallback kept for a correction that

@@ -342,6 +342,12 @@ typedef struct icx_newton_options {
    * the BSR product, in every precision mode. 0 (default): the assembled
    * Jacobian's BSR product. */
   int matrix_free;
+  /* GMRES orthogonalisation: 1 (default) classical Gram-Schmidt with a
+   * second pass every Arnoldi step; 0 one pass, which is PETSc's default
+   * (KSPGMRES with refinement "never", what the reference's
+   * KSPSetFromOptions, petsc_newton.hpp:175-182, gets without options) and
+   * reads the Krylov basis half as often */
+  int gmres_cgs_refine;
 } icx_newton_options;
 
 typedef struct icx_newton_report {

@@ -11,7 +11,8 @@ equals the same part solved alone (icx_newton_solve).
   own solve's (relative to the larger L2 norm of that state and the initial
   state: the Burgers parts' steady state is u = 0);
 * the same set in mixed precision reaches the FP64 states within 1e-10;
-* the Arnoldi steps of the set are replayed from CUDA graphs.
+* the Arnoldi steps of the set are replayed from CUDA graphs;
+* the same with one Gram-Schmidt pass per step (gmres_cgs_refine = 0).
 """
 import numpy as np
 import pytest
@@ -60,19 +61,21 @@ def test_set_residual_is_each_parts_residual(problem_set):
         assert np.abs(ps.part(r, k) - ref).max() <= 1e-14 * max(np.abs(ref).max(), 1e-300), k
 
 
-def _newton(ps, parts, u0, precision):
+def _newton(ps, parts, u0, precision, refine=1):
     import iceicle_b200 as ib
     o = ib.default_newton_options()
     o.precision = precision
+    o.gmres_cgs_refine = refine
     u = torch.from_numpy(ps.gather(u0)).cuda()
     reps, stats = ps.newton_solve(u, o)
     return u.cpu().numpy(), reps, stats, o
 
 
-def test_set_newton_equals_solving_each_part_alone(problem_set):
+@pytest.mark.parametrize("refine", [1, 0], ids=["cgs2", "cgs1"])
+def test_set_newton_equals_solving_each_part_alone(problem_set, refine):
     import iceicle_b200 as ib
     ps, parts, u0 = problem_set
-    u, reps, stats, o = _newton(ps, parts, u0, 0)
+    u, reps, stats, o = _newton(ps, parts, u0, 0, refine)
     assert stats.orders >= 4
     assert stats.graph_launches > 0
     for k, c in enumerate(parts):

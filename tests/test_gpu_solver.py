@@ -356,3 +356,31 @@ def test_newton_bf16_factors_reach_the_fp64_state():
         assert rep.converged and rep.r_final <= 1e-11, (mf, list(rep.residual_history[:rep.iterations + 1]))
         assert np.linalg.norm(du.cpu().numpy() - ua) <= 1e-10 * np.linalg.norm(ua)
         assert rep.graph_steps > 0
+
+
+@pytest.mark.parametrize("precision,tile,mf", [(0, 0, 0), (1, 0, 0), (3, 3, 1)], ids=["fp64", "mixed", "bf16_mf"])
+def test_newton_single_gram_schmidt_pass_reaches_the_same_state(precision, tile, mf):
+    """gmres_cgs_refine = 0: one classical Gram-Schmidt pass per Arnoldi step
+    (PETSc's default GMRES orthogonalisation). Newton converges to the state
+    of the two-pass FP64 solve within 1e-10 (L2, relative), and its graph
+    replay is bit-identical to eager steps."""
+    spec = Spec(pde=NS, nx=6, ny=5, p=2, g=2, ip=True, source=True, perturb=0.05)
+    ctx = spec.context()
+    u0 = _ns_mms_state(ctx, 1e-2, 23)
+    du = torch.from_numpy(u0.copy()).cuda()
+    r0 = ctx.newton_solve(du, _newton_opts(tau_abs=1e-11, kmax=20, linesearch=1, gmres_rtol=1e-6, gmres_max_it=5000))
+    assert r0.converged
+    ua = du.cpu().numpy()
+    out = {}
+    for graphs in (0, 1):
+        du = torch.from_numpy(u0.copy()).cuda()
+        rep = ctx.newton_solve(du, _newton_opts(tau_abs=1e-11, kmax=20, linesearch=1, gmres_rtol=1e-6,
+                                                gmres_max_it=5000, precision=precision, ilu_tile=tile,
+                                                matrix_free=mf, gmres_cgs_refine=0, cuda_graphs=graphs))
+        assert rep.converged and rep.r_final <= 1e-11
+        u = du.cpu().numpy()
+        assert np.linalg.norm(u - ua) <= 1e-10 * np.linalg.norm(ua)
+        out[graphs] = (u, list(rep.linear_iterations[:rep.iterations]), rep.graph_steps)
+    assert out[1][2] > 0 and out[0][2] == 0
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0].view(np.uint64), out[1][0].view(np.uint64))
