@@ -456,7 +456,8 @@ def lm_bench(torch, dev, kmax=1, maxit=300, orders=(1,)):
 
 
 def newton_bench(torch, dev, tune=True):
-    """Newton solve time to |r| <= 1e-10 (FP64 residual), all-FP64 vs mixed
+    """Newton solve time to |r| <= 1e-10 (FP64 residual; GMRES with PETSc's
+    default orthogonalisation, one classical Gram-Schmidt pass), all-FP64 vs mixed
     precision (FP32 Jacobian and preconditioner copies) and FP32 flux
     quadrature (the Jacobian itself formed in FP32): 32 x 32 viscous
     Burgers p=2 and the 128 x 128 Navier-Stokes manufactured solution p=3,
@@ -491,6 +492,7 @@ def newton_bench(torch, dev, tune=True):
             opt.precision = prec
             opt.ilu_tile = t
             opt.matrix_free = mf
+            opt.gmres_cgs_refine = 0  # PETSc's default GMRES orthogonalisation (one Gram-Schmidt pass)
             u = torch.from_numpy(wl.u0).to(dev)
             if name.startswith("burgers"):
                 wl.ctx.newton_solve(torch.from_numpy(wl.u0).to(dev), opt)  # warm-up (one-time setup)
@@ -637,8 +639,10 @@ def factor_bench():
 
 
 def learned_bench(torch, dev, tune=True, n_seeds=3):
-    """Newton solve time to |r| <= 1e-10 on fresh seeded instances of the
-    256 x 256 p = 2 Navier-Stokes manufactured solution (Re drawn from
+    """Newton solve time to |r| <= 1e-10 (every row with PETSc's default
+    GMRES orthogonalisation, as the reference's KSPSetFromOptions gets it) on
+    fresh seeded instances of the 256 x 256 p = 2 Navier-Stokes manufactured
+    solution (Re drawn from
     [50, 500]): the plain all-FP64 GMRES(30) + block-ILU(0) solve (whole grid,
     natural order) against the learned preconditioner (shipped model) in mixed
     precision on its base preconditioner (block-ILU(0) on element tiles), with
@@ -971,6 +975,7 @@ def solve_mode(tile, precision, matrix_free=0):
     wl.ctx.autotune(u0, ib.TUNE_RESIDUAL | ib.TUNE_ILU | ib.TUNE_ILU_FP32)
     opt = ib.default_newton_options()
     opt.precision, opt.ilu_tile, opt.gmres_max_it, opt.matrix_free = precision, tile, 20000, matrix_free
+    opt.gmres_cgs_refine = 0  # PETSc's default GMRES orthogonalisation
     u = u0.clone()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)

@@ -163,11 +163,14 @@ def select_scale(model, instance, n=256, sweeps=0, ilu_tile=0, candidates=(0.0, 
                 candidates={str(g): dict(gmres_its=v[0], s=v[1], pc_fallbacks=v[2]) for g, v in its.items()})
 
 
-def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu_tile=0, matrix_free=0):
-    """one Newton solve of an instance to |r| <= 1e-10 (GMRES(30), Wolfe line
-    search), timed with CUDA events; matrix_free = 1: the GMRES operator is
-    the residual's directional difference (the assembled Jacobian then only
-    preconditions); returns (report dict, final state)"""
+def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu_tile=0, matrix_free=0,
+          cgs_refine=0):
+    """one Newton solve of an instance to |r| <= 1e-10 (GMRES(30) with
+    PETSc's default orthogonalisation, one classical Gram-Schmidt pass per
+    step unless cgs_refine = 1; Wolfe line search), timed with CUDA events;
+    matrix_free = 1: the GMRES operator is the residual's directional
+    difference (the assembled Jacobian then only preconditions); returns
+    (report dict, final state)"""
     import torch
     dev = torch.device("cuda", device)
     opt = default_newton_options()
@@ -176,6 +179,7 @@ def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu
     opt.pc_sweeps = sweeps
     opt.ilu_tile = ilu_tile
     opt.matrix_free = matrix_free
+    opt.gmres_cgs_refine = cgs_refine
     opt.gmres_max_it = 20000
     if model is not None:
         wl.ctx.lpc_attach(model)
@@ -188,7 +192,8 @@ def solve(wl, model=None, preconditioner=2, precision=0, sweeps=1, device=0, ilu
     torch.cuda.synchronize(dev)
     if model is not None:
         wl.ctx.lpc_attach(None)
-    return dict(s=e0.elapsed_time(e1) * 1e-3, ilu_tile=ilu_tile, matrix_free=matrix_free, newton_its=rep.iterations,
+    return dict(s=e0.elapsed_time(e1) * 1e-3, ilu_tile=ilu_tile, matrix_free=matrix_free, cgs_refine=cgs_refine,
+                newton_its=rep.iterations,
                 gmres_its=rep.linear_iterations_total,
                 gmres_its_per_step=list(rep.linear_iterations[:rep.iterations]), r_final=rep.r_final,
                 converged=bool(rep.converged), pc_fallbacks=rep.pc_fallbacks), u.cpu().numpy()
